@@ -1,0 +1,919 @@
+// ft_build.cu -- HLBVH build on sm_100a: bounding box, SFC keys, onesweep radix sort of
+// (key, original index), leaf gather, Karras radix-tree topology and the bottom-up box refit
+// that also writes the traversal's node records.
+//
+// Reference pipeline: build_bvh (src/hlbvh.hpp:2165-2290) -> compute_bbox (462-572) ->
+// sfc_encode (357-423) -> oneDPL sort (2202-2232) -> gather (2266-2279) -> build_tree
+// (773-982: Karras 861-903, refit 925-969).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <vector>
+
+#include "ft_common.cuh"
+#include "ft_internal.h"
+
+namespace ft {
+
+// =========================================================================================
+// Peano-Hilbert state tables (AREPO's rottable3 / subpix3, reproduced in
+// src/sfc.peano_hilbert.hpp:332-376).  The curve is defined by these values.
+// =========================================================================================
+__constant__ uint8_t c_rot[48 * 8] = {
+    36, 28, 25, 27, 10, 10, 25, 27, 29, 11, 24, 24, 37, 11, 26, 26, 8,  8,  25, 27, 30, 38, 25, 27,
+    9,  39, 24, 24, 9,  31, 26, 26, 40, 24, 44, 32, 40, 6,  44, 6,  25, 7,  33, 7,  41, 41, 45, 45,
+    4,  42, 4,  46, 26, 42, 34, 46, 43, 43, 47, 47, 5,  27, 5,  35, 33, 35, 36, 28, 33, 35, 2,  2,
+    32, 32, 29, 3,  34, 34, 37, 3,  33, 35, 0,  0,  33, 35, 30, 38, 32, 32, 1,  39, 34, 34, 1,  31,
+    24, 42, 32, 46, 14, 42, 14, 46, 43, 43, 47, 47, 25, 15, 33, 15, 40, 12, 44, 12, 40, 26, 44, 34,
+    13, 27, 13, 35, 41, 41, 45, 45, 28, 41, 28, 22, 38, 43, 38, 22, 42, 40, 23, 23, 29, 39, 29, 39,
+    41, 36, 20, 36, 43, 30, 20, 30, 37, 31, 37, 31, 42, 40, 21, 21, 28, 18, 28, 45, 38, 18, 38, 47,
+    19, 19, 46, 44, 29, 39, 29, 39, 16, 36, 45, 36, 16, 30, 47, 30, 37, 31, 37, 31, 17, 17, 46, 44,
+    12, 4,  1,  3,  34, 34, 1,  3,  5,  35, 0,  0,  13, 35, 2,  2,  32, 32, 1,  3,  6,  14, 1,  3,
+    33, 15, 0,  0,  33, 7,  2,  2,  16, 0,  20, 8,  16, 30, 20, 30, 1,  31, 9,  31, 17, 17, 21, 21,
+    28, 18, 28, 22, 2,  18, 10, 22, 19, 19, 23, 23, 29, 3,  29, 11, 9,  11, 12, 4,  9,  11, 26, 26,
+    8,  8,  5,  27, 10, 10, 13, 27, 9,  11, 24, 24, 9,  11, 6,  14, 8,  8,  25, 15, 10, 10, 25, 7,
+    0,  18, 8,  22, 38, 18, 38, 22, 19, 19, 23, 23, 1,  39, 9,  39, 16, 36, 20, 36, 16, 2,  20, 10,
+    37, 3,  37, 11, 17, 17, 21, 21, 4,  17, 4,  46, 14, 19, 14, 46, 18, 16, 47, 47, 5,  15, 5,  15,
+    17, 12, 44, 12, 19, 6,  44, 6,  13, 7,  13, 7,  18, 16, 45, 45, 4,  42, 4,  21, 14, 42, 14, 23,
+    43, 43, 22, 20, 5,  15, 5,  15, 40, 12, 21, 12, 40, 6,  23, 6,  13, 7,  13, 7,  41, 41, 22, 20};
+__constant__ uint8_t c_sub[48 * 8] = {
+    0, 7, 1, 6, 3, 4, 2, 5, 7, 4, 6, 5, 0, 3, 1, 2, 4, 3, 5, 2, 7, 0, 6, 1, 3, 0, 2, 1, 4, 7, 5, 6,
+    1, 0, 6, 7, 2, 3, 5, 4, 0, 3, 7, 4, 1, 2, 6, 5, 3, 2, 4, 5, 0, 1, 7, 6, 2, 1, 5, 6, 3, 0, 4, 7,
+    6, 1, 7, 0, 5, 2, 4, 3, 1, 2, 0, 3, 6, 5, 7, 4, 2, 5, 3, 4, 1, 6, 0, 7, 5, 6, 4, 7, 2, 1, 3, 0,
+    7, 6, 0, 1, 4, 5, 3, 2, 6, 5, 1, 2, 7, 4, 0, 3, 5, 4, 2, 3, 6, 7, 1, 0, 4, 7, 3, 0, 5, 6, 2, 1,
+    6, 7, 5, 4, 1, 0, 2, 3, 7, 0, 4, 3, 6, 1, 5, 2, 0, 1, 3, 2, 7, 6, 4, 5, 1, 6, 2, 5, 0, 7, 3, 4,
+    2, 3, 1, 0, 5, 4, 6, 7, 3, 4, 0, 7, 2, 5, 1, 6, 4, 5, 7, 6, 3, 2, 0, 1, 5, 2, 6, 1, 4, 3, 7, 0,
+    7, 0, 6, 1, 4, 3, 5, 2, 0, 3, 1, 2, 7, 4, 6, 5, 3, 4, 2, 5, 0, 7, 1, 6, 4, 7, 5, 6, 3, 0, 2, 1,
+    6, 7, 1, 0, 5, 4, 2, 3, 7, 4, 0, 3, 6, 5, 1, 2, 4, 5, 3, 2, 7, 6, 0, 1, 5, 6, 2, 1, 4, 7, 3, 0,
+    1, 6, 0, 7, 2, 5, 3, 4, 6, 5, 7, 4, 1, 2, 0, 3, 5, 2, 4, 3, 6, 1, 7, 0, 2, 1, 3, 0, 5, 6, 4, 7,
+    0, 1, 7, 6, 3, 2, 4, 5, 1, 2, 6, 5, 0, 3, 7, 4, 2, 3, 5, 4, 1, 0, 6, 7, 3, 0, 4, 7, 2, 1, 5, 6,
+    1, 0, 2, 3, 6, 7, 5, 4, 0, 7, 3, 4, 1, 6, 2, 5, 7, 6, 4, 5, 0, 1, 3, 2, 6, 1, 5, 2, 7, 0, 4, 3,
+    5, 4, 6, 7, 2, 3, 1, 0, 4, 3, 7, 0, 5, 2, 6, 1, 3, 2, 0, 1, 4, 5, 7, 6, 2, 5, 1, 6, 3, 4, 0, 7};
+
+static constexpr int kSpinLimit = 1 << 24;
+
+size_t coord_bytes(int coord) { return (coord == F32 || coord == U32) ? 4 : 8; }
+
+static int key_words(const ft_options &o) { return (o.coord_type == U64) ? 2 : 1; }
+
+// Karras tie-break / prefix flavour: 0 Morton (clz64), 1 63-bit PH (clz64 - 1), 2 126-bit PH.
+static int delta_kind(const ft_options &o) {
+    if (o.sfc_type == MORTON) return 0;
+    return (o.coord_type == U64) ? 2 : 1;
+}
+
+size_t ref_key_bytes(const ft_options &o) {
+    if (o.sfc_type == MORTON) return 8;       // uint64 (src/sfc.morton.hpp:17)
+    return (o.coord_type == U64) ? 24 : 12;   // {hs,is,ls} of 64- or 32-bit words
+}
+
+// =========================================================================================
+// Bounding box: per-block partials, then one block folds them (two passes keep the result
+// independent of scheduling).  min: (v < m) ? v : m; max: (m < v) ? v : m, as
+// sycl::minimum / sycl::maximum.
+// =========================================================================================
+static constexpr int kBboxBlocks  = 1184; // 8 x 148 SMs
+static constexpr int kBboxThreads = 256;
+
+template <class T> FT_D void bb_fold(T *m, const T *v) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (v[2 * d] < m[2 * d]) m[2 * d] = v[2 * d];
+        if (m[2 * d + 1] < v[2 * d + 1]) m[2 * d + 1] = v[2 * d + 1];
+    }
+}
+template <class T> FT_HD void bb_identity(T *m) {
+    T lo, hi;
+    if constexpr (std::is_floating_point<T>::value) {
+        lo = std::is_same<T, float>::value ? (T)FLT_MAX : (T)DBL_MAX;
+        hi = -lo;
+    } else {
+        lo = (T)~T(0);
+        hi = 0;
+    }
+    m[0] = m[2] = m[4] = lo;
+    m[1] = m[3] = m[5] = hi;
+}
+
+template <class T> FT_D void bb_block_reduce(T *m) {
+    __shared__ T s[kBboxThreads / 32][6];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        T o[6];
+#pragma unroll
+        for (int d = 0; d < 6; ++d) o[d] = __shfl_down_sync(0xffffffffu, m[d], off);
+        bb_fold(m, o);
+    }
+    if (lane == 0)
+#pragma unroll
+        for (int d = 0; d < 6; ++d) s[w][d] = m[d];
+    __syncthreads();
+    if (w == 0) {
+        if (lane < kBboxThreads / 32)
+#pragma unroll
+            for (int d = 0; d < 6; ++d) m[d] = s[lane][d];
+        else
+            bb_identity(m);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            T o[6];
+#pragma unroll
+            for (int d = 0; d < 6; ++d) o[d] = __shfl_down_sync(0xffffffffu, m[d], off);
+            bb_fold(m, o);
+        }
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(kBboxThreads) bbox_partial_kernel(const T *__restrict__ x, const T *__restrict__ y,
+                                                                    const T *__restrict__ z, size_t n, T *partial) {
+    T m[6];
+    bb_identity(m);
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        T v[6] = {x[i], x[i], y[i], y[i], z[i], z[i]};
+        bb_fold(m, v);
+    }
+    bb_block_reduce(m);
+    if (threadIdx.x == 0)
+        for (int d = 0; d < 6; ++d) partial[blockIdx.x * 6 + d] = m[d];
+}
+
+template <class T> __global__ void __launch_bounds__(kBboxThreads) bbox_final_kernel(const T *partial, int nparts, T *out) {
+    T m[6];
+    bb_identity(m);
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x) bb_fold(m, partial + 6 * b);
+    bb_block_reduce(m);
+    if (threadIdx.x == 0)
+        for (int d = 0; d < 6; ++d) out[d] = m[d];
+}
+
+// =========================================================================================
+// SFC keys (sfc_encode, src/hlbvh.hpp:357-423).  Internal key format: lo (and hi for the
+// 126-bit Peano-Hilbert key of 42-bit integer positions).  Also writes perm = iota.
+// =========================================================================================
+FT_D unsigned long long spread3(unsigned long long x) { // src/sfc.morton.hpp:33-41
+    x &= 0x1FFFFFull;
+    x = (x | (x << 32)) & 0x1F00000000FFFFull;
+    x = (x | (x << 16)) & 0x1F0000FF0000FFull;
+    x = (x | (x << 8)) & 0x100F00F00F00F00Full;
+    x = (x | (x << 4)) & 0x10C30C30C30C30C3ull;
+    x = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+}
+
+// Peano-Hilbert key: B rounds of octant index -> table lookup (src/sfc.peano_hilbert.hpp:569-600);
+// the key register is shifted 3 bits per round (396-405).
+template <int B>
+FT_D void ph_key(unsigned long long px, unsigned long long py, unsigned long long pz, const uint8_t *rot_t,
+                 const uint8_t *sub_t, unsigned long long &hi, unsigned long long &lo) {
+    unsigned long long h = 0, l = 0;
+    unsigned           rot = 0;
+#pragma unroll 6
+    for (int b = B - 1; b >= 0; --b) {
+        unsigned pix = (unsigned)((((px >> b) & 1ull) << 2) | (((py >> b) & 1ull) << 1) | ((pz >> b) & 1ull));
+        unsigned e   = rot * 8u + pix;
+        h            = (h << 3) | (l >> 61);
+        l            = (l << 3) | sub_t[e];
+        rot          = rot_t[e];
+    }
+    hi = h;
+    lo = l;
+}
+
+template <class T> FT_D unsigned long long morton_cell(T nx) { // encode_to_sfc1d (src/hlbvh.hpp:246-271)
+    T v = add_rn(T(1), nx);
+    if constexpr (sizeof(T) == 4) return (unsigned long long)((__float_as_uint(v) & 0x007FFFFFu) >> 2);
+    else return ((unsigned long long)__double_as_longlong(v) & 0x000FFFFFFFFFFFFFull) >> 31;
+}
+template <class T> FT_D unsigned long long ph_cell(T nx) { // quantize_coord (src/sfc.peano_hilbert.hpp:472-476)
+    double b = c_fmin(__dadd_rn(1.0, (double)nx), 0x1.fffffffffffffp+0);
+    return (((unsigned long long)__double_as_longlong(b) & 0x000FFFFFFFFFFFFFull) >> 31) & 0x1FFFFFull;
+}
+
+template <class T, int SFC>
+__global__ void __launch_bounds__(256) encode_kernel(const T *__restrict__ x, const T *__restrict__ y,
+                                                     const T *__restrict__ z, size_t n, const T *__restrict__ bbox,
+                                                     unsigned long long *klo, unsigned long long *khi, uint32_t *perm) {
+    using C = Coord<T>;
+    __shared__ uint8_t s_rot[48 * 8], s_sub[48 * 8];
+    __shared__ T       s_par[9]; // min, inv per axis; upper
+    for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x) {
+        s_rot[i] = c_rot[i];
+        s_sub[i] = c_sub[i];
+    }
+    if constexpr (C::is_float) {
+        if (threadIdx.x < 3) {
+            int d    = threadIdx.x;
+            T   lo   = bbox[2 * d], hi = bbox[2 * d + 1];
+            T   dd   = sub_rn(hi, lo);
+            T   inv;
+            if constexpr (sizeof(T) == 4) inv = (dd == 0.0f) ? 0.0f : __fdiv_rn(1.0f, dd);
+            else inv = (dd == 0.0) ? 0.0 : __ddiv_rn(1.0, dd);
+            s_par[2 * d]     = lo;
+            s_par[2 * d + 1] = inv;
+        }
+    }
+    __syncthreads();
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        unsigned long long hi = 0, lo = 0;
+        if constexpr (!C::is_float) {
+            const unsigned long long mask = (1ull << C::bits) - 1ull; // 375-387
+            ph_key<C::bits>((unsigned long long)x[i] & mask, (unsigned long long)y[i] & mask,
+                            (unsigned long long)z[i] & mask, s_rot, s_sub, hi, lo);
+        } else {
+            // nx = clamp((p - min) * inv, 0, nextafter(1, 0)) in T (389-403)
+            const T upper = (sizeof(T) == 4) ? (T)0x1.fffffep-1f : (T)0x1.fffffffffffffp-1;
+            T       p[3]  = {x[i], y[i], z[i]};
+            unsigned long long c[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                T nx = c_fmin(c_fmax(mul_rn(sub_rn(p[d], s_par[2 * d]), s_par[2 * d + 1]), T(0)), upper);
+                c[d] = (SFC == MORTON) ? morton_cell(nx) : ph_cell(nx);
+            }
+            if (SFC == MORTON) lo = spread3(c[0]) | (spread3(c[1]) << 1) | (spread3(c[2]) << 2);
+            else ph_key<21>(c[0], c[1], c[2], s_rot, s_sub, hi, lo);
+        }
+        klo[i] = lo;
+        if (C::key_words == 2) khi[i] = hi;
+        perm[i] = (uint32_t)i;
+    }
+}
+
+// Key layout conversions between the reference's sfc_key and the internal (hi, lo) pair.
+// mode 0: Morton uint64; 1: {hs,is,ls} uint32; 2: {hs,is,ls} uint64.
+__global__ void keys_from_ref_kernel(const void *ref, size_t n, int mode, unsigned long long *klo,
+                                     unsigned long long *khi, uint32_t *perm) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (mode == 0) {
+            klo[i] = ((const unsigned long long *)ref)[i];
+        } else if (mode == 1) {
+            const uint32_t *w = (const uint32_t *)ref + 3 * i;
+            klo[i]            = ((unsigned long long)w[1] << 32) | w[2];
+        } else {
+            const unsigned long long *w = (const unsigned long long *)ref + 3 * i;
+            khi[i]                      = w[1];
+            klo[i]                      = w[2];
+        }
+        if (perm) perm[i] = (uint32_t)i;
+    }
+}
+
+__global__ void keys_to_ref_kernel(const unsigned long long *klo, const unsigned long long *khi, size_t n, int mode,
+                                   void *ref) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        if (mode == 0) {
+            ((unsigned long long *)ref)[i] = klo[i];
+        } else if (mode == 1) {
+            uint32_t *w = (uint32_t *)ref + 3 * i;
+            w[0]        = 0;
+            w[1]        = (uint32_t)(klo[i] >> 32);
+            w[2]        = (uint32_t)klo[i];
+        } else {
+            unsigned long long *w = (unsigned long long *)ref + 3 * i;
+            w[0]                  = 0;
+            w[1]                  = khi[i];
+            w[2]                  = klo[i];
+        }
+    }
+}
+
+// =========================================================================================
+// Onesweep LSD radix sort of (key, perm): 8-bit digits, one upfront histogram pass for all
+// digit positions, then one pass per non-constant digit.  Each pass: a tile of 256 threads x
+// ITEMS keys ranks its keys with warp match-any histograms, publishes its digit counts,
+// resolves its global offsets by decoupled look-back over preceding tiles (tiles are
+// numbered by an atomic ticket so every predecessor is running or done), stages the tile
+// in shared memory in digit order and writes each digit run contiguously.  Stable, so equal
+// keys keep their original index order.
+// =========================================================================================
+static constexpr int kSortThreads = 256;
+static constexpr int kSortWarps   = kSortThreads / 32;
+static constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kFlagMask = 3u << 30,
+                          kCountMask = (1u << 30) - 1u;
+
+template <int W> struct SortCfg {
+    static constexpr int items = (W == 1) ? 16 : 12;
+    static constexpr int tile  = kSortThreads * items;
+    static constexpr size_t smem = (size_t)tile * (8 * W + 4) + (size_t)kSortWarps * 256 * 4;
+};
+
+template <int W>
+__global__ void __launch_bounds__(256) radix_hist_kernel(const unsigned long long *__restrict__ klo,
+                                                         const unsigned long long *__restrict__ khi, size_t n,
+                                                         uint32_t *hist) {
+    constexpr int D = 8 * W;
+    __shared__ uint32_t s[D * 256];
+    for (int i = threadIdx.x; i < D * 256; i += blockDim.x) s[i] = 0;
+    __syncthreads();
+    const unsigned lane = threadIdx.x & 31;
+    const size_t   stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t base = blockIdx.x * (size_t)blockDim.x; base < n; base += stride) {
+        size_t i     = base + threadIdx.x;
+        bool   valid = i < n;
+        unsigned long long w[2] = {valid ? klo[i] : 0ull, (W == 2 && valid) ? khi[i] : 0ull};
+        unsigned active = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+            unsigned digit = (unsigned)(w[d >> 3] >> (8 * (d & 7))) & 255u;
+            unsigned peers = __match_any_sync(0xffffffffu, valid ? digit : 256u + lane);
+            if (valid && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&s[d * 256 + digit], __popc(peers & active));
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < D * 256; i += blockDim.x)
+        if (s[i]) atomicAdd(&hist[i], s[i]);
+}
+
+// Exclusive offsets per digit position; skip[d] = 1 when one digit value holds every key.
+__global__ void radix_scan_kernel(uint32_t *hist, size_t n, uint32_t *skip) {
+    __shared__ uint32_t s[256];
+    __shared__ int      s_full;
+    const int d = blockIdx.x, t = threadIdx.x;
+    uint32_t  c = hist[d * 256 + t];
+    if (t == 0) s_full = 0;
+    __syncthreads();
+    if ((size_t)c == n) s_full = 1;
+    s[t] = c;
+    __syncthreads();
+    for (int off = 1; off < 256; off <<= 1) {
+        uint32_t v = (t >= off) ? s[t - off] : 0u;
+        __syncthreads();
+        s[t] += v;
+        __syncthreads();
+    }
+    hist[d * 256 + t] = s[t] - c;
+    if (t == 0) skip[d] = (uint32_t)s_full;
+}
+
+FT_D uint32_t ld_volatile(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.volatile.global.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+FT_D void st_volatile(uint32_t *p, uint32_t v) { asm volatile("st.volatile.global.u32 [%0], %1;" ::"l"(p), "r"(v)); }
+
+template <int W>
+__global__ void __launch_bounds__(kSortThreads, 1)
+    onesweep_kernel(const unsigned long long *__restrict__ in_lo, const unsigned long long *__restrict__ in_hi,
+                    const uint32_t *__restrict__ in_v, unsigned long long *__restrict__ out_lo,
+                    unsigned long long *__restrict__ out_hi, uint32_t *__restrict__ out_v, size_t n, int word,
+                    int shift, const uint32_t *__restrict__ offsets, uint32_t *lookback, uint32_t *tile_counter,
+                    uint32_t *status) {
+    using Cfg           = SortCfg<W>;
+    constexpr int ITEMS = Cfg::items;
+    constexpr int TILE  = Cfg::tile;
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned long long *s_lo = reinterpret_cast<unsigned long long *>(smem);
+    unsigned long long *s_hi = s_lo + TILE; // only used when W == 2
+    uint32_t           *s_v  = reinterpret_cast<uint32_t *>(s_lo + (size_t)TILE * W);
+    uint32_t           *s_wh = s_v + TILE; // [warp][256]
+    __shared__ uint32_t s_tile_excl[256];
+    __shared__ uint32_t s_base[256];
+    __shared__ uint32_t s_ticket;
+    __shared__ uint32_t s_wsum[kSortWarps];
+
+    const int      tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    if (tid == 0) s_ticket = atomicAdd(tile_counter, 1u);
+    for (int i = tid; i < kSortWarps * 256; i += kSortThreads) s_wh[i] = 0;
+    __syncthreads();
+    const size_t tile = s_ticket;
+    const size_t base = tile * (size_t)TILE;
+
+    unsigned long long klo[ITEMS], khi[ITEMS];
+    uint32_t           val[ITEMS], dig[ITEMS], rank[ITEMS];
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        size_t pos   = base + (size_t)warp * 32 * ITEMS + (size_t)i * 32 + lane;
+        bool   valid = pos < n;
+        klo[i]       = valid ? in_lo[pos] : 0ull;
+        khi[i]       = (W == 2 && valid) ? in_hi[pos] : 0ull;
+        val[i]       = valid ? in_v[pos] : 0u;
+        unsigned long long w = (W == 2 && word == 1) ? khi[i] : klo[i];
+        dig[i]       = valid ? (uint32_t)(w >> shift) & 255u : 256u + lane;
+    }
+    uint32_t *wh = s_wh + warp * 256;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        unsigned peers = __match_any_sync(0xffffffffu, dig[i]);
+        bool     valid = dig[i] < 256u;
+        uint32_t before = valid ? wh[dig[i]] : 0u;
+        __syncwarp();
+        if (valid && lane == __ffs(peers) - 1) wh[dig[i]] = before + __popc(peers);
+        __syncwarp();
+        rank[i] = before + __popc(peers & lt_mask);
+    }
+    __syncthreads();
+
+    // per-digit: warp exclusive prefixes and the tile count
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) {
+        uint32_t c            = s_wh[w * 256 + tid];
+        s_wh[w * 256 + tid]   = run;
+        run += c;
+    }
+    const uint32_t tile_count = run;
+
+    // exclusive scan of tile counts over digits (block scan, 256 threads)
+    uint32_t incl = tile_count;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        uint32_t v = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl += v;
+    }
+    if (lane == 31) s_wsum[warp] = incl;
+    __syncthreads();
+    uint32_t wpre = 0;
+    for (int w = 0; w < warp; ++w) wpre += s_wsum[w];
+    s_tile_excl[tid] = wpre + incl - tile_count;
+
+    // decoupled look-back for digit tid
+    uint32_t *lb     = lookback + tile * 256;
+    uint32_t  prefix = 0;
+    if (tile == 0) {
+        st_volatile(lb + tid, kFlagInc | tile_count);
+    } else {
+        st_volatile(lb + tid, kFlagAgg | tile_count);
+        for (long long j = (long long)tile - 1; j >= 0; --j) {
+            uint32_t s;
+            int      spins = 0;
+            for (;;) {
+                s = ld_volatile(lookback + (size_t)j * 256 + tid);
+                if (s & kFlagMask) break;
+                if (++spins > 64) __nanosleep(32);
+                if (spins > kSpinLimit) break;
+            }
+            if (!(s & kFlagMask)) {
+                atomicOr(status, STATUS_SPIN_LIMIT);
+                break;
+            }
+            prefix += s & kCountMask;
+            if (s & kFlagInc) break;
+        }
+        st_volatile(lb + tid, kFlagInc | (prefix + tile_count));
+    }
+    s_base[tid] = offsets[tid] + prefix;
+    __syncthreads();
+
+    // stage the tile in digit order
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) {
+        if (dig[i] < 256u) {
+            uint32_t lp = s_tile_excl[dig[i]] + s_wh[warp * 256 + dig[i]] + rank[i];
+            s_lo[lp]    = klo[i];
+            if (W == 2) s_hi[lp] = khi[i];
+            s_v[lp] = val[i];
+        }
+    }
+    __syncthreads();
+    const int tile_n = (int)min((size_t)TILE, n - base);
+    for (int j = tid; j < tile_n; j += kSortThreads) {
+        unsigned long long lo = s_lo[j];
+        unsigned long long hi = (W == 2) ? s_hi[j] : 0ull;
+        unsigned long long w  = (W == 2 && word == 1) ? hi : lo;
+        uint32_t           d  = (uint32_t)(w >> shift) & 255u;
+        size_t             gp = (size_t)s_base[d] + (size_t)(j - (int)s_tile_excl[d]);
+        out_lo[gp]            = lo;
+        if (W == 2) out_hi[gp] = hi;
+        out_v[gp] = s_v[j];
+    }
+}
+
+// =========================================================================================
+// Leaf gather (src/hlbvh.hpp:2266-2279): leaf slot n-1+i <- input point perm[i].
+// =========================================================================================
+template <class T>
+__global__ void gather_kernel(const T *__restrict__ x, const T *__restrict__ y, const T *__restrict__ z,
+                              const uint32_t *__restrict__ perm, size_t n, const uint32_t *__restrict__ id,
+                              const int8_t *__restrict__ ghost, T *mnx, T *mxx, T *mny, T *mxy, T *mnz, T *mxz,
+                              uint32_t *tid_out, int8_t *ghost_out, int32_t *orig_out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        uint32_t src  = perm[i];
+        size_t   leaf = i + n - 1;
+        T        a = x[src], b = y[src], c = z[src];
+        mnx[leaf] = a;
+        mxx[leaf] = a;
+        mny[leaf] = b;
+        mxy[leaf] = b;
+        mnz[leaf] = c;
+        mxz[leaf] = c;
+        tid_out[leaf]   = id ? id[src] : src;
+        ghost_out[leaf] = ghost ? ghost[src] : (int8_t)0;
+        orig_out[leaf]  = (int32_t)src;
+    }
+}
+
+// Leaf init of build_tree with caller arrays (src/hlbvh.hpp:906-923).
+template <class T>
+__global__ void leaf_init_kernel(const T *sx, const T *sy, const T *sz, size_t n, const uint32_t *sid,
+                                 const int8_t *sghost, const int32_t *sorig, T *mnx, T *mxx, T *mny, T *mxy,
+                                 T *mnz, T *mxz, uint32_t *tid_out, int8_t *ghost_out, int32_t *orig_out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        size_t leaf = i + n - 1;
+        mnx[leaf] = mxx[leaf] = sx[i];
+        mny[leaf] = mxy[leaf] = sy[i];
+        mnz[leaf] = mxz[leaf] = sz[i];
+        if (sid) tid_out[leaf] = sid[i];
+        if (sghost) ghost_out[leaf] = sghost[i];
+        if (sorig) orig_out[leaf] = sorig[i];
+    }
+}
+
+// =========================================================================================
+// Karras 2012 radix-tree topology (src/hlbvh.hpp:852-903).  delta() is the common prefix
+// length of two sorted keys (get_common_prefix_length, 283-340), with the index tie-break
+// for equal keys.
+// =========================================================================================
+template <int KIND> struct Delta {
+    const unsigned long long *lo, *hi;
+    int                       n;
+    unsigned long long        ilo, ihi;
+    int                       i;
+    FT_D int operator()(int j) const {
+        if (j < 0 || j >= n) return -1;
+        unsigned long long jlo = lo[j];
+        if (KIND == 2) {
+            unsigned long long jhi = hi[j];
+            if (jhi != ihi) return clz64(jhi ^ ihi) - 2;
+            if (jlo != ilo) return 62 + clz64(jlo ^ ilo);
+        } else {
+            if (jlo != ilo) return clz64(jlo ^ ilo) - (KIND == 1 ? 1 : 0);
+        }
+        return (KIND == 2 ? 126 : 63) + clz64((unsigned long long)(long long)i ^ (unsigned long long)(long long)j);
+    }
+};
+
+FT_D int sgn(int v) { return (v > 0) - (v < 0); }
+
+template <int KIND>
+__global__ void __launch_bounds__(256) karras_kernel(const unsigned long long *__restrict__ klo,
+                                                     const unsigned long long *__restrict__ khi, int n,
+                                                     int32_t *left, int32_t *right, int32_t *parent) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x) {
+        Delta<KIND> delta{klo, khi, n, klo[i], KIND == 2 ? khi[i] : 0ull, i};
+        int d         = sgn(delta(i + 1) - delta(i - 1));
+        int delta_min = delta(i - d);
+        int l_max     = 2;
+        while (delta(i + l_max * d) > delta_min) l_max *= 2;
+        int l = 0;
+        for (int t = l_max / 2; t >= 1; t /= 2)
+            if (delta(i + (l + t) * d) > delta_min) l += t;
+        int j          = i + l * d;
+        int delta_node = delta(j);
+        int s          = 0;
+        int t_split    = 1;
+        while (t_split <= l) t_split *= 2;
+        t_split /= 2;
+        for (int t = t_split; t >= 1; t /= 2)
+            if (s + t < l && delta(i + (s + t) * d) > delta_node) s += t;
+        int split = i + s * d + min(d, 0);
+        int lc    = (min(i, j) == split) ? split + n - 1 : split;
+        int rc    = (max(i, j) == split + 1) ? split + 1 + n - 1 : split + 1;
+        left[i]   = lc;
+        right[i]  = rc;
+        parent[lc] = i;
+        parent[rc] = i;
+    }
+}
+
+// =========================================================================================
+// Bottom-up refit (src/hlbvh.hpp:925-969): one thread per leaf climbs; at each parent the
+// first arrival stops and the second merges both child boxes.  The merge also writes the
+// traversal record (both child boxes + indices) and the subtree height.  Child boxes that
+// other threads wrote in this launch are read through L2 (ld.cg) after the acquire fence.
+// =========================================================================================
+template <class T> FT_D void load_box_cg(const T *const *soa, int node, T b[6]) {
+#pragma unroll
+    for (int d = 0; d < 6; ++d) b[d] = __ldcg(soa[d] + node);
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) refit_kernel(int n, const int32_t *__restrict__ left,
+                                                    const int32_t *__restrict__ right,
+                                                    const int32_t *__restrict__ parent, T *mnx, T *mxx, T *mny,
+                                                    T *mxy, T *mnz, T *mxz, NodeRec<T> *recs, uint8_t *height,
+                                                    int32_t *counters) {
+    const T *soa[6] = {mnx, mxx, mny, mxy, mnz, mxz};
+    T       *soa_w[6] = {mnx, mxx, mny, mxy, mnz, mxz};
+    for (int leaf = blockIdx.x * blockDim.x + threadIdx.x; leaf < n; leaf += gridDim.x * blockDim.x) {
+        int curr = leaf + n - 1;
+        while (curr != 0) {
+            int p = parent[curr];
+            if (p < 0 || p >= n - 1) break;
+            __threadfence();
+            if (atomicAdd(&counters[p], 1) == 0) break;
+            __threadfence();
+            int l = left[p], r = right[p];
+            T   lb[6], rb[6];
+            load_box_cg(soa, l, lb);
+            load_box_cg(soa, r, rb);
+            int hl = (l >= n - 1) ? 0 : (int)__ldcg(height + l);
+            int hr = (r >= n - 1) ? 0 : (int)__ldcg(height + r);
+            T   pb[6];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                pb[2 * d]     = box_min(lb[2 * d], rb[2 * d]);
+                pb[2 * d + 1] = box_max(lb[2 * d + 1], rb[2 * d + 1]);
+            }
+#pragma unroll
+            for (int d = 0; d < 6; ++d) __stcg(soa_w[d] + p, pb[d]);
+            NodeRec<T> rec;
+#pragma unroll
+            for (int d = 0; d < 6; ++d) {
+                rec.lb[d] = lb[d];
+                rec.rb[d] = rb[d];
+            }
+            rec.l = l;
+            rec.r = r;
+#pragma unroll
+            for (int d = 0; d < (int)(sizeof(rec.pad) / 4); ++d) rec.pad[d] = 0;
+            recs[p] = rec;
+            int h   = 1 + max(hl, hr);
+            __stcg(height + p, (uint8_t)min(h, 255));
+            curr = p;
+        }
+    }
+}
+
+// =========================================================================================
+// Host orchestration
+// =========================================================================================
+static int grid_for(size_t n, int threads, int max_blocks = 148 * 16) {
+    size_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    return (int)std::min<size_t>(b, (size_t)max_blocks);
+}
+
+template <class T> static void *alloc_dev(size_t count) {
+    void *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(FT_ERR_OUT_OF_MEMORY, "cudaMalloc of build scratch failed");
+    }
+    return p;
+}
+
+void free_scratch(TreeImpl &s) {
+    void *ptrs[] = {s.recs, s.height, s.counters, s.key_lo, s.key_hi, s.tmp_lo, s.tmp_hi, s.perm, s.tmp_perm,
+                    s.bbox, s.bbox_partial, s.hist, s.lookback, s.tile_counter, s.status};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    int coord = s.coord;
+    s         = TreeImpl{};
+    s.coord   = coord;
+}
+
+static size_t sort_tiles(size_t n, int W) {
+    size_t tile = (W == 1) ? SortCfg<1>::tile : SortCfg<2>::tile;
+    return (n + tile - 1) / tile;
+}
+
+void ensure_scratch(TreeImpl &s, const ft_options &o, size_t n) {
+    if (n <= s.cap && s.key_lo) return;
+    free_scratch(s);
+    size_t cap = n + n / 2 + 1024;
+    int    W   = key_words(o);
+    size_t cb  = coord_bytes(o.coord_type);
+    s.coord    = o.coord_type;
+    s.cap      = cap;
+    s.recs     = alloc_dev<unsigned char>((cap > 1 ? cap - 1 : 1) * 16 * cb);
+    s.height   = (uint8_t *)alloc_dev<uint8_t>(cap);
+    s.counters = (int32_t *)alloc_dev<int32_t>(cap);
+    s.key_lo   = (uint64_t *)alloc_dev<uint64_t>(cap);
+    s.tmp_lo   = (uint64_t *)alloc_dev<uint64_t>(cap);
+    if (W == 2) {
+        s.key_hi = (uint64_t *)alloc_dev<uint64_t>(cap);
+        s.tmp_hi = (uint64_t *)alloc_dev<uint64_t>(cap);
+    }
+    s.perm         = (uint32_t *)alloc_dev<uint32_t>(cap);
+    s.tmp_perm     = (uint32_t *)alloc_dev<uint32_t>(cap);
+    s.bbox         = alloc_dev<uint64_t>(6);
+    s.bbox_partial = alloc_dev<uint64_t>((size_t)kBboxBlocks * 6);
+    s.hist         = (uint32_t *)alloc_dev<uint32_t>(16 * 256 + 16);
+    s.lookback_words = 16 * sort_tiles(cap, W) * 256;
+    s.lookback     = (uint32_t *)alloc_dev<uint32_t>(s.lookback_words);
+    s.tile_counter = (uint32_t *)alloc_dev<uint32_t>(16);
+    s.status       = (uint32_t *)alloc_dev<uint32_t>(4);
+    FT_CUDA(cudaMemset(s.status, 0, 16));
+}
+
+template <class T>
+static void bbox_typed(const void *x, const void *y, const void *z, size_t n, void *partial, void *out,
+                       cudaStream_t st) {
+    int blocks = grid_for(n, kBboxThreads, kBboxBlocks);
+    bbox_partial_kernel<T><<<blocks, kBboxThreads, 0, st>>>((const T *)x, (const T *)y, (const T *)z, n, (T *)partial);
+    bbox_final_kernel<T><<<1, kBboxThreads, 0, st>>>((const T *)partial, blocks, (T *)out);
+    FT_CUDA(cudaGetLastError());
+}
+
+void compute_bbox(Context &ctx, TreeImpl *scratch, const void *x, const void *y, const void *z, size_t n,
+                  void *bbox_dev, cudaStream_t st) {
+    void *partial = scratch->bbox_partial;
+    switch (ctx.opts.coord_type) {
+    case F32: bbox_typed<float>(x, y, z, n, partial, bbox_dev, st); break;
+    case F64: bbox_typed<double>(x, y, z, n, partial, bbox_dev, st); break;
+    case U32: bbox_typed<uint32_t>(x, y, z, n, partial, bbox_dev, st); break;
+    case U64: bbox_typed<unsigned long long>(x, y, z, n, partial, bbox_dev, st); break;
+    }
+}
+
+template <class T>
+static void encode_typed(const ft_options &o, const void *x, const void *y, const void *z, size_t n,
+                         const void *bbox, TreeImpl &s, cudaStream_t st) {
+    int blocks = grid_for(n, 256);
+    if (o.sfc_type == MORTON)
+        encode_kernel<T, MORTON><<<blocks, 256, 0, st>>>((const T *)x, (const T *)y, (const T *)z, n,
+                                                         (const T *)bbox, (unsigned long long *)s.key_lo,
+                                                         (unsigned long long *)s.key_hi, s.perm);
+    else
+        encode_kernel<T, PEANO_HILBERT><<<blocks, 256, 0, st>>>((const T *)x, (const T *)y, (const T *)z, n,
+                                                                (const T *)bbox, (unsigned long long *)s.key_lo,
+                                                                (unsigned long long *)s.key_hi, s.perm);
+    FT_CUDA(cudaGetLastError());
+}
+
+static void encode(const ft_options &o, const void *x, const void *y, const void *z, size_t n, const void *bbox,
+                   TreeImpl &s, cudaStream_t st) {
+    switch (o.coord_type) {
+    case F32: encode_typed<float>(o, x, y, z, n, bbox, s, st); break;
+    case F64: encode_typed<double>(o, x, y, z, n, bbox, s, st); break;
+    case U32: encode_typed<uint32_t>(o, x, y, z, n, bbox, s, st); break;
+    case U64: encode_typed<unsigned long long>(o, x, y, z, n, bbox, s, st); break;
+    }
+}
+
+static int ref_key_mode(const ft_options &o) {
+    if (o.sfc_type == MORTON) return 0;
+    return (o.coord_type == U64) ? 2 : 1;
+}
+
+void sfc_encode_ref_layout(Context &ctx, TreeImpl &s, const void *x, const void *y, const void *z, size_t n,
+                           const void *bbox_dev, void *keys_ref_dev, cudaStream_t st) {
+    encode(ctx.opts, x, y, z, n, bbox_dev, s, st);
+    keys_to_ref_kernel<<<grid_for(n, 256), 256, 0, st>>>((const unsigned long long *)s.key_lo,
+                                                          (const unsigned long long *)s.key_hi, n,
+                                                          ref_key_mode(ctx.opts), keys_ref_dev);
+    FT_CUDA(cudaGetLastError());
+}
+
+template <int W> static void sort_impl(TreeImpl &s, size_t n, cudaStream_t st) {
+    using Cfg     = SortCfg<W>;
+    const int D   = 8 * W;
+    size_t tiles  = (n + Cfg::tile - 1) / Cfg::tile;
+    FT_CUDA(cudaMemsetAsync(s.hist, 0, (16 * 256 + 16) * sizeof(uint32_t), st));
+    radix_hist_kernel<W><<<grid_for(n, 256, 148 * 4), 256, 0, st>>>((const unsigned long long *)s.key_lo,
+                                                                      (const unsigned long long *)s.key_hi, n,
+                                                                      s.hist);
+    uint32_t *skip_dev = s.hist + 16 * 256;
+    radix_scan_kernel<<<D, 256, 0, st>>>(s.hist, n, skip_dev);
+    FT_CUDA(cudaGetLastError());
+    uint32_t skip[16] = {0};
+    FT_CUDA(cudaMemcpyAsync(skip, skip_dev, D * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    FT_CUDA(cudaStreamSynchronize(st));
+    FT_CUDA(cudaMemsetAsync(s.lookback, 0, (size_t)D * tiles * 256 * sizeof(uint32_t), st));
+    FT_CUDA(cudaMemsetAsync(s.tile_counter, 0, 16 * sizeof(uint32_t), st));
+    static bool attr_set = false;
+    if (!attr_set) {
+        FT_CUDA(cudaFuncSetAttribute(onesweep_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem));
+    }
+    for (int d = 0; d < D; ++d) {
+        if (skip[d]) continue;
+        int word  = d >> 3;
+        int shift = 8 * (d & 7);
+        onesweep_kernel<W><<<(unsigned)tiles, kSortThreads, Cfg::smem, st>>>(
+            (const unsigned long long *)s.key_lo, (const unsigned long long *)s.key_hi, s.perm,
+            (unsigned long long *)s.tmp_lo, (unsigned long long *)s.tmp_hi, s.tmp_perm, n, word, shift,
+            s.hist + d * 256, s.lookback + (size_t)d * tiles * 256, s.tile_counter + d, s.status);
+        FT_CUDA(cudaGetLastError());
+        std::swap(s.key_lo, s.tmp_lo);
+        std::swap(s.key_hi, s.tmp_hi);
+        std::swap(s.perm, s.tmp_perm);
+    }
+}
+
+static void sort_keys(const ft_options &o, TreeImpl &s, size_t n, cudaStream_t st) {
+    if (n < 2) return;
+    if (key_words(o) == 1) sort_impl<1>(s, n, st);
+    else sort_impl<2>(s, n, st);
+}
+
+template <class T> struct SoA {
+    T *mnx, *mxx, *mny, *mxy, *mnz, *mxz;
+    explicit SoA(const ft_tree &t)
+        : mnx((T *)t.min_x), mxx((T *)t.max_x), mny((T *)t.min_y), mxy((T *)t.max_y), mnz((T *)t.min_z),
+          mxz((T *)t.max_z) {}
+};
+
+template <class T>
+static void topology_and_refit(const ft_options &o, ft_tree &t, TreeImpl &s, size_t n, cudaStream_t st) {
+    if (n < 2) {
+        s.height_root = 0;
+        return;
+    }
+    FT_CUDA(cudaMemsetAsync(t.parent, 0xFF, (2 * n - 1) * sizeof(int32_t), st)); // -1 (849)
+    int blocks = grid_for(n, 256, 148 * 32);
+    const unsigned long long *lo = (const unsigned long long *)s.key_lo, *hi = (const unsigned long long *)s.key_hi;
+    switch (delta_kind(o)) {
+    case 0: karras_kernel<0><<<blocks, 256, 0, st>>>(lo, hi, (int)n, t.left_child, t.right_child, t.parent); break;
+    case 1: karras_kernel<1><<<blocks, 256, 0, st>>>(lo, hi, (int)n, t.left_child, t.right_child, t.parent); break;
+    default: karras_kernel<2><<<blocks, 256, 0, st>>>(lo, hi, (int)n, t.left_child, t.right_child, t.parent); break;
+    }
+    FT_CUDA(cudaGetLastError());
+    FT_CUDA(cudaMemsetAsync(s.counters, 0, (n - 1) * sizeof(int32_t), st));
+    SoA<T> a(t);
+    refit_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, t.parent, a.mnx, a.mxx, a.mny,
+                                            a.mxy, a.mnz, a.mxz, (NodeRec<T> *)s.recs, s.height, s.counters);
+    FT_CUDA(cudaGetLastError());
+}
+
+template <class T>
+static void build_bvh_typed(Context &ctx, ft_tree &t, const void *x, const void *y, const void *z, size_t n,
+                            const uint32_t *id, const int8_t *ghost, const void *bbox_host, void *caller_keys,
+                            cudaStream_t st) {
+    TreeImpl &s = *(TreeImpl *)t.impl;
+    ensure_scratch(s, ctx.opts, n);
+    // 1. bounding box (only the float encode reads it)
+    if (bbox_host) FT_CUDA(cudaMemcpyAsync(s.bbox, bbox_host, 6 * sizeof(T), cudaMemcpyHostToDevice, st));
+    else compute_bbox(ctx, &s, x, y, z, n, s.bbox, st);
+    // 2. keys + iota permutation
+    if (caller_keys) {
+        keys_from_ref_kernel<<<grid_for(n, 256), 256, 0, st>>>(caller_keys, n, ref_key_mode(ctx.opts),
+                                                               (unsigned long long *)s.key_lo,
+                                                               (unsigned long long *)s.key_hi, s.perm);
+        FT_CUDA(cudaGetLastError());
+    } else {
+        encode(ctx.opts, x, y, z, n, s.bbox, s, st);
+    }
+    // 3. sort (key, perm)
+    sort_keys(ctx.opts, s, n, st);
+    if (caller_keys) {
+        keys_to_ref_kernel<<<grid_for(n, 256), 256, 0, st>>>((const unsigned long long *)s.key_lo,
+                                                              (const unsigned long long *)s.key_hi, n,
+                                                              ref_key_mode(ctx.opts), caller_keys);
+        FT_CUDA(cudaGetLastError());
+    }
+    // 4. gather into leaf slots; internal slots of id / is_ghost / orig_idx are zeroed
+    SoA<T> a(t);
+    if (n > 1) {
+        FT_CUDA(cudaMemsetAsync(t.id, 0, (n - 1) * sizeof(uint32_t), st));
+        FT_CUDA(cudaMemsetAsync(t.is_ghost, 0, (n - 1) * sizeof(int8_t), st));
+        FT_CUDA(cudaMemsetAsync(t.orig_idx, 0, (n - 1) * sizeof(int32_t), st));
+    }
+    gather_kernel<T><<<grid_for(n, 256), 256, 0, st>>>((const T *)x, (const T *)y, (const T *)z, s.perm, n, id, ghost,
+                                                       a.mnx, a.mxx, a.mny, a.mxy, a.mnz, a.mxz, t.id, t.is_ghost,
+                                                       t.orig_idx);
+    FT_CUDA(cudaGetLastError());
+    if (n == 1) FT_CUDA(cudaMemsetAsync(t.parent, 0xFF, sizeof(int32_t), st));
+    // 5. topology + refit
+    topology_and_refit<T>(ctx.opts, t, s, n, st);
+}
+
+void build_bvh(Context &ctx, ft_tree &t, const void *x, const void *y, const void *z, size_t n, const uint32_t *id,
+               const int8_t *ghost, const void *bbox_host, void *caller_keys, cudaStream_t st) {
+    switch (ctx.opts.coord_type) {
+    case F32: build_bvh_typed<float>(ctx, t, x, y, z, n, id, ghost, bbox_host, caller_keys, st); break;
+    case F64: build_bvh_typed<double>(ctx, t, x, y, z, n, id, ghost, bbox_host, caller_keys, st); break;
+    case U32: build_bvh_typed<uint32_t>(ctx, t, x, y, z, n, id, ghost, bbox_host, caller_keys, st); break;
+    case U64: build_bvh_typed<unsigned long long>(ctx, t, x, y, z, n, id, ghost, bbox_host, caller_keys, st); break;
+    }
+}
+
+template <class T>
+static void build_tree_typed(Context &ctx, ft_tree &t, const void *keys_ref, const void *sx, const void *sy,
+                             const void *sz, const uint32_t *sid, const int8_t *sghost, const int32_t *sorig,
+                             cudaStream_t st) {
+    TreeImpl &s = *(TreeImpl *)t.impl;
+    size_t    n = t.num_leaves;
+    ensure_scratch(s, ctx.opts, n);
+    keys_from_ref_kernel<<<grid_for(n, 256), 256, 0, st>>>(keys_ref, n, ref_key_mode(ctx.opts),
+                                                           (unsigned long long *)s.key_lo,
+                                                           (unsigned long long *)s.key_hi, nullptr);
+    FT_CUDA(cudaGetLastError());
+    SoA<T> a(t);
+    if (sx && sy && sz)
+        leaf_init_kernel<T><<<grid_for(n, 256), 256, 0, st>>>((const T *)sx, (const T *)sy, (const T *)sz, n, sid,
+                                                              sghost, sorig, a.mnx, a.mxx, a.mny, a.mxy, a.mnz,
+                                                              a.mxz, t.id, t.is_ghost, t.orig_idx);
+    FT_CUDA(cudaGetLastError());
+    if (n == 1) FT_CUDA(cudaMemsetAsync(t.parent, 0xFF, sizeof(int32_t), st));
+    topology_and_refit<T>(ctx.opts, t, s, n, st);
+}
+
+void build_tree_from_keys(Context &ctx, ft_tree &t, const void *keys_ref, const void *sx, const void *sy,
+                          const void *sz, const uint32_t *sid, const int8_t *sghost, const int32_t *sorig,
+                          cudaStream_t st) {
+    switch (ctx.opts.coord_type) {
+    case F32: build_tree_typed<float>(ctx, t, keys_ref, sx, sy, sz, sid, sghost, sorig, st); break;
+    case F64: build_tree_typed<double>(ctx, t, keys_ref, sx, sy, sz, sid, sghost, sorig, st); break;
+    case U32: build_tree_typed<uint32_t>(ctx, t, keys_ref, sx, sy, sz, sid, sghost, sorig, st); break;
+    case U64: build_tree_typed<unsigned long long>(ctx, t, keys_ref, sx, sy, sz, sid, sghost, sorig, st); break;
+    }
+}
+
+} // namespace ft

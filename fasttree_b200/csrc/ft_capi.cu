@@ -1,0 +1,480 @@
+// ft_capi.cu -- the extern "C" boundary (include/fasttree_b200.h): argument checks, host
+// pointer staging, tree allocation and error mapping around the build and query kernels.
+#include <cuda_runtime.h>
+
+#include <climits>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "ft_common.cuh"
+#include "ft_internal.h"
+
+namespace ft {
+
+static thread_local std::string g_last_error;
+
+void fail(ft_status s, const std::string &msg) { throw Error{s, msg}; }
+
+void check_cuda(cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return;
+    cudaGetLastError();
+    ft_status s = (e == cudaErrorMemoryAllocation) ? FT_ERR_OUT_OF_MEMORY : FT_ERR_CUDA;
+    fail(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Makes ctx->device current for the duration of a call and restores the caller's device.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        FT_CUDA(cudaGetDevice(&prev));
+        if (prev != dev) FT_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (cudaGetDevice(&cur) == cudaSuccess && prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// Host pointer check: the reference stages exactly the pointers that are not USM
+// allocations (sycl::usm::alloc::unknown, src/hlbvh.hpp:131-137); here, pointers the CUDA
+// runtime does not know (pageable host memory).
+static bool is_host_only(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    cudaError_t           e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered;
+}
+
+// Stream-ordered staging of one host buffer (ensure_device_readable / _writable and
+// copy_back_and_free, src/hlbvh.hpp:125-200).
+struct Staged {
+    void        *host  = nullptr;
+    void        *dev   = nullptr;
+    size_t       bytes = 0;
+    bool         owned = false;
+    bool         out   = false;
+    cudaStream_t st    = nullptr;
+    Staged()           = default;
+    Staged(const Staged &) = delete;
+    Staged &operator=(const Staged &) = delete;
+    void init(const void *p, size_t nbytes, bool readable, bool writable, cudaStream_t s) {
+        host  = const_cast<void *>(p);
+        bytes = nbytes;
+        st    = s;
+        out   = writable;
+        if (!p || nbytes == 0 || !is_host_only(p)) {
+            dev = host;
+            return;
+        }
+        FT_CUDA(cudaMallocAsync(&dev, nbytes, st));
+        owned = true;
+        if (readable) FT_CUDA(cudaMemcpyAsync(dev, p, nbytes, cudaMemcpyHostToDevice, st));
+    }
+    void copy_back() {
+        if (owned && out) FT_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, st));
+    }
+    ~Staged() {
+        if (owned) cudaFreeAsync(dev, st);
+    }
+};
+
+static void validate_options(const ft_options &o) {
+    if (o.coord_type < F32 || o.coord_type > U64) fail(FT_ERR_INVALID_ARGUMENT, "unknown coord_type");
+    if (o.sfc_type != MORTON && o.sfc_type != PEANO_HILBERT) fail(FT_ERR_INVALID_ARGUMENT, "unknown sfc_type");
+    if (o.sfc_type == MORTON && (o.coord_type == U32 || o.coord_type == U64))
+        fail(FT_ERR_INVALID_ARGUMENT, "Morton keys are defined for floating-point coordinates only");
+}
+
+static void check_status_word(TreeImpl &s, cudaStream_t st) {
+    uint32_t v = 0;
+    FT_CUDA(cudaMemcpyAsync(&v, s.status, sizeof(v), cudaMemcpyDeviceToHost, st));
+    FT_CUDA(cudaStreamSynchronize(st));
+    if (v) {
+        FT_CUDA(cudaMemsetAsync(s.status, 0, sizeof(uint32_t), st));
+        fail(FT_ERR_TIMEOUT, "a bounded device-side wait gave up (radix-sort look-back)");
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Tree storage
+// ---------------------------------------------------------------------------------------
+static void tree_free_arrays(ft_tree &t) {
+    void *ptrs[] = {t.min_x, t.max_x, t.min_y, t.max_y, t.min_z, t.max_z, t.left_child,
+                    t.right_child, t.parent, t.id, t.is_ghost, t.orig_idx};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    t.min_x = t.max_x = t.min_y = t.max_y = t.min_z = t.max_z = nullptr;
+    t.left_child = t.right_child = t.parent = nullptr;
+    t.id                                    = nullptr;
+    t.is_ghost                              = nullptr;
+    t.orig_idx                              = nullptr;
+    t.capacity                              = 0;
+}
+
+static void *tree_alloc(size_t bytes, bool managed) {
+    void *p = nullptr;
+    if (bytes == 0) return nullptr;
+    cudaError_t e = managed ? cudaMallocManaged(&p, bytes) : cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        fail(FT_ERR_OUT_OF_MEMORY, "tree allocation failed");
+    }
+    return p;
+}
+
+static void tree_alloc_arrays(Context &ctx, ft_tree &t, size_t cap) {
+    bool   m   = ctx.opts.host_readable_tree != 0;
+    size_t tot = cap > 0 ? 2 * cap - 1 : 0;
+    size_t ni  = cap > 0 ? cap - 1 : 0;
+    size_t cb  = coord_bytes(ctx.opts.coord_type);
+    try {
+        t.min_x       = tree_alloc(tot * cb, m);
+        t.max_x       = tree_alloc(tot * cb, m);
+        t.min_y       = tree_alloc(tot * cb, m);
+        t.max_y       = tree_alloc(tot * cb, m);
+        t.min_z       = tree_alloc(tot * cb, m);
+        t.max_z       = tree_alloc(tot * cb, m);
+        t.left_child  = (int32_t *)tree_alloc(ni * 4, m);
+        t.right_child = (int32_t *)tree_alloc(ni * 4, m);
+        t.parent      = (int32_t *)tree_alloc(tot * 4, m);
+        t.id          = (uint32_t *)tree_alloc(tot * 4, m);
+        t.is_ghost    = (int8_t *)tree_alloc(tot, m);
+        t.orig_idx    = (int32_t *)tree_alloc(tot * 4, m);
+    } catch (...) {
+        tree_free_arrays(t);
+        throw;
+    }
+    t.capacity = cap;
+}
+
+} // namespace ft
+
+using namespace ft;
+
+struct ft_context : public ft::Context {};
+
+#define FT_API_BEGIN try {
+#define FT_API_END                                                                                \
+    }                                                                                             \
+    catch (const ft::Error &e) {                                                                  \
+        ft::g_last_error = e.msg;                                                                 \
+        return e.status;                                                                          \
+    }                                                                                             \
+    catch (const std::bad_alloc &) {                                                              \
+        ft::g_last_error = "host allocation failed";                                              \
+        return FT_ERR_OUT_OF_MEMORY;                                                              \
+    }                                                                                             \
+    catch (...) {                                                                                 \
+        ft::g_last_error = "unknown error";                                                       \
+        return FT_ERR_RUNTIME;                                                                    \
+    }                                                                                             \
+    return FT_OK;
+
+static void need(bool c, const char *msg) {
+    if (!c) fail(FT_ERR_INVALID_ARGUMENT, msg);
+}
+
+extern "C" {
+
+const char *ft_last_error(void) { return ft::g_last_error.c_str(); }
+
+int ft_version(void) { return 10000; }
+
+ft_status ft_context_create(const ft_options *opts, int device, ft_context **out) {
+    FT_API_BEGIN
+    need(opts && out, "null argument");
+    validate_options(*opts);
+    int count = 0;
+    FT_CUDA(cudaGetDeviceCount(&count));
+    need(device >= 0 && device < count, "device ordinal out of range");
+    ft_context *c = new ft_context();
+    c->opts       = *opts;
+    c->device     = device;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->num_sms = prop.multiProcessorCount;
+    else cudaGetLastError();
+    *out = c;
+    FT_API_END
+}
+
+ft_status ft_context_destroy(ft_context *ctx) {
+    delete ctx;
+    return FT_OK;
+}
+
+ft_status ft_get_query_stats(ft_context *ctx, ft_query_stats *out) {
+    FT_API_BEGIN
+    need(ctx && out, "null argument");
+    *out = ctx->stats;
+    FT_API_END
+}
+
+ft_status ft_tree_create(ft_context *ctx, size_t n, ft_tree **out) {
+    FT_API_BEGIN
+    need(ctx && out, "null argument");
+    DeviceGuard g(ctx->device);
+    ft_tree *t = new ft_tree();
+    std::memset(t, 0, sizeof(*t));
+    TreeImpl *impl = new TreeImpl();
+    impl->coord    = ctx->opts.coord_type;
+    t->impl        = impl;
+    try {
+        tree_alloc_arrays(*ctx, *t, n);
+    } catch (...) {
+        delete impl;
+        delete t;
+        throw;
+    }
+    t->num_leaves   = n;
+    t->num_internal = n > 0 ? n - 1 : 0;
+    *out            = t;
+    FT_API_END
+}
+
+ft_status ft_tree_ensure(ft_context *ctx, ft_tree *t, size_t n) {
+    FT_API_BEGIN
+    need(ctx && t, "null argument");
+    DeviceGuard g(ctx->device);
+    if (n > t->capacity) { // TreePool::ensure (src/hlbvh.hpp:691-705)
+        tree_free_arrays(*t);
+        tree_alloc_arrays(*ctx, *t, n + n / 2 + 1024);
+    }
+    t->num_leaves   = n;
+    t->num_internal = n > 0 ? n - 1 : 0;
+    FT_API_END
+}
+
+ft_status ft_tree_destroy(ft_context *ctx, ft_tree *t) {
+    FT_API_BEGIN
+    if (!t) return FT_OK;
+    need(ctx != nullptr, "null context");
+    DeviceGuard g(ctx->device);
+    tree_free_arrays(*t);
+    if (t->impl) {
+        TreeImpl *impl = (TreeImpl *)t->impl;
+        free_scratch(*impl);
+        delete impl;
+    }
+    delete t;
+    FT_API_END
+}
+
+ft_status ft_tree_height(ft_context *ctx, const ft_tree *t, int *height_out) {
+    FT_API_BEGIN
+    need(ctx && t && height_out, "null argument");
+    *height_out = ((TreeImpl *)t->impl)->height_root;
+    FT_API_END
+}
+
+ft_status ft_compute_bbox(ft_context *ctx, const void *x, const void *y, const void *z, size_t n, void *out6,
+                          ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && out6, "null argument");
+    DeviceGuard  g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t       cb = coord_bytes(ctx->opts.coord_type);
+    if (n > 0) need(x && y && z, "null coordinate array");
+    Staged sx, sy, sz;
+    sx.init(x, n * cb, true, false, st);
+    sy.init(y, n * cb, true, false, st);
+    sz.init(z, n * cb, true, false, st);
+    TreeImpl tmp;
+    void    *out_dev = nullptr;
+    FT_CUDA(cudaMallocAsync(&tmp.bbox_partial, 1184 * 6 * 8, st));
+    FT_CUDA(cudaMallocAsync(&out_dev, 6 * 8, st));
+    ft::compute_bbox(*ctx, &tmp, sx.dev, sy.dev, sz.dev, n, out_dev, st);
+    FT_CUDA(cudaMemcpyAsync(out6, out_dev, 6 * cb, cudaMemcpyDeviceToHost, st));
+    cudaFreeAsync(tmp.bbox_partial, st);
+    cudaFreeAsync(out_dev, st);
+    tmp.bbox_partial = nullptr;
+    FT_CUDA(cudaStreamSynchronize(st));
+    FT_API_END
+}
+
+ft_status ft_sfc_encode(ft_context *ctx, const void *x, const void *y, const void *z, size_t n, void *keys,
+                        const void *bbox6, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx != nullptr, "null context");
+    if (n == 0) return FT_OK;
+    need(x && y && z && keys, "null argument");
+    bool is_float = ctx->opts.coord_type == F32 || ctx->opts.coord_type == F64;
+    need(!is_float || bbox6, "floating-point encoding needs a bounding box");
+    DeviceGuard  g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t       cb = coord_bytes(ctx->opts.coord_type);
+    Staged       sx, sy, sz, sk;
+    sx.init(x, n * cb, true, false, st);
+    sy.init(y, n * cb, true, false, st);
+    sz.init(z, n * cb, true, false, st);
+    sk.init(keys, n * ref_key_bytes(ctx->opts), false, true, st);
+    TreeImpl tmp;
+    void    *bb = nullptr;
+    FT_CUDA(cudaMallocAsync((void **)&tmp.key_lo, n * 8, st));
+    FT_CUDA(cudaMallocAsync((void **)&tmp.key_hi, n * 8, st));
+    FT_CUDA(cudaMallocAsync((void **)&tmp.perm, n * 4, st));
+    FT_CUDA(cudaMallocAsync(&bb, 6 * 8, st));
+    if (bbox6) FT_CUDA(cudaMemcpyAsync(bb, bbox6, 6 * cb, cudaMemcpyHostToDevice, st));
+    else FT_CUDA(cudaMemsetAsync(bb, 0, 6 * 8, st));
+    sfc_encode_ref_layout(*ctx, tmp, sx.dev, sy.dev, sz.dev, n, bb, sk.dev, st);
+    sk.copy_back();
+    cudaFreeAsync(tmp.key_lo, st);
+    cudaFreeAsync(tmp.key_hi, st);
+    cudaFreeAsync(tmp.perm, st);
+    cudaFreeAsync(bb, st);
+    tmp.key_lo = tmp.key_hi = nullptr;
+    tmp.perm                = nullptr;
+    FT_CUDA(cudaStreamSynchronize(st));
+    FT_API_END
+}
+
+ft_status ft_build_bvh(ft_context *ctx, const void *x, const void *y, const void *z, size_t n, const uint32_t *id,
+                       const int8_t *is_ghost, const void *bbox6, void *keys, ft_tree *tree, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree, "null argument");
+    if (n == 0) return FT_OK; // src/hlbvh.hpp:2174
+    if (n > (size_t)(INT_MAX / 2))
+        fail(FT_ERR_RUNTIME, "Particle count n exceeds maximum supported tree size (INT_MAX / 2).");
+    need(x && y && z, "null coordinate array");
+    need(tree->capacity >= n, "tree capacity is smaller than the particle count");
+    DeviceGuard  g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t       cb = coord_bytes(ctx->opts.coord_type);
+    Staged       sx, sy, sz, sid, sgh, sk;
+    sx.init(x, n * cb, true, false, st);
+    sy.init(y, n * cb, true, false, st);
+    sz.init(z, n * cb, true, false, st);
+    sid.init(id, id ? n * 4 : 0, true, false, st);
+    sgh.init(is_ghost, is_ghost ? n : 0, true, false, st);
+    sk.init(keys, keys ? n * ref_key_bytes(ctx->opts) : 0, true, true, st);
+    tree->num_leaves   = n;
+    tree->num_internal = n - 1;
+    TreeImpl &impl     = *(TreeImpl *)tree->impl;
+    impl.height_root   = -1;
+    ft::build_bvh(*ctx, *tree, sx.dev, sy.dev, sz.dev, n, (const uint32_t *)sid.dev, (const int8_t *)sgh.dev, bbox6,
+                  sk.dev, st);
+    if (keys) sk.copy_back();
+    if (n > 1) {
+        uint8_t h = 0;
+        FT_CUDA(cudaMemcpyAsync(&h, impl.height, 1, cudaMemcpyDeviceToHost, st));
+        check_status_word(impl, st);
+        impl.height_root = h;
+    } else {
+        check_status_word(impl, st);
+        impl.height_root = 0;
+    }
+    FT_API_END
+}
+
+ft_status ft_build_tree(ft_context *ctx, ft_tree *tree, const void *sorted_keys, const void *sorted_x,
+                        const void *sorted_y, const void *sorted_z, const uint32_t *sorted_id,
+                        const int8_t *sorted_is_ghost, const int32_t *sorted_orig_idx, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree, "null argument");
+    size_t n = tree->num_leaves;
+    if (n == 0) return FT_OK;
+    need(sorted_keys != nullptr, "null key array");
+    need(tree->capacity >= n, "tree capacity is smaller than num_leaves");
+    DeviceGuard  g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t       cb = coord_bytes(ctx->opts.coord_type);
+    bool         xyz = sorted_x && sorted_y && sorted_z;
+    Staged       sk, sx, sy, sz, sid, sgh, sor;
+    sk.init(sorted_keys, n * ref_key_bytes(ctx->opts), true, false, st);
+    sx.init(xyz ? sorted_x : nullptr, n * cb, true, false, st);
+    sy.init(xyz ? sorted_y : nullptr, n * cb, true, false, st);
+    sz.init(xyz ? sorted_z : nullptr, n * cb, true, false, st);
+    sid.init(sorted_id, sorted_id ? n * 4 : 0, true, false, st);
+    sgh.init(sorted_is_ghost, sorted_is_ghost ? n : 0, true, false, st);
+    sor.init(sorted_orig_idx, sorted_orig_idx ? n * 4 : 0, true, false, st);
+    tree->num_internal = n - 1;
+    TreeImpl &impl     = *(TreeImpl *)tree->impl;
+    build_tree_from_keys(*ctx, *tree, sk.dev, sx.dev, sy.dev, sz.dev, (const uint32_t *)sid.dev,
+                         (const int8_t *)sgh.dev, (const int32_t *)sor.dev, st);
+    if (n > 1) {
+        uint8_t h = 0;
+        FT_CUDA(cudaMemcpyAsync(&h, impl.height, 1, cudaMemcpyDeviceToHost, st));
+        check_status_word(impl, st);
+        impl.height_root = h;
+    } else {
+        check_status_word(impl, st);
+        impl.height_root = 0;
+    }
+    FT_API_END
+}
+
+ft_status ft_self_knn(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_ids, size_t num, int k,
+                      int exclude_self, uint64_t *idx_out, void *dist_out, const ft_query_options *qopts,
+                      ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree, "null argument");
+    ft_query_options q{};
+    if (qopts) q = *qopts;
+    if (!leaf_ids) num = tree->num_leaves;
+    if (num > 0 && k > 0 && tree->num_leaves > 0) need(idx_out && dist_out, "null output array");
+    DeviceGuard g(ctx->device);
+    ft::self_knn(*ctx, *tree, leaf_ids, num, k, exclude_self != 0, idx_out, dist_out, q, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_knn(ft_context *ctx, const ft_tree *tree, const void *qx, const void *qy, const void *qz,
+                 size_t num_queries, int k, uint64_t *idx_out, void *dist_out, const ft_query_options *qopts,
+                 ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree, "null argument");
+    ft_query_options q{};
+    if (qopts) q = *qopts;
+    if (tree->num_leaves == 0 || num_queries == 0 || k <= 0) return FT_OK; // src/hlbvh.hpp:1418
+    need(qx && qy && qz && idx_out && dist_out, "null argument");
+    DeviceGuard  g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t       cb = coord_bytes(ctx->opts.coord_type);
+    size_t       nk = num_queries * (size_t)k;
+    Staged       sx, sy, sz, si, sd;
+    sx.init(qx, num_queries * cb, true, false, st);
+    sy.init(qy, num_queries * cb, true, false, st);
+    sz.init(qz, num_queries * cb, true, false, st);
+    si.init(idx_out, nk * 8, false, true, st);
+    sd.init(dist_out, nk * 8, false, true, st);
+    ft::knn(*ctx, *tree, sx.dev, sy.dev, sz.dev, num_queries, k, q.max_k, (uint64_t *)si.dev, sd.dev, q, st);
+    si.copy_back();
+    sd.copy_back();
+    FT_CUDA(cudaStreamSynchronize(st));
+    FT_API_END
+}
+
+ft_status ft_range(ft_context *ctx, const ft_tree *tree, const void *qx, const void *qy, const void *qz,
+                   const void *r_min, const void *r_max, size_t num_queries, int32_t *results, int32_t *counts,
+                   int max_results_per_query, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree, "null argument");
+    if (tree->num_leaves == 0 || num_queries == 0) return FT_OK; // src/hlbvh.hpp:2020
+    need(qx && qy && qz && r_min && r_max && counts, "null argument");
+    need(max_results_per_query >= 0, "negative max_results_per_query");
+    need(results || max_results_per_query == 0, "null results");
+    DeviceGuard  g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t       cb = coord_bytes(ctx->opts.coord_type);
+    Staged       sx, sy, sz, s0, s1, sr, sc;
+    sx.init(qx, num_queries * cb, true, false, st);
+    sy.init(qy, num_queries * cb, true, false, st);
+    sz.init(qz, num_queries * cb, true, false, st);
+    s0.init(r_min, num_queries * cb, true, false, st);
+    s1.init(r_max, num_queries * cb, true, false, st);
+    // the reference leaves unused result slots untouched: stage with a copy-in
+    sr.init(results, num_queries * (size_t)max_results_per_query * 4, true, true, st);
+    sc.init(counts, num_queries * 4, false, true, st);
+    ft::range(*ctx, *tree, sx.dev, sy.dev, sz.dev, s0.dev, s1.dev, num_queries, (int32_t *)sr.dev, (int32_t *)sc.dev,
+              max_results_per_query, st);
+    sr.copy_back();
+    sc.copy_back();
+    FT_CUDA(cudaStreamSynchronize(st));
+    FT_API_END
+}
+
+} // extern "C"

@@ -1,0 +1,184 @@
+// ft_common.cuh -- shared device definitions: coordinate traits, SFC cells and keys, the
+// point-to-box distance, node records and small helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cfloat>
+#include <type_traits>
+
+#define FT_HD __host__ __device__ __forceinline__
+#define FT_D __device__ __forceinline__
+
+namespace ft {
+
+enum CoordType : int32_t { F32 = 0, F64 = 1, U32 = 2, U64 = 3 };
+enum SfcType : int32_t { MORTON = 0, PEANO_HILBERT = 1 };
+
+// ---------------------------------------------------------------------------------------
+// Coordinate traits.  The constants are those of the reference's configurations:
+//   float/double with Peano-Hilbert: 32-bit position words, 21 bits per axis
+//     (src/sfc.peano_hilbert.hpp:123-129, 168-172); Morton: 21 bits (src/sfc.morton.hpp:11)
+//   uint32: 21 bits, SHIFT_BITS 11, _DIST_SHIFT 0   (src/sfc.peano_hilbert.hpp:169-172, 188)
+//   uint64: 42 bits, SHIFT_BITS 22, _DIST_SHIFT 11  (src/sfc.peano_hilbert.hpp:173-176, 188)
+// ---------------------------------------------------------------------------------------
+template <class T> struct Coord {
+    static constexpr bool is_float  = std::is_floating_point<T>::value;
+    using dist_t                    = typename std::conditional<is_float, double, unsigned long long>::type;
+    static constexpr int bits       = (!is_float && sizeof(T) == 8) ? 42 : 21;
+    static constexpr int shift_bits = (sizeof(T) == 8) ? 22 : 11;
+    static constexpr int dist_shift = (!is_float && bits > 31) ? bits - 31 : 0;
+    static constexpr int key_words  = (!is_float && sizeof(T) == 8) ? 2 : 1; // 126- or 63-bit
+};
+
+// heap sentinel DIST_MAX (src/maxheap.hpp:45) and the "missing" output distance
+// type_identity_max<dist_t>() (src/hlbvh.hpp:59-69)
+template <class D> FT_HD D dist_heap_max();
+template <> FT_HD double dist_heap_max<double>() { return DBL_MAX; }
+template <> FT_HD unsigned long long dist_heap_max<unsigned long long>() { return ~0ull; }
+template <class D> FT_HD D dist_missing();
+template <> FT_HD double dist_missing<double>() { return -DBL_MAX; }
+template <> FT_HD unsigned long long dist_missing<unsigned long long>() { return 0ull; }
+
+// fmin / fmax with the C library's generic semantics: equality returns the first
+// argument, a NaN argument yields the other one.  Written as compares so the sign of a
+// zero result is defined (hardware min/max may pick either).
+template <class T> FT_HD T c_fmin(T a, T b) { return (a <= b || b != b) ? a : b; }
+template <class T> FT_HD T c_fmax(T a, T b) { return (a >= b || b != b) ? a : b; }
+
+// sfc_min / sfc_max (src/hlbvh.hpp:580-594)
+template <class T> FT_HD T box_min(T a, T b) {
+    if constexpr (std::is_floating_point<T>::value) return c_fmin(a, b);
+    else return (a < b) ? a : b;
+}
+template <class T> FT_HD T box_max(T a, T b) {
+    if constexpr (std::is_floating_point<T>::value) return c_fmax(a, b);
+    else return (a < b) ? b : a;
+}
+
+// IEEE round-to-nearest arithmetic with no contraction.
+FT_D float add_rn(float a, float b) { return __fadd_rn(a, b); }
+FT_D double add_rn(double a, double b) { return __dadd_rn(a, b); }
+FT_D float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+FT_D double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+FT_D float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+FT_D double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
+// ---------------------------------------------------------------------------------------
+// Point-to-box squared distance (node_distance_sq, src/hlbvh.hpp:998-1055).
+// ---------------------------------------------------------------------------------------
+template <class T> struct Metric {
+    using C      = Coord<T>;
+    using dist_t = typename C::dist_t;
+
+    // open integer axis: gap to the nearer face, low word shifted (1043-1047)
+    static FT_D unsigned long long open_axis(T v, T lo, T hi) {
+        if (v < lo) return (unsigned long long)(T)(lo - v) >> C::dist_shift;
+        if (v > hi) return (unsigned long long)(T)(v - hi) >> C::dist_shift;
+        return 0ull;
+    }
+    // shortest_periodic_distance in T's width (src/sfc.peano_hilbert.hpp:532-538)
+    static FT_D long long spd(T a, T b) {
+        if constexpr (sizeof(T) == 8) {
+            return (long long)((unsigned long long)(T)(a - b) << C::shift_bits) >> C::shift_bits;
+        } else {
+            return (long long)((int32_t)((uint32_t)(a - b) << C::shift_bits) >> C::shift_bits);
+        }
+    }
+    // periodic integer axis (1021-1033)
+    static FT_D unsigned long long periodic_axis(T v, T lo, T hi) {
+        if constexpr (sizeof(T) >= 8) v &= (T)((T(1) << C::bits) - T(1));
+        if (v >= lo && v <= hi) return 0ull;
+        long long          dl = spd(v, lo), dh = spd(v, hi);
+        unsigned long long al = (unsigned long long)(dl < 0 ? -dl : dl);
+        unsigned long long ah = (unsigned long long)(dh < 0 ? -dh : dh);
+        return ((al < ah) ? al : ah) >> C::dist_shift;
+    }
+    static FT_D unsigned long long sq(unsigned long long g) {
+        // gaps are < 2^32 for every configuration, so a 32x32->64 multiply is exact
+        return (g >> 32) ? g * g : (unsigned long long)(uint32_t)g * (uint32_t)g;
+    }
+
+    template <bool PERIODIC>
+    static FT_D dist_t dist(T px, T py, T pz, T x0, T x1, T y0, T y1, T z0, T z1) {
+        if constexpr (C::is_float) {
+            T dx = c_fmax(sub_rn(x0, px), c_fmax(T(0), sub_rn(px, x1)));
+            T dy = c_fmax(sub_rn(y0, py), c_fmax(T(0), sub_rn(py, y1)));
+            T dz = c_fmax(sub_rn(z0, pz), c_fmax(T(0), sub_rn(pz, z1)));
+            T s  = add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
+            return (double)s;
+        } else {
+            unsigned long long ax, ay, az;
+            if constexpr (PERIODIC) {
+                ax = periodic_axis(px, x0, x1);
+                ay = periodic_axis(py, y0, y1);
+                az = periodic_axis(pz, z0, z1);
+            } else {
+                ax = open_axis(px, x0, x1);
+                ay = open_axis(py, y0, y1);
+                az = open_axis(pz, z0, z1);
+            }
+            return sq(ax) + sq(ay) + sq(az);
+        }
+    }
+};
+
+// ---------------------------------------------------------------------------------------
+// Internal node record used by the traversals: both child boxes and child indices in one
+// 16-word line (64 B for 4-byte coordinates, 128 B for 8-byte ones), fetched with 16-byte
+// vector loads.  Words 0-5: left box (minx,maxx,miny,maxy,minz,maxz); 6-11: right box;
+// then the child indices (Karras encoding: index >= n-1 is a leaf slot).
+// ---------------------------------------------------------------------------------------
+template <class T> struct alignas(16 * sizeof(T)) NodeRec {
+    T       lb[6];
+    T       rb[6];
+    int32_t l, r;
+    int32_t pad[(16 * sizeof(T) - 12 * sizeof(T) - 8) / 4];
+};
+static_assert(sizeof(NodeRec<float>) == 64, "record size");
+static_assert(sizeof(NodeRec<double>) == 128, "record size");
+
+template <class T> FT_D void load_rec(const NodeRec<T> *recs, int node, T lb[6], T rb[6], int &l, int &r) {
+    const uint4 *p = reinterpret_cast<const uint4 *>(recs + node);
+    if constexpr (sizeof(T) == 8) {
+        uint4 w[7];
+#pragma unroll
+        for (int i = 0; i < 7; ++i) w[i] = __ldg(p + i);
+        const T *v = reinterpret_cast<const T *>(w);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            lb[i] = v[i];
+            rb[i] = v[6 + i];
+        }
+        l = (int)w[6].x;
+        r = (int)w[6].y;
+    } else {
+        uint4 w[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) w[i] = __ldg(p + i);
+        const T *v = reinterpret_cast<const T *>(w);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            lb[i] = v[i];
+            rb[i] = v[6 + i];
+        }
+        l = (int)w[3].x;
+        r = (int)w[3].y;
+    }
+}
+
+// Device view of a built tree.
+template <class T> struct TreeDev {
+    const T *min_x, *max_x, *min_y, *max_y, *min_z, *max_z;
+    const int32_t    *orig_idx;
+    const NodeRec<T> *recs;
+    int               n; // leaves
+};
+
+// ---------------------------------------------------------------------------------------
+// Bit tricks
+// ---------------------------------------------------------------------------------------
+FT_D int clz64(unsigned long long x) { return __clzll((long long)x); }
+
+} // namespace ft

@@ -1,0 +1,85 @@
+// ft_internal.h -- host-side structures shared by the build, query and C-ABI units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/fasttree_b200.h"
+
+namespace ft {
+
+// Error carried from deep inside the library to the C ABI.
+struct Error {
+    ft_status   status;
+    std::string msg;
+};
+
+[[noreturn]] void fail(ft_status s, const std::string &msg);
+void              check_cuda(cudaError_t e, const char *what);
+#define FT_CUDA(call) ::ft::check_cuda((call), #call)
+
+// Device status word bits (written by kernels instead of trapping).
+enum : uint32_t { STATUS_SPIN_LIMIT = 1u };
+
+// Library-owned per-tree acceleration data and build scratch (the persistent part plays
+// the role of the reference's BvhScratch, src/hlbvh.hpp:720-745).
+struct TreeImpl {
+    size_t    cap          = 0; // leaf capacity
+    int       coord        = 0;
+    void     *recs         = nullptr; // NodeRec<T>[cap-1]
+    uint8_t  *height       = nullptr; // subtree height of internal nodes
+    int32_t  *counters     = nullptr; // refit arrival counters
+    uint64_t *key_lo       = nullptr; // sorted keys (low word)
+    uint64_t *key_hi       = nullptr; // sorted keys (high word, 126-bit keys only)
+    uint64_t *tmp_lo       = nullptr; // sort ping-pong
+    uint64_t *tmp_hi       = nullptr;
+    uint32_t *perm         = nullptr; // sorted permutation (original index per leaf rank)
+    uint32_t *tmp_perm     = nullptr;
+    void     *bbox         = nullptr; // 6 coords on the device
+    void     *bbox_partial = nullptr; // per-block partial boxes
+    uint32_t *hist         = nullptr; // [digit position][256] counts, then offsets
+    uint32_t *lookback     = nullptr; // onesweep tile status
+    size_t    lookback_words = 0;
+    uint32_t *tile_counter = nullptr; // per-pass tile ticket
+    uint32_t *status       = nullptr; // device status word
+    bool      managed      = false;
+    int       height_root  = -1; // host copy after a build
+};
+
+struct Context {
+    ft_options     opts{};
+    int            device = 0;
+    int            num_sms = 148;
+    ft_query_stats stats{};
+};
+
+// ---- build (ft_build.cu) ----
+void build_bvh(Context &ctx, ft_tree &tree, const void *x, const void *y, const void *z, size_t n,
+               const uint32_t *id, const int8_t *ghost, const void *bbox_host, void *caller_keys_dev,
+               cudaStream_t st);
+void build_tree_from_keys(Context &ctx, ft_tree &tree, const void *keys_ref_dev, const void *sx,
+                          const void *sy, const void *sz, const uint32_t *sid, const int8_t *sghost,
+                          const int32_t *sorig, cudaStream_t st);
+void compute_bbox(Context &ctx, TreeImpl *scratch, const void *x, const void *y, const void *z, size_t n,
+                  void *bbox_dev, cudaStream_t st);
+void sfc_encode_ref_layout(Context &ctx, TreeImpl &scratch, const void *x, const void *y, const void *z,
+                           size_t n, const void *bbox_dev, void *keys_ref_dev, cudaStream_t st);
+size_t ref_key_bytes(const ft_options &o);
+void   ensure_scratch(TreeImpl &impl, const ft_options &o, size_t n);
+void   free_scratch(TreeImpl &impl);
+
+// ---- queries (ft_query.cu) ----
+void self_knn(Context &ctx, const ft_tree &tree, const int32_t *leaf_ids, size_t num, int k,
+              bool exclude_self, uint64_t *idx, void *dist, const ft_query_options &q, cudaStream_t st);
+void knn(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz, size_t nq,
+         int k, int max_k, uint64_t *idx, void *dist, const ft_query_options &q, cudaStream_t st);
+void range(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz,
+           const void *rmin, const void *rmax, size_t nq, int32_t *results, int32_t *counts,
+           int max_per_q, cudaStream_t st);
+
+size_t coord_bytes(int coord);
+
+} // namespace ft

@@ -1,0 +1,537 @@
+// ft_query.cu -- neighbour queries on sm_100a with the reference's exact semantics.
+//
+// Traversal (src/hlbvh.hpp:1079-1182, 1520-1647, 1690-1818): depth-first from the root with a
+// 64-entry stack that drops both children when 62 entries are in use; a popped node is pruned
+// when the heap holds k entries and its distance is >= the heap maximum; leaves are pushed
+// into a binary max-heap (RegisterMaxHeap / LocalMaxHeap, src/maxheap.hpp:33-144, 340-478);
+// internal nodes push the farther child first (ld2 <= rd2 -> push right, then left).  Results
+// leave through an in-place heapsort.  Ties among equal distances therefore come out exactly
+// as the reference orders them.
+//
+// B200 layout: one thread per query (queries in SFC leaf order, so a warp walks neighbouring
+// regions), the child boxes of a node arrive in one 64/128-byte record, the stack keeps the
+// distance computed at push time (the same value the reference recomputes at pop), and the
+// heap lives in shared memory as [slot][thread] so that heap operations of a warp hit
+// distinct banks.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "ft_common.cuh"
+#include "ft_internal.h"
+
+namespace ft {
+
+static constexpr int kStack = 64; // MAX_STACK_DEPTH (src/hlbvh.hpp:984)
+
+template <class T, bool PER, class D = typename Coord<T>::dist_t>
+FT_D D box_dist(T px, T py, T pz, const T *b) {
+    return Metric<T>::template dist<PER>(px, py, pz, b[0], b[1], b[2], b[3], b[4], b[5]);
+}
+template <class T, bool PER, class D = typename Coord<T>::dist_t>
+FT_D D node_dist_soa(const TreeDev<T> &t, int node, T px, T py, T pz) {
+    return Metric<T>::template dist<PER>(px, py, pz, t.min_x[node], t.max_x[node], t.min_y[node], t.max_y[node],
+                                         t.min_z[node], t.max_z[node]);
+}
+
+// -----------------------------------------------------------------------------------------
+// Exact kNN: SELF = self_knn_query[_subset] (query = sorted leaf), else knn_query small-k.
+// -----------------------------------------------------------------------------------------
+template <class T, int CAP, int QT, bool SELF, bool PER>
+__global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t, const T *__restrict__ qx,
+                                                       const T *__restrict__ qy, const T *__restrict__ qz,
+                                                       const int32_t *__restrict__ leaf_ids, int num, int k,
+                                                       int exclude_self, int ret_orig,
+                                                       unsigned long long *__restrict__ out_idx,
+                                                       typename Coord<T>::dist_t *__restrict__ out_dist) {
+    using D = typename Coord<T>::dist_t;
+    extern __shared__ __align__(16) unsigned char smem[];
+    D       *hd  = reinterpret_cast<D *>(smem);
+    int32_t *hix = reinterpret_cast<int32_t *>(hd + CAP * QT);
+    const int tid = threadIdx.x;
+    const int q   = blockIdx.x * QT + tid;
+    if (q >= num) return;
+    const int n = t.n;
+#define HD(s) hd[(s) * QT + tid]
+#define HI(s) hix[(s) * QT + tid]
+
+    T   px, py, pz;
+    int self_leaf = -1;
+    if (SELF) {
+        int rank = leaf_ids ? leaf_ids[q] : q;
+        int slot = rank + n - 1;
+        px = t.min_x[slot];
+        py = t.min_y[slot];
+        pz = t.min_z[slot];
+        if (exclude_self) self_leaf = slot;
+    } else {
+        px = qx[q];
+        py = qy[q];
+        pz = qz[q];
+    }
+
+    int sn[kStack];
+    D   sd[kStack];
+    int sp = 1;
+    sn[0]  = 0;
+    sd[0]  = node_dist_soa<T, PER>(t, 0, px, py, pz);
+    int count = 0;
+    D   hmax  = D(0);
+
+    while (sp > 0) {
+        --sp;
+        const int node = sn[sp];
+        const D   d2   = sd[sp];
+        if (count >= k && d2 >= hmax) continue; // should_prune
+        if (node >= n - 1) {                    // leaf (the n == 1 root included)
+            if (node == self_leaf) continue;
+            const int32_t id = ret_orig ? t.orig_idx[node] : node - (n - 1);
+            if (count < k) { // append + sift_up
+                int i = count;
+                while (i > 0) {
+                    int p  = (i - 1) >> 1;
+                    D   pd = HD(p);
+                    if (d2 <= pd) break;
+                    HD(i) = pd;
+                    HI(i) = HI(p);
+                    i     = p;
+                }
+                HD(i) = d2;
+                HI(i) = id;
+                ++count;
+            } else if (d2 < HD(0)) { // replace root + sift_down
+                int i = 0;
+                for (;;) {
+                    int l = 2 * i + 1;
+                    if (l >= k) break;
+                    int r  = l + 1;
+                    int c  = i;
+                    D   cd = d2;
+                    D   ld = HD(l);
+                    if (ld > cd) {
+                        c  = l;
+                        cd = ld;
+                    }
+                    if (r < k) {
+                        D rd = HD(r);
+                        if (rd > cd) {
+                            c  = r;
+                            cd = rd;
+                        }
+                    }
+                    if (c == i) break;
+                    HD(i) = cd;
+                    HI(i) = HI(c);
+                    i     = c;
+                }
+                HD(i) = d2;
+                HI(i) = id;
+            }
+            if (count >= k) hmax = HD(0);
+        } else {
+            T   lb[6], rb[6];
+            int l, r;
+            load_rec(t.recs, node, lb, rb, l, r);
+            const D ld2 = box_dist<T, PER>(px, py, pz, lb);
+            const D rd2 = box_dist<T, PER>(px, py, pz, rb);
+            if (sp < kStack - 2) {
+                if (ld2 <= rd2) {
+                    sn[sp] = r;
+                    sd[sp] = rd2;
+                    sn[sp + 1] = l;
+                    sd[sp + 1] = ld2;
+                } else {
+                    sn[sp] = l;
+                    sd[sp] = ld2;
+                    sn[sp + 1] = r;
+                    sd[sp + 1] = rd2;
+                }
+                sp += 2;
+            }
+        }
+    }
+
+    // extract_sorted / sort_in_place: heapsort in place
+    for (int hs = count; hs > 1; --hs) {
+        D       last  = HD(hs - 1);
+        int32_t lasti = HI(hs - 1);
+        HD(hs - 1)    = HD(0);
+        HI(hs - 1)    = HI(0);
+        const int size = hs - 1;
+        int       i    = 0;
+        for (;;) {
+            int l = 2 * i + 1;
+            if (l >= size) break;
+            int r  = l + 1;
+            int c  = i;
+            D   cd = last;
+            D   ld = HD(l);
+            if (ld > cd) {
+                c  = l;
+                cd = ld;
+            }
+            if (r < size) {
+                D rd = HD(r);
+                if (rd > cd) {
+                    c  = r;
+                    cd = rd;
+                }
+            }
+            if (c == i) break;
+            HD(i) = cd;
+            HI(i) = HI(c);
+            i     = c;
+        }
+        HD(i) = last;
+        HI(i) = lasti;
+    }
+    const size_t off = (size_t)q * (size_t)k;
+    for (int i = 0; i < k; ++i) {
+        if (i < count) {
+            __stcs(out_idx + off + i, (unsigned long long)(long long)HI(i));
+            __stcs(out_dist + off + i, HD(i));
+        } else {
+            __stcs(out_idx + off + i, ~0ull);
+            __stcs(out_dist + off + i, dist_missing<D>());
+        }
+    }
+#undef HD
+#undef HI
+}
+
+// -----------------------------------------------------------------------------------------
+// knn_query_large_k (src/hlbvh.hpp:1185-1388) with SortedMergeHeap (src/maxheap.hpp:193-324):
+// one warp per query; every lane walks the same traversal, each leaf is merged as a 32-wide
+// batch holding one real candidate, and the list is re-sorted with the reference's bitonic
+// network so equal distances land where the reference puts them.
+// -----------------------------------------------------------------------------------------
+template <class D> FT_D void warp_bitonic(D *d, int32_t *ix, int n, int lane) {
+    for (int kk = 2; kk <= n; kk <<= 1)
+        for (int j = kk >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < n; i += 32) {
+                int l = i ^ j;
+                if (l > i && l < n) {
+                    bool asc = (i & kk) == 0;
+                    D    a = d[i], b = d[l];
+                    if ((a > b) == asc) {
+                        d[i] = b;
+                        d[l] = a;
+                        int32_t t = ix[i];
+                        ix[i]     = ix[l];
+                        ix[l]     = t;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+}
+
+static constexpr int kMergeWarps = 4;
+
+template <class T, bool PER>
+__global__ void __launch_bounds__(32 * kMergeWarps)
+    merge_knn_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
+                     int nq, int k, int cap, int ret_orig, unsigned long long *__restrict__ out_idx,
+                     typename Coord<T>::dist_t *__restrict__ out_dist) {
+    using D = typename Coord<T>::dist_t;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int q    = blockIdx.x * kMergeWarps + w;
+    if (q >= nq) return;
+    D       *hd  = reinterpret_cast<D *>(smem) + (size_t)w * (cap + 32);
+    D       *sgd = hd + cap;
+    int32_t *hix = reinterpret_cast<int32_t *>(reinterpret_cast<D *>(smem) + (size_t)kMergeWarps * (cap + 32)) +
+                   (size_t)w * (cap + 32);
+    int32_t *sgi = hix + cap;
+    const D DMAX = dist_heap_max<D>();
+    for (int i = lane; i < cap; i += 32) {
+        hd[i]  = DMAX;
+        hix[i] = -1;
+    }
+    int count = 0;
+    __syncwarp();
+    const int n  = t.n;
+    const T   px = qx[q], py = qy[q], pz = qz[q];
+    int       sn[kStack];
+    D         sd[kStack];
+    int       sp = 1;
+    sn[0]        = 0;
+    sd[0]        = node_dist_soa<T, PER>(t, 0, px, py, pz);
+    while (sp > 0) {
+        --sp;
+        const int node = sn[sp];
+        const D   d2   = sd[sp];
+        if (count >= k && d2 >= hd[k - 1]) continue;
+        if (node >= n - 1) {
+            const int32_t id = ret_orig ? t.orig_idx[node] : node - (n - 1);
+            // merge_batch: stage [candidate, 31 empty lanes], bitonic-sort it (32)
+            sgd[lane] = (lane == 0) ? d2 : DMAX;
+            sgi[lane] = (lane == 0) ? id : -1;
+            __syncwarp();
+            if (d2 == DMAX) warp_bitonic(sgd, sgi, 32, lane); // otherwise already sorted
+            // append at [count, count + 32) within cap
+            int dst = count + lane;
+            D   vd  = sgd[lane];
+            int vi  = sgi[lane];
+            __syncwarp();
+            if (dst < cap) {
+                hd[dst]  = vd;
+                hix[dst] = vi;
+            }
+            const int nc = min(count + 32, cap);
+            int       p2 = 1;
+            while (p2 < nc) p2 <<= 1;
+            for (int i = nc + lane; i < p2 && i < cap; i += 32) {
+                hd[i]  = DMAX;
+                hix[i] = -1;
+            }
+            __syncwarp();
+            warp_bitonic(hd, hix, p2, lane);
+            count = min(nc, k);
+        } else {
+            T   lb[6], rb[6];
+            int l, r;
+            load_rec(t.recs, node, lb, rb, l, r);
+            const D ld2 = box_dist<T, PER>(px, py, pz, lb);
+            const D rd2 = box_dist<T, PER>(px, py, pz, rb);
+            if (sp < kStack - 2) {
+                if (ld2 <= rd2) {
+                    sn[sp] = r;
+                    sd[sp] = rd2;
+                    sn[sp + 1] = l;
+                    sd[sp + 1] = ld2;
+                } else {
+                    sn[sp] = l;
+                    sd[sp] = ld2;
+                    sn[sp + 1] = r;
+                    sd[sp + 1] = rd2;
+                }
+                sp += 2;
+            }
+        }
+    }
+    const size_t off = (size_t)q * (size_t)k;
+    for (int i = lane; i < k; i += 32) {
+        if (hix[i] >= 0) {
+            out_idx[off + i]  = (unsigned long long)(long long)hix[i];
+            out_dist[off + i] = hd[i];
+        } else {
+            out_idx[off + i]  = ~0ull;
+            out_dist[off + i] = dist_missing<D>();
+        }
+    }
+}
+
+// -----------------------------------------------------------------------------------------
+// range_query (src/hlbvh.hpp:2046-2119): left-first DFS, descend while d2 <= rmax^2, count
+// leaves with d2 >= rmin^2, store while the row has room.
+// -----------------------------------------------------------------------------------------
+template <class T, bool PER>
+__global__ void __launch_bounds__(128) range_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy,
+                                                    const T *__restrict__ qz, const T *__restrict__ rmin,
+                                                    const T *__restrict__ rmax, int nq, int32_t *__restrict__ results,
+                                                    int32_t *__restrict__ counts, int max_per, int ret_orig) {
+    using C = Coord<T>;
+    using D = typename C::dist_t;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    const int n = t.n;
+    D         rm2, RM2;
+    if constexpr (C::is_float) {
+        double a = (double)rmin[q], b = (double)rmax[q];
+        rm2      = __dmul_rn(a, a);
+        RM2      = __dmul_rn(b, b);
+    } else {
+        unsigned long long a = (unsigned long long)rmin[q] >> C::dist_shift;
+        unsigned long long b = (unsigned long long)rmax[q] >> C::dist_shift;
+        rm2                  = a * a;
+        RM2                  = b * b;
+    }
+    const T px = qx[q], py = qy[q], pz = qz[q];
+    int     sn[kStack];
+    D       sd[kStack];
+    int     sp = 1;
+    sn[0]      = 0;
+    sd[0]      = node_dist_soa<T, PER>(t, 0, px, py, pz);
+    int          count = 0;
+    const size_t off   = (size_t)q * (size_t)max_per;
+    while (sp > 0) {
+        --sp;
+        const int node = sn[sp];
+        const D   d2   = sd[sp];
+        if (!(d2 <= RM2)) continue;
+        if (node >= n - 1) {
+            if (d2 >= rm2) {
+                if (count < max_per) results[off + count] = ret_orig ? t.orig_idx[node] : node - (n - 1);
+                ++count;
+            }
+        } else if (sp < kStack - 2) {
+            T   lb[6], rb[6];
+            int l, r;
+            load_rec(t.recs, node, lb, rb, l, r);
+            sn[sp]     = r;
+            sd[sp]     = box_dist<T, PER>(px, py, pz, rb);
+            sn[sp + 1] = l;
+            sd[sp + 1] = box_dist<T, PER>(px, py, pz, lb);
+            sp += 2;
+        }
+    }
+    counts[q] = count;
+}
+
+// =========================================================================================
+// Host side
+// =========================================================================================
+template <class T> static TreeDev<T> dev_view(const ft_tree &tr) {
+    TreeDev<T> v;
+    v.min_x    = (const T *)tr.min_x;
+    v.max_x    = (const T *)tr.max_x;
+    v.min_y    = (const T *)tr.min_y;
+    v.max_y    = (const T *)tr.max_y;
+    v.min_z    = (const T *)tr.min_z;
+    v.max_z    = (const T *)tr.max_z;
+    v.orig_idx = tr.orig_idx;
+    v.recs     = (const NodeRec<T> *)((TreeImpl *)tr.impl)->recs;
+    v.n        = (int)tr.num_leaves;
+    return v;
+}
+
+// Heap capacity tiers and the threads per block that keep the heap at <= 96 KB.
+template <class T, int CAP, int QT, bool SELF, bool PER>
+static void launch_exact_t(const TreeDev<T> &tv, const void *qx, const void *qy, const void *qz,
+                           const int32_t *leaf_ids, int num, int k, bool excl, bool ro, uint64_t *idx, void *dist,
+                           cudaStream_t st) {
+    using D     = typename Coord<T>::dist_t;
+    size_t smem = (size_t)CAP * QT * (sizeof(D) + 4);
+    auto   fn   = exact_knn_kernel<T, CAP, QT, SELF, PER>;
+    FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int blocks = (num + QT - 1) / QT;
+    fn<<<blocks, QT, smem, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz, leaf_ids, num, k, excl ? 1 : 0,
+                                 ro ? 1 : 0, (unsigned long long *)idx, (D *)dist);
+    FT_CUDA(cudaGetLastError());
+}
+
+template <class T, bool SELF, bool PER>
+static void launch_exact_cap(const TreeDev<T> &tv, const void *qx, const void *qy, const void *qz,
+                             const int32_t *leaf_ids, int num, int k, bool excl, bool ro, uint64_t *idx, void *dist,
+                             cudaStream_t st) {
+    if (k <= 32) launch_exact_t<T, 32, 128, SELF, PER>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
+    else if (k <= 64) launch_exact_t<T, 64, 128, SELF, PER>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
+    else if (k <= 128) launch_exact_t<T, 128, 64, SELF, PER>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
+    else if (k <= 256) launch_exact_t<T, 256, 32, SELF, PER>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
+    else launch_exact_t<T, 512, 32, SELF, PER>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
+}
+
+template <class T, bool SELF>
+static void launch_exact(const ft_options &o, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
+                         const int32_t *leaf_ids, int num, int k, bool excl, uint64_t *idx, void *dist,
+                         cudaStream_t st) {
+    TreeDev<T> tv = dev_view<T>(tr);
+    bool       ro = o.return_orig_indices != 0;
+    if (!Coord<T>::is_float && o.periodic)
+        launch_exact_cap<T, SELF, true>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
+    else
+        launch_exact_cap<T, SELF, false>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
+}
+
+static constexpr int kMaxExactK = 512;
+
+void self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, bool excl, uint64_t *idx,
+              void *dist, const ft_query_options &qo, cudaStream_t st) {
+    int max_k = qo.max_k > 0 ? qo.max_k : (leaf_ids ? 256 : 32);
+    if (k > max_k)
+        fail(FT_ERR_INVALID_ARGUMENT,
+             "k exceeds _MAX_K_ template parameter. Instantiate self_knn_query with larger _MAX_K_.");
+    if (tr.num_leaves == 0 || num == 0 || k <= 0) return;
+    if (k > kMaxExactK) fail(FT_ERR_RUNTIME, "self_knn_query: k too large for shared memory.");
+    if (num > (size_t)INT32_MAX) fail(FT_ERR_INVALID_ARGUMENT, "too many queries");
+    ctx.stats.queries = (int64_t)num;
+    ctx.stats.replayed = 0;
+    switch (ctx.opts.coord_type) {
+    case F32: launch_exact<float, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, st); break;
+    case F64: launch_exact<double, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, st); break;
+    case U32: launch_exact<uint32_t, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, st); break;
+    case U64: launch_exact<unsigned long long, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, st); break;
+    }
+}
+
+template <class T, bool PER>
+static void launch_merge(const TreeDev<T> &tv, const void *qx, const void *qy, const void *qz, int nq, int k, int cap,
+                         bool ro, uint64_t *idx, void *dist, cudaStream_t st) {
+    using D     = typename Coord<T>::dist_t;
+    size_t smem = (size_t)kMergeWarps * (cap + 32) * (sizeof(D) + 4);
+    auto   fn   = merge_knn_kernel<T, PER>;
+    FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int blocks = (nq + kMergeWarps - 1) / kMergeWarps;
+    fn<<<blocks, 32 * kMergeWarps, smem, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz, nq, k, cap,
+                                               ro ? 1 : 0, (unsigned long long *)idx, (D *)dist);
+    FT_CUDA(cudaGetLastError());
+}
+
+template <class T>
+static void knn_typed(const ft_options &o, const ft_tree &tr, const void *qx, const void *qy, const void *qz, int nq,
+                      int k, int max_k, uint64_t *idx, void *dist, cudaStream_t st) {
+    if (k <= 32 || max_k <= 32) {
+        launch_exact<T, false>(o, tr, qx, qy, qz, nullptr, nq, k, false, idx, dist, st);
+        return;
+    }
+    int cap = 1;
+    while (cap < max_k) cap <<= 1;
+    TreeDev<T> tv = dev_view<T>(tr);
+    bool       ro = o.return_orig_indices != 0;
+    if (!Coord<T>::is_float && o.periodic) launch_merge<T, true>(tv, qx, qy, qz, nq, k, cap, ro, idx, dist, st);
+    else launch_merge<T, false>(tv, qx, qy, qz, nq, k, cap, ro, idx, dist, st);
+}
+
+void knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz, size_t nq, int k, int max_k,
+         uint64_t *idx, void *dist, const ft_query_options &qo, cudaStream_t st) {
+    (void)qo;
+    if (max_k <= 0) max_k = 256;
+    if (tr.num_leaves == 0 || nq == 0 || k <= 0) return;
+    if (max_k > 32 && k > 32 && k > max_k)
+        fail(FT_ERR_INVALID_ARGUMENT, "k exceeds _MAX_K_ template parameter. Instantiate knn_query with larger _MAX_K_.");
+    if (max_k <= 32 && k > 32)
+        fail(FT_ERR_INVALID_ARGUMENT, "k exceeds _MAX_K_ template parameter. Instantiate knn_query with larger _MAX_K_.");
+    if (max_k > 4096) fail(FT_ERR_RUNTIME, "knn_query_large_k: k too large, local memory requirement exceeds device limit.");
+    if (nq > (size_t)INT32_MAX) fail(FT_ERR_INVALID_ARGUMENT, "too many queries");
+    ctx.stats.queries  = (int64_t)nq;
+    ctx.stats.replayed = 0;
+    switch (ctx.opts.coord_type) {
+    case F32: knn_typed<float>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, st); break;
+    case F64: knn_typed<double>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, st); break;
+    case U32: knn_typed<uint32_t>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, st); break;
+    case U64: knn_typed<unsigned long long>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, st); break;
+    }
+}
+
+template <class T>
+static void range_typed(const ft_options &o, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
+                        const void *rmin, const void *rmax, int nq, int32_t *results, int32_t *counts, int max_per,
+                        cudaStream_t st) {
+    TreeDev<T> tv     = dev_view<T>(tr);
+    int        blocks = (nq + 127) / 128;
+    bool       ro     = o.return_orig_indices != 0;
+    if (!Coord<T>::is_float && o.periodic)
+        range_kernel<T, true><<<blocks, 128, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz,
+                                                      (const T *)rmin, (const T *)rmax, nq, results, counts, max_per,
+                                                      ro ? 1 : 0);
+    else
+        range_kernel<T, false><<<blocks, 128, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz,
+                                                       (const T *)rmin, (const T *)rmax, nq, results, counts, max_per,
+                                                       ro ? 1 : 0);
+    FT_CUDA(cudaGetLastError());
+}
+
+void range(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz, const void *rmin,
+           const void *rmax, size_t nq, int32_t *results, int32_t *counts, int max_per, cudaStream_t st) {
+    if (tr.num_leaves == 0 || nq == 0) return;
+    if (nq > (size_t)INT32_MAX) fail(FT_ERR_INVALID_ARGUMENT, "too many queries");
+    switch (ctx.opts.coord_type) {
+    case F32: range_typed<float>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, st); break;
+    case F64: range_typed<double>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, st); break;
+    case U32: range_typed<uint32_t>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, st); break;
+    case U64: range_typed<unsigned long long>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, st); break;
+    }
+}
+
+} // namespace ft

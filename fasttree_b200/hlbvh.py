@@ -1,0 +1,391 @@
+"""Python mirror of FastTree's C++ API (src/hlbvh.hpp) over the C ABI.
+
+Names and argument meaning follow the reference: particles, BoundingBox, TreeSoA, TreePool,
+compute_bbox, sfc_encode, build_tree, build_bvh, knn_query, self_knn_query,
+self_knn_query_subset, range_query.  The sycl::queue argument becomes a Context (device +
+compile-time options of the reference, now runtime fields) and an optional CUDA stream.
+Errors raise ValueError where the reference throws std::invalid_argument and RuntimeError
+where it throws std::runtime_error.
+
+Arrays may be torch tensors (CUDA or CPU) or numpy arrays; host arrays are staged by the
+library as the reference stages non-USM pointers.  Query outputs of self_knn_query* must be
+device tensors (the reference requires USM there and does not wait).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import capi
+from .capi import F32, F64, U32, U64, MORTON, PEANO_HILBERT, check, lib
+
+_COORD_NAMES = {"f32": F32, "float": F32, "float32": F32, "f64": F64, "double": F64, "float64": F64,
+                "u32": U32, "uint32": U32, "u64": U64, "uint64": U64}
+_SFC_NAMES = {"morton": MORTON, "ph": PEANO_HILBERT, "peano_hilbert": PEANO_HILBERT, "hilbert": PEANO_HILBERT}
+TORCH_COORD = {F32: torch.float32, F64: torch.float64, U32: torch.uint32, U64: torch.uint64}
+NP_COORD = {F32: np.float32, F64: np.float64, U32: np.uint32, U64: np.uint64}
+
+
+def dist_torch_dtype(coord: int):
+    """dist_t: double for floating-point coordinates, uint64 for integer coordinates."""
+    return torch.float64 if coord in (F32, F64) else torch.uint64
+
+
+def _stream_handle(stream) -> int:
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, torch.cuda.Stream):
+        return stream.cuda_stream
+    return int(stream)
+
+
+def _ptr(a) -> Optional[int]:
+    if a is None:
+        return None
+    if isinstance(a, torch.Tensor):
+        assert a.is_contiguous(), "arrays must be contiguous"
+        return a.data_ptr()
+    if isinstance(a, np.ndarray):
+        assert a.flags.c_contiguous, "arrays must be contiguous"
+        return a.ctypes.data
+    raise TypeError(f"unsupported array type {type(a)}")
+
+
+def _as_coord(a, coord: int):
+    """Contiguous array of the coordinate type (keeps device/host placement)."""
+    if isinstance(a, torch.Tensor):
+        t = a if a.dtype == TORCH_COORD[coord] else a.to(TORCH_COORD[coord])
+        return t.contiguous()
+    return np.ascontiguousarray(a, dtype=NP_COORD[coord])
+
+
+class Context:
+    """Device plus the reference's compile-time configuration (CMakeLists.txt:63-125)."""
+
+    def __init__(self, coord="f64", sfc="morton", periodic=False, return_orig_indices=False,
+                 host_readable_tree=False, device: Optional[int] = None):
+        self.coord = _COORD_NAMES[coord] if isinstance(coord, str) else int(coord)
+        self.sfc = _SFC_NAMES[sfc] if isinstance(sfc, str) else int(sfc)
+        self.periodic = bool(periodic)
+        self.return_orig_indices = bool(return_orig_indices)
+        self.device = torch.cuda.current_device() if device is None else int(device)
+        o = capi.FtOptions(self.coord, self.sfc, int(self.periodic), int(self.return_orig_indices),
+                           int(host_readable_tree))
+        h = ctypes.c_void_p()
+        self._h = None
+        _call(lib().ft_context_create(ctypes.byref(o), self.device, ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def is_float(self):
+        return self.coord in (F32, F64)
+
+    def torch_coord(self):
+        return TORCH_COORD[self.coord]
+
+    def query_stats(self):
+        s = capi.FtQueryStats()
+        check(lib().ft_get_query_stats(self._h, ctypes.byref(s)))
+        return {"queries": s.queries, "replayed": s.replayed}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ft_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class particles:
+    """SoA particle input (src/hlbvh.hpp:26-34)."""
+    pos_x: object
+    pos_y: object
+    pos_z: object
+    id: Optional[object] = None
+    is_ghost: Optional[object] = None
+
+
+@dataclass
+class BoundingBox:
+    min_x: float
+    max_x: float
+    min_y: float
+    max_y: float
+    min_z: float
+    max_z: float
+
+    def array(self, coord: int) -> np.ndarray:
+        return np.array([self.min_x, self.max_x, self.min_y, self.max_y, self.min_z, self.max_z],
+                        dtype=NP_COORD[coord])
+
+
+class _RawCuda:
+    """__cuda_array_interface__ view of library-owned device memory."""
+
+    def __init__(self, ptr: int, n: int, dtype: np.dtype):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": np.dtype(dtype).str,
+                                         "data": (int(ptr), False), "version": 3, "strides": None}
+
+
+class TreeSoA:
+    """Flat tree (src/hlbvh.hpp:609-673).  Arrays are exposed as zero-copy torch tensors."""
+
+    def __init__(self, ctx: Context, n: int):
+        self.ctx = ctx
+        p = ctypes.POINTER(capi.FtTree)()
+        check(lib().ft_tree_create(ctx.handle, int(n), ctypes.byref(p)))
+        self._p = p
+
+    @property
+    def c(self):
+        return self._p
+
+    @property
+    def num_leaves(self) -> int:
+        return int(self._p.contents.num_leaves)
+
+    @property
+    def num_internal(self) -> int:
+        return int(self._p.contents.num_internal)
+
+    @property
+    def capacity(self) -> int:
+        return int(self._p.contents.capacity)
+
+    def _view(self, name: str, count: int, dtype) -> torch.Tensor:
+        ptr = getattr(self._p.contents, name)
+        if not ptr or count == 0:
+            return torch.empty(0, dtype=torch.from_numpy(np.zeros(0, dtype)).dtype, device=f"cuda:{self.ctx.device}")
+        return torch.as_tensor(_RawCuda(ptr, count, dtype), device=f"cuda:{self.ctx.device}")
+
+    def array(self, name: str) -> torch.Tensor:
+        n = self.num_leaves
+        tot = 2 * n - 1 if n > 0 else 0
+        if name in ("min_x", "max_x", "min_y", "max_y", "min_z", "max_z"):
+            return self._view(name, tot, NP_COORD[self.ctx.coord])
+        if name in ("left_child", "right_child"):
+            return self._view(name, max(n - 1, 0), np.int32)
+        if name in ("parent", "orig_idx"):
+            return self._view(name, tot, np.int32)
+        if name == "id":
+            return self._view(name, tot, np.uint32)
+        if name == "is_ghost":
+            return self._view(name, tot, np.int8)
+        raise KeyError(name)
+
+    def __getattr__(self, name):
+        if name in ("min_x", "max_x", "min_y", "max_y", "min_z", "max_z", "left_child", "right_child",
+                    "parent", "id", "is_ghost", "orig_idx"):
+            return self.array(name)
+        raise AttributeError(name)
+
+    def to_numpy(self) -> dict:
+        torch.cuda.synchronize(self.ctx.device)
+        return {k: self.array(k).cpu().numpy() for k in ("min_x", "max_x", "min_y", "max_y", "min_z", "max_z",
+                                                          "left_child", "right_child", "parent", "id",
+                                                          "is_ghost", "orig_idx")}
+
+    def leaf_coords(self):
+        s, n = self.num_internal, self.num_leaves
+        return self.min_x[s:s + n], self.min_y[s:s + n], self.min_z[s:s + n]
+
+    def height(self) -> int:
+        h = ctypes.c_int(0)
+        check(lib().ft_tree_height(self.ctx.handle, self._p, ctypes.byref(h)))
+        return h.value
+
+    def free(self):
+        if getattr(self, "_p", None):
+            lib().ft_tree_destroy(self.ctx.handle, self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class TreePool:
+    """Persistent tree that reallocates only when n exceeds capacity (src/hlbvh.hpp:682-715)."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self.tree: Optional[TreeSoA] = None
+
+    def ensure(self, n: int) -> TreeSoA:
+        if self.tree is None:
+            self.tree = TreeSoA(self.ctx, 0)
+        check(lib().ft_tree_ensure(self.ctx.handle, self.tree.c, int(n)))
+        return self.tree
+
+    @property
+    def capacity(self):
+        return 0 if self.tree is None else self.tree.capacity
+
+    def free_all(self):
+        if self.tree is not None:
+            self.tree.free()
+            self.tree = None
+
+
+def _raise_for(e: capi.FastTreeError):
+    if e.status == capi.FT_ERR_INVALID_ARGUMENT:
+        raise ValueError(str(e)) from e
+    if e.status in (capi.FT_ERR_RUNTIME, capi.FT_ERR_TIMEOUT):
+        raise RuntimeError(str(e)) from e
+    if e.status == capi.FT_ERR_OUT_OF_MEMORY:
+        raise MemoryError(str(e)) from e
+    raise e
+
+
+def _call(status):
+    try:
+        check(status)
+    except capi.FastTreeError as e:
+        _raise_for(e)
+
+
+def compute_bbox(ctx: Context, pos_x, pos_y, pos_z, n: Optional[int] = None, stream=None) -> np.ndarray:
+    """compute_bbox (src/hlbvh.hpp:462-572): {min_x, max_x, min_y, max_y, min_z, max_z}."""
+    x, y, z = (_as_coord(a, ctx.coord) for a in (pos_x, pos_y, pos_z))
+    n = len(x) if n is None else int(n)
+    out = np.zeros(6, NP_COORD[ctx.coord])
+    _call(lib().ft_compute_bbox(ctx.handle, _ptr(x), _ptr(y), _ptr(z), n, out.ctypes.data, _stream_handle(stream)))
+    return out
+
+
+def ref_key_dtype(ctx: Context):
+    """numpy dtype of one reference sfc_key: uint64 (Morton), 3 x uint32 or 3 x uint64."""
+    if ctx.sfc == MORTON:
+        return np.dtype(np.uint64), 1
+    return (np.dtype(np.uint64), 3) if ctx.coord == U64 else (np.dtype(np.uint32), 3)
+
+
+def sfc_encode(ctx: Context, pos_x, pos_y, pos_z, bbox=None, keys=None, stream=None):
+    """sfc_encode (src/hlbvh.hpp:357-423); keys in the reference's sfc_key layout, shape (n, words)."""
+    x, y, z = (_as_coord(a, ctx.coord) for a in (pos_x, pos_y, pos_z))
+    n = len(x)
+    dt, words = ref_key_dtype(ctx)
+    if keys is None:
+        keys = np.zeros((n, words), dt)
+    bb = None
+    if bbox is not None:
+        bb = bbox.array(ctx.coord) if isinstance(bbox, BoundingBox) else np.ascontiguousarray(bbox, NP_COORD[ctx.coord])
+    _call(lib().ft_sfc_encode(ctx.handle, _ptr(x), _ptr(y), _ptr(z), n, _ptr(keys),
+                              None if bb is None else bb.ctypes.data, _stream_handle(stream)))
+    return keys
+
+
+def build_bvh(ctx: Context, p, tree: TreeSoA, bbox=None, key=None, scratch=None, stream=None) -> TreeSoA:
+    """build_bvh (src/hlbvh.hpp:2165-2302).  key: caller keys (reference layout), sorted in place.
+    `scratch` is accepted for signature parity; scratch is owned by the tree."""
+    if not isinstance(p, particles):
+        p = particles(*p)
+    x, y, z = (_as_coord(a, ctx.coord) for a in (p.pos_x, p.pos_y, p.pos_z))
+    n = len(x)
+    ids = None
+    if p.id is not None and len(p.id) > 0:
+        if isinstance(p.id, torch.Tensor):
+            assert p.id.element_size() == 4, "id must hold 32-bit values"
+            ids = p.id.contiguous()
+        else:
+            ids = np.ascontiguousarray(p.id, np.uint32)
+    gh = None
+    if p.is_ghost is not None and len(p.is_ghost) > 0:
+        gh = p.is_ghost.to(torch.int8).contiguous() if isinstance(p.is_ghost, torch.Tensor) else \
+            np.ascontiguousarray(p.is_ghost, np.int8)
+    bb = None
+    if bbox is not None:
+        bb = bbox.array(ctx.coord) if isinstance(bbox, BoundingBox) else np.ascontiguousarray(bbox, NP_COORD[ctx.coord])
+    if tree.capacity < n:
+        raise ValueError("tree capacity is smaller than the particle count")
+    _call(lib().ft_build_bvh(ctx.handle, _ptr(x), _ptr(y), _ptr(z), n, _ptr(ids), _ptr(gh),
+                             None if bb is None else bb.ctypes.data, _ptr(key), tree.c, _stream_handle(stream)))
+    return tree
+
+
+def build_tree(ctx: Context, tree: TreeSoA, sorted_keys, sorted_x=None, sorted_y=None, sorted_z=None,
+               sorted_id=None, sorted_is_ghost=None, sorted_orig_idx=None, stream=None) -> TreeSoA:
+    """build_tree (src/hlbvh.hpp:773-982) from caller-sorted keys (reference layout)."""
+    args = [None if a is None else _as_coord(a, ctx.coord) for a in (sorted_x, sorted_y, sorted_z)]
+    sid = None if sorted_id is None else np.ascontiguousarray(sorted_id, np.uint32)
+    sg = None if sorted_is_ghost is None else np.ascontiguousarray(sorted_is_ghost, np.int8)
+    so = None if sorted_orig_idx is None else np.ascontiguousarray(sorted_orig_idx, np.int32)
+    _call(lib().ft_build_tree(ctx.handle, tree.c, _ptr(sorted_keys), *[_ptr(a) for a in args], _ptr(sid), _ptr(sg),
+                              _ptr(so), _stream_handle(stream)))
+    return tree
+
+
+def _qopts(max_k: int, method: int = 0):
+    return capi.FtQueryOptions(int(max_k), int(method))
+
+
+def _alloc_knn_out(ctx: Context, rows: int, k: int):
+    dev = f"cuda:{ctx.device}"
+    return (torch.empty(rows * k, dtype=torch.uint64, device=dev),
+            torch.empty(rows * k, dtype=dist_torch_dtype(ctx.coord), device=dev))
+
+
+def self_knn_query(ctx: Context, tree: TreeSoA, k: int, results=None, result_dists=None, exclude_self=True,
+                   max_k: int = 32, method: int = 0, stream=None):
+    """self_knn_query<MAXK> (src/hlbvh.hpp:1929-1954).  Asynchronous; returns (idx, dist) of shape
+    (num_leaves, k)."""
+    n = tree.num_leaves
+    if results is None:
+        results, result_dists = _alloc_knn_out(ctx, n, k)
+    _call(lib().ft_self_knn(ctx.handle, tree.c, None, n, int(k), int(bool(exclude_self)), _ptr(results),
+                            _ptr(result_dists), ctypes.byref(_qopts(max_k, method)), _stream_handle(stream)))
+    return results.view(n, k) if n * k else results, result_dists.view(n, k) if n * k else result_dists
+
+
+def self_knn_query_subset(ctx: Context, tree: TreeSoA, leaf_ids, k: int, results=None, result_dists=None,
+                          exclude_self=True, max_k: int = 256, method: int = 0, stream=None):
+    """self_knn_query_subset<MAXK> (src/hlbvh.hpp:1956-1983); leaf_ids is a device int32 tensor."""
+    num = len(leaf_ids)
+    if results is None:
+        results, result_dists = _alloc_knn_out(ctx, num, k)
+    _call(lib().ft_self_knn(ctx.handle, tree.c, _ptr(leaf_ids), num, int(k), int(bool(exclude_self)),
+                            _ptr(results), _ptr(result_dists), ctypes.byref(_qopts(max_k, method)),
+                            _stream_handle(stream)))
+    return results.view(num, k) if num * k else results, result_dists.view(num, k) if num * k else result_dists
+
+
+def knn_query(ctx: Context, tree: TreeSoA, qx, qy, qz, k: int, results=None, result_dists=None, max_k: int = 256,
+              method: int = 0, stream=None):
+    """knn_query<MAXK> (src/hlbvh.hpp:1405-1472).  Blocking."""
+    x, y, z = (_as_coord(a, ctx.coord) for a in (qx, qy, qz))
+    nq = len(x)
+    if results is None:
+        results, result_dists = _alloc_knn_out(ctx, nq, k)
+    _call(lib().ft_knn(ctx.handle, tree.c, _ptr(x), _ptr(y), _ptr(z), nq, int(k), _ptr(results), _ptr(result_dists),
+                       ctypes.byref(_qopts(max_k, method)), _stream_handle(stream)))
+    return results.view(nq, k) if nq * k else results, result_dists.view(nq, k) if nq * k else result_dists
+
+
+def range_query(ctx: Context, tree: TreeSoA, qx, qy, qz, r_min, r_max, max_results_per_query: int, results=None,
+                result_counts=None, stream=None):
+    """range_query (src/hlbvh.hpp:2006-2136).  Blocking; returns (results, counts)."""
+    x, y, z, r0, r1 = (_as_coord(a, ctx.coord) for a in (qx, qy, qz, r_min, r_max))
+    nq = len(x)
+    dev = f"cuda:{ctx.device}"
+    if results is None:
+        results = torch.full((nq * max_results_per_query,), -1, dtype=torch.int32, device=dev)
+    if result_counts is None:
+        result_counts = torch.zeros(nq, dtype=torch.int32, device=dev)
+    _call(lib().ft_range(ctx.handle, tree.c, _ptr(x), _ptr(y), _ptr(z), _ptr(r0), _ptr(r1), nq, _ptr(results),
+                         _ptr(result_counts), int(max_results_per_query), _stream_handle(stream)))
+    return results.view(nq, max_results_per_query) if nq * max_results_per_query else results, result_counts

@@ -1,0 +1,178 @@
+/* fasttree_b200.h -- C ABI of the B200 (sm_100a) HLBVH build and neighbour-query library.
+ *
+ * One entry point per operation of FastTree's C++ API (sparxastronomy/fasttree,
+ * src/hlbvh.hpp).  The reference is a header-only C++/SYCL library; its callers bind the
+ * C++ templates directly.  The functions below are what a non-C++ caller (or the C++
+ * wrapper in include/fasttree/hlbvh.hpp) binds instead: plain pointers and sizes, a
+ * cudaStream_t in place of the sycl::queue, status codes in place of exceptions.
+ *
+ * Compile-time choices of the reference (coordinate type, SFC type, PERIODIC_BC,
+ * RETURN_ORIG_INDICES; CMakeLists.txt:63-125) are runtime fields of ft_options.
+ *
+ * Pointers: any argument documented as "host or device" may be a host pointer; it is
+ * staged through device memory (the reference's ensure_device_readable /
+ * ensure_device_writable rule, src/hlbvh.hpp:125-200).  Arguments documented as "device"
+ * must be device-accessible (cudaMalloc, cudaMallocManaged or mapped memory).
+ */
+#ifndef FASTTREE_B200_H
+#define FASTTREE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *ft_stream_t; /* == cudaStream_t; NULL = legacy default stream */
+
+typedef enum ft_status {
+    FT_OK                   = 0,
+    FT_ERR_INVALID_ARGUMENT = 1, /* reference: std::invalid_argument (e.g. k > MAXK)       */
+    FT_ERR_RUNTIME          = 2, /* reference: std::runtime_error (n > INT_MAX/2, ...)      */
+    FT_ERR_CUDA             = 3, /* a CUDA runtime call failed; see ft_last_error()         */
+    FT_ERR_OUT_OF_MEMORY    = 4,
+    FT_ERR_TIMEOUT          = 5  /* a bounded device-side wait gave up (status word set)   */
+} ft_status;
+
+typedef enum ft_coord_type { /* coord_t (src/hlbvh.hpp:202-209)                                   */
+    FT_COORD_F32 = 0,        /* COORDS_TYPE_FLOAT                                                 */
+    FT_COORD_F64 = 1,        /* COORDS_TYPE_DOUBLE                                                */
+    FT_COORD_U32 = 2,        /* FASTTREE_INTEGER_COORDS + POSITIONS_IN_32BIT (21 bits per axis)   */
+    FT_COORD_U64 = 3         /* FASTTREE_INTEGER_COORDS + POSITIONS_IN_64BIT (42 bits per axis)   */
+} ft_coord_type;
+
+typedef enum ft_sfc_type {
+    FT_SFC_MORTON        = 0, /* SFC_TYPE_MORTON (floating-point coordinates only) */
+    FT_SFC_PEANO_HILBERT = 1  /* SFC_TYPE_PEANO_HILBERT                            */
+} ft_sfc_type;
+
+typedef struct ft_options {
+    int32_t coord_type;          /* ft_coord_type                                          */
+    int32_t sfc_type;            /* ft_sfc_type                                            */
+    int32_t periodic;            /* PERIODIC_BC: toroidal distance (integer coords only)   */
+    int32_t return_orig_indices; /* RETURN_ORIG_INDICES: queries return input indices      */
+    int32_t host_readable_tree;  /* 1: tree arrays in managed memory (the reference's USM
+                                    shared allocation, src/hlbvh.hpp:632-650); 0: device  */
+    int32_t reserved[3];
+} ft_options;
+
+typedef struct ft_context ft_context;
+
+/* Flat tree with TreeSoA's members and index layout (src/hlbvh.hpp:609-673): internal
+ * nodes [0, n-2] (root 0), leaves [n-1, 2n-2]; leaf boxes have min == max. Coordinate
+ * arrays hold ft_options.coord_type values. */
+typedef struct ft_tree {
+    void     *min_x, *max_x, *min_y, *max_y, *min_z, *max_z; /* 2n-1 each                  */
+    int32_t  *left_child, *right_child;                      /* n-1 each                    */
+    int32_t  *parent;                                        /* 2n-1, root -1               */
+    uint32_t *id;                                            /* 2n-1 (leaf slots used)      */
+    int8_t   *is_ghost;                                      /* 2n-1 (leaf slots used)      */
+    int32_t  *orig_idx;                                      /* 2n-1 (leaf slots used)      */
+    size_t    num_leaves;
+    size_t    num_internal;
+    size_t    capacity;  /* leaf capacity of the allocation (TreePool::capacity)           */
+    void     *impl;      /* library-owned acceleration data; do not touch                  */
+} ft_tree;
+
+/* Per-query-call options (the reference's template parameters and dispatch choices). */
+typedef struct ft_query_options {
+    int32_t max_k;        /* _MAX_K_ template argument; 0 = the reference's default         */
+    int32_t method;       /* 0 = plain (reference traversal), 1 = fast with exact fallback  */
+    int32_t reserved[6];
+} ft_query_options;
+
+/* Statistics of the last query on a context (fallback rate, visits). */
+typedef struct ft_query_stats {
+    int64_t queries;
+    int64_t replayed;      /* queries rerun by the plain traversal (ties / bound misses)    */
+    int64_t reserved[6];
+} ft_query_stats;
+
+/* ---------------------------------------------------------------------------------- */
+/* Context                                                                             */
+/* ---------------------------------------------------------------------------------- */
+ft_status   ft_context_create(const ft_options *opts, int device, ft_context **out);
+ft_status   ft_context_destroy(ft_context *ctx);
+const char *ft_last_error(void); /* thread-local message of the last failing call */
+int         ft_version(void);
+ft_status   ft_get_query_stats(ft_context *ctx, ft_query_stats *out);
+
+/* ---------------------------------------------------------------------------------- */
+/* Trees: TreeSoA(q, n) / TreeSoA::free (src/hlbvh.hpp:632-672) and                    */
+/* TreePool::ensure (src/hlbvh.hpp:682-705): reallocation only when n exceeds capacity. */
+/* ---------------------------------------------------------------------------------- */
+ft_status ft_tree_create(ft_context *ctx, size_t n, ft_tree **out);
+ft_status ft_tree_ensure(ft_context *ctx, ft_tree *tree, size_t n);
+ft_status ft_tree_destroy(ft_context *ctx, ft_tree *tree);
+
+/* ---------------------------------------------------------------------------------- */
+/* Build                                                                               */
+/* ---------------------------------------------------------------------------------- */
+
+/* compute_bbox (src/hlbvh.hpp:462-572).  x/y/z: host or device, n coords each.
+ * out6 (host): {min_x, max_x, min_y, max_y, min_z, max_z} in the coordinate type.
+ * Blocking.  n == 0 returns the identity box. */
+ft_status ft_compute_bbox(ft_context *ctx, const void *x, const void *y, const void *z, size_t n,
+                          void *out6, ft_stream_t stream);
+
+/* sfc_encode (src/hlbvh.hpp:357-423).  keys: host or device, n keys in the reference's
+ * sfc_key layout: uint64 for Morton; {hs,is,ls} uint32 triples (12 B) for Peano-Hilbert
+ * with 32-bit positions (F32/F64/U32); {hs,is,ls} uint64 triples (24 B) for U64.
+ * bbox6: host, ignored for integer coordinates.  Blocking. */
+ft_status ft_sfc_encode(ft_context *ctx, const void *x, const void *y, const void *z, size_t n,
+                        void *keys, const void *bbox6, ft_stream_t stream);
+
+/* build_bvh (src/hlbvh.hpp:2165-2302).  x/y/z: host or device; id, is_ghost: host or
+ * device or NULL (then iota / 0, as the reference fills them).  bbox6: host or NULL
+ * (computed).  keys: NULL or the caller's keys in sfc_key layout (host or device), which
+ * are sorted in place as in the reference.  tree: from ft_tree_create/ensure; resized to
+ * n.  Blocking (the reference waits internally). */
+ft_status ft_build_bvh(ft_context *ctx, const void *x, const void *y, const void *z, size_t n,
+                       const uint32_t *id, const int8_t *is_ghost, const void *bbox6, void *keys,
+                       ft_tree *tree, ft_stream_t stream);
+
+/* build_tree (src/hlbvh.hpp:773-982) from caller-sorted keys (sfc_key layout) and
+ * optional sorted leaf attributes (each host or device or NULL).  tree->num_leaves keys. */
+ft_status ft_build_tree(ft_context *ctx, ft_tree *tree, const void *sorted_keys,
+                        const void *sorted_x, const void *sorted_y, const void *sorted_z,
+                        const uint32_t *sorted_id, const int8_t *sorted_is_ghost,
+                        const int32_t *sorted_orig_idx, ft_stream_t stream);
+
+/* ---------------------------------------------------------------------------------- */
+/* Queries.  Output rows are k wide: idx (size_t, SIZE_MAX when missing) and dist        */
+/* (double for float coords, uint64 for integer coords; -DBL_MAX / 0 when missing).     */
+/* ---------------------------------------------------------------------------------- */
+
+/* self_knn_query<MAXK> (leaf_ids == NULL, num = tree->num_leaves; src/hlbvh.hpp:1929-1954)
+ * and self_knn_query_subset<MAXK> (src/hlbvh.hpp:1956-1983).  leaf_ids, idx_out, dist_out:
+ * device.  Asynchronous on stream, like the reference.  k > max_k -> INVALID_ARGUMENT.
+ * Default max_k: 32 for the full query, 256 for the subset. */
+ft_status ft_self_knn(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_ids, size_t num,
+                      int k, int exclude_self, uint64_t *idx_out, void *dist_out,
+                      const ft_query_options *qopts, ft_stream_t stream);
+
+/* knn_query<MAXK> (src/hlbvh.hpp:1405-1472).  qx/qy/qz, idx_out, dist_out: host or device.
+ * Default max_k 256.  Blocking. */
+ft_status ft_knn(ft_context *ctx, const ft_tree *tree, const void *qx, const void *qy,
+                 const void *qz, size_t num_queries, int k, uint64_t *idx_out, void *dist_out,
+                 const ft_query_options *qopts, ft_stream_t stream);
+
+/* range_query (src/hlbvh.hpp:2006-2136).  All arrays host or device.  results: num_queries
+ * x max_results_per_query ints (sorted leaf ranks, or input indices with
+ * return_orig_indices); counts: the full count (may exceed the row width).  Blocking. */
+ft_status ft_range(ft_context *ctx, const ft_tree *tree, const void *qx, const void *qy,
+                   const void *qz, const void *r_min, const void *r_max, size_t num_queries,
+                   int32_t *results, int32_t *counts, int max_results_per_query,
+                   ft_stream_t stream);
+
+/* Height of the built tree (root to deepest leaf).  The traversal stack of the reference
+ * drops children below depth 61 (src/hlbvh.hpp:1152, 1618); trees of height <= 62 never
+ * reach that guard. */
+ft_status ft_tree_height(ft_context *ctx, const ft_tree *tree, int *height_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FASTTREE_B200_H */

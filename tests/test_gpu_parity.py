@@ -1,0 +1,219 @@
+"""GPU library vs CPU oracle: trees, self-kNN, kNN and range queries, bit-exact.
+
+Every case runs the same seeded input through the CUDA library (through the C ABI) and the
+oracle restatement, and compares every output array bit for bit: leaf order, topology,
+boxes, neighbour indices (ties included) and distances.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.gpu_util import (CONFIG_IDS, CONFIGS, NAMES, assert_tree_equal, dist_bits, gen, radius,
+                            to_coord, tree_height)
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+import fasttree_b200 as ft  # noqa: E402
+
+
+def make(coord, sfc, periodic, ret_orig=False):
+    ctx = ft.Context(NAMES[coord], sfc, periodic=periodic, return_orig_indices=ret_orig)
+    opts = O.Options(coord, sfc, periodic, ret_orig)
+    return ctx, opts
+
+
+def build_both(ctx, opts, x, y, z, **kw):
+    tree = ft.TreeSoA(ctx, len(x))
+    ft.build_bvh(ctx, ft.particles(x, y, z, kw.get("id"), kw.get("ghost")), tree, bbox=kw.get("bbox"))
+    ot = O.build_bvh(opts, x, y, z, kw.get("id"), kw.get("ghost"), kw.get("bbox"))
+    return tree, ot
+
+
+@pytest.mark.parametrize("cfg", CONFIGS, ids=CONFIG_IDS)
+@pytest.mark.parametrize("kind", ["uniform", "clustered", "degenerate"])
+def test_build_matches_oracle(cfg, kind):
+    coord, sfc, per = cfg
+    ctx, opts = make(coord, sfc, per)
+    n = 20000
+    x, y, z = gen(kind, n, coord, seed=11)
+    ids = np.arange(n, dtype=np.uint32)[::-1].copy()
+    ghost = (np.arange(n) % 7 == 0).astype(np.int8)
+    tree, ot = build_both(ctx, opts, x, y, z, id=ids, ghost=ghost)
+    g = tree.to_numpy()
+    assert_tree_equal(g, ot, n)
+    assert tree.height() == tree_height(ot.parent, n)
+
+
+@pytest.mark.parametrize("cfg", CONFIGS, ids=CONFIG_IDS)
+@pytest.mark.parametrize("kind", ["uniform", "clustered", "degenerate"])
+@pytest.mark.parametrize("k", [1, 16, 32, 33, 64])
+def test_self_knn_matches_oracle(cfg, kind, k):
+    coord, sfc, per = cfg
+    ctx, opts = make(coord, sfc, per)
+    n = 4000
+    x, y, z = gen(kind, n, coord, seed=5)
+    tree, ot = build_both(ctx, opts, x, y, z)
+    for excl in (True, False):
+        gi, gd = ft.self_knn_query(ctx, tree, k, exclude_self=excl, max_k=max(k, 32))
+        torch.cuda.synchronize()
+        oi, od = O.self_knn(opts, ot, k, excl)
+        gi, gd = gi.cpu().numpy(), gd.cpu().numpy()
+        assert np.array_equal(gi, oi), f"indices differ (excl={excl}), first row {np.argmax((gi != oi).any(1))}"
+        assert np.array_equal(dist_bits(gd), dist_bits(od)), f"distances differ (excl={excl})"
+
+
+@pytest.mark.parametrize("cfg", [CONFIGS[1], CONFIGS[7]], ids=[CONFIG_IDS[1], CONFIG_IDS[7]])
+@pytest.mark.parametrize("k", [16, 33, 128, 256])
+def test_self_knn_subset_and_orig_indices(cfg, k):
+    coord, sfc, per = cfg
+    for ret_orig in (False, True):
+        ctx, opts = make(coord, sfc, per, ret_orig)
+        n = 3000
+        x, y, z = gen("clustered", n, coord, seed=7)
+        tree, ot = build_both(ctx, opts, x, y, z)
+        sub = sorted(set(list(range(0, n, n // 17)) + [0, n - 1, n // 2]))
+        leaf_ids = torch.tensor(sub, dtype=torch.int32, device="cuda")
+        for excl in (True, False):
+            gi, gd = ft.self_knn_query_subset(ctx, tree, leaf_ids, k, exclude_self=excl)
+            torch.cuda.synchronize()
+            oi, od = O.self_knn(opts, ot, k, excl, leaf_ids=np.array(sub, np.int32))
+            assert np.array_equal(gi.cpu().numpy(), oi)
+            assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od))
+
+
+@pytest.mark.parametrize("cfg", CONFIGS, ids=CONFIG_IDS)
+@pytest.mark.parametrize("k,max_k", [(5, 256), (32, 256), (33, 256), (48, 128), (64, 256), (64, 64), (128, 128)])
+def test_knn_query_matches_oracle(cfg, k, max_k):
+    coord, sfc, per = cfg
+    ctx, opts = make(coord, sfc, per)
+    n = 3000
+    x, y, z = gen("clustered", n, coord, seed=3)
+    tree, ot = build_both(ctx, opts, x, y, z)
+    rng = np.random.default_rng(9)
+    q = rng.uniform(0, 100.0, (3, 200))
+    qx, qy, qz = (to_coord(a, coord) for a in q)
+    # half the queries on particles (ties with exact hits)
+    qx[:50], qy[:50], qz[:50] = x[:50], y[:50], z[:50]
+    gi, gd = ft.knn_query(ctx, tree, qx, qy, qz, k, max_k=max_k)
+    oi, od = O.knn(opts, ot, qx, qy, qz, k, max_k)
+    assert np.array_equal(gi.cpu().numpy(), oi)
+    assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od))
+
+
+@pytest.mark.parametrize("cfg", CONFIGS, ids=CONFIG_IDS)
+@pytest.mark.parametrize("max_per", [0, 7, 64])
+def test_range_query_matches_oracle(cfg, max_per):
+    coord, sfc, per = cfg
+    ctx, opts = make(coord, sfc, per)
+    n = 5000
+    x, y, z = gen("uniform", n, coord, seed=4)
+    tree, ot = build_both(ctx, opts, x, y, z)
+    rng = np.random.default_rng(10)
+    q = rng.uniform(0, 100.0, (3, 300))
+    qx, qy, qz = (to_coord(a, coord) for a in q)
+    dt = qx.dtype
+    rmin = np.array([radius(r, coord) for r in rng.uniform(0, 2, 300)], dt)
+    rmax = np.array([radius(r, coord) for r in rng.uniform(2, 8, 300)], dt)
+    gr, gc = ft.range_query(ctx, tree, qx, qy, qz, rmin, rmax, max_per)
+    orr, oc = O.range_query(opts, ot, qx, qy, qz, rmin, rmax, max_per)
+    gc = gc.cpu().numpy()
+    assert np.array_equal(gc, oc)
+    gr = gr.cpu().numpy().reshape(300, max_per) if max_per else gr.cpu().numpy()
+    for i in range(300):
+        m = min(oc[i], max_per)
+        assert np.array_equal(gr[i, :m], orr[i, :m])
+
+
+@pytest.mark.parametrize("cfg", [CONFIGS[1], CONFIGS[4], CONFIGS[7]], ids=[CONFIG_IDS[1], CONFIG_IDS[4], CONFIG_IDS[7]])
+@pytest.mark.parametrize("n", [1, 2, 7, 31, 33, 63, 65, 99])
+def test_edge_sizes(cfg, n):
+    """n = 1, 2 and partial warps (test/test_self_knn.cpp:876-1003)."""
+    coord, sfc, per = cfg
+    ctx, opts = make(coord, sfc, per)
+    x, y, z = gen("uniform", n, coord, seed=777)
+    tree, ot = build_both(ctx, opts, x, y, z)
+    assert_tree_equal(tree.to_numpy(), ot, n)
+    for k in (1, 2, 4, 32, 33, 64):
+        for excl in (True, False):
+            gi, gd = ft.self_knn_query(ctx, tree, k, exclude_self=excl, max_k=max(k, 32))
+            torch.cuda.synchronize()
+            oi, od = O.self_knn(opts, ot, k, excl)
+            assert np.array_equal(gi.cpu().numpy(), oi), (n, k, excl)
+            assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od)), (n, k, excl)
+        gi, gd = ft.knn_query(ctx, tree, x[:3], y[:3], z[:3], k, max_k=64)
+        oi, od = O.knn(opts, ot, x[:3], y[:3], z[:3], k, 64)
+        assert np.array_equal(gi.cpu().numpy(), oi)
+
+
+def test_caller_keys_sorted_in_place():
+    """build_bvh with caller keys sorts them in place (src/hlbvh.hpp:2198-2232)."""
+    ctx, opts = make(O.U64, O.PEANO_HILBERT, True)
+    x, y, z = gen("clustered", 5000, O.U64, seed=8)
+    keys = ft.sfc_encode(ctx, x, y, z)  # (n, 3) uint64 {hs, is, ls}
+    hi, lo = O.sfc_encode(opts, x, y, z)
+    assert np.array_equal(keys[:, 1], hi) and np.array_equal(keys[:, 2], lo) and not keys[:, 0].any()
+    tree = ft.TreeSoA(ctx, 5000)
+    k2 = keys.copy()
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree, key=k2)
+    ot = O.build_bvh(opts, x, y, z, keys=(hi.copy(), lo.copy()))
+    assert np.array_equal(k2[:, 1], ot.sorted_hi) and np.array_equal(k2[:, 2], ot.sorted_lo)
+    assert_tree_equal(tree.to_numpy(), ot, 5000)
+
+
+@pytest.mark.parametrize("coord", [O.F32, O.F64])
+def test_build_tree_line_fixture(coord):
+    """test/test_mpi.cpp:183-217: 1000 points on a line, keys 0..999, 20 within 10 of 500.5."""
+    ctx, opts = make(coord, O.MORTON, False)
+    n = 1000
+    xs = np.arange(n).astype(O.NP_COORD[coord])
+    zs = np.zeros(n, O.NP_COORD[coord])
+    tree = ft.TreeSoA(ctx, n)
+    ft.build_tree(ctx, tree, np.arange(n, dtype=np.uint64), xs, zs, zs)
+    res, cnt = ft.range_query(ctx, tree, [500.5], [0.0], [0.0], [0.0], [10.0], 100)
+    assert int(cnt[0]) == 20
+    ot = O.build_tree(opts, None, np.arange(n, dtype=np.uint64), xs, zs, zs)
+    g = tree.to_numpy()
+    for k in ("left_child", "right_child", "parent", "min_x", "max_x"):
+        o = getattr(ot, k)
+        assert np.array_equal(g[k], o[:len(g[k])]), k
+
+
+def test_ghost_fixture():
+    """test/test_domain_decomposition.cpp:360-470: ghosts survive the sort and are found."""
+    ctx, opts = make(O.F64, O.MORTON, False)
+    x = np.array([1.0, 2.0, 3.0, -1.0, 10.0])
+    y = np.zeros(5)
+    z = np.zeros(5)
+    ids = np.array([100, 101, 102, 200, 201], np.uint32)
+    gh = np.array([0, 0, 0, 1, 1], np.int8)
+    tree = ft.TreeSoA(ctx, 5)
+    ft.build_bvh(ctx, ft.particles(x, y, z, ids, gh), tree)
+    g = tree.to_numpy()
+    assert int((g["is_ghost"][4:] == 1).sum()) == 2
+    res, cnt = ft.range_query(ctx, tree, [-0.5], [0.0], [0.0], [0.0], [2.0], 10)
+    hit = sorted(int(g["id"][4 + int(r)]) for r in res.cpu().numpy()[0, :int(cnt[0])])
+    assert hit == [100, 200]
+    idx, d = ft.knn_query(ctx, tree, [9.5], [0.0], [0.0], 2)
+    first = int(idx.cpu().numpy()[0, 0])
+    assert g["id"][4 + first] == 201 and g["is_ghost"][4 + first] == 1
+    assert abs(float(d.cpu().numpy()[0, 0]) - 0.25) < 1e-12
+
+
+def test_invalid_arguments():
+    ctx, opts = make(O.F64, O.MORTON, False)
+    x, y, z = gen("uniform", 100, O.F64, seed=1)
+    tree = ft.TreeSoA(ctx, 100)
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree)
+    with pytest.raises(ValueError):
+        ft.self_knn_query(ctx, tree, 33, max_k=32)  # k > MAXK (src/hlbvh.hpp:1940-1944)
+    with pytest.raises(ValueError):
+        ft.knn_query(ctx, tree, x[:2], y[:2], z[:2], 300, max_k=256)
+    small = ft.TreeSoA(ctx, 10)
+    with pytest.raises(ValueError):
+        ft.build_bvh(ctx, ft.particles(x, y, z), small)
+    with pytest.raises(ValueError):
+        ft.Context("u64", "morton")
