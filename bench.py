@@ -1,0 +1,335 @@
+"""Benchmark: self-kNN queries/s on 10M clustered points (k = 32), plus build ms.
+
+Workload (default "cfg2"): N = 10,000,000 clustered points in a periodic unit box, uint64
+fixed point with 2^40 cells per side (70% in 20,000 Plummer spheres, 30% uniform, seed 2),
+42-bit Peano-Hilbert keys, periodic distances; build_bvh then self_knn_query k = 32 with
+exclude_self = true.  Synthetic stand-in for the reference's HDF5 snapshots.
+
+One step = one self-kNN pass over all N leaves of the resident tree (the reference's
+SelfKNN benchmark, test/benchmark/self_knn_query_scaling.cpp).  The build is timed the same
+way and reported as build_ms.  e2e = the same queries/s through the public API with host
+buffers: pinned H2D of the coordinates, build_bvh, self_knn_query and D2H of the results
+inside the timed region.
+
+Multi-GPU: one process per GPU (torchrun); each rank builds and queries its own replica of
+the workload (independent point sets, no collective on the data path) -> weak scaling.
+
+--impl reference: the CPU restatement of the reference's algorithm (oracle/, the reference's
+SYCL build cannot be compiled here) timed on this host's cores on a bounded query sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "self-kNN queries/s @10M k=32 (clustered uint64, Peano-Hilbert, periodic)"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1"])
+    p.add_argument("--n", type=int, default=0, help="override the point count (tests only)")
+    p.add_argument("--k", type=int, default=32)
+    p.add_argument("--method", default="plain", choices=["plain", "fast"])
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--cpu-sample", type=int, default=200_000)
+    return p.parse_args()
+
+
+def workload(args):
+    from fasttree_b200 import datasets
+    if args.workload == "cfg2":
+        n = args.n or 10_000_000
+        x, y, z = datasets.clustered_fixed(n, n_spheres=20000 if n >= 1_000_000 else max(10, n // 500), seed=2)
+        return dict(name="cfg2: 10M clustered uint64 (2^40/side), Peano-Hilbert, periodic", n=n, coord="u64",
+                    sfc="ph", periodic=True, x=x, y=y, z=z, dtype="u64")
+    n = args.n or 100_000
+    x, y, z = datasets.uniform(n, seed=1)
+    return dict(name="cfg1: 100K uniform float64, Morton, open", n=n, coord="f64", sfc="morton", periodic=False,
+                x=x, y=y, z=z, dtype="f64")
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(w, args, threads=None):
+    """The oracle port on this host's cores: build the tree, then self-kNN on a bounded,
+    evenly spaced sample of leaf queries."""
+    from oracle import oracle as O
+    nthreads = O.set_threads(threads or os.cpu_count() or 1)
+    coord = {"u64": O.U64, "f64": O.F64}[w["coord"]]
+    sfc = O.PEANO_HILBERT if w["sfc"] == "ph" else O.MORTON
+    opts = O.Options(coord, sfc, w["periodic"])
+    t0 = time.perf_counter()
+    tree = O.build_bvh(opts, w["x"], w["y"], w["z"])
+    build_s = time.perf_counter() - t0
+    sample = min(args.cpu_sample, w["n"])
+    ids = np.linspace(0, w["n"] - 1, sample).astype(np.int32)
+    t0 = time.perf_counter()
+    O.self_knn(opts, tree, args.k, True, leaf_ids=ids)
+    q_s = time.perf_counter() - t0
+    return tree, {"value": sample / q_s, "unit": "queries/s", "cores": nthreads, "kind": "port",
+                  "sample": f"{sample} evenly spaced leaf queries of the {w['n']}-point tree (k={args.k}); "
+                            f"CPU build of the same tree took {build_s * 1e3:.0f} ms",
+                  "build_ms": build_s * 1e3}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    w = workload(args)
+    from oracle import oracle as O
+    nthreads = O.set_threads(os.cpu_count() or 1)
+    coord = {"u64": O.U64, "f64": O.F64}[w["coord"]]
+    opts = O.Options(coord, O.PEANO_HILBERT if w["sfc"] == "ph" else O.MORTON, w["periodic"])
+    tree = O.build_bvh(opts, w["x"], w["y"], w["z"])
+    sample = min(args.cpu_sample // 2, w["n"])
+    ids = np.linspace(0, w["n"] - 1, sample).astype(np.int32)
+    for _ in range(max(0, min(args.warmup, 1))):
+        O.self_knn(opts, tree, args.k, True, leaf_ids=ids[: max(1, sample // 10)])
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        O.self_knn(opts, tree, args.k, True, leaf_ids=ids)
+        times.append(time.perf_counter() - t0)
+    t = sum(times) / len(times)
+    v = sample / t
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": w["dtype"], "data": "synthetic",
+           "config": {"workload": w["name"], "n_points": w["n"], "k": args.k, "exclude_self": True},
+           "cpu_baseline": {"value": v, "unit": "queries/s", "cores": nthreads, "kind": "port",
+                            "sample": f"{sample} evenly spaced leaf queries per step on the full tree"},
+           "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import fasttree_b200 as ft
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    w = workload(args)
+    n, k = w["n"], args.k
+    ctx = ft.Context(w["coord"], w["sfc"], periodic=w["periodic"], device=local)
+    dev = f"cuda:{local}"
+    x, y, z = (torch.from_numpy(a).to(dev) for a in (w["x"], w["y"], w["z"]))
+    tree = ft.TreeSoA(ctx, n)
+    p = ft.particles(x, y, z)
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- build_bvh timing ----
+    for _ in range(args.warmup):
+        ft.build_bvh(ctx, p, tree)
+    barrier()
+    bt = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ft.build_bvh(ctx, p, tree)
+        e1.record(stream)
+        e1.synchronize()
+        bt.append(e0.elapsed_time(e1))
+    build_ms = statistics.median(bt)
+    height = tree.height()
+
+    # ---- self-kNN timing (device-resident tree and outputs) ----
+    method = 1 if args.method == "fast" else 0
+    idx = torch.empty(n * k, dtype=torch.uint64, device=dev)
+    dst = torch.empty(n * k, dtype=ft.dist_torch_dtype(ctx.coord), device=dev)
+    for _ in range(args.warmup):
+        ft.self_knn_query(ctx, tree, k, idx, dst, exclude_self=True, max_k=max(32, k), method=method)
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for a, b in evs:
+        a.record(stream)
+        ft.self_knn_query(ctx, tree, k, idx, dst, exclude_self=True, max_k=max(32, k), method=method)
+        b.record(stream)
+    g1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    total_ms = g0.elapsed_time(g1)
+    per_launch = [a.elapsed_time(b) for a, b in evs]
+    t_local = torch.tensor([total_ms], device=dev)
+    if world > 1:
+        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+    total_ms = float(t_local.item())
+    ms_per_step = total_ms / args.steps
+    value = world * n / (ms_per_step / 1e3)
+    stats = ctx.query_stats()
+
+    # ---- e2e through the public API with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        hx, hy, hz = (torch.from_numpy(a).pin_memory() for a in (w["x"], w["y"], w["z"]))
+        hi = torch.empty(n * k, dtype=torch.uint64).pin_memory()
+        hd = torch.empty(n * k, dtype=dst.dtype).pin_memory()
+        e_steps = max(1, min(args.steps, 3))
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e_steps):
+            dx, dy, dz = (t.to(dev, non_blocking=True) for t in (hx, hy, hz))
+            ft.build_bvh(ctx, ft.particles(dx, dy, dz), tree)
+            ft.self_knn_query(ctx, tree, k, idx, dst, exclude_self=True, max_k=max(32, k), method=method)
+            hi.copy_(idx, non_blocking=True)
+            hd.copy_(dst, non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e_ms = e0.elapsed_time(e1) / e_steps
+        te = torch.tensor([e_ms], device=dev)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e_ms = float(te.item())
+        e2e = {"value": world * n / (e_ms / 1e3), "unit": "queries/s",
+               "h2d_bytes_per_step": int(3 * n * x.element_size()),
+               "d2h_bytes_per_step": int(n * k * (idx.element_size() + dst.element_size())), "ms_per_step": e_ms}
+
+    # ---- roofline of the self-kNN kernel (algorithmic bytes per launch / launch time) ----
+    sc = x.element_size()
+    tree_bytes = (2 * n - 1) * 6 * sc + (n - 1) * 8
+    out_bytes = 16 * n * k
+    alg = tree_bytes + out_bytes
+    peak, peak_kind = measured_peaks()
+    launch_ms = statistics.mean(per_launch)
+    achieved = alg / (launch_ms / 1e3) / 1e9
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "self_knn_traffic.json")
+    if os.path.exists(tf):
+        try:
+            with open(tf) as f:
+                tj = json.load(f)
+            if tj.get("workload") == w["name"] and tj.get("method") == args.method:
+                traffic = tj.get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": peak_kind,
+                "algorithmic_bytes": alg, "kernel": "exact_knn_kernel (self_knn_query)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        del tree
+        torch.cuda.empty_cache()
+        _, cpu = cpu_baseline(w, args)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": w["dtype"], "data": "synthetic",
+               "config": {"workload": w["name"], "n_points": n, "k": k, "exclude_self": True,
+                          "method": args.method, "parallelism": f"replicas x{world}",
+                          "l2": "inputs larger than L2: tree records + boxes ~2.3 GB, output 5.1 GB"},
+               "build_ms": build_ms, "tree_height": height, "query_stats": stats,
+               "e2e": e2e, "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu,
+               "clocks": clocks}
+        print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

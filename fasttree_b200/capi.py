@@ -17,6 +17,7 @@ MORTON, PEANO_HILBERT = 0, 1
 # Every entry point declared in include/fasttree_b200.h.
 EXPORTED = (
     "ft_context_create", "ft_context_destroy", "ft_last_error", "ft_version", "ft_get_query_stats",
+    "ft_check_device_status",
     "ft_tree_create", "ft_tree_ensure", "ft_tree_destroy", "ft_compute_bbox", "ft_sfc_encode",
     "ft_build_bvh", "ft_build_tree", "ft_self_knn", "ft_knn", "ft_range", "ft_tree_height",
 )
@@ -57,6 +58,7 @@ _SIGS = {
     "ft_context_create": [ctypes.POINTER(FtOptions), _i, ctypes.POINTER(_vp)],
     "ft_context_destroy": [_vp],
     "ft_get_query_stats": [_vp, ctypes.POINTER(FtQueryStats)],
+    "ft_check_device_status": [_vp, _st],
     "ft_tree_create": [_vp, _sz, ctypes.POINTER(ctypes.POINTER(FtTree))],
     "ft_tree_ensure": [_vp, ctypes.POINTER(FtTree), _sz],
     "ft_tree_destroy": [_vp, ctypes.POINTER(FtTree)],

@@ -477,6 +477,10 @@ __global__ void __launch_bounds__(kSortThreads, 1)
         unsigned long long w  = (W == 2 && word == 1) ? hi : lo;
         uint32_t           d  = (uint32_t)(w >> shift) & 255u;
         size_t             gp = (size_t)s_base[d] + (size_t)(j - (int)s_tile_excl[d]);
+        if (gp >= n) { // only reachable after a failed look-back; never write out of bounds
+            atomicOr(status, STATUS_SPIN_LIMIT);
+            continue;
+        }
         out_lo[gp]            = lo;
         if (W == 2) out_hi[gp] = hi;
         out_v[gp] = s_v[j];
@@ -600,8 +604,9 @@ __global__ void __launch_bounds__(256) refit_kernel(int n, const int32_t *__rest
     const T *soa[6] = {mnx, mxx, mny, mxy, mnz, mxz};
     T       *soa_w[6] = {mnx, mxx, mny, mxy, mnz, mxz};
     for (int leaf = blockIdx.x * blockDim.x + threadIdx.x; leaf < n; leaf += gridDim.x * blockDim.x) {
-        int curr = leaf + n - 1;
-        while (curr != 0) {
+        int curr  = leaf + n - 1;
+        int steps = 0;
+        while (curr != 0 && ++steps < n) { // a valid tree is climbed in < n steps
             int p = parent[curr];
             if (p < 0 || p >= n - 1) break;
             __threadfence();

@@ -91,15 +91,19 @@ static void validate_options(const ft_options &o) {
         fail(FT_ERR_INVALID_ARGUMENT, "Morton keys are defined for floating-point coordinates only");
 }
 
-static void check_status_word(TreeImpl &s, cudaStream_t st) {
+void check_device_status(uint32_t *status, cudaStream_t st) {
     uint32_t v = 0;
-    FT_CUDA(cudaMemcpyAsync(&v, s.status, sizeof(v), cudaMemcpyDeviceToHost, st));
+    FT_CUDA(cudaMemcpyAsync(&v, status, sizeof(v), cudaMemcpyDeviceToHost, st));
     FT_CUDA(cudaStreamSynchronize(st));
-    if (v) {
-        FT_CUDA(cudaMemsetAsync(s.status, 0, sizeof(uint32_t), st));
-        fail(FT_ERR_TIMEOUT, "a bounded device-side wait gave up (radix-sort look-back)");
-    }
+    if (!v) return;
+    FT_CUDA(cudaMemsetAsync(status, 0, sizeof(uint32_t), st));
+    FT_CUDA(cudaStreamSynchronize(st));
+    if (v & STATUS_BAD_INPUT) fail(FT_ERR_INVALID_ARGUMENT, "a leaf id was outside [0, num_leaves)");
+    if (v & STATUS_SPIN_LIMIT) fail(FT_ERR_TIMEOUT, "a bounded device-side wait gave up (radix-sort look-back)");
+    fail(FT_ERR_RUNTIME, "a traversal exceeded its visit bound (corrupt tree)");
 }
+
+static void check_status_word(TreeImpl &s, cudaStream_t st) { check_device_status(s.status, st); }
 
 // ---------------------------------------------------------------------------------------
 // Tree storage
@@ -193,9 +197,15 @@ ft_status ft_context_create(const ft_options *opts, int device, ft_context **out
     int count = 0;
     FT_CUDA(cudaGetDeviceCount(&count));
     need(device >= 0 && device < count, "device ordinal out of range");
+    DeviceGuard g(device);
     ft_context *c = new ft_context();
     c->opts       = *opts;
     c->device     = device;
+    if (cudaMalloc(&c->status, 16) != cudaSuccess || cudaMemset(c->status, 0, 16) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        fail(FT_ERR_CUDA, "device status word allocation failed");
+    }
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->num_sms = prop.multiProcessorCount;
     else cudaGetLastError();
@@ -204,8 +214,17 @@ ft_status ft_context_create(const ft_options *opts, int device, ft_context **out
 }
 
 ft_status ft_context_destroy(ft_context *ctx) {
+    if (ctx && ctx->status) cudaFree(ctx->status);
     delete ctx;
     return FT_OK;
+}
+
+ft_status ft_check_device_status(ft_context *ctx, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx != nullptr, "null context");
+    DeviceGuard g(ctx->device);
+    check_device_status(ctx->status, (cudaStream_t)stream);
+    FT_API_END
 }
 
 ft_status ft_get_query_stats(ft_context *ctx, ft_query_stats *out) {
@@ -444,7 +463,7 @@ ft_status ft_knn(ft_context *ctx, const ft_tree *tree, const void *qx, const voi
     ft::knn(*ctx, *tree, sx.dev, sy.dev, sz.dev, num_queries, k, q.max_k, (uint64_t *)si.dev, sd.dev, q, st);
     si.copy_back();
     sd.copy_back();
-    FT_CUDA(cudaStreamSynchronize(st));
+    check_device_status(ctx->status, st);
     FT_API_END
 }
 
@@ -473,7 +492,7 @@ ft_status ft_range(ft_context *ctx, const ft_tree *tree, const void *qx, const v
               max_results_per_query, st);
     sr.copy_back();
     sc.copy_back();
-    FT_CUDA(cudaStreamSynchronize(st));
+    check_device_status(ctx->status, st);
     FT_API_END
 }
 

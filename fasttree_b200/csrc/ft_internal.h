@@ -22,7 +22,7 @@ void              check_cuda(cudaError_t e, const char *what);
 #define FT_CUDA(call) ::ft::check_cuda((call), #call)
 
 // Device status word bits (written by kernels instead of trapping).
-enum : uint32_t { STATUS_SPIN_LIMIT = 1u };
+enum : uint32_t { STATUS_SPIN_LIMIT = 1u, STATUS_TRAVERSAL_LIMIT = 2u, STATUS_BAD_INPUT = 4u };
 
 // Library-owned per-tree acceleration data and build scratch (the persistent part plays
 // the role of the reference's BvhScratch, src/hlbvh.hpp:720-745).
@@ -54,7 +54,11 @@ struct Context {
     int            device = 0;
     int            num_sms = 148;
     ft_query_stats stats{};
+    uint32_t      *status = nullptr; // device status word of query kernels
 };
+
+// Reads and clears a device status word (synchronises the stream); throws on a set bit.
+void check_device_status(uint32_t *status, cudaStream_t st);
 
 // ---- build (ft_build.cu) ----
 void build_bvh(Context &ctx, ft_tree &tree, const void *x, const void *y, const void *z, size_t n,

@@ -43,7 +43,8 @@ __global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t, const T *__
                                                        const int32_t *__restrict__ leaf_ids, int num, int k,
                                                        int exclude_self, int ret_orig,
                                                        unsigned long long *__restrict__ out_idx,
-                                                       typename Coord<T>::dist_t *__restrict__ out_dist) {
+                                                       typename Coord<T>::dist_t *__restrict__ out_dist,
+                                                       uint32_t *status) {
     using D = typename Coord<T>::dist_t;
     extern __shared__ __align__(16) unsigned char smem[];
     D       *hd  = reinterpret_cast<D *>(smem);
@@ -59,6 +60,14 @@ __global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t, const T *__
     int self_leaf = -1;
     if (SELF) {
         int rank = leaf_ids ? leaf_ids[q] : q;
+        if (rank < 0 || rank >= n) { // invalid caller leaf id: empty row, flag the call
+            atomicOr(status, STATUS_BAD_INPUT);
+            for (int i = 0; i < k; ++i) {
+                out_idx[(size_t)q * k + i]  = ~0ull;
+                out_dist[(size_t)q * k + i] = dist_missing<D>();
+            }
+            return;
+        }
         int slot = rank + n - 1;
         px = t.min_x[slot];
         py = t.min_y[slot];
@@ -77,8 +86,14 @@ __global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t, const T *__
     sd[0]  = node_dist_soa<T, PER>(t, 0, px, py, pz);
     int count = 0;
     D   hmax  = D(0);
+    // each node is pushed once by its parent in a valid tree: 2n-1 pops at most
+    long long budget = 2ll * n + 64;
 
     while (sp > 0) {
+        if (--budget < 0) {
+            atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+            break;
+        }
         --sp;
         const int node = sn[sp];
         const D   d2   = sd[sp];
@@ -232,7 +247,7 @@ template <class T, bool PER>
 __global__ void __launch_bounds__(32 * kMergeWarps)
     merge_knn_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
                      int nq, int k, int cap, int ret_orig, unsigned long long *__restrict__ out_idx,
-                     typename Coord<T>::dist_t *__restrict__ out_dist) {
+                     typename Coord<T>::dist_t *__restrict__ out_dist, uint32_t *status) {
     using D = typename Coord<T>::dist_t;
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -257,7 +272,12 @@ __global__ void __launch_bounds__(32 * kMergeWarps)
     int       sp = 1;
     sn[0]        = 0;
     sd[0]        = node_dist_soa<T, PER>(t, 0, px, py, pz);
+    long long budget = 2ll * n + 64;
     while (sp > 0) {
+        if (--budget < 0) {
+            if (lane == 0) atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+            break;
+        }
         --sp;
         const int node = sn[sp];
         const D   d2   = sd[sp];
@@ -330,7 +350,8 @@ template <class T, bool PER>
 __global__ void __launch_bounds__(128) range_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy,
                                                     const T *__restrict__ qz, const T *__restrict__ rmin,
                                                     const T *__restrict__ rmax, int nq, int32_t *__restrict__ results,
-                                                    int32_t *__restrict__ counts, int max_per, int ret_orig) {
+                                                    int32_t *__restrict__ counts, int max_per, int ret_orig,
+                                                    uint32_t *status) {
     using C = Coord<T>;
     using D = typename C::dist_t;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -355,7 +376,12 @@ __global__ void __launch_bounds__(128) range_kernel(TreeDev<T> t, const T *__res
     sd[0]      = node_dist_soa<T, PER>(t, 0, px, py, pz);
     int          count = 0;
     const size_t off   = (size_t)q * (size_t)max_per;
+    long long    budget = 2ll * n + 64;
     while (sp > 0) {
+        if (--budget < 0) {
+            atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+            break;
+        }
         --sp;
         const int node = sn[sp];
         const D   d2   = sd[sp];
@@ -400,38 +426,41 @@ template <class T> static TreeDev<T> dev_view(const ft_tree &tr) {
 template <class T, int CAP, int QT, bool SELF, bool PER>
 static void launch_exact_t(const TreeDev<T> &tv, const void *qx, const void *qy, const void *qz,
                            const int32_t *leaf_ids, int num, int k, bool excl, bool ro, uint64_t *idx, void *dist,
-                           cudaStream_t st) {
+                           uint32_t *status, cudaStream_t st) {
     using D     = typename Coord<T>::dist_t;
     size_t smem = (size_t)CAP * QT * (sizeof(D) + 4);
     auto   fn   = exact_knn_kernel<T, CAP, QT, SELF, PER>;
     FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int blocks = (num + QT - 1) / QT;
     fn<<<blocks, QT, smem, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz, leaf_ids, num, k, excl ? 1 : 0,
-                                 ro ? 1 : 0, (unsigned long long *)idx, (D *)dist);
+                                 ro ? 1 : 0, (unsigned long long *)idx, (D *)dist, status);
     FT_CUDA(cudaGetLastError());
 }
 
 template <class T, bool SELF, bool PER>
 static void launch_exact_cap(const TreeDev<T> &tv, const void *qx, const void *qy, const void *qz,
                              const int32_t *leaf_ids, int num, int k, bool excl, bool ro, uint64_t *idx, void *dist,
-                             cudaStream_t st) {
-    if (k <= 32) launch_exact_t<T, 32, 128, SELF, PER>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
-    else if (k <= 64) launch_exact_t<T, 64, 128, SELF, PER>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
-    else if (k <= 128) launch_exact_t<T, 128, 64, SELF, PER>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
-    else if (k <= 256) launch_exact_t<T, 256, 32, SELF, PER>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
-    else launch_exact_t<T, 512, 32, SELF, PER>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
+                             uint32_t *status, cudaStream_t st) {
+#define FT_LAUNCH(CAP, QT) \
+    launch_exact_t<T, CAP, QT, SELF, PER>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, status, st)
+    if (k <= 32) FT_LAUNCH(32, 128);
+    else if (k <= 64) FT_LAUNCH(64, 128);
+    else if (k <= 128) FT_LAUNCH(128, 64);
+    else if (k <= 256) FT_LAUNCH(256, 32);
+    else FT_LAUNCH(512, 32);
+#undef FT_LAUNCH
 }
 
 template <class T, bool SELF>
 static void launch_exact(const ft_options &o, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
                          const int32_t *leaf_ids, int num, int k, bool excl, uint64_t *idx, void *dist,
-                         cudaStream_t st) {
+                         uint32_t *status, cudaStream_t st) {
     TreeDev<T> tv = dev_view<T>(tr);
     bool       ro = o.return_orig_indices != 0;
     if (!Coord<T>::is_float && o.periodic)
-        launch_exact_cap<T, SELF, true>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
+        launch_exact_cap<T, SELF, true>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, status, st);
     else
-        launch_exact_cap<T, SELF, false>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, st);
+        launch_exact_cap<T, SELF, false>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, status, st);
 }
 
 static constexpr int kMaxExactK = 512;
@@ -448,39 +477,39 @@ void self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t n
     ctx.stats.queries = (int64_t)num;
     ctx.stats.replayed = 0;
     switch (ctx.opts.coord_type) {
-    case F32: launch_exact<float, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, st); break;
-    case F64: launch_exact<double, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, st); break;
-    case U32: launch_exact<uint32_t, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, st); break;
-    case U64: launch_exact<unsigned long long, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, st); break;
+    case F32: launch_exact<float, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, ctx.status, st); break;
+    case F64: launch_exact<double, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, ctx.status, st); break;
+    case U32: launch_exact<uint32_t, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, ctx.status, st); break;
+    case U64: launch_exact<unsigned long long, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, ctx.status, st); break;
     }
 }
 
 template <class T, bool PER>
 static void launch_merge(const TreeDev<T> &tv, const void *qx, const void *qy, const void *qz, int nq, int k, int cap,
-                         bool ro, uint64_t *idx, void *dist, cudaStream_t st) {
+                         bool ro, uint64_t *idx, void *dist, uint32_t *status, cudaStream_t st) {
     using D     = typename Coord<T>::dist_t;
     size_t smem = (size_t)kMergeWarps * (cap + 32) * (sizeof(D) + 4);
     auto   fn   = merge_knn_kernel<T, PER>;
     FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int blocks = (nq + kMergeWarps - 1) / kMergeWarps;
     fn<<<blocks, 32 * kMergeWarps, smem, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz, nq, k, cap,
-                                               ro ? 1 : 0, (unsigned long long *)idx, (D *)dist);
+                                               ro ? 1 : 0, (unsigned long long *)idx, (D *)dist, status);
     FT_CUDA(cudaGetLastError());
 }
 
 template <class T>
 static void knn_typed(const ft_options &o, const ft_tree &tr, const void *qx, const void *qy, const void *qz, int nq,
-                      int k, int max_k, uint64_t *idx, void *dist, cudaStream_t st) {
+                      int k, int max_k, uint64_t *idx, void *dist, uint32_t *status, cudaStream_t st) {
     if (k <= 32 || max_k <= 32) {
-        launch_exact<T, false>(o, tr, qx, qy, qz, nullptr, nq, k, false, idx, dist, st);
+        launch_exact<T, false>(o, tr, qx, qy, qz, nullptr, nq, k, false, idx, dist, status, st);
         return;
     }
     int cap = 1;
     while (cap < max_k) cap <<= 1;
     TreeDev<T> tv = dev_view<T>(tr);
     bool       ro = o.return_orig_indices != 0;
-    if (!Coord<T>::is_float && o.periodic) launch_merge<T, true>(tv, qx, qy, qz, nq, k, cap, ro, idx, dist, st);
-    else launch_merge<T, false>(tv, qx, qy, qz, nq, k, cap, ro, idx, dist, st);
+    if (!Coord<T>::is_float && o.periodic) launch_merge<T, true>(tv, qx, qy, qz, nq, k, cap, ro, idx, dist, status, st);
+    else launch_merge<T, false>(tv, qx, qy, qz, nq, k, cap, ro, idx, dist, status, st);
 }
 
 void knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz, size_t nq, int k, int max_k,
@@ -497,28 +526,28 @@ void knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const 
     ctx.stats.queries  = (int64_t)nq;
     ctx.stats.replayed = 0;
     switch (ctx.opts.coord_type) {
-    case F32: knn_typed<float>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, st); break;
-    case F64: knn_typed<double>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, st); break;
-    case U32: knn_typed<uint32_t>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, st); break;
-    case U64: knn_typed<unsigned long long>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, st); break;
+    case F32: knn_typed<float>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, ctx.status, st); break;
+    case F64: knn_typed<double>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, ctx.status, st); break;
+    case U32: knn_typed<uint32_t>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, ctx.status, st); break;
+    case U64: knn_typed<unsigned long long>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, ctx.status, st); break;
     }
 }
 
 template <class T>
 static void range_typed(const ft_options &o, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
                         const void *rmin, const void *rmax, int nq, int32_t *results, int32_t *counts, int max_per,
-                        cudaStream_t st) {
+                        uint32_t *status, cudaStream_t st) {
     TreeDev<T> tv     = dev_view<T>(tr);
     int        blocks = (nq + 127) / 128;
     bool       ro     = o.return_orig_indices != 0;
     if (!Coord<T>::is_float && o.periodic)
         range_kernel<T, true><<<blocks, 128, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz,
                                                       (const T *)rmin, (const T *)rmax, nq, results, counts, max_per,
-                                                      ro ? 1 : 0);
+                                                      ro ? 1 : 0, status);
     else
         range_kernel<T, false><<<blocks, 128, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz,
                                                        (const T *)rmin, (const T *)rmax, nq, results, counts, max_per,
-                                                       ro ? 1 : 0);
+                                                       ro ? 1 : 0, status);
     FT_CUDA(cudaGetLastError());
 }
 
@@ -527,10 +556,10 @@ void range(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, cons
     if (tr.num_leaves == 0 || nq == 0) return;
     if (nq > (size_t)INT32_MAX) fail(FT_ERR_INVALID_ARGUMENT, "too many queries");
     switch (ctx.opts.coord_type) {
-    case F32: range_typed<float>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, st); break;
-    case F64: range_typed<double>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, st); break;
-    case U32: range_typed<uint32_t>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, st); break;
-    case U64: range_typed<unsigned long long>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, st); break;
+    case F32: range_typed<float>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, ctx.status, st); break;
+    case F64: range_typed<double>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, ctx.status, st); break;
+    case U32: range_typed<uint32_t>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, ctx.status, st); break;
+    case U64: range_typed<unsigned long long>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, ctx.status, st); break;
     }
 }
 

@@ -97,6 +97,10 @@ ft_status   ft_context_destroy(ft_context *ctx);
 const char *ft_last_error(void); /* thread-local message of the last failing call */
 int         ft_version(void);
 ft_status   ft_get_query_stats(ft_context *ctx, ft_query_stats *out);
+/* Synchronises stream and reports (then clears) the context's device status word: kernels
+ * record bad leaf ids or an exceeded traversal bound there instead of trapping.  Blocking
+ * calls check it themselves; call this after asynchronous self-kNN queries. */
+ft_status   ft_check_device_status(ft_context *ctx, ft_stream_t stream);
 
 /* ---------------------------------------------------------------------------------- */
 /* Trees: TreeSoA(q, n) / TreeSoA::free (src/hlbvh.hpp:632-672) and                    */
