@@ -122,7 +122,9 @@ def test_range_query_matches_oracle(cfg, max_per):
     orr, oc = O.range_query(opts, ot, qx, qy, qz, rmin, rmax, max_per)
     gc = gc.cpu().numpy()
     assert np.array_equal(gc, oc)
-    gr = gr.cpu().numpy().reshape(300, max_per) if max_per else gr.cpu().numpy()
+    if max_per == 0:
+        return
+    gr = gr.cpu().numpy().reshape(300, max_per)
     for i in range(300):
         m = min(oc[i], max_per)
         assert np.array_equal(gr[i, :m], orr[i, :m])
