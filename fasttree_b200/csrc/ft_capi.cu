@@ -214,7 +214,11 @@ ft_status ft_context_create(const ft_options *opts, int device, ft_context **out
 }
 
 ft_status ft_context_destroy(ft_context *ctx) {
-    if (ctx && ctx->status) cudaFree(ctx->status);
+    if (ctx) {
+        if (ctx->status) cudaFree(ctx->status);
+        if (ctx->replay_ranks) cudaFree(ctx->replay_ranks);
+        if (ctx->replay_rows) cudaFree(ctx->replay_rows);
+    }
     delete ctx;
     return FT_OK;
 }
@@ -230,6 +234,15 @@ ft_status ft_check_device_status(ft_context *ctx, ft_stream_t stream) {
 ft_status ft_get_query_stats(ft_context *ctx, ft_query_stats *out) {
     FT_API_BEGIN
     need(ctx && out, "null argument");
+    if (ctx->last_fast) { // replay count of the last fast self-kNN (synchronises the device)
+        DeviceGuard g(ctx->device);
+        uint32_t    w[3] = {0, 0, 0};
+        FT_CUDA(cudaMemcpy(w, ctx->status + 1, sizeof(w), cudaMemcpyDeviceToHost));
+        ctx->stats.replayed = w[0];
+        unsigned long long v;
+        std::memcpy(&v, &w[1], sizeof(v));
+        ctx->stats.reserved[0] = (int64_t)v; // lane-node visits of the fast walk
+    }
     *out = ctx->stats;
     FT_API_END
 }

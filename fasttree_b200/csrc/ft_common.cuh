@@ -86,14 +86,31 @@ template <class T> struct Metric {
             return (long long)((int32_t)((uint32_t)(a - b) << C::shift_bits) >> C::shift_bits);
         }
     }
-    // periodic integer axis (1021-1033)
+    // periodic integer axis (1021-1033): inside [lo, hi] -> 0, else the smaller of the two
+    // wrapped gaps, shifted.  Same value as the reference's formulation, fewer operations:
+    //  * inside test: for lo <= hi, lo <= v <= hi  <=>  (v - lo) <= (hi - lo) as unsigned;
+    //    for lo > hi the reference's test is false and so is the fallback compare used here;
+    //  * a wrapped gap is x = sext_B(v - b); y = (v - b) << SHIFT_BITS holds x << SHIFT_BITS
+    //    exactly, so |x| >> DIST_SHIFT == |y| >> (SHIFT_BITS + DIST_SHIFT) with |y| taken as
+    //    an unsigned 64-bit value (covers |x| = 2^(B-1)).
     static FT_D unsigned long long periodic_axis(T v, T lo, T hi) {
-        if constexpr (sizeof(T) >= 8) v &= (T)((T(1) << C::bits) - T(1));
-        if (v >= lo && v <= hi) return 0ull;
-        long long          dl = spd(v, lo), dh = spd(v, hi);
-        unsigned long long al = (unsigned long long)(dl < 0 ? -dl : dl);
-        unsigned long long ah = (unsigned long long)(dh < 0 ? -dh : dh);
-        return ((al < ah) ? al : ah) >> C::dist_shift;
+        if constexpr (sizeof(T) == 8) {
+            v &= (T)((T(1) << C::bits) - T(1));
+            const unsigned long long dl = (unsigned long long)(v - lo), dh = (unsigned long long)(v - hi);
+            const bool inside = (lo <= hi) ? (dl <= (unsigned long long)(hi - lo)) : false;
+            const long long  yl = (long long)(dl << C::shift_bits), yh = (long long)(dh << C::shift_bits);
+            const unsigned long long al = yl < 0 ? 0ull - (unsigned long long)yl : (unsigned long long)yl;
+            const unsigned long long ah = yh < 0 ? 0ull - (unsigned long long)yh : (unsigned long long)yh;
+            constexpr int s  = C::shift_bits + C::dist_shift; // 33 for 42-bit positions
+            const uint32_t gl = (uint32_t)(al >> s), gh = (uint32_t)(ah >> s);
+            return inside ? 0ull : (unsigned long long)min(gl, gh);
+        } else {
+            if (v >= lo && v <= hi) return 0ull;
+            long long          dl = spd(v, lo), dh = spd(v, hi);
+            unsigned long long al = (unsigned long long)(dl < 0 ? -dl : dl);
+            unsigned long long ah = (unsigned long long)(dh < 0 ? -dh : dh);
+            return ((al < ah) ? al : ah) >> C::dist_shift;
+        }
     }
     static FT_D unsigned long long sq(unsigned long long g) {
         // gaps are < 2^32 for every configuration, so a 32x32->64 multiply is exact

@@ -1,0 +1,437 @@
+// ft_fast.cu -- fast self-kNN with exact fallback ("method 1").
+//
+// A warp takes 32 consecutive queries (sorted leaves, i.e. neighbours along the SFC).
+//  1. Seeding: each lane inserts the leaves of its SFC window [r - h, r + h] into its heap,
+//     so the heap is full, and pruning effective, before the tree walk starts.
+//  2. Walk: one stack shared by the warp.  A node is expanded when any lane still needs it;
+//     each lane tests its own distance against its own heap maximum (and its optional
+//     per-query bound), pushes leaves it needs, and the warp orders the two children by the
+//     majority of the lanes' near/far votes.  Control flow is warp-uniform except the heap
+//     insertion itself.
+//  3. Exactness: the result set is the exact k nearest; only the order among equal distances
+//     can differ from the reference (its per-lane visit order and heap history decide it).
+//     A lane flags its query when any tie could matter -- equal distances inside the top k,
+//     a candidate or a pruned node at exactly the current k-th distance, an eviction that
+//     leaves an equal maximum -- or when its bound cut off a possible neighbour.  Flagged
+//     queries are rerun by the reference traversal (exact_replay_kernel).  Trees taller than
+//     62 levels (where the reference's stack guard can drop subtrees) always take the
+//     reference traversal.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "ft_common.cuh"
+#include "ft_internal.h"
+
+namespace ft {
+
+static constexpr int kFastStack = 64;
+static constexpr int kFastWarps = 4;
+static constexpr int kFastThreads = 32 * kFastWarps;
+
+template <class T, bool PER, int KC, int VAR>
+__global__ void __launch_bounds__(kFastThreads)
+    fast_self_knn_kernel(TreeDev<T> t, const int32_t *__restrict__ leaf_ids, int num, int k, int half_window,
+                         int exclude_self, int ret_orig, const typename Coord<T>::dist_t *__restrict__ bound,
+                         unsigned long long *__restrict__ out_idx, typename Coord<T>::dist_t *__restrict__ out_dist,
+                         int32_t *__restrict__ replay_ranks, int32_t *__restrict__ replay_rows,
+                         uint32_t *replay_count, uint32_t *status, unsigned long long *visit_count) {
+    using D = typename Coord<T>::dist_t;
+    extern __shared__ __align__(16) unsigned char smem[];
+    D       *hd  = reinterpret_cast<D *>(smem);
+    int32_t *hix = reinterpret_cast<int32_t *>(hd + KC * kFastThreads);
+    __shared__ int32_t s_node[kFastWarps][kFastStack];
+
+    const int      tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const unsigned FULL = 0xffffffffu;
+    const int      qbase = (blockIdx.x * kFastWarps + warp) * 32;
+    if (qbase >= num) return; // warp-uniform
+    const int q      = qbase + lane;
+    bool      active = q < num;
+    const int n      = t.n;
+#define HD(s) hd[(s) * kFastThreads + tid]
+#define HI(s) hix[(s) * kFastThreads + tid]
+
+    int rank = active ? (leaf_ids ? leaf_ids[q] : q) : 0;
+    if (active && (rank < 0 || rank >= n)) {
+        atomicOr(status, STATUS_BAD_INPUT);
+        for (int i = 0; i < k; ++i) {
+            out_idx[(size_t)q * k + i]  = ~0ull;
+            out_dist[(size_t)q * k + i] = dist_missing<D>();
+        }
+        active = false;
+        rank   = 0;
+    }
+    const int slot      = rank + n - 1;
+    const T   px        = t.min_x[slot], py = t.min_y[slot], pz = t.min_z[slot];
+    const int self_leaf = exclude_self ? slot : -1;
+    const D   B         = (bound && active) ? bound[q] : dist_heap_max<D>();
+
+    int  count = 0;
+    D    hmax  = D(0);
+    bool flag  = false;
+
+    auto insert = [&](D d2, int32_t id) {
+        if (count < k) {
+            int i = count;
+            while (i > 0) {
+                int p  = (i - 1) >> 1;
+                D   pd = HD(p);
+                if (d2 <= pd) break;
+                HD(i) = pd;
+                HI(i) = HI(p);
+                i     = p;
+            }
+            HD(i) = d2;
+            HI(i) = id;
+            ++count;
+            if (count == k) hmax = HD(0);
+        } else if (d2 < hmax) {
+            const D old = hmax;
+            int     i   = 0;
+            for (;;) {
+                int l = 2 * i + 1;
+                if (l >= k) break;
+                int r  = l + 1;
+                int c  = i;
+                D   cd = d2;
+                D   ld = HD(l);
+                if (ld > cd) {
+                    c  = l;
+                    cd = ld;
+                }
+                if (r < k) {
+                    D rd = HD(r);
+                    if (rd > cd) {
+                        c  = r;
+                        cd = rd;
+                    }
+                }
+                if (c == i) break;
+                HD(i) = cd;
+                HI(i) = HI(c);
+                i     = c;
+            }
+            HD(i) = d2;
+            HI(i) = id;
+            hmax  = HD(0);
+            if (hmax == old) flag = true; // an equal distance stays at the boundary
+        } else if (d2 == hmax) {
+            flag = true; // a candidate at exactly the k-th distance was left out
+        }
+    };
+
+    // ---- 1. seed from the SFC window ----
+    const int W  = min(n, 2 * half_window + 1);
+    const int w0 = active ? max(0, min(rank - half_window, n - W)) : 0;
+    const int w1 = active ? w0 + W - 1 : -1;
+    for (int j = 0; j < W; ++j) {
+        const int leaf = w0 + j;
+        if (active && leaf + n - 1 != self_leaf) {
+            const int s  = leaf + n - 1;
+            const D   d2 = Metric<T>::template dist<PER>(px, py, pz, t.min_x[s], t.max_x[s], t.min_y[s], t.max_y[s],
+                                                       t.min_z[s], t.max_z[s]);
+            insert(d2, ret_orig ? t.orig_idx[s] : leaf);
+        }
+    }
+
+    // ---- 2. walk ----
+    D   sd[kFastStack];
+    int sp = 1;
+    sd[0]  = Metric<T>::template dist<PER>(px, py, pz, t.min_x[0], t.max_x[0], t.min_y[0], t.max_y[0], t.min_z[0],
+                                          t.max_z[0]);
+    long long budget = 2ll * n + 64;
+    long long visits = 0;
+    // A node is needed unless it is strictly beyond the lane's bound or its k-th distance.
+    // Nodes at exactly the k-th distance are walked (not pruned), so any other point at
+    // that distance reaches insert() and raises the tie flag there.
+    auto needs = [&](D d2) { return active && !(d2 > B) && !(count >= k && d2 > hmax); };
+    if constexpr (VAR == 2) {
+        // per-lane walk over internal nodes only: leaf children go to the heap as soon as
+        // their parent is expanded, the nearer internal child is walked next from registers
+        // and only the farther one is stacked.  Every iteration is one expansion, so lanes
+        // of a warp run the same instructions.
+        int  sn[kFastStack];
+        int  cur  = 0;
+        bool have = active && n > 1 && needs(sd[0]);
+        sp        = 0;
+        while (have) {
+            if (--budget < 0) {
+                atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+                break;
+            }
+            ++visits;
+            T   lb[6], rb[6];
+            int l, r;
+            load_rec(t.recs, cur, lb, rb, l, r);
+            const D    ld2 = Metric<T>::template dist<PER>(px, py, pz, lb[0], lb[1], lb[2], lb[3], lb[4], lb[5]);
+            const D    rd2 = Metric<T>::template dist<PER>(px, py, pz, rb[0], rb[1], rb[2], rb[3], rb[4], rb[5]);
+            const bool lleaf = l >= n - 1, rleaf = r >= n - 1;
+            if (lleaf && needs(ld2) && (l - (n - 1) < w0 || l - (n - 1) > w1) && l != self_leaf)
+                insert(ld2, ret_orig ? t.orig_idx[l] : l - (n - 1));
+            if (rleaf && needs(rd2) && (r - (n - 1) < w0 || r - (n - 1) > w1) && r != self_leaf)
+                insert(rd2, ret_orig ? t.orig_idx[r] : r - (n - 1));
+            const bool li = !lleaf && needs(ld2), ri = !rleaf && needs(rd2);
+            if (li && ri) {
+                const bool ln = ld2 <= rd2;
+                if (sp >= kFastStack) {
+                    atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+                    break;
+                }
+                sn[sp] = ln ? r : l;
+                sd[sp] = ln ? rd2 : ld2;
+                ++sp;
+                cur = ln ? l : r;
+            } else if (li) {
+                cur = l;
+            } else if (ri) {
+                cur = r;
+            } else {
+                have = false;
+                while (sp > 0) {
+                    --sp;
+                    if (needs(sd[sp])) {
+                        cur  = sn[sp];
+                        have = true;
+                        break;
+                    }
+                }
+            }
+        }
+        sp = 0;
+    }
+    if constexpr (VAR == 1) {
+        // per-lane walk: own stack, own near-first order (the reference's order)
+        int sn[kFastStack];
+        sn[0] = 0;
+        if (!active) sp = 0;
+        while (sp > 0) {
+            if (--budget < 0) {
+                atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+                break;
+            }
+            --sp;
+            const int node = sn[sp];
+            const D   d2   = sd[sp];
+            if (!needs(d2)) continue;
+            ++visits;
+            if (node >= n - 1) {
+                const int lr = node - (n - 1);
+                if ((lr < w0 || lr > w1) && node != self_leaf) insert(d2, ret_orig ? t.orig_idx[node] : lr);
+            } else {
+                T   lb[6], rb[6];
+                int l, r;
+                load_rec(t.recs, node, lb, rb, l, r);
+                const D ld2 = Metric<T>::template dist<PER>(px, py, pz, lb[0], lb[1], lb[2], lb[3], lb[4], lb[5]);
+                const D rd2 = Metric<T>::template dist<PER>(px, py, pz, rb[0], rb[1], rb[2], rb[3], rb[4], rb[5]);
+                if (sp + 2 > kFastStack) {
+                    atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+                    break;
+                }
+                const bool ln = ld2 <= rd2;
+                if (needs(ln ? rd2 : ld2)) {
+                    sn[sp] = ln ? r : l;
+                    sd[sp] = ln ? rd2 : ld2;
+                    ++sp;
+                }
+                if (needs(ln ? ld2 : rd2)) {
+                    sn[sp] = ln ? l : r;
+                    sd[sp] = ln ? ld2 : rd2;
+                    ++sp;
+                }
+            }
+        }
+        sp = 0;
+    }
+    constexpr bool SHARED = VAR == 0;
+    if (SHARED && lane == 0) s_node[warp][0] = 0;
+    __syncwarp();
+    while (SHARED && sp > 0) {
+        if (--budget < 0) {
+            if (lane == 0) atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+            break;
+        }
+        --sp;
+        const int  node = s_node[warp][sp];
+        const D    d2   = sd[sp];
+        const bool nd   = needs(d2);
+        if (!__any_sync(FULL, nd)) continue;
+        ++visits;
+        if (node >= n - 1) {
+            const int lr = node - (n - 1);
+            // window leaves were already offered to the heap during seeding
+            if (nd && (lr < w0 || lr > w1) && node != self_leaf) insert(d2, ret_orig ? t.orig_idx[node] : lr);
+        } else {
+            T   lb[6], rb[6];
+            int l, r;
+            load_rec(t.recs, node, lb, rb, l, r);
+            const D  ld2 = Metric<T>::template dist<PER>(px, py, pz, lb[0], lb[1], lb[2], lb[3], lb[4], lb[5]);
+            const D  rd2 = Metric<T>::template dist<PER>(px, py, pz, rb[0], rb[1], rb[2], rb[3], rb[4], rb[5]);
+            const bool nl = needs(ld2), nr = needs(rd2);
+            const unsigned bl = __ballot_sync(FULL, nl), br = __ballot_sync(FULL, nr);
+            if (bl | br) {
+                if (sp + 2 > kFastStack) {
+                    if (lane == 0) atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+                    break;
+                }
+                const unsigned votes     = __ballot_sync(FULL, (nl || nr) && ld2 <= rd2);
+                const bool     left_near = 2 * __popc(votes) >= __popc(bl | br);
+                // push the farther child first so the nearer one is walked next
+                const int  first = left_near ? r : l, second = left_near ? l : r;
+                const D    fd = left_near ? rd2 : ld2, sd2 = left_near ? ld2 : rd2;
+                const bool fneed = left_near ? (br != 0) : (bl != 0);
+                const bool sneed = left_near ? (bl != 0) : (br != 0);
+                if (fneed) {
+                    if (lane == 0) s_node[warp][sp] = first;
+                    sd[sp] = fd;
+                    ++sp;
+                }
+                if (sneed) {
+                    if (lane == 0) s_node[warp][sp] = second;
+                    sd[sp] = sd2;
+                    ++sp;
+                }
+                __syncwarp();
+            }
+        }
+    }
+
+    // visit statistics: lane-node evaluations summed per warp
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) visits += __shfl_down_sync(FULL, visits, off);
+    if (lane == 0 && visit_count) atomicAdd(visit_count, (unsigned long long)visits);
+
+    // ---- 3. sort, check, write ----
+    if (active) {
+        if (count >= k && hmax > B) flag = true;             // the bound may have cut a neighbour
+        if (count < k && B != dist_heap_max<D>()) flag = true; // fewer than k inside the bound
+        for (int hs = count; hs > 1; --hs) {
+            D       last  = HD(hs - 1);
+            int32_t lasti = HI(hs - 1);
+            HD(hs - 1)    = HD(0);
+            HI(hs - 1)    = HI(0);
+            const int size = hs - 1;
+            int       i    = 0;
+            for (;;) {
+                int l = 2 * i + 1;
+                if (l >= size) break;
+                int r  = l + 1;
+                int c  = i;
+                D   cd = last;
+                D   ld = HD(l);
+                if (ld > cd) {
+                    c  = l;
+                    cd = ld;
+                }
+                if (r < size) {
+                    D rd = HD(r);
+                    if (rd > cd) {
+                        c  = r;
+                        cd = rd;
+                    }
+                }
+                if (c == i) break;
+                HD(i) = cd;
+                HI(i) = HI(c);
+                i     = c;
+            }
+            HD(i) = last;
+            HI(i) = lasti;
+        }
+        for (int i = 1; i < count; ++i)
+            if (HD(i) == HD(i - 1)) flag = true;
+        const size_t off = (size_t)q * (size_t)k;
+        for (int i = 0; i < k; ++i) {
+            if (i < count) {
+                __stcs(out_idx + off + i, (unsigned long long)(long long)HI(i));
+                __stcs(out_dist + off + i, HD(i));
+            } else {
+                __stcs(out_idx + off + i, ~0ull);
+                __stcs(out_dist + off + i, dist_missing<D>());
+            }
+        }
+        if (flag) {
+            uint32_t at      = atomicAdd(replay_count, 1u);
+            replay_ranks[at] = rank;
+            replay_rows[at]  = q;
+        }
+    }
+#undef HD
+#undef HI
+}
+
+// -----------------------------------------------------------------------------------------
+template <class T, bool PER, int KC>
+static void launch_fast_t(const TreeDev<T> &tv, const int32_t *leaf_ids, int num, int k, int half, bool excl, bool ro,
+                          const void *bound, uint64_t *idx, void *dist, int32_t *rr, int32_t *rw, uint32_t *rc,
+                          uint32_t *status, int variant, unsigned long long *visits, cudaStream_t st) {
+    using D     = typename Coord<T>::dist_t;
+    size_t smem = (size_t)KC * kFastThreads * (sizeof(D) + 4);
+    auto   fn   = variant == 0 ? fast_self_knn_kernel<T, PER, KC, 0>
+                  : variant == 1 ? fast_self_knn_kernel<T, PER, KC, 1>
+                                 : fast_self_knn_kernel<T, PER, KC, 2>;
+    FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int blocks = (num + kFastThreads - 1) / kFastThreads;
+    fn<<<blocks, kFastThreads, smem, st>>>(tv, leaf_ids, num, k, half, excl ? 1 : 0, ro ? 1 : 0, (const D *)bound,
+                                           (unsigned long long *)idx, (D *)dist, rr, rw, rc, status, visits);
+    FT_CUDA(cudaGetLastError());
+}
+
+template <class T>
+static void launch_fast(const ft_options &o, const ft_tree &tr, const int32_t *leaf_ids, int num, int k, int half,
+                        bool excl, const void *bound, uint64_t *idx, void *dist, int32_t *rr, int32_t *rw,
+                        uint32_t *rc, uint32_t *status, int variant, unsigned long long *visits, cudaStream_t st) {
+    TreeDev<T> tv;
+    tv.min_x    = (const T *)tr.min_x;
+    tv.max_x    = (const T *)tr.max_x;
+    tv.min_y    = (const T *)tr.min_y;
+    tv.max_y    = (const T *)tr.max_y;
+    tv.min_z    = (const T *)tr.min_z;
+    tv.max_z    = (const T *)tr.max_z;
+    tv.orig_idx = tr.orig_idx;
+    tv.recs     = (const NodeRec<T> *)((TreeImpl *)tr.impl)->recs;
+    tv.n        = (int)tr.num_leaves;
+    bool ro     = o.return_orig_indices != 0;
+    bool per    = !Coord<T>::is_float && o.periodic;
+#define FT_FAST(PER, KC) launch_fast_t<T, PER, KC>(tv, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc, status, variant, visits, st)
+    if (k <= 32) {
+        if (per) FT_FAST(true, 32);
+        else FT_FAST(false, 32);
+    } else {
+        if (per) FT_FAST(true, 64);
+        else FT_FAST(false, 64);
+    }
+#undef FT_FAST
+}
+
+bool fast_self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, bool excl,
+                   uint64_t *idx, void *dist, const void *bound, int half_window, int variant, cudaStream_t st) {
+    TreeImpl *impl = (TreeImpl *)tr.impl;
+    if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0 || impl->height_root > 62) return false;
+    if (half_window <= 0) half_window = k;
+    ensure_replay(ctx, num);
+    uint32_t           *rc     = ctx.status + 1;
+    unsigned long long *visits = (unsigned long long *)(ctx.status + 2);
+    FT_CUDA(cudaMemsetAsync(rc, 0, 3 * sizeof(uint32_t), st));
+    switch (ctx.opts.coord_type) {
+    case F32: launch_fast<float>(ctx.opts, tr, leaf_ids, (int)num, k, half_window, excl, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st); break;
+    case F64: launch_fast<double>(ctx.opts, tr, leaf_ids, (int)num, k, half_window, excl, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st); break;
+    case U32: launch_fast<uint32_t>(ctx.opts, tr, leaf_ids, (int)num, k, half_window, excl, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st); break;
+    case U64: launch_fast<unsigned long long>(ctx.opts, tr, leaf_ids, (int)num, k, half_window, excl, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st); break;
+    }
+    replay_exact(ctx, tr, ctx.replay_ranks, ctx.replay_rows, rc, k, excl, idx, dist, st);
+    return true;
+}
+
+void ensure_replay(Context &ctx, size_t num) {
+    if (num <= ctx.replay_cap && ctx.replay_ranks) return;
+    if (ctx.replay_ranks) cudaFree(ctx.replay_ranks);
+    if (ctx.replay_rows) cudaFree(ctx.replay_rows);
+    ctx.replay_ranks = ctx.replay_rows = nullptr;
+    size_t cap = num + num / 4 + 1024;
+    FT_CUDA(cudaMalloc(&ctx.replay_ranks, cap * sizeof(int32_t)));
+    FT_CUDA(cudaMalloc(&ctx.replay_rows, cap * sizeof(int32_t)));
+    ctx.replay_cap = cap;
+}
+
+} // namespace ft

@@ -54,8 +54,22 @@ struct Context {
     int            device = 0;
     int            num_sms = 148;
     ft_query_stats stats{};
-    uint32_t      *status = nullptr; // device status word of query kernels
+    uint32_t      *status = nullptr; // [0] status word of query kernels, [1] replay count
+    int32_t       *replay_ranks = nullptr; // queries the fast traversal hands to the exact one
+    int32_t       *replay_rows  = nullptr;
+    size_t         replay_cap   = 0;
+    bool           last_fast    = false; // the last self-kNN call used the fast traversal
 };
+
+// ---- fast self-kNN (ft_fast.cu) ----
+// Returns false when the fast traversal does not apply (k > 64, tree taller than 62).
+bool fast_self_knn(Context &ctx, const ft_tree &tree, const int32_t *leaf_ids, size_t num, int k, bool exclude_self,
+                   uint64_t *idx, void *dist, const void *bound, int half_window, int variant, cudaStream_t st);
+void ensure_replay(Context &ctx, size_t num);
+// Reruns the listed self queries (ranks[i] -> row rows[i], *count_dev of them) with the
+// reference traversal (ft_query.cu).
+void replay_exact(Context &ctx, const ft_tree &tree, const int32_t *ranks, const int32_t *rows, uint32_t *count_dev,
+                  int k, bool exclude_self, uint64_t *idx, void *dist, cudaStream_t st);
 
 // Reads and clears a device status word (synchronises the stream); throws on a set bit.
 void check_device_status(uint32_t *status, cudaStream_t st);

@@ -37,48 +37,17 @@ FT_D D node_dist_soa(const TreeDev<T> &t, int node, T px, T py, T pz) {
 // -----------------------------------------------------------------------------------------
 // Exact kNN: SELF = self_knn_query[_subset] (query = sorted leaf), else knn_query small-k.
 // -----------------------------------------------------------------------------------------
-template <class T, int CAP, int QT, bool SELF, bool PER>
-__global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t, const T *__restrict__ qx,
-                                                       const T *__restrict__ qy, const T *__restrict__ qz,
-                                                       const int32_t *__restrict__ leaf_ids, int num, int k,
-                                                       int exclude_self, int ret_orig,
-                                                       unsigned long long *__restrict__ out_idx,
-                                                       typename Coord<T>::dist_t *__restrict__ out_dist,
-                                                       uint32_t *status) {
-    using D = typename Coord<T>::dist_t;
-    extern __shared__ __align__(16) unsigned char smem[];
-    D       *hd  = reinterpret_cast<D *>(smem);
-    int32_t *hix = reinterpret_cast<int32_t *>(hd + CAP * QT);
-    const int tid = threadIdx.x;
-    const int q   = blockIdx.x * QT + tid;
-    if (q >= num) return;
+// One query with the reference's traversal and heap; the heap rows live in shared memory
+// at hd[slot * QT + tid] / hix[slot * QT + tid].  Writes the k results of row `row`.
+template <class T, int CAP, int QT, bool PER>
+FT_D void exact_query(const TreeDev<T> &t, T px, T py, T pz, int self_leaf, int k, int ret_orig,
+                      typename Coord<T>::dist_t *hd, int32_t *hix, int tid, size_t row,
+                      unsigned long long *__restrict__ out_idx, typename Coord<T>::dist_t *__restrict__ out_dist,
+                      uint32_t *status) {
+    using D     = typename Coord<T>::dist_t;
     const int n = t.n;
 #define HD(s) hd[(s) * QT + tid]
 #define HI(s) hix[(s) * QT + tid]
-
-    T   px, py, pz;
-    int self_leaf = -1;
-    if (SELF) {
-        int rank = leaf_ids ? leaf_ids[q] : q;
-        if (rank < 0 || rank >= n) { // invalid caller leaf id: empty row, flag the call
-            atomicOr(status, STATUS_BAD_INPUT);
-            for (int i = 0; i < k; ++i) {
-                out_idx[(size_t)q * k + i]  = ~0ull;
-                out_dist[(size_t)q * k + i] = dist_missing<D>();
-            }
-            return;
-        }
-        int slot = rank + n - 1;
-        px = t.min_x[slot];
-        py = t.min_y[slot];
-        pz = t.min_z[slot];
-        if (exclude_self) self_leaf = slot;
-    } else {
-        px = qx[q];
-        py = qy[q];
-        pz = qz[q];
-    }
-
     int sn[kStack];
     D   sd[kStack];
     int sp = 1;
@@ -200,7 +169,7 @@ __global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t, const T *__
         HD(i) = last;
         HI(i) = lasti;
     }
-    const size_t off = (size_t)q * (size_t)k;
+    const size_t off = row * (size_t)k;
     for (int i = 0; i < k; ++i) {
         if (i < count) {
             __stcs(out_idx + off + i, (unsigned long long)(long long)HI(i));
@@ -212,6 +181,83 @@ __global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t, const T *__
     }
 #undef HD
 #undef HI
+}
+
+// Query point of a self query (sorted leaf `rank`); false (and an empty row) for a bad id.
+template <class T>
+FT_D bool self_point(const TreeDev<T> &t, int rank, int k, size_t row, unsigned long long *out_idx,
+                     typename Coord<T>::dist_t *out_dist, uint32_t *status, T &px, T &py, T &pz) {
+    using D = typename Coord<T>::dist_t;
+    if (rank < 0 || rank >= t.n) { // invalid caller leaf id: empty row, flag the call
+        atomicOr(status, STATUS_BAD_INPUT);
+        for (int i = 0; i < k; ++i) {
+            out_idx[row * k + i]  = ~0ull;
+            out_dist[row * k + i] = dist_missing<D>();
+        }
+        return false;
+    }
+    int slot = rank + t.n - 1;
+    px       = t.min_x[slot];
+    py       = t.min_y[slot];
+    pz       = t.min_z[slot];
+    return true;
+}
+
+template <class T, int CAP, int QT, bool SELF, bool PER>
+__global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t, const T *__restrict__ qx,
+                                                       const T *__restrict__ qy, const T *__restrict__ qz,
+                                                       const int32_t *__restrict__ leaf_ids, int num, int k,
+                                                       int exclude_self, int ret_orig,
+                                                       unsigned long long *__restrict__ out_idx,
+                                                       typename Coord<T>::dist_t *__restrict__ out_dist,
+                                                       uint32_t *status) {
+    using D = typename Coord<T>::dist_t;
+    extern __shared__ __align__(16) unsigned char smem[];
+    D       *hd  = reinterpret_cast<D *>(smem);
+    int32_t *hix = reinterpret_cast<int32_t *>(hd + CAP * QT);
+    const int tid = threadIdx.x;
+    const int q   = blockIdx.x * QT + tid;
+    if (q >= num) return;
+    T   px, py, pz;
+    int self_leaf = -1;
+    if (SELF) {
+        int rank = leaf_ids ? leaf_ids[q] : q;
+        if (!self_point(t, rank, k, (size_t)q, out_idx, out_dist, status, px, py, pz)) return;
+        if (exclude_self) self_leaf = rank + t.n - 1;
+    } else {
+        px = qx[q];
+        py = qy[q];
+        pz = qz[q];
+    }
+    exact_query<T, CAP, QT, PER>(t, px, py, pz, self_leaf, k, ret_orig, hd, hix, tid, (size_t)q, out_idx, out_dist,
+                                 status);
+}
+
+// Replays the self queries listed by the fast traversal (ranks[i] -> output row rows[i]) with
+// the reference traversal; grid-stride over a count that lives on the device, so no host
+// synchronisation is needed between the two launches.
+template <class T, int CAP, int QT, bool PER>
+__global__ void __launch_bounds__(QT) exact_replay_kernel(TreeDev<T> t, const int32_t *__restrict__ ranks,
+                                                          const int32_t *__restrict__ rows,
+                                                          const uint32_t *__restrict__ count_dev, int k,
+                                                          int exclude_self, int ret_orig,
+                                                          unsigned long long *__restrict__ out_idx,
+                                                          typename Coord<T>::dist_t *__restrict__ out_dist,
+                                                          uint32_t *status) {
+    using D = typename Coord<T>::dist_t;
+    extern __shared__ __align__(16) unsigned char smem[];
+    D       *hd    = reinterpret_cast<D *>(smem);
+    int32_t *hix   = reinterpret_cast<int32_t *>(hd + CAP * QT);
+    const int tid  = threadIdx.x;
+    const int cnt  = (int)*count_dev;
+    for (int i = blockIdx.x * QT + tid; i < cnt; i += gridDim.x * QT) {
+        const int rank = ranks[i];
+        const int row  = rows[i];
+        T         px, py, pz;
+        if (!self_point(t, rank, k, (size_t)row, out_idx, out_dist, status, px, py, pz)) continue;
+        exact_query<T, CAP, QT, PER>(t, px, py, pz, exclude_self ? rank + t.n - 1 : -1, k, ret_orig, hd, hix, tid,
+                                     (size_t)row, out_idx, out_dist, status);
+    }
 }
 
 // -----------------------------------------------------------------------------------------
@@ -474,13 +520,59 @@ void self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t n
     if (tr.num_leaves == 0 || num == 0 || k <= 0) return;
     if (k > kMaxExactK) fail(FT_ERR_RUNTIME, "self_knn_query: k too large for shared memory.");
     if (num > (size_t)INT32_MAX) fail(FT_ERR_INVALID_ARGUMENT, "too many queries");
-    ctx.stats.queries = (int64_t)num;
+    ctx.stats.queries  = (int64_t)num;
     ctx.stats.replayed = 0;
+    ctx.last_fast      = false;
+    if (qo.method == 1 &&
+        fast_self_knn(ctx, tr, leaf_ids, num, k, excl, idx, dist, nullptr, qo.reserved[0], qo.reserved[1], st)) {
+        ctx.last_fast = true;
+        return;
+    }
     switch (ctx.opts.coord_type) {
     case F32: launch_exact<float, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, ctx.status, st); break;
     case F64: launch_exact<double, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, ctx.status, st); break;
     case U32: launch_exact<uint32_t, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, ctx.status, st); break;
     case U64: launch_exact<unsigned long long, true>(ctx.opts, tr, nullptr, nullptr, nullptr, leaf_ids, (int)num, k, excl, idx, dist, ctx.status, st); break;
+    }
+}
+
+template <class T, int CAP, int QT, bool PER>
+static void replay_t(const TreeDev<T> &tv, const int32_t *ranks, const int32_t *rows, uint32_t *cnt, int k, bool excl,
+                     bool ro, uint64_t *idx, void *dist, uint32_t *status, int num_sms, cudaStream_t st) {
+    using D     = typename Coord<T>::dist_t;
+    size_t smem = (size_t)CAP * QT * (sizeof(D) + 4);
+    auto   fn   = exact_replay_kernel<T, CAP, QT, PER>;
+    FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    fn<<<num_sms * 4, QT, smem, st>>>(tv, ranks, rows, cnt, k, excl ? 1 : 0, ro ? 1 : 0, (unsigned long long *)idx,
+                                       (D *)dist, status);
+    FT_CUDA(cudaGetLastError());
+}
+
+template <class T>
+static void replay_typed(Context &ctx, const ft_tree &tr, const int32_t *ranks, const int32_t *rows, uint32_t *cnt,
+                         int k, bool excl, uint64_t *idx, void *dist, cudaStream_t st) {
+    TreeDev<T> tv  = dev_view<T>(tr);
+    bool       ro  = ctx.opts.return_orig_indices != 0;
+    bool       per = !Coord<T>::is_float && ctx.opts.periodic;
+    int        sms = ctx.num_sms;
+#define FT_RP(CAP, QT)                                                                                          \
+    (per ? replay_t<T, CAP, QT, true>(tv, ranks, rows, cnt, k, excl, ro, idx, dist, ctx.status, sms, st)        \
+         : replay_t<T, CAP, QT, false>(tv, ranks, rows, cnt, k, excl, ro, idx, dist, ctx.status, sms, st))
+    if (k <= 32) FT_RP(32, 128);
+    else if (k <= 64) FT_RP(64, 128);
+    else if (k <= 128) FT_RP(128, 64);
+    else if (k <= 256) FT_RP(256, 32);
+    else FT_RP(512, 32);
+#undef FT_RP
+}
+
+void replay_exact(Context &ctx, const ft_tree &tr, const int32_t *ranks, const int32_t *rows, uint32_t *cnt, int k,
+                  bool excl, uint64_t *idx, void *dist, cudaStream_t st) {
+    switch (ctx.opts.coord_type) {
+    case F32: replay_typed<float>(ctx, tr, ranks, rows, cnt, k, excl, idx, dist, st); break;
+    case F64: replay_typed<double>(ctx, tr, ranks, rows, cnt, k, excl, idx, dist, st); break;
+    case U32: replay_typed<uint32_t>(ctx, tr, ranks, rows, cnt, k, excl, idx, dist, st); break;
+    case U64: replay_typed<unsigned long long>(ctx, tr, ranks, rows, cnt, k, excl, idx, dist, st); break;
     }
 }
 

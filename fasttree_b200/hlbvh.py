@@ -94,7 +94,7 @@ class Context:
     def query_stats(self):
         s = capi.FtQueryStats()
         check(lib().ft_get_query_stats(self._h, ctypes.byref(s)))
-        return {"queries": s.queries, "replayed": s.replayed}
+        return {"queries": s.queries, "replayed": s.replayed, "visits": s.reserved[0]}
 
     def close(self):
         if getattr(self, "_h", None):
@@ -330,8 +330,11 @@ def build_tree(ctx: Context, tree: TreeSoA, sorted_keys, sorted_x=None, sorted_y
     return tree
 
 
-def _qopts(max_k: int, method: int = 0):
-    return capi.FtQueryOptions(int(max_k), int(method))
+def _qopts(max_k: int, method: int = 0, half_window: int = 0, variant: int = 0):
+    o = capi.FtQueryOptions(int(max_k), int(method))
+    o.reserved[0] = int(half_window)  # fast walk: SFC seeding half-window (0 = k)
+    o.reserved[1] = int(variant)      # fast walk: 0 warp-shared order, 1 per-lane order
+    return o
 
 
 def _alloc_knn_out(ctx: Context, rows: int, k: int):
@@ -341,14 +344,15 @@ def _alloc_knn_out(ctx: Context, rows: int, k: int):
 
 
 def self_knn_query(ctx: Context, tree: TreeSoA, k: int, results=None, result_dists=None, exclude_self=True,
-                   max_k: int = 32, method: int = 0, stream=None):
+                   max_k: int = 32, method: int = 0, stream=None, half_window: int = 0, variant: int = 0):
     """self_knn_query<MAXK> (src/hlbvh.hpp:1929-1954).  Asynchronous; returns (idx, dist) of shape
-    (num_leaves, k)."""
+    (num_leaves, k).  method=1 takes the fast walk (same output, see ft_fast.cu)."""
     n = tree.num_leaves
     if results is None:
         results, result_dists = _alloc_knn_out(ctx, n, k)
     _call(lib().ft_self_knn(ctx.handle, tree.c, None, n, int(k), int(bool(exclude_self)), _ptr(results),
-                            _ptr(result_dists), ctypes.byref(_qopts(max_k, method)), _stream_handle(stream)))
+                            _ptr(result_dists), ctypes.byref(_qopts(max_k, method, half_window, variant)),
+                            _stream_handle(stream)))
     return results.view(n, k) if n * k else results, result_dists.view(n, k) if n * k else result_dists
 
 

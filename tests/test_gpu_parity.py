@@ -219,3 +219,44 @@ def test_invalid_arguments():
         ft.build_bvh(ctx, ft.particles(x, y, z), small)
     with pytest.raises(ValueError):
         ft.Context("u64", "morton")
+
+
+@pytest.mark.parametrize("cfg", CONFIGS, ids=CONFIG_IDS)
+@pytest.mark.parametrize("kind", ["uniform", "clustered", "degenerate"])
+@pytest.mark.parametrize("k", [1, 8, 32, 33, 64])
+def test_fast_self_knn_matches_oracle(cfg, kind, k):
+    """method=1 (warp-shared walk + SFC-window seeding + exact replay of tied queries) gives
+    the reference's output bit for bit."""
+    coord, sfc, per = cfg
+    ctx, opts = make(coord, sfc, per)
+    n = 6000
+    x, y, z = gen(kind, n, coord, seed=15)
+    tree, ot = build_both(ctx, opts, x, y, z)
+    for excl in (True, False):
+        gi, gd = ft.self_knn_query(ctx, tree, k, exclude_self=excl, max_k=max(k, 32), method=1)
+        torch.cuda.synchronize()
+        stats = ctx.query_stats()
+        oi, od = O.self_knn(opts, ot, k, excl)
+        assert np.array_equal(gi.cpu().numpy(), oi), (excl, stats)
+        assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od)), (excl, stats)
+        if kind == "degenerate" and k > 1:
+            assert stats["replayed"] > 0  # duplicate points force the exact replay
+
+
+@pytest.mark.parametrize("cfg", [CONFIGS[1], CONFIGS[7]], ids=[CONFIG_IDS[1], CONFIG_IDS[7]])
+def test_fast_self_knn_subset_and_orig(cfg):
+    coord, sfc, per = cfg
+    for ret_orig in (False, True):
+        ctx, opts = make(coord, sfc, per, ret_orig)
+        n = 5000
+        x, y, z = gen("clustered", n, coord, seed=19)
+        tree, ot = build_both(ctx, opts, x, y, z)
+        rng = np.random.default_rng(1)
+        sub = np.sort(rng.choice(n, 700, replace=False)).astype(np.int32)
+        ids = torch.from_numpy(sub).cuda()
+        for k in (16, 40):
+            gi, gd = ft.self_knn_query_subset(ctx, tree, ids, k, exclude_self=True, method=1)
+            torch.cuda.synchronize()
+            oi, od = O.self_knn(opts, ot, k, True, leaf_ids=sub)
+            assert np.array_equal(gi.cpu().numpy(), oi)
+            assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od))
