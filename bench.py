@@ -45,7 +45,11 @@ def parse():
     p.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1"])
     p.add_argument("--n", type=int, default=0, help="override the point count (tests only)")
     p.add_argument("--k", type=int, default=32)
-    p.add_argument("--method", default="plain", choices=["plain", "fast"])
+    p.add_argument("--method", default="fast", choices=["plain", "fast"],
+                   help="headline method; the other is timed beside it unless --only-headline")
+    p.add_argument("--only-headline", action="store_true")
+    p.add_argument("--half", type=int, default=0, help="fast walk: SFC seeding half-window (0 = k)")
+    p.add_argument("--variant", type=int, default=0, help="fast walk variant (0 = default)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-sample", type=int, default=200_000)
@@ -222,36 +226,49 @@ def run_ours(args):
     height = tree.height()
 
     # ---- self-kNN timing (device-resident tree and outputs) ----
-    method = 1 if args.method == "fast" else 0
     idx = torch.empty(n * k, dtype=torch.uint64, device=dev)
     dst = torch.empty(n * k, dtype=ft.dist_torch_dtype(ctx.coord), device=dev)
-    for _ in range(args.warmup):
-        ft.self_knn_query(ctx, tree, k, idx, dst, exclude_self=True, max_k=max(32, k), method=method)
-    barrier()
+
+    def query(method):
+        ft.self_knn_query(ctx, tree, k, idx, dst, exclude_self=True, max_k=max(32, k), method=method,
+                          half_window=args.half, variant=args.variant)
+
+    def time_method(method):
+        for _ in range(args.warmup):
+            query(method)
+        barrier()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for a, b in evs:
+            a.record(stream)
+            query(method)
+            b.record(stream)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        t_local = torch.tensor([g0.elapsed_time(g1)], device=dev)
+        if world > 1:
+            dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
+        total = float(t_local.item())
+        return total / args.steps, [a.elapsed_time(b) for a, b in evs], ctx.query_stats()
+
+    headline = 1 if args.method == "fast" else 0
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    g0 = torch.cuda.Event(enable_timing=True)
-    g1 = torch.cuda.Event(enable_timing=True)
-    g0.record(stream)
-    for a, b in evs:
-        a.record(stream)
-        ft.self_knn_query(ctx, tree, k, idx, dst, exclude_self=True, max_k=max(32, k), method=method)
-        b.record(stream)
-    g1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
+    results = {}
+    for m in ([0, 1] if not args.only_headline else [headline]):
+        results[m] = time_method(m)
     clocks = sampler.stop()
-    total_ms = g0.elapsed_time(g1)
-    per_launch = [a.elapsed_time(b) for a, b in evs]
-    t_local = torch.tensor([total_ms], device=dev)
-    if world > 1:
-        dist.all_reduce(t_local, op=dist.ReduceOp.MAX)
-    total_ms = float(t_local.item())
-    ms_per_step = total_ms / args.steps
+    ms_per_step, per_launch, stats = results[headline]
     value = world * n / (ms_per_step / 1e3)
-    stats = ctx.query_stats()
+    method = headline
+    plain = None
+    if 0 in results and headline != 0:
+        plain = {"value": world * n / (results[0][0] / 1e3), "unit": "queries/s", "ms_per_step": results[0][0],
+                 "kernel": "exact_knn_kernel (reference traversal and heap)"}
 
     # ---- e2e through the public API with host buffers ----
     e2e = None
@@ -266,7 +283,7 @@ def run_ours(args):
         for _ in range(e_steps):
             dx, dy, dz = (t.to(dev, non_blocking=True) for t in (hx, hy, hz))
             ft.build_bvh(ctx, ft.particles(dx, dy, dz), tree)
-            ft.self_knn_query(ctx, tree, k, idx, dst, exclude_self=True, max_k=max(32, k), method=method)
+            query(method)
             hi.copy_(idx, non_blocking=True)
             hd.copy_(dst, non_blocking=True)
         e1.record(stream)
@@ -294,13 +311,15 @@ def run_ours(args):
         try:
             with open(tf) as f:
                 tj = json.load(f)
-            if tj.get("workload") == w["name"] and tj.get("method") == args.method:
-                traffic = tj.get("bytes_per_launch")
+            entry = tj.get(args.method)
+            if entry and entry.get("workload") == w["name"] and entry.get("n_points") == n:
+                traffic = entry.get("bytes_per_launch")
         except Exception:
             traffic = None
+    kname = "fast_self_knn_kernel (+ exact_replay_kernel)" if method == 1 else "exact_knn_kernel"
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "peak_source": peak_kind,
-                "algorithmic_bytes": alg, "kernel": "exact_knn_kernel (self_knn_query)"}
+                "traffic": traffic, "peak_source": peak_kind, "algorithmic_bytes": alg, "kernel": kname,
+                "note": "latency/ALU bound tree walk; algorithmic bytes = tree (2N-1)*6*s_c + (N-1)*8 + output 16*N*k"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -317,9 +336,9 @@ def run_ours(args):
                "config": {"workload": w["name"], "n_points": n, "k": k, "exclude_self": True,
                           "method": args.method, "parallelism": f"replicas x{world}",
                           "l2": "inputs larger than L2: tree records + boxes ~2.3 GB, output 5.1 GB"},
-               "build_ms": build_ms, "tree_height": height, "query_stats": stats,
-               "e2e": e2e, "gpu_launches": args.steps, "roofline": roofline, "cpu_baseline": cpu,
-               "clocks": clocks}
+               "plain": plain, "build_ms": build_ms, "tree_height": height, "query_stats": stats,
+               "e2e": e2e, "gpu_launches": args.steps * (2 if method == 1 else 1),
+               "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(out), flush=True)
 
 

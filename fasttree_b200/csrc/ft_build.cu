@@ -843,8 +843,10 @@ static void build_bvh_typed(Context &ctx, ft_tree &t, const void *x, const void 
                             cudaStream_t st) {
     TreeImpl &s = *(TreeImpl *)t.impl;
     ensure_scratch(s, ctx.opts, n);
-    // 1. bounding box (only the float encode reads it)
-    if (bbox_host) FT_CUDA(cudaMemcpyAsync(s.bbox, bbox_host, 6 * sizeof(T), cudaMemcpyHostToDevice, st));
+    // 1. bounding box.  Only the float encode reads it; integer encoding ignores it, so an
+    // integer tree always keeps its true box (the query distance mode depends on it).
+    if (bbox_host && Coord<T>::is_float)
+        FT_CUDA(cudaMemcpyAsync(s.bbox, bbox_host, 6 * sizeof(T), cudaMemcpyHostToDevice, st));
     else compute_bbox(ctx, &s, x, y, z, n, s.bbox, st);
     // 2. keys + iota permutation
     if (caller_keys) {

@@ -388,9 +388,13 @@ ft_status ft_build_bvh(ft_context *ctx, const void *x, const void *y, const void
     tree->num_internal = n - 1;
     TreeImpl &impl     = *(TreeImpl *)tree->impl;
     impl.height_root   = -1;
+    impl.clean42       = false;
     ft::build_bvh(*ctx, *tree, sx.dev, sy.dev, sz.dev, n, (const uint32_t *)sid.dev, (const int8_t *)sgh.dev, bbox6,
                   sk.dev, st);
     if (keys) sk.copy_back();
+    uint64_t box[6] = {0, 0, 0, 0, 0, 0};
+    if (ctx->opts.coord_type == FT_COORD_U64)
+        FT_CUDA(cudaMemcpyAsync(box, impl.bbox, sizeof(box), cudaMemcpyDeviceToHost, st));
     if (n > 1) {
         uint8_t h = 0;
         FT_CUDA(cudaMemcpyAsync(&h, impl.height, 1, cudaMemcpyDeviceToHost, st));
@@ -400,6 +404,9 @@ ft_status ft_build_bvh(ft_context *ctx, const void *x, const void *y, const void
         check_status_word(impl, st);
         impl.height_root = 0;
     }
+    // boxes of a 42-bit tree stay below 2^42 when every coordinate does (max entries 1, 3, 5)
+    impl.clean42 = ctx->opts.coord_type == FT_COORD_U64 && box[1] < (1ull << 42) && box[3] < (1ull << 42) &&
+                   box[5] < (1ull << 42);
     FT_API_END
 }
 
@@ -426,6 +433,8 @@ ft_status ft_build_tree(ft_context *ctx, ft_tree *tree, const void *sorted_keys,
     sor.init(sorted_orig_idx, sorted_orig_idx ? n * 4 : 0, true, false, st);
     tree->num_internal = n - 1;
     TreeImpl &impl     = *(TreeImpl *)tree->impl;
+    impl.clean42       = false; // caller leaf arrays: the general periodic distance form
+    impl.height_root   = -1;
     build_tree_from_keys(*ctx, *tree, sk.dev, sx.dev, sy.dev, sz.dev, (const uint32_t *)sid.dev,
                          (const int8_t *)sgh.dev, (const int32_t *)sor.dev, st);
     if (n > 1) {

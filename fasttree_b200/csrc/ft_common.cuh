@@ -112,12 +112,28 @@ template <class T> struct Metric {
             return ((al < ah) ? al : ah) >> C::dist_shift;
         }
     }
+    // periodic 42-bit axis for trees whose coordinates are all below 2^42 (checked at build
+    // time from the bounding box).  With v masked and lo <= hi < 2^42:
+    //   a = (lo - v) mod 2^42 (up from v to lo),  b = (v - hi) mod 2^42 (down from v to hi);
+    //   v strictly inside (lo, hi)  <=>  a + b > 2^42  (a + b = 2^43 - (hi - lo) there and
+    //   2^42 - (hi - lo) outside), an endpoint gives a or b = 0, and outside the interval
+    //   the reference's min(|sext(v - lo)|, |sext(v - hi)|) equals min(a, b).
+    static FT_D unsigned long long periodic_axis_clean(T v, T lo, T hi) {
+        static_assert(sizeof(T) == 8, "42-bit positions only");
+        constexpr unsigned long long M = (1ull << C::bits) - 1ull;
+        const unsigned long long     vv = (unsigned long long)v & M;
+        const unsigned long long     a  = ((unsigned long long)lo - vv) & M;
+        const unsigned long long     b  = (vv - (unsigned long long)hi) & M;
+        const unsigned long long     g  = a < b ? a : b;
+        return (a + b > M + 1ull) ? 0ull : (unsigned long long)(uint32_t)(g >> C::dist_shift);
+    }
     static FT_D unsigned long long sq(unsigned long long g) {
         // gaps are < 2^32 for every configuration, so a 32x32->64 multiply is exact
         return (g >> 32) ? g * g : (unsigned long long)(uint32_t)g * (uint32_t)g;
     }
 
-    template <bool PERIODIC>
+    // CLEAN: the tree's coordinates are all below 2^bits (42-bit periodic fast form).
+    template <bool PERIODIC, bool CLEAN = false>
     static FT_D dist_t dist(T px, T py, T pz, T x0, T x1, T y0, T y1, T z0, T z1) {
         if constexpr (C::is_float) {
             T dx = c_fmax(sub_rn(x0, px), c_fmax(T(0), sub_rn(px, x1)));
@@ -127,7 +143,11 @@ template <class T> struct Metric {
             return (double)s;
         } else {
             unsigned long long ax, ay, az;
-            if constexpr (PERIODIC) {
+            if constexpr (PERIODIC && CLEAN && sizeof(T) == 8) {
+                ax = periodic_axis_clean(px, x0, x1);
+                ay = periodic_axis_clean(py, y0, y1);
+                az = periodic_axis_clean(pz, z0, z1);
+            } else if constexpr (PERIODIC) {
                 ax = periodic_axis(px, x0, x1);
                 ay = periodic_axis(py, y0, y1);
                 az = periodic_axis(pz, z0, z1);
@@ -182,6 +202,22 @@ template <class T> FT_D void load_rec(const NodeRec<T> *recs, int node, T lb[6],
         }
         l = (int)w[3].x;
         r = (int)w[3].y;
+    }
+}
+
+// Distance mode of a query launch: 0 open box, 1 periodic, 2 periodic with every tree
+// coordinate below 2^bits (the cheaper exact form of Metric::periodic_axis_clean).
+// met_dispatch calls f(std::integral_constant<int, mode>) for the modes a type can have.
+template <class T, class F> inline void met_dispatch(int met, F &&f) {
+    if constexpr (Coord<T>::is_float) {
+        f(std::integral_constant<int, 0>{});
+    } else if constexpr (sizeof(T) == 4) {
+        if (met) f(std::integral_constant<int, 1>{});
+        else f(std::integral_constant<int, 0>{});
+    } else {
+        if (met == 2) f(std::integral_constant<int, 2>{});
+        else if (met == 1) f(std::integral_constant<int, 1>{});
+        else f(std::integral_constant<int, 0>{});
     }
 }
 

@@ -29,7 +29,7 @@ static constexpr int kFastStack = 64;
 static constexpr int kFastWarps = 4;
 static constexpr int kFastThreads = 32 * kFastWarps;
 
-template <class T, bool PER, int KC, int VAR>
+template <class T, int PER, int KC, int VAR>
 __global__ void __launch_bounds__(kFastThreads)
     fast_self_knn_kernel(TreeDev<T> t, const int32_t *__restrict__ leaf_ids, int num, int k, int half_window,
                          int exclude_self, int ret_orig, const typename Coord<T>::dist_t *__restrict__ bound,
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(kFastThreads)
         const int leaf = w0 + j;
         if (active && leaf + n - 1 != self_leaf) {
             const int s  = leaf + n - 1;
-            const D   d2 = Metric<T>::template dist<PER>(px, py, pz, t.min_x[s], t.max_x[s], t.min_y[s], t.max_y[s],
+            const D   d2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, t.min_x[s], t.max_x[s], t.min_y[s], t.max_y[s],
                                                        t.min_z[s], t.max_z[s]);
             insert(d2, ret_orig ? t.orig_idx[s] : leaf);
         }
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(kFastThreads)
     // ---- 2. walk ----
     D   sd[kFastStack];
     int sp = 1;
-    sd[0]  = Metric<T>::template dist<PER>(px, py, pz, t.min_x[0], t.max_x[0], t.min_y[0], t.max_y[0], t.min_z[0],
+    sd[0]  = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, t.min_x[0], t.max_x[0], t.min_y[0], t.max_y[0], t.min_z[0],
                                           t.max_z[0]);
     long long budget = 2ll * n + 64;
     long long visits = 0;
@@ -164,8 +164,8 @@ __global__ void __launch_bounds__(kFastThreads)
             T   lb[6], rb[6];
             int l, r;
             load_rec(t.recs, cur, lb, rb, l, r);
-            const D    ld2 = Metric<T>::template dist<PER>(px, py, pz, lb[0], lb[1], lb[2], lb[3], lb[4], lb[5]);
-            const D    rd2 = Metric<T>::template dist<PER>(px, py, pz, rb[0], rb[1], rb[2], rb[3], rb[4], rb[5]);
+            const D    ld2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, lb[0], lb[1], lb[2], lb[3], lb[4], lb[5]);
+            const D    rd2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, rb[0], rb[1], rb[2], rb[3], rb[4], rb[5]);
             const bool lleaf = l >= n - 1, rleaf = r >= n - 1;
             if (lleaf && needs(ld2) && (l - (n - 1) < w0 || l - (n - 1) > w1) && l != self_leaf)
                 insert(ld2, ret_orig ? t.orig_idx[l] : l - (n - 1));
@@ -222,8 +222,8 @@ __global__ void __launch_bounds__(kFastThreads)
                 T   lb[6], rb[6];
                 int l, r;
                 load_rec(t.recs, node, lb, rb, l, r);
-                const D ld2 = Metric<T>::template dist<PER>(px, py, pz, lb[0], lb[1], lb[2], lb[3], lb[4], lb[5]);
-                const D rd2 = Metric<T>::template dist<PER>(px, py, pz, rb[0], rb[1], rb[2], rb[3], rb[4], rb[5]);
+                const D ld2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, lb[0], lb[1], lb[2], lb[3], lb[4], lb[5]);
+                const D rd2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, rb[0], rb[1], rb[2], rb[3], rb[4], rb[5]);
                 if (sp + 2 > kFastStack) {
                     atomicOr(status, STATUS_TRAVERSAL_LIMIT);
                     break;
@@ -265,8 +265,8 @@ __global__ void __launch_bounds__(kFastThreads)
             T   lb[6], rb[6];
             int l, r;
             load_rec(t.recs, node, lb, rb, l, r);
-            const D  ld2 = Metric<T>::template dist<PER>(px, py, pz, lb[0], lb[1], lb[2], lb[3], lb[4], lb[5]);
-            const D  rd2 = Metric<T>::template dist<PER>(px, py, pz, rb[0], rb[1], rb[2], rb[3], rb[4], rb[5]);
+            const D  ld2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, lb[0], lb[1], lb[2], lb[3], lb[4], lb[5]);
+            const D  rd2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, rb[0], rb[1], rb[2], rb[3], rb[4], rb[5]);
             const bool nl = needs(ld2), nr = needs(rd2);
             const unsigned bl = __ballot_sync(FULL, nl), br = __ballot_sync(FULL, nr);
             if (bl | br) {
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(kFastThreads)
 }
 
 // -----------------------------------------------------------------------------------------
-template <class T, bool PER, int KC>
+template <class T, int PER, int KC>
 static void launch_fast_t(const TreeDev<T> &tv, const int32_t *leaf_ids, int num, int k, int half, bool excl, bool ro,
                           const void *bound, uint64_t *idx, void *dist, int32_t *rr, int32_t *rw, uint32_t *rc,
                           uint32_t *status, int variant, unsigned long long *visits, cudaStream_t st) {
@@ -392,16 +392,15 @@ static void launch_fast(const ft_options &o, const ft_tree &tr, const int32_t *l
     tv.recs     = (const NodeRec<T> *)((TreeImpl *)tr.impl)->recs;
     tv.n        = (int)tr.num_leaves;
     bool ro     = o.return_orig_indices != 0;
-    bool per    = !Coord<T>::is_float && o.periodic;
-#define FT_FAST(PER, KC) launch_fast_t<T, PER, KC>(tv, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc, status, variant, visits, st)
-    if (k <= 32) {
-        if (per) FT_FAST(true, 32);
-        else FT_FAST(false, 32);
-    } else {
-        if (per) FT_FAST(true, 64);
-        else FT_FAST(false, 64);
-    }
-#undef FT_FAST
+    met_dispatch<T>(metric_mode<T>(o, tr), [&](auto M) {
+        constexpr int PER = decltype(M)::value;
+        if (k <= 32)
+            launch_fast_t<T, PER, 32>(tv, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc, status,
+                                      variant, visits, st);
+        else
+            launch_fast_t<T, PER, 64>(tv, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc, status,
+                                      variant, visits, st);
+    });
 }
 
 bool fast_self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, bool excl,
@@ -409,6 +408,8 @@ bool fast_self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, siz
     TreeImpl *impl = (TreeImpl *)tr.impl;
     if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0 || impl->height_root > 62) return false;
     if (half_window <= 0) half_window = k;
+    // variant: 0 default (= 2), 1 per-lane walk, 2 compact per-lane walk, 3 warp-shared walk
+    variant = variant == 0 ? 2 : variant == 3 ? 0 : variant;
     ensure_replay(ctx, num);
     uint32_t           *rc     = ctx.status + 1;
     unsigned long long *visits = (unsigned long long *)(ctx.status + 2);

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <type_traits>
 
 #include "../../include/fasttree_b200.h"
 
@@ -46,8 +47,15 @@ struct TreeImpl {
     uint32_t *tile_counter = nullptr; // per-pass tile ticket
     uint32_t *status       = nullptr; // device status word
     bool      managed      = false;
-    int       height_root  = -1; // host copy after a build
+    int       height_root  = -1;    // host copy after a build
+    bool      clean42      = false; // 64-bit integer tree with every coordinate below 2^42
 };
+
+// Distance mode of query kernels on this tree (see met_dispatch in ft_common.cuh).
+template <class T> inline int metric_mode(const ft_options &o, const ft_tree &t) {
+    if (std::is_floating_point<T>::value || !o.periodic) return 0;
+    return (sizeof(T) == 8 && ((const TreeImpl *)t.impl)->clean42) ? 2 : 1;
+}
 
 struct Context {
     ft_options     opts{};

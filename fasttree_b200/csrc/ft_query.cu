@@ -24,13 +24,13 @@ namespace ft {
 
 static constexpr int kStack = 64; // MAX_STACK_DEPTH (src/hlbvh.hpp:984)
 
-template <class T, bool PER, class D = typename Coord<T>::dist_t>
+template <class T, int PER, class D = typename Coord<T>::dist_t>
 FT_D D box_dist(T px, T py, T pz, const T *b) {
-    return Metric<T>::template dist<PER>(px, py, pz, b[0], b[1], b[2], b[3], b[4], b[5]);
+    return Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, b[0], b[1], b[2], b[3], b[4], b[5]);
 }
-template <class T, bool PER, class D = typename Coord<T>::dist_t>
+template <class T, int PER, class D = typename Coord<T>::dist_t>
 FT_D D node_dist_soa(const TreeDev<T> &t, int node, T px, T py, T pz) {
-    return Metric<T>::template dist<PER>(px, py, pz, t.min_x[node], t.max_x[node], t.min_y[node], t.max_y[node],
+    return Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, t.min_x[node], t.max_x[node], t.min_y[node], t.max_y[node],
                                          t.min_z[node], t.max_z[node]);
 }
 
@@ -39,7 +39,7 @@ FT_D D node_dist_soa(const TreeDev<T> &t, int node, T px, T py, T pz) {
 // -----------------------------------------------------------------------------------------
 // One query with the reference's traversal and heap; the heap rows live in shared memory
 // at hd[slot * QT + tid] / hix[slot * QT + tid].  Writes the k results of row `row`.
-template <class T, int CAP, int QT, bool PER>
+template <class T, int CAP, int QT, int PER>
 FT_D void exact_query(const TreeDev<T> &t, T px, T py, T pz, int self_leaf, int k, int ret_orig,
                       typename Coord<T>::dist_t *hd, int32_t *hix, int tid, size_t row,
                       unsigned long long *__restrict__ out_idx, typename Coord<T>::dist_t *__restrict__ out_dist,
@@ -203,7 +203,7 @@ FT_D bool self_point(const TreeDev<T> &t, int rank, int k, size_t row, unsigned 
     return true;
 }
 
-template <class T, int CAP, int QT, bool SELF, bool PER>
+template <class T, int CAP, int QT, bool SELF, int PER>
 __global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t, const T *__restrict__ qx,
                                                        const T *__restrict__ qy, const T *__restrict__ qz,
                                                        const int32_t *__restrict__ leaf_ids, int num, int k,
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t, const T *__
 // Replays the self queries listed by the fast traversal (ranks[i] -> output row rows[i]) with
 // the reference traversal; grid-stride over a count that lives on the device, so no host
 // synchronisation is needed between the two launches.
-template <class T, int CAP, int QT, bool PER>
+template <class T, int CAP, int QT, int PER>
 __global__ void __launch_bounds__(QT) exact_replay_kernel(TreeDev<T> t, const int32_t *__restrict__ ranks,
                                                           const int32_t *__restrict__ rows,
                                                           const uint32_t *__restrict__ count_dev, int k,
@@ -289,7 +289,7 @@ template <class D> FT_D void warp_bitonic(D *d, int32_t *ix, int n, int lane) {
 
 static constexpr int kMergeWarps = 4;
 
-template <class T, bool PER>
+template <class T, int PER>
 __global__ void __launch_bounds__(32 * kMergeWarps)
     merge_knn_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
                      int nq, int k, int cap, int ret_orig, unsigned long long *__restrict__ out_idx,
@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(32 * kMergeWarps)
 // range_query (src/hlbvh.hpp:2046-2119): left-first DFS, descend while d2 <= rmax^2, count
 // leaves with d2 >= rmin^2, store while the row has room.
 // -----------------------------------------------------------------------------------------
-template <class T, bool PER>
+template <class T, int PER>
 __global__ void __launch_bounds__(128) range_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy,
                                                     const T *__restrict__ qz, const T *__restrict__ rmin,
                                                     const T *__restrict__ rmax, int nq, int32_t *__restrict__ results,
@@ -469,7 +469,7 @@ template <class T> static TreeDev<T> dev_view(const ft_tree &tr) {
 }
 
 // Heap capacity tiers and the threads per block that keep the heap at <= 96 KB.
-template <class T, int CAP, int QT, bool SELF, bool PER>
+template <class T, int CAP, int QT, bool SELF, int PER>
 static void launch_exact_t(const TreeDev<T> &tv, const void *qx, const void *qy, const void *qz,
                            const int32_t *leaf_ids, int num, int k, bool excl, bool ro, uint64_t *idx, void *dist,
                            uint32_t *status, cudaStream_t st) {
@@ -483,7 +483,7 @@ static void launch_exact_t(const TreeDev<T> &tv, const void *qx, const void *qy,
     FT_CUDA(cudaGetLastError());
 }
 
-template <class T, bool SELF, bool PER>
+template <class T, bool SELF, int PER>
 static void launch_exact_cap(const TreeDev<T> &tv, const void *qx, const void *qy, const void *qz,
                              const int32_t *leaf_ids, int num, int k, bool excl, bool ro, uint64_t *idx, void *dist,
                              uint32_t *status, cudaStream_t st) {
@@ -503,10 +503,9 @@ static void launch_exact(const ft_options &o, const ft_tree &tr, const void *qx,
                          uint32_t *status, cudaStream_t st) {
     TreeDev<T> tv = dev_view<T>(tr);
     bool       ro = o.return_orig_indices != 0;
-    if (!Coord<T>::is_float && o.periodic)
-        launch_exact_cap<T, SELF, true>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, status, st);
-    else
-        launch_exact_cap<T, SELF, false>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, status, st);
+    met_dispatch<T>(metric_mode<T>(o, tr), [&](auto M) {
+        launch_exact_cap<T, SELF, decltype(M)::value>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, status, st);
+    });
 }
 
 static constexpr int kMaxExactK = 512;
@@ -536,7 +535,7 @@ void self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t n
     }
 }
 
-template <class T, int CAP, int QT, bool PER>
+template <class T, int CAP, int QT, int PER>
 static void replay_t(const TreeDev<T> &tv, const int32_t *ranks, const int32_t *rows, uint32_t *cnt, int k, bool excl,
                      bool ro, uint64_t *idx, void *dist, uint32_t *status, int num_sms, cudaStream_t st) {
     using D     = typename Coord<T>::dist_t;
@@ -553,11 +552,12 @@ static void replay_typed(Context &ctx, const ft_tree &tr, const int32_t *ranks, 
                          int k, bool excl, uint64_t *idx, void *dist, cudaStream_t st) {
     TreeDev<T> tv  = dev_view<T>(tr);
     bool       ro  = ctx.opts.return_orig_indices != 0;
-    bool       per = !Coord<T>::is_float && ctx.opts.periodic;
+    int        met = metric_mode<T>(ctx.opts, tr);
     int        sms = ctx.num_sms;
 #define FT_RP(CAP, QT)                                                                                          \
-    (per ? replay_t<T, CAP, QT, true>(tv, ranks, rows, cnt, k, excl, ro, idx, dist, ctx.status, sms, st)        \
-         : replay_t<T, CAP, QT, false>(tv, ranks, rows, cnt, k, excl, ro, idx, dist, ctx.status, sms, st))
+    met_dispatch<T>(met, [&](auto M) {                                                                          \
+        replay_t<T, CAP, QT, decltype(M)::value>(tv, ranks, rows, cnt, k, excl, ro, idx, dist, ctx.status, sms, st); \
+    })
     if (k <= 32) FT_RP(32, 128);
     else if (k <= 64) FT_RP(64, 128);
     else if (k <= 128) FT_RP(128, 64);
@@ -576,7 +576,7 @@ void replay_exact(Context &ctx, const ft_tree &tr, const int32_t *ranks, const i
     }
 }
 
-template <class T, bool PER>
+template <class T, int PER>
 static void launch_merge(const TreeDev<T> &tv, const void *qx, const void *qy, const void *qz, int nq, int k, int cap,
                          bool ro, uint64_t *idx, void *dist, uint32_t *status, cudaStream_t st) {
     using D     = typename Coord<T>::dist_t;
@@ -600,8 +600,9 @@ static void knn_typed(const ft_options &o, const ft_tree &tr, const void *qx, co
     while (cap < max_k) cap <<= 1;
     TreeDev<T> tv = dev_view<T>(tr);
     bool       ro = o.return_orig_indices != 0;
-    if (!Coord<T>::is_float && o.periodic) launch_merge<T, true>(tv, qx, qy, qz, nq, k, cap, ro, idx, dist, status, st);
-    else launch_merge<T, false>(tv, qx, qy, qz, nq, k, cap, ro, idx, dist, status, st);
+    met_dispatch<T>(metric_mode<T>(o, tr), [&](auto M) {
+        launch_merge<T, decltype(M)::value>(tv, qx, qy, qz, nq, k, cap, ro, idx, dist, status, st);
+    });
 }
 
 void knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz, size_t nq, int k, int max_k,
@@ -632,14 +633,11 @@ static void range_typed(const ft_options &o, const ft_tree &tr, const void *qx, 
     TreeDev<T> tv     = dev_view<T>(tr);
     int        blocks = (nq + 127) / 128;
     bool       ro     = o.return_orig_indices != 0;
-    if (!Coord<T>::is_float && o.periodic)
-        range_kernel<T, true><<<blocks, 128, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz,
-                                                      (const T *)rmin, (const T *)rmax, nq, results, counts, max_per,
-                                                      ro ? 1 : 0, status);
-    else
-        range_kernel<T, false><<<blocks, 128, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz,
-                                                       (const T *)rmin, (const T *)rmax, nq, results, counts, max_per,
-                                                       ro ? 1 : 0, status);
+    met_dispatch<T>(metric_mode<T>(o, tr), [&](auto M) {
+        range_kernel<T, decltype(M)::value><<<blocks, 128, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz,
+                                                                    (const T *)rmin, (const T *)rmax, nq, results,
+                                                                    counts, max_per, ro ? 1 : 0, status);
+    });
     FT_CUDA(cudaGetLastError());
 }
 

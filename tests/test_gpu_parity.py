@@ -260,3 +260,27 @@ def test_fast_self_knn_subset_and_orig(cfg):
             oi, od = O.self_knn(opts, ot, k, True, leaf_ids=sub)
             assert np.array_equal(gi.cpu().numpy(), oi)
             assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od))
+
+
+@pytest.mark.parametrize("method", [0, 1])
+def test_periodic_wrap_edges_u64(method):
+    """42-bit periodic distances at the wrap: points at 0, 2^41 (half the period) and
+    2^42 - 1, where the wrapped gap reaches its extreme values."""
+    ctx, opts = make(O.U64, O.PEANO_HILBERT, True)
+    rng = np.random.default_rng(5)
+    n = 3000
+    B = 1 << 42
+    base = np.array([0, 1, B // 2 - 1, B // 2, B // 2 + 1, B - 2, B - 1, 3 * (B // 4)], np.uint64)
+    x = rng.choice(base, n).astype(np.uint64)
+    y = rng.choice(base, n).astype(np.uint64)
+    z = (rng.integers(0, B, n)).astype(np.uint64)
+    tree, ot = build_both(ctx, opts, x, y, z)
+    for k in (4, 32):
+        gi, gd = ft.self_knn_query(ctx, tree, k, method=method)
+        torch.cuda.synchronize()
+        oi, od = O.self_knn(opts, ot, k, True)
+        assert np.array_equal(gi.cpu().numpy(), oi) and np.array_equal(gd.cpu().numpy(), od)
+    q = np.array([0, B // 2, B - 1, B // 4], np.uint64)
+    gi, gd = ft.knn_query(ctx, tree, q, q, q, 16)
+    oi, od = O.knn(opts, ot, q, q, q, 16)
+    assert np.array_equal(gi.cpu().numpy(), oi) and np.array_equal(gd.cpu().numpy(), od)
