@@ -20,6 +20,7 @@ EXPORTED = (
     "ft_check_device_status",
     "ft_tree_create", "ft_tree_ensure", "ft_tree_destroy", "ft_compute_bbox", "ft_sfc_encode",
     "ft_build_bvh", "ft_build_tree", "ft_self_knn", "ft_knn", "ft_range", "ft_tree_height",
+    "ft_self_knn_noalloc",
 )
 
 
@@ -68,6 +69,7 @@ _SIGS = {
     "ft_build_bvh": [_vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _vp, ctypes.POINTER(FtTree), _st],
     "ft_build_tree": [_vp, ctypes.POINTER(FtTree), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _st],
     "ft_self_knn": [_vp, ctypes.POINTER(FtTree), _vp, _sz, _i, _i, _vp, _vp, ctypes.POINTER(FtQueryOptions), _st],
+    "ft_self_knn_noalloc": [_vp, ctypes.POINTER(FtTree), _vp, _sz, _i, _i, _vp, _vp, _st],
     "ft_knn": [_vp, ctypes.POINTER(FtTree), _vp, _vp, _vp, _sz, _i, _vp, _vp, ctypes.POINTER(FtQueryOptions), _st],
     "ft_range": [_vp, ctypes.POINTER(FtTree), _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _i, _st],
 }

@@ -463,6 +463,29 @@ ft_status ft_self_knn(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_
     FT_API_END
 }
 
+// Self-kNN for callers that cannot have device memory allocated for them (see
+// fast_self_knn_noalloc in ft_fast.cu): the fast walk's scratch is a fixed static array.
+ft_status ft_self_knn_noalloc(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_ids, size_t num, int k,
+                              int exclude_self, uint64_t *idx_out, void *dist_out, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree, "null argument");
+    if (!leaf_ids) num = tree->num_leaves;
+    if (num > ft::noalloc_max_queries())
+        fail(FT_ERR_INVALID_ARGUMENT, "ft_self_knn_noalloc: more than 1048576 queries in one call (the fixed "
+                                      "scratch holds 2^20); split the call");
+    if (tree->num_leaves == 0 || num == 0 || k <= 0) return FT_OK;
+    need(idx_out && dist_out, "null output array");
+    if (k > 512) fail(FT_ERR_RUNTIME, "self_knn_query: k too large for shared memory.");
+    DeviceGuard  g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!ft::fast_self_knn_noalloc(*ctx, *tree, leaf_ids, num, k, exclude_self != 0, idx_out, dist_out, st)) {
+        ft_query_options q{}; // reference traversal: it uses no scratch
+        q.max_k = k < 32 ? 32 : k;
+        ft::self_knn(*ctx, *tree, leaf_ids, num, k, exclude_self != 0, idx_out, dist_out, q, st);
+    }
+    FT_API_END
+}
+
 ft_status ft_knn(ft_context *ctx, const ft_tree *tree, const void *qx, const void *qy, const void *qz,
                  size_t num_queries, int k, uint64_t *idx_out, void *dist_out, const ft_query_options *qopts,
                  ft_stream_t stream) {

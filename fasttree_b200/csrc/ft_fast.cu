@@ -19,6 +19,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
+#include <string>
 
 #include "ft_common.cuh"
 #include "ft_internal.h"
@@ -433,6 +435,80 @@ void ensure_replay(Context &ctx, size_t num) {
     FT_CUDA(cudaMalloc(&ctx.replay_ranks, cap * sizeof(int32_t)));
     FT_CUDA(cudaMalloc(&ctx.replay_rows, cap * sizeof(int32_t)));
     ctx.replay_cap = cap;
+}
+
+// =========================================================================================
+// Self-kNN without any device allocation (ft_self_knn_noalloc).
+//
+// Some callers cannot let a library allocate device memory in the middle of their work: a
+// simulation that hands the whole GPU to its own memory pool at start-up (a cudaMalloc then
+// fails), or a time step that must not stall every stream (cudaMalloc / cudaFree
+// synchronise the device).  This variant runs the fast self-kNN walk with its only scratch
+// -- the list of queries handed to the exact replay and its counter -- in the fixed array
+// below, instead of the context's growable buffers.
+//
+// * The array lives in every GPU that loads the library, for the life of the process:
+//   kNoAllocMaxQueries (2^20) queries per call, 8 MiB + a small header.  Larger calls are
+//   rejected with FT_ERR_INVALID_ARGUMENT.
+// * Host code needs the array's device address: the first call on a device looks it up
+//   with cudaGetSymbolAddress (with that device current) and keeps it; make that first call
+//   before any stream capture.  The symbol itself is only a host-side stand-in, never a
+//   device pointer.
+// * All calls share the array.  Each call clears the counter it needs on its stream first;
+//   calls whose work overlaps on the GPU (different streams, or threads racing on one
+//   device) race on the array and must be serialised by the caller.
+// =========================================================================================
+static constexpr size_t kNoAllocMaxQueries = size_t(1) << 20;
+static constexpr size_t kNoAllocHeader     = 64; // words: [0] replay count, [2..3] visit counter
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocHeader + 2 * kNoAllocMaxQueries];
+
+static constexpr int kNoAllocMaxDevices = 64;
+static std::mutex    g_noalloc_mutex;
+static uint32_t     *g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on `device` (looked up once; device must be current).
+static uint32_t *noalloc_scratch(int device) {
+    if (device < 0 || device >= kNoAllocMaxDevices) fail(FT_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[device]) {
+        void       *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            cudaGetLastError();
+            fail(FT_ERR_CUDA, std::string("cudaGetSymbolAddress of the no-allocation scratch failed: ") +
+                                  cudaGetErrorString(e));
+        }
+        g_noalloc_addr[device] = static_cast<uint32_t *>(p);
+    }
+    return g_noalloc_addr[device];
+}
+
+size_t noalloc_max_queries() { return kNoAllocMaxQueries; }
+
+// Returns false when the fast walk does not apply (k > 64 or a tree taller than 62); the
+// caller then runs the reference traversal, which needs no scratch.
+bool fast_self_knn_noalloc(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, bool excl,
+                           uint64_t *idx, void *dist, cudaStream_t st) {
+    if (num > kNoAllocMaxQueries)
+        fail(FT_ERR_INVALID_ARGUMENT, "ft_self_knn_noalloc: more than 1048576 queries in one call (the fixed "
+                                      "scratch holds 2^20); split the call");
+    TreeImpl *impl = (TreeImpl *)tr.impl;
+    if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0 || impl->height_root > 62) return false;
+    uint32_t           *s      = noalloc_scratch(ctx.device);
+    uint32_t           *rc     = s;
+    unsigned long long *visits = reinterpret_cast<unsigned long long *>(s + 2);
+    int32_t            *ranks  = reinterpret_cast<int32_t *>(s + kNoAllocHeader);
+    int32_t            *rows   = ranks + kNoAllocMaxQueries;
+    FT_CUDA(cudaMemsetAsync(s, 0, 4 * sizeof(uint32_t), st)); // the replay count must start at zero
+    const int half = k, variant = 2;
+    switch (ctx.opts.coord_type) {
+    case F32: launch_fast<float>(ctx.opts, tr, leaf_ids, (int)num, k, half, excl, nullptr, idx, dist, ranks, rows, rc, ctx.status, variant, visits, st); break;
+    case F64: launch_fast<double>(ctx.opts, tr, leaf_ids, (int)num, k, half, excl, nullptr, idx, dist, ranks, rows, rc, ctx.status, variant, visits, st); break;
+    case U32: launch_fast<uint32_t>(ctx.opts, tr, leaf_ids, (int)num, k, half, excl, nullptr, idx, dist, ranks, rows, rc, ctx.status, variant, visits, st); break;
+    case U64: launch_fast<unsigned long long>(ctx.opts, tr, leaf_ids, (int)num, k, half, excl, nullptr, idx, dist, ranks, rows, rc, ctx.status, variant, visits, st); break;
+    }
+    replay_exact(ctx, tr, ranks, rows, rc, k, excl, idx, dist, st);
+    return true;
 }
 
 } // namespace ft

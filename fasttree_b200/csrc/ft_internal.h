@@ -74,6 +74,11 @@ struct Context {
 bool fast_self_knn(Context &ctx, const ft_tree &tree, const int32_t *leaf_ids, size_t num, int k, bool exclude_self,
                    uint64_t *idx, void *dist, const void *bound, int half_window, int variant, cudaStream_t st);
 void ensure_replay(Context &ctx, size_t num);
+// Fast self-kNN whose scratch is a fixed static device array (no allocation); false when
+// the fast walk does not apply.  At most noalloc_max_queries() queries per call.
+bool   fast_self_knn_noalloc(Context &ctx, const ft_tree &tree, const int32_t *leaf_ids, size_t num, int k,
+                             bool exclude_self, uint64_t *idx, void *dist, cudaStream_t st);
+size_t noalloc_max_queries();
 // Reruns the listed self queries (ranks[i] -> row rows[i], *count_dev of them) with the
 // reference traversal (ft_query.cu).
 void replay_exact(Context &ctx, const ft_tree &tree, const int32_t *ranks, const int32_t *rows, uint32_t *count_dev,

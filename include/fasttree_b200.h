@@ -156,6 +156,20 @@ ft_status ft_self_knn(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_
                       int k, int exclude_self, uint64_t *idx_out, void *dist_out,
                       const ft_query_options *qopts, ft_stream_t stream);
 
+/* Self-kNN (full, leaf_ids == NULL, or subset) that allocates no device memory itself, for
+ * callers that cannot let a library allocate: codes that give the whole GPU to their own
+ * memory pool at start-up, or steps that must not be stalled by the device-wide
+ * synchronisation of cudaMalloc / cudaFree.  No counterpart in the reference.
+ * Same results as ft_self_knn (fast walk with exact replay; the reference traversal when
+ * k > 64 or the tree is taller than 62).  The replay list lives in a fixed array that every
+ * GPU loading this library holds until exit: at most 1048576 (2^20) queries per call, more
+ * is FT_ERR_INVALID_ARGUMENT.  The first call on a device looks up that array's address;
+ * make it before any stream capture.  All calls share the array: calls that overlap on the
+ * GPU race and must be serialised by the caller.  leaf_ids, idx_out, dist_out: device.
+ * Asynchronous on stream; errors from the kernels surface in ft_check_device_status. */
+ft_status ft_self_knn_noalloc(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_ids, size_t num,
+                              int k, int exclude_self, uint64_t *idx_out, void *dist_out, ft_stream_t stream);
+
 /* knn_query<MAXK> (src/hlbvh.hpp:1405-1472).  qx/qy/qz, idx_out, dist_out: host or device.
  * Default max_k 256.  Blocking. */
 ft_status ft_knn(ft_context *ctx, const ft_tree *tree, const void *qx, const void *qy,
