@@ -6,7 +6,7 @@ buffers and streams.  Importing the package does not need a GPU; calling into it
 there is no CPU fallback.
 """
 from .capi import F32, F64, U32, U64, MORTON, PEANO_HILBERT, FastTreeError  # noqa: F401
-from .hlbvh import (BoundingBox, Context, TreePool, TreeSoA, build_bvh, build_tree,  # noqa: F401
+from .hlbvh import (BatchedSets, BoundingBox, Context, TreePool, TreeSoA, build_bvh, build_tree,  # noqa: F401
                     compute_bbox, dist_torch_dtype, knn_query, particles, range_query,
                     self_knn_query, self_knn_query_subset, sfc_encode)
 

@@ -21,6 +21,8 @@ EXPORTED = (
     "ft_tree_create", "ft_tree_ensure", "ft_tree_destroy", "ft_compute_bbox", "ft_sfc_encode",
     "ft_build_bvh", "ft_build_tree", "ft_self_knn", "ft_knn", "ft_range", "ft_tree_height",
     "ft_self_knn_noalloc",
+    "ft_batch_create", "ft_batch_destroy", "ft_batch_build", "ft_batch_self_knn", "ft_batch_build_knn",
+    "ft_batch_tree", "ft_batch_set_info", "ft_batch_query_stats",
 )
 
 
@@ -72,6 +74,15 @@ _SIGS = {
     "ft_self_knn_noalloc": [_vp, ctypes.POINTER(FtTree), _vp, _sz, _i, _i, _vp, _vp, _st],
     "ft_knn": [_vp, ctypes.POINTER(FtTree), _vp, _vp, _vp, _sz, _i, _vp, _vp, ctypes.POINTER(FtQueryOptions), _st],
     "ft_range": [_vp, ctypes.POINTER(FtTree), _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _i, _st],
+    "ft_batch_create": [_vp, _sz, _sz, ctypes.POINTER(_vp)],
+    "ft_batch_destroy": [_vp, _vp],
+    "ft_batch_build": [_vp, _vp, _vp, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _st],
+    "ft_batch_self_knn": [_vp, _vp, _i, _i, _vp, _vp, ctypes.POINTER(FtQueryOptions), _st],
+    "ft_batch_build_knn": [_vp, _vp, _vp, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp,
+                           ctypes.POINTER(FtQueryOptions), _st],
+    "ft_batch_tree": [_vp, _vp, _sz, ctypes.POINTER(FtTree), _st],
+    "ft_batch_set_info": [_vp, _vp, _vp, _vp, _st],
+    "ft_batch_query_stats": [_vp, _vp, ctypes.POINTER(FtQueryStats)],
 }
 
 

@@ -12,45 +12,11 @@
 #include <cstring>
 #include <vector>
 
+#include "ft_build_dev.cuh"
 #include "ft_common.cuh"
 #include "ft_internal.h"
 
 namespace ft {
-
-// =========================================================================================
-// Peano-Hilbert state tables (AREPO's rottable3 / subpix3, reproduced in
-// src/sfc.peano_hilbert.hpp:332-376).  The curve is defined by these values.
-// =========================================================================================
-__constant__ uint8_t c_rot[48 * 8] = {
-    36, 28, 25, 27, 10, 10, 25, 27, 29, 11, 24, 24, 37, 11, 26, 26, 8,  8,  25, 27, 30, 38, 25, 27,
-    9,  39, 24, 24, 9,  31, 26, 26, 40, 24, 44, 32, 40, 6,  44, 6,  25, 7,  33, 7,  41, 41, 45, 45,
-    4,  42, 4,  46, 26, 42, 34, 46, 43, 43, 47, 47, 5,  27, 5,  35, 33, 35, 36, 28, 33, 35, 2,  2,
-    32, 32, 29, 3,  34, 34, 37, 3,  33, 35, 0,  0,  33, 35, 30, 38, 32, 32, 1,  39, 34, 34, 1,  31,
-    24, 42, 32, 46, 14, 42, 14, 46, 43, 43, 47, 47, 25, 15, 33, 15, 40, 12, 44, 12, 40, 26, 44, 34,
-    13, 27, 13, 35, 41, 41, 45, 45, 28, 41, 28, 22, 38, 43, 38, 22, 42, 40, 23, 23, 29, 39, 29, 39,
-    41, 36, 20, 36, 43, 30, 20, 30, 37, 31, 37, 31, 42, 40, 21, 21, 28, 18, 28, 45, 38, 18, 38, 47,
-    19, 19, 46, 44, 29, 39, 29, 39, 16, 36, 45, 36, 16, 30, 47, 30, 37, 31, 37, 31, 17, 17, 46, 44,
-    12, 4,  1,  3,  34, 34, 1,  3,  5,  35, 0,  0,  13, 35, 2,  2,  32, 32, 1,  3,  6,  14, 1,  3,
-    33, 15, 0,  0,  33, 7,  2,  2,  16, 0,  20, 8,  16, 30, 20, 30, 1,  31, 9,  31, 17, 17, 21, 21,
-    28, 18, 28, 22, 2,  18, 10, 22, 19, 19, 23, 23, 29, 3,  29, 11, 9,  11, 12, 4,  9,  11, 26, 26,
-    8,  8,  5,  27, 10, 10, 13, 27, 9,  11, 24, 24, 9,  11, 6,  14, 8,  8,  25, 15, 10, 10, 25, 7,
-    0,  18, 8,  22, 38, 18, 38, 22, 19, 19, 23, 23, 1,  39, 9,  39, 16, 36, 20, 36, 16, 2,  20, 10,
-    37, 3,  37, 11, 17, 17, 21, 21, 4,  17, 4,  46, 14, 19, 14, 46, 18, 16, 47, 47, 5,  15, 5,  15,
-    17, 12, 44, 12, 19, 6,  44, 6,  13, 7,  13, 7,  18, 16, 45, 45, 4,  42, 4,  21, 14, 42, 14, 23,
-    43, 43, 22, 20, 5,  15, 5,  15, 40, 12, 21, 12, 40, 6,  23, 6,  13, 7,  13, 7,  41, 41, 22, 20};
-__constant__ uint8_t c_sub[48 * 8] = {
-    0, 7, 1, 6, 3, 4, 2, 5, 7, 4, 6, 5, 0, 3, 1, 2, 4, 3, 5, 2, 7, 0, 6, 1, 3, 0, 2, 1, 4, 7, 5, 6,
-    1, 0, 6, 7, 2, 3, 5, 4, 0, 3, 7, 4, 1, 2, 6, 5, 3, 2, 4, 5, 0, 1, 7, 6, 2, 1, 5, 6, 3, 0, 4, 7,
-    6, 1, 7, 0, 5, 2, 4, 3, 1, 2, 0, 3, 6, 5, 7, 4, 2, 5, 3, 4, 1, 6, 0, 7, 5, 6, 4, 7, 2, 1, 3, 0,
-    7, 6, 0, 1, 4, 5, 3, 2, 6, 5, 1, 2, 7, 4, 0, 3, 5, 4, 2, 3, 6, 7, 1, 0, 4, 7, 3, 0, 5, 6, 2, 1,
-    6, 7, 5, 4, 1, 0, 2, 3, 7, 0, 4, 3, 6, 1, 5, 2, 0, 1, 3, 2, 7, 6, 4, 5, 1, 6, 2, 5, 0, 7, 3, 4,
-    2, 3, 1, 0, 5, 4, 6, 7, 3, 4, 0, 7, 2, 5, 1, 6, 4, 5, 7, 6, 3, 2, 0, 1, 5, 2, 6, 1, 4, 3, 7, 0,
-    7, 0, 6, 1, 4, 3, 5, 2, 0, 3, 1, 2, 7, 4, 6, 5, 3, 4, 2, 5, 0, 7, 1, 6, 4, 7, 5, 6, 3, 0, 2, 1,
-    6, 7, 1, 0, 5, 4, 2, 3, 7, 4, 0, 3, 6, 5, 1, 2, 4, 5, 3, 2, 7, 6, 0, 1, 5, 6, 2, 1, 4, 7, 3, 0,
-    1, 6, 0, 7, 2, 5, 3, 4, 6, 5, 7, 4, 1, 2, 0, 3, 5, 2, 4, 3, 6, 1, 7, 0, 2, 1, 3, 0, 5, 6, 4, 7,
-    0, 1, 7, 6, 3, 2, 4, 5, 1, 2, 6, 5, 0, 3, 7, 4, 2, 3, 5, 4, 1, 0, 6, 7, 3, 0, 4, 7, 2, 1, 5, 6,
-    1, 0, 2, 3, 6, 7, 5, 4, 0, 7, 3, 4, 1, 6, 2, 5, 7, 6, 4, 5, 0, 1, 3, 2, 6, 1, 5, 2, 7, 0, 4, 3,
-    5, 4, 6, 7, 2, 3, 1, 0, 4, 3, 7, 0, 5, 2, 6, 1, 3, 2, 0, 1, 4, 5, 7, 6, 2, 5, 1, 6, 3, 4, 0, 7};
 
 static constexpr int kSpinLimit = 1 << 24;
 
@@ -71,61 +37,9 @@ size_t ref_key_bytes(const ft_options &o) {
 
 // =========================================================================================
 // Bounding box: per-block partials, then one block folds them (two passes keep the result
-// independent of scheduling).  min: (v < m) ? v : m; max: (m < v) ? v : m, as
-// sycl::minimum / sycl::maximum.
+// independent of scheduling); the fold is bb_fold.
 // =========================================================================================
-static constexpr int kBboxBlocks  = 1184; // 8 x 148 SMs
-static constexpr int kBboxThreads = 256;
-
-template <class T> FT_D void bb_fold(T *m, const T *v) {
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        if (v[2 * d] < m[2 * d]) m[2 * d] = v[2 * d];
-        if (m[2 * d + 1] < v[2 * d + 1]) m[2 * d + 1] = v[2 * d + 1];
-    }
-}
-template <class T> FT_HD void bb_identity(T *m) {
-    T lo, hi;
-    if constexpr (std::is_floating_point<T>::value) {
-        lo = std::is_same<T, float>::value ? (T)FLT_MAX : (T)DBL_MAX;
-        hi = -lo;
-    } else {
-        lo = (T)~T(0);
-        hi = 0;
-    }
-    m[0] = m[2] = m[4] = lo;
-    m[1] = m[3] = m[5] = hi;
-}
-
-template <class T> FT_D void bb_block_reduce(T *m) {
-    __shared__ T s[kBboxThreads / 32][6];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-        T o[6];
-#pragma unroll
-        for (int d = 0; d < 6; ++d) o[d] = __shfl_down_sync(0xffffffffu, m[d], off);
-        bb_fold(m, o);
-    }
-    if (lane == 0)
-#pragma unroll
-        for (int d = 0; d < 6; ++d) s[w][d] = m[d];
-    __syncthreads();
-    if (w == 0) {
-        if (lane < kBboxThreads / 32)
-#pragma unroll
-            for (int d = 0; d < 6; ++d) m[d] = s[lane][d];
-        else
-            bb_identity(m);
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            T o[6];
-#pragma unroll
-            for (int d = 0; d < 6; ++d) o[d] = __shfl_down_sync(0xffffffffu, m[d], off);
-            bb_fold(m, o);
-        }
-    }
-}
+static constexpr int kBboxBlocks = 1184; // 8 x 148 SMs
 
 template <class T>
 __global__ void __launch_bounds__(kBboxThreads) bbox_partial_kernel(const T *__restrict__ x, const T *__restrict__ y,
@@ -154,88 +68,24 @@ template <class T> __global__ void __launch_bounds__(kBboxThreads) bbox_final_ke
 // SFC keys (sfc_encode, src/hlbvh.hpp:357-423).  Internal key format: lo (and hi for the
 // 126-bit Peano-Hilbert key of 42-bit integer positions).  Also writes perm = iota.
 // =========================================================================================
-FT_D unsigned long long spread3(unsigned long long x) { // src/sfc.morton.hpp:33-41
-    x &= 0x1FFFFFull;
-    x = (x | (x << 32)) & 0x1F00000000FFFFull;
-    x = (x | (x << 16)) & 0x1F0000FF0000FFull;
-    x = (x | (x << 8)) & 0x100F00F00F00F00Full;
-    x = (x | (x << 4)) & 0x10C30C30C30C30C3ull;
-    x = (x | (x << 2)) & 0x1249249249249249ull;
-    return x;
-}
-
-// Peano-Hilbert key: B rounds of octant index -> table lookup (src/sfc.peano_hilbert.hpp:569-600);
-// the key register is shifted 3 bits per round (396-405).
-template <int B>
-FT_D void ph_key(unsigned long long px, unsigned long long py, unsigned long long pz, const uint8_t *rot_t,
-                 const uint8_t *sub_t, unsigned long long &hi, unsigned long long &lo) {
-    unsigned long long h = 0, l = 0;
-    unsigned           rot = 0;
-#pragma unroll 6
-    for (int b = B - 1; b >= 0; --b) {
-        unsigned pix = (unsigned)((((px >> b) & 1ull) << 2) | (((py >> b) & 1ull) << 1) | ((pz >> b) & 1ull));
-        unsigned e   = rot * 8u + pix;
-        h            = (h << 3) | (l >> 61);
-        l            = (l << 3) | sub_t[e];
-        rot          = rot_t[e];
-    }
-    hi = h;
-    lo = l;
-}
-
-template <class T> FT_D unsigned long long morton_cell(T nx) { // encode_to_sfc1d (src/hlbvh.hpp:246-271)
-    T v = add_rn(T(1), nx);
-    if constexpr (sizeof(T) == 4) return (unsigned long long)((__float_as_uint(v) & 0x007FFFFFu) >> 2);
-    else return ((unsigned long long)__double_as_longlong(v) & 0x000FFFFFFFFFFFFFull) >> 31;
-}
-template <class T> FT_D unsigned long long ph_cell(T nx) { // quantize_coord (src/sfc.peano_hilbert.hpp:472-476)
-    double b = c_fmin(__dadd_rn(1.0, (double)nx), 0x1.fffffffffffffp+0);
-    return (((unsigned long long)__double_as_longlong(b) & 0x000FFFFFFFFFFFFFull) >> 31) & 0x1FFFFFull;
-}
-
 template <class T, int SFC>
 __global__ void __launch_bounds__(256) encode_kernel(const T *__restrict__ x, const T *__restrict__ y,
                                                      const T *__restrict__ z, size_t n, const T *__restrict__ bbox,
                                                      unsigned long long *klo, unsigned long long *khi, uint32_t *perm) {
     using C = Coord<T>;
     __shared__ uint8_t s_rot[48 * 8], s_sub[48 * 8];
-    __shared__ T       s_par[9]; // min, inv per axis; upper
+    __shared__ T       s_par[6]; // lo, inv per axis
     for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x) {
         s_rot[i] = c_rot[i];
         s_sub[i] = c_sub[i];
     }
-    if constexpr (C::is_float) {
-        if (threadIdx.x < 3) {
-            int d    = threadIdx.x;
-            T   lo   = bbox[2 * d], hi = bbox[2 * d + 1];
-            T   dd   = sub_rn(hi, lo);
-            T   inv;
-            if constexpr (sizeof(T) == 4) inv = (dd == 0.0f) ? 0.0f : __fdiv_rn(1.0f, dd);
-            else inv = (dd == 0.0) ? 0.0 : __ddiv_rn(1.0, dd);
-            s_par[2 * d]     = lo;
-            s_par[2 * d + 1] = inv;
-        }
-    }
+    if constexpr (C::is_float)
+        if (threadIdx.x < 3) sfc_axis_params(bbox[2 * threadIdx.x], bbox[2 * threadIdx.x + 1], s_par[2 * threadIdx.x],
+                                             s_par[2 * threadIdx.x + 1]);
     __syncthreads();
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        unsigned long long hi = 0, lo = 0;
-        if constexpr (!C::is_float) {
-            const unsigned long long mask = (1ull << C::bits) - 1ull; // 375-387
-            ph_key<C::bits>((unsigned long long)x[i] & mask, (unsigned long long)y[i] & mask,
-                            (unsigned long long)z[i] & mask, s_rot, s_sub, hi, lo);
-        } else {
-            // nx = clamp((p - min) * inv, 0, nextafter(1, 0)) in T (389-403)
-            const T upper = (sizeof(T) == 4) ? (T)0x1.fffffep-1f : (T)0x1.fffffffffffffp-1;
-            T       p[3]  = {x[i], y[i], z[i]};
-            unsigned long long c[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                T nx = c_fmin(c_fmax(mul_rn(sub_rn(p[d], s_par[2 * d]), s_par[2 * d + 1]), T(0)), upper);
-                c[d] = (SFC == MORTON) ? morton_cell(nx) : ph_cell(nx);
-            }
-            if (SFC == MORTON) lo = spread3(c[0]) | (spread3(c[1]) << 1) | (spread3(c[2]) << 2);
-            else ph_key<21>(c[0], c[1], c[2], s_rot, s_sub, hi, lo);
-        }
+        unsigned long long hi, lo;
+        encode_point<T, SFC>(x[i], y[i], z[i], s_par, s_rot, s_sub, hi, lo);
         klo[i] = lo;
         if (C::key_words == 2) khi[i] = hi;
         perm[i] = (uint32_t)i;
@@ -532,116 +382,26 @@ __global__ void leaf_init_kernel(const T *sx, const T *sy, const T *sz, size_t n
 // length of two sorted keys (get_common_prefix_length, 283-340), with the index tie-break
 // for equal keys.
 // =========================================================================================
-template <int KIND> struct Delta {
-    const unsigned long long *lo, *hi;
-    int                       n;
-    unsigned long long        ilo, ihi;
-    int                       i;
-    FT_D int operator()(int j) const {
-        if (j < 0 || j >= n) return -1;
-        unsigned long long jlo = lo[j];
-        if (KIND == 2) {
-            unsigned long long jhi = hi[j];
-            if (jhi != ihi) return clz64(jhi ^ ihi) - 2;
-            if (jlo != ilo) return 62 + clz64(jlo ^ ilo);
-        } else {
-            if (jlo != ilo) return clz64(jlo ^ ilo) - (KIND == 1 ? 1 : 0);
-        }
-        return (KIND == 2 ? 126 : 63) + clz64((unsigned long long)(long long)i ^ (unsigned long long)(long long)j);
-    }
-};
-
-FT_D int sgn(int v) { return (v > 0) - (v < 0); }
-
 template <int KIND>
 __global__ void __launch_bounds__(256) karras_kernel(const unsigned long long *__restrict__ klo,
                                                      const unsigned long long *__restrict__ khi, int n,
                                                      int32_t *left, int32_t *right, int32_t *parent) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x) {
-        Delta<KIND> delta{klo, khi, n, klo[i], KIND == 2 ? khi[i] : 0ull, i};
-        int d         = sgn(delta(i + 1) - delta(i - 1));
-        int delta_min = delta(i - d);
-        int l_max     = 2;
-        while (delta(i + l_max * d) > delta_min) l_max *= 2;
-        int l = 0;
-        for (int t = l_max / 2; t >= 1; t /= 2)
-            if (delta(i + (l + t) * d) > delta_min) l += t;
-        int j          = i + l * d;
-        int delta_node = delta(j);
-        int s          = 0;
-        int t_split    = 1;
-        while (t_split <= l) t_split *= 2;
-        t_split /= 2;
-        for (int t = t_split; t >= 1; t /= 2)
-            if (s + t < l && delta(i + (s + t) * d) > delta_node) s += t;
-        int split = i + s * d + min(d, 0);
-        int lc    = (min(i, j) == split) ? split + n - 1 : split;
-        int rc    = (max(i, j) == split + 1) ? split + 1 + n - 1 : split + 1;
-        left[i]   = lc;
-        right[i]  = rc;
-        parent[lc] = i;
-        parent[rc] = i;
-    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x)
+        karras_node<KIND>(klo, khi, n, i, left, right, parent);
 }
 
 // =========================================================================================
-// Bottom-up refit (src/hlbvh.hpp:925-969): one thread per leaf climbs; at each parent the
-// first arrival stops and the second merges both child boxes.  The merge also writes the
-// traversal record (both child boxes + indices) and the subtree height.  Child boxes that
-// other threads wrote in this launch are read through L2 (ld.cg) after the acquire fence.
+// Bottom-up refit (src/hlbvh.hpp:925-969), one thread per leaf (refit_leaf).
 // =========================================================================================
-template <class T> FT_D void load_box_cg(const T *const *soa, int node, T b[6]) {
-#pragma unroll
-    for (int d = 0; d < 6; ++d) b[d] = __ldcg(soa[d] + node);
-}
-
 template <class T>
 __global__ void __launch_bounds__(256) refit_kernel(int n, const int32_t *__restrict__ left,
                                                     const int32_t *__restrict__ right,
                                                     const int32_t *__restrict__ parent, T *mnx, T *mxx, T *mny,
                                                     T *mxy, T *mnz, T *mxz, NodeRec<T> *recs, uint8_t *height,
                                                     int32_t *counters) {
-    const T *soa[6] = {mnx, mxx, mny, mxy, mnz, mxz};
-    T       *soa_w[6] = {mnx, mxx, mny, mxy, mnz, mxz};
-    for (int leaf = blockIdx.x * blockDim.x + threadIdx.x; leaf < n; leaf += gridDim.x * blockDim.x) {
-        int curr  = leaf + n - 1;
-        int steps = 0;
-        while (curr != 0 && ++steps < n) { // a valid tree is climbed in < n steps
-            int p = parent[curr];
-            if (p < 0 || p >= n - 1) break;
-            __threadfence();
-            if (atomicAdd(&counters[p], 1) == 0) break;
-            __threadfence();
-            int l = left[p], r = right[p];
-            T   lb[6], rb[6];
-            load_box_cg(soa, l, lb);
-            load_box_cg(soa, r, rb);
-            int hl = (l >= n - 1) ? 0 : (int)__ldcg(height + l);
-            int hr = (r >= n - 1) ? 0 : (int)__ldcg(height + r);
-            T   pb[6];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                pb[2 * d]     = box_min(lb[2 * d], rb[2 * d]);
-                pb[2 * d + 1] = box_max(lb[2 * d + 1], rb[2 * d + 1]);
-            }
-#pragma unroll
-            for (int d = 0; d < 6; ++d) __stcg(soa_w[d] + p, pb[d]);
-            NodeRec<T> rec;
-#pragma unroll
-            for (int d = 0; d < 6; ++d) {
-                rec.lb[d] = lb[d];
-                rec.rb[d] = rb[d];
-            }
-            rec.l = l;
-            rec.r = r;
-#pragma unroll
-            for (int d = 0; d < (int)(sizeof(rec.pad) / 4); ++d) rec.pad[d] = 0;
-            recs[p] = rec;
-            int h   = 1 + max(hl, hr);
-            __stcg(height + p, (uint8_t)min(h, 255));
-            curr = p;
-        }
-    }
+    T *const soa[6] = {mnx, mxx, mny, mxy, mnz, mxz};
+    for (int leaf = blockIdx.x * blockDim.x + threadIdx.x; leaf < n; leaf += gridDim.x * blockDim.x)
+        refit_leaf<T>(leaf, n, left, right, parent, soa, recs, height, counters);
 }
 
 // =========================================================================================
@@ -801,6 +561,42 @@ template <int W> static void sort_impl(TreeImpl &s, size_t n, cudaStream_t st) {
         std::swap(s.perm, s.tmp_perm);
     }
 }
+
+// The same sort over a fixed list of digit positions: no histogram read-back, so no host
+// synchronisation (used by the batched build, whose launch sequence is graph-captured).
+template <int W> static void sort_fixed_impl(TreeImpl &s, size_t n, int ndig, const int *digits, cudaStream_t st) {
+    using Cfg    = SortCfg<W>;
+    const int D  = 8 * W;
+    size_t tiles = (n + Cfg::tile - 1) / Cfg::tile;
+    FT_CUDA(cudaMemsetAsync(s.hist, 0, (16 * 256 + 16) * sizeof(uint32_t), st));
+    radix_hist_kernel<W><<<grid_for(n, 256, 148 * 4), 256, 0, st>>>((const unsigned long long *)s.key_lo,
+                                                                      (const unsigned long long *)s.key_hi, n,
+                                                                      s.hist);
+    radix_scan_kernel<<<D, 256, 0, st>>>(s.hist, n, s.hist + 16 * 256);
+    FT_CUDA(cudaGetLastError());
+    FT_CUDA(cudaMemsetAsync(s.lookback, 0, (size_t)D * tiles * 256 * sizeof(uint32_t), st));
+    FT_CUDA(cudaMemsetAsync(s.tile_counter, 0, 16 * sizeof(uint32_t), st));
+    FT_CUDA(cudaFuncSetAttribute(onesweep_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem));
+    for (int i = 0; i < ndig; ++i) {
+        const int d = digits[i];
+        onesweep_kernel<W><<<(unsigned)tiles, kSortThreads, Cfg::smem, st>>>(
+            (const unsigned long long *)s.key_lo, (const unsigned long long *)s.key_hi, s.perm,
+            (unsigned long long *)s.tmp_lo, (unsigned long long *)s.tmp_hi, s.tmp_perm, n, d >> 3, 8 * (d & 7),
+            s.hist + d * 256, s.lookback + (size_t)d * tiles * 256, s.tile_counter + d, s.status);
+        FT_CUDA(cudaGetLastError());
+        std::swap(s.key_lo, s.tmp_lo);
+        std::swap(s.key_hi, s.tmp_hi);
+        std::swap(s.perm, s.tmp_perm);
+    }
+}
+
+void sort_pairs_fixed(TreeImpl &s, size_t n, int words, int ndigits, const int *digits, cudaStream_t st) {
+    if (n < 2 || ndigits <= 0) return;
+    if (words == 1) sort_fixed_impl<1>(s, n, ndigits, digits, st);
+    else sort_fixed_impl<2>(s, n, ndigits, digits, st);
+}
+
+size_t sort_lookback_words(size_t n, int words) { return 16 * sort_tiles(n, words) * 256; }
 
 static void sort_keys(const ft_options &o, TreeImpl &s, size_t n, cudaStream_t st) {
     if (n < 2) return;

@@ -98,7 +98,9 @@ void check_device_status(uint32_t *status, cudaStream_t st) {
     if (!v) return;
     FT_CUDA(cudaMemsetAsync(status, 0, sizeof(uint32_t), st));
     FT_CUDA(cudaStreamSynchronize(st));
-    if (v & STATUS_BAD_INPUT) fail(FT_ERR_INVALID_ARGUMENT, "a leaf id was outside [0, num_leaves)");
+    if (v & STATUS_BAD_INPUT)
+        fail(FT_ERR_INVALID_ARGUMENT, "bad input on the device: a leaf id outside [0, num_leaves), or batch set "
+                                      "offsets that do not start at 0, end at num_points and increase");
     if (v & STATUS_SPIN_LIMIT) fail(FT_ERR_TIMEOUT, "a bounded device-side wait gave up (radix-sort look-back)");
     fail(FT_ERR_RUNTIME, "a traversal exceeded its visit bound (corrupt tree)");
 }
@@ -183,6 +185,22 @@ struct ft_context : public ft::Context {};
 static void need(bool c, const char *msg) {
     if (!c) fail(FT_ERR_INVALID_ARGUMENT, msg);
 }
+
+// Trees handed out by ft_batch_tree live inside their batch.
+static void need_owned(const ft_tree *t) {
+    if (t && t->impl && ((const TreeImpl *)t->impl)->view)
+        fail(FT_ERR_INVALID_ARGUMENT, "a set view of a batch cannot be rebuilt, resized or destroyed");
+}
+
+// Arguments of the batched entry points must be device-accessible (no staging: the calls
+// are asynchronous and may be captured in a CUDA graph).
+static void need_device(const void *p, const char *what) {
+    if (p && is_host_only(p)) fail(FT_ERR_INVALID_ARGUMENT, std::string(what) + " must be device memory");
+}
+
+struct ft_batch {
+    ft::BatchImpl *impl;
+};
 
 extern "C" {
 
@@ -272,6 +290,7 @@ ft_status ft_tree_create(ft_context *ctx, size_t n, ft_tree **out) {
 ft_status ft_tree_ensure(ft_context *ctx, ft_tree *t, size_t n) {
     FT_API_BEGIN
     need(ctx && t, "null argument");
+    need_owned(t);
     DeviceGuard g(ctx->device);
     if (n > t->capacity) { // TreePool::ensure (src/hlbvh.hpp:691-705)
         tree_free_arrays(*t);
@@ -286,6 +305,7 @@ ft_status ft_tree_destroy(ft_context *ctx, ft_tree *t) {
     FT_API_BEGIN
     if (!t) return FT_OK;
     need(ctx != nullptr, "null context");
+    need_owned(t);
     DeviceGuard g(ctx->device);
     tree_free_arrays(*t);
     if (t->impl) {
@@ -369,6 +389,7 @@ ft_status ft_build_bvh(ft_context *ctx, const void *x, const void *y, const void
                        const int8_t *is_ghost, const void *bbox6, void *keys, ft_tree *tree, ft_stream_t stream) {
     FT_API_BEGIN
     need(ctx && tree, "null argument");
+    need_owned(tree);
     if (n == 0) return FT_OK; // src/hlbvh.hpp:2174
     if (n > (size_t)(INT_MAX / 2))
         fail(FT_ERR_RUNTIME, "Particle count n exceeds maximum supported tree size (INT_MAX / 2).");
@@ -415,6 +436,7 @@ ft_status ft_build_tree(ft_context *ctx, ft_tree *tree, const void *sorted_keys,
                         const int8_t *sorted_is_ghost, const int32_t *sorted_orig_idx, ft_stream_t stream) {
     FT_API_BEGIN
     need(ctx && tree, "null argument");
+    need_owned(tree);
     size_t n = tree->num_leaves;
     if (n == 0) return FT_OK;
     need(sorted_keys != nullptr, "null key array");
@@ -538,6 +560,119 @@ ft_status ft_range(ft_context *ctx, const ft_tree *tree, const void *qx, const v
     sr.copy_back();
     sc.copy_back();
     check_device_status(ctx->status, st);
+    FT_API_END
+}
+
+// ---------------------------------------------------------------------------------------
+// Batched sets (ft_batch.cu)
+// ---------------------------------------------------------------------------------------
+ft_status ft_batch_create(ft_context *ctx, size_t max_points, size_t max_sets, ft_batch **out) {
+    FT_API_BEGIN
+    need(ctx && out, "null argument");
+    DeviceGuard g(ctx->device);
+    ft::BatchImpl *b = ft::batch_create(*ctx, max_points, max_sets);
+    ft_batch      *h = new (std::nothrow) ft_batch{b};
+    if (!h) {
+        ft::batch_free(b);
+        throw std::bad_alloc();
+    }
+    *out = h;
+    FT_API_END
+}
+
+ft_status ft_batch_destroy(ft_context *ctx, ft_batch *batch) {
+    FT_API_BEGIN
+    if (!batch) return FT_OK;
+    need(ctx != nullptr, "null context");
+    DeviceGuard g(ctx->device);
+    ft::batch_free(batch->impl);
+    delete batch;
+    FT_API_END
+}
+
+static void batch_args(const int64_t *off, size_t num_points, const void *x, const void *y, const void *z,
+                       const uint32_t *id, const int8_t *is_ghost) {
+    need(off != nullptr, "null set_offsets");
+    need(num_points == 0 || (x && y && z), "null coordinate array");
+    need_device(off, "set_offsets");
+    need_device(x, "x");
+    need_device(y, "y");
+    need_device(z, "z");
+    need_device(id, "id");
+    need_device(is_ghost, "is_ghost");
+}
+
+ft_status ft_batch_build(ft_context *ctx, ft_batch *batch, const int64_t *set_offsets, size_t num_sets,
+                         size_t num_points, const void *x, const void *y, const void *z, const uint32_t *id,
+                         const int8_t *is_ghost, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && batch, "null argument");
+    DeviceGuard g(ctx->device);
+    batch_args(set_offsets, num_points, x, y, z, id, is_ghost);
+    ft::batch_build(*ctx, *batch->impl, (const long long *)set_offsets, num_sets, num_points, x, y, z, id, is_ghost,
+                    (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_batch_self_knn(ft_context *ctx, ft_batch *batch, int k, int exclude_self, uint64_t *idx_out,
+                            void *dist_out, const ft_query_options *qopts, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && batch, "null argument");
+    ft_query_options q{};
+    if (qopts) q = *qopts;
+    DeviceGuard g(ctx->device);
+    if (k > 0) {
+        need(idx_out && dist_out, "null output array");
+        need_device(idx_out, "idx_out");
+        need_device(dist_out, "dist_out");
+    }
+    ft::batch_query(*ctx, *batch->impl, k, exclude_self != 0, idx_out, dist_out, q, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_batch_build_knn(ft_context *ctx, ft_batch *batch, const int64_t *set_offsets, size_t num_sets,
+                             size_t num_points, const void *x, const void *y, const void *z, const uint32_t *id,
+                             const int8_t *is_ghost, int k, int exclude_self, uint64_t *idx_out, void *dist_out,
+                             const ft_query_options *qopts, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && batch, "null argument");
+    ft_query_options q{};
+    if (qopts) q = *qopts;
+    DeviceGuard g(ctx->device);
+    batch_args(set_offsets, num_points, x, y, z, id, is_ghost);
+    if (k > 0) {
+        need(idx_out && dist_out, "null output array");
+        need_device(idx_out, "idx_out");
+        need_device(dist_out, "dist_out");
+    }
+    ft::batch_build_query_graph(*ctx, *batch->impl, (const long long *)set_offsets, num_sets, num_points, x, y, z,
+                                id, is_ghost, k, exclude_self != 0, idx_out, dist_out, q, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_batch_tree(ft_context *ctx, ft_batch *batch, size_t set, ft_tree *out, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && batch && out, "null argument");
+    DeviceGuard g(ctx->device);
+    ft::batch_tree_view(*ctx, *batch->impl, set, *out, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_batch_set_info(ft_context *ctx, ft_batch *batch, void *bbox_out, uint8_t *height_out,
+                            ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && batch, "null argument");
+    DeviceGuard g(ctx->device);
+    ft::batch_set_info(*ctx, *batch->impl, bbox_out, height_out, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_batch_query_stats(ft_context *ctx, ft_batch *batch, ft_query_stats *out) {
+    FT_API_BEGIN
+    need(ctx && batch && out, "null argument");
+    DeviceGuard g(ctx->device);
+    *out = ft_query_stats{};
+    ft::batch_stats(*batch->impl, *out);
     FT_API_END
 }
 

@@ -8,6 +8,8 @@
 #include <cfloat>
 #include <type_traits>
 
+#include "ft_internal.h"
+
 #define FT_HD __host__ __device__ __forceinline__
 #define FT_D __device__ __forceinline__
 
@@ -228,6 +230,50 @@ template <class T> struct TreeDev {
     const NodeRec<T> *recs;
     int               n; // leaves
 };
+
+// Device view of a built tree.
+template <class T> inline TreeDev<T> tree_view(const ft_tree &tr) {
+    TreeDev<T> v;
+    v.min_x    = (const T *)tr.min_x;
+    v.max_x    = (const T *)tr.max_x;
+    v.min_y    = (const T *)tr.min_y;
+    v.max_y    = (const T *)tr.max_y;
+    v.min_z    = (const T *)tr.min_z;
+    v.max_z    = (const T *)tr.max_z;
+    v.orig_idx = tr.orig_idx;
+    v.recs     = (const NodeRec<T> *)((TreeImpl *)tr.impl)->recs;
+    v.n        = (int)tr.num_leaves;
+    return v;
+}
+
+// ---------------------------------------------------------------------------------------
+// Batched trees (BatchDev, ft_internal.h): locating a leaf's set and viewing one set.
+// ---------------------------------------------------------------------------------------
+// Set holding global leaf q (the largest s with off[s] <= q; empty sets are skipped).
+FT_D int find_set(const long long *off, int S, long long q) {
+    int lo = 0, hi = S;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (off[mid] <= q) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <class T> FT_D TreeDev<T> set_view(const TreeDev<T> &all, const BatchDev &b, int s) {
+    const long long nb = b.node_off[s], rb = b.rec_off[s];
+    TreeDev<T>      t;
+    t.min_x    = all.min_x + nb;
+    t.max_x    = all.max_x + nb;
+    t.min_y    = all.min_y + nb;
+    t.max_y    = all.max_y + nb;
+    t.min_z    = all.min_z + nb;
+    t.max_z    = all.max_z + nb;
+    t.orig_idx = all.orig_idx + nb;
+    t.recs     = all.recs + rb;
+    t.n        = (int)(b.off[s + 1] - b.off[s]);
+    return t;
+}
 
 // ---------------------------------------------------------------------------------------
 // Bit tricks

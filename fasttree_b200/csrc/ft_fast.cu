@@ -33,8 +33,9 @@ static constexpr int kFastThreads = 32 * kFastWarps;
 
 template <class T, int PER, int KC, int VAR>
 __global__ void __launch_bounds__(kFastThreads)
-    fast_self_knn_kernel(TreeDev<T> t, const int32_t *__restrict__ leaf_ids, int num, int k, int half_window,
-                         int exclude_self, int ret_orig, const typename Coord<T>::dist_t *__restrict__ bound,
+    fast_self_knn_kernel(TreeDev<T> t_all, BatchDev bt, const int32_t *__restrict__ leaf_ids, int num, int k,
+                         int half_window, int exclude_self, int ret_orig,
+                         const typename Coord<T>::dist_t *__restrict__ bound,
                          unsigned long long *__restrict__ out_idx, typename Coord<T>::dist_t *__restrict__ out_dist,
                          int32_t *__restrict__ replay_ranks, int32_t *__restrict__ replay_rows,
                          uint32_t *replay_count, uint32_t *status, unsigned long long *visit_count) {
@@ -50,11 +51,26 @@ __global__ void __launch_bounds__(kFastThreads)
     if (qbase >= num) return; // warp-uniform
     const int q      = qbase + lane;
     bool      active = q < num;
-    const int n      = t.n;
+    // Batched sets: each lane walks the tree of the set its query belongs to (rank local to
+    // the set, output row global); a set taller than 62 goes straight to the replay.
+    TreeDev<T> t            = t_all;
+    int        rank         = 0;
+    bool       force_replay = false;
+    if (bt.off) {
+        const int s = find_set(bt.off, bt.S, active ? q : num - 1);
+        t           = set_view(t_all, bt, s);
+        rank        = (active ? q : num - 1) - (int)bt.off[s];
+        if (active && bt.height[s] > 62) {
+            force_replay = true;
+            active       = false;
+        }
+    } else {
+        rank = active ? (leaf_ids ? leaf_ids[q] : q) : 0;
+    }
+    const int n = t.n;
 #define HD(s) hd[(s) * kFastThreads + tid]
 #define HI(s) hix[(s) * kFastThreads + tid]
 
-    int rank = active ? (leaf_ids ? leaf_ids[q] : q) : 0;
     if (active && (rank < 0 || rank >= n)) {
         atomicOr(status, STATUS_BAD_INPUT);
         for (int i = 0; i < k; ++i) {
@@ -352,11 +368,11 @@ __global__ void __launch_bounds__(kFastThreads)
                 __stcs(out_dist + off + i, dist_missing<D>());
             }
         }
-        if (flag) {
-            uint32_t at      = atomicAdd(replay_count, 1u);
-            replay_ranks[at] = rank;
-            replay_rows[at]  = q;
-        }
+    }
+    if ((active && flag) || force_replay) {
+        uint32_t at      = atomicAdd(replay_count, 1u);
+        replay_ranks[at] = rank;
+        replay_rows[at]  = q;
     }
 #undef HD
 #undef HI
@@ -364,9 +380,9 @@ __global__ void __launch_bounds__(kFastThreads)
 
 // -----------------------------------------------------------------------------------------
 template <class T, int PER, int KC>
-static void launch_fast_t(const TreeDev<T> &tv, const int32_t *leaf_ids, int num, int k, int half, bool excl, bool ro,
-                          const void *bound, uint64_t *idx, void *dist, int32_t *rr, int32_t *rw, uint32_t *rc,
-                          uint32_t *status, int variant, unsigned long long *visits, cudaStream_t st) {
+static void launch_fast_t(const TreeDev<T> &tv, const BatchDev &bt, const int32_t *leaf_ids, int num, int k, int half,
+                          bool excl, bool ro, const void *bound, uint64_t *idx, void *dist, int32_t *rr, int32_t *rw,
+                          uint32_t *rc, uint32_t *status, int variant, unsigned long long *visits, cudaStream_t st) {
     using D     = typename Coord<T>::dist_t;
     size_t smem = (size_t)KC * kFastThreads * (sizeof(D) + 4);
     auto   fn   = variant == 0 ? fast_self_knn_kernel<T, PER, KC, 0>
@@ -374,35 +390,35 @@ static void launch_fast_t(const TreeDev<T> &tv, const int32_t *leaf_ids, int num
                                  : fast_self_knn_kernel<T, PER, KC, 2>;
     FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int blocks = (num + kFastThreads - 1) / kFastThreads;
-    fn<<<blocks, kFastThreads, smem, st>>>(tv, leaf_ids, num, k, half, excl ? 1 : 0, ro ? 1 : 0, (const D *)bound,
-                                           (unsigned long long *)idx, (D *)dist, rr, rw, rc, status, visits);
+    fn<<<blocks, kFastThreads, smem, st>>>(tv, bt, leaf_ids, num, k, half, excl ? 1 : 0, ro ? 1 : 0,
+                                           (const D *)bound, (unsigned long long *)idx, (D *)dist, rr, rw, rc,
+                                           status, visits);
     FT_CUDA(cudaGetLastError());
+}
+
+// Launches the fast walk over `tv` (one tree, or every set of a batch when bt.off is set).
+template <class T>
+static void launch_fast_view(const TreeDev<T> &tv, const BatchDev &bt, int met, bool ro, const int32_t *leaf_ids,
+                             int num, int k, int half, bool excl, const void *bound, uint64_t *idx, void *dist,
+                             int32_t *rr, int32_t *rw, uint32_t *rc, uint32_t *status, int variant,
+                             unsigned long long *visits, cudaStream_t st) {
+    met_dispatch<T>(met, [&](auto M) {
+        constexpr int PER = decltype(M)::value;
+        if (k <= 32)
+            launch_fast_t<T, PER, 32>(tv, bt, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc, status,
+                                      variant, visits, st);
+        else
+            launch_fast_t<T, PER, 64>(tv, bt, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc, status,
+                                      variant, visits, st);
+    });
 }
 
 template <class T>
 static void launch_fast(const ft_options &o, const ft_tree &tr, const int32_t *leaf_ids, int num, int k, int half,
                         bool excl, const void *bound, uint64_t *idx, void *dist, int32_t *rr, int32_t *rw,
                         uint32_t *rc, uint32_t *status, int variant, unsigned long long *visits, cudaStream_t st) {
-    TreeDev<T> tv;
-    tv.min_x    = (const T *)tr.min_x;
-    tv.max_x    = (const T *)tr.max_x;
-    tv.min_y    = (const T *)tr.min_y;
-    tv.max_y    = (const T *)tr.max_y;
-    tv.min_z    = (const T *)tr.min_z;
-    tv.max_z    = (const T *)tr.max_z;
-    tv.orig_idx = tr.orig_idx;
-    tv.recs     = (const NodeRec<T> *)((TreeImpl *)tr.impl)->recs;
-    tv.n        = (int)tr.num_leaves;
-    bool ro     = o.return_orig_indices != 0;
-    met_dispatch<T>(metric_mode<T>(o, tr), [&](auto M) {
-        constexpr int PER = decltype(M)::value;
-        if (k <= 32)
-            launch_fast_t<T, PER, 32>(tv, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc, status,
-                                      variant, visits, st);
-        else
-            launch_fast_t<T, PER, 64>(tv, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc, status,
-                                      variant, visits, st);
-    });
+    launch_fast_view<T>(tree_view<T>(tr), BatchDev{}, metric_mode<T>(o, tr), o.return_orig_indices != 0, leaf_ids,
+                        num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st);
 }
 
 bool fast_self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, bool excl,
@@ -424,6 +440,33 @@ bool fast_self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, siz
     }
     replay_exact(ctx, tr, ctx.replay_ranks, ctx.replay_rows, rc, k, excl, idx, dist, st);
     return true;
+}
+
+void batch_self_knn(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, bool excl, uint64_t *idx,
+                    void *dist, bool fast, int half_window, int variant, int32_t *rr, int32_t *rw, uint32_t *counters,
+                    cudaStream_t st) {
+    if (num == 0 || k <= 0) return;
+    if (!fast || k > 64) {
+        batch_self_knn_exact(ctx, all, bt, num, k, excl, idx, dist, st);
+        return;
+    }
+    if (half_window <= 0) half_window = k;
+    variant                        = variant == 0 ? 2 : variant == 3 ? 0 : variant;
+    unsigned long long *visits     = (unsigned long long *)(counters + 2);
+    const bool          ro         = ctx.opts.return_orig_indices != 0;
+    const int           n          = (int)num;
+    FT_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), st));
+#define FT_BF(T)                                                                                                   \
+    launch_fast_view<T>(tree_view<T>(all), bt, metric_mode<T>(ctx.opts, all), ro, nullptr, n, k, half_window, excl, \
+                        nullptr, idx, dist, rr, rw, counters, ctx.status, variant, visits, st)
+    switch (ctx.opts.coord_type) {
+    case F32: FT_BF(float); break;
+    case F64: FT_BF(double); break;
+    case U32: FT_BF(uint32_t); break;
+    case U64: FT_BF(unsigned long long); break;
+    }
+#undef FT_BF
+    replay_exact(ctx, all, rr, rw, counters, k, excl, idx, dist, st, bt);
 }
 
 void ensure_replay(Context &ctx, size_t num) {

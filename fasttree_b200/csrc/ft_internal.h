@@ -49,6 +49,19 @@ struct TreeImpl {
     bool      managed      = false;
     int       height_root  = -1;    // host copy after a build
     bool      clean42      = false; // 64-bit integer tree with every coordinate below 2^42
+    bool      view         = false; // one set of a batch: arrays owned by the batch, no builds
+};
+
+// Batched trees: S independent trees stored back to back.  Set s owns leaves (queries)
+// [off[s], off[s+1]); its nodes start at node_off[s] in the node arrays and its internal
+// records / child arrays at rec_off[s].  Inside a set, indices follow TreeSoA's layout.
+// All arrays live on the device.
+struct BatchDev {
+    const long long *off      = nullptr; // S + 1 leaf offsets (null: a single tree)
+    const long long *node_off = nullptr;
+    const long long *rec_off  = nullptr;
+    const uint8_t   *height   = nullptr; // root height of each set's tree
+    int              S        = 0;
 };
 
 // Distance mode of query kernels on this tree (see met_dispatch in ft_common.cuh).
@@ -82,7 +95,16 @@ size_t noalloc_max_queries();
 // Reruns the listed self queries (ranks[i] -> row rows[i], *count_dev of them) with the
 // reference traversal (ft_query.cu).
 void replay_exact(Context &ctx, const ft_tree &tree, const int32_t *ranks, const int32_t *rows, uint32_t *count_dev,
-                  int k, bool exclude_self, uint64_t *idx, void *dist, cudaStream_t st);
+                  int k, bool exclude_self, uint64_t *idx, void *dist, cudaStream_t st, const BatchDev &bt = {});
+// Self-kNN over every leaf of a batch of trees (`all` spans the concatenated arrays):
+// the fast walk with its replay (replay lists rr / rw, counters = 4 device words) or, with
+// fast == false or k > 64, the reference traversal.  No allocation, no host synchronisation.
+void batch_self_knn(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, bool exclude_self,
+                    uint64_t *idx, void *dist, bool fast, int half_window, int variant, int32_t *rr, int32_t *rw,
+                    uint32_t *counters, cudaStream_t st);
+// The reference traversal over every leaf of a batch (ft_query.cu).
+void batch_self_knn_exact(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, bool exclude_self,
+                          uint64_t *idx, void *dist, cudaStream_t st);
 
 // Reads and clears a device status word (synchronises the stream); throws on a set bit.
 void check_device_status(uint32_t *status, cudaStream_t st);
@@ -99,6 +121,10 @@ void compute_bbox(Context &ctx, TreeImpl *scratch, const void *x, const void *y,
 void sfc_encode_ref_layout(Context &ctx, TreeImpl &scratch, const void *x, const void *y, const void *z,
                            size_t n, const void *bbox_dev, void *keys_ref_dev, cudaStream_t st);
 size_t ref_key_bytes(const ft_options &o);
+// Onesweep sort of (key_lo[, key_hi], perm) in s over a fixed digit list (8-bit digits,
+// d < 8: low word, 8 <= d < 16: high word); no host synchronisation.
+void   sort_pairs_fixed(TreeImpl &s, size_t n, int words, int ndigits, const int *digits, cudaStream_t st);
+size_t sort_lookback_words(size_t n, int words);
 void   ensure_scratch(TreeImpl &impl, const ft_options &o, size_t n);
 void   free_scratch(TreeImpl &impl);
 
@@ -112,5 +138,22 @@ void range(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, co
            int max_per_q, cudaStream_t st);
 
 size_t coord_bytes(int coord);
+
+// ---- batched sets (ft_batch.cu) ----
+struct BatchImpl;
+BatchImpl *batch_create(Context &ctx, size_t max_points, size_t max_sets);
+void       batch_free(BatchImpl *b);
+// set_offsets: device, S + 1 entries.  Asynchronous; no allocation, no host synchronisation.
+void batch_build(Context &ctx, BatchImpl &b, const long long *set_offsets, size_t S, size_t N, const void *x,
+                 const void *y, const void *z, const uint32_t *id, const int8_t *ghost, cudaStream_t st);
+void batch_query(Context &ctx, BatchImpl &b, int k, bool exclude_self, uint64_t *idx, void *dist,
+                 const ft_query_options &q, cudaStream_t st);
+void batch_build_query_graph(Context &ctx, BatchImpl &b, const long long *set_offsets, size_t S, size_t N,
+                             const void *x, const void *y, const void *z, const uint32_t *id, const int8_t *ghost,
+                             int k, bool exclude_self, uint64_t *idx, void *dist, const ft_query_options &q,
+                             cudaStream_t st);
+void batch_tree_view(Context &ctx, BatchImpl &b, size_t set, ft_tree &out, cudaStream_t st);
+void batch_set_info(Context &ctx, BatchImpl &b, void *bbox_out, uint8_t *height_out, cudaStream_t st);
+void batch_stats(BatchImpl &b, ft_query_stats &out);
 
 } // namespace ft

@@ -204,7 +204,7 @@ FT_D bool self_point(const TreeDev<T> &t, int rank, int k, size_t row, unsigned 
 }
 
 template <class T, int CAP, int QT, bool SELF, int PER>
-__global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t, const T *__restrict__ qx,
+__global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t_all, BatchDev bt, const T *__restrict__ qx,
                                                        const T *__restrict__ qy, const T *__restrict__ qz,
                                                        const int32_t *__restrict__ leaf_ids, int num, int k,
                                                        int exclude_self, int ret_orig,
@@ -218,10 +218,18 @@ __global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t, const T *__
     const int tid = threadIdx.x;
     const int q   = blockIdx.x * QT + tid;
     if (q >= num) return;
-    T   px, py, pz;
-    int self_leaf = -1;
+    T          px, py, pz;
+    int        self_leaf = -1;
+    TreeDev<T> t         = t_all;
     if (SELF) {
-        int rank = leaf_ids ? leaf_ids[q] : q;
+        int rank;
+        if (bt.off) { // batched sets: row q is leaf q - off[s] of set s
+            const int s = find_set(bt.off, bt.S, q);
+            t           = set_view(t_all, bt, s);
+            rank        = q - (int)bt.off[s];
+        } else {
+            rank = leaf_ids ? leaf_ids[q] : q;
+        }
         if (!self_point(t, rank, k, (size_t)q, out_idx, out_dist, status, px, py, pz)) return;
         if (exclude_self) self_leaf = rank + t.n - 1;
     } else {
@@ -235,9 +243,11 @@ __global__ void __launch_bounds__(QT) exact_knn_kernel(TreeDev<T> t, const T *__
 
 // Replays the self queries listed by the fast traversal (ranks[i] -> output row rows[i]) with
 // the reference traversal; grid-stride over a count that lives on the device, so no host
-// synchronisation is needed between the two launches.
+// synchronisation is needed between the two launches.  For batched sets the row names the
+// set and the rank is local to it.
 template <class T, int CAP, int QT, int PER>
-__global__ void __launch_bounds__(QT) exact_replay_kernel(TreeDev<T> t, const int32_t *__restrict__ ranks,
+__global__ void __launch_bounds__(QT) exact_replay_kernel(TreeDev<T> t_all, BatchDev bt,
+                                                          const int32_t *__restrict__ ranks,
                                                           const int32_t *__restrict__ rows,
                                                           const uint32_t *__restrict__ count_dev, int k,
                                                           int exclude_self, int ret_orig,
@@ -251,9 +261,10 @@ __global__ void __launch_bounds__(QT) exact_replay_kernel(TreeDev<T> t, const in
     const int tid  = threadIdx.x;
     const int cnt  = (int)*count_dev;
     for (int i = blockIdx.x * QT + tid; i < cnt; i += gridDim.x * QT) {
-        const int rank = ranks[i];
-        const int row  = rows[i];
-        T         px, py, pz;
+        const int  rank = ranks[i];
+        const int  row  = rows[i];
+        TreeDev<T> t    = bt.off ? set_view(t_all, bt, find_set(bt.off, bt.S, row)) : t_all;
+        T          px, py, pz;
         if (!self_point(t, rank, k, (size_t)row, out_idx, out_dist, status, px, py, pz)) continue;
         exact_query<T, CAP, QT, PER>(t, px, py, pz, exclude_self ? rank + t.n - 1 : -1, k, ret_orig, hd, hix, tid,
                                      (size_t)row, out_idx, out_dist, status);
@@ -454,23 +465,9 @@ __global__ void __launch_bounds__(128) range_kernel(TreeDev<T> t, const T *__res
 // =========================================================================================
 // Host side
 // =========================================================================================
-template <class T> static TreeDev<T> dev_view(const ft_tree &tr) {
-    TreeDev<T> v;
-    v.min_x    = (const T *)tr.min_x;
-    v.max_x    = (const T *)tr.max_x;
-    v.min_y    = (const T *)tr.min_y;
-    v.max_y    = (const T *)tr.max_y;
-    v.min_z    = (const T *)tr.min_z;
-    v.max_z    = (const T *)tr.max_z;
-    v.orig_idx = tr.orig_idx;
-    v.recs     = (const NodeRec<T> *)((TreeImpl *)tr.impl)->recs;
-    v.n        = (int)tr.num_leaves;
-    return v;
-}
-
 // Heap capacity tiers and the threads per block that keep the heap at <= 96 KB.
 template <class T, int CAP, int QT, bool SELF, int PER>
-static void launch_exact_t(const TreeDev<T> &tv, const void *qx, const void *qy, const void *qz,
+static void launch_exact_t(const TreeDev<T> &tv, const BatchDev &bt, const void *qx, const void *qy, const void *qz,
                            const int32_t *leaf_ids, int num, int k, bool excl, bool ro, uint64_t *idx, void *dist,
                            uint32_t *status, cudaStream_t st) {
     using D     = typename Coord<T>::dist_t;
@@ -478,17 +475,17 @@ static void launch_exact_t(const TreeDev<T> &tv, const void *qx, const void *qy,
     auto   fn   = exact_knn_kernel<T, CAP, QT, SELF, PER>;
     FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int blocks = (num + QT - 1) / QT;
-    fn<<<blocks, QT, smem, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz, leaf_ids, num, k, excl ? 1 : 0,
-                                 ro ? 1 : 0, (unsigned long long *)idx, (D *)dist, status);
+    fn<<<blocks, QT, smem, st>>>(tv, bt, (const T *)qx, (const T *)qy, (const T *)qz, leaf_ids, num, k,
+                                 excl ? 1 : 0, ro ? 1 : 0, (unsigned long long *)idx, (D *)dist, status);
     FT_CUDA(cudaGetLastError());
 }
 
 template <class T, bool SELF, int PER>
-static void launch_exact_cap(const TreeDev<T> &tv, const void *qx, const void *qy, const void *qz,
-                             const int32_t *leaf_ids, int num, int k, bool excl, bool ro, uint64_t *idx, void *dist,
-                             uint32_t *status, cudaStream_t st) {
+static void launch_exact_cap(const TreeDev<T> &tv, const BatchDev &bt, const void *qx, const void *qy,
+                             const void *qz, const int32_t *leaf_ids, int num, int k, bool excl, bool ro,
+                             uint64_t *idx, void *dist, uint32_t *status, cudaStream_t st) {
 #define FT_LAUNCH(CAP, QT) \
-    launch_exact_t<T, CAP, QT, SELF, PER>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, status, st)
+    launch_exact_t<T, CAP, QT, SELF, PER>(tv, bt, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, status, st)
     if (k <= 32) FT_LAUNCH(32, 128);
     else if (k <= 64) FT_LAUNCH(64, 128);
     else if (k <= 128) FT_LAUNCH(128, 64);
@@ -500,11 +497,12 @@ static void launch_exact_cap(const TreeDev<T> &tv, const void *qx, const void *q
 template <class T, bool SELF>
 static void launch_exact(const ft_options &o, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
                          const int32_t *leaf_ids, int num, int k, bool excl, uint64_t *idx, void *dist,
-                         uint32_t *status, cudaStream_t st) {
-    TreeDev<T> tv = dev_view<T>(tr);
+                         uint32_t *status, cudaStream_t st, const BatchDev &bt = {}) {
+    TreeDev<T> tv = tree_view<T>(tr);
     bool       ro = o.return_orig_indices != 0;
     met_dispatch<T>(metric_mode<T>(o, tr), [&](auto M) {
-        launch_exact_cap<T, SELF, decltype(M)::value>(tv, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist, status, st);
+        launch_exact_cap<T, SELF, decltype(M)::value>(tv, bt, qx, qy, qz, leaf_ids, num, k, excl, ro, idx, dist,
+                                                      status, st);
     });
 }
 
@@ -536,27 +534,30 @@ void self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t n
 }
 
 template <class T, int CAP, int QT, int PER>
-static void replay_t(const TreeDev<T> &tv, const int32_t *ranks, const int32_t *rows, uint32_t *cnt, int k, bool excl,
-                     bool ro, uint64_t *idx, void *dist, uint32_t *status, int num_sms, cudaStream_t st) {
+static void replay_t(const TreeDev<T> &tv, const BatchDev &bt, const int32_t *ranks, const int32_t *rows,
+                     uint32_t *cnt, int k, bool excl, bool ro, uint64_t *idx, void *dist, uint32_t *status,
+                     int num_sms, cudaStream_t st) {
     using D     = typename Coord<T>::dist_t;
     size_t smem = (size_t)CAP * QT * (sizeof(D) + 4);
     auto   fn   = exact_replay_kernel<T, CAP, QT, PER>;
     FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    fn<<<num_sms * 4, QT, smem, st>>>(tv, ranks, rows, cnt, k, excl ? 1 : 0, ro ? 1 : 0, (unsigned long long *)idx,
-                                       (D *)dist, status);
+    fn<<<num_sms * 4, QT, smem, st>>>(tv, bt, ranks, rows, cnt, k, excl ? 1 : 0, ro ? 1 : 0,
+                                       (unsigned long long *)idx, (D *)dist, status);
     FT_CUDA(cudaGetLastError());
 }
 
 template <class T>
-static void replay_typed(Context &ctx, const ft_tree &tr, const int32_t *ranks, const int32_t *rows, uint32_t *cnt,
-                         int k, bool excl, uint64_t *idx, void *dist, cudaStream_t st) {
-    TreeDev<T> tv  = dev_view<T>(tr);
+static void replay_typed(Context &ctx, const ft_tree &tr, const BatchDev &bt, const int32_t *ranks,
+                         const int32_t *rows, uint32_t *cnt, int k, bool excl, uint64_t *idx, void *dist,
+                         cudaStream_t st) {
+    TreeDev<T> tv  = tree_view<T>(tr);
     bool       ro  = ctx.opts.return_orig_indices != 0;
     int        met = metric_mode<T>(ctx.opts, tr);
     int        sms = ctx.num_sms;
-#define FT_RP(CAP, QT)                                                                                          \
-    met_dispatch<T>(met, [&](auto M) {                                                                          \
-        replay_t<T, CAP, QT, decltype(M)::value>(tv, ranks, rows, cnt, k, excl, ro, idx, dist, ctx.status, sms, st); \
+#define FT_RP(CAP, QT)                                                                                             \
+    met_dispatch<T>(met, [&](auto M) {                                                                             \
+        replay_t<T, CAP, QT, decltype(M)::value>(tv, bt, ranks, rows, cnt, k, excl, ro, idx, dist, ctx.status, sms, \
+                                                 st);                                                              \
     })
     if (k <= 32) FT_RP(32, 128);
     else if (k <= 64) FT_RP(64, 128);
@@ -567,12 +568,25 @@ static void replay_typed(Context &ctx, const ft_tree &tr, const int32_t *ranks, 
 }
 
 void replay_exact(Context &ctx, const ft_tree &tr, const int32_t *ranks, const int32_t *rows, uint32_t *cnt, int k,
-                  bool excl, uint64_t *idx, void *dist, cudaStream_t st) {
+                  bool excl, uint64_t *idx, void *dist, cudaStream_t st, const BatchDev &bt) {
     switch (ctx.opts.coord_type) {
-    case F32: replay_typed<float>(ctx, tr, ranks, rows, cnt, k, excl, idx, dist, st); break;
-    case F64: replay_typed<double>(ctx, tr, ranks, rows, cnt, k, excl, idx, dist, st); break;
-    case U32: replay_typed<uint32_t>(ctx, tr, ranks, rows, cnt, k, excl, idx, dist, st); break;
-    case U64: replay_typed<unsigned long long>(ctx, tr, ranks, rows, cnt, k, excl, idx, dist, st); break;
+    case F32: replay_typed<float>(ctx, tr, bt, ranks, rows, cnt, k, excl, idx, dist, st); break;
+    case F64: replay_typed<double>(ctx, tr, bt, ranks, rows, cnt, k, excl, idx, dist, st); break;
+    case U32: replay_typed<uint32_t>(ctx, tr, bt, ranks, rows, cnt, k, excl, idx, dist, st); break;
+    case U64: replay_typed<unsigned long long>(ctx, tr, bt, ranks, rows, cnt, k, excl, idx, dist, st); break;
+    }
+}
+
+void batch_self_knn_exact(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, bool excl,
+                          uint64_t *idx, void *dist, cudaStream_t st) {
+    if (num == 0 || k <= 0) return;
+    if (k > kMaxExactK) fail(FT_ERR_RUNTIME, "self_knn_query: k too large for shared memory.");
+    const int n = (int)num;
+    switch (ctx.opts.coord_type) {
+    case F32: launch_exact<float, true>(ctx.opts, all, nullptr, nullptr, nullptr, nullptr, n, k, excl, idx, dist, ctx.status, st, bt); break;
+    case F64: launch_exact<double, true>(ctx.opts, all, nullptr, nullptr, nullptr, nullptr, n, k, excl, idx, dist, ctx.status, st, bt); break;
+    case U32: launch_exact<uint32_t, true>(ctx.opts, all, nullptr, nullptr, nullptr, nullptr, n, k, excl, idx, dist, ctx.status, st, bt); break;
+    case U64: launch_exact<unsigned long long, true>(ctx.opts, all, nullptr, nullptr, nullptr, nullptr, n, k, excl, idx, dist, ctx.status, st, bt); break;
     }
 }
 
@@ -598,7 +612,7 @@ static void knn_typed(const ft_options &o, const ft_tree &tr, const void *qx, co
     }
     int cap = 1;
     while (cap < max_k) cap <<= 1;
-    TreeDev<T> tv = dev_view<T>(tr);
+    TreeDev<T> tv = tree_view<T>(tr);
     bool       ro = o.return_orig_indices != 0;
     met_dispatch<T>(metric_mode<T>(o, tr), [&](auto M) {
         launch_merge<T, decltype(M)::value>(tv, qx, qy, qz, nq, k, cap, ro, idx, dist, status, st);
@@ -630,7 +644,7 @@ template <class T>
 static void range_typed(const ft_options &o, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
                         const void *rmin, const void *rmax, int nq, int32_t *results, int32_t *counts, int max_per,
                         uint32_t *status, cudaStream_t st) {
-    TreeDev<T> tv     = dev_view<T>(tr);
+    TreeDev<T> tv     = tree_view<T>(tr);
     int        blocks = (nq + 127) / 128;
     bool       ro     = o.return_orig_indices != 0;
     met_dispatch<T>(metric_mode<T>(o, tr), [&](auto M) {

@@ -393,3 +393,122 @@ def range_query(ctx: Context, tree: TreeSoA, qx, qy, qz, r_min, r_max, max_resul
     _call(lib().ft_range(ctx.handle, tree.c, _ptr(x), _ptr(y), _ptr(z), _ptr(r0), _ptr(r1), nq, _ptr(results),
                          _ptr(result_counts), int(max_results_per_query), _stream_handle(stream)))
     return results.view(nq, max_results_per_query) if nq * max_results_per_query else results, result_counts
+
+
+class _BatchSetTree(TreeSoA):
+    """One set of a BatchedSets as a TreeSoA (arrays inside the batch; valid until its next build)."""
+
+    def __init__(self, ctx: Context, batch: "BatchedSets", c: capi.FtTree):
+        self.ctx = ctx
+        self._batch = batch  # keeps the batch's storage alive
+        self._c = c
+        self._p = ctypes.pointer(c)
+
+    def free(self):
+        self._p = None
+
+
+class BatchedSets:
+    """Many independent point sets of uneven size built and queried together (ft_batch_*; no
+    counterpart in the reference, whose callers loop build_bvh + self_knn_query over sets).
+
+    Set s holds points [set_offsets[s], set_offsets[s+1]) of the concatenated coordinates; its
+    tree and neighbour rows are those of its own build_bvh / self_knn_query calls.  Every array
+    is device memory; build and queries are asynchronous and never synchronise the host."""
+
+    def __init__(self, ctx: Context, max_points: int, max_sets: int):
+        self.ctx = ctx
+        h = ctypes.c_void_p()
+        self._h = None
+        _call(lib().ft_batch_create(ctx.handle, int(max_points), int(max_sets), ctypes.byref(h)))
+        self._h = h
+        self._keep = ()
+        self.num_sets = 0
+        self.num_points = 0
+
+    def _device(self, a, dtype):
+        dev = f"cuda:{self.ctx.device}"
+        if isinstance(a, torch.Tensor):
+            t = a if a.dtype == dtype else a.to(dtype)
+            return t.to(dev).contiguous()
+        return torch.as_tensor(np.ascontiguousarray(a), device=dev).to(dtype).contiguous()
+
+    def _inputs(self, set_offsets, pos_x, pos_y, pos_z, id, is_ghost):
+        off = self._device(set_offsets, torch.int64)
+        xyz = [self._device(a, TORCH_COORD[self.ctx.coord]) for a in (pos_x, pos_y, pos_z)]
+        ids = None
+        if id is not None:  # 32-bit ids, passed through bit for bit
+            ids = (id if isinstance(id, torch.Tensor) and id.element_size() == 4 else
+                   torch.as_tensor(np.ascontiguousarray(id, np.uint32).view(np.int32)))
+            ids = ids.to(f"cuda:{self.ctx.device}").contiguous()
+        gh = None if is_ghost is None else self._device(is_ghost, torch.int8)
+        return off, xyz, ids, gh
+
+    def build(self, set_offsets, pos_x, pos_y, pos_z, id=None, is_ghost=None, stream=None):
+        off, xyz, ids, gh = self._inputs(set_offsets, pos_x, pos_y, pos_z, id, is_ghost)
+        S, N = off.numel() - 1, xyz[0].numel()
+        _call(lib().ft_batch_build(self.ctx.handle, self._h, _ptr(off), S, N, *[_ptr(a) for a in xyz], _ptr(ids),
+                                   _ptr(gh), _stream_handle(stream)))
+        self._keep = (off, xyz, ids, gh)
+        self.num_sets, self.num_points = S, N
+        return self
+
+    def self_knn(self, k: int, exclude_self=True, max_k: int = 32, method: int = 0, results=None,
+                 result_dists=None, stream=None, half_window: int = 0, variant: int = 0):
+        """self_knn_query<MAXK> of every set; rows in set order, indices local to each set."""
+        N = self.num_points
+        if results is None:
+            results, result_dists = _alloc_knn_out(self.ctx, N, k)
+        _call(lib().ft_batch_self_knn(self.ctx.handle, self._h, int(k), int(bool(exclude_self)), _ptr(results),
+                                      _ptr(result_dists), ctypes.byref(_qopts(max_k, method, half_window, variant)),
+                                      _stream_handle(stream)))
+        return results.view(N, k) if N * k else results, result_dists.view(N, k) if N * k else result_dists
+
+    def build_knn(self, set_offsets, pos_x, pos_y, pos_z, k: int, results, result_dists, exclude_self=True,
+                  max_k: int = 32, method: int = 1, id=None, is_ghost=None, stream=None):
+        """build + self_knn as one CUDA graph (captured on the first call with these arrays, replayed
+        afterwards).  The arrays must stay alive and in place between calls: pass device tensors
+        of the right dtype, which are used as they are."""
+        off, xyz, ids, gh = self._inputs(set_offsets, pos_x, pos_y, pos_z, id, is_ghost)
+        S, N = off.numel() - 1, xyz[0].numel()
+        _call(lib().ft_batch_build_knn(self.ctx.handle, self._h, _ptr(off), S, N, *[_ptr(a) for a in xyz],
+                                       _ptr(ids), _ptr(gh), int(k), int(bool(exclude_self)), _ptr(results),
+                                       _ptr(result_dists), ctypes.byref(_qopts(max_k, method)),
+                                       _stream_handle(stream)))
+        self._keep = (off, xyz, ids, gh, results, result_dists)
+        self.num_sets, self.num_points = S, N
+        return results.view(N, k) if N * k else results, result_dists.view(N, k) if N * k else result_dists
+
+    def tree(self, s: int, stream=None) -> TreeSoA:
+        c = capi.FtTree()
+        _call(lib().ft_batch_tree(self.ctx.handle, self._h, int(s), ctypes.byref(c), _stream_handle(stream)))
+        return _BatchSetTree(self.ctx, self, c)
+
+    def set_info(self, stream=None):
+        """(boxes (S, 6) in the coordinate type, tree heights (S,) uint8) of the last build."""
+        S = self.num_sets
+        box = np.zeros((S, 6), NP_COORD[self.ctx.coord])
+        h = np.zeros(S, np.uint8)
+        _call(lib().ft_batch_set_info(self.ctx.handle, self._h, box.ctypes.data, h.ctypes.data,
+                                      _stream_handle(stream)))
+        return box, h
+
+    def query_stats(self):
+        st = capi.FtQueryStats()
+        _call(lib().ft_batch_query_stats(self.ctx.handle, self._h, ctypes.byref(st)))
+        return {"queries": st.queries, "replayed": st.replayed, "visits": st.reserved[0]}
+
+    def check(self, stream=None):
+        """Reports errors the kernels recorded (bad set offsets, bounded waits); synchronises."""
+        _call(lib().ft_check_device_status(self.ctx.handle, _stream_handle(stream)))
+
+    def free(self):
+        if getattr(self, "_h", None):
+            lib().ft_batch_destroy(self.ctx.handle, self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -189,6 +189,61 @@ ft_status ft_range(ft_context *ctx, const ft_tree *tree, const void *qx, const v
  * reach that guard. */
 ft_status ft_tree_height(ft_context *ctx, const ft_tree *tree, int *height_out);
 
+/* ---------------------------------------------------------------------------------- */
+/* Batched point sets.  No counterpart in the reference: its callers loop over sets and   */
+/* call build_bvh (src/hlbvh.hpp:2165-2302) and self_knn_query<MAXK> (1929-1954) once per */
+/* set.  Here num_sets independent sets of uneven size lie back to back in x/y/z (set s =  */
+/* points [set_offsets[s], set_offsets[s+1])) and go through one launch sequence; every    */
+/* set's tree and neighbour rows equal those of its own reference calls (own bounding box  */
+/* and keys, own leaf ranks, indices local to the set).                                  */
+/*                                                                                         */
+/* Keys must fit 63 bits: F32 / F64 coordinates (Morton or Peano-Hilbert) or U32 with      */
+/* Peano-Hilbert keys; a U64 context is rejected.  Every array argument is device memory.  */
+/* Build and query allocate nothing and never synchronise the host, so they may be        */
+/* captured in a CUDA graph; bad offsets (set_offsets[0] != 0, set_offsets[num_sets] !=   */
+/* num_points, or a decreasing pair) surface in ft_check_device_status.                   */
+/* ---------------------------------------------------------------------------------- */
+typedef struct ft_batch ft_batch;
+
+/* Storage for up to max_points points in up to max_sets (<= 2^24) sets. */
+ft_status ft_batch_create(ft_context *ctx, size_t max_points, size_t max_sets, ft_batch **out);
+ft_status ft_batch_destroy(ft_context *ctx, ft_batch *batch);
+
+/* build_bvh of every set.  set_offsets: num_sets + 1 int64.  id / is_ghost: NULL or
+ * num_points entries (NULL: the index within the set / 0, as the reference fills them).
+ * Asynchronous. */
+ft_status ft_batch_build(ft_context *ctx, ft_batch *batch, const int64_t *set_offsets, size_t num_sets,
+                         size_t num_points, const void *x, const void *y, const void *z, const uint32_t *id,
+                         const int8_t *is_ghost, ft_stream_t stream);
+
+/* self_knn_query<MAXK> of every set: row j (set s = the set holding j) is leaf j - off[s] of
+ * set s; indices are that set's leaf ranks (or input indices within the set with
+ * return_orig_indices).  idx_out / dist_out: num_points x k.  Default max_k 32; method 1
+ * selects the fast walk with exact replay.  Asynchronous. */
+ft_status ft_batch_self_knn(ft_context *ctx, ft_batch *batch, int k, int exclude_self, uint64_t *idx_out,
+                            void *dist_out, const ft_query_options *qopts, ft_stream_t stream);
+
+/* ft_batch_build + ft_batch_self_knn as one CUDA graph, captured on the first call with
+ * these arguments and replayed by later calls with the same arguments (array contents may
+ * change between calls).  Asynchronous. */
+ft_status ft_batch_build_knn(ft_context *ctx, ft_batch *batch, const int64_t *set_offsets, size_t num_sets,
+                             size_t num_points, const void *x, const void *y, const void *z, const uint32_t *id,
+                             const int8_t *is_ghost, int k, int exclude_self, uint64_t *idx_out, void *dist_out,
+                             const ft_query_options *qopts, ft_stream_t stream);
+
+/* View of one built set as an ft_tree (arrays inside the batch; valid until the next build
+ * of the batch).  Usable with every query entry point; not with builds, ensure or destroy.
+ * Blocking. */
+ft_status ft_batch_tree(ft_context *ctx, ft_batch *batch, size_t set, ft_tree *out, ft_stream_t stream);
+
+/* Per-set bounding boxes (host, 6 coordinates per set, or NULL) and tree heights (host,
+ * one byte per set, or NULL) of the last build.  Blocking. */
+ft_status ft_batch_set_info(ft_context *ctx, ft_batch *batch, void *bbox_out, uint8_t *height_out,
+                            ft_stream_t stream);
+
+/* Replay count and visits of the last ft_batch_self_knn / ft_batch_build_knn (synchronises). */
+ft_status ft_batch_query_stats(ft_context *ctx, ft_batch *batch, ft_query_stats *out);
+
 #ifdef __cplusplus
 }
 #endif

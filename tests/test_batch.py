@@ -1,0 +1,234 @@
+"""Batched point sets (ft_batch_*): every set of a batch must equal its own independent
+build_bvh + self_knn_query, bit for bit -- tree arrays, heights, neighbour indices and
+distances -- for uneven sizes including empty sets and sets of 1, 2 and 3 points.  The
+single-tree path is itself pinned to the oracle; a few sets are also checked against the
+oracle directly."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+import fasttree_b200 as ft  # noqa: E402
+from fasttree_b200 import datasets  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+from tests.gpu_util import assert_tree_equal, dist_bits, gen  # noqa: E402
+
+CASES = [
+    ("f32", "morton", False),
+    ("f64", "morton", False),
+    ("f32", "ph", False),
+    ("f64", "ph", False),
+    ("u32", "ph", False),
+    ("u32", "ph", True),
+]
+CODES = {"f32": O.F32, "f64": O.F64, "u32": O.U32, "morton": O.MORTON, "ph": O.PEANO_HILBERT}
+SIZES = [0, 300, 1, 2, 0, 3, 17, 1000, 257, 64, 4096, 5, 2000, 0]
+KINDS = ["uniform", "clustered", "degenerate"]
+
+
+def make_sets(coord, sizes, seed=7):
+    parts = [gen(KINDS[i % 3], int(n), CODES[coord], seed + i) for i, n in enumerate(sizes)]
+    x, y, z = (np.concatenate([p[d] for p in parts]) for d in range(3))
+    off = np.zeros(len(sizes) + 1, np.int64)
+    off[1:] = np.cumsum(sizes)
+    return x, y, z, off
+
+
+def single(ctx, xs, ys, zs, k, method=0, ids=None):
+    tree = ft.TreeSoA(ctx, len(xs))
+    ft.build_bvh(ctx, ft.particles(xs, ys, zs, ids), tree)
+    i, d = ft.self_knn_query(ctx, tree, k, max_k=max(32, k), method=method)
+    torch.cuda.synchronize()
+    return tree, i.cpu().numpy(), d.cpu().numpy()
+
+
+def rows(a, off, s):
+    return a[off[s]:off[s + 1]]
+
+
+@pytest.mark.parametrize("coord,sfc,periodic", CASES, ids=[f"{c}-{s}{'-per' if p else ''}" for c, s, p in CASES])
+def test_each_set_equals_its_own_calls(coord, sfc, periodic):
+    ctx = ft.Context(coord, sfc, periodic=periodic)
+    x, y, z, off = make_sets(coord, SIZES)
+    b = ft.BatchedSets(ctx, len(x), len(SIZES))
+    b.build(off, x, y, z)
+    b.check()
+    box, heights = b.set_info()
+    for k in (1, 16, 32):
+        for method in (0, 1):
+            bi, bd = b.self_knn(k, method=method)
+            torch.cuda.synchronize()
+            b.check()
+            bi, bd = bi.cpu().numpy(), bd.cpu().numpy()
+            for s, n in enumerate(SIZES):
+                if n == 0:
+                    continue
+                sl = slice(off[s], off[s + 1])
+                tree, si, sd = single(ctx, x[sl], y[sl], z[sl], k)
+                assert np.array_equal(rows(bi, off, s), si), (s, k, method)
+                assert np.array_equal(dist_bits(rows(bd, off, s)), dist_bits(sd)), (s, k, method)
+                if k == 16 and method == 0:
+                    view = b.tree(s)
+                    got, want = view.to_numpy(), tree.to_numpy()
+                    for name, a in want.items():
+                        g = got[name]
+                        assert np.array_equal(g.view(np.uint8), a.view(np.uint8)), (s, name)
+                    assert heights[s] == tree.height() == view.height()
+                    if ctx.is_float:
+                        want_box = ft.compute_bbox(ctx, x[sl], y[sl], z[sl])
+                        assert np.array_equal(box[s].view(np.uint8), want_box.view(np.uint8)), s
+
+
+@pytest.mark.parametrize("coord,sfc,periodic", [("f32", "morton", False), ("u32", "ph", True)])
+def test_sets_against_the_oracle(coord, sfc, periodic):
+    ctx = ft.Context(coord, sfc, periodic=periodic)
+    x, y, z, off = make_sets(coord, SIZES, seed=11)
+    b = ft.BatchedSets(ctx, len(x), len(SIZES))
+    b.build(off, x, y, z)
+    bi, bd = b.self_knn(32, method=1)
+    torch.cuda.synchronize()
+    b.check()
+    bi, bd = bi.cpu().numpy(), bd.cpu().numpy()
+    opts = O.Options(CODES[coord], CODES[sfc], periodic)
+    for s in (1, 2, 5, 7, 10, 12):
+        n = SIZES[s]
+        sl = slice(off[s], off[s + 1])
+        ot = O.build_bvh(opts, x[sl], y[sl], z[sl])
+        assert_tree_equal(b.tree(s).to_numpy(), ot, n)
+        oi, od = O.self_knn(opts, ot, 32)
+        assert np.array_equal(rows(bi, off, s), oi), s
+        assert np.array_equal(dist_bits(rows(bd, off, s)), dist_bits(od)), s
+
+
+def test_ids_ghosts_and_original_indices():
+    ctx = ft.Context("f64", "morton", return_orig_indices=True)
+    sizes = [500, 1, 0, 77, 1200]
+    x, y, z, off = make_sets("f64", sizes, seed=3)
+    rng = np.random.default_rng(5)
+    ids = rng.integers(0, 2**32, len(x), dtype=np.uint64).astype(np.uint32)
+    ghost = (rng.random(len(x)) < 0.2).astype(np.int8)
+    b = ft.BatchedSets(ctx, len(x), len(sizes))
+    b.build(off, x, y, z, id=ids, is_ghost=ghost)
+    bi, bd = b.self_knn(8, method=1, max_k=32)
+    torch.cuda.synchronize()
+    b.check()
+    bi, bd = bi.cpu().numpy(), bd.cpu().numpy()
+    for s, n in enumerate(sizes):
+        if n == 0:
+            continue
+        sl = slice(off[s], off[s + 1])
+        tree = ft.TreeSoA(ctx, n)
+        ft.build_bvh(ctx, ft.particles(x[sl], y[sl], z[sl], ids[sl], ghost[sl]), tree)
+        si, sd = ft.self_knn_query(ctx, tree, 8)
+        torch.cuda.synchronize()
+        got, want = b.tree(s).to_numpy(), tree.to_numpy()
+        for name in ("id", "is_ghost", "orig_idx"):
+            assert np.array_equal(got[name], want[name]), (s, name)
+        assert np.array_equal(rows(bi, off, s), si.cpu().numpy())
+        assert np.array_equal(dist_bits(rows(bd, off, s)), dist_bits(sd.cpu().numpy()))
+
+
+def test_large_k_takes_the_reference_traversal():
+    ctx = ft.Context("f32", "ph")
+    sizes = [3000, 2, 150, 0, 900]
+    x, y, z, off = make_sets("f32", sizes, seed=9)
+    b = ft.BatchedSets(ctx, len(x), len(sizes))
+    b.build(off, x, y, z)
+    for k, method in ((100, 1), (100, 0), (64, 1)):
+        bi, bd = b.self_knn(k, method=method, max_k=128)
+        torch.cuda.synchronize()
+        b.check()
+        bi, bd = bi.cpu().numpy(), bd.cpu().numpy()
+        for s, n in enumerate(sizes):
+            if n == 0:
+                continue
+            sl = slice(off[s], off[s + 1])
+            _, si, sd = single(ctx, x[sl], y[sl], z[sl], k)
+            assert np.array_equal(rows(bi, off, s), si), (s, k)
+            assert np.array_equal(dist_bits(rows(bd, off, s)), dist_bits(sd)), (s, k)
+
+
+def test_plummer_sets_fast_equals_plain_and_sampled_sets_equal_single_builds():
+    # the batched-sets workload's shape at 512 sets (log-normal sizes, Plummer spheres, f32 Morton)
+    sizes = datasets.batched_set_sizes(512, seed=4, median=2000.0, hi=60_000)
+    x, y, z, off = datasets.batched_sets(sizes=sizes, seed=4)
+    ctx = ft.Context("f32", "morton")
+    b = ft.BatchedSets(ctx, len(x), len(sizes))
+    b.build(off, x, y, z)
+    fi, fd = b.self_knn(32, method=1)
+    torch.cuda.synchronize()
+    st = b.query_stats()
+    pi, pd = b.self_knn(32, method=0)
+    torch.cuda.synchronize()
+    b.check()
+    assert torch.equal(fi, pi) and torch.equal(fd, pd)
+    assert st["replayed"] < len(x)
+    fi, fd = fi.cpu().numpy(), fd.cpu().numpy()
+    for s in np.random.default_rng(1).choice(len(sizes), 12, replace=False):
+        sl = slice(off[s], off[s + 1])
+        _, si, sd = single(ctx, x[sl], y[sl], z[sl], 32)
+        assert np.array_equal(rows(fi, off, s), si), s
+        assert np.array_equal(dist_bits(rows(fd, off, s)), dist_bits(sd)), s
+
+
+def test_graph_replay_follows_new_coordinates():
+    sizes = [700, 1, 3, 0, 2500, 40]
+    ctx = ft.Context("f32", "morton")
+    x, y, z, off = make_sets("f32", sizes, seed=21)
+    N, k = len(x), 32
+    dx, dy, dz = (torch.as_tensor(a, device="cuda") for a in (x, y, z))
+    doff = torch.as_tensor(off, device="cuda")
+    gi = torch.empty(N * k, dtype=torch.uint64, device="cuda")
+    gd = torch.empty(N * k, dtype=torch.float64, device="cuda")
+    b = ft.BatchedSets(ctx, N, len(sizes))
+    ref = ft.BatchedSets(ctx, N, len(sizes))
+    for rnd in range(3):
+        if rnd:
+            # new coordinates in the same buffers: the replayed graph must read them
+            x2, y2, z2, _ = make_sets("f32", sizes, seed=100 + rnd)
+            for d, a in zip((dx, dy, dz), (x2, y2, z2)):
+                d.copy_(torch.as_tensor(a, device="cuda"))
+        b.build_knn(doff, dx, dy, dz, k, gi, gd, method=1)
+        ref.build(doff, dx, dy, dz)
+        ri, rd = ref.self_knn(k, method=0)
+        torch.cuda.synchronize()
+        b.check()
+        assert torch.equal(gi.view(N, k), ri) and torch.equal(gd.view(N, k), rd), rnd
+
+
+def test_bad_offsets_are_reported_and_contained():
+    ctx = ft.Context("f32", "morton")
+    x, y, z, off = make_sets("f32", [100, 50, 80], seed=2)
+    b = ft.BatchedSets(ctx, len(x), 3)
+    for bad in (np.array([0, 100, 40, 230]), np.array([0, 100, 150, 200]), np.array([5, 100, 150, 230])):
+        b.build(bad, x, y, z)
+        b.self_knn(4)
+        with pytest.raises(ValueError):
+            b.check()
+    b.build(off, x, y, z)  # the batch stays usable
+    b.self_knn(4)
+    b.check()
+
+
+def test_rejections():
+    with pytest.raises(ValueError):
+        ft.BatchedSets(ft.Context("u64", "ph", periodic=True), 100, 2)
+    ctx = ft.Context("f32", "morton")
+    x, y, z, off = make_sets("f32", [10, 20], seed=1)
+    b = ft.BatchedSets(ctx, 30, 2)
+    with pytest.raises(ValueError):
+        b.self_knn(4)  # not built yet
+    with pytest.raises(ValueError):
+        ft.BatchedSets(ctx, 10, 2).build(off, x, y, z)  # more points than max_points
+    b.build(off, x, y, z)
+    with pytest.raises(ValueError):
+        b.self_knn(40)  # k > max_k
+    view = b.tree(1)
+    with pytest.raises(ValueError):
+        ft.build_bvh(ctx, ft.particles(x[:20], y[:20], z[:20]), view)
+    with pytest.raises(ValueError):
+        b.tree(5)
