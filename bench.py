@@ -42,7 +42,9 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1"])
+    p.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg4"])
+    p.add_argument("--no-batched", action="store_true", help="skip the batched-sets section of the default run")
+    p.add_argument("--sets", type=int, default=4096, help="batched sets: number of sets")
     p.add_argument("--n", type=int, default=0, help="override the point count (tests only)")
     p.add_argument("--k", type=int, default=32)
     p.add_argument("--method", default="fast", choices=["plain", "fast"],
@@ -67,6 +69,76 @@ def workload(args):
     x, y, z = datasets.uniform(n, seed=1)
     return dict(name="cfg1: 100K uniform float64, Morton, open", n=n, coord="f64", sfc="morton", periodic=False,
                 x=x, y=y, z=z, dtype="f64")
+
+
+def batched_workload(args):
+    """4096 independent Plummer spheres (scale 0.05) in float32, log-normal sizes (median 8000,
+    sigma 1.2, clipped to [256, 500000]), seed 4: about 50M points in total."""
+    from fasttree_b200 import datasets
+    sizes = datasets.batched_set_sizes(args.sets, seed=4)
+    x, y, z, off = datasets.batched_sets(sizes=sizes, seed=4)
+    return dict(name=f"cfg4: {args.sets} Plummer sets, float32, Morton, open, per-set boxes",
+                n=len(x), sets=len(sizes), x=x, y=y, z=z, off=off)
+
+
+def run_batched(args, dev, stream, timed_steps, warmup):
+    """Batched build + self-kNN (k=32, fast walk) as one CUDA graph, next to the same work
+    done eagerly and to a loop of single-set build_bvh + self_knn_query calls."""
+    import torch
+
+    import fasttree_b200 as ft
+    w = batched_workload(args)
+    N, S, k = w["n"], w["sets"], 32
+    ctx = ft.Context("f32", "morton", device=torch.device(dev).index or 0)
+    x, y, z = (torch.from_numpy(a).to(dev) for a in (w["x"], w["y"], w["z"]))
+    off = torch.from_numpy(w["off"]).to(dev)
+    idx = torch.empty(N * k, dtype=torch.uint64, device=dev)
+    dst = torch.empty(N * k, dtype=torch.float64, device=dev)
+    b = ft.BatchedSets(ctx, N, S)
+
+    def timed(fn, steps):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(steps):
+            fn()
+        g1.record(stream)
+        torch.cuda.synchronize()
+        return g0.elapsed_time(g1) / steps
+
+    graph_ms = timed(lambda: b.build_knn(off, x, y, z, k, idx, dst, method=1), timed_steps)
+    b.check()
+    stats = b.query_stats()
+    build_ms = timed(lambda: b.build(off, x, y, z), timed_steps)
+    fast_ms = timed(lambda: b.self_knn(k, method=1, results=idx, result_dists=dst), timed_steps)
+    plain_ms = timed(lambda: b.self_knn(k, method=0, results=idx, result_dists=dst), max(1, timed_steps // 2))
+    b.check()
+    # the same sets one by one through the single-tree API (the non-batched way)
+    offs = w["off"]
+    tree = ft.TreeSoA(ctx, int(np.diff(offs).max()))
+    li = torch.empty(int(np.diff(offs).max()) * k, dtype=torch.uint64, device=dev)
+    ld = torch.empty_like(li, dtype=torch.float64)
+
+    def loop():
+        for s in range(S):
+            a, e = int(offs[s]), int(offs[s + 1])
+            ft.build_bvh(ctx, ft.particles(x[a:e], y[a:e], z[a:e]), tree)
+            ft.self_knn_query(ctx, tree, k, li[:(e - a) * k], ld[:(e - a) * k], method=1)
+    t0 = time.perf_counter()
+    loop()
+    torch.cuda.synchronize()
+    loop_ms = (time.perf_counter() - t0) * 1e3
+    del b, tree
+    return {"workload": w["name"], "n_sets": S, "n_points": N, "k": k,
+            "graph_build_plus_query_ms": graph_ms, "value": N / (graph_ms / 1e3), "unit": "queries/s",
+            "build_ms": build_ms, "query_fast_ms": fast_ms, "query_plain_ms": plain_ms,
+            "query_fast_qps": N / (fast_ms / 1e3), "query_plain_qps": N / (plain_ms / 1e3),
+            "per_set_loop_ms": loop_ms, "per_set_loop_qps": N / (loop_ms / 1e3),
+            "replayed": stats["replayed"],
+            "note": "graph = ft_batch_build_knn (build + fast self-kNN, one CUDA graph); per-set loop = "
+                    "build_bvh + self_knn_query(method=1) per set through the single-tree API (wall clock)"}
 
 
 def measured_peaks():
@@ -196,6 +268,13 @@ def run_ours(args):
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    if args.workload == "cfg4":
+        r = run_batched(args, f"cuda:{local}", torch.cuda.current_stream(), args.steps, args.warmup)
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(r), flush=True)
+        return
     w = workload(args)
     n, k = w["n"], args.k
     ctx = ft.Context(w["coord"], w["sfc"], periodic=w["periodic"], device=local)
@@ -321,6 +400,13 @@ def run_ours(args):
                 "traffic": traffic, "peak_source": peak_kind, "algorithmic_bytes": alg, "kernel": kname,
                 "note": "latency/ALU bound tree walk; algorithmic bytes = tree (2N-1)*6*s_c + (N-1)*8 + output 16*N*k"}
 
+    batched = None
+    if world == 1 and not args.no_batched and args.workload == "cfg2":
+        del idx, dst
+        torch.cuda.empty_cache()
+        batched = run_batched(args, dev, stream, 3, 2)
+        torch.cuda.empty_cache()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         del tree
@@ -336,7 +422,7 @@ def run_ours(args):
                "config": {"workload": w["name"], "n_points": n, "k": k, "exclude_self": True,
                           "method": args.method, "parallelism": f"replicas x{world}",
                           "l2": "inputs larger than L2: tree records + boxes ~2.3 GB, output 5.1 GB"},
-               "plain": plain, "build_ms": build_ms, "tree_height": height, "query_stats": stats,
+               "plain": plain, "batched": batched, "build_ms": build_ms, "tree_height": height, "query_stats": stats,
                "e2e": e2e, "gpu_launches": args.steps * (2 if method == 1 else 1),
                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(out), flush=True)
