@@ -20,9 +20,12 @@ EXPORTED = (
     "ft_check_device_status",
     "ft_tree_create", "ft_tree_ensure", "ft_tree_destroy", "ft_compute_bbox", "ft_sfc_encode",
     "ft_build_bvh", "ft_build_tree", "ft_self_knn", "ft_knn", "ft_range", "ft_tree_height",
-    "ft_self_knn_noalloc",
+    "ft_self_knn_noalloc", "ft_self_knn_bounded",
     "ft_batch_create", "ft_batch_destroy", "ft_batch_build", "ft_batch_self_knn", "ft_batch_build_knn",
     "ft_batch_tree", "ft_batch_set_info", "ft_batch_query_stats",
+    "ft_bound_model_create", "ft_bound_model_destroy", "ft_bound_model_get_params", "ft_bound_model_set_params",
+    "ft_bound_model_set_norm", "ft_bound_features", "ft_bound_targets", "ft_bound_model_gradient",
+    "ft_bound_model_fit", "ft_bound_model_predict", "ft_self_knn_learned",
 )
 
 
@@ -72,6 +75,8 @@ _SIGS = {
     "ft_build_tree": [_vp, ctypes.POINTER(FtTree), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _st],
     "ft_self_knn": [_vp, ctypes.POINTER(FtTree), _vp, _sz, _i, _i, _vp, _vp, ctypes.POINTER(FtQueryOptions), _st],
     "ft_self_knn_noalloc": [_vp, ctypes.POINTER(FtTree), _vp, _sz, _i, _i, _vp, _vp, _st],
+    "ft_self_knn_bounded": [_vp, ctypes.POINTER(FtTree), _vp, _sz, _i, _i, _vp, _vp, _vp,
+                            ctypes.POINTER(FtQueryOptions), _st],
     "ft_knn": [_vp, ctypes.POINTER(FtTree), _vp, _vp, _vp, _sz, _i, _vp, _vp, ctypes.POINTER(FtQueryOptions), _st],
     "ft_range": [_vp, ctypes.POINTER(FtTree), _vp, _vp, _vp, _vp, _vp, _sz, _vp, _vp, _i, _st],
     "ft_batch_create": [_vp, _sz, _sz, ctypes.POINTER(_vp)],
@@ -83,6 +88,18 @@ _SIGS = {
     "ft_batch_tree": [_vp, _vp, _sz, ctypes.POINTER(FtTree), _st],
     "ft_batch_set_info": [_vp, _vp, _vp, _vp, _st],
     "ft_batch_query_stats": [_vp, _vp, ctypes.POINTER(FtQueryStats)],
+    "ft_bound_model_create": [_vp, ctypes.c_uint64, ctypes.POINTER(_vp)],
+    "ft_bound_model_destroy": [_vp, _vp],
+    "ft_bound_model_get_params": [_vp, _vp, _vp],
+    "ft_bound_model_set_params": [_vp, _vp, _vp],
+    "ft_bound_model_set_norm": [_vp, _vp, _vp, _vp, ctypes.c_float, ctypes.c_float],
+    "ft_bound_features": [_vp, ctypes.POINTER(FtTree), _vp, _sz, _i, _vp, _st],
+    "ft_bound_targets": [_vp, _vp, _vp, _sz, _i, _vp, _st],
+    "ft_bound_model_gradient": [_vp, _vp, _vp, _vp, _sz, _vp, _vp, _st],
+    "ft_bound_model_fit": [_vp, _vp, _vp, _vp, _sz, _i, _i, ctypes.c_float, ctypes.c_uint64, _vp, _st],
+    "ft_bound_model_predict": [_vp, _vp, _vp, _sz, ctypes.c_float, _vp, _vp, _st],
+    "ft_self_knn_learned": [_vp, ctypes.POINTER(FtTree), _vp, _vp, _sz, _i, _i, ctypes.c_float, _vp, _vp,
+                            ctypes.POINTER(FtQueryOptions), _st],
 }
 
 

@@ -202,6 +202,10 @@ struct ft_batch {
     ft::BatchImpl *impl;
 };
 
+struct ft_bound_model {
+    ft::BoundModel *impl;
+};
+
 extern "C" {
 
 const char *ft_last_error(void) { return ft::g_last_error.c_str(); }
@@ -236,6 +240,8 @@ ft_status ft_context_destroy(ft_context *ctx) {
         if (ctx->status) cudaFree(ctx->status);
         if (ctx->replay_ranks) cudaFree(ctx->replay_ranks);
         if (ctx->replay_rows) cudaFree(ctx->replay_rows);
+        if (ctx->learned_feats) cudaFree(ctx->learned_feats);
+        if (ctx->learned_bound) cudaFree(ctx->learned_bound);
     }
     delete ctx;
     return FT_OK;
@@ -485,6 +491,22 @@ ft_status ft_self_knn(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_
     FT_API_END
 }
 
+ft_status ft_self_knn_bounded(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_ids, size_t num, int k,
+                              int exclude_self, const void *bound, uint64_t *idx_out, void *dist_out,
+                              const ft_query_options *qopts, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree, "null argument");
+    ft_query_options q{};
+    if (qopts) q = *qopts;
+    if (!leaf_ids) num = tree->num_leaves;
+    if (num > 0 && k > 0 && tree->num_leaves > 0) need(idx_out && dist_out && bound, "null array argument");
+    need_device(bound, "bound");
+    DeviceGuard g(ctx->device);
+    ft::self_knn(*ctx, *tree, leaf_ids, num, k, exclude_self != 0, idx_out, dist_out, q, (cudaStream_t)stream,
+                 bound);
+    FT_API_END
+}
+
 // Self-kNN for callers that cannot have device memory allocated for them (see
 // fast_self_knn_noalloc in ft_fast.cu): the fast walk's scratch is a fixed static array.
 ft_status ft_self_knn_noalloc(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_ids, size_t num, int k,
@@ -560,6 +582,139 @@ ft_status ft_range(ft_context *ctx, const ft_tree *tree, const void *qx, const v
     sr.copy_back();
     sc.copy_back();
     check_device_status(ctx->status, st);
+    FT_API_END
+}
+
+// ---------------------------------------------------------------------------------------
+// Learned radius bound (ft_learned.cu)
+// ---------------------------------------------------------------------------------------
+ft_status ft_bound_model_create(ft_context *ctx, uint64_t seed, ft_bound_model **out) {
+    FT_API_BEGIN
+    need(ctx && out, "null argument");
+    DeviceGuard     g(ctx->device);
+    ft::BoundModel *b = ft::bound_model_create(*ctx, seed);
+    ft_bound_model *h = new (std::nothrow) ft_bound_model{b};
+    if (!h) {
+        ft::bound_model_free(b);
+        throw std::bad_alloc();
+    }
+    *out = h;
+    FT_API_END
+}
+
+ft_status ft_bound_model_destroy(ft_context *ctx, ft_bound_model *model) {
+    FT_API_BEGIN
+    if (!model) return FT_OK;
+    need(ctx != nullptr, "null context");
+    DeviceGuard g(ctx->device);
+    ft::bound_model_free(model->impl);
+    delete model;
+    FT_API_END
+}
+
+ft_status ft_bound_model_get_params(ft_context *ctx, ft_bound_model *model, float *params_out) {
+    FT_API_BEGIN
+    need(ctx && model && params_out, "null argument");
+    DeviceGuard g(ctx->device);
+    ft::bound_model_get_params(*model->impl, params_out);
+    FT_API_END
+}
+
+ft_status ft_bound_model_set_params(ft_context *ctx, ft_bound_model *model, const float *params) {
+    FT_API_BEGIN
+    need(ctx && model && params, "null argument");
+    DeviceGuard g(ctx->device);
+    ft::bound_model_set_params(*model->impl, params, nullptr);
+    FT_API_END
+}
+
+ft_status ft_bound_model_set_norm(ft_context *ctx, ft_bound_model *model, const float *feature_mean,
+                                  const float *feature_std, float target_mean, float target_std) {
+    FT_API_BEGIN
+    need(ctx && model && feature_mean && feature_std, "null argument");
+    DeviceGuard g(ctx->device);
+    ft::bound_model_set_norm(*model->impl, feature_mean, feature_std, target_mean, target_std);
+    FT_API_END
+}
+
+ft_status ft_bound_features(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_ids, size_t num, int k,
+                            float *features_out, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree, "null argument");
+    if (!leaf_ids) num = tree->num_leaves;
+    need(num <= (size_t)INT32_MAX, "too many queries");
+    if (num > 0) need(features_out != nullptr, "null output array");
+    need_device(features_out, "features_out");
+    DeviceGuard g(ctx->device);
+    ft::bound_features(*ctx, *tree, leaf_ids, num, k, features_out, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_bound_targets(ft_context *ctx, const uint64_t *idx, const void *dist, size_t num, int k,
+                           float *targets_out, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx != nullptr, "null context");
+    need(k > 0, "k must be positive");
+    need(num <= (size_t)INT32_MAX, "too many rows");
+    if (num > 0) need(idx && dist && targets_out, "null array argument");
+    DeviceGuard g(ctx->device);
+    ft::bound_targets(*ctx, idx, dist, num, k, targets_out, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_bound_model_gradient(ft_context *ctx, ft_bound_model *model, const float *features,
+                                  const float *targets, size_t n, float *grad_out, float *loss_out,
+                                  ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && model && features && targets, "null argument");
+    need(n >= 1 && n <= (size_t)(1 << 24), "n must be in [1, 2^24]");
+    DeviceGuard g(ctx->device);
+    ft::bound_model_gradient(*model->impl, features, targets, (int)n, grad_out, loss_out, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_bound_model_fit(ft_context *ctx, ft_bound_model *model, const float *features, const float *targets,
+                             size_t n, int steps, int batch, float lr, uint64_t seed, float *loss_out,
+                             ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && model && features && targets, "null argument");
+    need(n >= 1 && n <= (size_t)INT32_MAX, "n must be in [1, 2^31)");
+    need(batch >= 1 && batch <= (1 << 20), "batch must be in [1, 2^20]");
+    need(steps >= 0, "negative step count");
+    DeviceGuard g(ctx->device);
+    ft::bound_model_fit(*model->impl, features, targets, (int)n, steps, batch, lr, seed, loss_out,
+                        (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_bound_model_predict(ft_context *ctx, ft_bound_model *model, const float *features, size_t n,
+                                 float inflation, float *pred_out, void *bound_out, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && model, "null argument");
+    need(n <= (size_t)INT32_MAX, "too many rows");
+    if (n > 0) need(features != nullptr, "null features");
+    DeviceGuard g(ctx->device);
+    ft::bound_model_predict(*ctx, *model->impl, features, n, inflation, pred_out, bound_out, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_self_knn_learned(ft_context *ctx, const ft_tree *tree, ft_bound_model *model, const int32_t *leaf_ids,
+                              size_t num, int k, int exclude_self, float inflation, uint64_t *idx_out,
+                              void *dist_out, const ft_query_options *qopts, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree && model, "null argument");
+    ft_query_options q{};
+    if (qopts) q = *qopts;
+    if (!leaf_ids) num = tree->num_leaves;
+    need(num <= (size_t)INT32_MAX, "too many queries");
+    const int max_k = q.max_k > 0 ? q.max_k : (leaf_ids ? 256 : 32);
+    if (k > max_k)
+        fail(FT_ERR_INVALID_ARGUMENT,
+             "k exceeds _MAX_K_ template parameter. Instantiate self_knn_query with larger _MAX_K_.");
+    if (num > 0 && k > 0 && tree->num_leaves > 0) need(idx_out && dist_out, "null output array");
+    DeviceGuard g(ctx->device);
+    ft::self_knn_learned(*ctx, *tree, *model->impl, leaf_ids, num, k, exclude_self != 0, inflation, idx_out,
+                         dist_out, q, (cudaStream_t)stream);
     FT_API_END
 }
 

@@ -80,6 +80,9 @@ struct Context {
     int32_t       *replay_rows  = nullptr;
     size_t         replay_cap   = 0;
     bool           last_fast    = false; // the last self-kNN call used the fast traversal
+    float         *learned_feats = nullptr; // learned-bound scratch: features and bounds
+    void          *learned_bound = nullptr;
+    size_t         learned_cap   = 0;
 };
 
 // ---- fast self-kNN (ft_fast.cu) ----
@@ -129,8 +132,10 @@ void   ensure_scratch(TreeImpl &impl, const ft_options &o, size_t n);
 void   free_scratch(TreeImpl &impl);
 
 // ---- queries (ft_query.cu) ----
+// bound: optional per-query pruning bound (device, dist units); it selects the fast walk.
 void self_knn(Context &ctx, const ft_tree &tree, const int32_t *leaf_ids, size_t num, int k,
-              bool exclude_self, uint64_t *idx, void *dist, const ft_query_options &q, cudaStream_t st);
+              bool exclude_self, uint64_t *idx, void *dist, const ft_query_options &q, cudaStream_t st,
+              const void *bound = nullptr);
 void knn(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz, size_t nq,
          int k, int max_k, uint64_t *idx, void *dist, const ft_query_options &q, cudaStream_t st);
 void range(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz,
@@ -155,5 +160,26 @@ void batch_build_query_graph(Context &ctx, BatchImpl &b, const long long *set_of
 void batch_tree_view(Context &ctx, BatchImpl &b, size_t set, ft_tree &out, cudaStream_t st);
 void batch_set_info(Context &ctx, BatchImpl &b, void *bbox_out, uint8_t *height_out, cudaStream_t st);
 void batch_stats(BatchImpl &b, ft_query_stats &out);
+
+// ---- learned radius bound (ft_learned.cu) ----
+struct BoundModel;
+BoundModel *bound_model_create(Context &ctx, unsigned long long seed);
+void        bound_model_free(BoundModel *b);
+void        bound_model_get_params(BoundModel &b, float *host);
+void        bound_model_set_params(BoundModel &b, const float *host, cudaStream_t st);
+void        bound_model_set_norm(BoundModel &b, const float *mean12, const float *std12, float t_mean, float t_std);
+void        bound_features(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, float *out,
+                           cudaStream_t st);
+void        bound_targets(Context &ctx, const uint64_t *idx, const void *dist, size_t num, int k, float *out,
+                          cudaStream_t st);
+void        bound_model_gradient(BoundModel &b, const float *feats, const float *targets, int n, float *grad_host,
+                                 float *loss_host, cudaStream_t st);
+void        bound_model_fit(BoundModel &b, const float *feats, const float *targets, int n, int steps, int batch,
+                            float lr, unsigned long long seed, float *loss_host, cudaStream_t st);
+void        bound_model_predict(Context &ctx, BoundModel &b, const float *feats, size_t n, float inflation,
+                                float *pred, void *bound, cudaStream_t st);
+void        self_knn_learned(Context &ctx, const ft_tree &tr, BoundModel &b, const int32_t *leaf_ids, size_t num,
+                             int k, bool exclude_self, float inflation, uint64_t *idx, void *dist,
+                             const ft_query_options &q, cudaStream_t st);
 
 } // namespace ft

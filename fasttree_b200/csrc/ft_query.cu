@@ -509,7 +509,7 @@ static void launch_exact(const ft_options &o, const ft_tree &tr, const void *qx,
 static constexpr int kMaxExactK = 512;
 
 void self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, bool excl, uint64_t *idx,
-              void *dist, const ft_query_options &qo, cudaStream_t st) {
+              void *dist, const ft_query_options &qo, cudaStream_t st, const void *bound) {
     int max_k = qo.max_k > 0 ? qo.max_k : (leaf_ids ? 256 : 32);
     if (k > max_k)
         fail(FT_ERR_INVALID_ARGUMENT,
@@ -520,8 +520,8 @@ void self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t n
     ctx.stats.queries  = (int64_t)num;
     ctx.stats.replayed = 0;
     ctx.last_fast      = false;
-    if (qo.method == 1 &&
-        fast_self_knn(ctx, tr, leaf_ids, num, k, excl, idx, dist, nullptr, qo.reserved[0], qo.reserved[1], st)) {
+    if ((qo.method == 1 || bound) &&
+        fast_self_knn(ctx, tr, leaf_ids, num, k, excl, idx, dist, bound, qo.reserved[0], qo.reserved[1], st)) {
         ctx.last_fast = true;
         return;
     }

@@ -356,6 +356,20 @@ def self_knn_query(ctx: Context, tree: TreeSoA, k: int, results=None, result_dis
     return results.view(n, k) if n * k else results, result_dists.view(n, k) if n * k else result_dists
 
 
+def self_knn_query_bounded(ctx: Context, tree: TreeSoA, k: int, bound, results=None, result_dists=None,
+                           exclude_self=True, leaf_ids=None, max_k: int = 32, stream=None, half_window: int = 0):
+    """self_knn_query with a per-query pruning bound (device tensor of dist_t, in the units of
+    the returned distances).  Output equals self_knn_query's for any bound; see
+    ft_self_knn_bounded."""
+    num = tree.num_leaves if leaf_ids is None else len(leaf_ids)
+    if results is None:
+        results, result_dists = _alloc_knn_out(ctx, num, k)
+    _call(lib().ft_self_knn_bounded(ctx.handle, tree.c, _ptr(leaf_ids), num, int(k), int(bool(exclude_self)),
+                                    _ptr(bound), _ptr(results), _ptr(result_dists),
+                                    ctypes.byref(_qopts(max_k, 1, half_window)), _stream_handle(stream)))
+    return results.view(num, k) if num * k else results, result_dists.view(num, k) if num * k else result_dists
+
+
 def self_knn_query_subset(ctx: Context, tree: TreeSoA, leaf_ids, k: int, results=None, result_dists=None,
                           exclude_self=True, max_k: int = 256, method: int = 0, stream=None):
     """self_knn_query_subset<MAXK> (src/hlbvh.hpp:1956-1983); leaf_ids is a device int32 tensor."""

@@ -170,6 +170,17 @@ ft_status ft_self_knn(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_
 ft_status ft_self_knn_noalloc(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_ids, size_t num,
                               int k, int exclude_self, uint64_t *idx_out, void *dist_out, ft_stream_t stream);
 
+/* Self-kNN with a per-query pruning bound: the hook of the learned radius bound.  No
+ * counterpart in the reference.  bound: device, one value per query in dist_out's units
+ * (the squared distance the query returns).  The fast walk prunes every node beyond the
+ * bound; a query that ends with its k-th distance above its bound, or with fewer than k
+ * points, is rerun by the reference traversal, so the output equals ft_self_knn's for any
+ * bound (a good bound only saves work).  k <= 64 and tree height <= 62 use the bound; other
+ * calls take the reference traversal.  Asynchronous. */
+ft_status ft_self_knn_bounded(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_ids, size_t num,
+                              int k, int exclude_self, const void *bound, uint64_t *idx_out, void *dist_out,
+                              const ft_query_options *qopts, ft_stream_t stream);
+
 /* knn_query<MAXK> (src/hlbvh.hpp:1405-1472).  qx/qy/qz, idx_out, dist_out: host or device.
  * Default max_k 256.  Blocking. */
 ft_status ft_knn(ft_context *ctx, const ft_tree *tree, const void *qx, const void *qy,
@@ -188,6 +199,61 @@ ft_status ft_range(ft_context *ctx, const ft_tree *tree, const void *qx, const v
  * drops children below depth 61 (src/hlbvh.hpp:1152, 1618); trees of height <= 62 never
  * reach that guard. */
 ft_status ft_tree_height(ft_context *ctx, const ft_tree *tree, int *height_out);
+
+/* ---------------------------------------------------------------------------------- */
+/* Learned radius bound.  No counterpart in the reference.  A 12 -> 64 -> 64 -> 1 GELU MLP  */
+/* (bfloat16 weights and activations, fp32 accumulation) predicts each self query's       */
+/* log2 k-th-neighbour distance from 12 tree features; the prediction times an inflation   */
+/* becomes the query's bound in ft_self_knn_bounded, so results stay identical to         */
+/* ft_self_knn's.  The network is trained on the GPU (forward, backward and Adam kernels)  */
+/* on targets taken from exact self-kNN results.  k <= 64.                                 */
+/* ---------------------------------------------------------------------------------- */
+#define FT_BOUND_FEATURES     12   /* features per query (float)                         */
+#define FT_BOUND_MODEL_PARAMS 5057 /* W1[64][12] b1[64] W2[64][64] b2[64] w3[64] b3        */
+
+typedef struct ft_bound_model ft_bound_model;
+
+/* New network with seeded U(-1/sqrt(fan_in), 1/sqrt(fan_in)) weights and identity
+ * standardisation. */
+ft_status ft_bound_model_create(ft_context *ctx, uint64_t seed, ft_bound_model **out);
+ft_status ft_bound_model_destroy(ft_context *ctx, ft_bound_model *model);
+/* fp32 master weights in the layout above (host arrays of FT_BOUND_MODEL_PARAMS floats);
+ * set also resets the Adam state. */
+ft_status ft_bound_model_get_params(ft_context *ctx, ft_bound_model *model, float *params_out);
+ft_status ft_bound_model_set_params(ft_context *ctx, ft_bound_model *model, const float *params);
+/* Input standardisation (host: 12 means, 12 standard deviations) and the target's mean and
+ * standard deviation (the network predicts the standardised target). */
+ft_status ft_bound_model_set_norm(ft_context *ctx, ft_bound_model *model, const float *feature_mean,
+                                  const float *feature_std, float target_mean, float target_std);
+
+/* The 12 features of self queries (leaf_ids NULL: every leaf) of a tree built by
+ * ft_build_bvh / ft_build_tree.  features_out: device, num x 12 floats.  Asynchronous. */
+ft_status ft_bound_features(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_ids, size_t num, int k,
+                            float *features_out, ft_stream_t stream);
+/* Training targets from self-kNN results (device idx / dist, num x k): 0.5 log2 of each
+ * row's k-th distance, NaN for rows with fewer than k neighbours.  Asynchronous. */
+ft_status ft_bound_targets(ft_context *ctx, const uint64_t *idx, const void *dist, size_t num, int k,
+                           float *targets_out, ft_stream_t stream);
+/* Gradient (host, FT_BOUND_MODEL_PARAMS floats) and loss (host, 1 float) of the mean squared
+ * error over all n samples, without an update.  features / targets: device.  Blocking. */
+ft_status ft_bound_model_gradient(ft_context *ctx, ft_bound_model *model, const float *features,
+                                  const float *targets, size_t n, float *grad_out, float *loss_out,
+                                  ft_stream_t stream);
+/* `steps` Adam steps (lr; beta 0.9 / 0.999) on minibatches of `batch` rows drawn from [0, n)
+ * with a seeded hash.  loss_out: NULL or host, one loss per step (then blocking).  Targets
+ * must be finite. */
+ft_status ft_bound_model_fit(ft_context *ctx, ft_bound_model *model, const float *features, const float *targets,
+                             size_t n, int steps, int batch, float lr, uint64_t seed, float *loss_out,
+                             ft_stream_t stream);
+/* Predicted log2 k-th distance (pred_out: NULL or device floats) and bound = (inflation x
+ * 2^pred)^2 in distance units (bound_out: NULL or device dist values).  Asynchronous. */
+ft_status ft_bound_model_predict(ft_context *ctx, ft_bound_model *model, const float *features, size_t n,
+                                 float inflation, float *pred_out, void *bound_out, ft_stream_t stream);
+/* Features -> bound -> ft_self_knn_bounded in one call (scratch kept in the context).
+ * Same output as ft_self_knn.  Asynchronous. */
+ft_status ft_self_knn_learned(ft_context *ctx, const ft_tree *tree, ft_bound_model *model, const int32_t *leaf_ids,
+                              size_t num, int k, int exclude_self, float inflation, uint64_t *idx_out,
+                              void *dist_out, const ft_query_options *qopts, ft_stream_t stream);
 
 /* ---------------------------------------------------------------------------------- */
 /* Batched point sets.  No counterpart in the reference: its callers loop over sets and   */
