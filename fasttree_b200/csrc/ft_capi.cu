@@ -240,6 +240,8 @@ ft_status ft_context_destroy(ft_context *ctx) {
         if (ctx->status) cudaFree(ctx->status);
         if (ctx->replay_ranks) cudaFree(ctx->replay_ranks);
         if (ctx->replay_rows) cudaFree(ctx->replay_rows);
+        if (ctx->seed_ranks) cudaFree(ctx->seed_ranks);
+        ft::free_query_sort(*ctx);
         if (ctx->learned_feats) cudaFree(ctx->learned_feats);
         if (ctx->learned_bound) cudaFree(ctx->learned_bound);
     }
@@ -416,8 +418,10 @@ ft_status ft_build_bvh(ft_context *ctx, const void *x, const void *y, const void
     TreeImpl &impl     = *(TreeImpl *)tree->impl;
     impl.height_root   = -1;
     impl.clean42       = false;
+    impl.own_keys      = false;
     ft::build_bvh(*ctx, *tree, sx.dev, sy.dev, sz.dev, n, (const uint32_t *)sid.dev, (const int8_t *)sgh.dev, bbox6,
                   sk.dev, st);
+    impl.own_keys = keys == nullptr; // the sorted keys are this library's encoding of bbox
     if (keys) sk.copy_back();
     uint64_t box[6] = {0, 0, 0, 0, 0, 0};
     if (ctx->opts.coord_type == FT_COORD_U64)
@@ -462,6 +466,7 @@ ft_status ft_build_tree(ft_context *ctx, ft_tree *tree, const void *sorted_keys,
     tree->num_internal = n - 1;
     TreeImpl &impl     = *(TreeImpl *)tree->impl;
     impl.clean42       = false; // caller leaf arrays: the general periodic distance form
+    impl.own_keys      = false;
     impl.height_root   = -1;
     build_tree_from_keys(*ctx, *tree, sk.dev, sx.dev, sy.dev, sz.dev, (const uint32_t *)sid.dev,
                          (const int8_t *)sgh.dev, (const int32_t *)sor.dev, st);

@@ -22,6 +22,7 @@
 #include <mutex>
 #include <string>
 
+#include "ft_build_dev.cuh"
 #include "ft_common.cuh"
 #include "ft_internal.h"
 
@@ -33,7 +34,9 @@ static constexpr int kFastThreads = 32 * kFastWarps;
 
 template <class T, int PER, int KC, int VAR>
 __global__ void __launch_bounds__(kFastThreads)
-    fast_self_knn_kernel(TreeDev<T> t_all, BatchDev bt, const int32_t *__restrict__ leaf_ids, int num, int k,
+    fast_self_knn_kernel(TreeDev<T> t_all, BatchDev bt, const T *__restrict__ qx, const T *__restrict__ qy,
+                         const T *__restrict__ qz, const uint32_t *__restrict__ order,
+                         const int32_t *__restrict__ leaf_ids, int num, int k,
                          int half_window, int exclude_self, int ret_orig,
                          const typename Coord<T>::dist_t *__restrict__ bound,
                          unsigned long long *__restrict__ out_idx, typename Coord<T>::dist_t *__restrict__ out_dist,
@@ -49,8 +52,10 @@ __global__ void __launch_bounds__(kFastThreads)
     const unsigned FULL = 0xffffffffu;
     const int      qbase = (blockIdx.x * kFastWarps + warp) * 32;
     if (qbase >= num) return; // warp-uniform
-    const int q      = qbase + lane;
-    bool      active = q < num;
+    // External query points are walked in the order `order` (sorted by SFC rank, so a warp
+    // takes neighbouring queries); q is the output row.
+    const int q      = (qx && order && qbase + lane < num) ? (int)order[qbase + lane] : qbase + lane;
+    bool      active = qbase + lane < num;
     // Batched sets: each lane walks the tree of the set its query belongs to (rank local to
     // the set, output row global); a set taller than 62 goes straight to the replay.
     TreeDev<T> t            = t_all;
@@ -71,7 +76,10 @@ __global__ void __launch_bounds__(kFastThreads)
 #define HD(s) hd[(s) * kFastThreads + tid]
 #define HI(s) hix[(s) * kFastThreads + tid]
 
-    if (active && (rank < 0 || rank >= n)) {
+    // External query points (knn_query): leaf_ids holds each point's SFC rank, the centre of
+    // its seeding window (-1: no window); there is no self leaf.
+    const bool ext = qx != nullptr;
+    if (!ext && active && (rank < 0 || rank >= n)) {
         atomicOr(status, STATUS_BAD_INPUT);
         for (int i = 0; i < k; ++i) {
             out_idx[(size_t)q * k + i]  = ~0ull;
@@ -80,9 +88,13 @@ __global__ void __launch_bounds__(kFastThreads)
         active = false;
         rank   = 0;
     }
-    const int slot      = rank + n - 1;
-    const T   px        = t.min_x[slot], py = t.min_y[slot], pz = t.min_z[slot];
-    const int self_leaf = exclude_self ? slot : -1;
+    const bool seeded   = !ext || rank >= 0;
+    if (ext) rank = min(max(rank, 0), n - 1);
+    const int  slot      = rank + n - 1;
+    const T    px        = ext ? qx[active ? q : 0] : t.min_x[slot];
+    const T    py        = ext ? qy[active ? q : 0] : t.min_y[slot];
+    const T    pz        = ext ? qz[active ? q : 0] : t.min_z[slot];
+    const int  self_leaf = (exclude_self && !ext) ? slot : -1;
     const D   B         = (bound && active) ? bound[q] : dist_heap_max<D>();
 
     int  count = 0;
@@ -140,7 +152,7 @@ __global__ void __launch_bounds__(kFastThreads)
     };
 
     // ---- 1. seed from the SFC window ----
-    const int W  = min(n, 2 * half_window + 1);
+    const int W  = seeded ? min(n, 2 * half_window + 1) : 0;
     const int w0 = active ? max(0, min(rank - half_window, n - W)) : 0;
     const int w1 = active ? w0 + W - 1 : -1;
     for (int j = 0; j < W; ++j) {
@@ -370,19 +382,26 @@ __global__ void __launch_bounds__(kFastThreads)
         }
     }
     if ((active && flag) || force_replay) {
-        uint32_t at      = atomicAdd(replay_count, 1u);
-        replay_ranks[at] = rank;
-        replay_rows[at]  = q;
+        uint32_t at = atomicAdd(replay_count, 1u);
+        if (!ext) replay_ranks[at] = rank;
+        replay_rows[at] = q;
     }
 #undef HD
 #undef HI
 }
 
 // -----------------------------------------------------------------------------------------
+// External query points: qx / qy / qz (else self queries) with leaf_ids = their seed ranks.
+struct ExtQueries {
+    const void     *x = nullptr, *y = nullptr, *z = nullptr;
+    const uint32_t *order = nullptr; // walk order (null: input order)
+};
+
 template <class T, int PER, int KC>
-static void launch_fast_t(const TreeDev<T> &tv, const BatchDev &bt, const int32_t *leaf_ids, int num, int k, int half,
-                          bool excl, bool ro, const void *bound, uint64_t *idx, void *dist, int32_t *rr, int32_t *rw,
-                          uint32_t *rc, uint32_t *status, int variant, unsigned long long *visits, cudaStream_t st) {
+static void launch_fast_t(const TreeDev<T> &tv, const BatchDev &bt, const ExtQueries &eq, const int32_t *leaf_ids,
+                          int num, int k, int half, bool excl, bool ro, const void *bound, uint64_t *idx, void *dist,
+                          int32_t *rr, int32_t *rw, uint32_t *rc, uint32_t *status, int variant,
+                          unsigned long long *visits, cudaStream_t st) {
     using D     = typename Coord<T>::dist_t;
     size_t smem = (size_t)KC * kFastThreads * (sizeof(D) + 4);
     auto   fn   = variant == 0 ? fast_self_knn_kernel<T, PER, KC, 0>
@@ -390,7 +409,8 @@ static void launch_fast_t(const TreeDev<T> &tv, const BatchDev &bt, const int32_
                                  : fast_self_knn_kernel<T, PER, KC, 2>;
     FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int blocks = (num + kFastThreads - 1) / kFastThreads;
-    fn<<<blocks, kFastThreads, smem, st>>>(tv, bt, leaf_ids, num, k, half, excl ? 1 : 0, ro ? 1 : 0,
+    fn<<<blocks, kFastThreads, smem, st>>>(tv, bt, (const T *)eq.x, (const T *)eq.y, (const T *)eq.z, eq.order,
+                                           leaf_ids, num, k, half, excl ? 1 : 0, ro ? 1 : 0,
                                            (const D *)bound, (unsigned long long *)idx, (D *)dist, rr, rw, rc,
                                            status, visits);
     FT_CUDA(cudaGetLastError());
@@ -401,24 +421,73 @@ template <class T>
 static void launch_fast_view(const TreeDev<T> &tv, const BatchDev &bt, int met, bool ro, const int32_t *leaf_ids,
                              int num, int k, int half, bool excl, const void *bound, uint64_t *idx, void *dist,
                              int32_t *rr, int32_t *rw, uint32_t *rc, uint32_t *status, int variant,
-                             unsigned long long *visits, cudaStream_t st) {
+                             unsigned long long *visits, cudaStream_t st, const ExtQueries &eq = {}) {
     met_dispatch<T>(met, [&](auto M) {
         constexpr int PER = decltype(M)::value;
         if (k <= 32)
-            launch_fast_t<T, PER, 32>(tv, bt, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc, status,
-                                      variant, visits, st);
+            launch_fast_t<T, PER, 32>(tv, bt, eq, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc,
+                                      status, variant, visits, st);
         else
-            launch_fast_t<T, PER, 64>(tv, bt, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc, status,
-                                      variant, visits, st);
+            launch_fast_t<T, PER, 64>(tv, bt, eq, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc,
+                                      status, variant, visits, st);
     });
 }
 
 template <class T>
 static void launch_fast(const ft_options &o, const ft_tree &tr, const int32_t *leaf_ids, int num, int k, int half,
                         bool excl, const void *bound, uint64_t *idx, void *dist, int32_t *rr, int32_t *rw,
-                        uint32_t *rc, uint32_t *status, int variant, unsigned long long *visits, cudaStream_t st) {
+                        uint32_t *rc, uint32_t *status, int variant, unsigned long long *visits, cudaStream_t st,
+                        const ExtQueries &eq = {}) {
     launch_fast_view<T>(tree_view<T>(tr), BatchDev{}, metric_mode<T>(o, tr), o.return_orig_indices != 0, leaf_ids,
-                        num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st);
+                        num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq);
+}
+
+// SFC rank of external query points: the point's key (the tree's own encoding and box) and
+// its lower bound among the sorted keys; -1 without usable keys.
+template <class T, int SFC>
+__global__ void __launch_bounds__(256)
+    seed_rank_kernel(const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz, int nq,
+                     const T *__restrict__ bbox, const unsigned long long *__restrict__ klo,
+                     const unsigned long long *__restrict__ khi, int n, int32_t *out) {
+    __shared__ uint8_t s_rot[48 * 8], s_sub[48 * 8];
+    __shared__ T       s_par[6];
+    for (int i = threadIdx.x; i < 48 * 8; i += blockDim.x) {
+        s_rot[i] = c_rot[i];
+        s_sub[i] = c_sub[i];
+    }
+    if constexpr (Coord<T>::is_float)
+        if (threadIdx.x < 3)
+            sfc_axis_params(bbox[2 * threadIdx.x], bbox[2 * threadIdx.x + 1], s_par[2 * threadIdx.x],
+                            s_par[2 * threadIdx.x + 1]);
+    __syncthreads();
+    const bool wide = Coord<T>::key_words == 2;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < nq; q += gridDim.x * blockDim.x) {
+        unsigned long long hi, lo;
+        encode_point<T, SFC>(qx[q], qy[q], qz[q], s_par, s_rot, s_sub, hi, lo);
+        int a = 0, b = n; // first j with key[j] >= key
+        while (a < b) {
+            const int  m    = (a + b) >> 1;
+            const bool less = wide ? (khi[m] < hi || (khi[m] == hi && klo[m] < lo)) : (klo[m] < lo);
+            if (less) a = m + 1;
+            else b = m;
+        }
+        out[q] = a;
+    }
+}
+
+template <class T>
+static void seed_ranks(const ft_options &o, const TreeImpl &impl, const void *qx, const void *qy, const void *qz,
+                       int nq, int n, int32_t *out, cudaStream_t st) {
+    const int grid = std::max(1, std::min((nq + 255) / 256, 148 * 16));
+    if (o.sfc_type == MORTON)
+        seed_rank_kernel<T, MORTON><<<grid, 256, 0, st>>>((const T *)qx, (const T *)qy, (const T *)qz, nq,
+                                                          (const T *)impl.bbox, (const unsigned long long *)impl.key_lo,
+                                                          (const unsigned long long *)impl.key_hi, n, out);
+    else
+        seed_rank_kernel<T, PEANO_HILBERT><<<grid, 256, 0, st>>>(
+            (const T *)qx, (const T *)qy, (const T *)qz, nq, (const T *)impl.bbox,
+            (const unsigned long long *)impl.key_lo, (const unsigned long long *)impl.key_hi, n, out);
+    FT_CUDA(cudaGetLastError());
 }
 
 bool fast_self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, bool excl,
@@ -439,6 +508,105 @@ bool fast_self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, siz
     case U64: launch_fast<unsigned long long>(ctx.opts, tr, leaf_ids, (int)num, k, half_window, excl, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st); break;
     }
     replay_exact(ctx, tr, ctx.replay_ranks, ctx.replay_rows, rc, k, excl, idx, dist, st);
+    return true;
+}
+
+// (seed rank, query index) pairs for the query sort.
+__global__ void rank_pairs_kernel(const int32_t *__restrict__ seeds, int nq, unsigned long long *key, uint32_t *perm) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += gridDim.x * blockDim.x) {
+        key[i]  = (unsigned long long)(uint32_t)seeds[i];
+        perm[i] = (uint32_t)i;
+    }
+}
+
+// Sort scratch for external queries (one key word, nq pairs); status words go to the context.
+static void ensure_query_sort(Context &ctx, size_t nq) {
+    TreeImpl &s = ctx.qsort;
+    if (nq <= s.cap && s.key_lo) return;
+    void *ptrs[] = {s.key_lo, s.tmp_lo, s.perm, s.tmp_perm, s.hist, s.lookback, s.tile_counter};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    s            = TreeImpl{};
+    const size_t cap = nq + nq / 4 + 1024;
+    auto alloc = [&](size_t bytes) {
+        void       *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            fail(FT_ERR_OUT_OF_MEMORY, "cudaMalloc of the query sort scratch failed");
+        }
+        return p;
+    };
+    s.key_lo         = (uint64_t *)alloc(cap * 8);
+    s.tmp_lo         = (uint64_t *)alloc(cap * 8);
+    s.perm           = (uint32_t *)alloc(cap * 4);
+    s.tmp_perm       = (uint32_t *)alloc(cap * 4);
+    s.hist           = (uint32_t *)alloc((16 * 256 + 16) * 4);
+    s.lookback_words = sort_lookback_words(cap, 1);
+    s.lookback       = (uint32_t *)alloc(s.lookback_words * 4);
+    s.tile_counter   = (uint32_t *)alloc(16 * 4);
+    s.cap            = cap;
+}
+
+void free_query_sort(Context &ctx) {
+    TreeImpl &s      = ctx.qsort;
+    void     *ptrs[] = {s.key_lo, s.tmp_lo, s.perm, s.tmp_perm, s.hist, s.lookback, s.tile_counter};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    s = TreeImpl{};
+}
+
+bool fast_knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz, size_t nq, int k,
+              int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st) {
+    TreeImpl *impl = (TreeImpl *)tr.impl;
+    if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0 || impl->height_root > 62) return false;
+    // SortedMergeHeap with k equal to its capacity keeps the first k leaves it meets, not the
+    // nearest: only the reference traversal reproduces that
+    int cap = 1;
+    while (cap < max_k) cap <<= 1;
+    if (k > 32 && max_k > 32 && k >= cap) return false;
+    if (half_window <= 0) half_window = k;
+    ensure_replay(ctx, nq);
+    const int n = (int)tr.num_leaves;
+    if (impl->own_keys && impl->key_lo) {
+        switch (ctx.opts.coord_type) {
+        case F32: seed_ranks<float>(ctx.opts, *impl, qx, qy, qz, (int)nq, n, ctx.seed_ranks, st); break;
+        case F64: seed_ranks<double>(ctx.opts, *impl, qx, qy, qz, (int)nq, n, ctx.seed_ranks, st); break;
+        case U32: seed_ranks<uint32_t>(ctx.opts, *impl, qx, qy, qz, (int)nq, n, ctx.seed_ranks, st); break;
+        case U64: seed_ranks<unsigned long long>(ctx.opts, *impl, qx, qy, qz, (int)nq, n, ctx.seed_ranks, st); break;
+        }
+    } else {
+        FT_CUDA(cudaMemsetAsync(ctx.seed_ranks, 0xFF, nq * sizeof(int32_t), st)); // -1: no seeding window
+    }
+    uint32_t           *rc     = ctx.status + 1;
+    unsigned long long *visits = (unsigned long long *)(ctx.status + 2);
+    FT_CUDA(cudaMemsetAsync(rc, 0, 3 * sizeof(uint32_t), st));
+    ExtQueries eq;
+    eq.x = qx;
+    eq.y = qy;
+    eq.z = qz;
+    if (impl->own_keys && impl->key_lo && nq > 1) {
+        // walk the queries in SFC order: sort (seed rank, index) on the rank's bytes
+        ensure_query_sort(ctx, nq);
+        TreeImpl &qs = ctx.qsort;
+        qs.status    = ctx.status;
+        rank_pairs_kernel<<<std::max(1, std::min((int)((nq + 255) / 256), 148 * 16)), 256, 0, st>>>(
+            ctx.seed_ranks, (int)nq, (unsigned long long *)qs.key_lo, qs.perm);
+        FT_CUDA(cudaGetLastError());
+        int bytes = 1;
+        while (bytes < 4 && ((unsigned long long)n >> (8 * bytes)) != 0) ++bytes;
+        static const int digits[4] = {0, 1, 2, 3};
+        sort_pairs_fixed(qs, nq, 1, bytes, digits, st);
+        eq.order = qs.perm;
+    }
+    const int variant = 2;
+    switch (ctx.opts.coord_type) {
+    case F32: launch_fast<float>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, nullptr, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
+    case F64: launch_fast<double>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, nullptr, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
+    case U32: launch_fast<uint32_t>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, nullptr, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
+    case U64: launch_fast<unsigned long long>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, nullptr, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
+    }
+    replay_external(ctx, tr, qx, qy, qz, ctx.replay_rows, rc, k, max_k, idx, dist, st);
     return true;
 }
 
@@ -473,10 +641,13 @@ void ensure_replay(Context &ctx, size_t num) {
     if (num <= ctx.replay_cap && ctx.replay_ranks) return;
     if (ctx.replay_ranks) cudaFree(ctx.replay_ranks);
     if (ctx.replay_rows) cudaFree(ctx.replay_rows);
-    ctx.replay_ranks = ctx.replay_rows = nullptr;
+    if (ctx.seed_ranks) cudaFree(ctx.seed_ranks);
+    ctx.replay_ranks = ctx.replay_rows = ctx.seed_ranks = nullptr;
+    ctx.replay_cap                                       = 0;
     size_t cap = num + num / 4 + 1024;
     FT_CUDA(cudaMalloc(&ctx.replay_ranks, cap * sizeof(int32_t)));
     FT_CUDA(cudaMalloc(&ctx.replay_rows, cap * sizeof(int32_t)));
+    FT_CUDA(cudaMalloc(&ctx.seed_ranks, cap * sizeof(int32_t)));
     ctx.replay_cap = cap;
 }
 

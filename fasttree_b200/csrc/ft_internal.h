@@ -50,6 +50,8 @@ struct TreeImpl {
     int       height_root  = -1;    // host copy after a build
     bool      clean42      = false; // 64-bit integer tree with every coordinate below 2^42
     bool      view         = false; // one set of a batch: arrays owned by the batch, no builds
+    bool      own_keys     = false; // key_lo / key_hi hold keys this library encoded (build_bvh
+                                    // without caller keys), with the box in bbox
 };
 
 // Batched trees: S independent trees stored back to back.  Set s owns leaves (queries)
@@ -78,8 +80,10 @@ struct Context {
     uint32_t      *status = nullptr; // [0] status word of query kernels, [1] replay count
     int32_t       *replay_ranks = nullptr; // queries the fast traversal hands to the exact one
     int32_t       *replay_rows  = nullptr;
+    int32_t       *seed_ranks   = nullptr; // SFC rank of each external query (fast knn)
     size_t         replay_cap   = 0;
     bool           last_fast    = false; // the last self-kNN call used the fast traversal
+    TreeImpl       qsort;                   // sort scratch of external queries (fast knn)
     float         *learned_feats = nullptr; // learned-bound scratch: features and bounds
     void          *learned_bound = nullptr;
     size_t         learned_cap   = 0;
@@ -108,6 +112,17 @@ void batch_self_knn(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t
 // The reference traversal over every leaf of a batch (ft_query.cu).
 void batch_self_knn_exact(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, bool exclude_self,
                           uint64_t *idx, void *dist, cudaStream_t st);
+
+// Fast kNN of external query points (knn_query): the same walk seeded from the SFC window
+// around each query's key rank; tied queries replayed by the reference's heap tier.  False
+// when it does not apply (k > 64, k equal to the merge heap's capacity, tall tree).
+void free_query_sort(Context &ctx);
+bool fast_knn(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz, size_t nq, int k,
+              int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st);
+// Reruns listed external queries (rows, *count_dev of them) with knn_query's heap tier.
+void replay_external(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz,
+                     const int32_t *rows, uint32_t *count_dev, int k, int max_k, uint64_t *idx, void *dist,
+                     cudaStream_t st);
 
 // Reads and clears a device status word (synchronises the stream); throws on a set bit.
 void check_device_status(uint32_t *status, cudaStream_t st);

@@ -300,21 +300,13 @@ template <class D> FT_D void warp_bitonic(D *d, int32_t *ix, int n, int lane) {
 
 static constexpr int kMergeWarps = 4;
 
+// One warp runs the SortedMergeHeap traversal of one query point and writes row `row`.
 template <class T, int PER>
-__global__ void __launch_bounds__(32 * kMergeWarps)
-    merge_knn_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
-                     int nq, int k, int cap, int ret_orig, unsigned long long *__restrict__ out_idx,
-                     typename Coord<T>::dist_t *__restrict__ out_dist, uint32_t *status) {
-    using D = typename Coord<T>::dist_t;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int q    = blockIdx.x * kMergeWarps + w;
-    if (q >= nq) return;
-    D       *hd  = reinterpret_cast<D *>(smem) + (size_t)w * (cap + 32);
-    D       *sgd = hd + cap;
-    int32_t *hix = reinterpret_cast<int32_t *>(reinterpret_cast<D *>(smem) + (size_t)kMergeWarps * (cap + 32)) +
-                   (size_t)w * (cap + 32);
-    int32_t *sgi = hix + cap;
+FT_D void merge_query(const TreeDev<T> &t, T px, T py, T pz, int k, int cap, int ret_orig, size_t row,
+                      typename Coord<T>::dist_t *hd, int32_t *hix, typename Coord<T>::dist_t *sgd, int32_t *sgi,
+                      int lane, unsigned long long *__restrict__ out_idx,
+                      typename Coord<T>::dist_t *__restrict__ out_dist, uint32_t *status) {
+    using D      = typename Coord<T>::dist_t;
     const D DMAX = dist_heap_max<D>();
     for (int i = lane; i < cap; i += 32) {
         hd[i]  = DMAX;
@@ -322,8 +314,7 @@ __global__ void __launch_bounds__(32 * kMergeWarps)
     }
     int count = 0;
     __syncwarp();
-    const int n  = t.n;
-    const T   px = qx[q], py = qy[q], pz = qz[q];
+    const int n = t.n;
     int       sn[kStack];
     D         sd[kStack];
     int       sp = 1;
@@ -387,7 +378,7 @@ __global__ void __launch_bounds__(32 * kMergeWarps)
             }
         }
     }
-    const size_t off = (size_t)q * (size_t)k;
+    const size_t off = row * (size_t)k;
     for (int i = lane; i < k; i += 32) {
         if (hix[i] >= 0) {
             out_idx[off + i]  = (unsigned long long)(long long)hix[i];
@@ -396,6 +387,67 @@ __global__ void __launch_bounds__(32 * kMergeWarps)
             out_idx[off + i]  = ~0ull;
             out_dist[off + i] = dist_missing<D>();
         }
+    }
+    __syncwarp();
+}
+
+template <class T, int PER>
+__global__ void __launch_bounds__(32 * kMergeWarps)
+    merge_knn_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
+                     int nq, int k, int cap, int ret_orig, unsigned long long *__restrict__ out_idx,
+                     typename Coord<T>::dist_t *__restrict__ out_dist, uint32_t *status) {
+    using D = typename Coord<T>::dist_t;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int q    = blockIdx.x * kMergeWarps + w;
+    if (q >= nq) return;
+    D       *hd  = reinterpret_cast<D *>(smem) + (size_t)w * (cap + 32);
+    int32_t *hix = reinterpret_cast<int32_t *>(reinterpret_cast<D *>(smem) + (size_t)kMergeWarps * (cap + 32)) +
+                   (size_t)w * (cap + 32);
+    merge_query<T, PER>(t, qx[q], qy[q], qz[q], k, cap, ret_orig, (size_t)q, hd, hix, hd + cap, hix + cap, lane,
+                        out_idx, out_dist, status);
+}
+
+// Reruns the external queries listed by the fast walk (rows[i], *count_dev of them) with the
+// SortedMergeHeap traversal: one warp per listed row, grid-stride over the device count.
+template <class T, int PER>
+__global__ void __launch_bounds__(32 * kMergeWarps)
+    merge_replay_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
+                        const int32_t *__restrict__ rows, const uint32_t *__restrict__ count_dev, int k, int cap,
+                        int ret_orig, unsigned long long *__restrict__ out_idx,
+                        typename Coord<T>::dist_t *__restrict__ out_dist, uint32_t *status) {
+    using D = typename Coord<T>::dist_t;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    D        *hd   = reinterpret_cast<D *>(smem) + (size_t)w * (cap + 32);
+    int32_t  *hix  = reinterpret_cast<int32_t *>(reinterpret_cast<D *>(smem) + (size_t)kMergeWarps * (cap + 32)) +
+                   (size_t)w * (cap + 32);
+    const int cnt  = (int)*count_dev;
+    for (int i = blockIdx.x * kMergeWarps + w; i < cnt; i += gridDim.x * kMergeWarps) {
+        const int row = rows[i];
+        merge_query<T, PER>(t, qx[row], qy[row], qz[row], k, cap, ret_orig, (size_t)row, hd, hix, hd + cap,
+                            hix + cap, lane, out_idx, out_dist, status);
+    }
+}
+
+// The same for the register / local heap tier (knn_query with k <= 32 or MAXK <= 32).
+template <class T, int CAP, int QT, int PER>
+__global__ void __launch_bounds__(QT)
+    exact_replay_ext_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy,
+                            const T *__restrict__ qz, const int32_t *__restrict__ rows,
+                            const uint32_t *__restrict__ count_dev, int k, int ret_orig,
+                            unsigned long long *__restrict__ out_idx, typename Coord<T>::dist_t *__restrict__ out_dist,
+                            uint32_t *status) {
+    using D = typename Coord<T>::dist_t;
+    extern __shared__ __align__(16) unsigned char smem[];
+    D       *hd   = reinterpret_cast<D *>(smem);
+    int32_t *hix  = reinterpret_cast<int32_t *>(hd + CAP * QT);
+    const int tid = threadIdx.x;
+    const int cnt = (int)*count_dev;
+    for (int i = blockIdx.x * QT + tid; i < cnt; i += gridDim.x * QT) {
+        const int row = rows[i];
+        exact_query<T, CAP, QT, PER>(t, qx[row], qy[row], qz[row], -1, k, ret_orig, hd, hix, tid, (size_t)row,
+                                     out_idx, out_dist, status);
     }
 }
 
@@ -619,9 +671,49 @@ static void knn_typed(const ft_options &o, const ft_tree &tr, const void *qx, co
     });
 }
 
+template <class T>
+static void replay_external_typed(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
+                                  const int32_t *rows, uint32_t *cnt, int k, int max_k, uint64_t *idx, void *dist,
+                                  cudaStream_t st) {
+    using D       = typename Coord<T>::dist_t;
+    TreeDev<T> tv = tree_view<T>(tr);
+    const bool ro = ctx.opts.return_orig_indices != 0;
+    const int  sms = ctx.num_sms;
+    met_dispatch<T>(metric_mode<T>(ctx.opts, tr), [&](auto M) {
+        constexpr int PER = decltype(M)::value;
+        if (k <= 32 || max_k <= 32) {
+            auto   fn   = exact_replay_ext_kernel<T, 32, 128, PER>;
+            size_t smem = (size_t)32 * 128 * (sizeof(D) + 4);
+            FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            fn<<<sms * 4, 128, smem, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz, rows, cnt, k, ro ? 1 : 0,
+                                          (unsigned long long *)idx, (D *)dist, ctx.status);
+        } else {
+            int cap = 1;
+            while (cap < max_k) cap <<= 1;
+            auto   fn   = merge_replay_kernel<T, PER>;
+            size_t smem = (size_t)kMergeWarps * (cap + 32) * (sizeof(D) + 4);
+            FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            fn<<<sms * 8, 32 * kMergeWarps, smem, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz, rows, cnt, k,
+                                                       cap, ro ? 1 : 0, (unsigned long long *)idx, (D *)dist,
+                                                       ctx.status);
+        }
+        FT_CUDA(cudaGetLastError());
+    });
+}
+
+void replay_external(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
+                     const int32_t *rows, uint32_t *cnt, int k, int max_k, uint64_t *idx, void *dist,
+                     cudaStream_t st) {
+    switch (ctx.opts.coord_type) {
+    case F32: replay_external_typed<float>(ctx, tr, qx, qy, qz, rows, cnt, k, max_k, idx, dist, st); break;
+    case F64: replay_external_typed<double>(ctx, tr, qx, qy, qz, rows, cnt, k, max_k, idx, dist, st); break;
+    case U32: replay_external_typed<uint32_t>(ctx, tr, qx, qy, qz, rows, cnt, k, max_k, idx, dist, st); break;
+    case U64: replay_external_typed<unsigned long long>(ctx, tr, qx, qy, qz, rows, cnt, k, max_k, idx, dist, st); break;
+    }
+}
+
 void knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz, size_t nq, int k, int max_k,
          uint64_t *idx, void *dist, const ft_query_options &qo, cudaStream_t st) {
-    (void)qo;
     if (max_k <= 0) max_k = 256;
     if (tr.num_leaves == 0 || nq == 0 || k <= 0) return;
     if (max_k > 32 && k > 32 && k > max_k)
@@ -632,6 +724,11 @@ void knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const 
     if (nq > (size_t)INT32_MAX) fail(FT_ERR_INVALID_ARGUMENT, "too many queries");
     ctx.stats.queries  = (int64_t)nq;
     ctx.stats.replayed = 0;
+    ctx.last_fast      = false;
+    if (qo.method == 1 && fast_knn(ctx, tr, qx, qy, qz, nq, k, max_k, idx, dist, qo.reserved[0], st)) {
+        ctx.last_fast = true;
+        return;
+    }
     switch (ctx.opts.coord_type) {
     case F32: knn_typed<float>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, ctx.status, st); break;
     case F64: knn_typed<double>(ctx.opts, tr, qx, qy, qz, (int)nq, k, max_k, idx, dist, ctx.status, st); break;

@@ -87,7 +87,8 @@ def test_self_knn_subset_and_orig_indices(cfg, k):
 
 @pytest.mark.parametrize("cfg", CONFIGS, ids=CONFIG_IDS)
 @pytest.mark.parametrize("k,max_k", [(5, 256), (32, 256), (33, 256), (48, 128), (64, 256), (64, 64), (128, 128)])
-def test_knn_query_matches_oracle(cfg, k, max_k):
+@pytest.mark.parametrize("method", [0, 1])
+def test_knn_query_matches_oracle(cfg, k, max_k, method):
     coord, sfc, per = cfg
     ctx, opts = make(coord, sfc, per)
     n = 3000
@@ -98,7 +99,7 @@ def test_knn_query_matches_oracle(cfg, k, max_k):
     qx, qy, qz = (to_coord(a, coord) for a in q)
     # half the queries on particles (ties with exact hits)
     qx[:50], qy[:50], qz[:50] = x[:50], y[:50], z[:50]
-    gi, gd = ft.knn_query(ctx, tree, qx, qy, qz, k, max_k=max_k)
+    gi, gd = ft.knn_query(ctx, tree, qx, qy, qz, k, max_k=max_k, method=method)
     oi, od = O.knn(opts, ot, qx, qy, qz, k, max_k)
     assert np.array_equal(gi.cpu().numpy(), oi)
     assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od))
