@@ -11,6 +11,12 @@ way and reported as build_ms.  e2e = the same queries/s through the public API w
 buffers: pinned H2D of the coordinates, build_bvh, self_knn_query and D2H of the results
 inside the timed region.
 
+Beside the headline, the single-GPU line carries three sections measured in the same run:
+"batched" (4096 Plummer sets in one CUDA graph, against the same sets looped through the
+single-tree API), "learned" (the headline tree with the learned radius bound, trained on a
+separate 2M draw) and "knn_query" (1M external queries, k=64, SortedMergeHeap tier, fast
+walk against the plain traversal).
+
 Multi-GPU: one process per GPU (torchrun); each rank builds and queries its own replica of
 the workload (independent point sets, no collective on the data path) -> weak scaling.
 
@@ -43,7 +49,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg4"])
-    p.add_argument("--no-batched", action="store_true", help="skip the batched-sets section of the default run")
+    p.add_argument("--no-batched", action="store_true",
+                   help="skip the batched-sets, learned-bound and knn_query sections of the default run")
     p.add_argument("--sets", type=int, default=4096, help="batched sets: number of sets")
     p.add_argument("--n", type=int, default=0, help="override the point count (tests only)")
     p.add_argument("--k", type=int, default=32)
@@ -139,6 +146,88 @@ def run_batched(args, dev, stream, timed_steps, warmup):
             "replayed": stats["replayed"],
             "note": "graph = ft_batch_build_knn (build + fast self-kNN, one CUDA graph); per-set loop = "
                     "build_bvh + self_knn_query(method=1) per set through the single-tree API (wall clock)"}
+
+
+def run_learned(args, ctx, tree, n, k, stream, fast_visits):
+    """Self-kNN with the learned radius bound on the resident tree: network trained on the
+    exact self-kNN of a separate 2M draw (same generator, seed 12), 2000 Adam steps."""
+    import torch
+
+    import fasttree_b200 as ft
+    from fasttree_b200 import datasets
+    from fasttree_b200 import learned as L
+    tx, ty, tz = datasets.clustered_fixed(2_000_000, n_spheres=4000, seed=12)
+    t0 = time.perf_counter()
+    model, losses = L.train_bound(ctx, tx, ty, tz, k, steps=2000, batch=8192, lr=3e-3, seed=0)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    dev = f"cuda:{ctx.device}"
+    idx = torch.empty(n * k, dtype=torch.uint64, device=dev)
+    dst = torch.empty(n * k, dtype=ft.dist_torch_dtype(ctx.coord), device=dev)
+
+    def timed(fn, steps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    out = {"train_draw": "2M clustered uint64 (4000 spheres, seed 12)", "train_s": train_s,
+           "final_loss": float(np.mean(losses[-100:])), "by_inflation": {}}
+    feats = L.features(ctx, tree, k)
+    out["features_ms"] = timed(lambda: L.features(ctx, tree, k), 3)
+    out["predict_ms"] = timed(lambda: model.predict(feats, 1.3, want_bound=True), 3)
+    for infl in (1.15, 1.3, 1.5):
+        ms = timed(lambda: L.self_knn_query_learned(ctx, tree, model, k, idx, dst, inflation=infl,
+                                                    max_k=max(32, k)), 3)
+        st = ctx.query_stats()
+        out["by_inflation"][str(infl)] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s",
+                                          "replayed": st["replayed"], "visits_per_query": st["visits"] / n}
+    out["fast_visits_per_query"] = fast_visits
+    out["note"] = ("features + predict + bounded walk + replay, bit-exact; see the fast walk's line for the "
+                   "method without the bound")
+    del model
+    return out
+
+
+def run_knn_external(args, stream):
+    """knn_query of 1M external points (half uniform, half particles jittered by 1e-4, seed 3)
+    on 100K uniform float64 points (seed 1), k=64, MAXK=256: fast walk and plain traversal."""
+    import torch
+
+    import fasttree_b200 as ft
+    from fasttree_b200 import datasets
+    x, y, z = datasets.uniform(100_000, seed=1)
+    qx, qy, qz = datasets.external_queries(x, y, z, 1_000_000, seed=3)
+    ctx = ft.Context("f64", "morton")
+    tree = ft.TreeSoA(ctx, len(x))
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree)
+    dq = [torch.from_numpy(a).to(f"cuda:{ctx.device}") for a in (qx, qy, qz)]
+    k, mk, nq = 64, 256, len(qx)
+    idx = torch.empty(nq * k, dtype=torch.uint64, device=dq[0].device)
+    dst = torch.empty(nq * k, dtype=torch.float64, device=dq[0].device)
+    res = {}
+    for method, steps in ((1, 5), (0, 1)):
+        ft.knn_query(ctx, tree, *dq, k, idx, dst, max_k=mk, method=method)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            ft.knn_query(ctx, tree, *dq, k, idx, dst, max_k=mk, method=method)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        res["fast" if method else "plain"] = {"ms_per_step": ms, "value": nq / (ms / 1e3), "unit": "queries/s"}
+        if method:
+            res["fast"]["replayed"] = ctx.query_stats()["replayed"]
+            fi = idx.clone()
+    res["bit_exact"] = bool(torch.equal(fi, idx))
+    res["workload"] = "1M external queries on 100K uniform float64, Morton, k=64, MAXK=256 (SortedMergeHeap)"
+    return res
 
 
 def measured_peaks():
@@ -400,6 +489,12 @@ def run_ours(args):
                 "traffic": traffic, "peak_source": peak_kind, "algorithmic_bytes": alg, "kernel": kname,
                 "note": "latency/ALU bound tree walk; algorithmic bytes = tree (2N-1)*6*s_c + (N-1)*8 + output 16*N*k"}
 
+    learned = knn_ext = None
+    if world == 1 and not args.no_batched and args.workload == "cfg2":
+        fast_visits = results[1][2]["visits"] / n if 1 in results else None
+        learned = run_learned(args, ctx, tree, n, k, stream, fast_visits)
+        knn_ext = run_knn_external(args, stream)
+
     batched = None
     if world == 1 and not args.no_batched and args.workload == "cfg2":
         del idx, dst
@@ -422,7 +517,7 @@ def run_ours(args):
                "config": {"workload": w["name"], "n_points": n, "k": k, "exclude_self": True,
                           "method": args.method, "parallelism": f"replicas x{world}",
                           "l2": "inputs larger than L2: tree records + boxes ~2.3 GB, output 5.1 GB"},
-               "plain": plain, "batched": batched, "build_ms": build_ms, "tree_height": height, "query_stats": stats,
+               "plain": plain, "batched": batched, "learned": learned, "knn_query": knn_ext, "build_ms": build_ms, "tree_height": height, "query_stats": stats,
                "e2e": e2e, "gpu_launches": args.steps * (2 if method == 1 else 1),
                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(out), flush=True)
