@@ -48,7 +48,9 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg4"])
+    p.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg3", "cfg4"])
+    p.add_argument("--no-per-set-loop", action="store_true",
+                   help="batched sets: skip the loop of single-set calls (profiling)")
     p.add_argument("--no-batched", action="store_true",
                    help="skip the batched-sets, learned-bound and knn_query sections of the default run")
     p.add_argument("--sets", type=int, default=4096, help="batched sets: number of sets")
@@ -70,8 +72,8 @@ def workload(args):
     if args.workload == "cfg2":
         n = args.n or 10_000_000
         x, y, z = datasets.clustered_fixed(n, n_spheres=20000 if n >= 1_000_000 else max(10, n // 500), seed=2)
-        return dict(name="cfg2: 10M clustered uint64 (2^40/side), Peano-Hilbert, periodic", n=n, coord="u64",
-                    sfc="ph", periodic=True, x=x, y=y, z=z, dtype="u64")
+        return dict(name=f"cfg2: {n / 1e6:g}M clustered uint64 (2^40/side), Peano-Hilbert, periodic", n=n,
+                    coord="u64", sfc="ph", periodic=True, x=x, y=y, z=z, dtype="u64")
     n = args.n or 100_000
     x, y, z = datasets.uniform(n, seed=1)
     return dict(name="cfg1: 100K uniform float64, Morton, open", n=n, coord="f64", sfc="morton", periodic=False,
@@ -80,7 +82,8 @@ def workload(args):
 
 def batched_workload(args):
     """4096 independent Plummer spheres (scale 0.05) in float32, log-normal sizes (median 8000,
-    sigma 1.2, clipped to [256, 500000]), seed 4: about 50M points in total."""
+    sigma 1.2, clipped to [256, 500000]), seed 4: 65.6M points in total (the log-normal's mean
+    is about twice its median)."""
     from fasttree_b200 import datasets
     sizes = datasets.batched_set_sizes(args.sets, seed=4)
     x, y, z, off = datasets.batched_sets(sizes=sizes, seed=4)
@@ -124,6 +127,12 @@ def run_batched(args, dev, stream, timed_steps, warmup):
     b.check()
     # the same sets one by one through the single-tree API (the non-batched way)
     offs = w["off"]
+    if getattr(args, "no_per_set_loop", False):
+        del b
+        return {"workload": w["name"], "n_sets": S, "n_points": N, "k": k,
+                "graph_build_plus_query_ms": graph_ms, "value": N / (graph_ms / 1e3), "unit": "queries/s",
+                "build_ms": build_ms, "query_fast_ms": fast_ms, "query_plain_ms": plain_ms,
+                "replayed": stats["replayed"]}
     tree = ft.TreeSoA(ctx, int(np.diff(offs).max()))
     li = torch.empty(int(np.diff(offs).max()) * k, dtype=torch.uint64, device=dev)
     ld = torch.empty_like(li, dtype=torch.float64)
@@ -357,6 +366,13 @@ def run_ours(args):
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    if args.workload == "cfg3":
+        r = run_knn_external(args, torch.cuda.current_stream())
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(r), flush=True)
+        return
     if args.workload == "cfg4":
         r = run_batched(args, f"cuda:{local}", torch.cuda.current_stream(), args.steps, args.warmup)
         if world > 1:
