@@ -11,11 +11,13 @@ way and reported as build_ms.  e2e = the same queries/s through the public API w
 buffers: pinned H2D of the coordinates, build_bvh, self_knn_query and D2H of the results
 inside the timed region.
 
-Beside the headline, the single-GPU line carries three sections measured in the same run:
+Beside the headline, the single-GPU line carries sections measured in the same run:
+"other_k_and_range" (the same tree at k=1 and k=64, and range_query on all N points),
 "batched" (4096 Plummer sets in one CUDA graph, against the same sets looped through the
 single-tree API), "learned" (the headline tree with the learned radius bound, trained on a
 separate 2M draw) and "knn_query" (1M external queries, k=64, SortedMergeHeap tier, fast
-walk against the plain traversal).
+walk against the plain traversal).  --workload cfg5 runs the 50M-point k=64 workload
+(full, 10% subset, learned) on its own.
 
 Multi-GPU: one process per GPU (torchrun); each rank builds and queries its own replica of
 the workload (independent point sets, no collective on the data path) -> weak scaling.
@@ -48,7 +50,7 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg3", "cfg4"])
+    p.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg3", "cfg4", "cfg5"])
     p.add_argument("--no-per-set-loop", action="store_true",
                    help="batched sets: skip the loop of single-set calls (profiling)")
     p.add_argument("--no-batched", action="store_true",
@@ -239,6 +241,107 @@ def run_knn_external(args, stream):
     return res
 
 
+def _timed(stream, fn, steps, warmup=1):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_cfg2_extra(ctx, tree, x, y, z, n, stream):
+    """The rest of the clustered workload on its resident tree: self-kNN at k=1 (register heap)
+    and k=64 (shared-memory heap), fast and plain, and range_query on all N points with
+    r_min = 0, r_max = 2e-3 of the box (2e-3 * 2^40 units), 512 results per query."""
+    import torch
+
+    import fasttree_b200 as ft
+    dev = x.device
+    out = {}
+    for k2, mk in ((1, 32), (64, 64)):
+        idx = torch.empty(n * k2, dtype=torch.uint64, device=dev)
+        dst = torch.empty(n * k2, dtype=ft.dist_torch_dtype(ctx.coord), device=dev)
+        row = {}
+        for name, method, steps in (("fast", 1, 3), ("plain", 0, 2)):
+            ms = _timed(stream, lambda: ft.self_knn_query(ctx, tree, k2, idx, dst, max_k=mk, method=method), steps)
+            row[name] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s"}
+            if method:
+                row[name]["replayed"] = ctx.query_stats()["replayed"]
+        out[f"self_knn_k{k2}"] = row
+        del idx, dst
+    max_per = 512
+    r0 = torch.zeros(n, dtype=torch.int64, device=dev).view(torch.uint64)
+    r1 = torch.full((n,), int(2e-3 * 2 ** 40), dtype=torch.int64, device=dev).view(torch.uint64)
+    res = torch.empty(n * max_per, dtype=torch.int32, device=dev)
+    cnt = torch.empty(n, dtype=torch.int32, device=dev)
+    sub = 100_000  # warm-up on a subset (allocates the query-sort scratch), then one full pass
+    ft.range_query(ctx, tree, x[:sub], y[:sub], z[:sub], r0[:sub], r1[:sub], max_per, res, cnt)
+    ms = _timed(stream, lambda: ft.range_query(ctx, tree, x, y, z, r0, r1, max_per, res, cnt), 1, warmup=0)
+    c = cnt.double()
+    out["range_query"] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s",
+                          "mean_count": float(c.mean()), "max_count": int(cnt.max()),
+                          "truncated_queries": int((cnt > max_per).sum()), "max_results_per_query": max_per,
+                          "queries": "the N particle positions in input order (the library walks them in SFC "
+                                     "order); one blocking call, including its status check"}
+    del res, cnt
+    return out
+
+
+def run_cfg5(args, stream):
+    """50M clustered uint64 points (100,000 spheres, seed 5), Peano-Hilbert, periodic:
+    self_knn_query k=64 (fast and plain), self_knn_query_subset on a random 10% of the
+    leaves (seed 5), and the learned bound retrained on a separate 2M draw; 51 GB output."""
+    import torch
+
+    import fasttree_b200 as ft
+    from fasttree_b200 import datasets
+    from fasttree_b200 import learned as L
+    n, k = args.n or 50_000_000, 64
+    t0 = time.perf_counter()
+    x, y, z = datasets.clustered_fixed(n, n_spheres=100_000 if n >= 5_000_000 else max(10, n // 500), seed=5)
+    gen_s = time.perf_counter() - t0
+    ctx = ft.Context("u64", "ph", periodic=True)
+    dev = f"cuda:{ctx.device}"
+    dx, dy, dz = (torch.from_numpy(a).to(dev) for a in (x, y, z))
+    del x, y, z
+    tree = ft.TreeSoA(ctx, n)
+    p = ft.particles(dx, dy, dz)
+    build_ms = _timed(stream, lambda: ft.build_bvh(ctx, p, tree), 2)
+    idx = torch.empty(n * k, dtype=torch.uint64, device=dev)
+    dst = torch.empty(n * k, dtype=torch.uint64, device=dev)
+    out = {"workload": f"cfg5: {n / 1e6:g}M clustered uint64 (100,000 spheres, seed 5), Peano-Hilbert, periodic, k=64",
+           "n_points": n, "gen_s": gen_s, "build_ms": build_ms, "tree_height": tree.height(),
+           "output_bytes": 2 * idx.numel() * 8}
+    for name, method, steps in (("fast", 1, 2), ("plain", 0, 1)):
+        ms = _timed(stream, lambda: ft.self_knn_query(ctx, tree, k, idx, dst, max_k=k, method=method), steps)
+        out[name] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s"}
+        if method:
+            out[name]["replayed"] = ctx.query_stats()["replayed"]
+    g = torch.Generator(device="cpu").manual_seed(5)
+    ids = torch.randperm(n, generator=g)[: n // 10].to(torch.int32).to(dev)
+    si = torch.empty(len(ids) * k, dtype=torch.uint64, device=dev)
+    sd = torch.empty(len(ids) * k, dtype=torch.uint64, device=dev)
+    for name, method in (("subset_fast", 1), ("subset_plain", 0)):
+        ms = _timed(stream, lambda: ft.self_knn_query_subset(ctx, tree, ids, k, si, sd, max_k=k, method=method), 2)
+        out[name] = {"ms_per_step": ms, "value": len(ids) / (ms / 1e3), "unit": "queries/s",
+                     "queries": f"{len(ids)} random leaf ids (10%, seed 5)"}
+    del si, sd
+    tx, ty, tz = datasets.clustered_fixed(2_000_000, n_spheres=4000, seed=15)
+    model, losses = L.train_bound(ctx, tx, ty, tz, k, steps=2000, batch=8192, seed=0)
+    ms = _timed(stream, lambda: L.self_knn_query_learned(ctx, tree, model, k, idx, dst, inflation=1.3, max_k=k), 2)
+    st = ctx.query_stats()
+    out["learned"] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s", "inflation": 1.3,
+                      "replayed": st["replayed"], "train_draw": "2M clustered uint64 (4000 spheres, seed 15)",
+                      "final_loss": float(np.mean(losses[-100:]))}
+    return out
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -366,6 +469,13 @@ def run_ours(args):
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    if args.workload == "cfg5":
+        r = run_cfg5(args, torch.cuda.current_stream())
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(r), flush=True)
+        return
     if args.workload == "cfg3":
         r = run_knn_external(args, torch.cuda.current_stream())
         if world > 1:
@@ -505,11 +615,12 @@ def run_ours(args):
                 "traffic": traffic, "peak_source": peak_kind, "algorithmic_bytes": alg, "kernel": kname,
                 "note": "latency/ALU bound tree walk; algorithmic bytes = tree (2N-1)*6*s_c + (N-1)*8 + output 16*N*k"}
 
-    learned = knn_ext = None
+    learned = knn_ext = extra = None
     if world == 1 and not args.no_batched and args.workload == "cfg2":
         fast_visits = results[1][2]["visits"] / n if 1 in results else None
         learned = run_learned(args, ctx, tree, n, k, stream, fast_visits)
         knn_ext = run_knn_external(args, stream)
+        extra = run_cfg2_extra(ctx, tree, x, y, z, n, stream)
 
     batched = None
     if world == 1 and not args.no_batched and args.workload == "cfg2":
@@ -533,7 +644,8 @@ def run_ours(args):
                "config": {"workload": w["name"], "n_points": n, "k": k, "exclude_self": True,
                           "method": args.method, "parallelism": f"replicas x{world}",
                           "l2": "inputs larger than L2: tree records + boxes ~2.3 GB, output 5.1 GB"},
-               "plain": plain, "batched": batched, "learned": learned, "knn_query": knn_ext, "build_ms": build_ms, "tree_height": height, "query_stats": stats,
+               "plain": plain, "other_k_and_range": extra, "batched": batched, "learned": learned,
+               "knn_query": knn_ext, "build_ms": build_ms, "tree_height": height, "query_stats": stats,
                "e2e": e2e, "gpu_launches": args.steps * (2 if method == 1 else 1),
                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(out), flush=True)

@@ -244,14 +244,16 @@ template <int KIND>
 __global__ void __launch_bounds__(256)
     batch_karras_kernel(const long long *__restrict__ off, const long long *__restrict__ node_off,
                         const long long *__restrict__ rec_off, int S, long long N,
-                        const unsigned long long *__restrict__ klo, int32_t *left, int32_t *right, int32_t *parent) {
+                        const unsigned long long *__restrict__ klo, int32_t *left, int32_t *right, int32_t *parent,
+                        int32_t *leaves) {
     const long long total = rec_off[S];
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < N && g < total;
          g += (long long)gridDim.x * blockDim.x) {
         const int       s  = find_set(rec_off, S, g);
         const long long ro = rec_off[s];
         const int       n  = (int)(off[s + 1] - off[s]);
-        karras_node<KIND>(klo + off[s], nullptr, n, (int)(g - ro), left + ro, right + ro, parent + node_off[s]);
+        karras_node<KIND>(klo + off[s], nullptr, n, (int)(g - ro), left + ro, right + ro, parent + node_off[s],
+                          leaves + ro);
     }
 }
 
@@ -371,6 +373,7 @@ BatchImpl *batch_create(Context &ctx, size_t max_points, size_t max_sets) {
     s.recs        = dalloc<unsigned char>(P * 16 * cb);
     s.height      = dalloc<uint8_t>(P);
     s.counters    = dalloc<int32_t>(P);
+    s.leafcount   = dalloc<int32_t>(P);
     s.key_lo      = (uint64_t *)dalloc<unsigned long long>(P);
     s.tmp_lo      = (uint64_t *)dalloc<unsigned long long>(P);
     s.perm        = dalloc<uint32_t>(P);
@@ -479,11 +482,11 @@ static void batch_build_typed(Context &ctx, BatchImpl &b, const long long *in_of
     if (o.sfc_type == MORTON)
         batch_karras_kernel<0><<<gK, 256, 0, st>>>(b.off, b.node_off, b.rec_off, S, N,
                                                    (const unsigned long long *)s.key_lo, t.left_child, t.right_child,
-                                                   t.parent);
+                                                   t.parent, s.leafcount);
     else
         batch_karras_kernel<1><<<gK, 256, 0, st>>>(b.off, b.node_off, b.rec_off, S, N,
                                                    (const unsigned long long *)s.key_lo, t.left_child, t.right_child,
-                                                   t.parent);
+                                                   t.parent, s.leafcount);
     FT_CUDA(cudaGetLastError());
     FT_CUDA(cudaMemsetAsync(s.counters, 0, (size_t)N * sizeof(int32_t), st));
     batch_refit_kernel<T><<<gK, 256, 0, st>>>(b.off, b.node_off, b.rec_off, S, N, t.left_child, t.right_child,
@@ -587,6 +590,7 @@ void batch_tree_view(Context &ctx, BatchImpl &b, size_t s, ft_tree &out, cudaStr
     v.view           = true;
     v.recs           = (unsigned char *)b.scr.recs + (size_t)ro * 16 * cb;
     v.height         = b.scr.height + ro;
+    v.leafcount      = b.scr.leafcount + ro;
     v.height_root    = n >= 2 ? (int)h : 0;
     v.clean42        = false;
     std::memset(&out, 0, sizeof(out));

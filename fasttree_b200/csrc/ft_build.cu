@@ -385,9 +385,10 @@ __global__ void leaf_init_kernel(const T *sx, const T *sy, const T *sz, size_t n
 template <int KIND>
 __global__ void __launch_bounds__(256) karras_kernel(const unsigned long long *__restrict__ klo,
                                                      const unsigned long long *__restrict__ khi, int n,
-                                                     int32_t *left, int32_t *right, int32_t *parent) {
+                                                     int32_t *left, int32_t *right, int32_t *parent,
+                                                     int32_t *leaves) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1; i += gridDim.x * blockDim.x)
-        karras_node<KIND>(klo, khi, n, i, left, right, parent);
+        karras_node<KIND>(klo, khi, n, i, left, right, parent, leaves);
 }
 
 // =========================================================================================
@@ -425,8 +426,8 @@ template <class T> static void *alloc_dev(size_t count) {
 }
 
 void free_scratch(TreeImpl &s) {
-    void *ptrs[] = {s.recs, s.height, s.counters, s.key_lo, s.key_hi, s.tmp_lo, s.tmp_hi, s.perm, s.tmp_perm,
-                    s.bbox, s.bbox_partial, s.hist, s.lookback, s.tile_counter, s.status};
+    void *ptrs[] = {s.recs, s.height, s.counters, s.leafcount, s.key_lo, s.key_hi, s.tmp_lo, s.tmp_hi, s.perm,
+                    s.tmp_perm, s.bbox, s.bbox_partial, s.hist, s.lookback, s.tile_counter, s.status};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     int coord = s.coord;
@@ -450,6 +451,7 @@ void ensure_scratch(TreeImpl &s, const ft_options &o, size_t n) {
     s.recs     = alloc_dev<unsigned char>((cap > 1 ? cap - 1 : 1) * 16 * cb);
     s.height   = (uint8_t *)alloc_dev<uint8_t>(cap);
     s.counters = (int32_t *)alloc_dev<int32_t>(cap);
+    s.leafcount = (int32_t *)alloc_dev<int32_t>(cap);
     s.key_lo   = (uint64_t *)alloc_dev<uint64_t>(cap);
     s.tmp_lo   = (uint64_t *)alloc_dev<uint64_t>(cap);
     if (W == 2) {
@@ -621,9 +623,9 @@ static void topology_and_refit(const ft_options &o, ft_tree &t, TreeImpl &s, siz
     int blocks = grid_for(n, 256, 148 * 32);
     const unsigned long long *lo = (const unsigned long long *)s.key_lo, *hi = (const unsigned long long *)s.key_hi;
     switch (delta_kind(o)) {
-    case 0: karras_kernel<0><<<blocks, 256, 0, st>>>(lo, hi, (int)n, t.left_child, t.right_child, t.parent); break;
-    case 1: karras_kernel<1><<<blocks, 256, 0, st>>>(lo, hi, (int)n, t.left_child, t.right_child, t.parent); break;
-    default: karras_kernel<2><<<blocks, 256, 0, st>>>(lo, hi, (int)n, t.left_child, t.right_child, t.parent); break;
+    case 0: karras_kernel<0><<<blocks, 256, 0, st>>>(lo, hi, (int)n, t.left_child, t.right_child, t.parent, s.leafcount); break;
+    case 1: karras_kernel<1><<<blocks, 256, 0, st>>>(lo, hi, (int)n, t.left_child, t.right_child, t.parent, s.leafcount); break;
+    default: karras_kernel<2><<<blocks, 256, 0, st>>>(lo, hi, (int)n, t.left_child, t.right_child, t.parent, s.leafcount); break;
     }
     FT_CUDA(cudaGetLastError());
     FT_CUDA(cudaMemsetAsync(s.counters, 0, (n - 1) * sizeof(int32_t), st));

@@ -199,11 +199,11 @@ FT_D void encode_point(T x, T y, T z, const T *par, const uint8_t *s_rot, const 
 // =========================================================================================
 // Karras 2012 topology of internal node i of an n-leaf tree over sorted keys (src/hlbvh.hpp:
 // 852-903): direction, range end by exponential + binary search, split by binary search.
-// Child indices >= n-1 are leaves.
+// Child indices >= n-1 are leaves; leaves[i] receives the node's leaf count.
 // =========================================================================================
 template <int KIND>
 FT_D void karras_node(const unsigned long long *klo, const unsigned long long *khi, int n, int i, int32_t *left,
-                      int32_t *right, int32_t *parent) {
+                      int32_t *right, int32_t *parent, int32_t *leaves) {
     Delta<KIND> delta{klo, khi, n, klo[i], KIND == 2 ? khi[i] : 0ull, i};
     int d         = sgn(delta(i + 1) - delta(i - 1));
     int delta_min = delta(i - d);
@@ -227,6 +227,7 @@ FT_D void karras_node(const unsigned long long *klo, const unsigned long long *k
     right[i]   = rc;
     parent[lc] = i;
     parent[rc] = i;
+    leaves[i]  = l + 1; // node i covers leaves i .. j
 }
 
 // =========================================================================================

@@ -228,7 +228,9 @@ template <class T> struct TreeDev {
     const T *min_x, *max_x, *min_y, *max_y, *min_z, *max_z;
     const int32_t    *orig_idx;
     const NodeRec<T> *recs;
-    int               n; // leaves
+    const uint8_t    *height; // subtree height of each internal node
+    const int32_t    *leaves; // leaf count of each internal node
+    int               n;      // leaves
 };
 
 // Device view of a built tree.
@@ -242,6 +244,8 @@ template <class T> inline TreeDev<T> tree_view(const ft_tree &tr) {
     v.max_z    = (const T *)tr.max_z;
     v.orig_idx = tr.orig_idx;
     v.recs     = (const NodeRec<T> *)((TreeImpl *)tr.impl)->recs;
+    v.height   = ((TreeImpl *)tr.impl)->height;
+    v.leaves   = ((TreeImpl *)tr.impl)->leafcount;
     v.n        = (int)tr.num_leaves;
     return v;
 }
@@ -271,6 +275,8 @@ template <class T> FT_D TreeDev<T> set_view(const TreeDev<T> &all, const BatchDe
     t.max_z    = all.max_z + nb;
     t.orig_idx = all.orig_idx + nb;
     t.recs     = all.recs + rb;
+    t.height   = all.height + rb;
+    t.leaves   = all.leaves + rb;
     t.n        = (int)(b.off[s + 1] - b.off[s]);
     return t;
 }

@@ -556,6 +556,47 @@ void free_query_sort(Context &ctx) {
     s = TreeImpl{};
 }
 
+// SFC rank of each external query in ctx.seed_ranks (-1 without usable keys).
+static bool compute_seed_ranks(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
+                               size_t nq, cudaStream_t st) {
+    TreeImpl *impl = (TreeImpl *)tr.impl;
+    ensure_replay(ctx, nq);
+    const int n = (int)tr.num_leaves;
+    if (!(impl->own_keys && impl->key_lo)) {
+        FT_CUDA(cudaMemsetAsync(ctx.seed_ranks, 0xFF, nq * sizeof(int32_t), st)); // -1: no seeding window
+        return false;
+    }
+    switch (ctx.opts.coord_type) {
+    case F32: seed_ranks<float>(ctx.opts, *impl, qx, qy, qz, (int)nq, n, ctx.seed_ranks, st); break;
+    case F64: seed_ranks<double>(ctx.opts, *impl, qx, qy, qz, (int)nq, n, ctx.seed_ranks, st); break;
+    case U32: seed_ranks<uint32_t>(ctx.opts, *impl, qx, qy, qz, (int)nq, n, ctx.seed_ranks, st); break;
+    case U64: seed_ranks<unsigned long long>(ctx.opts, *impl, qx, qy, qz, (int)nq, n, ctx.seed_ranks, st); break;
+    }
+    return true;
+}
+
+// Query order by SFC rank (ctx.seed_ranks must hold the ranks): sorts (rank, index) pairs.
+static const uint32_t *order_by_rank(Context &ctx, size_t nq, int n, cudaStream_t st) {
+    ensure_query_sort(ctx, nq);
+    TreeImpl &qs = ctx.qsort;
+    qs.status    = ctx.status;
+    rank_pairs_kernel<<<std::max(1, std::min((int)((nq + 255) / 256), 148 * 16)), 256, 0, st>>>(
+        ctx.seed_ranks, (int)nq, (unsigned long long *)qs.key_lo, qs.perm);
+    FT_CUDA(cudaGetLastError());
+    int bytes = 1;
+    while (bytes < 4 && ((unsigned long long)n >> (8 * bytes)) != 0) ++bytes;
+    static const int digits[4] = {0, 1, 2, 3};
+    sort_pairs_fixed(qs, nq, 1, bytes, digits, st);
+    return qs.perm;
+}
+
+const uint32_t *sfc_query_order(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
+                                size_t nq, cudaStream_t st) {
+    if (nq < 2 || tr.num_leaves < 2 || !tr.impl) return nullptr;
+    if (!compute_seed_ranks(ctx, tr, qx, qy, qz, nq, st)) return nullptr;
+    return order_by_rank(ctx, nq, (int)tr.num_leaves, st);
+}
+
 bool fast_knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz, size_t nq, int k,
               int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st) {
     TreeImpl *impl = (TreeImpl *)tr.impl;
@@ -566,18 +607,8 @@ bool fast_knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, c
     while (cap < max_k) cap <<= 1;
     if (k > 32 && max_k > 32 && k >= cap) return false;
     if (half_window <= 0) half_window = k;
-    ensure_replay(ctx, nq);
-    const int n = (int)tr.num_leaves;
-    if (impl->own_keys && impl->key_lo) {
-        switch (ctx.opts.coord_type) {
-        case F32: seed_ranks<float>(ctx.opts, *impl, qx, qy, qz, (int)nq, n, ctx.seed_ranks, st); break;
-        case F64: seed_ranks<double>(ctx.opts, *impl, qx, qy, qz, (int)nq, n, ctx.seed_ranks, st); break;
-        case U32: seed_ranks<uint32_t>(ctx.opts, *impl, qx, qy, qz, (int)nq, n, ctx.seed_ranks, st); break;
-        case U64: seed_ranks<unsigned long long>(ctx.opts, *impl, qx, qy, qz, (int)nq, n, ctx.seed_ranks, st); break;
-        }
-    } else {
-        FT_CUDA(cudaMemsetAsync(ctx.seed_ranks, 0xFF, nq * sizeof(int32_t), st)); // -1: no seeding window
-    }
+    const int  n      = (int)tr.num_leaves;
+    const bool ranked = compute_seed_ranks(ctx, tr, qx, qy, qz, nq, st);
     uint32_t           *rc     = ctx.status + 1;
     unsigned long long *visits = (unsigned long long *)(ctx.status + 2);
     FT_CUDA(cudaMemsetAsync(rc, 0, 3 * sizeof(uint32_t), st));
@@ -585,20 +616,7 @@ bool fast_knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, c
     eq.x = qx;
     eq.y = qy;
     eq.z = qz;
-    if (impl->own_keys && impl->key_lo && nq > 1) {
-        // walk the queries in SFC order: sort (seed rank, index) on the rank's bytes
-        ensure_query_sort(ctx, nq);
-        TreeImpl &qs = ctx.qsort;
-        qs.status    = ctx.status;
-        rank_pairs_kernel<<<std::max(1, std::min((int)((nq + 255) / 256), 148 * 16)), 256, 0, st>>>(
-            ctx.seed_ranks, (int)nq, (unsigned long long *)qs.key_lo, qs.perm);
-        FT_CUDA(cudaGetLastError());
-        int bytes = 1;
-        while (bytes < 4 && ((unsigned long long)n >> (8 * bytes)) != 0) ++bytes;
-        static const int digits[4] = {0, 1, 2, 3};
-        sort_pairs_fixed(qs, nq, 1, bytes, digits, st);
-        eq.order = qs.perm;
-    }
+    if (ranked && nq > 1) eq.order = order_by_rank(ctx, nq, n, st); // walk the queries in SFC order
     const int variant = 2;
     switch (ctx.opts.coord_type) {
     case F32: launch_fast<float>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, nullptr, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;

@@ -33,6 +33,7 @@ struct TreeImpl {
     void     *recs         = nullptr; // NodeRec<T>[cap-1]
     uint8_t  *height       = nullptr; // subtree height of internal nodes
     int32_t  *counters     = nullptr; // refit arrival counters
+    int32_t  *leafcount    = nullptr; // leaves under each internal node (Karras range size)
     uint64_t *key_lo       = nullptr; // sorted keys (low word)
     uint64_t *key_hi       = nullptr; // sorted keys (high word, 126-bit keys only)
     uint64_t *tmp_lo       = nullptr; // sort ping-pong
@@ -117,6 +118,11 @@ void batch_self_knn_exact(Context &ctx, const ft_tree &all, const BatchDev &bt, 
 // around each query's key rank; tied queries replayed by the reference's heap tier.  False
 // when it does not apply (k > 64, k equal to the merge heap's capacity, tall tree).
 void free_query_sort(Context &ctx);
+// Order of external query points along the tree's SFC (sorted by each point's key rank), so
+// that neighbouring threads take neighbouring queries; null when the tree's keys are not
+// this library's own encoding.  Valid until the next call on the context.
+const uint32_t *sfc_query_order(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz,
+                                size_t nq, cudaStream_t st);
 bool fast_knn(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz, size_t nq, int k,
               int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st);
 // Reruns listed external queries (rows, *count_dev of them) with knn_query's heap tier.

@@ -453,18 +453,69 @@ __global__ void __launch_bounds__(QT)
 
 // -----------------------------------------------------------------------------------------
 // range_query (src/hlbvh.hpp:2046-2119): left-first DFS, descend while d2 <= rmax^2, count
-// leaves with d2 >= rmin^2, store while the row has room.
+// leaves with d2 >= rmin^2, store while the row has room; subtrees inside the shell are
+// counted whole once the row is full (same counts, far fewer visits for large radii).
 // -----------------------------------------------------------------------------------------
+// Squared distance from the query to the farthest point of a box, never below the distance
+// node_distance_sq gives any point inside it: the same operations per axis on the farther
+// face (rounding and the shift are monotone).  42-bit periodic trees (PER 2): the wrapped
+// gap over [lo, hi] peaks at the query's antipode when the interval holds it, else at an
+// end.  false when no such bound is provided (general periodic form).
+template <class T, int PER>
+FT_D bool far_dist(T px, T py, T pz, const TreeDev<T> &t, int node, typename Coord<T>::dist_t &out) {
+    using C      = Coord<T>;
+    const T p[3] = {px, py, pz};
+    const T lo[3] = {t.min_x[node], t.min_y[node], t.min_z[node]};
+    const T hi[3] = {t.max_x[node], t.max_y[node], t.max_z[node]};
+    if constexpr (C::is_float) {
+        T f[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) f[d] = c_fmax(sub_rn(hi[d], p[d]), sub_rn(p[d], lo[d]));
+        out = (double)add_rn(add_rn(mul_rn(f[0], f[0]), mul_rn(f[1], f[1])), mul_rn(f[2], f[2]));
+        return true;
+    } else if constexpr (PER == 0) {
+        unsigned long long s = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const unsigned long long a = p[d] > lo[d] ? (unsigned long long)(T)(p[d] - lo[d]) : 0ull;
+            const unsigned long long b = hi[d] > p[d] ? (unsigned long long)(T)(hi[d] - p[d]) : 0ull;
+            s += Metric<T>::sq((a > b ? a : b) >> C::dist_shift);
+        }
+        out = s;
+        return true;
+    } else if constexpr (PER == 2 && sizeof(T) == 8) {
+        constexpr unsigned long long M = (1ull << C::bits) - 1ull, H = 1ull << (C::bits - 1);
+        unsigned long long           s = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const unsigned long long v = (unsigned long long)p[d] & M, l = lo[d], h = hi[d];
+            const unsigned long long a = (v + H) & M; // antipode
+            auto w = [&](unsigned long long x) {
+                const unsigned long long u = (x - v) & M, e = (v - x) & M;
+                return u < e ? u : e;
+            };
+            const unsigned long long wl = w(l), wh = w(h);
+            const unsigned long long g  = (a >= l && a <= h) ? H : (wl > wh ? wl : wh);
+            s += Metric<T>::sq((unsigned long long)(uint32_t)(g >> C::dist_shift));
+        }
+        out = s;
+        return true;
+    } else {
+        return false;
+    }
+}
+
 template <class T, int PER>
 __global__ void __launch_bounds__(128) range_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy,
                                                     const T *__restrict__ qz, const T *__restrict__ rmin,
                                                     const T *__restrict__ rmax, int nq, int32_t *__restrict__ results,
                                                     int32_t *__restrict__ counts, int max_per, int ret_orig,
-                                                    uint32_t *status) {
+                                                    const uint32_t *__restrict__ order, uint32_t *status) {
     using C = Coord<T>;
     using D = typename C::dist_t;
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nq) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    const int q = order ? (int)order[i] : i; // queries taken in SFC order when given
     const int n = t.n;
     D         rm2, RM2;
     if constexpr (C::is_float) {
@@ -500,15 +551,29 @@ __global__ void __launch_bounds__(128) range_kernel(TreeDev<T> t, const T *__res
                 if (count < max_per) results[off + count] = ret_orig ? t.orig_idx[node] : node - (n - 1);
                 ++count;
             }
-        } else if (sp < kStack - 2) {
-            T   lb[6], rb[6];
-            int l, r;
-            load_rec(t.recs, node, lb, rb, l, r);
-            sn[sp]     = r;
-            sd[sp]     = box_dist<T, PER>(px, py, pz, rb);
-            sn[sp + 1] = l;
-            sd[sp + 1] = box_dist<T, PER>(px, py, pz, lb);
-            sp += 2;
+        } else {
+            // Once the row is full only the count changes.  A subtree that lies entirely in
+            // the shell is then counted at once: every leaf under it passes both tests, and
+            // the traversal would visit all of them -- popped at stack size sp, a subtree of
+            // height h reaches stack size sp + h - 1 < 62 on its deepest path, so the stack
+            // guard below drops none of it.
+            if (count >= max_per && d2 >= rm2 && sp + (int)t.height[node] <= kStack - 2) {
+                D far;
+                if (far_dist<T, PER>(px, py, pz, t, node, far) && far <= RM2) {
+                    count += t.leaves[node];
+                    continue;
+                }
+            }
+            if (sp < kStack - 2) {
+                T   lb[6], rb[6];
+                int l, r;
+                load_rec(t.recs, node, lb, rb, l, r);
+                sn[sp]     = r;
+                sd[sp]     = box_dist<T, PER>(px, py, pz, rb);
+                sn[sp + 1] = l;
+                sd[sp + 1] = box_dist<T, PER>(px, py, pz, lb);
+                sp += 2;
+            }
         }
     }
     counts[q] = count;
@@ -740,14 +805,14 @@ void knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const 
 template <class T>
 static void range_typed(const ft_options &o, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
                         const void *rmin, const void *rmax, int nq, int32_t *results, int32_t *counts, int max_per,
-                        uint32_t *status, cudaStream_t st) {
+                        const uint32_t *order, uint32_t *status, cudaStream_t st) {
     TreeDev<T> tv     = tree_view<T>(tr);
     int        blocks = (nq + 127) / 128;
     bool       ro     = o.return_orig_indices != 0;
     met_dispatch<T>(metric_mode<T>(o, tr), [&](auto M) {
         range_kernel<T, decltype(M)::value><<<blocks, 128, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz,
                                                                     (const T *)rmin, (const T *)rmax, nq, results,
-                                                                    counts, max_per, ro ? 1 : 0, status);
+                                                                    counts, max_per, ro ? 1 : 0, order, status);
     });
     FT_CUDA(cudaGetLastError());
 }
@@ -756,11 +821,13 @@ void range(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, cons
            const void *rmax, size_t nq, int32_t *results, int32_t *counts, int max_per, cudaStream_t st) {
     if (tr.num_leaves == 0 || nq == 0) return;
     if (nq > (size_t)INT32_MAX) fail(FT_ERR_INVALID_ARGUMENT, "too many queries");
+    // each query's output is independent of the others: take them in SFC order
+    const uint32_t *order = sfc_query_order(ctx, tr, qx, qy, qz, nq, st);
     switch (ctx.opts.coord_type) {
-    case F32: range_typed<float>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, ctx.status, st); break;
-    case F64: range_typed<double>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, ctx.status, st); break;
-    case U32: range_typed<uint32_t>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, ctx.status, st); break;
-    case U64: range_typed<unsigned long long>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, ctx.status, st); break;
+    case F32: range_typed<float>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, order, ctx.status, st); break;
+    case F64: range_typed<double>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, order, ctx.status, st); break;
+    case U32: range_typed<uint32_t>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, order, ctx.status, st); break;
+    case U64: range_typed<unsigned long long>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, order, ctx.status, st); break;
     }
 }
 

@@ -1,0 +1,93 @@
+"""range_query with large radii (whole subtrees inside the ball are counted at once when the
+row is full) and every query on a tree taller than 62 levels, where the reference's
+traversal stack guard drops subtrees: GPU against the oracle, bit for bit."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+import fasttree_b200 as ft  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+from tests.gpu_util import dist_bits, gen, radius, to_coord  # noqa: E402
+
+CASES = [("f32", "morton", False, O.F32, O.MORTON), ("f64", "ph", False, O.F64, O.PEANO_HILBERT),
+         ("u32", "ph", False, O.U32, O.PEANO_HILBERT), ("u64", "ph", False, O.U64, O.PEANO_HILBERT),
+         ("u64", "ph", True, O.U64, O.PEANO_HILBERT), ("u32", "ph", True, O.U32, O.PEANO_HILBERT)]
+
+
+@pytest.mark.parametrize("coord,sfc,per,oc,os_", CASES, ids=[f"{c[0]}-{c[1]}{'-per' if c[2] else ''}" for c in CASES])
+@pytest.mark.parametrize("r_phys,max_per", [(8.0, 16), (30.0, 64), (60.0, 0), (200.0, 7)])
+def test_range_large_radii_match_oracle(coord, sfc, per, oc, os_, r_phys, max_per):
+    n = 6000
+    x, y, z = gen("clustered", n, oc, 12)
+    ctx = ft.Context(coord, sfc, periodic=per)
+    tree = ft.TreeSoA(ctx, n)
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree)
+    opts = O.Options(oc, os_, per)
+    ot = O.build_bvh(opts, x, y, z)
+    rng = np.random.default_rng(4)
+    q = [to_coord(a, oc) for a in rng.uniform(0, 100.0, (3, 700))]
+    for d, a in enumerate((x, y, z)):
+        q[d][:300] = a[:300]
+    r0 = np.zeros(700, q[0].dtype)
+    r1 = np.full(700, radius(r_phys, oc), q[0].dtype)
+    r0[:100] = radius(r_phys / 4, oc)  # hollow shells too
+    gr, gc = ft.range_query(ctx, tree, *q, r0, r1, max_per)
+    orr, oc_ = O.range_query(opts, ot, *q, r0, r1, max_per)
+    assert np.array_equal(gc.cpu().numpy(), oc_)
+    if max_per:
+        g, o = gr.cpu().numpy(), orr
+        for i in range(700):
+            m = min(int(oc_[i]), max_per)
+            assert np.array_equal(g[i, :m], o[i, :m]), i
+
+
+def tall_points():
+    """63 points with single-bit Morton keys in the unit box (2^-i on one axis, i = 1..21) and
+    16 copies of the origin: a chain of 63 splits over the duplicates' subtree."""
+    pts = [(0.0, 0.0, 0.0)] * 16
+    for axis in range(3):
+        for i in range(1, 22):
+            p = [0.0, 0.0, 0.0]
+            p[axis] = 2.0 ** -i
+            pts.append(tuple(p))
+    a = np.array(pts, np.float64)
+    return a[:, 0].copy(), a[:, 1].copy(), a[:, 2].copy()
+
+
+def test_tree_taller_than_62_matches_oracle():
+    x, y, z = tall_points()
+    n = len(x)
+    ctx = ft.Context("f64", "morton")
+    opts = O.Options(O.F64, O.MORTON, False)
+    box = ft.BoundingBox(0.0, 1.0, 0.0, 1.0, 0.0, 1.0)
+    tree = ft.TreeSoA(ctx, n)
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree, bbox=box)
+    ot = O.build_bvh(opts, x, y, z, bbox=box.array(O.F64))
+    assert tree.height() > 62, tree.height()
+    for k in (1, 5, 32):
+        for method in (0, 1):
+            gi, gd = ft.self_knn_query(ctx, tree, k, max_k=32, method=method)
+            oi, od = O.self_knn(opts, ot, k)
+            assert np.array_equal(gi.cpu().numpy(), oi), (k, method)
+            assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od)), (k, method)
+    rng = np.random.default_rng(3)
+    q = [np.concatenate([x, rng.uniform(0, 2.0 ** -10, 40)]) for _ in range(3)]
+    for k, mk in ((4, 32), (40, 256)):
+        for method in (0, 1):
+            gi, gd = ft.knn_query(ctx, tree, *q, k, max_k=mk, method=method)
+            oi, od = O.knn(opts, ot, *q, k, mk)
+            assert np.array_equal(gi.cpu().numpy(), oi), (k, method)
+            assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od)), (k, method)
+    for r, max_per in ((0.6, 0), (0.6, 5), (1e-4, 3), (2.0, 100)):
+        r0 = np.zeros(len(q[0]))
+        r1 = np.full(len(q[0]), r)
+        gr, gc = ft.range_query(ctx, tree, *q, r0, r1, max_per)
+        orr, oc_ = O.range_query(opts, ot, *q, r0, r1, max_per)
+        assert np.array_equal(gc.cpu().numpy(), oc_), (r, max_per)
+        if max_per:
+            assert np.array_equal(gr.cpu().numpy(), orr), (r, max_per)
