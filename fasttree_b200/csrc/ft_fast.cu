@@ -29,7 +29,9 @@
 namespace ft {
 
 static constexpr int kFastStack = 64;
-static constexpr int kFastWarps = 4;
+// Two warps per block: each thread's heap takes k x 12 B of shared memory (48 KB per 128
+// threads at k = 32), so small blocks pack 9 per SM (18 warps) where 128-thread blocks fit 4.
+static constexpr int kFastWarps = 2;
 static constexpr int kFastThreads = 32 * kFastWarps;
 
 template <class T, int PER, int KC, int VAR>

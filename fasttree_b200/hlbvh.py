@@ -55,6 +55,14 @@ def _ptr(a) -> Optional[int]:
     raise TypeError(f"unsupported array type {type(a)}")
 
 
+def _rows(a, rows: int, width: int):
+    """The first rows x width entries of a flat result buffer (which may be larger), as rows."""
+    if rows * width == 0:
+        return a
+    flat = a.reshape(-1) if isinstance(a, torch.Tensor) else np.asarray(a).reshape(-1)
+    return flat[: rows * width].reshape(rows, width)
+
+
 def _as_coord(a, coord: int):
     """Contiguous array of the coordinate type (keeps device/host placement)."""
     if isinstance(a, torch.Tensor):
@@ -353,7 +361,7 @@ def self_knn_query(ctx: Context, tree: TreeSoA, k: int, results=None, result_dis
     _call(lib().ft_self_knn(ctx.handle, tree.c, None, n, int(k), int(bool(exclude_self)), _ptr(results),
                             _ptr(result_dists), ctypes.byref(_qopts(max_k, method, half_window, variant)),
                             _stream_handle(stream)))
-    return results.view(n, k) if n * k else results, result_dists.view(n, k) if n * k else result_dists
+    return _rows(results, n, k), _rows(result_dists, n, k)
 
 
 def self_knn_query_bounded(ctx: Context, tree: TreeSoA, k: int, bound, results=None, result_dists=None,
@@ -367,7 +375,7 @@ def self_knn_query_bounded(ctx: Context, tree: TreeSoA, k: int, bound, results=N
     _call(lib().ft_self_knn_bounded(ctx.handle, tree.c, _ptr(leaf_ids), num, int(k), int(bool(exclude_self)),
                                     _ptr(bound), _ptr(results), _ptr(result_dists),
                                     ctypes.byref(_qopts(max_k, 1, half_window)), _stream_handle(stream)))
-    return results.view(num, k) if num * k else results, result_dists.view(num, k) if num * k else result_dists
+    return _rows(results, num, k), _rows(result_dists, num, k)
 
 
 def self_knn_query_subset(ctx: Context, tree: TreeSoA, leaf_ids, k: int, results=None, result_dists=None,
@@ -379,7 +387,7 @@ def self_knn_query_subset(ctx: Context, tree: TreeSoA, leaf_ids, k: int, results
     _call(lib().ft_self_knn(ctx.handle, tree.c, _ptr(leaf_ids), num, int(k), int(bool(exclude_self)),
                             _ptr(results), _ptr(result_dists), ctypes.byref(_qopts(max_k, method)),
                             _stream_handle(stream)))
-    return results.view(num, k) if num * k else results, result_dists.view(num, k) if num * k else result_dists
+    return _rows(results, num, k), _rows(result_dists, num, k)
 
 
 def knn_query(ctx: Context, tree: TreeSoA, qx, qy, qz, k: int, results=None, result_dists=None, max_k: int = 256,
@@ -391,7 +399,7 @@ def knn_query(ctx: Context, tree: TreeSoA, qx, qy, qz, k: int, results=None, res
         results, result_dists = _alloc_knn_out(ctx, nq, k)
     _call(lib().ft_knn(ctx.handle, tree.c, _ptr(x), _ptr(y), _ptr(z), nq, int(k), _ptr(results), _ptr(result_dists),
                        ctypes.byref(_qopts(max_k, method)), _stream_handle(stream)))
-    return results.view(nq, k) if nq * k else results, result_dists.view(nq, k) if nq * k else result_dists
+    return _rows(results, nq, k), _rows(result_dists, nq, k)
 
 
 def range_query(ctx: Context, tree: TreeSoA, qx, qy, qz, r_min, r_max, max_results_per_query: int, results=None,
@@ -406,7 +414,7 @@ def range_query(ctx: Context, tree: TreeSoA, qx, qy, qz, r_min, r_max, max_resul
         result_counts = torch.zeros(nq, dtype=torch.int32, device=dev)
     _call(lib().ft_range(ctx.handle, tree.c, _ptr(x), _ptr(y), _ptr(z), _ptr(r0), _ptr(r1), nq, _ptr(results),
                          _ptr(result_counts), int(max_results_per_query), _stream_handle(stream)))
-    return results.view(nq, max_results_per_query) if nq * max_results_per_query else results, result_counts
+    return _rows(results, nq, max_results_per_query), result_counts
 
 
 class _BatchSetTree(TreeSoA):
@@ -476,7 +484,7 @@ class BatchedSets:
         _call(lib().ft_batch_self_knn(self.ctx.handle, self._h, int(k), int(bool(exclude_self)), _ptr(results),
                                       _ptr(result_dists), ctypes.byref(_qopts(max_k, method, half_window, variant)),
                                       _stream_handle(stream)))
-        return results.view(N, k) if N * k else results, result_dists.view(N, k) if N * k else result_dists
+        return _rows(results, N, k), _rows(result_dists, N, k)
 
     def build_knn(self, set_offsets, pos_x, pos_y, pos_z, k: int, results, result_dists, exclude_self=True,
                   max_k: int = 32, method: int = 1, id=None, is_ghost=None, stream=None):
@@ -491,7 +499,7 @@ class BatchedSets:
                                        _stream_handle(stream)))
         self._keep = (off, xyz, ids, gh, results, result_dists)
         self.num_sets, self.num_points = S, N
-        return results.view(N, k) if N * k else results, result_dists.view(N, k) if N * k else result_dists
+        return _rows(results, N, k), _rows(result_dists, N, k)
 
     def tree(self, s: int, stream=None) -> TreeSoA:
         c = capi.FtTree()

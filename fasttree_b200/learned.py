@@ -16,7 +16,7 @@ import torch
 
 from . import capi
 from .capi import lib
-from .hlbvh import (Context, TreeSoA, _alloc_knn_out, _call, _ptr, _qopts, _stream_handle, build_bvh,
+from .hlbvh import (Context, TreeSoA, _alloc_knn_out, _call, _ptr, _qopts, _rows, _stream_handle, build_bvh,
                     dist_torch_dtype, particles, self_knn_query)
 
 N_FEATURES = 12
@@ -152,4 +152,4 @@ def self_knn_query_learned(ctx: Context, tree: TreeSoA, model: BoundModel, k: in
     _call(lib().ft_self_knn_learned(ctx.handle, tree.c, model._h, _ptr(leaf_ids), num, int(k),
                                     int(bool(exclude_self)), ctypes.c_float(inflation), _ptr(results),
                                     _ptr(result_dists), ctypes.byref(_qopts(max_k, 1)), _stream_handle(stream)))
-    return results.view(num, k) if num * k else results, result_dists.view(num, k) if num * k else result_dists
+    return _rows(results, num, k), _rows(result_dists, num, k)

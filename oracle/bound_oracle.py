@@ -177,23 +177,34 @@ def unpack(params):
             p[OFF_B2:OFF_W3], p[OFF_W3:OFF_B3], p[OFF_B3])
 
 
-def standardise(raw, norm):
+def _round(a, rounding):
+    return bf16(a).astype(np.float64) if rounding else np.asarray(a, np.float64)
+
+
+def standardise(raw, norm, rounding=True):
     """norm = (mean[12], std[12], target_mean, target_std) as the library stores it."""
     mean, std, _, _ = norm
     isd = (np.float32(1.0) / np.maximum(np.asarray(std, np.float32), np.float32(1e-3))).astype(np.float32)
     x = (np.asarray(raw, np.float32) - np.asarray(mean, np.float32)) * isd
-    return bf16(x).astype(np.float64)
+    return _round(x, rounding)
 
 
-def forward(params, raw, norm):
-    W1, b1, W2, b2, w3, b3 = unpack(params)
-    x = standardise(raw, norm)
+def forward(params, raw, norm, rounding=True):
+    """rounding=False keeps every value in float64 (for derivative checks of the oracle)."""
+    W1, b1, W2, b2, w3, b3 = unpack(params) if rounding else unpack_exact(params)
+    x = standardise(raw, norm, rounding)
     z1 = x @ W1.T + b1
-    h1 = bf16(gelu(z1)).astype(np.float64)
+    h1 = _round(gelu(z1), rounding)
     z2 = h1 @ W2.T + b2
-    h2 = bf16(gelu(z2)).astype(np.float64)
+    h2 = _round(gelu(z2), rounding)
     y = h2 @ w3 + b3
     return y, (x, z1, h1, z2, h2)
+
+
+def unpack_exact(params):
+    p = np.asarray(params, np.float64)
+    return (p[OFF_W1:OFF_B1].reshape(N_HID, N_FEATURES), p[OFF_B1:OFF_W2], p[OFF_W2:OFF_B2].reshape(N_HID, N_HID),
+            p[OFF_B2:OFF_W3], p[OFF_W3:OFF_B3], p[OFF_B3])
 
 
 def predict_log2(params, raw, norm):
@@ -203,14 +214,15 @@ def predict_log2(params, raw, norm):
     return np.asarray(raw, np.float64)[:, 10] + y * t_std + t_mean
 
 
-def loss_and_grad(params, raw, tgt, norm):
+def loss_and_grad(params, raw, tgt, norm, rounding=True):
     """Mean squared error of the standardised residual target (log2 d_k - feature 10) and its
-    gradient w.r.t. the weights."""
+    gradient w.r.t. the weights.  The gradient treats the bfloat16 roundings as identity (the
+    straight-through rule the GPU kernels follow)."""
     t_mean, t_std = norm[2], max(norm[3], 1e-3)
     res = np.asarray(tgt, np.float32) - np.asarray(raw, np.float32)[:, 10]
     t = (res.astype(np.float64) - t_mean) / t_std
-    W1, b1, W2, b2, w3, b3 = unpack(params)
-    y, (x, z1, h1, z2, h2) = forward(params, raw, norm)
+    W1, b1, W2, b2, w3, b3 = unpack(params) if rounding else unpack_exact(params)
+    y, (x, z1, h1, z2, h2) = forward(params, raw, norm, rounding)
     B = len(t)
     dy = 2.0 * (y - t) / B
     g = np.zeros(N_PARAMS, np.float64)
