@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg3", "cfg4", "cfg5"])
+    p.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg3", "cfg4", "cfg5", "learned"])
     p.add_argument("--no-per-set-loop", action="store_true",
                    help="batched sets: skip the loop of single-set calls (profiling)")
     p.add_argument("--no-batched", action="store_true",
@@ -469,6 +469,23 @@ def run_ours(args):
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    if args.workload == "learned":
+        # the learned-bound section alone, on the clustered workload at --n points
+        w = workload(argparse.Namespace(**{**vars(args), "workload": "cfg2"}))
+        ctx = ft.Context(w["coord"], w["sfc"], periodic=w["periodic"], device=local)
+        tree = ft.TreeSoA(ctx, w["n"])
+        ft.build_bvh(ctx, ft.particles(*(torch.from_numpy(a).to(f"cuda:{local}") for a in (w["x"], w["y"], w["z"]))),
+                     tree)
+        st = torch.cuda.current_stream()
+        ft.self_knn_query(ctx, tree, args.k, method=1)
+        torch.cuda.synchronize()
+        r = run_learned(args, ctx, tree, w["n"], args.k, st, ctx.query_stats()["visits"] / w["n"])
+        r["workload"] = w["name"]
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(r), flush=True)
+        return
     if args.workload == "cfg5":
         r = run_cfg5(args, torch.cuda.current_stream())
         if world > 1:

@@ -300,7 +300,7 @@ __global__ void bound_targets_kernel(const unsigned long long *__restrict__ idx,
 // =========================================================================================
 // MLP
 // =========================================================================================
-// Shared-memory copy of the network as fp32 values of the bfloat16 weights.
+// Shared-memory copy of the network as fp32 values of the bfloat16 weights (training tiles).
 struct SmemNet {
     float w1t[kFeat * kHid]; // [i][j]
     float b1[kHid];
@@ -343,47 +343,247 @@ FT_D void load_net(SmemNet &s, const __nv_bfloat16 *__restrict__ pb, const float
 // Standardised input rounded to bfloat16.
 FT_D float in_feat(const SmemNet &s, const float *raw, int i) { return bf16r((raw[i] - s.mu[i]) * s.isd[i]); }
 
-// One sample's forward pass (inference): standardised log2 k-th distance.
-FT_D float net_forward(const SmemNet &s, const float *raw) {
-    float x[kFeat], h1[kHid];
-#pragma unroll
-    for (int i = 0; i < kFeat; ++i) x[i] = in_feat(s, raw, i);
-#pragma unroll 8
-    for (int j = 0; j < kHid; ++j) {
-        float z = s.b1[j];
-#pragma unroll
-        for (int i = 0; i < kFeat; ++i) z = fmaf(s.w1t[i * kHid + j], x[i], z);
-        h1[j] = bf16r(gelu(z));
-    }
-    float y = s.b3;
-    for (int j = 0; j < kHid; ++j) {
-        float z = s.b2[j];
-#pragma unroll
-        for (int i = 0; i < kHid; ++i) z = fmaf(s.w2[j * kHid + i], h1[i], z);
-        y = fmaf(s.w3[j], bf16r(gelu(z)), y);
-    }
-    return y;
+// =========================================================================================
+// Inference on the 5th-generation tensor cores (tcgen05, accumulators in tensor memory).
+// Persistent CTAs of 128 threads take tiles of 128 queries:
+//   A1 [128 x 16] = standardised features in bfloat16 (K padded from 12 with zeros)
+//   D1 [128 x 64] = A1 x W1^T          one tcgen05.mma M=128 N=64 K=16, fp32 in TMEM
+//   A2 [128 x 64] = bf16(gelu(D1 + b1)) epilogue: tcgen05.ld -> registers -> shared memory
+//   D2 [128 x 64] = A2 x W2^T          four K=16 steps into the same 64 TMEM columns
+//   y             = w3 . bf16(gelu(D2 + b2)) + b3, one query per thread (TMEM lane = row)
+// Operands sit in shared memory in the canonical no-swizzle K-major layout: 8-row x 16-byte
+// core matrices, adjacent along K 128 bytes apart (leading byte offset), adjacent along
+// M / N (K/8) x 128 bytes apart (stride byte offset).  One thread issues the MMAs; their
+// completion reaches an mbarrier through tcgen05.commit, and every wait on it is bounded.
+// =========================================================================================
+static constexpr int kTcRows  = 128;
+static constexpr int kTcCols  = 64; // TMEM columns per CTA (fp32 accumulator N = 64)
+static constexpr int kK1      = 16; // layer-1 K (12 features + 4 zero columns)
+
+struct TcSmem {
+    __align__(16) uint16_t w1[kHid * kK1];   // B operand of layer 1, canonical layout
+    __align__(16) uint16_t w2[kHid * kHid];  // B operand of layer 2
+    __align__(16) uint16_t a1[kTcRows * kK1];
+    __align__(16) uint16_t a2[kTcRows * kHid];
+    float    b1[kHid], b2[kHid], w3[kHid];
+    float    mu[kFeat], isd[kFeat];
+    float    b3, t_mu, t_sd;
+    uint64_t mbar;
+    uint32_t tmem;
+    int      abort;
+};
+
+// Byte offset of element (row, k) of an operand with K columns in the canonical layout.
+FT_HD uint32_t canon(int row, int k, int K) {
+    return (uint32_t)((((row >> 3) * (K >> 3) + (k >> 3)) * 128) + (row & 7) * 16 + (k & 7) * 2);
 }
 
-// Predicted log2 k-th distance (pred) and / or the inflated bound in distance units.
+FT_D uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor: start address, leading / stride byte offsets (all >> 4),
+// the fixed 0b001 at bits 46-48, base offset 0, no swizzle.
+FT_D uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: fp32 accumulator, bf16 A and B, both K-major, N, M.
+__host__ __device__ constexpr uint32_t tc_idesc(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+FT_D void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate) {
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+                 "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+FT_D void tc_commit(uint32_t mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+                 : "memory");
+}
+FT_D bool mbar_try_wait(uint32_t mbar, uint32_t phase) {
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}\n"
+                 : "=r"(ok)
+                 : "r"(mbar), "r"(phase)
+                 : "memory");
+    return ok != 0;
+}
+// Bounded wait for an mbarrier phase; false when it gave up.
+FT_D bool mbar_wait(uint32_t mbar, uint32_t phase) {
+    for (long long it = 0; it < (1ll << 26); ++it) {
+        if (mbar_try_wait(mbar, phase)) return true;
+        if (it > 64) __nanosleep(64);
+    }
+    return false;
+}
+FT_D void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+FT_D void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+FT_D void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 16 consecutive fp32 columns of this thread's TMEM lane.
+FT_D void tc_ld16(uint32_t taddr, float *v) {
+    uint32_t r[16];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                 "%13, %14, %15}, [%16];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                   "=r"(r[15])
+                 : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+FT_D void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 template <class D>
-__global__ void __launch_bounds__(128)
-    bound_predict_kernel(const __nv_bfloat16 *__restrict__ pb, const float *__restrict__ norm,
-                         const float *__restrict__ feats, int num, float inflation, float *pred, D *bound) {
-    __shared__ SmemNet s;
-    load_net(s, pb, norm);
+__global__ void __launch_bounds__(kTcRows)
+    bound_predict_tc_kernel(const __nv_bfloat16 *__restrict__ pb, const float *__restrict__ norm,
+                            const float *__restrict__ feats, int num, float inflation, float *pred, D *bound,
+                            uint32_t *status) {
+    extern __shared__ __align__(16) unsigned char smem_tc[];
+    TcSmem        &s    = *reinterpret_cast<TcSmem *>(smem_tc);
+    const int      tid  = threadIdx.x, warp = tid >> 5;
+    const uint16_t *raw = reinterpret_cast<const uint16_t *>(pb);
+    // weights into the canonical layouts (W1's columns 12..15 are zero)
+    for (int e = tid; e < kHid * kK1; e += kTcRows) {
+        const int j = e / kK1, k = e % kK1;
+        *reinterpret_cast<uint16_t *>(reinterpret_cast<unsigned char *>(s.w1) + canon(j, k, kK1)) =
+            k < kFeat ? raw[kOffW1 + j * kFeat + k] : (uint16_t)0;
+    }
+    for (int e = tid; e < kHid * kHid; e += kTcRows) {
+        const int j = e / kHid, k = e % kHid;
+        *reinterpret_cast<uint16_t *>(reinterpret_cast<unsigned char *>(s.w2) + canon(j, k, kHid)) = raw[kOffW2 + e];
+    }
+    for (int e = tid; e < kHid; e += kTcRows) {
+        s.b1[e] = __bfloat162float(pb[kOffB1 + e]);
+        s.b2[e] = __bfloat162float(pb[kOffB2 + e]);
+        s.w3[e] = __bfloat162float(pb[kOffW3 + e]);
+    }
+    if (tid < kFeat) {
+        s.mu[tid]  = norm[tid];
+        s.isd[tid] = norm[kFeat + tid];
+    }
+    if (tid == 0) {
+        s.b3    = __bfloat162float(pb[kOffB3]);
+        s.t_mu  = norm[2 * kFeat];
+        s.t_sd  = norm[2 * kFeat + 1];
+        s.abort = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s.mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem)),
+                     "r"(kTcCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    tc_fence_before();
     __syncthreads();
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < num; q += gridDim.x * blockDim.x) {
-        const float *raw = feats + (size_t)q * kFeat;
-        const float  y   = net_forward(s, raw);
-        const float  lp  = raw[10] + fmaf(y, s.t_sd, s.t_mu); // log2 of the k-th distance (length)
-        if (pred) pred[q] = lp;
-        if (bound) {
-            const double len = exp2((double)lp) * (double)inflation;
-            const double b2  = len * len;
-            if constexpr (std::is_same<D, double>::value) bound[q] = b2;
-            else bound[q] = (b2 >= 1.8446744073709552e19) ? ~0ull : (unsigned long long)ceil(b2);
+    tc_fence_after();
+    const uint32_t tmem  = s.tmem;
+    const uint32_t mbar  = smem_u32(&s.mbar);
+    const uint32_t lane0 = tmem + ((uint32_t)(32 * warp) << 16); // this warp's TMEM lanes
+    const uint32_t id1 = tc_idesc(kTcRows, kHid), id2 = tc_idesc(kTcRows, kHid);
+    const uint32_t a1 = smem_u32(s.a1), a2 = smem_u32(s.a2), w1 = smem_u32(s.w1), w2 = smem_u32(s.w2);
+    uint32_t       phase = 0;
+    unsigned char *sa1 = reinterpret_cast<unsigned char *>(s.a1), *sa2 = reinterpret_cast<unsigned char *>(s.a2);
+
+    for (int tile = blockIdx.x; tile * kTcRows < num; tile += gridDim.x) {
+        const int q = tile * kTcRows + tid;
+        // ---- A1: this thread's row ----
+        {
+            __align__(16) uint16_t v[kK1];
+#pragma unroll
+            for (int k = 0; k < kK1; ++k) {
+                float x = 0.0f;
+                if (k < kFeat && q < num) x = (feats[(size_t)q * kFeat + k] - s.mu[k]) * s.isd[k];
+                v[k] = __bfloat16_as_ushort(__float2bfloat16_rn(x));
+            }
+#pragma unroll
+            for (int c = 0; c < kK1 / 8; ++c)
+                *reinterpret_cast<uint4 *>(sa1 + canon(tid, 8 * c, kK1)) = *reinterpret_cast<const uint4 *>(v + 8 * c);
         }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            tc_mma(tmem, tc_desc(a1, 128, (kK1 / 8) * 128), tc_desc(w1, 128, (kK1 / 8) * 128), id1, 0u);
+            tc_commit(mbar);
+        }
+        if (!mbar_wait(mbar, phase)) atomicOr(&s.abort, 1);
+        phase ^= 1u;
+        tc_fence_after();
+        __syncthreads();
+        if (s.abort) break;
+        // ---- epilogue 1: bias, GELU, bf16 -> A2 row ----
+        {
+            float z[16];
+#pragma unroll
+            for (int c = 0; c < kHid / 16; ++c) {
+                tc_ld16(lane0 + 16 * c, z);
+                tc_wait_ld();
+                __align__(16) uint16_t h[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i)
+                    h[i] = __bfloat16_as_ushort(__float2bfloat16_rn(gelu(z[i] + s.b1[16 * c + i])));
+                *reinterpret_cast<uint4 *>(sa2 + canon(tid, 16 * c, kHid))     = *reinterpret_cast<const uint4 *>(h);
+                *reinterpret_cast<uint4 *>(sa2 + canon(tid, 16 * c + 8, kHid)) = *reinterpret_cast<const uint4 *>(h + 8);
+            }
+        }
+        fence_async_smem();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int ks = 0; ks < kHid / 16; ++ks) // K step of 16 = two core matrices = 256 bytes
+                tc_mma(tmem, tc_desc(a2 + 256 * ks, 128, (kHid / 8) * 128), tc_desc(w2 + 256 * ks, 128, (kHid / 8) * 128),
+                       id2, ks > 0 ? 1u : 0u);
+            tc_commit(mbar);
+        }
+        if (!mbar_wait(mbar, phase)) atomicOr(&s.abort, 1);
+        phase ^= 1u;
+        tc_fence_after();
+        __syncthreads();
+        if (s.abort) break;
+        // ---- epilogue 2: bias, GELU, bf16, output layer ----
+        float y = s.b3;
+        {
+            float z[16];
+#pragma unroll
+            for (int c = 0; c < kHid / 16; ++c) {
+                tc_ld16(lane0 + 16 * c, z);
+                tc_wait_ld();
+#pragma unroll
+                for (int i = 0; i < 16; ++i) y = fmaf(s.w3[16 * c + i], bf16r(gelu(z[i] + s.b2[16 * c + i])), y);
+            }
+        }
+        if (q < num) {
+            const float lp = feats[(size_t)q * kFeat + 10] + fmaf(y, s.t_sd, s.t_mu);
+            if (pred) pred[q] = lp;
+            if (bound) {
+                const double len = exp2((double)lp) * (double)inflation;
+                const double b2  = len * len;
+                if constexpr (std::is_same<D, double>::value) bound[q] = b2;
+                else bound[q] = (b2 >= 1.8446744073709552e19) ? ~0ull : (unsigned long long)ceil(b2);
+            }
+        }
+        tc_fence_before();
+        __syncthreads(); // every lane has read D2 before the next tile's MMA overwrites it
+        tc_fence_after();
+    }
+    if (s.abort) {
+        if (tid == 0) atomicOr(status, STATUS_SPIN_LIMIT);
+        mbar_wait(mbar, phase ^ 1u); // the phase that timed out: let its MMA finish (bounded) before freeing TMEM
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols) : "memory");
     }
 }
 
@@ -729,16 +929,26 @@ void bound_model_fit(BoundModel &b, const float *feats, const float *targets, in
     if (loss_host) FT_CUDA(cudaStreamSynchronize(st));
 }
 
+// Inference runs on the tensor cores (bound_predict_tc_kernel): 4 CTAs of 128 threads per
+// SM, each holding 64 TMEM columns (256 of the SM's 512 even with 8 resident), over tiles of
+// 128 queries.
+static_assert(sizeof(TcSmem) + 1024 >= 227 * 1024 / 8, "at most 8 CTAs per SM, 64 TMEM columns each");
 void bound_model_predict(Context &ctx, BoundModel &b, const float *feats, size_t n, float inflation, float *pred,
                          void *bound, cudaStream_t st) {
     if (n == 0) return;
-    const int grid = (int)std::min<size_t>((n + 127) / 128, (size_t)ctx.num_sms * 16);
-    if (ctx.opts.coord_type == F32 || ctx.opts.coord_type == F64)
-        bound_predict_kernel<double><<<grid, 128, 0, st>>>(b.pb, b.norm, feats, (int)n, inflation, pred,
-                                                           (double *)bound);
-    else
-        bound_predict_kernel<unsigned long long><<<grid, 128, 0, st>>>(b.pb, b.norm, feats, (int)n, inflation, pred,
-                                                                       (unsigned long long *)bound);
+    const int    grid = (int)std::min<size_t>((n + kTcRows - 1) / kTcRows, (size_t)ctx.num_sms * 4);
+    const size_t smem = sizeof(TcSmem) + 1024; // padding keeps residency at <= 8 CTAs per SM
+    if (ctx.opts.coord_type == F32 || ctx.opts.coord_type == F64) {
+        FT_CUDA(cudaFuncSetAttribute(bound_predict_tc_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+        bound_predict_tc_kernel<double><<<grid, kTcRows, smem, st>>>(b.pb, b.norm, feats, (int)n, inflation, pred,
+                                                                     (double *)bound, ctx.status);
+    } else {
+        FT_CUDA(cudaFuncSetAttribute(bound_predict_tc_kernel<unsigned long long>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        bound_predict_tc_kernel<unsigned long long><<<grid, kTcRows, smem, st>>>(
+            b.pb, b.norm, feats, (int)n, inflation, pred, (unsigned long long *)bound, ctx.status);
+    }
     FT_CUDA(cudaGetLastError());
 }
 
