@@ -51,6 +51,17 @@ static bool is_host_only(const void *p) {
     return a.type == cudaMemoryTypeUnregistered;
 }
 
+// Host memory of either kind (pinned or pageable): not device memory or managed memory.
+static bool is_host_memory(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered || a.type == cudaMemoryTypeHost;
+}
+
 // Stream-ordered staging of one host buffer (ensure_device_readable / _writable and
 // copy_back_and_free, src/hlbvh.hpp:125-200).
 struct Staged {
@@ -241,6 +252,14 @@ ft_status ft_context_destroy(ft_context *ctx) {
         if (ctx->replay_ranks) cudaFree(ctx->replay_ranks);
         if (ctx->replay_rows) cudaFree(ctx->replay_rows);
         if (ctx->seed_ranks) cudaFree(ctx->seed_ranks);
+        for (int b = 0; b < 2; ++b) {
+            if (ctx->stage_idx[b]) cudaFree(ctx->stage_idx[b]);
+            if (ctx->stage_dist[b]) cudaFree(ctx->stage_dist[b]);
+            if (ctx->ev_walked[b]) cudaEventDestroy(ctx->ev_walked[b]);
+            if (ctx->ev_copied[b]) cudaEventDestroy(ctx->ev_copied[b]);
+        }
+        if (ctx->iota) cudaFree(ctx->iota);
+        if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
         ft::free_query_sort(*ctx);
         if (ctx->learned_feats) cudaFree(ctx->learned_feats);
         if (ctx->learned_bound) cudaFree(ctx->learned_bound);
@@ -492,7 +511,13 @@ ft_status ft_self_knn(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_
     if (!leaf_ids) num = tree->num_leaves;
     if (num > 0 && k > 0 && tree->num_leaves > 0) need(idx_out && dist_out, "null output array");
     DeviceGuard g(ctx->device);
-    ft::self_knn(*ctx, *tree, leaf_ids, num, k, exclude_self != 0, idx_out, dist_out, q, (cudaStream_t)stream);
+    const bool host_idx = is_host_memory(idx_out), host_dist = is_host_memory(dist_out);
+    need(host_idx == host_dist, "idx_out and dist_out must both be host or both be device memory");
+    if (host_idx) // results straight to host memory, copy-out overlapped with the walk
+        ft::self_knn_to_host(*ctx, *tree, leaf_ids, num, k, exclude_self != 0, idx_out, dist_out, q,
+                             (cudaStream_t)stream);
+    else
+        ft::self_knn(*ctx, *tree, leaf_ids, num, k, exclude_self != 0, idx_out, dist_out, q, (cudaStream_t)stream);
     FT_API_END
 }
 

@@ -160,9 +160,10 @@ __global__ void __launch_bounds__(kFastThreads)
     for (int j = 0; j < W; ++j) {
         const int leaf = w0 + j;
         if (active && leaf + n - 1 != self_leaf) {
+            // a leaf's box is its point (min == max): read the min arrays only
             const int s  = leaf + n - 1;
-            const D   d2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, t.min_x[s], t.max_x[s], t.min_y[s], t.max_y[s],
-                                                       t.min_z[s], t.max_z[s]);
+            const T   x = t.min_x[s], y = t.min_y[s], z = t.min_z[s];
+            const D   d2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, x, x, y, y, z, z);
             insert(d2, ret_orig ? t.orig_idx[s] : leaf);
         }
     }

@@ -85,6 +85,14 @@ struct Context {
     size_t         replay_cap   = 0;
     bool           last_fast    = false; // the last self-kNN call used the fast traversal
     TreeImpl       qsort;                   // sort scratch of external queries (fast knn)
+    void          *stage_idx[2]  = {nullptr, nullptr}; // device staging of host-output self-kNN
+    void          *stage_dist[2] = {nullptr, nullptr};
+    size_t         stage_cap     = 0;       // rows x k per staging buffer
+    int32_t       *iota          = nullptr; // leaf ranks 0 .. iota_cap-1
+    size_t         iota_cap      = 0;
+    cudaStream_t   copy_stream   = nullptr;
+    cudaEvent_t    ev_walked[2]  = {nullptr, nullptr};
+    cudaEvent_t    ev_copied[2]  = {nullptr, nullptr};
     float         *learned_feats = nullptr; // learned-bound scratch: features and bounds
     void          *learned_bound = nullptr;
     size_t         learned_cap   = 0;
@@ -157,6 +165,10 @@ void   free_scratch(TreeImpl &impl);
 void self_knn(Context &ctx, const ft_tree &tree, const int32_t *leaf_ids, size_t num, int k,
               bool exclude_self, uint64_t *idx, void *dist, const ft_query_options &q, cudaStream_t st,
               const void *bound = nullptr);
+// Self-kNN into host memory with the copy-out overlapped (chunks walked into two device
+// buffers in turn; copies on a second stream).
+void self_knn_to_host(Context &ctx, const ft_tree &tree, const int32_t *leaf_ids, size_t num, int k,
+                      bool exclude_self, uint64_t *h_idx, void *h_dist, const ft_query_options &q, cudaStream_t st);
 void knn(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz, size_t nq,
          int k, int max_k, uint64_t *idx, void *dist, const ft_query_options &q, cudaStream_t st);
 void range(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz,

@@ -650,6 +650,97 @@ void self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t n
     }
 }
 
+__global__ void iota_i32_kernel(int32_t *a, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i;
+}
+
+// Self-kNN whose outputs are host memory.  The leaves are walked in chunks into two device
+// buffers in turn; each chunk's rows go to the host on a second stream while the next chunk
+// is walked, so the copy-out (16 k bytes per query) overlaps the walk.  Pinned host memory
+// gives full overlap; with pageable memory the host waits for each chunk's copy while the
+// next chunk runs.  The caller's stream is complete when the last rows are in host memory.
+// Query statistics describe the last chunk.
+void self_knn_to_host(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, bool excl,
+                      uint64_t *h_idx, void *h_dist, const ft_query_options &qo, cudaStream_t st) {
+    const int max_k = qo.max_k > 0 ? qo.max_k : (leaf_ids ? 256 : 32);
+    if (k > max_k)
+        fail(FT_ERR_INVALID_ARGUMENT,
+             "k exceeds _MAX_K_ template parameter. Instantiate self_knn_query with larger _MAX_K_.");
+    if (tr.num_leaves == 0 || num == 0 || k <= 0) return;
+    if (k > kMaxExactK) fail(FT_ERR_RUNTIME, "self_knn_query: k too large for shared memory.");
+    if (num > (size_t)INT32_MAX) fail(FT_ERR_INVALID_ARGUMENT, "too many queries");
+    ft_query_options q = qo;
+    q.max_k            = max_k;
+    const size_t chunk = std::max<size_t>(size_t(1) << 18, (num + 15) / 16);
+    const size_t rows  = std::min(chunk, num);
+    auto ensure = [&](void *&p, size_t bytes) {
+        if (p) return;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+            fail(FT_ERR_OUT_OF_MEMORY, "cudaMalloc of the host-output staging buffers failed");
+        }
+    };
+    if (rows * (size_t)k > ctx.stage_cap) {
+        for (int b = 0; b < 2; ++b) {
+            if (ctx.stage_idx[b]) cudaFree(ctx.stage_idx[b]);
+            if (ctx.stage_dist[b]) cudaFree(ctx.stage_dist[b]);
+            ctx.stage_idx[b] = ctx.stage_dist[b] = nullptr;
+        }
+        ctx.stage_cap = 0;
+        for (int b = 0; b < 2; ++b) {
+            ensure(ctx.stage_idx[b], rows * (size_t)k * 8);
+            ensure(ctx.stage_dist[b], rows * (size_t)k * 8);
+        }
+        ctx.stage_cap = rows * (size_t)k;
+    }
+    if (!ctx.copy_stream) {
+        FT_CUDA(cudaStreamCreateWithFlags(&ctx.copy_stream, cudaStreamNonBlocking));
+        for (int b = 0; b < 2; ++b) {
+            FT_CUDA(cudaEventCreateWithFlags(&ctx.ev_walked[b], cudaEventDisableTiming));
+            FT_CUDA(cudaEventCreateWithFlags(&ctx.ev_copied[b], cudaEventDisableTiming));
+        }
+    }
+    const int32_t *ids = leaf_ids;
+    if (!ids) { // the full query: leaf ranks 0 .. num-1
+        if (num > ctx.iota_cap) {
+            if (ctx.iota) cudaFree(ctx.iota);
+            ctx.iota     = nullptr;
+            ctx.iota_cap = 0;
+            void *p      = nullptr;
+            ensure(p, num * sizeof(int32_t));
+            ctx.iota     = (int32_t *)p;
+            ctx.iota_cap = num;
+            iota_i32_kernel<<<(int)std::min<size_t>((num + 255) / 256, 148 * 16), 256, 0, st>>>(ctx.iota, (int)num);
+            FT_CUDA(cudaGetLastError());
+        }
+        ids = ctx.iota;
+    }
+    auto copy_out = [&](size_t c0, size_t cnt, int b) {
+        FT_CUDA(cudaStreamWaitEvent(ctx.copy_stream, ctx.ev_walked[b], 0));
+        FT_CUDA(cudaMemcpyAsync(h_idx + c0 * k, ctx.stage_idx[b], cnt * k * 8, cudaMemcpyDeviceToHost,
+                                ctx.copy_stream));
+        FT_CUDA(cudaMemcpyAsync((char *)h_dist + c0 * k * 8, ctx.stage_dist[b], cnt * k * 8, cudaMemcpyDeviceToHost,
+                                ctx.copy_stream));
+        FT_CUDA(cudaEventRecord(ctx.ev_copied[b], ctx.copy_stream));
+    };
+    size_t prev0 = 0, prevn = 0;
+    int    c     = 0;
+    for (size_t c0 = 0; c0 < num; c0 += rows, ++c) {
+        const size_t cnt = std::min(rows, num - c0);
+        const int    b   = c & 1;
+        if (c >= 2) FT_CUDA(cudaStreamWaitEvent(st, ctx.ev_copied[b], 0)); // buffer b's last rows are out
+        self_knn(ctx, tr, ids + c0, cnt, k, excl, (uint64_t *)ctx.stage_idx[b], ctx.stage_dist[b], q, st);
+        FT_CUDA(cudaEventRecord(ctx.ev_walked[b], st));
+        if (c >= 1) copy_out(prev0, prevn, b ^ 1); // the previous chunk, while this one is walked
+        prev0 = c0;
+        prevn = cnt;
+    }
+    copy_out(prev0, prevn, (c - 1) & 1);
+    FT_CUDA(cudaStreamWaitEvent(st, ctx.ev_copied[(c - 1) & 1], 0));
+}
+
 template <class T, int CAP, int QT, int PER>
 static void replay_t(const TreeDev<T> &tv, const BatchDev &bt, const int32_t *ranks, const int32_t *rows,
                      uint32_t *cnt, int k, bool excl, bool ro, uint64_t *idx, void *dist, uint32_t *status,

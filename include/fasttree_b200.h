@@ -149,9 +149,12 @@ ft_status ft_build_tree(ft_context *ctx, ft_tree *tree, const void *sorted_keys,
 /* ---------------------------------------------------------------------------------- */
 
 /* self_knn_query<MAXK> (leaf_ids == NULL, num = tree->num_leaves; src/hlbvh.hpp:1929-1954)
- * and self_knn_query_subset<MAXK> (src/hlbvh.hpp:1956-1983).  leaf_ids, idx_out, dist_out:
- * device.  Asynchronous on stream, like the reference.  k > max_k -> INVALID_ARGUMENT.
- * Default max_k: 32 for the full query, 256 for the subset. */
+ * and self_knn_query_subset<MAXK> (src/hlbvh.hpp:1956-1983).  leaf_ids: device.  idx_out,
+ * dist_out: both device, or both host memory (the reference requires USM here; host
+ * buffers are filled chunk by chunk through device staging, each chunk's copy-out
+ * overlapping the next chunk's walk -- pinned memory overlaps fully).  Asynchronous on
+ * stream, like the reference.  k > max_k -> INVALID_ARGUMENT.  Default max_k: 32 for the
+ * full query, 256 for the subset. */
 ft_status ft_self_knn(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_ids, size_t num,
                       int k, int exclude_self, uint64_t *idx_out, void *dist_out,
                       const ft_query_options *qopts, ft_stream_t stream);
