@@ -22,6 +22,8 @@ walk against the plain traversal).  --workload cfg5 runs the 50M-point k=64 work
 
 Multi-GPU: one process per GPU (torchrun); each rank builds and queries its own replica of
 the workload (independent point sets, no collective on the data path) -> weak scaling.
+With --shard every rank builds the same tree and answers a contiguous SFC range of its
+leaves (fasttree_b200/sharding.py) -> strong scaling.  Times are the maximum over ranks.
 
 --impl reference: the CPU restatement of the reference's algorithm (oracle/, the reference's
 SYCL build cannot be compiled here) timed on this host's cores on a bounded query sample.
@@ -64,6 +66,9 @@ def parse():
     p.add_argument("--only-headline", action="store_true")
     p.add_argument("--half", type=int, default=0, help="fast walk: SFC seeding half-window (0 = k)")
     p.add_argument("--variant", type=int, default=0, help="fast walk variant (0 = default)")
+    p.add_argument("--shard", action="store_true",
+                   help="N > 1: one tree on every rank, its queries split into contiguous SFC ranges (strong "
+                        "scaling); default: each rank its own point set (weak scaling)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-sample", type=int, default=200_000)
@@ -541,9 +546,19 @@ def run_ours(args):
     idx = torch.empty(n * k, dtype=torch.uint64, device=dev)
     dst = torch.empty(n * k, dtype=ft.dist_torch_dtype(ctx.coord), device=dev)
 
+    shard = args.shard and world > 1
+    if shard:  # this rank's contiguous share of the leaf ranks (same tree on every rank)
+        from fasttree_b200.sharding import shard_ranges
+        s0, s1 = shard_ranges(n, world)[rank]
+        shard_ids = torch.arange(s0, s1, dtype=torch.int32, device=dev)
+
     def query(method):
-        ft.self_knn_query(ctx, tree, k, idx, dst, exclude_self=True, max_k=max(32, k), method=method,
-                          half_window=args.half, variant=args.variant)
+        if shard:
+            ft.self_knn_query_subset(ctx, tree, shard_ids, k, idx, dst, exclude_self=True, max_k=max(32, k),
+                                     method=method)
+        else:
+            ft.self_knn_query(ctx, tree, k, idx, dst, exclude_self=True, max_k=max(32, k), method=method,
+                              half_window=args.half, variant=args.variant)
 
     def time_method(method):
         for _ in range(args.warmup):
@@ -575,11 +590,12 @@ def run_ours(args):
         results[m] = time_method(m)
     clocks = sampler.stop()
     ms_per_step, per_launch, stats = results[headline]
-    value = world * n / (ms_per_step / 1e3)
+    units = n if shard else world * n  # queries answered by all ranks in one step
+    value = units / (ms_per_step / 1e3)
     method = headline
     plain = None
     if 0 in results and headline != 0:
-        plain = {"value": world * n / (results[0][0] / 1e3), "unit": "queries/s", "ms_per_step": results[0][0],
+        plain = {"value": units / (results[0][0] / 1e3), "unit": "queries/s", "ms_per_step": results[0][0],
                  "kernel": "exact_knn_kernel (reference traversal and heap)"}
 
     # ---- e2e through the public API with host buffers ----
@@ -596,8 +612,12 @@ def run_ours(args):
             dx, dy, dz = (t.to(dev, non_blocking=True) for t in (hx, hy, hz))
             ft.build_bvh(ctx, ft.particles(dx, dy, dz), tree)
             # results straight into pinned host memory (the library overlaps the copy-out)
-            ft.self_knn_query(ctx, tree, k, hi, hd, exclude_self=True, max_k=max(32, k), method=method,
-                              half_window=args.half, variant=args.variant)
+            if shard:
+                ft.self_knn_query_subset(ctx, tree, shard_ids, k, hi, hd, exclude_self=True, max_k=max(32, k),
+                                         method=method)
+            else:
+                ft.self_knn_query(ctx, tree, k, hi, hd, exclude_self=True, max_k=max(32, k), method=method,
+                                  half_window=args.half, variant=args.variant)
         e1.record(stream)
         torch.cuda.synchronize()
         e_ms = e0.elapsed_time(e1) / e_steps
@@ -605,9 +625,9 @@ def run_ours(args):
         if world > 1:
             dist.all_reduce(te, op=dist.ReduceOp.MAX)
         e_ms = float(te.item())
-        e2e = {"value": world * n / (e_ms / 1e3), "unit": "queries/s",
-               "h2d_bytes_per_step": int(3 * n * x.element_size()),
-               "d2h_bytes_per_step": int(n * k * (idx.element_size() + dst.element_size())), "ms_per_step": e_ms}
+        e2e = {"value": units / (e_ms / 1e3), "unit": "queries/s",
+               "h2d_bytes_per_step": int(3 * world * n * x.element_size()),  # every rank uploads n points
+               "d2h_bytes_per_step": int(units * k * (idx.element_size() + dst.element_size())), "ms_per_step": e_ms}
 
     # ---- roofline of the self-kNN kernel (algorithmic bytes per launch / launch time) ----
     sc = x.element_size()
@@ -657,10 +677,12 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
-               "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+               "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+               "scaling": "strong" if shard else "weak",
                "vs_baseline": None, "dtype": w["dtype"], "data": "synthetic",
                "config": {"workload": w["name"], "n_points": n, "k": k, "exclude_self": True,
-                          "method": args.method, "parallelism": f"replicas x{world}",
+                          "method": args.method,
+                          "parallelism": f"query shards x{world}" if shard else f"replicas x{world}",
                           "l2": "inputs larger than L2: tree records + boxes ~2.3 GB, output 5.1 GB"},
                "plain": plain, "other_k_and_range": extra, "batched": batched, "learned": learned,
                "knn_query": knn_ext, "build_ms": build_ms, "tree_height": height, "query_stats": stats,

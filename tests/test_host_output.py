@@ -49,3 +49,21 @@ def test_mixed_placement_is_rejected():
     with pytest.raises(ValueError):
         ft.self_knn_query(ctx, tree, 4, torch.empty(4000, dtype=torch.uint64),
                           torch.empty(4000, dtype=torch.float64, device="cuda"))
+
+
+def test_sharded_rows_concatenate_to_the_full_query():
+    from fasttree_b200.sharding import sharded_self_knn
+    n, k = 300_000, 32
+    x, y, z = datasets.clustered_fixed(n, n_spheres=600, seed=7)
+    ctx = ft.Context("u64", "ph", periodic=True)
+    tree = ft.TreeSoA(ctx, n)
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree)
+    fi, fd = ft.self_knn_query(ctx, tree, k, method=1)
+    torch.cuda.synchronize()
+    costs = np.random.default_rng(1).lognormal(0, 1, n)
+    for world, c in ((3, None), (4, costs)):
+        parts = [sharded_self_knn(ctx, tree, k, r, world, costs=c) for r in range(world)]
+        torch.cuda.synchronize()
+        assert parts[0][0] == 0 and parts[-1][1] == n
+        assert torch.equal(torch.cat([p[2] for p in parts]), fi)
+        assert torch.equal(torch.cat([p[3] for p in parts]), fd)
