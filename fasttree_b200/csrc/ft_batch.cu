@@ -277,6 +277,23 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+template <class T>
+__global__ void __launch_bounds__(256)
+    batch_collapse_kernel(const long long *__restrict__ off, const long long *__restrict__ node_off,
+                          const long long *__restrict__ rec_off, int S, long long N, const int32_t *__restrict__ left,
+                          const int32_t *__restrict__ right, const T *mnx, const T *mxx, const T *mny, const T *mxy,
+                          const T *mnz, const T *mxz, WideRec<T> *wide) {
+    const long long total = rec_off[S];
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < N && g < total;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int       s  = find_set(rec_off, S, g);
+        const long long ro = rec_off[s], no = node_off[s];
+        const int       n  = (int)(off[s + 1] - off[s]);
+        const T *const  soa[6] = {mnx + no, mxx + no, mny + no, mxy + no, mnz + no, mxz + no};
+        collapse_node<T>((int)(g - ro), n, left + ro, right + ro, soa, wide + ro);
+    }
+}
+
 __global__ void batch_heights_kernel(const long long *__restrict__ off, const long long *__restrict__ rec_off, int S,
                                      const uint8_t *__restrict__ height, uint8_t *set_height) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x)
@@ -374,6 +391,7 @@ BatchImpl *batch_create(Context &ctx, size_t max_points, size_t max_sets) {
     s.height      = dalloc<uint8_t>(P);
     s.counters    = dalloc<int32_t>(P);
     s.leafcount   = dalloc<int32_t>(P);
+    s.wide        = dalloc<unsigned char>(P * wide_bytes(o.coord_type));
     s.key_lo      = (uint64_t *)dalloc<unsigned long long>(P);
     s.tmp_lo      = (uint64_t *)dalloc<unsigned long long>(P);
     s.perm        = dalloc<uint32_t>(P);
@@ -492,6 +510,8 @@ static void batch_build_typed(Context &ctx, BatchImpl &b, const long long *in_of
     batch_refit_kernel<T><<<gK, 256, 0, st>>>(b.off, b.node_off, b.rec_off, S, N, t.left_child, t.right_child,
                                               t.parent, mnx, mxx, mny, mxy, mnz, mxz, (NodeRec<T> *)s.recs, s.height,
                                               s.counters);
+    batch_collapse_kernel<T><<<gK, 256, 0, st>>>(b.off, b.node_off, b.rec_off, S, N, t.left_child, t.right_child,
+                                                 mnx, mxx, mny, mxy, mnz, mxz, (WideRec<T> *)s.wide);
     batch_heights_kernel<<<grid_of((size_t)S, 256, sm * 4), 256, 0, st>>>(b.off, b.rec_off, S, s.height,
                                                                           b.set_height);
     FT_CUDA(cudaGetLastError());
@@ -591,6 +611,7 @@ void batch_tree_view(Context &ctx, BatchImpl &b, size_t s, ft_tree &out, cudaStr
     v.recs           = (unsigned char *)b.scr.recs + (size_t)ro * 16 * cb;
     v.height         = b.scr.height + ro;
     v.leafcount      = b.scr.leafcount + ro;
+    v.wide           = (unsigned char *)b.scr.wide + (size_t)ro * wide_bytes(ctx.opts.coord_type);
     v.height_root    = n >= 2 ? (int)h : 0;
     v.clean42        = false;
     std::memset(&out, 0, sizeof(out));

@@ -405,6 +405,17 @@ __global__ void __launch_bounds__(256) refit_kernel(int n, const int32_t *__rest
         refit_leaf<T>(leaf, n, left, right, parent, soa, recs, height, counters);
 }
 
+// 4-wide records of every internal node (collapse_node), after the refit.
+template <class T>
+__global__ void __launch_bounds__(256) collapse_kernel(int n, const int32_t *__restrict__ left,
+                                                       const int32_t *__restrict__ right, const T *mnx,
+                                                       const T *mxx, const T *mny, const T *mxy, const T *mnz,
+                                                       const T *mxz, WideRec<T> *wide) {
+    const T *const soa[6] = {mnx, mxx, mny, mxy, mnz, mxz};
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n - 1; v += gridDim.x * blockDim.x)
+        collapse_node<T>(v, n, left, right, soa, wide);
+}
+
 // =========================================================================================
 // Host orchestration
 // =========================================================================================
@@ -426,8 +437,8 @@ template <class T> static void *alloc_dev(size_t count) {
 }
 
 void free_scratch(TreeImpl &s) {
-    void *ptrs[] = {s.recs, s.height, s.counters, s.leafcount, s.key_lo, s.key_hi, s.tmp_lo, s.tmp_hi, s.perm,
-                    s.tmp_perm, s.bbox, s.bbox_partial, s.hist, s.lookback, s.tile_counter, s.status};
+    void *ptrs[] = {s.recs, s.height, s.counters, s.leafcount, s.wide, s.key_lo, s.key_hi, s.tmp_lo, s.tmp_hi,
+                    s.perm, s.tmp_perm, s.bbox, s.bbox_partial, s.hist, s.lookback, s.tile_counter, s.status};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     int coord = s.coord;
@@ -452,6 +463,7 @@ void ensure_scratch(TreeImpl &s, const ft_options &o, size_t n) {
     s.height   = (uint8_t *)alloc_dev<uint8_t>(cap);
     s.counters = (int32_t *)alloc_dev<int32_t>(cap);
     s.leafcount = (int32_t *)alloc_dev<int32_t>(cap);
+    s.wide      = alloc_dev<unsigned char>((cap > 1 ? cap - 1 : 1) * wide_bytes(o.coord_type));
     s.key_lo   = (uint64_t *)alloc_dev<uint64_t>(cap);
     s.tmp_lo   = (uint64_t *)alloc_dev<uint64_t>(cap);
     if (W == 2) {
@@ -632,6 +644,8 @@ static void topology_and_refit(const ft_options &o, ft_tree &t, TreeImpl &s, siz
     SoA<T> a(t);
     refit_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, t.parent, a.mnx, a.mxx, a.mny,
                                             a.mxy, a.mnz, a.mxz, (NodeRec<T> *)s.recs, s.height, s.counters);
+    collapse_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, a.mnx, a.mxx, a.mny, a.mxy,
+                                               a.mnz, a.mxz, (WideRec<T> *)s.wide);
     FT_CUDA(cudaGetLastError());
 }
 

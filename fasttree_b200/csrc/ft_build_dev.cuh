@@ -284,4 +284,34 @@ FT_D void refit_leaf(int leaf, int n, const int32_t *__restrict__ left, const in
 }
 
 
+// =========================================================================================
+// 4-wide record of internal node v (the fast walk's node format): its grandchildren, where
+// a child that is a leaf stands for itself; boxes from the SoA arrays of the built tree.
+// =========================================================================================
+template <class T>
+FT_D void collapse_node(int v, int n, const int32_t *__restrict__ left, const int32_t *__restrict__ right,
+                        const T *const *soa, WideRec<T> *out) {
+    int       ch[4] = {-1, -1, -1, -1};
+    int       c     = 0;
+    const int l = left[v], r = right[v];
+    if (l >= n - 1) ch[c++] = l;
+    else {
+        ch[c++] = left[l];
+        ch[c++] = right[l];
+    }
+    if (r >= n - 1) ch[c++] = r;
+    else {
+        ch[c++] = left[r];
+        ch[c++] = right[r];
+    }
+    WideRec<T> w;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+#pragma unroll
+        for (int d = 0; d < 6; ++d) w.box[i][d] = ch[i] >= 0 ? soa[d][ch[i]] : T(0);
+        w.child[i] = ch[i];
+    }
+    out[v] = w;
+}
+
 } // namespace ft

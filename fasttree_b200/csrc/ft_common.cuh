@@ -178,6 +178,31 @@ template <class T> struct alignas(16 * sizeof(T)) NodeRec {
 static_assert(sizeof(NodeRec<float>) == 64, "record size");
 static_assert(sizeof(NodeRec<double>) == 128, "record size");
 
+// 4-wide record of an internal node for the fast walk: the node's grandchildren (a child
+// that is a leaf stands for itself), up to four boxes and their node indices (-1: absent).
+template <class T> struct alignas(16) WideRec {
+    T       box[4][6];
+    int32_t child[4];
+};
+static_assert(sizeof(WideRec<float>) == 112, "wide record size");
+static_assert(sizeof(WideRec<double>) == 208, "wide record size");
+
+template <class T> FT_D void load_wide(const WideRec<T> *w, int node, T b[4][6], int c[4]) {
+    constexpr int NW = (int)(sizeof(WideRec<T>) / 16);
+    const uint4  *p  = reinterpret_cast<const uint4 *>(w + node);
+    uint4         v[NW];
+#pragma unroll
+    for (int i = 0; i < NW; ++i) v[i] = __ldg(p + i);
+    const T *f = reinterpret_cast<const T *>(v);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int d = 0; d < 6; ++d) b[i][d] = f[6 * i + d];
+    const int32_t *ci = reinterpret_cast<const int32_t *>(f + 24);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) c[i] = ci[i];
+}
+
 template <class T> FT_D void load_rec(const NodeRec<T> *recs, int node, T lb[6], T rb[6], int &l, int &r) {
     const uint4 *p = reinterpret_cast<const uint4 *>(recs + node);
     if constexpr (sizeof(T) == 8) {
@@ -230,6 +255,7 @@ template <class T> struct TreeDev {
     const NodeRec<T> *recs;
     const uint8_t    *height; // subtree height of each internal node
     const int32_t    *leaves; // leaf count of each internal node
+    const WideRec<T> *wide;   // 4-wide record of each internal node
     int               n;      // leaves
 };
 
@@ -246,6 +272,7 @@ template <class T> inline TreeDev<T> tree_view(const ft_tree &tr) {
     v.recs     = (const NodeRec<T> *)((TreeImpl *)tr.impl)->recs;
     v.height   = ((TreeImpl *)tr.impl)->height;
     v.leaves   = ((TreeImpl *)tr.impl)->leafcount;
+    v.wide     = (const WideRec<T> *)((TreeImpl *)tr.impl)->wide;
     v.n        = (int)tr.num_leaves;
     return v;
 }
@@ -277,6 +304,7 @@ template <class T> FT_D TreeDev<T> set_view(const TreeDev<T> &all, const BatchDe
     t.recs     = all.recs + rb;
     t.height   = all.height + rb;
     t.leaves   = all.leaves + rb;
+    t.wide     = all.wide + rb;
     t.n        = (int)(b.off[s + 1] - b.off[s]);
     return t;
 }

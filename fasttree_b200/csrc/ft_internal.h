@@ -34,6 +34,7 @@ struct TreeImpl {
     uint8_t  *height       = nullptr; // subtree height of internal nodes
     int32_t  *counters     = nullptr; // refit arrival counters
     int32_t  *leafcount    = nullptr; // leaves under each internal node (Karras range size)
+    void     *wide         = nullptr; // WideRec<T>[cap-1]: grandchildren of each internal node
     uint64_t *key_lo       = nullptr; // sorted keys (low word)
     uint64_t *key_hi       = nullptr; // sorted keys (high word, 126-bit keys only)
     uint64_t *tmp_lo       = nullptr; // sort ping-pong
@@ -176,6 +177,7 @@ void range(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, co
            int max_per_q, cudaStream_t st);
 
 size_t coord_bytes(int coord);
+inline size_t wide_bytes(int coord) { return coord_bytes(coord) == 8 ? 208 : 112; } // sizeof(WideRec<T>)
 
 // ---- batched sets (ft_batch.cu) ----
 struct BatchImpl;

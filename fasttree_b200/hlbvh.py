@@ -341,7 +341,7 @@ def build_tree(ctx: Context, tree: TreeSoA, sorted_keys, sorted_x=None, sorted_y
 def _qopts(max_k: int, method: int = 0, half_window: int = 0, variant: int = 0):
     o = capi.FtQueryOptions(int(max_k), int(method))
     o.reserved[0] = int(half_window)  # fast walk: SFC seeding half-window (0 = k)
-    o.reserved[1] = int(variant)      # fast walk: 0 warp-shared order, 1 per-lane order
+    o.reserved[1] = int(variant)      # fast walk: 0 default (4-wide), 1 per-lane, 2 compact, 3 warp-shared, 4 4-wide
     return o
 
 

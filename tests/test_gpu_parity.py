@@ -244,6 +244,23 @@ def test_fast_self_knn_matches_oracle(cfg, kind, k):
             assert stats["replayed"] > 0  # duplicate points force the exact replay
 
 
+@pytest.mark.parametrize("cfg", CONFIGS, ids=CONFIG_IDS)
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+def test_fast_walk_variants_match_oracle(cfg, variant):
+    """Every walk of the fast path (1 per-lane, 2 compact per-lane, 3 warp-shared, 4 over the
+    4-wide records) gives the reference's output, ties included."""
+    coord, sfc, per = cfg
+    ctx, opts = make(coord, sfc, per)
+    for kind, k in (("clustered", 32), ("degenerate", 16), ("uniform", 64)):
+        x, y, z = gen(kind, 5000, coord, seed=23)
+        tree, ot = build_both(ctx, opts, x, y, z)
+        gi, gd = ft.self_knn_query(ctx, tree, k, max_k=max(k, 32), method=1, variant=variant)
+        torch.cuda.synchronize()
+        oi, od = O.self_knn(opts, ot, k, True)
+        assert np.array_equal(gi.cpu().numpy(), oi), (kind, k)
+        assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od)), (kind, k)
+
+
 @pytest.mark.parametrize("cfg", [CONFIGS[1], CONFIGS[7]], ids=[CONFIG_IDS[1], CONFIG_IDS[7]])
 def test_fast_self_knn_subset_and_orig(cfg):
     coord, sfc, per = cfg
