@@ -301,11 +301,21 @@ inline void build_bvh(queue &q, const particles<coord_t> &p, TreeSoA &tree, Boun
 }
 
 // ---- queries -----------------------------------------------------------------------------
+// The kNN queries take the fast walk (SFC-window seeding, exact replay of tied queries):
+// its output is bit-identical to the reference traversal's.  Define
+// FASTTREE_B200_PLAIN_TRAVERSAL to run the reference traversal itself.
+#if defined(FASTTREE_B200_PLAIN_TRAVERSAL)
+inline constexpr int kQueryMethod = 0;
+#else
+inline constexpr int kQueryMethod = 1;
+#endif
+
 template <int _MAX_K_ = 256>
 inline void knn_query(queue &q, const TreeSoA &tree, const coord_t *qx, const coord_t *qy, const coord_t *qz, int k,
                       int num_queries, size_t *results, dist_t *result_dists) {
     ft_query_options o{};
-    o.max_k = _MAX_K_;
+    o.max_k  = _MAX_K_;
+    o.method = kQueryMethod;
     check(ft_knn(q.context(), tree.handle, qx, qy, qz, (size_t)num_queries, k, reinterpret_cast<uint64_t *>(results),
                  result_dists, &o, q.stream()));
 }
@@ -314,7 +324,8 @@ template <int _MAX_K_ = 32>
 inline void self_knn_query(queue &q, const TreeSoA &tree, int k, size_t *results, dist_t *result_dists,
                            bool exclude_self = true) {
     ft_query_options o{};
-    o.max_k = _MAX_K_;
+    o.max_k  = _MAX_K_;
+    o.method = kQueryMethod;
     check(ft_self_knn(q.context(), tree.handle, nullptr, tree.num_leaves, k, exclude_self ? 1 : 0,
                       reinterpret_cast<uint64_t *>(results), result_dists, &o, q.stream()));
 }
@@ -324,7 +335,8 @@ inline void self_knn_query_subset(queue &q, const TreeSoA &tree, const int *leaf
                                   size_t *results, dist_t *result_dists, bool exclude_self = true) {
     if (num_ids == 0) return;
     ft_query_options o{};
-    o.max_k = _MAX_K_;
+    o.max_k  = _MAX_K_;
+    o.method = kQueryMethod;
     check(ft_self_knn(q.context(), tree.handle, leaf_ids, (size_t)num_ids, k, exclude_self ? 1 : 0,
                       reinterpret_cast<uint64_t *>(results), result_dists, &o, q.stream()));
 }

@@ -19,6 +19,10 @@ CONFIGS = {
     "ph_u64_per": ["-DSFC_TYPE_PEANO_HILBERT", "-DFASTTREE_INTEGER_COORDS", "-DPOSITIONS_IN_64BIT", "-DPERIODIC_BC"],
     "ph_u64_per_orig": ["-DSFC_TYPE_PEANO_HILBERT", "-DFASTTREE_INTEGER_COORDS", "-DPOSITIONS_IN_64BIT",
                         "-DPERIODIC_BC", "-DRETURN_ORIG_INDICES"],
+    # the header's default is the fast walk; this one runs the reference traversal itself
+    "ph_u64_per_plain": ["-DSFC_TYPE_PEANO_HILBERT", "-DFASTTREE_INTEGER_COORDS", "-DPOSITIONS_IN_64BIT",
+                         "-DPERIODIC_BC", "-DFASTTREE_B200_PLAIN_TRAVERSAL"],
+    "morton_f64_plain": ["-DSFC_TYPE_MORTON", "-DCOORDS_TYPE_DOUBLE", "-DFASTTREE_B200_PLAIN_TRAVERSAL"],
 }
 
 
