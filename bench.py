@@ -240,9 +240,28 @@ def run_knn_external(args, stream):
         ms = e0.elapsed_time(e1) / steps
         res["fast" if method else "plain"] = {"ms_per_step": ms, "value": nq / (ms / 1e3), "unit": "queries/s"}
         if method:
-            res["fast"]["replayed"] = ctx.query_stats()["replayed"]
+            st = ctx.query_stats()
+            res["fast"]["replayed"] = st["replayed"]
+            res["fast"]["visits_per_query"] = st["visits"] / nq
             fi = idx.clone()
     res["bit_exact"] = bool(torch.equal(fi, idx))
+    pi = idx.clone()
+    # learned bound: network trained on the exact self-kNN of a separate 100K uniform draw
+    from fasttree_b200 import learned as L
+    tx, ty, tz = datasets.uniform(100_000, seed=11)
+    t0 = time.perf_counter()
+    model, _ = L.train_bound(ctx, tx, ty, tz, k, steps=1000, batch=8192, lr=3e-3, seed=0)
+    torch.cuda.synchronize()
+    learned = {"train_draw": "100K uniform float64 (seed 11), 1000 Adam steps",
+               "train_s": time.perf_counter() - t0, "by_inflation": {}}
+    for infl in (1.15, 1.3):
+        ms = _timed(stream, lambda: L.knn_query_learned(ctx, tree, model, *dq, k, idx, dst, inflation=infl,
+                                                        max_k=mk), 3)
+        st = ctx.query_stats()
+        learned["by_inflation"][str(infl)] = {"ms_per_step": ms, "value": nq / (ms / 1e3), "unit": "queries/s",
+                                              "replayed": st["replayed"], "visits_per_query": st["visits"] / nq,
+                                              "bit_exact": bool(torch.equal(pi, idx))}
+    res["learned"] = learned
     res["workload"] = "1M external queries on 100K uniform float64, Morton, k=64, MAXK=256 (SortedMergeHeap)"
     return res
 

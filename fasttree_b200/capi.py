@@ -25,7 +25,8 @@ EXPORTED = (
     "ft_batch_tree", "ft_batch_set_info", "ft_batch_query_stats",
     "ft_bound_model_create", "ft_bound_model_destroy", "ft_bound_model_get_params", "ft_bound_model_set_params",
     "ft_bound_model_set_norm", "ft_bound_features", "ft_bound_targets", "ft_bound_model_gradient",
-    "ft_bound_model_fit", "ft_bound_model_predict", "ft_self_knn_learned",
+    "ft_bound_model_fit", "ft_bound_model_predict", "ft_self_knn_learned", "ft_bound_features_points",
+    "ft_knn_learned",
 )
 
 
@@ -100,6 +101,9 @@ _SIGS = {
     "ft_bound_model_predict": [_vp, _vp, _vp, _sz, ctypes.c_float, _vp, _vp, _st],
     "ft_self_knn_learned": [_vp, ctypes.POINTER(FtTree), _vp, _vp, _sz, _i, _i, ctypes.c_float, _vp, _vp,
                             ctypes.POINTER(FtQueryOptions), _st],
+    "ft_bound_features_points": [_vp, ctypes.POINTER(FtTree), _vp, _vp, _vp, _sz, _i, _vp, _st],
+    "ft_knn_learned": [_vp, ctypes.POINTER(FtTree), _vp, _vp, _vp, _vp, _sz, _i, ctypes.c_float, _vp, _vp,
+                       ctypes.POINTER(FtQueryOptions), _st],
 }
 
 

@@ -728,6 +728,53 @@ ft_status ft_bound_model_predict(ft_context *ctx, ft_bound_model *model, const f
     FT_API_END
 }
 
+ft_status ft_bound_features_points(ft_context *ctx, const ft_tree *tree, const void *qx, const void *qy,
+                                   const void *qz, size_t num_queries, int k, float *features_out,
+                                   ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree, "null argument");
+    need(num_queries <= (size_t)INT32_MAX, "too many queries");
+    if (num_queries > 0) need(qx && qy && qz && features_out, "null array argument");
+    need_device(qx, "qx");
+    need_device(qy, "qy");
+    need_device(qz, "qz");
+    need_device(features_out, "features_out");
+    DeviceGuard g(ctx->device);
+    ft::bound_features_points(*ctx, *tree, qx, qy, qz, num_queries, k, features_out, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_knn_learned(ft_context *ctx, const ft_tree *tree, ft_bound_model *model, const void *qx,
+                         const void *qy, const void *qz, size_t num_queries, int k, float inflation,
+                         uint64_t *idx_out, void *dist_out, const ft_query_options *qopts, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree && model, "null argument");
+    ft_query_options q{};
+    if (qopts) q = *qopts;
+    if (tree->num_leaves == 0 || num_queries == 0 || k <= 0) return FT_OK;
+    need(qx && qy && qz && idx_out && dist_out, "null argument");
+    need(num_queries <= (size_t)INT32_MAX, "too many queries");
+    const int max_k = q.max_k > 0 ? q.max_k : 256;
+    if ((max_k > 32 && k > 32 && k > max_k) || (max_k <= 32 && k > 32))
+        fail(FT_ERR_INVALID_ARGUMENT, "k exceeds _MAX_K_ template parameter. Instantiate knn_query with larger _MAX_K_.");
+    DeviceGuard  g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t       cb = coord_bytes(ctx->opts.coord_type);
+    size_t       nk = num_queries * (size_t)k;
+    Staged       sx, sy, sz, si, sd;
+    sx.init(qx, num_queries * cb, true, false, st);
+    sy.init(qy, num_queries * cb, true, false, st);
+    sz.init(qz, num_queries * cb, true, false, st);
+    si.init(idx_out, nk * 8, false, true, st);
+    sd.init(dist_out, nk * 8, false, true, st);
+    ft::knn_learned(*ctx, *tree, *model->impl, sx.dev, sy.dev, sz.dev, num_queries, k, max_k, inflation,
+                    (uint64_t *)si.dev, sd.dev, q, st);
+    si.copy_back();
+    sd.copy_back();
+    check_device_status(ctx->status, st);
+    FT_API_END
+}
+
 ft_status ft_self_knn_learned(ft_context *ctx, const ft_tree *tree, ft_bound_model *model, const int32_t *leaf_ids,
                               size_t num, int k, int exclude_self, float inflation, uint64_t *idx_out,
                               void *dist_out, const ft_query_options *qopts, ft_stream_t stream) {

@@ -682,6 +682,11 @@ static bool compute_seed_ranks(Context &ctx, const ft_tree &tr, const void *qx, 
     return true;
 }
 
+void query_seed_ranks(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz, size_t nq,
+                      cudaStream_t st) {
+    compute_seed_ranks(ctx, tr, qx, qy, qz, nq, st);
+}
+
 // Query order by SFC rank (ctx.seed_ranks must hold the ranks): sorts (rank, index) pairs.
 static const uint32_t *order_by_rank(Context &ctx, size_t nq, int n, cudaStream_t st) {
     ensure_query_sort(ctx, nq);
@@ -705,7 +710,7 @@ const uint32_t *sfc_query_order(Context &ctx, const ft_tree &tr, const void *qx,
 }
 
 bool fast_knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz, size_t nq, int k,
-              int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st) {
+              int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st, const void *bound) {
     TreeImpl *impl = (TreeImpl *)tr.impl;
     if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0 || impl->height_root > 62) return false;
     // SortedMergeHeap with k equal to its capacity keeps the first k leaves it meets, not the
@@ -726,10 +731,10 @@ bool fast_knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, c
     if (ranked && nq > 1) eq.order = order_by_rank(ctx, nq, n, st); // walk the queries in SFC order
     const int variant = walk_variant(0, k);
     switch (ctx.opts.coord_type) {
-    case F32: launch_fast<float>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, nullptr, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
-    case F64: launch_fast<double>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, nullptr, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
-    case U32: launch_fast<uint32_t>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, nullptr, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
-    case U64: launch_fast<unsigned long long>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, nullptr, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
+    case F32: launch_fast<float>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
+    case F64: launch_fast<double>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
+    case U32: launch_fast<uint32_t>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
+    case U64: launch_fast<unsigned long long>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
     }
     replay_external(ctx, tr, qx, qy, qz, ctx.replay_rows, rc, k, max_k, idx, dist, st);
     return true;

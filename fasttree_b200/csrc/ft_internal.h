@@ -133,7 +133,10 @@ void free_query_sort(Context &ctx);
 const uint32_t *sfc_query_order(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz,
                                 size_t nq, cudaStream_t st);
 bool fast_knn(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz, size_t nq, int k,
-              int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st);
+              int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st, const void *bound = nullptr);
+// SFC rank of each external query point in ctx.seed_ranks (-1 without this library's keys).
+void query_seed_ranks(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz, size_t nq,
+                      cudaStream_t st);
 // Reruns listed external queries (rows, *count_dev of them) with knn_query's heap tier.
 void replay_external(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz,
                      const int32_t *rows, uint32_t *count_dev, int k, int max_k, uint64_t *idx, void *dist,
@@ -170,8 +173,10 @@ void self_knn(Context &ctx, const ft_tree &tree, const int32_t *leaf_ids, size_t
 // buffers in turn; copies on a second stream).
 void self_knn_to_host(Context &ctx, const ft_tree &tree, const int32_t *leaf_ids, size_t num, int k,
                       bool exclude_self, uint64_t *h_idx, void *h_dist, const ft_query_options &q, cudaStream_t st);
+// bound: optional per-query pruning bound (device, dist units); it selects the fast walk.
 void knn(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz, size_t nq,
-         int k, int max_k, uint64_t *idx, void *dist, const ft_query_options &q, cudaStream_t st);
+         int k, int max_k, uint64_t *idx, void *dist, const ft_query_options &q, cudaStream_t st,
+         const void *bound = nullptr);
 void range(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz,
            const void *rmin, const void *rmax, size_t nq, int32_t *results, int32_t *counts,
            int max_per_q, cudaStream_t st);
@@ -213,6 +218,11 @@ void        bound_model_fit(BoundModel &b, const float *feats, const float *targ
                             float lr, unsigned long long seed, float *loss_host, cudaStream_t st);
 void        bound_model_predict(Context &ctx, BoundModel &b, const float *feats, size_t n, float inflation,
                                 float *pred, void *bound, cudaStream_t st);
+void        bound_features_points(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
+                                  size_t nq, int k, float *out, cudaStream_t st);
+void        knn_learned(Context &ctx, const ft_tree &tr, BoundModel &b, const void *qx, const void *qy,
+                        const void *qz, size_t nq, int k, int max_k, float inflation, uint64_t *idx, void *dist,
+                        const ft_query_options &q, cudaStream_t st);
 void        self_knn_learned(Context &ctx, const ft_tree &tr, BoundModel &b, const int32_t *leaf_ids, size_t num,
                              int k, bool exclude_self, float inflation, uint64_t *idx, void *dist,
                              const ft_query_options &q, cudaStream_t st);

@@ -153,13 +153,18 @@ template <class T, int PER>
 __global__ void __launch_bounds__(kFeatThreads)
     bound_features_kernel(TreeDev<T> t, const int32_t *__restrict__ parent, const unsigned long long *klo,
                           const unsigned long long *khi, const int32_t *__restrict__ leaf_ids, int num, int k,
+                          const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
                           float *__restrict__ out, uint32_t *status) {
     using D = typename Coord<T>::dist_t;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= num) return;
-    const int n    = t.n;
-    const int rank = leaf_ids ? leaf_ids[q] : q;
-    float    *f    = out + (size_t)q * kFeat;
+    const int  n   = t.n;
+    // external query points (qx != null): leaf_ids holds each point's SFC rank (the lower
+    // bound of its key among the sorted keys); the leaf there stands for the point, and the
+    // window is the 2k leaves [r - k, r + k) seen from the point itself
+    const bool ext  = qx != nullptr;
+    const int  rank = ext ? min(max(leaf_ids[q], 0), n - 1) : (leaf_ids ? leaf_ids[q] : q);
+    float     *f    = out + (size_t)q * kFeat;
     if (rank < 0 || rank >= n) {
         atomicOr(status, STATUS_BAD_INPUT);
         for (int i = 0; i < kFeat; ++i) f[i] = 0.0f;
@@ -184,9 +189,9 @@ __global__ void __launch_bounds__(kFeatThreads)
     f[9] = (float)log2((double)k);
 
     // k-th and ceil(k/2)-th nearest distance in the SFC window
-    const T   px = t.min_x[slot], py = t.min_y[slot], pz = t.min_z[slot];
+    const T   px = ext ? qx[q] : t.min_x[slot], py = ext ? qy[q] : t.min_y[slot], pz = ext ? qz[q] : t.min_z[slot];
     const int kk = min(k, kMaxBoundK);
-    const int r0 = max(0, rank - k), r1 = min(n - 1, rank + k);
+    const int r0 = max(0, rank - k), r1 = min(n - 1, ext ? rank + k - 1 : rank + k);
     auto      wdist = [&](int j) -> float {
         const int s = j + n - 1;
         return (float)Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, t.min_x[s], t.max_x[s],
@@ -199,11 +204,11 @@ __global__ void __launch_bounds__(kFeatThreads)
         float v[64];
 #pragma unroll
         for (int i = 0; i < 64; ++i) {
-            const int j = rank - k + (i < k ? i : i + 1); // skips the query itself
+            const int j = rank - k + ((i < k || ext) ? i : i + 1); // a self query skips its own leaf
             v[i]        = (i < 2 * k && j >= r0 && j <= r1) ? wdist(j) : __int_as_float(0x7f800000);
         }
         bitonic_sort64(v);
-        const int cnt = (r1 - r0); // window leaves other than the query
+        const int cnt = ext ? (r1 - r0 + 1) : (r1 - r0); // window leaves other than a self query's own
         if (cnt > 0) {
             const int m = min(kk, cnt);
             wk          = pick64(v, m - 1);
@@ -214,7 +219,7 @@ __global__ void __launch_bounds__(kFeatThreads)
         float hp[kMaxBoundK];
         int   cnt = 0;
         for (int j = r0; j <= r1; ++j) {
-            if (j == rank) continue;
+            if (j == rank && !ext) continue;
             const float vv = wdist(j);
             if (cnt < kk) { // sift up
                 int i = cnt++;
@@ -953,32 +958,56 @@ void bound_model_predict(Context &ctx, BoundModel &b, const float *feats, size_t
 }
 
 template <class T>
-static void features_typed(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, int num, int k, float *out,
-                           cudaStream_t st) {
+static void features_typed(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, int num, int k, const void *qx,
+                           const void *qy, const void *qz, float *out, cudaStream_t st) {
     const TreeImpl &impl = *(const TreeImpl *)tr.impl;
     TreeDev<T>      tv   = tree_view<T>(tr);
     const int       grid = (num + kFeatThreads - 1) / kFeatThreads;
     met_dispatch<T>(metric_mode<T>(ctx.opts, tr), [&](auto M) {
         bound_features_kernel<T, decltype(M)::value><<<grid, kFeatThreads, 0, st>>>(
             tv, tr.parent, (const unsigned long long *)impl.key_lo, (const unsigned long long *)impl.key_hi, leaf_ids,
-            num, k, out, ctx.status);
+            num, k, (const T *)qx, (const T *)qy, (const T *)qz, out, ctx.status);
     });
     FT_CUDA(cudaGetLastError());
 }
 
-void bound_features(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, float *out,
-                    cudaStream_t st) {
+// leaf_ids: self queries (null: every leaf); or, with qx/qy/qz, the SFC ranks of external
+// query points.
+static void features_impl(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k,
+                          const void *qx, const void *qy, const void *qz, float *out, cudaStream_t st) {
+    switch (ctx.opts.coord_type) {
+    case F32: features_typed<float>(ctx, tr, leaf_ids, (int)num, k, qx, qy, qz, out, st); break;
+    case F64: features_typed<double>(ctx, tr, leaf_ids, (int)num, k, qx, qy, qz, out, st); break;
+    case U32: features_typed<uint32_t>(ctx, tr, leaf_ids, (int)num, k, qx, qy, qz, out, st); break;
+    case U64: features_typed<unsigned long long>(ctx, tr, leaf_ids, (int)num, k, qx, qy, qz, out, st); break;
+    }
+}
+
+static void check_bound_tree(const ft_tree &tr, int k) {
     const TreeImpl *impl = (const TreeImpl *)tr.impl;
     if (k < 1 || k > kMaxBoundK) fail(FT_ERR_INVALID_ARGUMENT, "learned bound: k must be in [1, 64]");
     if (!impl || impl->view || !impl->key_lo || impl->height_root < 0)
         fail(FT_ERR_INVALID_ARGUMENT, "learned bound: the tree must be built by ft_build_bvh / ft_build_tree");
+}
+
+void bound_features(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, float *out,
+                    cudaStream_t st) {
+    check_bound_tree(tr, k);
     if (num == 0 || tr.num_leaves == 0) return;
-    switch (ctx.opts.coord_type) {
-    case F32: features_typed<float>(ctx, tr, leaf_ids, (int)num, k, out, st); break;
-    case F64: features_typed<double>(ctx, tr, leaf_ids, (int)num, k, out, st); break;
-    case U32: features_typed<uint32_t>(ctx, tr, leaf_ids, (int)num, k, out, st); break;
-    case U64: features_typed<unsigned long long>(ctx, tr, leaf_ids, (int)num, k, out, st); break;
-    }
+    features_impl(ctx, tr, leaf_ids, num, k, nullptr, nullptr, nullptr, out, st);
+}
+
+// Features of external query points: their SFC ranks first (the tree's own keys), then the
+// features seen from each point.
+void bound_features_points(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
+                           size_t nq, int k, float *out, cudaStream_t st) {
+    check_bound_tree(tr, k);
+    if (!((const TreeImpl *)tr.impl)->own_keys)
+        fail(FT_ERR_INVALID_ARGUMENT, "learned bound: the tree's keys must be this library's (ft_build_bvh "
+                                      "without caller keys) to place external points");
+    if (nq == 0 || tr.num_leaves == 0) return;
+    query_seed_ranks(ctx, tr, qx, qy, qz, nq, st);
+    features_impl(ctx, tr, ctx.seed_ranks, nq, k, qx, qy, qz, out, st);
 }
 
 void bound_targets(Context &ctx, const uint64_t *idx, const void *dist, size_t num, int k, float *out,
@@ -995,23 +1024,42 @@ void bound_targets(Context &ctx, const uint64_t *idx, const void *dist, size_t n
     FT_CUDA(cudaGetLastError());
 }
 
+static void ensure_learned(Context &ctx, size_t num) {
+    if (num <= ctx.learned_cap) return;
+    if (ctx.learned_feats) cudaFree(ctx.learned_feats);
+    if (ctx.learned_bound) cudaFree(ctx.learned_bound);
+    ctx.learned_feats = nullptr;
+    ctx.learned_bound = nullptr;
+    ctx.learned_cap   = 0;
+    const size_t cap  = num + num / 4 + 1024;
+    ctx.learned_feats = dmalloc<float>(cap * kFeat);
+    ctx.learned_bound = dmalloc<unsigned long long>(cap);
+    ctx.learned_cap   = cap;
+}
+
+// knn_query of external points with the learned bound: features (from each point's SFC
+// rank) -> bound -> the fast walk with the bound; misses and ties are rerun by knn_query's
+// heap tier, so the output equals knn_query's.
+void knn_learned(Context &ctx, const ft_tree &tr, BoundModel &b, const void *qx, const void *qy, const void *qz,
+                 size_t nq, int k, int max_k, float inflation, uint64_t *idx, void *dist, const ft_query_options &q,
+                 cudaStream_t st) {
+    if (nq == 0 || k <= 0 || tr.num_leaves == 0) return;
+    if (k > kMaxBoundK) fail(FT_ERR_INVALID_ARGUMENT, "learned bound: k must be in [1, 64]");
+    ensure_learned(ctx, nq);
+    bound_features_points(ctx, tr, qx, qy, qz, nq, k, ctx.learned_feats, st);
+    bound_model_predict(ctx, b, ctx.learned_feats, nq, inflation, nullptr, ctx.learned_bound, st);
+    ft_query_options qb = q;
+    qb.method           = 1;
+    knn(ctx, tr, qx, qy, qz, nq, k, max_k, idx, dist, qb, st, ctx.learned_bound);
+}
+
 // Features -> bound -> bounded fast walk; scratch grows in the context.
 void self_knn_learned(Context &ctx, const ft_tree &tr, BoundModel &b, const int32_t *leaf_ids, size_t num, int k,
                       bool excl, float inflation, uint64_t *idx, void *dist, const ft_query_options &q,
                       cudaStream_t st) {
     if (num == 0 || k <= 0 || tr.num_leaves == 0) return;
     if (k > kMaxBoundK) fail(FT_ERR_INVALID_ARGUMENT, "learned bound: k must be in [1, 64]");
-    if (num > ctx.learned_cap) {
-        if (ctx.learned_feats) cudaFree(ctx.learned_feats);
-        if (ctx.learned_bound) cudaFree(ctx.learned_bound);
-        ctx.learned_feats = nullptr;
-        ctx.learned_bound = nullptr;
-        ctx.learned_cap   = 0;
-        const size_t cap  = num + num / 4 + 1024;
-        ctx.learned_feats = dmalloc<float>(cap * kFeat);
-        ctx.learned_bound = dmalloc<unsigned long long>(cap);
-        ctx.learned_cap   = cap;
-    }
+    ensure_learned(ctx, num);
     bound_features(ctx, tr, leaf_ids, num, k, ctx.learned_feats, st);
     bound_model_predict(ctx, b, ctx.learned_feats, num, inflation, nullptr, ctx.learned_bound, st);
     self_knn(ctx, tr, leaf_ids, num, k, excl, idx, dist, q, st, ctx.learned_bound);

@@ -869,7 +869,7 @@ void replay_external(Context &ctx, const ft_tree &tr, const void *qx, const void
 }
 
 void knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz, size_t nq, int k, int max_k,
-         uint64_t *idx, void *dist, const ft_query_options &qo, cudaStream_t st) {
+         uint64_t *idx, void *dist, const ft_query_options &qo, cudaStream_t st, const void *bound) {
     if (max_k <= 0) max_k = 256;
     if (tr.num_leaves == 0 || nq == 0 || k <= 0) return;
     if (max_k > 32 && k > 32 && k > max_k)
@@ -881,7 +881,7 @@ void knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const 
     ctx.stats.queries  = (int64_t)nq;
     ctx.stats.replayed = 0;
     ctx.last_fast      = false;
-    if (qo.method == 1 && fast_knn(ctx, tr, qx, qy, qz, nq, k, max_k, idx, dist, qo.reserved[0], st)) {
+    if ((qo.method == 1 || bound) && fast_knn(ctx, tr, qx, qy, qz, nq, k, max_k, idx, dist, qo.reserved[0], st, bound)) {
         ctx.last_fast = true;
         return;
     }

@@ -16,8 +16,8 @@ import torch
 
 from . import capi
 from .capi import lib
-from .hlbvh import (Context, TreeSoA, _alloc_knn_out, _call, _ptr, _qopts, _rows, _stream_handle, build_bvh,
-                    dist_torch_dtype, particles, self_knn_query)
+from .hlbvh import (Context, TreeSoA, _alloc_knn_out, _as_coord, _call, _ptr, _qopts, _rows, _stream_handle,
+                    build_bvh, dist_torch_dtype, particles, self_knn_query)
 
 N_FEATURES = 12
 N_PARAMS = 5057
@@ -153,3 +153,26 @@ def self_knn_query_learned(ctx: Context, tree: TreeSoA, model: BoundModel, k: in
                                     int(bool(exclude_self)), ctypes.c_float(inflation), _ptr(results),
                                     _ptr(result_dists), ctypes.byref(_qopts(max_k, 1)), _stream_handle(stream)))
     return _rows(results, num, k), _rows(result_dists, num, k)
+
+
+def features_points(ctx: Context, tree: TreeSoA, qx, qy, qz, k: int, stream=None) -> torch.Tensor:
+    """(nq, 12) float32 features of external query points."""
+    x, y, z = (torch.as_tensor(_as_coord(a, ctx.coord)).to(f"cuda:{ctx.device}") for a in (qx, qy, qz))
+    nq = len(x)
+    out = torch.empty((nq, N_FEATURES), dtype=torch.float32, device=f"cuda:{ctx.device}")
+    _call(lib().ft_bound_features_points(ctx.handle, tree.c, _ptr(x), _ptr(y), _ptr(z), nq, int(k),
+                                         _ptr(out) if nq else None, _stream_handle(stream)))
+    return out
+
+
+def knn_query_learned(ctx: Context, tree: TreeSoA, model: BoundModel, qx, qy, qz, k: int, results=None,
+                      result_dists=None, inflation: float = 1.3, max_k: int = 256, stream=None):
+    """knn_query<MAXK> with the learned bound (same output as knn_query); blocking."""
+    x, y, z = (_as_coord(a, ctx.coord) for a in (qx, qy, qz))
+    nq = len(x)
+    if results is None:
+        results, result_dists = _alloc_knn_out(ctx, nq, k)
+    _call(lib().ft_knn_learned(ctx.handle, tree.c, model._h, _ptr(x), _ptr(y), _ptr(z), nq, int(k),
+                               ctypes.c_float(inflation), _ptr(results), _ptr(result_dists),
+                               ctypes.byref(_qopts(max_k, 1)), _stream_handle(stream)))
+    return _rows(results, nq, k), _rows(result_dists, nq, k)

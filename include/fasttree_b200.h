@@ -252,6 +252,18 @@ ft_status ft_bound_model_fit(ft_context *ctx, ft_bound_model *model, const float
  * 2^pred)^2 in distance units (bound_out: NULL or device dist values).  Asynchronous. */
 ft_status ft_bound_model_predict(ft_context *ctx, ft_bound_model *model, const float *features, size_t n,
                                  float inflation, float *pred_out, void *bound_out, ft_stream_t stream);
+/* The 12 features of external query points (knn_query): each point is placed at the SFC
+ * rank of its key among the tree's sorted keys (trees from ft_build_bvh without caller
+ * keys); the leaf there stands for the point and the window is seen from the point.
+ * qx/qy/qz, features_out: device.  Asynchronous. */
+ft_status ft_bound_features_points(ft_context *ctx, const ft_tree *tree, const void *qx, const void *qy,
+                                   const void *qz, size_t num_queries, int k, float *features_out, ft_stream_t stream);
+/* knn_query<MAXK> of external points with the learned bound: features -> bound -> the fast
+ * walk; queries whose bound proves too small, or with ties, are rerun by knn_query's own heap
+ * tier, so the output equals ft_knn's.  Arrays as ft_knn (host or device).  Blocking. */
+ft_status ft_knn_learned(ft_context *ctx, const ft_tree *tree, ft_bound_model *model, const void *qx,
+                         const void *qy, const void *qz, size_t num_queries, int k, float inflation,
+                         uint64_t *idx_out, void *dist_out, const ft_query_options *qopts, ft_stream_t stream);
 /* Features -> bound -> ft_self_knn_bounded in one call (scratch kept in the context).
  * Same output as ft_self_knn.  Asynchronous. */
 ft_status ft_self_knn_learned(ft_context *ctx, const ft_tree *tree, ft_bound_model *model, const int32_t *leaf_ids,

@@ -75,9 +75,10 @@ def _leaf_dist(opts: O.Options, tree: O.Tree, i: np.ndarray, j: np.ndarray) -> n
     return s
 
 
-def features(opts: O.Options, tree: O.Tree, k: int, leaf_ids=None) -> np.ndarray:
+def _common_features(opts: O.Options, tree: O.Tree, k: int, ranks: np.ndarray, window) -> np.ndarray:
+    """Features of queries placed at sorted-leaf `ranks`; window(r_i, r) gives the squared
+    distances (float32 values) from query r_i to its SFC-window leaves."""
     n = tree.n
-    ranks = np.arange(n) if leaf_ids is None else np.asarray(leaf_ids, np.int64)
     q = len(ranks)
     F = np.zeros((q, N_FEATURES), np.float64)
     isf = opts.coord in (O.F32, O.F64)
@@ -86,12 +87,8 @@ def features(opts: O.Options, tree: O.Tree, k: int, leaf_ids=None) -> np.ndarray
     par = tree.parent.astype(np.int64)
 
     def diag(a):
-        out = []
-        for lo, hi in ((tree.min_x, tree.max_x), (tree.min_y, tree.max_y), (tree.min_z, tree.max_z)):
-            if isf:
-                out.append((hi[a] - lo[a]).astype(np.float64))
-            else:
-                out.append((hi[a] - lo[a]).astype(np.float64))  # unsigned difference, hi >= lo in a box
+        out = [(hi[a] - lo[a]).astype(np.float64)  # unsigned difference, hi >= lo in a box
+               for lo, hi in ((tree.min_x, tree.max_x), (tree.min_y, tree.max_y), (tree.min_z, tree.max_z))]
         return np.sqrt(out[0] ** 2 + out[1] ** 2 + out[2] ** 2)
 
     slot = ranks + n - 1
@@ -113,12 +110,10 @@ def features(opts: O.Options, tree: O.Tree, k: int, leaf_ids=None) -> np.ndarray
     kk = min(k, 64)
     lwk = np.zeros(q)
     for r_i, r in enumerate(ranks):
-        lo, hi = max(0, r - k), min(n - 1, r + k)
-        js = np.array([j for j in range(lo, hi + 1) if j != r], np.int64)
-        if len(js) == 0:
+        d = np.sort(np.asarray(window(r_i, int(r)), np.float32).astype(np.float64))
+        if len(d) == 0:
             wk = wk2 = 0.0
         else:
-            d = np.sort(_leaf_dist(opts, tree, np.full(len(js), r), js).astype(np.float32).astype(np.float64))
             m = min(kk, len(d))
             wk = d[m - 1]
             wk2 = d[min((kk + 1) // 2, m) - 1]
@@ -147,6 +142,52 @@ def features(opts: O.Options, tree: O.Tree, k: int, leaf_ids=None) -> np.ndarray
             m = Ls == L
             F[m, 4 + c] = np.log2(cnt[inv][ranks[m]].astype(np.float64))
     return F.astype(np.float32)
+
+
+def features(opts: O.Options, tree: O.Tree, k: int, leaf_ids=None) -> np.ndarray:
+    """Features of self queries (every leaf, or the sorted-leaf ranks leaf_ids): the window is
+    ranks r-k .. r+k without the query's own leaf."""
+    n = tree.n
+    ranks = np.arange(n) if leaf_ids is None else np.asarray(leaf_ids, np.int64)
+
+    def window(_, r):
+        js = np.array([j for j in range(max(0, r - k), min(n - 1, r + k) + 1) if j != r], np.int64)
+        return _leaf_dist(opts, tree, np.full(len(js), r), js).astype(np.float32) if len(js) else []
+
+    return _common_features(opts, tree, k, ranks, window)
+
+
+def seed_ranks(opts: O.Options, tree: O.Tree, qx, qy, qz, bbox) -> np.ndarray:
+    """Each external point's SFC rank: the first sorted key >= the point's key (keys encoded
+    with the tree's build box), as an insertion point in [0, n]."""
+    hi, lo = O.sfc_encode(opts, qx, qy, qz, bbox)
+    n = tree.n
+    shi, slo = tree.sorted_hi[:n].astype(object), tree.sorted_lo[:n].astype(object)
+    comp = [(int(a) << 64) | int(b) for a, b in zip(shi, slo)]
+    import bisect
+    return np.array([bisect.bisect_left(comp, (int(a) << 64) | int(b)) for a, b in zip(hi, lo)], np.int64)
+
+
+def features_points(opts: O.Options, tree: O.Tree, k: int, qx, qy, qz, bbox) -> np.ndarray:
+    """Features of external query points: each point stands at its seed rank r (clamped to the
+    last leaf), the ancestor and prefix features are those of the leaf there, and the window
+    is the leaves r-k .. r+k-1 seen from the point (point-to-leaf distances)."""
+    n = tree.n
+    dt = O.NP_COORD[opts.coord]
+    qx, qy, qz = (np.asarray(a, dt) for a in (qx, qy, qz))
+    ranks = np.minimum(seed_ranks(opts, tree, qx, qy, qz, bbox), n - 1)
+
+    def window(r_i, r):
+        p3 = np.array([qx[r_i], qy[r_i], qz[r_i]], dt)
+        out = []
+        for j in range(max(0, r - k), min(n - 1, r + k - 1) + 1):
+            s = j + n - 1
+            box = np.array([tree.min_x[s], tree.max_x[s], tree.min_y[s], tree.max_y[s], tree.min_z[s],
+                            tree.max_z[s]], dt)
+            out.append(float(O.point_dist(opts, p3, box)))
+        return out
+
+    return _common_features(opts, tree, k, ranks, window)
 
 
 def targets(opts: O.Options, dist: np.ndarray, idx: np.ndarray, k: int) -> np.ndarray:

@@ -191,3 +191,77 @@ def test_trained_bound_saves_visits():
           f"replayed fast {fast['replayed']} learned {learned['replayed']}")
     assert learned["visits"] < fast["visits"]
     assert learned["replayed"] < 0.2 * len(x)
+
+
+def _point_queries(n_q, oc, x, y, z, seed):
+    """External points: a uniform draw, copies of tree points (exact key matches) and, for
+    float coordinates, points outside the tree's box."""
+    qx, qy, qz = gen("uniform", n_q, oc, seed)
+    qx, qy, qz = (np.array(a) for a in (qx, qy, qz))
+    m = n_q // 4
+    qx[:m], qy[:m], qz[:m] = x[:m], y[:m], z[:m]
+    if oc in (O.F32, O.F64):
+        qx[m:m + 8] = -5.0
+        qz[m + 8:m + 16] = qz.max() * 3
+    return qx, qy, qz
+
+
+@pytest.mark.parametrize("coord,sfc,per,oc,os_", FEAT_CASES, ids=[f"{c[0]}-{c[1]}{'-per' if c[2] else ''}"
+                                                                  for c in FEAT_CASES])
+@pytest.mark.parametrize("k", [1, 8, 32, 48])
+def test_point_features_match_oracle(coord, sfc, per, oc, os_, k):
+    n, n_q = 2500, 500
+    x, y, z = gen("clustered", n, oc, 41)
+    qx, qy, qz = _point_queries(n_q, oc, x, y, z, 42)
+    ctx = ft.Context(coord, sfc, periodic=per)
+    tree = ft.TreeSoA(ctx, n)
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree)
+    got = L.features_points(ctx, tree, qx, qy, qz, k).cpu().numpy()
+    opts = O.Options(oc, os_, per)
+    ot = O.build_bvh(opts, x, y, z)
+    want = BO.features_points(opts, ot, k, qx, qy, qz, O.compute_bbox(opts, x, y, z))
+    assert got.shape == want.shape
+    assert np.array_equal(got[:, 4:10], want[:, 4:10])
+    assert np.allclose(got, want, rtol=0, atol=2e-5), np.abs(got - want).max(0)
+
+
+def test_point_features_need_library_keys():
+    n = 3000
+    x, y, z = gen("uniform", n, O.U64, 3)
+    ctx = ft.Context("u64", "ph", periodic=True)
+    keys = ft.sfc_encode(ctx, x, y, z)
+    tree = ft.TreeSoA(ctx, n)
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree, key=keys)
+    with pytest.raises(ValueError, match="keys"):
+        L.features_points(ctx, tree, x[:10], y[:10], z[:10], 8)
+
+
+@pytest.mark.parametrize("coord,sfc,per", [("u64", "ph", True), ("f32", "morton", False), ("u32", "ph", True)])
+def test_learned_knn_query_is_exact_for_any_network(coord, sfc, per):
+    n, n_q = 150_000, 40_000
+    oc = {"u64": O.U64, "f32": O.F32, "u32": O.U32}[coord]
+    x, y, z = gen("clustered", n, oc, 18)
+    qx, qy, qz = _point_queries(n_q, oc, x, y, z, 19)
+    tx, ty, tz = gen("clustered", 60_000, oc, 20)
+    ctx = ft.Context(coord, sfc, periodic=per)
+    tree = ft.TreeSoA(ctx, n)
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree)
+    trained, _ = L.train_bound(ctx, tx, ty, tz, 16, steps=200, batch=4096)
+    untrained = L.BoundModel(ctx, seed=9)
+    tiny = L.BoundModel(ctx, seed=9)
+    p = tiny.params
+    p[BO.OFF_B3] = -60.0
+    tiny.params = p
+    huge = L.BoundModel(ctx, seed=9)
+    p[BO.OFF_B3] = 60.0
+    huge.params = p
+    # both of knn_query's heap tiers: the register heap (MAXK <= 32) and the merge heap
+    for k, max_k in ((16, 32), (16, 256), (32, 32), (40, 64)):
+        pi, pd = ft.knn_query(ctx, tree, qx, qy, qz, k, max_k=max_k, method=0)
+        pi, pd = pi.clone(), pd.clone()
+        for name, model in (("trained", trained), ("untrained", untrained), ("tiny", tiny), ("huge", huge)):
+            i, d = L.knn_query_learned(ctx, tree, model, qx, qy, qz, k, max_k=max_k, inflation=1.15)
+            torch.cuda.synchronize()
+            assert torch.equal(i, pi) and torch.equal(d, pd), (name, k, max_k)
+            if name == "tiny":
+                assert ctx.query_stats()["replayed"] >= n_q - 10
