@@ -39,6 +39,100 @@ static constexpr int kFastStack = 64;
 static constexpr int kFastWarps = 2;
 static constexpr int kFastThreads = 32 * kFastWarps;
 
+// Group walk (variant 5): a lower bound of the walk's distance from every point of the
+// group box [g0, g1] (per axis) to a node box b (minx, maxx, miny, maxy, minz, maxz).  Each
+// axis gap is measured from the group's nearer side, so it is no larger than the gap from
+// any point inside the group box, and the distance is monotone in the three gaps (rounded
+// subtraction, products and sums of non-negative values included).  Periodic trees: the
+// clean 42-bit form only (coordinates below 2^42, group coordinates masked); on the circle,
+// the group interval and the node interval are disjoint exactly when the two gaps a, b and
+// the two lengths add up to one period, and then every group point is at least min(a, b)
+// from the node.
+template <class T, int PER>
+FT_D typename Coord<T>::dist_t group_lb(const T g0[3], const T g1[3], const T b[6]) {
+    using C = Coord<T>;
+    if constexpr (C::is_float) {
+        const T dx = c_fmax(sub_rn(b[0], g1[0]), c_fmax(T(0), sub_rn(g0[0], b[1])));
+        const T dy = c_fmax(sub_rn(b[2], g1[1]), c_fmax(T(0), sub_rn(g0[1], b[3])));
+        const T dz = c_fmax(sub_rn(b[4], g1[2]), c_fmax(T(0), sub_rn(g0[2], b[5])));
+        return (double)add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
+    } else {
+        unsigned long long a[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            const T lo = b[2 * i], hi = b[2 * i + 1];
+            if constexpr (PER == 2) {
+                constexpr unsigned long long M = (1ull << C::bits) - 1ull;
+                const unsigned long long ga = ((unsigned long long)lo - (unsigned long long)g1[i]) & M;
+                const unsigned long long gb = ((unsigned long long)g0[i] - (unsigned long long)hi) & M;
+                const unsigned long long span =
+                    ((unsigned long long)g1[i] - (unsigned long long)g0[i]) + ((unsigned long long)hi - lo);
+                const unsigned long long g = ga < gb ? ga : gb;
+                a[i] = (ga + gb + span > M + 1ull) ? 0ull : (unsigned long long)(uint32_t)(g >> C::dist_shift);
+            } else {
+                a[i] = g1[i] < lo   ? (unsigned long long)(T)(lo - g1[i]) >> C::dist_shift
+                       : g0[i] > hi ? (unsigned long long)(T)(g0[i] - hi) >> C::dist_shift
+                                    : 0ull;
+            }
+        }
+        return Metric<T>::sq(a[0]) + Metric<T>::sq(a[1]) + Metric<T>::sq(a[2]);
+    }
+}
+
+// Signed offset of coordinate v from the group's corner o (integer coordinates): the
+// wrapped 42-bit difference for the clean periodic metric, else the plain difference.
+template <class T, int PER> FT_D long long group_offset(T v, T o) {
+    if constexpr (PER == 2) {
+        constexpr int sh = 64 - Coord<T>::bits;
+        return (long long)(((unsigned long long)v - (unsigned long long)o) << sh) >> sh;
+    } else {
+        return (long long)((unsigned long long)v - (unsigned long long)o);
+    }
+}
+
+// Float lower bound of the exact integer distance between a staged leaf (offsets e.xyz from
+// the group's corner) and a query (offsets q), given gerr >= the error of |e - q| against the
+// exact gap G on any axis (2^-21 of the largest offset magnitude: two conversions and one
+// subtraction, each within 2^-24 of its magnitude, with a factor of two to spare).  Per axis
+// the exact term is floor(G / 2^shift) > G / 2^shift - 1 >= (|e - q| - gerr) / 2^shift - 1,
+// and scale = 2^-shift (1 - 2^-20) absorbs the roundings of that bound, so each float term is
+// at most the exact one and the float sum of squares is at most the exact sum times
+// (1 + 2^-22).  A leaf is skipped only when that sum, shrunk by 2^-16, still exceeds the
+// lane's radius rounded up: then the exact distance exceeds the radius too.
+FT_D float group_filter(const float4 &e, const float q[3], float gerr, float scale) {
+    const float lx = fmaxf(0.0f, fmaf(fabsf(e.x - q[0]) - gerr, scale, -1.0f));
+    const float ly = fmaxf(0.0f, fmaf(fabsf(e.y - q[1]) - gerr, scale, -1.0f));
+    const float lz = fmaxf(0.0f, fmaf(fabsf(e.z - q[2]) - gerr, scale, -1.0f));
+    return fmaf(lz, lz, fmaf(ly, ly, lx * lx));
+}
+
+template <class T> FT_D T coord_top() {
+    if constexpr (std::is_same<T, float>::value) return 3.402823466e38f;
+    else if constexpr (std::is_same<T, double>::value) return 1.7976931348623157e308;
+    else return ~T(0);
+}
+template <class T> FT_D T coord_bottom() {
+    if constexpr (Coord<T>::is_float) return -coord_top<T>();
+    else return T(0);
+}
+
+template <class T> FT_D T warp_min_t(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const T w = __shfl_xor_sync(0xffffffffu, v, o);
+        v         = w < v ? w : v;
+    }
+    return v;
+}
+template <class T> FT_D T warp_max_t(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const T w = __shfl_xor_sync(0xffffffffu, v, o);
+        v         = w > v ? w : v;
+    }
+    return v;
+}
+
 template <class T, int PER, int KC, int VAR>
 __global__ void __launch_bounds__(kFastThreads)
     fast_self_knn_kernel(TreeDev<T> t_all, BatchDev bt, const T *__restrict__ qx, const T *__restrict__ qy,
@@ -184,6 +278,184 @@ __global__ void __launch_bounds__(kFastThreads)
     // Nodes at exactly the k-th distance are walked (not pruned), so any other point at
     // that distance reaches insert() and raises the tie flag there.
     auto needs = [&](D d2) { return active && !(d2 > B) && !(count >= k && d2 > hmax); };
+    bool group_done = false;
+    if constexpr (VAR == 5) {
+        // Group walk: the warp's 32 queries (neighbours on the curve) walk the tree once
+        // together.  Lanes expand up to 32 records at a time from a shared stack and keep a
+        // child when its distance from the group's box is within the largest of the lanes'
+        // radii (k-th distance or bound); kept leaves are staged in shared memory and every
+        // lane then tests every staged leaf against its own radius.  Radii only shrink, so a
+        // pruned node is beyond every lane's final k-th distance, and every leaf a lane needs
+        // (ties at its k-th distance included) reaches its heap.
+        // Integer coordinates: the staged leaves hold float offsets from the group's corner,
+        // and a lane first evaluates a float lower bound of the exact distance (group_filter);
+        // only leaves that pass get the exact distance and the heap, so the exact 64-bit
+        // arithmetic and the divergent insertions run for a few leaves per lane.
+        // Used when every lane's heap is already full (seeded) on a single tree with the open,
+        // float or clean periodic metric; other warps take the 4-wide walk.
+        constexpr bool FILT    = !Coord<T>::is_float;
+        constexpr int  kGStack = 256, kGCand = 128;
+        __shared__ int32_t g_stk[kFastWarps][kGStack];
+        __shared__ float4  g_cf[kFastWarps][FILT ? kGCand : 1];  // offsets x, y, z; slot bits in w
+        __shared__ T       g_cx[kFastWarps][FILT ? 1 : kGCand], g_cy[kFastWarps][FILT ? 1 : kGCand],
+            g_cz[kFastWarps][FILT ? 1 : kGCand];
+        __shared__ int32_t g_cs[kFastWarps][FILT ? 1 : kGCand];
+        bool finite = true;
+        if constexpr (Coord<T>::is_float)
+            finite = !active || (isfinite((double)px) && isfinite((double)py) && isfinite((double)pz));
+        const bool can = !bt.off && PER != 1 && n > 1 && __all_sync(FULL, (!active || count >= k) && finite) &&
+                         __any_sync(FULL, active);
+        auto gm = [](T v) -> T {
+            if constexpr (PER == 2) return (T)((unsigned long long)v & ((1ull << Coord<T>::bits) - 1ull));
+            else return v;
+        };
+        const T pv[3] = {gm(px), gm(py), gm(pz)};
+        T       g0[3], g1[3];
+        D       R = D(0);
+        float   qf[3] = {0.0f, 0.0f, 0.0f}, gerr = 0.0f;
+        bool    ok = can;
+        auto radius = [&]() { return warp_max_t<D>(active ? (hmax < B ? hmax : B) : D(0)); };
+        if (can) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                g0[a] = warp_min_t<T>(active ? pv[a] : coord_top<T>());
+                g1[a] = warp_max_t<T>(active ? pv[a] : coord_bottom<T>());
+            }
+            R = radius();
+            if constexpr (FILT) {
+                // every staged leaf is within span + (sqrt(R) + 1) 2^shift of the group's
+                // corner on each axis; offsets below 2^40 keep the float filter's error bound
+                // (and the periodic differences unwrapped)
+                double span = 0.0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) span = fmax(span, (double)(unsigned long long)(g1[a] - g0[a]));
+                const double lam = span + (sqrt((double)R) + 2.0) * (double)(1ull << Coord<T>::dist_shift);
+                ok   = lam < 0x1p40;
+                gerr = (float)(lam * 0x1p-21);
+#pragma unroll
+                for (int a = 0; a < 3; ++a) qf[a] = (float)group_offset<T, PER>(pv[a], g0[a]);
+            }
+        }
+        if (ok) {
+            group_done = true;
+            int  top = 1, cc = 0;
+            bool overflow = false;
+            if (lane == 0) g_stk[warp][0] = 0;
+            __syncwarp();
+            auto offer = [&](D d2, int s) {
+                const int leaf = s - (n - 1);
+                if (active && !(d2 > hmax) && !(d2 > B) && (leaf < w0 || leaf > w1) && s != self_leaf)
+                    insert(d2, ret_orig ? t.orig_idx[s] : leaf);
+            };
+            auto flush = [&]() {
+                if constexpr (FILT) {
+                    // per word of 32 staged leaves: the float filter against the lane's
+                    // current radius sets one bit per leaf that may be within it, then each
+                    // lane takes the exact distance of its set bits and offers them to its
+                    // heap (the warp loops as long as its busiest lane)
+                    constexpr float kScale = 1.0f / (float)(1ull << Coord<T>::dist_shift) * (1.0f - 0x1p-20f);
+                    for (int w = 0; w < cc; w += 32) {
+                        const D     H    = hmax < B ? hmax : B;
+                        const float Hup  = (float)H * (1.0f + 0x1p-20f);
+                        const int   nw   = min(32, cc - w);
+                        uint32_t    bits = 0;
+#pragma unroll 4
+                        for (int j = 0; j < nw; ++j) {
+                            const float f = group_filter(g_cf[warp][w + j], qf, gerr, kScale);
+                            bits |= (uint32_t)(!(f * (1.0f - 0x1p-16f) > Hup)) << j;
+                        }
+                        if (!active) bits = 0;
+                        while (bits) {
+                            const int j = __ffs(bits) - 1;
+                            bits &= bits - 1;
+                            const int s = __float_as_int(g_cf[warp][w + j].w);
+                            const T   x = t.min_x[s], y = t.min_y[s], z = t.min_z[s];
+                            offer(Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, x, x, y, y, z, z), s);
+                        }
+                    }
+                } else {
+                    // every lane tests every staged leaf (two at a time, loads ahead of insertions)
+                    for (int c = 0; c < cc; c += 2) {
+                        const int c1 = c + 1 < cc ? c + 1 : c;
+                        const T   x0 = g_cx[warp][c], y0 = g_cy[warp][c], z0 = g_cz[warp][c];
+                        const T   x1 = g_cx[warp][c1], y1 = g_cy[warp][c1], z1 = g_cz[warp][c1];
+                        const int s0 = g_cs[warp][c], s1 = g_cs[warp][c1];
+                        const D   d0 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, x0, x0, y0, y0, z0, z0);
+                        const D   d1 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, x1, x1, y1, y1, z1, z1);
+                        offer(d0, s0);
+                        if (c1 != c) offer(d1, s1);
+                    }
+                }
+                visits += cc;
+                cc = 0;
+                R  = radius();
+                __syncwarp();
+            };
+            while (top > 0) {
+                if (--budget < 0) {
+                    if (lane == 0) atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+                    overflow = true;
+                    break;
+                }
+                // pop up to 32 records, leaving room for four children each
+                const int m = min(min(top, 32), (kGStack - top) / 3);
+                if (m <= 0) {
+                    overflow = true; // the stack is full: the queries go to the replay
+                    break;
+                }
+                const int base = top - m;
+                const int node = lane < m ? g_stk[warp][base + lane] : -1;
+                top            = base;
+                __syncwarp();
+                T        bx[4][6];
+                int      ch[4] = {-1, -1, -1, -1};
+                unsigned kl = 0, ki = 0;
+                if (node >= 0) {
+                    ++visits;
+                    load_wide(t.wide, node, bx, ch);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        if (ch[i] >= 0 && !(group_lb<T, PER>(g0, g1, bx[i]) > R)) {
+                            if (ch[i] >= n - 1) kl |= 1u << i;
+                            else ki |= 1u << i;
+                        }
+                }
+                const int nl = __popc(kl), ni = __popc(ki);
+                int       incl = nl | (ni << 16);
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const int tot = __shfl_sync(FULL, incl, 31);
+                if (cc + (tot & 0xffff) > kGCand) flush();
+                int pl = cc + (incl & 0xffff) - nl, pi = top + (incl >> 16) - ni;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    if ((kl >> i) & 1u) {
+                        if constexpr (FILT) {
+                            g_cf[warp][pl] = make_float4((float)group_offset<T, PER>(bx[i][0], g0[0]),
+                                                         (float)group_offset<T, PER>(bx[i][2], g0[1]),
+                                                         (float)group_offset<T, PER>(bx[i][4], g0[2]),
+                                                         __int_as_float(ch[i]));
+                        } else {
+                            g_cx[warp][pl] = bx[i][0];
+                            g_cy[warp][pl] = bx[i][2];
+                            g_cz[warp][pl] = bx[i][4];
+                            g_cs[warp][pl] = ch[i];
+                        }
+                        ++pl;
+                    }
+                    if ((ki >> i) & 1u) g_stk[warp][pi++] = ch[i];
+                }
+                cc += tot & 0xffff;
+                top += tot >> 16;
+                __syncwarp();
+            }
+            if (overflow) flag = true;
+            else flush();
+        }
+    }
     if constexpr (VAR == 2) {
         // per-lane walk over internal nodes only: leaf children go to the heap as soon as
         // their parent is expanded, the nearer internal child is walked next from registers
@@ -238,7 +510,7 @@ __global__ void __launch_bounds__(kFastThreads)
         }
         sp = 0;
     }
-    if constexpr (VAR == 4) {
+    if constexpr (VAR == 4 || VAR == 5) {
         // per-lane walk over the 4-wide records: each step evaluates up to four grandchildren
         // (half the dependent steps of the binary walk); leaves go to the heap, the nearest
         // needed internal node is walked next and the others are stacked farthest first.  A
@@ -248,7 +520,7 @@ __global__ void __launch_bounds__(kFastThreads)
         D             sw[kWideStack];
         int           cur  = 0;
         int           wsp  = 0;
-        bool          have = active && n > 1 && needs(sd[0]);
+        bool          have = !group_done && active && n > 1 && needs(sd[0]);
         while (have) {
             if (--budget < 0) {
                 atomicOr(status, STATUS_TRAVERSAL_LIMIT);
@@ -491,7 +763,7 @@ struct ExtQueries {
 };
 
 // Walk of the fast path: caller's 0 = default, 1 per-lane binary walk, 2 compact per-lane
-// binary walk, 3 warp-shared walk, 4 the 4-wide walk.  The default is the 4-wide walk, and
+// binary walk, 3 warp-shared walk, 4 the 4-wide walk, 5 the group walk.  The default is the 4-wide walk, and
 // the compact binary walk for k <= 4 (measured on 10M clustered points: k = 32 64.2 against
 // 66.8 ms, k = 1 10.2 against 9.2 ms).  Returns the kernel's VAR template value.
 static int walk_variant(int v, int k) {
@@ -500,6 +772,7 @@ static int walk_variant(int v, int k) {
     case 2: return 2;
     case 3: return 0;
     case 4: return 4;
+    case 5: return 5;
     default: return k <= 4 ? 2 : 4;
     }
 }
@@ -514,6 +787,7 @@ static void launch_fast_t(const TreeDev<T> &tv, const BatchDev &bt, const ExtQue
     auto   fn   = variant == 0 ? fast_self_knn_kernel<T, PER, KC, 0>
                   : variant == 1 ? fast_self_knn_kernel<T, PER, KC, 1>
                   : variant == 4 ? fast_self_knn_kernel<T, PER, KC, 4>
+                  : variant == 5 ? fast_self_knn_kernel<T, PER, KC, 5>
                                  : fast_self_knn_kernel<T, PER, KC, 2>;
     FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int blocks = (num + kFastThreads - 1) / kFastThreads;
@@ -710,7 +984,8 @@ const uint32_t *sfc_query_order(Context &ctx, const ft_tree &tr, const void *qx,
 }
 
 bool fast_knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz, size_t nq, int k,
-              int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st, const void *bound) {
+              int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st, const void *bound,
+              int walk) {
     TreeImpl *impl = (TreeImpl *)tr.impl;
     if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0 || impl->height_root > 62) return false;
     // SortedMergeHeap with k equal to its capacity keeps the first k leaves it meets, not the
@@ -729,7 +1004,7 @@ bool fast_knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, c
     eq.y = qy;
     eq.z = qz;
     if (ranked && nq > 1) eq.order = order_by_rank(ctx, nq, n, st); // walk the queries in SFC order
-    const int variant = walk_variant(0, k);
+    const int variant = walk_variant(walk, k);
     switch (ctx.opts.coord_type) {
     case F32: launch_fast<float>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
     case F64: launch_fast<double>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;

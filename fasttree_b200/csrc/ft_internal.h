@@ -133,7 +133,8 @@ void free_query_sort(Context &ctx);
 const uint32_t *sfc_query_order(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz,
                                 size_t nq, cudaStream_t st);
 bool fast_knn(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz, size_t nq, int k,
-              int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st, const void *bound = nullptr);
+              int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st, const void *bound = nullptr,
+              int walk = 0);
 // SFC rank of each external query point in ctx.seed_ranks (-1 without this library's keys).
 void query_seed_ranks(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz, size_t nq,
                       cudaStream_t st);

@@ -881,7 +881,8 @@ void knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const 
     ctx.stats.queries  = (int64_t)nq;
     ctx.stats.replayed = 0;
     ctx.last_fast      = false;
-    if ((qo.method == 1 || bound) && fast_knn(ctx, tr, qx, qy, qz, nq, k, max_k, idx, dist, qo.reserved[0], st, bound)) {
+    if ((qo.method == 1 || bound) && fast_knn(ctx, tr, qx, qy, qz, nq, k, max_k, idx, dist, qo.reserved[0], st, bound,
+                                                qo.reserved[1])) {
         ctx.last_fast = true;
         return;
     }

@@ -341,7 +341,7 @@ def build_tree(ctx: Context, tree: TreeSoA, sorted_keys, sorted_x=None, sorted_y
 def _qopts(max_k: int, method: int = 0, half_window: int = 0, variant: int = 0):
     o = capi.FtQueryOptions(int(max_k), int(method))
     o.reserved[0] = int(half_window)  # fast walk: SFC seeding half-window (0 = k)
-    o.reserved[1] = int(variant)      # fast walk: 0 default (4-wide), 1 per-lane, 2 compact, 3 warp-shared, 4 4-wide
+    o.reserved[1] = int(variant)      # fast walk: 0 default, 1 per-lane, 2 compact, 3 warp-shared, 4 4-wide, 5 group
     return o
 
 
@@ -365,7 +365,8 @@ def self_knn_query(ctx: Context, tree: TreeSoA, k: int, results=None, result_dis
 
 
 def self_knn_query_bounded(ctx: Context, tree: TreeSoA, k: int, bound, results=None, result_dists=None,
-                           exclude_self=True, leaf_ids=None, max_k: int = 32, stream=None, half_window: int = 0):
+                           exclude_self=True, leaf_ids=None, max_k: int = 32, stream=None, half_window: int = 0,
+                           variant: int = 0):
     """self_knn_query with a per-query pruning bound (device tensor of dist_t, in the units of
     the returned distances).  Output equals self_knn_query's for any bound; see
     ft_self_knn_bounded."""
@@ -374,31 +375,31 @@ def self_knn_query_bounded(ctx: Context, tree: TreeSoA, k: int, bound, results=N
         results, result_dists = _alloc_knn_out(ctx, num, k)
     _call(lib().ft_self_knn_bounded(ctx.handle, tree.c, _ptr(leaf_ids), num, int(k), int(bool(exclude_self)),
                                     _ptr(bound), _ptr(results), _ptr(result_dists),
-                                    ctypes.byref(_qopts(max_k, 1, half_window)), _stream_handle(stream)))
+                                    ctypes.byref(_qopts(max_k, 1, half_window, variant)), _stream_handle(stream)))
     return _rows(results, num, k), _rows(result_dists, num, k)
 
 
 def self_knn_query_subset(ctx: Context, tree: TreeSoA, leaf_ids, k: int, results=None, result_dists=None,
-                          exclude_self=True, max_k: int = 256, method: int = 0, stream=None):
+                          exclude_self=True, max_k: int = 256, method: int = 0, stream=None, variant: int = 0):
     """self_knn_query_subset<MAXK> (src/hlbvh.hpp:1956-1983); leaf_ids is a device int32 tensor."""
     num = len(leaf_ids)
     if results is None:
         results, result_dists = _alloc_knn_out(ctx, num, k)
     _call(lib().ft_self_knn(ctx.handle, tree.c, _ptr(leaf_ids), num, int(k), int(bool(exclude_self)),
-                            _ptr(results), _ptr(result_dists), ctypes.byref(_qopts(max_k, method)),
+                            _ptr(results), _ptr(result_dists), ctypes.byref(_qopts(max_k, method, variant=variant)),
                             _stream_handle(stream)))
     return _rows(results, num, k), _rows(result_dists, num, k)
 
 
 def knn_query(ctx: Context, tree: TreeSoA, qx, qy, qz, k: int, results=None, result_dists=None, max_k: int = 256,
-              method: int = 0, stream=None):
+              method: int = 0, stream=None, variant: int = 0):
     """knn_query<MAXK> (src/hlbvh.hpp:1405-1472).  Blocking."""
     x, y, z = (_as_coord(a, ctx.coord) for a in (qx, qy, qz))
     nq = len(x)
     if results is None:
         results, result_dists = _alloc_knn_out(ctx, nq, k)
     _call(lib().ft_knn(ctx.handle, tree.c, _ptr(x), _ptr(y), _ptr(z), nq, int(k), _ptr(results), _ptr(result_dists),
-                       ctypes.byref(_qopts(max_k, method)), _stream_handle(stream)))
+                       ctypes.byref(_qopts(max_k, method, variant=variant)), _stream_handle(stream)))
     return _rows(results, nq, k), _rows(result_dists, nq, k)
 
 

@@ -18,21 +18,22 @@ from oracle import oracle as O  # noqa: E402
 from tests.gpu_util import dist_bits, gen, to_coord  # noqa: E402
 
 
-def both(ctx, tree, q, k, max_k):
+def both(ctx, tree, q, k, max_k, variant=0):
     pi, pd = ft.knn_query(ctx, tree, *q, k, max_k=max_k, method=0)
-    fi, fd = ft.knn_query(ctx, tree, *q, k, max_k=max_k, method=1)
+    fi, fd = ft.knn_query(ctx, tree, *q, k, max_k=max_k, method=1, variant=variant)
     torch.cuda.synchronize()
     return (pi, pd), (fi, fd), ctx.query_stats()
 
 
+@pytest.mark.parametrize("variant", [0, 5])
 @pytest.mark.parametrize("k,max_k", [(1, 32), (16, 32), (32, 32), (33, 64), (48, 256), (64, 256), (64, 128)])
-def test_external_queries_uniform_f64(k, max_k):
+def test_external_queries_uniform_f64(k, max_k, variant):
     x, y, z = datasets.uniform(100_000, seed=1)
     ctx = ft.Context("f64", "morton")
     tree = ft.TreeSoA(ctx, len(x))
     ft.build_bvh(ctx, ft.particles(x, y, z), tree)
     qx, qy, qz = datasets.external_queries(x, y, z, 50_000, seed=3)
-    (pi, pd), (fi, fd), st = both(ctx, tree, (qx, qy, qz), k, max_k)
+    (pi, pd), (fi, fd), st = both(ctx, tree, (qx, qy, qz), k, max_k, variant)
     assert torch.equal(pi, fi) and torch.equal(pd, fd)
     assert st["replayed"] < 0.05 * len(qx)
 
@@ -40,7 +41,8 @@ def test_external_queries_uniform_f64(k, max_k):
 @pytest.mark.parametrize("coord,sfc,per", [("u64", "ph", True), ("u32", "ph", False), ("f32", "ph", False),
                                            ("f32", "morton", False)])
 @pytest.mark.parametrize("kind", ["clustered", "degenerate"])
-def test_external_queries_hard_sets(coord, sfc, per, kind):
+@pytest.mark.parametrize("variant", [0, 5])
+def test_external_queries_hard_sets(coord, sfc, per, kind, variant):
     oc = {"u64": O.U64, "u32": O.U32, "f32": O.F32}[coord]
     x, y, z = gen(kind, 40_000, oc, 5)
     ctx = ft.Context(coord, sfc, periodic=per)
@@ -51,7 +53,7 @@ def test_external_queries_hard_sets(coord, sfc, per, kind):
     for d, a in enumerate((x, y, z)):  # a third exactly on particles (exact ties, duplicates)
         q[d][:2000] = a[rng.integers(0, len(x), 2000)]
     for k, max_k in ((8, 32), (32, 256), (64, 256)):
-        (pi, pd), (fi, fd), _ = both(ctx, tree, q, k, max_k)
+        (pi, pd), (fi, fd), _ = both(ctx, tree, q, k, max_k, variant)
         assert torch.equal(pi, fi) and torch.equal(pd, fd), (k, max_k)
 
 

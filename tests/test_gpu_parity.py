@@ -245,10 +245,10 @@ def test_fast_self_knn_matches_oracle(cfg, kind, k):
 
 
 @pytest.mark.parametrize("cfg", CONFIGS, ids=CONFIG_IDS)
-@pytest.mark.parametrize("variant", [1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5])
 def test_fast_walk_variants_match_oracle(cfg, variant):
     """Every walk of the fast path (1 per-lane, 2 compact per-lane, 3 warp-shared, 4 over the
-    4-wide records) gives the reference's output, ties included."""
+    4-wide records, 5 the group walk) gives the reference's output, ties included."""
     coord, sfc, per = cfg
     ctx, opts = make(coord, sfc, per)
     for kind, k in (("clustered", 32), ("degenerate", 16), ("uniform", 64)):
@@ -280,8 +280,8 @@ def test_fast_self_knn_subset_and_orig(cfg):
             assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od))
 
 
-@pytest.mark.parametrize("method", [0, 1])
-def test_periodic_wrap_edges_u64(method):
+@pytest.mark.parametrize("method,variant", [(0, 0), (1, 0), (1, 5)])
+def test_periodic_wrap_edges_u64(method, variant):
     """42-bit periodic distances at the wrap: points at 0, 2^41 (half the period) and
     2^42 - 1, where the wrapped gap reaches its extreme values."""
     ctx, opts = make(O.U64, O.PEANO_HILBERT, True)
@@ -294,11 +294,11 @@ def test_periodic_wrap_edges_u64(method):
     z = (rng.integers(0, B, n)).astype(np.uint64)
     tree, ot = build_both(ctx, opts, x, y, z)
     for k in (4, 32):
-        gi, gd = ft.self_knn_query(ctx, tree, k, method=method)
+        gi, gd = ft.self_knn_query(ctx, tree, k, method=method, variant=variant)
         torch.cuda.synchronize()
         oi, od = O.self_knn(opts, ot, k, True)
         assert np.array_equal(gi.cpu().numpy(), oi) and np.array_equal(gd.cpu().numpy(), od)
     q = np.array([0, B // 2, B - 1, B // 4], np.uint64)
-    gi, gd = ft.knn_query(ctx, tree, q, q, q, 16)
+    gi, gd = ft.knn_query(ctx, tree, q, q, q, 16, method=method, variant=variant)
     oi, od = O.knn(opts, ot, q, q, q, 16)
     assert np.array_equal(gi.cpu().numpy(), oi) and np.array_equal(gd.cpu().numpy(), od)
