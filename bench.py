@@ -282,8 +282,9 @@ def _timed(stream, fn, steps, warmup=1):
 
 def run_cfg2_extra(ctx, tree, x, y, z, n, stream):
     """The rest of the clustered workload on its resident tree: self-kNN at k=1 (register heap)
-    and k=64 (shared-memory heap), fast and plain, and range_query on all N points with
-    r_min = 0, r_max = 2e-3 of the box (2e-3 * 2^40 units), 512 results per query."""
+    and k=64 (shared-memory heap), fast and plain, range_query on all N points with
+    r_min = 0, r_max = 2e-3 of the box (2e-3 * 2^40 units), 512 results per query, and a
+    refit-only update of the tree for slightly moved points (last: it changes the tree)."""
     import torch
 
     import fasttree_b200 as ft
@@ -315,6 +316,30 @@ def run_cfg2_extra(ctx, tree, x, y, z, n, stream):
                           "queries": "the N particle positions in input order (the library walks them in SFC "
                                      "order); one blocking call, including its status check"}
     del res, cnt
+    # refit-only update (a simulation step): every point moved by N(0, sigma^2) per axis (kept
+    # inside the 2^40 box), refit on the kept topology, then the fast self-kNN (k=32) on the
+    # refit tree against a rebuild of the moved points.  sigma = 1e-6 of the box is a fraction
+    # of the spacing in the densest spheres; 1e-4 scrambles them (a rebuild pays off there).
+    g = torch.Generator(device=dev).manual_seed(9)
+    idx = torch.empty(n * 32, dtype=torch.uint64, device=dev)
+    dst = torch.empty(n * 32, dtype=ft.dist_torch_dtype(ctx.coord), device=dev)
+    fresh = ft.TreeSoA(ctx, n)
+    out["refit"] = {}
+    for sigma in (1e-6, 1e-4):
+        def moved(a):
+            step = (torch.randn(n, generator=g, device=dev, dtype=torch.float64) * (sigma * 2 ** 40)).to(torch.int64)
+            return (a.view(torch.int64) + step).clamp(0, 2 ** 40 - 1).view(torch.uint64)
+
+        ft.build_bvh(ctx, ft.particles(x, y, z), tree)  # start from the tree of the unmoved points
+        np_ = ft.particles(moved(x), moved(y), moved(z))
+        refit_ms = _timed(stream, lambda: ft.refit_bvh(ctx, np_, tree), 3)
+        q_refit = _timed(stream, lambda: ft.self_knn_query(ctx, tree, 32, idx, dst, method=1), 2)
+        rebuild_ms = _timed(stream, lambda: ft.build_bvh(ctx, np_, fresh), 2)
+        q_fresh = _timed(stream, lambda: ft.self_knn_query(ctx, fresh, 32, idx, dst, method=1), 2)
+        out["refit"][f"sigma_{sigma:g}_box"] = {"refit_ms": refit_ms, "rebuild_ms": rebuild_ms,
+                                               "self_knn_k32_on_refit_ms": q_refit,
+                                               "self_knn_k32_on_rebuild_ms": q_fresh}
+    del idx, dst, fresh
     return out
 
 

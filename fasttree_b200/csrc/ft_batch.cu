@@ -632,6 +632,16 @@ void batch_tree_view(Context &ctx, BatchImpl &b, size_t s, ft_tree &out, cudaStr
     out.num_internal = n > 0 ? n - 1 : 0;
     out.capacity     = 0;
     out.impl         = &v;
+    // periodic integer sets with a coordinate at or above the period keep the reference
+    // traversal (the same test the batched fast walk makes per set)
+    if (n > 0 && ctx.opts.periodic && (ctx.opts.coord_type == U32 || ctx.opts.coord_type == U64)) {
+        unsigned long long m[3] = {0, 0, 0};
+        const void        *src[3] = {out.max_x, out.max_y, out.max_z};
+        for (int a = 0; a < 3; ++a) FT_CUDA(cudaMemcpyAsync(&m[a], src[a], cb, cudaMemcpyDeviceToHost, st));
+        FT_CUDA(cudaStreamSynchronize(st));
+        const unsigned long long P = ctx.opts.coord_type == U64 ? (1ull << 42) : (1ull << 21);
+        v.in_period                = m[0] < P && m[1] < P && m[2] < P;
+    }
 }
 
 // Per-set boxes and root heights, for inspection (blocking).

@@ -361,6 +361,30 @@ __global__ void gather_kernel(const T *__restrict__ x, const T *__restrict__ y, 
     }
 }
 
+// Refit-only update: leaf slot n-1+i takes the new position of the point it already holds
+// (input index orig_idx[n-1+i], or i itself when the positions come in leaf order).  An
+// index outside [0, n) leaves the slot unchanged and sets the bad-input status bit.
+template <class T>
+__global__ void refit_gather_kernel(const T *__restrict__ x, const T *__restrict__ y, const T *__restrict__ z,
+                                    const int32_t *__restrict__ orig, size_t n, T *mnx, T *mxx, T *mny, T *mxy,
+                                    T *mnz, T *mxz, uint32_t *status) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t  leaf = i + n - 1;
+        const int64_t src  = orig ? (int64_t)orig[leaf] : (int64_t)i;
+        if (src < 0 || src >= (int64_t)n) {
+            atomicOr(status, STATUS_BAD_INPUT);
+            continue;
+        }
+        const T a = x[src], b = y[src], c = z[src];
+        mnx[leaf] = a;
+        mxx[leaf] = a;
+        mny[leaf] = b;
+        mxy[leaf] = b;
+        mnz[leaf] = c;
+        mxz[leaf] = c;
+    }
+}
+
 // Leaf init of build_tree with caller arrays (src/hlbvh.hpp:906-923).
 template <class T>
 __global__ void leaf_init_kernel(const T *sx, const T *sy, const T *sz, size_t n, const uint32_t *sid,
@@ -722,6 +746,40 @@ static void build_tree_typed(Context &ctx, ft_tree &t, const void *keys_ref, con
     FT_CUDA(cudaGetLastError());
     if (n == 1) FT_CUDA(cudaMemsetAsync(t.parent, 0xFF, sizeof(int32_t), st));
     topology_and_refit<T>(ctx.opts, t, s, n, st);
+}
+
+// Refit-only update of a built tree (no reference counterpart: the reference rebuilds).  The
+// keys, leaf order and topology stay; the leaves take the new positions and the bottom-up
+// refit recomputes every internal box, the node records, heights and 4-wide records.  The
+// result is the tree build_tree (src/hlbvh.hpp:773-982) makes from the same sorted keys with
+// the new positions as its leaf arrays.
+template <class T>
+static void refit_typed(ft_tree &t, const void *x, const void *y, const void *z, size_t n, bool leaf_order,
+                        cudaStream_t st) {
+    TreeImpl &s = *(TreeImpl *)t.impl;
+    SoA<T>    a(t);
+    refit_gather_kernel<T><<<grid_for(n, 256), 256, 0, st>>>((const T *)x, (const T *)y, (const T *)z,
+                                                             leaf_order ? nullptr : t.orig_idx, n, a.mnx, a.mxx,
+                                                             a.mny, a.mxy, a.mnz, a.mxz, s.status);
+    FT_CUDA(cudaGetLastError());
+    if (n < 2) return;
+    const int blocks = grid_for(n, 256, 148 * 32);
+    FT_CUDA(cudaMemsetAsync(s.counters, 0, (n - 1) * sizeof(int32_t), st));
+    refit_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, t.parent, a.mnx, a.mxx, a.mny,
+                                            a.mxy, a.mnz, a.mxz, (NodeRec<T> *)s.recs, s.height, s.counters);
+    collapse_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, a.mnx, a.mxx, a.mny, a.mxy,
+                                               a.mnz, a.mxz, (WideRec<T> *)s.wide);
+    FT_CUDA(cudaGetLastError());
+}
+
+void refit_bvh(Context &ctx, ft_tree &t, const void *x, const void *y, const void *z, size_t n, bool leaf_order,
+               cudaStream_t st) {
+    switch (ctx.opts.coord_type) {
+    case F32: refit_typed<float>(t, x, y, z, n, leaf_order, st); break;
+    case F64: refit_typed<double>(t, x, y, z, n, leaf_order, st); break;
+    case U32: refit_typed<uint32_t>(t, x, y, z, n, leaf_order, st); break;
+    case U64: refit_typed<unsigned long long>(t, x, y, z, n, leaf_order, st); break;
+    }
 }
 
 void build_tree_from_keys(Context &ctx, ft_tree &t, const void *keys_ref, const void *sx, const void *sy,

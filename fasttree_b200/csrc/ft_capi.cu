@@ -412,6 +412,56 @@ ft_status ft_sfc_encode(ft_context *ctx, const void *x, const void *y, const voi
     FT_API_END
 }
 
+// Root box maxima of an integer tree below the period 2^42 (64-bit) / 2^21 (32-bit), i.e.
+// every coordinate is (TreeImpl::in_period).  Blocking.
+static bool root_in_period(const ft_context *ctx, const ft_tree *tree, cudaStream_t st) {
+    const int ct = ctx->opts.coord_type;
+    if (ct == FT_COORD_F32 || ct == FT_COORD_F64 || tree->num_leaves == 0) return true;
+    const void *src[3] = {tree->max_x, tree->max_y, tree->max_z};
+    if (ct == FT_COORD_U64) {
+        uint64_t m[3] = {0, 0, 0};
+        for (int a = 0; a < 3; ++a) FT_CUDA(cudaMemcpyAsync(&m[a], src[a], 8, cudaMemcpyDefault, st));
+        FT_CUDA(cudaStreamSynchronize(st));
+        return m[0] < (1ull << 42) && m[1] < (1ull << 42) && m[2] < (1ull << 42);
+    }
+    uint32_t m[3] = {0, 0, 0};
+    for (int a = 0; a < 3; ++a) FT_CUDA(cudaMemcpyAsync(&m[a], src[a], 4, cudaMemcpyDefault, st));
+    FT_CUDA(cudaStreamSynchronize(st));
+    return m[0] < (1u << 21) && m[1] < (1u << 21) && m[2] < (1u << 21);
+}
+
+ft_status ft_refit_bvh(ft_context *ctx, const void *x, const void *y, const void *z, size_t n, int leaf_order,
+                       ft_tree *tree, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree, "null argument");
+    need_owned(tree);
+    need(n == tree->num_leaves, "refit: n must equal the tree's leaf count (build the tree first)");
+    if (n == 0) return FT_OK;
+    need(x && y && z, "null coordinate array");
+    TreeImpl &impl = *(TreeImpl *)tree->impl;
+    need(impl.height_root >= 0, "refit: the tree has not been built");
+    DeviceGuard  g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    size_t       cb = coord_bytes(ctx->opts.coord_type);
+    Staged       sx, sy, sz;
+    sx.init(x, n * cb, true, false, st);
+    sy.init(y, n * cb, true, false, st);
+    sz.init(z, n * cb, true, false, st);
+    ft::refit_bvh(*ctx, *tree, sx.dev, sy.dev, sz.dev, n, leaf_order != 0, st);
+    // the 42-bit periodic fast form needs every coordinate below 2^42: the root box's maxima
+    uint64_t mx[3] = {0, 0, 0};
+    if (ctx->opts.coord_type == FT_COORD_U64) {
+        FT_CUDA(cudaMemcpyAsync(&mx[0], tree->max_x, 8, cudaMemcpyDefault, st));
+        FT_CUDA(cudaMemcpyAsync(&mx[1], tree->max_y, 8, cudaMemcpyDefault, st));
+        FT_CUDA(cudaMemcpyAsync(&mx[2], tree->max_z, 8, cudaMemcpyDefault, st));
+    }
+    check_status_word(impl, st);
+    impl.clean42 = impl.clean42_ok && ctx->opts.coord_type == FT_COORD_U64 && mx[0] < (1ull << 42) &&
+                   mx[1] < (1ull << 42) && mx[2] < (1ull << 42);
+    impl.in_period = root_in_period(ctx, tree, st);
+    FT_API_END
+}
+
 ft_status ft_build_bvh(ft_context *ctx, const void *x, const void *y, const void *z, size_t n, const uint32_t *id,
                        const int8_t *is_ghost, const void *bbox6, void *keys, ft_tree *tree, ft_stream_t stream) {
     FT_API_BEGIN
@@ -457,6 +507,8 @@ ft_status ft_build_bvh(ft_context *ctx, const void *x, const void *y, const void
     // boxes of a 42-bit tree stay below 2^42 when every coordinate does (max entries 1, 3, 5)
     impl.clean42 = ctx->opts.coord_type == FT_COORD_U64 && box[1] < (1ull << 42) && box[3] < (1ull << 42) &&
                    box[5] < (1ull << 42);
+    impl.clean42_ok = true;
+    impl.in_period  = root_in_period(ctx, tree, st);
     FT_API_END
 }
 
@@ -485,6 +537,7 @@ ft_status ft_build_tree(ft_context *ctx, ft_tree *tree, const void *sorted_keys,
     tree->num_internal = n - 1;
     TreeImpl &impl     = *(TreeImpl *)tree->impl;
     impl.clean42       = false; // caller leaf arrays: the general periodic distance form
+    impl.clean42_ok    = false;
     impl.own_keys      = false;
     impl.height_root   = -1;
     build_tree_from_keys(*ctx, *tree, sk.dev, sx.dev, sy.dev, sz.dev, (const uint32_t *)sid.dev,
@@ -498,6 +551,7 @@ ft_status ft_build_tree(ft_context *ctx, ft_tree *tree, const void *sorted_keys,
         check_status_word(impl, st);
         impl.height_root = 0;
     }
+    impl.in_period = root_in_period(ctx, tree, st);
     FT_API_END
 }
 

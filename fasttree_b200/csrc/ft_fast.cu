@@ -166,7 +166,15 @@ __global__ void __launch_bounds__(kFastThreads)
         const int s = find_set(bt.off, bt.S, active ? q : num - 1);
         t           = set_view(t_all, bt, s);
         rank        = (active ? q : num - 1) - (int)bt.off[s];
-        if (active && bt.height[s] > 62) {
+        bool outside = bt.height[s] > 62;
+        if constexpr (PER != 0 && !Coord<T>::is_float) {
+            // periodic integer set with a coordinate at or above the period (root box maxima):
+            // the box distance is not monotone there, so only the reference traversal applies
+            constexpr unsigned long long P = 1ull << Coord<T>::bits;
+            outside = outside || (unsigned long long)t.max_x[0] >= P || (unsigned long long)t.max_y[0] >= P ||
+                      (unsigned long long)t.max_z[0] >= P;
+        }
+        if (active && outside) {
             force_replay = true;
             active       = false;
         }
@@ -876,6 +884,7 @@ bool fast_self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, siz
                    uint64_t *idx, void *dist, const void *bound, int half_window, int variant, cudaStream_t st) {
     TreeImpl *impl = (TreeImpl *)tr.impl;
     if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0 || impl->height_root > 62) return false;
+    if (!fast_walk_applies(ctx.opts, *impl)) return false;
     if (half_window <= 0) half_window = k;
     variant = walk_variant(variant, k);
     ensure_replay(ctx, num);
@@ -988,6 +997,7 @@ bool fast_knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, c
               int walk) {
     TreeImpl *impl = (TreeImpl *)tr.impl;
     if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0 || impl->height_root > 62) return false;
+    if (!fast_walk_applies(ctx.opts, *impl)) return false;
     // SortedMergeHeap with k equal to its capacity keeps the first k leaves it meets, not the
     // nearest: only the reference traversal reproduces that
     int cap = 1;
@@ -1113,6 +1123,7 @@ bool fast_self_knn_noalloc(Context &ctx, const ft_tree &tr, const int32_t *leaf_
                                       "scratch holds 2^20); split the call");
     TreeImpl *impl = (TreeImpl *)tr.impl;
     if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0 || impl->height_root > 62) return false;
+    if (!fast_walk_applies(ctx.opts, *impl)) return false;
     uint32_t           *s      = noalloc_scratch(ctx.device);
     uint32_t           *rc     = s;
     unsigned long long *visits = reinterpret_cast<unsigned long long *>(s + 2);

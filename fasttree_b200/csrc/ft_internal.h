@@ -51,6 +51,10 @@ struct TreeImpl {
     bool      managed      = false;
     int       height_root  = -1;    // host copy after a build
     bool      clean42      = false; // 64-bit integer tree with every coordinate below 2^42
+    bool      clean42_ok   = false; // the tree may use that form (built by build_bvh)
+    bool      in_period    = true;  // integer coordinates all below 2^bits (42 for 64-bit, 21
+                                    // for 32-bit): the periodic distance is then monotone over
+                                    // nested boxes, which the fast walks rely on
     bool      view         = false; // one set of a batch: arrays owned by the batch, no builds
     bool      own_keys     = false; // key_lo / key_hi hold keys this library encoded (build_bvh
                                     // without caller keys), with the box in bbox
@@ -69,6 +73,14 @@ struct BatchDev {
 };
 
 // Distance mode of query kernels on this tree (see met_dispatch in ft_common.cuh).
+// The fast walks return the reference's rows only when the box distance never exceeds the
+// distance to any point inside the box.  Every metric has that property except the periodic
+// integer one on coordinates at or above the period (2^42 / 2^21), whose unmasked box bounds
+// break it; such trees keep the reference traversal.
+inline bool fast_walk_applies(const ft_options &o, const TreeImpl &t) {
+    return !o.periodic || o.coord_type == FT_COORD_F32 || o.coord_type == FT_COORD_F64 || t.in_period;
+}
+
 template <class T> inline int metric_mode(const ft_options &o, const ft_tree &t) {
     if (std::is_floating_point<T>::value || !o.periodic) return 0;
     return (sizeof(T) == 8 && ((const TreeImpl *)t.impl)->clean42) ? 2 : 1;
@@ -132,6 +144,8 @@ void free_query_sort(Context &ctx);
 // this library's own encoding.  Valid until the next call on the context.
 const uint32_t *sfc_query_order(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz,
                                 size_t nq, cudaStream_t st);
+void refit_bvh(Context &ctx, ft_tree &tree, const void *x, const void *y, const void *z, size_t n, bool leaf_order,
+               cudaStream_t st);
 bool fast_knn(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz, size_t nq, int k,
               int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st, const void *bound = nullptr,
               int walk = 0);

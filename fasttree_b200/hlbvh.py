@@ -326,6 +326,17 @@ def build_bvh(ctx: Context, p, tree: TreeSoA, bbox=None, key=None, scratch=None,
     return tree
 
 
+def refit_bvh(ctx: Context, p, tree: TreeSoA, leaf_order: bool = False, stream=None) -> TreeSoA:
+    """Refit-only update for moved points (ft_refit_bvh): new positions of the same points,
+    in the build's input order (or leaf order); keys and topology are kept.  Blocking."""
+    if not isinstance(p, particles):
+        p = particles(*p)
+    x, y, z = (_as_coord(a, ctx.coord) for a in (p.pos_x, p.pos_y, p.pos_z))
+    _call(lib().ft_refit_bvh(ctx.handle, _ptr(x), _ptr(y), _ptr(z), len(x), int(bool(leaf_order)), tree.c,
+                             _stream_handle(stream)))
+    return tree
+
+
 def build_tree(ctx: Context, tree: TreeSoA, sorted_keys, sorted_x=None, sorted_y=None, sorted_z=None,
                sorted_id=None, sorted_is_ghost=None, sorted_orig_idx=None, stream=None) -> TreeSoA:
     """build_tree (src/hlbvh.hpp:773-982) from caller-sorted keys (reference layout)."""

@@ -300,6 +300,14 @@ inline void build_bvh(queue &q, const particles<coord_t> &p, TreeSoA &tree, Boun
     build_bvh(q, p, tree, s, bbox, key);
 }
 
+// Refit-only update for moved points (no reference counterpart; ft_refit_bvh): the same
+// points at new positions, in build_bvh's input order; keys and topology are kept.
+inline void refit_bvh(queue &q, const particles<coord_t> &p, TreeSoA &tree) {
+    check(ft_refit_bvh(q.context(), p.pos_x.data(), p.pos_y.data(), p.pos_z.data(), p.pos_x.size(), 0,
+                       tree.handle, q.stream()));
+    tree.sync();
+}
+
 // ---- queries -----------------------------------------------------------------------------
 // The kNN queries take the fast walk (SFC-window seeding, exact replay of tied queries):
 // its output is bit-identical to the reference traversal's.  Define

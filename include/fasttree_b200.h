@@ -143,6 +143,17 @@ ft_status ft_build_tree(ft_context *ctx, ft_tree *tree, const void *sorted_keys,
                         const uint32_t *sorted_id, const int8_t *sorted_is_ghost,
                         const int32_t *sorted_orig_idx, ft_stream_t stream);
 
+/* Refit-only update of a built tree for moved points (no reference counterpart: the
+ * reference rebuilds, test/benchmark/rebuild_scaling.cpp).  x/y/z hold the new positions of
+ * the same n points, in the build's input order (leaf_order = 0: leaf i takes the point
+ * orig_idx[n-1+i]) or in leaf order (leaf_order = 1).  Keys, leaf order and topology are
+ * kept; every box, node record and height is recomputed, so the tree equals the one
+ * ft_build_tree makes from the build's sorted keys with the new positions as its leaf
+ * arrays.  Queries stay exact; they prune best while the points stay near their cells.
+ * Host or device arrays.  Blocking. */
+ft_status ft_refit_bvh(ft_context *ctx, const void *x, const void *y, const void *z, size_t n, int leaf_order,
+                       ft_tree *tree, ft_stream_t stream);
+
 /* ---------------------------------------------------------------------------------- */
 /* Queries.  Output rows are k wide: idx (size_t, SIZE_MAX when missing) and dist        */
 /* (double for float coords, uint64 for integer coords; -DBL_MAX / 0 when missing).     */

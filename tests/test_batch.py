@@ -232,3 +232,30 @@ def test_rejections():
         ft.build_bvh(ctx, ft.particles(x[:20], y[:20], z[:20]), view)
     with pytest.raises(ValueError):
         b.tree(5)
+
+
+def test_periodic_sets_beyond_the_period():
+    """u32 periodic sets where some sets hold coordinates at or above 2^21: those sets keep the
+    reference traversal (non-monotone box distance there); every set equals the oracle."""
+    ctx = ft.Context("u32", "ph", periodic=True)
+    sizes = [900, 1500, 700, 2000]
+    x, y, z, off = make_sets("u32", sizes, seed=21)
+    x = x.copy()
+    for s in (1, 3):  # push a few points of sets 1 and 3 past the period
+        x[off[s]:off[s + 1]:37] += np.uint32(1 << 21)
+    b = ft.BatchedSets(ctx, len(x), len(sizes))
+    b.build(off, x, y, z)
+    bi, bd = b.self_knn(16, method=1)
+    torch.cuda.synchronize()
+    b.check()
+    bi, bd = bi.cpu().numpy(), bd.cpu().numpy()
+    opts = O.Options(CODES["u32"], CODES["ph"], True)
+    for s in range(len(sizes)):
+        sl = slice(off[s], off[s + 1])
+        ot = O.build_bvh(opts, x[sl], y[sl], z[sl])
+        oi, od = O.self_knn(opts, ot, 16)
+        assert np.array_equal(rows(bi, off, s), oi), s
+        assert np.array_equal(dist_bits(rows(bd, off, s)), dist_bits(od)), s
+        vi, vd = ft.self_knn_query(ctx, b.tree(s), 16, method=1)  # the set as a single tree
+        torch.cuda.synchronize()
+        assert np.array_equal(vi.cpu().numpy(), oi), s

@@ -302,3 +302,28 @@ def test_periodic_wrap_edges_u64(method, variant):
     gi, gd = ft.knn_query(ctx, tree, q, q, q, 16, method=method, variant=variant)
     oi, od = O.knn(opts, ot, q, q, q, 16)
     assert np.array_equal(gi.cpu().numpy(), oi) and np.array_equal(gd.cpu().numpy(), od)
+
+
+@pytest.mark.parametrize("coord", [O.U64, O.U32])
+def test_periodic_coordinates_beyond_the_period(coord):
+    """Periodic integer trees holding coordinates at or above the period (2^42 / 2^21): the
+    reference masks only the query's coordinate, so its box distance is not monotone there;
+    the fast walk must not be taken and every method returns the reference's rows."""
+    ctx, opts = make(coord, O.PEANO_HILBERT, True)
+    x, y, z = gen("clustered", 4000, coord, seed=51)
+    bits = 42 if coord == O.U64 else 21
+    dt = x.dtype.type
+    x = x.copy()
+    x[::53] += dt(1 << bits)
+    tree, ot = build_both(ctx, opts, x, y, z)
+    for k in (8, 32):
+        oi, od = O.self_knn(opts, ot, k, True)
+        for method in (0, 1):
+            gi, gd = ft.self_knn_query(ctx, tree, k, max_k=32, method=method)
+            torch.cuda.synchronize()
+            assert np.array_equal(gi.cpu().numpy(), oi), (k, method)
+            assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od)), (k, method)
+    qx, qy, qz = gen("uniform", 300, coord, seed=52)
+    oi, od = O.knn(opts, ot, qx, qy, qz, 16)
+    gi, gd = ft.knn_query(ctx, tree, qx, qy, qz, 16, method=1)
+    assert np.array_equal(gi.cpu().numpy(), oi) and np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od))
