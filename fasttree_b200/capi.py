@@ -19,7 +19,7 @@ EXPORTED = (
     "ft_context_create", "ft_context_destroy", "ft_last_error", "ft_version", "ft_get_query_stats",
     "ft_check_device_status",
     "ft_tree_create", "ft_tree_ensure", "ft_tree_destroy", "ft_compute_bbox", "ft_sfc_encode",
-    "ft_build_bvh", "ft_build_tree", "ft_refit_bvh", "ft_self_knn", "ft_knn", "ft_range", "ft_tree_height",
+    "ft_build_bvh", "ft_build_tree", "ft_refit_bvh", "ft_tree_export", "ft_tree_import", "ft_self_knn", "ft_knn", "ft_range", "ft_tree_height",
     "ft_self_knn_noalloc", "ft_self_knn_bounded",
     "ft_batch_create", "ft_batch_destroy", "ft_batch_build", "ft_batch_self_knn", "ft_batch_build_knn",
     "ft_batch_tree", "ft_batch_set_info", "ft_batch_query_stats",
@@ -74,6 +74,8 @@ _SIGS = {
     "ft_sfc_encode": [_vp, _vp, _vp, _vp, _sz, _vp, _vp, _st],
     "ft_build_bvh": [_vp, _vp, _vp, _vp, _sz, _vp, _vp, _vp, _vp, ctypes.POINTER(FtTree), _st],
     "ft_refit_bvh": [_vp, _vp, _vp, _vp, _sz, _i, ctypes.POINTER(FtTree), _st],
+    "ft_tree_export": [_vp, ctypes.POINTER(FtTree), _vp, ctypes.POINTER(ctypes.c_size_t), _st],
+    "ft_tree_import": [_vp, _vp, _sz, ctypes.POINTER(FtTree), _st],
     "ft_build_tree": [_vp, ctypes.POINTER(FtTree), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _st],
     "ft_self_knn": [_vp, ctypes.POINTER(FtTree), _vp, _sz, _i, _i, _vp, _vp, ctypes.POINTER(FtQueryOptions), _st],
     "ft_self_knn_noalloc": [_vp, ctypes.POINTER(FtTree), _vp, _sz, _i, _i, _vp, _vp, _st],

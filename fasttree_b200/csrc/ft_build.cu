@@ -782,6 +782,19 @@ void refit_bvh(Context &ctx, ft_tree &t, const void *x, const void *y, const voi
     }
 }
 
+// Topology, internal boxes, node records, heights and 4-wide records recomputed from the
+// tree's sorted keys and leaf slots (an imported tree).
+void recompute_from_keys(Context &ctx, ft_tree &t, cudaStream_t st) {
+    TreeImpl &s = *(TreeImpl *)t.impl;
+    size_t    n = t.num_leaves;
+    switch (ctx.opts.coord_type) {
+    case F32: topology_and_refit<float>(ctx.opts, t, s, n, st); break;
+    case F64: topology_and_refit<double>(ctx.opts, t, s, n, st); break;
+    case U32: topology_and_refit<uint32_t>(ctx.opts, t, s, n, st); break;
+    case U64: topology_and_refit<unsigned long long>(ctx.opts, t, s, n, st); break;
+    }
+}
+
 void build_tree_from_keys(Context &ctx, ft_tree &t, const void *keys_ref, const void *sx, const void *sy,
                           const void *sz, const uint32_t *sid, const int8_t *sghost, const int32_t *sorig,
                           cudaStream_t st) {

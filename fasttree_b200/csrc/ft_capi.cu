@@ -196,6 +196,9 @@ struct ft_context : public ft::Context {};
 static void need(bool c, const char *msg) {
     if (!c) fail(FT_ERR_INVALID_ARGUMENT, msg);
 }
+static void need(bool c, const std::string &msg) {
+    if (!c) fail(FT_ERR_INVALID_ARGUMENT, msg);
+}
 
 // Trees handed out by ft_batch_tree live inside their batch.
 static void need_owned(const ft_tree *t) {
@@ -409,6 +412,151 @@ ft_status ft_sfc_encode(ft_context *ctx, const void *x, const void *y, const voi
     tmp.key_lo = tmp.key_hi = nullptr;
     tmp.perm                = nullptr;
     FT_CUDA(cudaStreamSynchronize(st));
+    FT_API_END
+}
+
+static bool root_in_period(const ft_context *ctx, const ft_tree *tree, cudaStream_t st);
+
+// ---------------------------------------------------------------------------------------
+// Tree serialisation (raw SoA arrays + sorted keys behind a fixed header)
+// ---------------------------------------------------------------------------------------
+struct TreeFileHeader {
+    char     magic[8];   // "FTB2TREE"
+    uint32_t version;    // 1
+    int32_t  coord_type, sfc_type, periodic, key_words, own_keys, clean42_ok, reserved0;
+    uint64_t n;
+    uint64_t bbox[6];    // build box, each coordinate in an 8-byte slot
+    uint8_t  pad[128 - 8 - 4 - 7 * 4 - 8 - 48];
+};
+static_assert(sizeof(TreeFileHeader) == 128, "tree file header size");
+
+struct TreeSection {
+    void  *dev;   // device array of the tree
+    size_t bytes; // its size in the file
+};
+
+static size_t align16(size_t v) { return (v + 15) & ~size_t(15); }
+
+static std::vector<TreeSection> tree_sections(const ft_context &ctx, const ft_tree &t, size_t n) {
+    const TreeImpl &impl = *(const TreeImpl *)t.impl;
+    const size_t    cb   = coord_bytes(ctx.opts.coord_type);
+    const size_t    nn   = n ? 2 * n - 1 : 0, ni = n ? n - 1 : 0;
+    std::vector<TreeSection> v = {{t.min_x, nn * cb},      {t.max_x, nn * cb},       {t.min_y, nn * cb},
+                                  {t.max_y, nn * cb},      {t.min_z, nn * cb},       {t.max_z, nn * cb},
+                                  {t.left_child, ni * 4},  {t.right_child, ni * 4},  {t.parent, nn * 4},
+                                  {t.id, nn * 4},          {t.is_ghost, nn},         {t.orig_idx, nn * 4},
+                                  {impl.key_lo, n * 8}};
+    if (ctx.opts.coord_type == FT_COORD_U64) v.push_back({impl.key_hi, n * 8});
+    return v;
+}
+
+static size_t tree_file_bytes(const std::vector<TreeSection> &secs) {
+    size_t b = sizeof(TreeFileHeader);
+    for (const TreeSection &s : secs) b += align16(s.bytes);
+    return b;
+}
+
+ft_status ft_tree_export(ft_context *ctx, const ft_tree *tree, void *buf, size_t *bytes, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree && bytes, "null argument");
+    const TreeImpl &impl = *(const TreeImpl *)tree->impl;
+    const size_t    n    = tree->num_leaves;
+    need(n == 0 || impl.height_root >= 0, "tree export: the tree has not been built");
+    need(n == 0 || impl.key_lo, "tree export: the tree has no keys");
+    DeviceGuard  g(ctx->device);
+    cudaStream_t st   = (cudaStream_t)stream;
+    auto         secs = tree_sections(*ctx, *tree, n);
+    const size_t need_bytes = tree_file_bytes(secs);
+    if (!buf) {
+        *bytes = need_bytes;
+        return FT_OK;
+    }
+    need(*bytes >= need_bytes, "tree export: buffer too small (" + std::to_string(*bytes) + " < " +
+                                   std::to_string(need_bytes) + " bytes)");
+    TreeFileHeader h;
+    std::memset(&h, 0, sizeof(h));
+    std::memcpy(h.magic, "FTB2TREE", 8);
+    h.version    = 1;
+    h.coord_type = ctx->opts.coord_type;
+    h.sfc_type   = ctx->opts.sfc_type;
+    h.periodic   = ctx->opts.periodic;
+    h.key_words  = ctx->opts.coord_type == FT_COORD_U64 ? 2 : 1;
+    h.own_keys   = impl.own_keys ? 1 : 0;
+    h.clean42_ok = impl.clean42_ok ? 1 : 0;
+    h.n          = n;
+    const size_t cb = coord_bytes(ctx->opts.coord_type);
+    if (n && impl.bbox) {
+        unsigned char box[48];
+        FT_CUDA(cudaMemcpyAsync(box, impl.bbox, 6 * cb, cudaMemcpyDeviceToHost, st));
+        FT_CUDA(cudaStreamSynchronize(st));
+        for (int i = 0; i < 6; ++i) std::memcpy(&h.bbox[i], box + i * cb, cb);
+    }
+    unsigned char *out = (unsigned char *)buf;
+    FT_CUDA(cudaMemcpyAsync(out, &h, sizeof(h), cudaMemcpyDefault, st));
+    size_t off = sizeof(h);
+    for (const TreeSection &s : secs) {
+        if (s.bytes) FT_CUDA(cudaMemcpyAsync(out + off, s.dev, s.bytes, cudaMemcpyDefault, st));
+        const size_t padded = align16(s.bytes);
+        static const unsigned char zeros[16] = {}; // padding (buf may be host or device memory)
+        if (padded > s.bytes) FT_CUDA(cudaMemcpyAsync(out + off + s.bytes, zeros, padded - s.bytes, cudaMemcpyDefault, st));
+        off += padded;
+    }
+    FT_CUDA(cudaStreamSynchronize(st));
+    *bytes = need_bytes;
+    FT_API_END
+}
+
+ft_status ft_tree_import(ft_context *ctx, const void *buf, size_t bytes, ft_tree *tree, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree && buf, "null argument");
+    need_owned(tree);
+    need(bytes >= sizeof(TreeFileHeader), "tree import: buffer smaller than the header");
+    DeviceGuard  g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    TreeFileHeader h;
+    FT_CUDA(cudaMemcpyAsync(&h, buf, sizeof(h), cudaMemcpyDefault, st));
+    FT_CUDA(cudaStreamSynchronize(st));
+    need(std::memcmp(h.magic, "FTB2TREE", 8) == 0, "tree import: not a fasttree_b200 tree (bad magic)");
+    need(h.version == 1, "tree import: unsupported format version " + std::to_string(h.version));
+    need(h.coord_type == ctx->opts.coord_type && h.sfc_type == ctx->opts.sfc_type &&
+             (h.periodic != 0) == (ctx->opts.periodic != 0),
+         "tree import: the context's coordinate type, SFC or periodic option differs from the tree's");
+    need(h.n <= (size_t)(INT_MAX / 2), "tree import: leaf count out of range");
+    const size_t n = (size_t)h.n;
+    need(tree->capacity >= n, "tree import: tree capacity is smaller than the stored leaf count");
+    TreeImpl &impl = *(TreeImpl *)tree->impl;
+    if (n) ensure_scratch(impl, ctx->opts, n);
+    tree->num_leaves   = n;
+    tree->num_internal = n ? n - 1 : 0;
+    auto secs          = tree_sections(*ctx, *tree, n);
+    need(bytes >= tree_file_bytes(secs), "tree import: buffer shorter than the stored arrays");
+    const unsigned char *in  = (const unsigned char *)buf;
+    size_t               off = sizeof(h);
+    for (const TreeSection &s : secs) {
+        if (s.bytes) FT_CUDA(cudaMemcpyAsync(s.dev, in + off, s.bytes, cudaMemcpyDefault, st));
+        off += align16(s.bytes);
+    }
+    const size_t cb = coord_bytes(ctx->opts.coord_type);
+    unsigned char box[48];
+    for (int i = 0; i < 6; ++i) std::memcpy(box + i * cb, &h.bbox[i], cb);
+    impl.height_root = -1;
+    if (n) {
+        FT_CUDA(cudaMemcpyAsync(impl.bbox, box, 6 * cb, cudaMemcpyHostToDevice, st));
+        recompute_from_keys(*ctx, *tree, st);
+    }
+    if (n > 1) {
+        uint8_t hr = 0;
+        FT_CUDA(cudaMemcpyAsync(&hr, impl.height, 1, cudaMemcpyDeviceToHost, st));
+        check_status_word(impl, st);
+        impl.height_root = hr;
+    } else {
+        FT_CUDA(cudaStreamSynchronize(st));
+        impl.height_root = 0;
+    }
+    impl.own_keys   = h.own_keys != 0;
+    impl.clean42_ok = h.clean42_ok != 0;
+    impl.in_period = root_in_period(ctx, tree, st);
+    impl.clean42   = impl.clean42_ok && ctx->opts.coord_type == FT_COORD_U64 && impl.in_period;
     FT_API_END
 }
 

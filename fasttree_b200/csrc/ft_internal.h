@@ -144,6 +144,7 @@ void free_query_sort(Context &ctx);
 // this library's own encoding.  Valid until the next call on the context.
 const uint32_t *sfc_query_order(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz,
                                 size_t nq, cudaStream_t st);
+void recompute_from_keys(Context &ctx, ft_tree &tree, cudaStream_t st);
 void refit_bvh(Context &ctx, ft_tree &tree, const void *x, const void *y, const void *z, size_t n, bool leaf_order,
                cudaStream_t st);
 bool fast_knn(Context &ctx, const ft_tree &tree, const void *qx, const void *qy, const void *qz, size_t nq, int k,

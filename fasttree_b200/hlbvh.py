@@ -215,6 +215,26 @@ class TreeSoA:
         check(lib().ft_tree_height(self.ctx.handle, self._p, ctypes.byref(h)))
         return h.value
 
+    def export_size(self) -> int:
+        """Bytes of the serialised tree (ft_tree_export)."""
+        size = ctypes.c_size_t(0)
+        _call(lib().ft_tree_export(self.ctx.handle, self._p, None, ctypes.byref(size), _stream_handle(None)))
+        return size.value
+
+    def export(self, out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+        """The tree in the library's serialised form (ft_tree_export) as a uint8 tensor (host
+        memory unless `out`, of sufficient size, is given, e.g. a device tensor)."""
+        if out is None:
+            out = torch.empty(self.export_size(), dtype=torch.uint8)
+        cap = ctypes.c_size_t(out.numel())
+        _call(lib().ft_tree_export(self.ctx.handle, self._p, _ptr(out), ctypes.byref(cap), _stream_handle(stream)))
+        return out[:cap.value]
+
+    def save(self, path: str):
+        """Writes the serialised tree to a file."""
+        with open(path, "wb") as f:
+            f.write(self.export().numpy().tobytes())
+
     def free(self):
         if getattr(self, "_p", None):
             lib().ft_tree_destroy(self.ctx.handle, self._p)
@@ -324,6 +344,28 @@ def build_bvh(ctx: Context, p, tree: TreeSoA, bbox=None, key=None, scratch=None,
     _call(lib().ft_build_bvh(ctx.handle, _ptr(x), _ptr(y), _ptr(z), n, _ptr(ids), _ptr(gh),
                              None if bb is None else bb.ctypes.data, _ptr(key), tree.c, _stream_handle(stream)))
     return tree
+
+
+def import_tree(ctx: Context, data, tree: Optional[TreeSoA] = None, stream=None) -> TreeSoA:
+    """A tree from its serialised form (ft_tree_import): bytes, a numpy array or a uint8 tensor
+    (host or device).  A new TreeSoA of the stored size unless `tree` is given."""
+    if isinstance(data, (bytes, bytearray, memoryview)):
+        data = np.frombuffer(data, np.uint8)
+    if isinstance(data, np.ndarray):
+        data = np.ascontiguousarray(data, np.uint8)
+    if tree is None:
+        head = data[:48].cpu().numpy() if isinstance(data, torch.Tensor) else data[:48]
+        n = int(np.frombuffer(np.ascontiguousarray(head).tobytes()[40:48], np.uint64)[0]) if len(head) >= 48 else 0
+        tree = TreeSoA(ctx, max(n, 1))
+    _call(lib().ft_tree_import(ctx.handle, _ptr(data), int(data.numel() if isinstance(data, torch.Tensor)
+                                                               else data.size), tree.c, _stream_handle(stream)))
+    return tree
+
+
+def load_tree(ctx: Context, path: str, tree: Optional[TreeSoA] = None) -> TreeSoA:
+    """A tree saved by TreeSoA.save."""
+    with open(path, "rb") as f:
+        return import_tree(ctx, f.read(), tree)
 
 
 def refit_bvh(ctx: Context, p, tree: TreeSoA, leaf_order: bool = False, stream=None) -> TreeSoA:

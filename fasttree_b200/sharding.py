@@ -2,7 +2,7 @@
 
 Self-kNN queries are independent: every rank holds the same tree (each rank builds it from
 the same points -- the build is deterministic, so the trees are bit-identical -- or receives
-it) and answers a contiguous range of sorted leaf ranks, i.e. a contiguous stretch of the
+it from one rank with broadcast_tree) and answers a contiguous range of sorted leaf ranks, i.e. a contiguous stretch of the
 space-filling curve, so each rank's queries stay spatially coherent.  No collective is on
 the data path; ranks only agree on the plan (computed identically everywhere) and reduce
 their timings.
@@ -54,6 +54,45 @@ def max_over_ranks(value: float, device=None) -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def broadcast_bytes(data, src: int, device=None):
+    """Rank src's uint8 tensor on every rank (its size first, then the bytes, both with the
+    process group's broadcast).  `data` is ignored on the other ranks."""
+    import torch
+    import torch.distributed as dist
+    rank = dist.get_rank()
+    size = torch.zeros(1, dtype=torch.int64, device=device)
+    if rank == src:
+        size[0] = int(data.numel())
+    dist.broadcast(size, src)
+    if rank == src:
+        buf = data.to(device).contiguous()
+    else:
+        buf = torch.empty(int(size.item()), dtype=torch.uint8, device=device)
+    dist.broadcast(buf, src)
+    return buf
+
+
+def broadcast_tree(ctx, tree, src: int = 0):
+    """Replicates rank src's built tree on every rank: src serialises it into one device byte
+    buffer (ft_tree_export), the process group broadcasts it (NCCL over NVLink on GPUs) and
+    the other ranks import it (ft_tree_import), so the trees are identical everywhere.
+    `tree` is rank src's tree; elsewhere a tree to import into (None: a new one).  Returns
+    this rank's tree."""
+    import torch
+    import torch.distributed as dist
+
+    from .hlbvh import import_tree
+    dev = f"cuda:{ctx.device}"
+    payload = None
+    if dist.get_rank() == src:
+        payload = torch.empty(tree.export_size(), dtype=torch.uint8, device=dev)
+        tree.export(out=payload)
+    buf = broadcast_bytes(payload, src, dev)
+    if dist.get_rank() == src:
+        return tree
+    return import_tree(ctx, buf, tree)
 
 
 def sharded_self_knn(ctx, tree, k: int, rank: int, world: int, costs=None, results=None, result_dists=None,

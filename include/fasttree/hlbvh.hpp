@@ -308,6 +308,20 @@ inline void refit_bvh(queue &q, const particles<coord_t> &p, TreeSoA &tree) {
     tree.sync();
 }
 
+// Tree serialisation (ft_tree_export / ft_tree_import): the raw SoA arrays and keys behind
+// a fixed header, e.g. to ship a tree between ranks as test/test_mpi.cpp ships its arrays.
+inline std::vector<unsigned char> save_tree(queue &q, const TreeSoA &tree) {
+    size_t bytes = 0;
+    check(ft_tree_export(q.context(), tree.handle, nullptr, &bytes, q.stream()));
+    std::vector<unsigned char> out(bytes);
+    check(ft_tree_export(q.context(), tree.handle, out.data(), &bytes, q.stream()));
+    return out;
+}
+inline void load_tree(queue &q, const std::vector<unsigned char> &data, TreeSoA &tree) {
+    check(ft_tree_import(q.context(), data.data(), data.size(), tree.handle, q.stream()));
+    tree.sync();
+}
+
 // ---- queries -----------------------------------------------------------------------------
 // The kNN queries take the fast walk (SFC-window seeding, exact replay of tied queries):
 // its output is bit-identical to the reference traversal's.  Define

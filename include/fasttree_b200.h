@@ -154,6 +154,21 @@ ft_status ft_build_tree(ft_context *ctx, ft_tree *tree, const void *sorted_keys,
 ft_status ft_refit_bvh(ft_context *ctx, const void *x, const void *y, const void *z, size_t n, int leaf_order,
                        ft_tree *tree, ft_stream_t stream);
 
+/* Tree serialisation: the raw SoA arrays the reference ships between ranks
+ * (test/test_mpi.cpp:71-101), plus the sorted keys, behind a 128-byte header (magic
+ * "FTB2TREE", format version, coordinate / SFC / periodic options, leaf count, build box).
+ * Layout, all little-endian, each array starting on a 16-byte boundary: min_x, max_x, min_y,
+ * max_y, min_z, max_z ((2n-1) coordinates each), left_child, right_child ((n-1) int32),
+ * parent, id, is_ghost (int8), orig_idx ((2n-1) each), key low words (n uint64), key high
+ * words (n uint64, 64-bit coordinates only).
+ * ft_tree_export: buf == NULL stores the size in *bytes; otherwise *bytes is buf's size.
+ * ft_tree_import: the context's options must match the header's and the tree's capacity must
+ * hold the leaves; topology, internal boxes and the query records are recomputed from the
+ * keys and leaves, so the tree equals the exported one.  buf may be host or device memory.
+ * Blocking. */
+ft_status ft_tree_export(ft_context *ctx, const ft_tree *tree, void *buf, size_t *bytes, ft_stream_t stream);
+ft_status ft_tree_import(ft_context *ctx, const void *buf, size_t bytes, ft_tree *tree, ft_stream_t stream);
+
 /* ---------------------------------------------------------------------------------- */
 /* Queries.  Output rows are k wide: idx (size_t, SIZE_MAX when missing) and dist        */
 /* (double for float coords, uint64 for integer coords; -DBL_MAX / 0 when missing).     */

@@ -79,3 +79,24 @@ def test_two_gloo_ranks_agree_and_cover():
     out = mgr.dict()
     mp.spawn(_worker, args=(2, _free_port(), costs, out), nprocs=2, join=True)
     assert out[0] == (True, True, 20.0) and out[1] == (True, True, 20.0)
+
+
+def _bytes_worker(rank, world, port, out):
+    from fasttree_b200.sharding import broadcast_bytes
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        data = torch.from_numpy(np.random.default_rng(4).integers(0, 256, 100_003, dtype=np.uint8))
+        got = broadcast_bytes(data if rank == 1 else None, 1)
+        out[rank] = bool(torch.equal(got, data))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_broadcast_bytes_two_gloo_ranks():
+    """The byte broadcast under broadcast_tree: a buffer of any size from a chosen rank."""
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        mp.start_processes(_bytes_worker, args=(2, _free_port(), out), nprocs=2, start_method="spawn")
+        assert out[0] and out[1]
