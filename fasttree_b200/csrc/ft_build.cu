@@ -565,6 +565,40 @@ void sfc_encode_ref_layout(Context &ctx, TreeImpl &s, const void *x, const void 
     FT_CUDA(cudaGetLastError());
 }
 
+// Two-word keys, second stage: after the passes over the high word, runs of equal high
+// words are put in (low word, input index) order.  The thread at the start of each run
+// insertion-sorts it in place when it holds at most kRunCap keys (stable, so equal keys keep
+// the index order the high-word passes left); a longer run sets flag[0], and the host then
+// finishes with the low-word and high-word passes instead.
+static constexpr int kRunCap = 32;
+
+__global__ void __launch_bounds__(256) hi_run_fixup_kernel(unsigned long long *__restrict__ klo,
+                                                           const unsigned long long *__restrict__ khi,
+                                                           uint32_t *__restrict__ perm, size_t n, uint32_t *flag) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i + 1 < n; i += (size_t)gridDim.x * blockDim.x) {
+        const unsigned long long h = khi[i];
+        if (khi[i + 1] != h || (i > 0 && khi[i - 1] == h)) continue; // not the start of a run
+        size_t e = i + 2;
+        while (e < n && e - i <= (size_t)kRunCap && khi[e] == h) ++e;
+        if (e - i > (size_t)kRunCap) {
+            atomicOr(flag, 1u);
+            continue;
+        }
+        for (size_t j = i + 1; j < e; ++j) {
+            const unsigned long long kl = klo[j];
+            const uint32_t           pv = perm[j];
+            size_t                   m  = j;
+            while (m > i && klo[m - 1] > kl) {
+                klo[m]  = klo[m - 1];
+                perm[m] = perm[m - 1];
+                --m;
+            }
+            klo[m]  = kl;
+            perm[m] = pv;
+        }
+    }
+}
+
 template <int W> static void sort_impl(TreeImpl &s, size_t n, cudaStream_t st) {
     using Cfg     = SortCfg<W>;
     const int D   = 8 * W;
@@ -585,8 +619,7 @@ template <int W> static void sort_impl(TreeImpl &s, size_t n, cudaStream_t st) {
     if (!attr_set) {
         FT_CUDA(cudaFuncSetAttribute(onesweep_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem));
     }
-    for (int d = 0; d < D; ++d) {
-        if (skip[d]) continue;
+    auto pass = [&](int d) {
         int word  = d >> 3;
         int shift = 8 * (d & 7);
         onesweep_kernel<W><<<(unsigned)tiles, kSortThreads, Cfg::smem, st>>>(
@@ -597,7 +630,28 @@ template <int W> static void sort_impl(TreeImpl &s, size_t n, cudaStream_t st) {
         std::swap(s.key_lo, s.tmp_lo);
         std::swap(s.key_hi, s.tmp_hi);
         std::swap(s.perm, s.tmp_perm);
+    };
+    if constexpr (W == 2) {
+        // high-word passes first; equal high words are rare (a 62-bit prefix of the curve), so
+        // a fix-up of their short runs replaces the eight low-word passes
+        for (int d = 8; d < 16; ++d)
+            if (!skip[d]) pass(d);
+        uint32_t *flag = s.tile_counter + 15; // the last high-word pass is done with its counter
+        FT_CUDA(cudaMemsetAsync(flag, 0, sizeof(uint32_t), st));
+        hi_run_fixup_kernel<<<grid_for(n, 256), 256, 0, st>>>((unsigned long long *)s.key_lo,
+                                                              (const unsigned long long *)s.key_hi, s.perm, n, flag);
+        FT_CUDA(cudaGetLastError());
+        uint32_t long_run = 0;
+        FT_CUDA(cudaMemcpyAsync(&long_run, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        FT_CUDA(cudaStreamSynchronize(st));
+        if (!long_run) return;
+        // a long run of equal high words: the full two-word sort from the current order (it
+        // is stable, and within equal keys the current order is the input index order)
+        FT_CUDA(cudaMemsetAsync(s.lookback, 0, (size_t)D * tiles * 256 * sizeof(uint32_t), st));
+        FT_CUDA(cudaMemsetAsync(s.tile_counter, 0, 16 * sizeof(uint32_t), st));
     }
+    for (int d = 0; d < D; ++d)
+        if (!skip[d]) pass(d);
 }
 
 // The same sort over a fixed list of digit positions: no histogram read-back, so no host

@@ -327,3 +327,33 @@ def test_periodic_coordinates_beyond_the_period(coord):
     oi, od = O.knn(opts, ot, qx, qy, qz, 16)
     gi, gd = ft.knn_query(ctx, tree, qx, qy, qz, 16, method=1)
     assert np.array_equal(gi.cpu().numpy(), oi) and np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od))
+
+
+@pytest.mark.parametrize("long_runs", [False, True])
+def test_u64_keys_equal_in_the_high_word(long_runs):
+    """126-bit keys that share their high word (points a few units apart) come out in the full
+    key order with equal keys by input index, through the short-run fix-up and, with runs
+    longer than it takes, through the full two-word sort."""
+    ctx, opts = make(O.U64, O.PEANO_HILBERT, True)
+    rng = np.random.default_rng(17)
+    n_cl = 1500
+    centres = rng.integers(0, 1 << 42, (3, n_cl), dtype=np.uint64)
+    sizes = rng.integers(1, 12, n_cl)
+    if long_runs:
+        sizes[::300] = 60  # runs longer than the fix-up's cap
+    cols = []
+    for d in range(3):
+        c = np.repeat(centres[d], sizes)
+        off = rng.integers(0, 1 << 12, len(c), dtype=np.uint64)  # below the high word's last bit
+        cols.append(np.minimum(c + off, np.uint64((1 << 42) - 1)))
+    perm = rng.permutation(len(cols[0]))
+    x, y, z = (a[perm] for a in cols)
+    x[:50] = x[50:100]  # exact duplicates as well
+    y[:50] = y[50:100]
+    z[:50] = z[50:100]
+    tree, ot = build_both(ctx, opts, x, y, z)
+    assert_tree_equal(tree.to_numpy(), ot, len(x))
+    gi, gd = ft.self_knn_query(ctx, tree, 16, method=1)
+    oi, od = O.self_knn(opts, ot, 16, True)
+    torch.cuda.synchronize()
+    assert np.array_equal(gi.cpu().numpy(), oi) and np.array_equal(gd.cpu().numpy(), od)
