@@ -150,11 +150,12 @@ template <int W> struct SortCfg {
     static constexpr size_t smem = (size_t)tile * (8 * W + 4) + (size_t)kSortWarps * 256 * 4;
 };
 
-template <int W>
+// Digit histograms of digit positions [d0, d0 + ND) (ND = 8 * W by default: every digit).
+template <int W, int ND = 8 * W>
 __global__ void __launch_bounds__(256) radix_hist_kernel(const unsigned long long *__restrict__ klo,
                                                          const unsigned long long *__restrict__ khi, size_t n,
-                                                         uint32_t *hist) {
-    constexpr int D = 8 * W;
+                                                         uint32_t *hist, int d0 = 0) {
+    constexpr int D = ND;
     __shared__ uint32_t s[D * 256];
     for (int i = threadIdx.x; i < D * 256; i += blockDim.x) s[i] = 0;
     __syncthreads();
@@ -166,15 +167,16 @@ __global__ void __launch_bounds__(256) radix_hist_kernel(const unsigned long lon
         unsigned long long w[2] = {valid ? klo[i] : 0ull, (W == 2 && valid) ? khi[i] : 0ull};
         unsigned active = __ballot_sync(0xffffffffu, valid);
 #pragma unroll
-        for (int d = 0; d < D; ++d) {
-            unsigned digit = (unsigned)(w[d >> 3] >> (8 * (d & 7))) & 255u;
+        for (int j = 0; j < D; ++j) {
+            const int d     = d0 + j;
+            unsigned  digit = (unsigned)(w[d >> 3] >> (8 * (d & 7))) & 255u;
             unsigned peers = __match_any_sync(0xffffffffu, valid ? digit : 256u + lane);
-            if (valid && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&s[d * 256 + digit], __popc(peers & active));
+            if (valid && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&s[j * 256 + digit], __popc(peers & active));
         }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < D * 256; i += blockDim.x)
-        if (s[i]) atomicAdd(&hist[i], s[i]);
+        if (s[i]) atomicAdd(&hist[d0 * 256 + i], s[i]);
 }
 
 // Exclusive offsets per digit position; skip[d] = 1 when one digit value holds every key.
@@ -604,15 +606,19 @@ template <int W> static void sort_impl(TreeImpl &s, size_t n, cudaStream_t st) {
     const int D   = 8 * W;
     size_t tiles  = (n + Cfg::tile - 1) / Cfg::tile;
     FT_CUDA(cudaMemsetAsync(s.hist, 0, (16 * 256 + 16) * sizeof(uint32_t), st));
-    radix_hist_kernel<W><<<grid_for(n, 256, 148 * 4), 256, 0, st>>>((const unsigned long long *)s.key_lo,
-                                                                      (const unsigned long long *)s.key_hi, n,
-                                                                      s.hist);
     uint32_t *skip_dev = s.hist + 16 * 256;
-    radix_scan_kernel<<<D, 256, 0, st>>>(s.hist, n, skip_dev);
-    FT_CUDA(cudaGetLastError());
-    uint32_t skip[16] = {0};
-    FT_CUDA(cudaMemcpyAsync(skip, skip_dev, D * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    FT_CUDA(cudaStreamSynchronize(st));
+    uint32_t  skip[16] = {0};
+    // histograms of the digit positions [d0, d0 + 8) of one key word (W == 2: the high word
+    // first; the low word's only if a long run of equal high words needs the full sort)
+    auto histogram = [&](int d0) {
+        radix_hist_kernel<W, 8><<<grid_for(n, 256, 148 * 4), 256, 0, st>>>(
+            (const unsigned long long *)s.key_lo, (const unsigned long long *)s.key_hi, n, s.hist, d0);
+        radix_scan_kernel<<<8, 256, 0, st>>>(s.hist + d0 * 256, n, skip_dev + d0);
+        FT_CUDA(cudaGetLastError());
+        FT_CUDA(cudaMemcpyAsync(skip + d0, skip_dev + d0, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        FT_CUDA(cudaStreamSynchronize(st));
+    };
+    histogram(W == 2 ? 8 : 0);
     FT_CUDA(cudaMemsetAsync(s.lookback, 0, (size_t)D * tiles * 256 * sizeof(uint32_t), st));
     FT_CUDA(cudaMemsetAsync(s.tile_counter, 0, 16 * sizeof(uint32_t), st));
     static bool attr_set = false;
@@ -647,6 +653,7 @@ template <int W> static void sort_impl(TreeImpl &s, size_t n, cudaStream_t st) {
         if (!long_run) return;
         // a long run of equal high words: the full two-word sort from the current order (it
         // is stable, and within equal keys the current order is the input index order)
+        histogram(0);
         FT_CUDA(cudaMemsetAsync(s.lookback, 0, (size_t)D * tiles * 256 * sizeof(uint32_t), st));
         FT_CUDA(cudaMemsetAsync(s.tile_counter, 0, 16 * sizeof(uint32_t), st));
     }
