@@ -234,9 +234,15 @@ FT_D void karras_node(const unsigned long long *klo, const unsigned long long *k
 // Bottom-up refit from one leaf (src/hlbvh.hpp:925-969): the thread climbs; at each parent
 // the first arrival stops and the second merges both child boxes.  The merge also writes
 // the traversal record (both child boxes + indices) and the subtree height.  Child boxes
-// that other threads wrote in this launch are read through L2 (ld.cg) after the acquire
-// fence.  A valid tree is climbed in fewer than n steps; a bad parent ends the climb.
+// that other threads wrote in this launch are read through L2 (ld.cg) after the acquiring
+// arrival.  A valid tree is climbed in fewer than n steps; a bad parent ends the climb.
 // =========================================================================================
+FT_D int atomic_add_acq_rel(int32_t *p, int v) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+
 template <class T>
 FT_D void refit_leaf(int leaf, int n, const int32_t *__restrict__ left, const int32_t *__restrict__ right,
                      const int32_t *__restrict__ parent, T *const *soa, NodeRec<T> *recs, uint8_t *height,
@@ -246,9 +252,9 @@ FT_D void refit_leaf(int leaf, int n, const int32_t *__restrict__ left, const in
     while (curr != 0 && ++steps < n) {
         int p = parent[curr];
         if (p < 0 || p >= n - 1) break;
-        __threadfence();
-        if (atomicAdd(&counters[p], 1) == 0) break;
-        __threadfence();
+        // one acquire-release arrival: this thread's writes of curr are released to the sibling
+        // that arrives second, and the second arrival acquires the first's writes
+        if (atomic_add_acq_rel(&counters[p], 1) == 0) break;
         int l = left[p], r = right[p];
         T   lb[6], rb[6];
 #pragma unroll
