@@ -725,10 +725,12 @@ void self_knn_to_host(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, 
                                 ctx.copy_stream));
         FT_CUDA(cudaEventRecord(ctx.ev_copied[b], ctx.copy_stream));
     };
-    size_t prev0 = 0, prevn = 0;
-    int    c     = 0;
-    for (size_t c0 = 0; c0 < num; c0 += rows, ++c) {
-        const size_t cnt = std::min(rows, num - c0);
+    // the first chunk is small: its walk is the only one no copy overlaps
+    const size_t first = std::min(rows, size_t(1) << 18);
+    size_t       prev0 = 0, prevn = 0;
+    int          c     = 0;
+    for (size_t c0 = 0, cnt = 0; c0 < num; c0 += cnt) {
+        cnt          = std::min(c == 0 ? first : rows, num - c0);
         const int    b   = c & 1;
         if (c >= 2) FT_CUDA(cudaStreamWaitEvent(st, ctx.ev_copied[b], 0)); // buffer b's last rows are out
         self_knn(ctx, tr, ids + c0, cnt, k, excl, (uint64_t *)ctx.stage_idx[b], ctx.stage_dist[b], q, st);
@@ -736,6 +738,7 @@ void self_knn_to_host(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, 
         if (c >= 1) copy_out(prev0, prevn, b ^ 1); // the previous chunk, while this one is walked
         prev0 = c0;
         prevn = cnt;
+        ++c;
     }
     copy_out(prev0, prevn, (c - 1) & 1);
     FT_CUDA(cudaStreamWaitEvent(st, ctx.ev_copied[(c - 1) & 1], 0));
