@@ -130,7 +130,8 @@ def run_batched(args, dev, stream, timed_steps, warmup):
     b.check()
     stats = b.query_stats()
     build_ms = timed(lambda: b.build(off, x, y, z), timed_steps)
-    fast_ms = timed(lambda: b.self_knn(k, method=1, results=idx, result_dists=dst), timed_steps)
+    fast_ms = timed(lambda: b.self_knn(k, method=1, results=idx, result_dists=dst,
+                                       variant=getattr(args, "variant", 0)), timed_steps)
     plain_ms = timed(lambda: b.self_knn(k, method=0, results=idx, result_dists=dst), max(1, timed_steps // 2))
     b.check()
     # the same sets one by one through the single-tree API (the non-batched way)
