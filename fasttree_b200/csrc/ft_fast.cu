@@ -208,6 +208,7 @@ __global__ void __launch_bounds__(kFastThreads)
 
     int  count = 0;
     D    hmax  = D(0);
+    D    thr   = B; // pruning threshold: B until the heap is full, then min(B, k-th distance)
     bool flag  = false;
 
     auto insert = [&](D d2, int32_t id) {
@@ -224,7 +225,10 @@ __global__ void __launch_bounds__(kFastThreads)
             HD(i) = d2;
             HI(i) = id;
             ++count;
-            if (count == k) hmax = HD(0);
+            if (count == k) {
+                hmax = HD(0);
+                thr  = hmax < B ? hmax : B;
+            }
         } else if (d2 < hmax) {
             const D old = hmax;
             int     i   = 0;
@@ -254,6 +258,7 @@ __global__ void __launch_bounds__(kFastThreads)
             HD(i) = d2;
             HI(i) = id;
             hmax  = HD(0);
+            thr   = hmax < B ? hmax : B;
             if (hmax == old) flag = true; // an equal distance stays at the boundary
         } else if (d2 == hmax) {
             flag = true; // a candidate at exactly the k-th distance was left out
@@ -285,7 +290,7 @@ __global__ void __launch_bounds__(kFastThreads)
     // A node is needed unless it is strictly beyond the lane's bound or its k-th distance.
     // Nodes at exactly the k-th distance are walked (not pruned), so any other point at
     // that distance reaches insert() and raises the tie flag there.
-    auto needs = [&](D d2) { return active && !(d2 > B) && !(count >= k && d2 > hmax); };
+    auto needs = [&](D d2) { return active && !(d2 > thr); };
     bool group_done = false;
     if constexpr (VAR == 5) {
         // Group walk: the warp's 32 queries (neighbours on the curve) walk the tree once
@@ -524,6 +529,7 @@ __global__ void __launch_bounds__(kFastThreads)
         // needed internal node is walked next and the others are stacked farthest first.  A
         // full stack hands the query to the replay instead of dropping anything.
         constexpr int kWideStack = 96;
+        const int     ws0 = w0 + n - 1, ws1 = w1 + n - 1; // the seeding window in slot numbers
         int           sn[kWideStack];
         D             sw[kWideStack];
         int           cur  = 0;
@@ -546,7 +552,7 @@ __global__ void __launch_bounds__(kFastThreads)
                                         px, py, pz, bx[i][0], bx[i][1], bx[i][2], bx[i][3], bx[i][4], bx[i][5])
                                   : dist_heap_max<D>();
                 const bool leaf = ch[i] >= n - 1;
-                if (leaf && needs(d[i]) && (ch[i] - (n - 1) < w0 || ch[i] - (n - 1) > w1) && ch[i] != self_leaf)
+                if (leaf && needs(d[i]) && (ch[i] < ws0 || ch[i] > ws1) && ch[i] != self_leaf)
                     insert(d[i], ret_orig ? t.orig_idx[ch[i]] : ch[i] - (n - 1));
             }
 #pragma unroll
