@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "ft_build_dev.cuh"
 #include "ft_common.cuh"
@@ -104,6 +105,23 @@ FT_D float group_filter(const float4 &e, const float q[3], float gerr, float sca
     const float ly = fmaxf(0.0f, fmaf(fabsf(e.y - q[1]) - gerr, scale, -1.0f));
     const float lz = fmaxf(0.0f, fmaf(fabsf(e.z - q[2]) - gerr, scale, -1.0f));
     return fmaf(lz, lz, fmaf(ly, ly, lx * lx));
+}
+
+// Sort key of a needed child in the 4-wide walk and its inverse.  Integer keys are d + 1
+// (0 marks a child that is not needed), saturating at the largest value, whose inverse is
+// then one below the distance: the stacked distance can only err low, which keeps the node
+// (never prunes it).  Floating-point distances are not negative, so -1 marks the others.
+template <class D> FT_D D walk_key(D d) {
+    if constexpr (std::is_floating_point<D>::value) return d;
+    else return d + D(d != ~D(0));
+}
+template <class D> FT_D D walk_key_none() {
+    if constexpr (std::is_floating_point<D>::value) return D(-1);
+    else return D(0);
+}
+template <class D> FT_D D walk_key_dist(D key) {
+    if constexpr (std::is_floating_point<D>::value) return key;
+    else return key - D(1);
 }
 
 template <class T> FT_D T coord_top() {
@@ -557,23 +575,20 @@ __global__ void __launch_bounds__(kFastThreads)
             }
 #pragma unroll
             for (int i = 0; i < 4; ++i) in[i] = ch[i] >= 0 && ch[i] < n - 1 && needs(d[i]);
-            // order the needed internal children farthest first (4-element network; entries
-            // that are not needed sort behind the needed ones)
-            int  oc[4] = {ch[0], ch[1], ch[2], ch[3]};
-            D    od[4] = {d[0], d[1], d[2], d[3]};
-            bool ov[4] = {in[0], in[1], in[2], in[3]};
-            auto cx    = [&](int a, int b) {
-                const bool keep = ov[a] ? (!ov[b] || od[a] >= od[b]) : !ov[b];
-                if (!keep) {
-                    const int  tc = oc[a];
-                    const D    td = od[a];
-                    const bool tv = ov[a];
-                    oc[a] = oc[b];
-                    od[a] = od[b];
-                    ov[a] = ov[b];
-                    oc[b] = tc;
-                    od[b] = td;
-                    ov[b] = tv;
+            // order the needed internal children farthest first (4-element network on one
+            // sort key, walk_key: children that are not needed sort behind the needed ones)
+            int oc[4] = {ch[0], ch[1], ch[2], ch[3]};
+            D   od[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) od[i] = in[i] ? walk_key<D>(d[i]) : walk_key_none<D>();
+            auto cx = [&](int a, int b) {
+                if (od[a] < od[b]) {
+                    const int tc = oc[a];
+                    const D   td = od[a];
+                    oc[a]        = oc[b];
+                    od[a]        = od[b];
+                    oc[b]        = tc;
+                    od[b]        = td;
                 }
             };
             cx(0, 1);
@@ -581,7 +596,7 @@ __global__ void __launch_bounds__(kFastThreads)
             cx(0, 2);
             cx(1, 3);
             cx(1, 2);
-            const int nv = (int)ov[0] + (int)ov[1] + (int)ov[2] + (int)ov[3];
+            const int nv = (int)in[0] + (int)in[1] + (int)in[2] + (int)in[3];
             if (nv > 0) {
                 if (wsp + nv - 1 > kWideStack) {
                     flag = true; // cannot stack them all: the reference traversal reruns the query
@@ -591,7 +606,7 @@ __global__ void __launch_bounds__(kFastThreads)
                 for (int i = 0; i < 3; ++i)
                     if (i < nv - 1) {
                         sn[wsp] = oc[i];
-                        sw[wsp] = od[i];
+                        sw[wsp] = walk_key_dist<D>(od[i]);
                         ++wsp;
                     }
                 cur = nv == 1 ? oc[0] : nv == 2 ? oc[1] : nv == 3 ? oc[2] : oc[3];
