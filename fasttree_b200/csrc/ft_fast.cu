@@ -107,6 +107,18 @@ FT_D float group_filter(const float4 &e, const float q[3], float gerr, float sca
     return fmaf(lz, lz, fmaf(ly, ly, lx * lx));
 }
 
+// Float bounds of a distance for the 4-wide walk's stack: rounded down for a stacked node,
+// rounded up for the threshold it is compared with (non-negative values, so the float order
+// never drops a node whose exact distance is within the threshold).  Only active lanes pop.
+template <class D> FT_D float stack_key_down(D d) {
+    if constexpr (std::is_floating_point<D>::value) return __double2float_rd((double)d);
+    else return __ull2float_rd((unsigned long long)d);
+}
+template <class D> FT_D float stack_key_up(D d) {
+    if constexpr (std::is_floating_point<D>::value) return __double2float_ru((double)d);
+    else return __ull2float_ru((unsigned long long)d);
+}
+
 // Sort key of a needed child in the 4-wide walk and its inverse.  Integer keys are d + 1
 // (0 marks a child that is not needed), saturating at the largest value, whose inverse is
 // then one below the distance: the stacked distance can only err low, which keeps the node
@@ -548,8 +560,12 @@ __global__ void __launch_bounds__(kFastThreads)
         // full stack hands the query to the replay instead of dropping anything.
         constexpr int kWideStack = 96;
         const int     ws0 = w0 + n - 1, ws1 = w1 + n - 1; // the seeding window in slot numbers
-        int           sn[kWideStack];
-        D             sw[kWideStack];
+        // stack entries: node index in the low word, a float lower bound of its distance in the
+        // high word (one 8-byte local-memory access per push or pop); thr_up is the pruning
+        // threshold rounded up, so a popped node is dropped only when it is surely beyond it
+        unsigned long long st[kWideStack];
+        float              thr_up = stack_key_up<D>(thr);
+        D                  thr_seen = thr;
         int           cur  = 0;
         int           wsp  = 0;
         bool          have = !group_done && active && n > 1 && needs(sd[0]);
@@ -605,17 +621,23 @@ __global__ void __launch_bounds__(kFastThreads)
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
                     if (i < nv - 1) {
-                        sn[wsp] = oc[i];
-                        sw[wsp] = walk_key_dist<D>(od[i]);
+                        st[wsp] = ((unsigned long long)__float_as_uint(stack_key_down<D>(walk_key_dist<D>(od[i])))
+                                   << 32) |
+                                  (uint32_t)oc[i];
                         ++wsp;
                     }
                 cur = nv == 1 ? oc[0] : nv == 2 ? oc[1] : nv == 3 ? oc[2] : oc[3];
             } else {
                 have = false;
+                if (thr != thr_seen) { // the heap tightened since the last pop
+                    thr_seen = thr;
+                    thr_up   = stack_key_up<D>(thr);
+                }
                 while (wsp > 0) {
                     --wsp;
-                    if (needs(sw[wsp])) {
-                        cur  = sn[wsp];
+                    const unsigned long long e = st[wsp];
+                    if (!(__uint_as_float((uint32_t)(e >> 32)) > thr_up)) {
+                        cur  = (int)(uint32_t)e;
                         have = true;
                         break;
                     }
