@@ -2,7 +2,8 @@
 // reference's test/test_self_knn.cpp and test/main.cpp: host brute force over the sorted
 // leaves, exact integer distances / 1e-4 relative float tolerance, indices compared at
 // untied ranks only, no duplicate indices, sentinels beyond the available count; range
-// count and kNN on the 10^3 grid; ghost visibility.  Built once per configuration macro set
+// count and kNN on the 10^3 grid; ghost visibility; a refit-only update and a save / load
+// round trip (this library's additions).  Built once per configuration macro set
 // (tests/test_cpp_api.py) and run on the GPU.  Exit code 0 = all passed.
 #include <fasttree/hlbvh.hpp>
 
@@ -210,6 +211,17 @@ int main() {
         }
         std::printf("  %s k > MAXK throws invalid_argument: %s\n", kind.c_str(), threw ? "PASSED" : "FAILED");
         failures += !threw;
+        // refit-only update (new positions for the same points, topology kept), then a
+        // save / load round trip of the refit tree
+        {
+            auto p2 = generate(kind, 1000, 43);
+            refit_bvh(q, p2, tree);
+            self_knn_case<32>(q, tree, 16, true, kind + " refit k=16");
+            std::vector<unsigned char> blob = save_tree(q, tree);
+            TreeSoA                    t2(q, tree.num_leaves);
+            load_tree(q, blob, t2);
+            self_knn_case<32>(q, t2, 16, true, kind + " loaded k=16");
+        }
     }
     // 10^3 grid (test/main.cpp:84-241): range count vs brute force at (52,52,52), r <= 20
     {
