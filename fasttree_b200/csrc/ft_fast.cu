@@ -39,6 +39,10 @@ static constexpr int kFastStack = 64;
 // threads at k = 32), so small blocks pack 9 per SM (18 warps) where 128-thread blocks fit 4.
 static constexpr int kFastWarps = 2;
 static constexpr int kFastThreads = 32 * kFastWarps;
+// Warps per block for a heap capacity: k <= 32 heaps take 12 KB per warp, so two-warp blocks
+// fit 9 per SM; 64-entry heaps take 24 KB per warp, and one-warp blocks fit 9 warps per SM
+// where two-warp blocks fit 8.
+template <int KC> constexpr int fast_warps() { return KC > 32 ? 1 : kFastWarps; }
 
 // Group walk (variant 5): a lower bound of the walk's distance from every point of the
 // group box [g0, g1] (per axis) to a node box b (minx, maxx, miny, maxy, minz, maxz).  Each
@@ -164,7 +168,7 @@ template <class T> FT_D T warp_max_t(T v) {
 }
 
 template <class T, int PER, int KC, int VAR>
-__global__ void __launch_bounds__(kFastThreads)
+__global__ void __launch_bounds__(32 * fast_warps<KC>())
     fast_self_knn_kernel(TreeDev<T> t_all, BatchDev bt, const T *__restrict__ qx, const T *__restrict__ qy,
                          const T *__restrict__ qz, const uint32_t *__restrict__ order,
                          const int32_t *__restrict__ leaf_ids, int num, int k,
@@ -174,6 +178,7 @@ __global__ void __launch_bounds__(kFastThreads)
                          int32_t *__restrict__ replay_ranks, int32_t *__restrict__ replay_rows,
                          uint32_t *replay_count, uint32_t *status, unsigned long long *visit_count) {
     using D = typename Coord<T>::dist_t;
+    constexpr int kFastWarps = fast_warps<KC>(), kFastThreads = 32 * kFastWarps; // this heap's block shape
     extern __shared__ __align__(16) unsigned char smem[];
     D       *hd  = reinterpret_cast<D *>(smem);
     int32_t *hix = reinterpret_cast<int32_t *>(hd + KC * kFastThreads);
@@ -834,15 +839,16 @@ static void launch_fast_t(const TreeDev<T> &tv, const BatchDev &bt, const ExtQue
                           int32_t *rr, int32_t *rw, uint32_t *rc, uint32_t *status, int variant,
                           unsigned long long *visits, cudaStream_t st) {
     using D     = typename Coord<T>::dist_t;
-    size_t smem = (size_t)KC * kFastThreads * (sizeof(D) + 4);
+    constexpr int threads = 32 * fast_warps<KC>();
+    size_t        smem    = (size_t)KC * threads * (sizeof(D) + 4);
     auto   fn   = variant == 0 ? fast_self_knn_kernel<T, PER, KC, 0>
                   : variant == 1 ? fast_self_knn_kernel<T, PER, KC, 1>
                   : variant == 4 ? fast_self_knn_kernel<T, PER, KC, 4>
                   : variant == 5 ? fast_self_knn_kernel<T, PER, KC, 5>
                                  : fast_self_knn_kernel<T, PER, KC, 2>;
     FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int blocks = (num + kFastThreads - 1) / kFastThreads;
-    fn<<<blocks, kFastThreads, smem, st>>>(tv, bt, (const T *)eq.x, (const T *)eq.y, (const T *)eq.z, eq.order,
+    int blocks = (num + threads - 1) / threads;
+    fn<<<blocks, threads, smem, st>>>(tv, bt, (const T *)eq.x, (const T *)eq.y, (const T *)eq.z, eq.order,
                                            leaf_ids, num, k, half, excl ? 1 : 0, ro ? 1 : 0,
                                            (const D *)bound, (unsigned long long *)idx, (D *)dist, rr, rw, rc,
                                            status, visits);
