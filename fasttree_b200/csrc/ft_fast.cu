@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(32 * fast_warps<KC>())
     constexpr int kFastWarps = fast_warps<KC>(), kFastThreads = 32 * kFastWarps; // this heap's block shape
     extern __shared__ __align__(16) unsigned char smem[];
     D       *hd  = reinterpret_cast<D *>(smem);
-    int32_t *hix = reinterpret_cast<int32_t *>(hd + KC * kFastThreads);
+    int32_t *hix = reinterpret_cast<int32_t *>(hd + k * kFastThreads); // heaps sized for k (<= KC)
     __shared__ int32_t s_node[kFastWarps][kFastStack];
 
     const int      tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -840,7 +840,7 @@ static void launch_fast_t(const TreeDev<T> &tv, const BatchDev &bt, const ExtQue
                           unsigned long long *visits, cudaStream_t st) {
     using D     = typename Coord<T>::dist_t;
     constexpr int threads = 32 * fast_warps<KC>();
-    size_t        smem    = (size_t)KC * threads * (sizeof(D) + 4);
+    size_t        smem    = (size_t)std::max(k, 1) * threads * (sizeof(D) + 4); // heaps of k entries
     auto   fn   = variant == 0 ? fast_self_knn_kernel<T, PER, KC, 0>
                   : variant == 1 ? fast_self_knn_kernel<T, PER, KC, 1>
                   : variant == 4 ? fast_self_knn_kernel<T, PER, KC, 4>
