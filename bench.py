@@ -647,12 +647,17 @@ def run_ours(args):
     e2e = None
     if not args.no_e2e:
         hx, hy, hz = (torch.from_numpy(a).pin_memory() for a in (w["x"], w["y"], w["z"]))
-        hi = torch.empty(n * k, dtype=torch.uint64).pin_memory()
-        hd = torch.empty(n * k, dtype=dst.dtype).pin_memory()
-        e_steps = max(1, min(args.steps, 3))
-        # double-buffered inputs: step s+1's coordinates go up on a side stream while step s
-        # walks and its results come down (PCIe carries both directions at once); each step
-        # still uploads its own inputs inside the timed region
+        e_steps = max(1, min(args.steps, 5))
+        # Two lanes, each with its own context (staging buffers, copy stream), tree, stream and
+        # pinned result buffers, take the steps in turn: step s+1's upload, build and first
+        # walk overlap step s's copy-out (the PCIe link then carries both directions and the
+        # SMs build while the copy engines drain).  Every step still uploads its own inputs,
+        # builds, queries and brings its 5 GB of rows to host memory inside the timed region.
+        ctxs = [ctx, ft.Context(w["coord"], w["sfc"], periodic=w["periodic"], device=local)]
+        trees = [tree, ft.TreeSoA(ctxs[1], n)]
+        lanes = [stream, torch.cuda.Stream(device=dev)]
+        his = [torch.empty(n * k, dtype=torch.uint64).pin_memory() for _ in range(2)]
+        hds = [torch.empty(n * k, dtype=dst.dtype).pin_memory() for _ in range(2)]
         up = torch.cuda.Stream(device=dev)
         bufs = [tuple(torch.empty(n, dtype=x.dtype, device=dev) for _ in range(3)) for _ in range(2)]
         uploaded = [torch.cuda.Event() for _ in range(2)]
@@ -665,25 +670,43 @@ def run_ours(args):
                     d.copy_(h, non_blocking=True)
                 uploaded[j % 2].record(up)
 
+        def step_on(lane, s):
+            st = lanes[lane]
+            with torch.cuda.stream(st):
+                st.wait_event(uploaded[s % 2])
+                dx, dy, dz = bufs[s % 2]
+                ft.build_bvh(ctxs[lane], ft.particles(dx, dy, dz), trees[lane], stream=st)
+                built[s % 2].record(st)
+                if s + 1 < e_steps:
+                    upload(s + 1)
+                # results straight into pinned host memory (the library overlaps the copy-out)
+                if shard:
+                    ft.self_knn_query_subset(ctxs[lane], trees[lane], shard_ids, k, his[lane], hds[lane],
+                                             exclude_self=True, max_k=max(32, k), method=method, stream=st)
+                else:
+                    ft.self_knn_query(ctxs[lane], trees[lane], k, his[lane], hds[lane], exclude_self=True,
+                                      max_k=max(32, k), method=method, half_window=args.half,
+                                      variant=args.variant, stream=st)
+
+        # untimed warm-up: one step on each lane (staging buffers, copy streams, tree scratch)
+        for lane in range(2):
+            upload(0)
+            step_on(lane, 0)
+            torch.cuda.synchronize()
+        uploaded = [torch.cuda.Event() for _ in range(2)]
+        built = [torch.cuda.Event() for _ in range(2)]
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        e0.record(lanes[0])
+        lanes[1].wait_event(e0)
+        up.wait_event(e0)  # the first upload is inside the timed region
         upload(0)
-        for step in range(e_steps):
-            stream.wait_event(uploaded[step % 2])
-            dx, dy, dz = bufs[step % 2]
-            ft.build_bvh(ctx, ft.particles(dx, dy, dz), tree)
-            built[step % 2].record(stream)
-            if step + 1 < e_steps:
-                upload(step + 1)
-            # results straight into pinned host memory (the library overlaps the copy-out)
-            if shard:
-                ft.self_knn_query_subset(ctx, tree, shard_ids, k, hi, hd, exclude_self=True, max_k=max(32, k),
-                                         method=method)
-            else:
-                ft.self_knn_query(ctx, tree, k, hi, hd, exclude_self=True, max_k=max(32, k), method=method,
-                                  half_window=args.half, variant=args.variant)
-        e1.record(stream)
+        for s in range(e_steps):
+            step_on(s % 2, s)
+        done = torch.cuda.Event()
+        done.record(lanes[1])
+        lanes[0].wait_event(done)
+        e1.record(lanes[0])
         torch.cuda.synchronize()
         e_ms = e0.elapsed_time(e1) / e_steps
         te = torch.tensor([e_ms], device=dev)
