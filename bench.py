@@ -126,14 +126,18 @@ def run_batched(args, dev, stream, timed_steps, warmup):
         torch.cuda.synchronize()
         return g0.elapsed_time(g1) / steps
 
-    graph_ms = timed(lambda: b.build_knn(off, x, y, z, k, idx, dst, method=1), timed_steps)
+    graph_ms = timed(lambda: b.build_knn(off, x, y, z, k, idx, dst, method="fast"), timed_steps)
     b.check()
     stats = b.query_stats()
     build_ms = timed(lambda: b.build(off, x, y, z), timed_steps)
-    fast_ms = timed(lambda: b.self_knn(k, method=1, results=idx, result_dists=dst,
+    fi, fd = torch.empty_like(idx), torch.empty_like(dst)
+    fast_ms = timed(lambda: b.self_knn(k, method="fast", results=fi, result_dists=fd,
                                        variant=getattr(args, "variant", 0)), timed_steps)
-    plain_ms = timed(lambda: b.self_knn(k, method=0, results=idx, result_dists=dst), max(1, timed_steps // 2))
+    pi, pd = torch.empty_like(idx), torch.empty_like(dst)
+    plain_ms = timed(lambda: b.self_knn(k, method="plain", results=pi, result_dists=pd), max(1, timed_steps // 2))
     b.check()
+    bit_exact = {"graph_vs_plain": rows_equal(idx, dst, pi, pd), "fast_vs_plain": rows_equal(fi, fd, pi, pd)}
+    del fi, fd, pi, pd
     # the same sets one by one through the single-tree API (the non-batched way)
     offs = w["off"]
     if getattr(args, "no_per_set_loop", False):
@@ -141,7 +145,7 @@ def run_batched(args, dev, stream, timed_steps, warmup):
         return {"workload": w["name"], "n_sets": S, "n_points": N, "k": k,
                 "graph_build_plus_query_ms": graph_ms, "value": N / (graph_ms / 1e3), "unit": "queries/s",
                 "build_ms": build_ms, "query_fast_ms": fast_ms, "query_plain_ms": plain_ms,
-                "replayed": stats["replayed"]}
+                "replayed": stats["replayed"], "bit_exact": bit_exact}
     tree = ft.TreeSoA(ctx, int(np.diff(offs).max()))
     li = torch.empty(int(np.diff(offs).max()) * k, dtype=torch.uint64, device=dev)
     ld = torch.empty_like(li, dtype=torch.float64)
@@ -150,7 +154,7 @@ def run_batched(args, dev, stream, timed_steps, warmup):
         for s in range(S):
             a, e = int(offs[s]), int(offs[s + 1])
             ft.build_bvh(ctx, ft.particles(x[a:e], y[a:e], z[a:e]), tree)
-            ft.self_knn_query(ctx, tree, k, li[:(e - a) * k], ld[:(e - a) * k], method=1)
+            ft.self_knn_query(ctx, tree, k, li[:(e - a) * k], ld[:(e - a) * k], method="fast")
     t0 = time.perf_counter()
     loop()
     torch.cuda.synchronize()
@@ -161,12 +165,12 @@ def run_batched(args, dev, stream, timed_steps, warmup):
             "build_ms": build_ms, "query_fast_ms": fast_ms, "query_plain_ms": plain_ms,
             "query_fast_qps": N / (fast_ms / 1e3), "query_plain_qps": N / (plain_ms / 1e3),
             "per_set_loop_ms": loop_ms, "per_set_loop_qps": N / (loop_ms / 1e3),
-            "replayed": stats["replayed"],
+            "replayed": stats["replayed"], "bit_exact": bit_exact,
             "note": "graph = ft_batch_build_knn (build + fast self-kNN, one CUDA graph); per-set loop = "
-                    "build_bvh + self_knn_query(method=1) per set through the single-tree API (wall clock)"}
+                    "build_bvh + self_knn_query(method='fast') per set through the single-tree API (wall clock)"}
 
 
-def run_learned(args, ctx, tree, n, k, stream, fast_visits):
+def run_learned(args, ctx, tree, n, k, stream, fast_visits, ref_rows=None):
     """Self-kNN with the learned radius bound on the resident tree: network trained on the
     exact self-kNN of a separate 2M draw (same generator, seed 12), 2000 Adam steps."""
     import torch
@@ -205,6 +209,8 @@ def run_learned(args, ctx, tree, n, k, stream, fast_visits):
         st = ctx.query_stats()
         out["by_inflation"][str(infl)] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s",
                                           "replayed": st["replayed"], "visits_per_query": st["visits"] / n}
+        if ref_rows is not None:
+            out["by_inflation"][str(infl)]["bit_exact"] = rows_equal(idx, dst, *ref_rows)
     out["fast_visits_per_query"] = fast_visits
     out["note"] = ("features + predict + bounded walk + replay, bit-exact; see the fast walk's line for the "
                    "method without the bound")
@@ -229,7 +235,7 @@ def run_knn_external(args, stream):
     idx = torch.empty(nq * k, dtype=torch.uint64, device=dq[0].device)
     dst = torch.empty(nq * k, dtype=torch.float64, device=dq[0].device)
     res = {}
-    for method, steps in ((1, 5), (0, 1)):
+    for method, steps in (("fast", 5), ("plain", 1)):
         ft.knn_query(ctx, tree, *dq, k, idx, dst, max_k=mk, method=method)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -239,14 +245,14 @@ def run_knn_external(args, stream):
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / steps
-        res["fast" if method else "plain"] = {"ms_per_step": ms, "value": nq / (ms / 1e3), "unit": "queries/s"}
-        if method:
+        res[method] = {"ms_per_step": ms, "value": nq / (ms / 1e3), "unit": "queries/s"}
+        if method == "fast":
             st = ctx.query_stats()
             res["fast"]["replayed"] = st["replayed"]
             res["fast"]["visits_per_query"] = st["visits"] / nq
-            fi = idx.clone()
-    res["bit_exact"] = bool(torch.equal(fi, idx))
-    pi = idx.clone()
+            fi, fd = idx.clone(), dst.clone()
+    res["bit_exact"] = rows_equal(fi, fd, idx, dst)
+    pi, pd = idx.clone(), dst.clone()
     # learned bound: network trained on the exact self-kNN of a separate 100K uniform draw
     from fasttree_b200 import learned as L
     tx, ty, tz = datasets.uniform(100_000, seed=11)
@@ -261,10 +267,19 @@ def run_knn_external(args, stream):
         st = ctx.query_stats()
         learned["by_inflation"][str(infl)] = {"ms_per_step": ms, "value": nq / (ms / 1e3), "unit": "queries/s",
                                               "replayed": st["replayed"], "visits_per_query": st["visits"] / nq,
-                                              "bit_exact": bool(torch.equal(pi, idx))}
+                                              "bit_exact": rows_equal(pi, pd, idx, dst)}
     res["learned"] = learned
     res["workload"] = "1M external queries on 100K uniform float64, Morton, k=64, MAXK=256 (SortedMergeHeap)"
     return res
+
+
+def rows_equal(ai, ad, bi, bd) -> bool:
+    """Two sets of kNN rows equal bit for bit: indices and the distances' bit patterns."""
+    import torch
+    if ai.numel() != bi.numel():
+        return False
+    return bool(torch.equal(ai.view(torch.int64), bi.view(torch.int64)) and
+                torch.equal(ad.view(torch.int64), bd.view(torch.int64)))
 
 
 def _timed(stream, fn, steps, warmup=1):
@@ -292,16 +307,18 @@ def run_cfg2_extra(ctx, tree, x, y, z, n, stream):
     dev = x.device
     out = {}
     for k2, mk in ((1, 32), (64, 64)):
-        idx = torch.empty(n * k2, dtype=torch.uint64, device=dev)
-        dst = torch.empty(n * k2, dtype=ft.dist_torch_dtype(ctx.coord), device=dev)
+        bufs = {m: (torch.empty(n * k2, dtype=torch.uint64, device=dev),
+                    torch.empty(n * k2, dtype=ft.dist_torch_dtype(ctx.coord), device=dev)) for m in ("fast", "plain")}
         row = {}
-        for name, method, steps in (("fast", 1, 3), ("plain", 0, 2)):
-            ms = _timed(stream, lambda: ft.self_knn_query(ctx, tree, k2, idx, dst, max_k=mk, method=method), steps)
+        for name, steps in (("fast", 3), ("plain", 2)):
+            bi, bd = bufs[name]
+            ms = _timed(stream, lambda: ft.self_knn_query(ctx, tree, k2, bi, bd, max_k=mk, method=name), steps)
             row[name] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s"}
-            if method:
+            if name == "fast":
                 row[name]["replayed"] = ctx.query_stats()["replayed"]
+        row["bit_exact"] = rows_equal(*bufs["fast"], *bufs["plain"])
         out[f"self_knn_k{k2}"] = row
-        del idx, dst
+        del bufs
     max_per = 512
     r0 = torch.zeros(n, dtype=torch.int64, device=dev).view(torch.uint64)
     r1 = torch.full((n,), int(2e-3 * 2 ** 40), dtype=torch.int64, device=dev).view(torch.uint64)
@@ -334,9 +351,9 @@ def run_cfg2_extra(ctx, tree, x, y, z, n, stream):
         ft.build_bvh(ctx, ft.particles(x, y, z), tree)  # start from the tree of the unmoved points
         np_ = ft.particles(moved(x), moved(y), moved(z))
         refit_ms = _timed(stream, lambda: ft.refit_bvh(ctx, np_, tree), 3)
-        q_refit = _timed(stream, lambda: ft.self_knn_query(ctx, tree, 32, idx, dst, method=1), 2)
+        q_refit = _timed(stream, lambda: ft.self_knn_query(ctx, tree, 32, idx, dst, method="fast"), 2)
         rebuild_ms = _timed(stream, lambda: ft.build_bvh(ctx, np_, fresh), 2)
-        q_fresh = _timed(stream, lambda: ft.self_knn_query(ctx, fresh, 32, idx, dst, method=1), 2)
+        q_fresh = _timed(stream, lambda: ft.self_knn_query(ctx, fresh, 32, idx, dst, method="fast"), 2)
         out["refit"][f"sigma_{sigma:g}_box"] = {"refit_ms": refit_ms, "rebuild_ms": rebuild_ms,
                                                "self_knn_k32_on_refit_ms": q_refit,
                                                "self_knn_k32_on_rebuild_ms": q_fresh}
@@ -369,25 +386,48 @@ def run_cfg5(args, stream):
     out = {"workload": f"cfg5: {n / 1e6:g}M clustered uint64 (100,000 spheres, seed 5), Peano-Hilbert, periodic, k=64",
            "n_points": n, "gen_s": gen_s, "build_ms": build_ms, "tree_height": tree.height(),
            "output_bytes": 2 * idx.numel() * 8}
-    for name, method, steps in (("fast", 1, 2), ("plain", 0, 1)):
-        ms = _timed(stream, lambda: ft.self_knn_query(ctx, tree, k, idx, dst, max_k=k, method=method), steps)
-        out[name] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s"}
-        if method:
-            out[name]["replayed"] = ctx.query_stats()["replayed"]
+    ms = _timed(stream, lambda: ft.self_knn_query(ctx, tree, k, idx, dst, max_k=k, method="plain"), 1)
+    out["plain"] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s"}
+    # the fast walk's rows are compared with the plain ones in slices (one extra row buffer
+    # of the 51 GB would not fit beside them)
+    fi = torch.empty(n // 10 * k, dtype=torch.uint64, device=dev)
+    fd = torch.empty_like(fi)
+    ms = _timed(stream, lambda: ft.self_knn_query(ctx, tree, k, idx, dst, max_k=k, method="fast"), 2)
+    out["fast"] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s",
+                   "replayed": ctx.query_stats()["replayed"]}
+    same = True
+    for s0 in range(0, n, n // 10):
+        s1 = min(n, s0 + n // 10)
+        ids = torch.arange(s0, s1, dtype=torch.int32, device=dev)
+        ft.self_knn_query_subset(ctx, tree, ids, k, fi[:(s1 - s0) * k], fd[:(s1 - s0) * k], max_k=k, method="plain")
+        same = same and rows_equal(idx[s0 * k:s1 * k], dst[s0 * k:s1 * k], fi[:(s1 - s0) * k], fd[:(s1 - s0) * k])
+    out["fast"]["bit_exact"] = same
+    del fi, fd
     g = torch.Generator(device="cpu").manual_seed(5)
     ids = torch.randperm(n, generator=g)[: n // 10].to(torch.int32).to(dev)
     si = torch.empty(len(ids) * k, dtype=torch.uint64, device=dev)
     sd = torch.empty(len(ids) * k, dtype=torch.uint64, device=dev)
-    for name, method in (("subset_fast", 1), ("subset_plain", 0)):
+    sub_rows = {}
+    for name, method in (("subset_fast", "fast"), ("subset_plain", "plain")):
         ms = _timed(stream, lambda: ft.self_knn_query_subset(ctx, tree, ids, k, si, sd, max_k=k, method=method), 2)
         out[name] = {"ms_per_step": ms, "value": len(ids) / (ms / 1e3), "unit": "queries/s",
                      "queries": f"{len(ids)} random leaf ids (10%, seed 5)"}
-    del si, sd
+        sub_rows[method] = (si.clone(), sd.clone())
+    out["subset_fast"]["bit_exact"] = rows_equal(*sub_rows["fast"], *sub_rows["plain"])
+    del si, sd, sub_rows
     tx, ty, tz = datasets.clustered_fixed(2_000_000, n_spheres=4000, seed=15)
     model, losses = L.train_bound(ctx, tx, ty, tz, k, steps=2000, batch=8192, seed=0)
     ms = _timed(stream, lambda: L.self_knn_query_learned(ctx, tree, model, k, idx, dst, inflation=1.3, max_k=k), 2)
     st = ctx.query_stats()
+    lsame = True
+    for s0 in range(0, n, n // 10):  # against the plain rows, a tenth at a time
+        s1 = min(n, s0 + n // 10)
+        ids2 = torch.arange(s0, s1, dtype=torch.int32, device=dev)
+        pi2, pd2 = ft.self_knn_query_subset(ctx, tree, ids2, k, max_k=k, method="plain")
+        lsame = lsame and rows_equal(idx[s0 * k:s1 * k], dst[s0 * k:s1 * k], pi2.reshape(-1), pd2.reshape(-1))
+        del pi2, pd2
     out["learned"] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s", "inflation": 1.3,
+                      "bit_exact": lsame,
                       "replayed": st["replayed"], "train_draw": "2M clustered uint64 (4000 spheres, seed 15)",
                       "final_loss": float(np.mean(losses[-100:]))}
     return out
@@ -469,9 +509,9 @@ def cpu_baseline(w, args, threads=None):
     sample = min(args.cpu_sample, w["n"])
     ids = np.linspace(0, w["n"] - 1, sample).astype(np.int32)
     t0 = time.perf_counter()
-    O.self_knn(opts, tree, args.k, True, leaf_ids=ids)
+    rows = O.self_knn(opts, tree, args.k, True, leaf_ids=ids)
     q_s = time.perf_counter() - t0
-    return tree, {"value": sample / q_s, "unit": "queries/s", "cores": nthreads, "kind": "port",
+    return rows, {"value": sample / q_s, "unit": "queries/s", "cores": nthreads, "kind": "port",
                   "sample": f"{sample} evenly spaced leaf queries of the {w['n']}-point tree (k={args.k}); "
                             f"CPU build of the same tree took {build_s * 1e3:.0f} ms",
                   "build_ms": build_s * 1e3}
@@ -528,7 +568,7 @@ def run_ours(args):
         ft.build_bvh(ctx, ft.particles(*(torch.from_numpy(a).to(f"cuda:{local}") for a in (w["x"], w["y"], w["z"]))),
                      tree)
         st = torch.cuda.current_stream()
-        ft.self_knn_query(ctx, tree, args.k, method=1)
+        ft.self_knn_query(ctx, tree, args.k, method="fast")
         torch.cuda.synchronize()
         r = run_learned(args, ctx, tree, w["n"], args.k, st, ctx.query_stats()["visits"] / w["n"])
         r["workload"] = w["name"]
@@ -590,6 +630,10 @@ def run_ours(args):
     # ---- self-kNN timing (device-resident tree and outputs) ----
     idx = torch.empty(n * k, dtype=torch.uint64, device=dev)
     dst = torch.empty(n * k, dtype=ft.dist_torch_dtype(ctx.coord), device=dev)
+    # each method writes its own rows, so the two can be compared bit for bit afterwards
+    out_bufs = {1: (idx, dst)}
+    if not args.only_headline:
+        out_bufs[0] = (torch.empty_like(idx), torch.empty_like(dst))
 
     shard = args.shard and world > 1
     if shard:  # this rank's contiguous share of the leaf ranks (same tree on every rank)
@@ -598,11 +642,13 @@ def run_ours(args):
         shard_ids = torch.arange(s0, s1, dtype=torch.int32, device=dev)
 
     def query(method):
+        oi, od = out_bufs[method] if method in out_bufs else out_bufs[1]
+        name = "fast" if method == 1 else "plain"
         if shard:
-            ft.self_knn_query_subset(ctx, tree, shard_ids, k, idx, dst, exclude_self=True, max_k=max(32, k),
-                                     method=method)
+            ft.self_knn_query_subset(ctx, tree, shard_ids, k, oi, od, exclude_self=True, max_k=max(32, k),
+                                     method=name)
         else:
-            ft.self_knn_query(ctx, tree, k, idx, dst, exclude_self=True, max_k=max(32, k), method=method,
+            ft.self_knn_query(ctx, tree, k, oi, od, exclude_self=True, max_k=max(32, k), method=name,
                               half_window=args.half, variant=args.variant)
 
     def time_method(method):
@@ -639,9 +685,20 @@ def run_ours(args):
     value = units / (ms_per_step / 1e3)
     method = headline
     plain = None
+    bit_exact = {"checked": "rows of the fast walk against the plain traversal on all queries; the "
+                            "headline rows at the CPU baseline's sample against the oracle"}
+    if 0 in results and 1 in results:
+        bit_exact["fast_vs_plain"] = rows_equal(*out_bufs[1], *out_bufs[0])
     if 0 in results and headline != 0:
         plain = {"value": units / (results[0][0] / 1e3), "unit": "queries/s", "ms_per_step": results[0][0],
                  "kernel": "exact_knn_kernel (reference traversal and heap)"}
+    # rows of the headline method at the CPU baseline's sample (checked against the oracle below)
+    sample_ids = np.linspace(0, (len(shard_ids) if shard else n) - 1, min(args.cpu_sample, n)).astype(np.int64)
+    hi_, hd_ = out_bufs[headline if headline in out_bufs else 1]
+    ts = torch.from_numpy(sample_ids).to(dev)
+    gpu_sample = (hi_.view(-1, k).index_select(0, ts).cpu().numpy(), hd_.view(-1, k).index_select(0, ts).cpu().numpy())
+    headline_rows = out_bufs.pop(1)  # kept for the learned-bound comparison
+    out_bufs.clear()
 
     # ---- e2e through the public API with host buffers ----
     e2e = None
@@ -682,10 +739,10 @@ def run_ours(args):
                 # results straight into pinned host memory (the library overlaps the copy-out)
                 if shard:
                     ft.self_knn_query_subset(ctxs[lane], trees[lane], shard_ids, k, his[lane], hds[lane],
-                                             exclude_self=True, max_k=max(32, k), method=method, stream=st)
+                                             exclude_self=True, max_k=max(32, k), method=("fast" if method == 1 else "plain"), stream=st)
                 else:
                     ft.self_knn_query(ctxs[lane], trees[lane], k, his[lane], hds[lane], exclude_self=True,
-                                      max_k=max(32, k), method=method, half_window=args.half,
+                                      max_k=max(32, k), method=("fast" if method == 1 else "plain"), half_window=args.half,
                                       variant=args.variant, stream=st)
 
         # untimed warm-up: one step on each lane (staging buffers, copy streams, tree scratch)
@@ -716,6 +773,12 @@ def run_ours(args):
         e2e = {"value": units / (e_ms / 1e3), "unit": "queries/s",
                "h2d_bytes_per_step": int(3 * world * n * x.element_size()),  # every rank uploads n points
                "d2h_bytes_per_step": int(units * k * (idx.element_size() + dst.element_size())), "ms_per_step": e_ms}
+        # the host rows of the last step equal the device-resident headline rows
+        last = (e_steps - 1) % 2
+        if not shard:
+            e2e["bit_exact"] = rows_equal(his[last].to(dev, non_blocking=False), hds[last].to(dev),
+                                          *headline_rows)
+        del his, hds, bufs
 
     # ---- roofline of the self-kNN kernel (algorithmic bytes per launch / launch time) ----
     sc = x.element_size()
@@ -744,7 +807,7 @@ def run_ours(args):
     learned = knn_ext = extra = None
     if world == 1 and not args.no_batched and args.workload == "cfg2":
         fast_visits = results[1][2]["visits"] / n if 1 in results else None
-        learned = run_learned(args, ctx, tree, n, k, stream, fast_visits)
+        learned = run_learned(args, ctx, tree, n, k, stream, fast_visits, headline_rows)
         knn_ext = run_knn_external(args, stream)
         extra = run_cfg2_extra(ctx, tree, x, y, z, n, stream)
 
@@ -759,7 +822,13 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         del tree
         torch.cuda.empty_cache()
-        _, cpu = cpu_baseline(w, args)
+        (oi, od), cpu = cpu_baseline(w, args)
+        # the GPU's rows at the same sampled queries, against the oracle's
+        oracle_same = bool(np.array_equal(gpu_sample[0], oi) and
+                           np.array_equal(gpu_sample[1].view(np.uint64), od.view(np.uint64)))
+        cpu["gpu_rows_equal_oracle"] = oracle_same
+        if isinstance(bit_exact, dict):
+            bit_exact["oracle_sample"] = oracle_same
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -774,6 +843,7 @@ def run_ours(args):
                           "l2": "inputs larger than L2: tree records + boxes ~2.3 GB, output 5.1 GB"},
                "plain": plain, "other_k_and_range": extra, "batched": batched, "learned": learned,
                "knn_query": knn_ext, "build_ms": build_ms, "tree_height": height, "query_stats": stats,
+               "bit_exact": bit_exact,
                "e2e": e2e, "gpu_launches": args.steps * (2 if method == 1 else 1),
                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(out), flush=True)

@@ -11,13 +11,14 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libfasttree_b200.so")
 
 FT_OK, FT_ERR_INVALID_ARGUMENT, FT_ERR_RUNTIME, FT_ERR_CUDA, FT_ERR_OUT_OF_MEMORY, FT_ERR_TIMEOUT = range(6)
+FT_METHOD_DEFAULT, FT_METHOD_FAST, FT_METHOD_PLAIN = 0, 1, 2
 F32, F64, U32, U64 = 0, 1, 2, 3
 MORTON, PEANO_HILBERT = 0, 1
 
 # Every entry point declared in include/fasttree_b200.h.
 EXPORTED = (
     "ft_context_create", "ft_context_destroy", "ft_last_error", "ft_version", "ft_get_query_stats",
-    "ft_check_device_status",
+    "ft_get_replayed_queries", "ft_check_device_status",
     "ft_tree_create", "ft_tree_ensure", "ft_tree_destroy", "ft_compute_bbox", "ft_sfc_encode",
     "ft_build_bvh", "ft_build_tree", "ft_refit_bvh", "ft_tree_export", "ft_tree_import", "ft_self_knn", "ft_knn", "ft_range", "ft_tree_height",
     "ft_self_knn_noalloc", "ft_self_knn_bounded",
@@ -65,6 +66,7 @@ _SIGS = {
     "ft_context_create": [ctypes.POINTER(FtOptions), _i, ctypes.POINTER(_vp)],
     "ft_context_destroy": [_vp],
     "ft_get_query_stats": [_vp, ctypes.POINTER(FtQueryStats)],
+    "ft_get_replayed_queries": [_vp, _vp, _sz, ctypes.POINTER(ctypes.c_size_t)],
     "ft_check_device_status": [_vp, _st],
     "ft_tree_create": [_vp, _sz, ctypes.POINTER(ctypes.POINTER(FtTree))],
     "ft_tree_ensure": [_vp, ctypes.POINTER(FtTree), _sz],

@@ -543,7 +543,7 @@ void batch_query(Context &ctx, BatchImpl &b, int k, bool excl, uint64_t *idx, vo
              "k exceeds _MAX_K_ template parameter. Instantiate self_knn_query with larger _MAX_K_.");
     if (k > 512) fail(FT_ERR_RUNTIME, "self_knn_query: k too large for shared memory.");
     if (b.N == 0 || k <= 0) return;
-    batch_self_knn(ctx, b.all, batch_dev(b), b.N, k, excl, idx, dist, q.method == 1, q.reserved[0], q.reserved[1],
+    batch_self_knn(ctx, b.all, batch_dev(b), b.N, k, excl, idx, dist, q.method != FT_METHOD_PLAIN, q.reserved[0], q.reserved[1],
                    b.rr, b.rw, b.counters, st);
 }
 

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "ft_build_dev.cuh"
@@ -141,6 +142,9 @@ __global__ void keys_to_ref_kernel(const unsigned long long *klo, const unsigned
 // =========================================================================================
 static constexpr int kSortThreads = 256;
 static constexpr int kSortWarps   = kSortThreads / 32;
+// Tile tickets of build_bvh's sort: [0, 16) one per digit pass, [16, 32) the two-word
+// fallback's passes; [32] the fallback switch (a long run of equal high words).
+static constexpr int kTicketWords = 64;
 static constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kFlagMask = 3u << 30,
                           kCountMask = (1u << 30) - 1u;
 
@@ -151,11 +155,14 @@ template <int W> struct SortCfg {
 };
 
 // Digit histograms of digit positions [d0, d0 + ND) (ND = 8 * W by default: every digit).
+// enable: null, or a device word whose 0 makes the launch a no-op.
 template <int W, int ND = 8 * W>
 __global__ void __launch_bounds__(256) radix_hist_kernel(const unsigned long long *__restrict__ klo,
                                                          const unsigned long long *__restrict__ khi, size_t n,
-                                                         uint32_t *hist, int d0 = 0) {
+                                                         uint32_t *hist, int d0 = 0,
+                                                         const uint32_t *enable = nullptr) {
     constexpr int D = ND;
+    if (enable && *enable == 0u) return;
     __shared__ uint32_t s[D * 256];
     for (int i = threadIdx.x; i < D * 256; i += blockDim.x) s[i] = 0;
     __syncthreads();
@@ -180,9 +187,11 @@ __global__ void __launch_bounds__(256) radix_hist_kernel(const unsigned long lon
 }
 
 // Exclusive offsets per digit position; skip[d] = 1 when one digit value holds every key.
-__global__ void radix_scan_kernel(uint32_t *hist, size_t n, uint32_t *skip) {
+// enable: as radix_hist_kernel's.
+__global__ void radix_scan_kernel(uint32_t *hist, size_t n, uint32_t *skip, const uint32_t *enable = nullptr) {
     __shared__ uint32_t s[256];
     __shared__ int      s_full;
+    if (enable && *enable == 0u) return;
     const int d = blockIdx.x, t = threadIdx.x;
     uint32_t  c = hist[d * 256 + t];
     if (t == 0) s_full = 0;
@@ -207,16 +216,25 @@ FT_D uint32_t ld_volatile(const uint32_t *p) {
 }
 FT_D void st_volatile(uint32_t *p, uint32_t v) { asm volatile("st.volatile.global.u32 [%0], %1;" ::"l"(p), "r"(v)); }
 
+// One onesweep pass over every tile.  The grid is persistent (at most the CTAs resident at
+// once): each CTA takes tiles by ticket until none are left, so a launch whose pass turns out
+// to have nothing to do costs one wave.  Device-side switches keep the host out of the loop:
+//  * enable (null or a device word): 0 makes the whole pass a no-op (passes of the two-word
+//    fallback, which only runs when a long run of equal high words was found);
+//  * skip (null or a device word): 1 when one digit value holds every key -- the pass then
+//    copies its tiles unchanged, so the ping-pong order the host planned still holds.
 template <int W>
 __global__ void __launch_bounds__(kSortThreads, 1)
     onesweep_kernel(const unsigned long long *__restrict__ in_lo, const unsigned long long *__restrict__ in_hi,
                     const uint32_t *__restrict__ in_v, unsigned long long *__restrict__ out_lo,
-                    unsigned long long *__restrict__ out_hi, uint32_t *__restrict__ out_v, size_t n, int word,
-                    int shift, const uint32_t *__restrict__ offsets, uint32_t *lookback, uint32_t *tile_counter,
-                    uint32_t *status) {
+                    unsigned long long *__restrict__ out_hi, uint32_t *__restrict__ out_v, size_t n, size_t num_tiles,
+                    int word, int shift, const uint32_t *__restrict__ offsets, uint32_t *lookback,
+                    uint32_t *tile_counter, const uint32_t *enable, const uint32_t *skip, uint32_t *status) {
     using Cfg           = SortCfg<W>;
     constexpr int ITEMS = Cfg::items;
     constexpr int TILE  = Cfg::tile;
+    if (enable && *enable == 0u) return; // grid-uniform
+    const bool copy = skip && *skip != 0u;
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long *s_lo = reinterpret_cast<unsigned long long *>(smem);
     unsigned long long *s_hi = s_lo + TILE; // only used when W == 2
@@ -229,113 +247,129 @@ __global__ void __launch_bounds__(kSortThreads, 1)
 
     const int      tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned lt_mask = (1u << lane) - 1u;
-    if (tid == 0) s_ticket = atomicAdd(tile_counter, 1u);
-    for (int i = tid; i < kSortWarps * 256; i += kSortThreads) s_wh[i] = 0;
-    __syncthreads();
-    const size_t tile = s_ticket;
-    const size_t base = tile * (size_t)TILE;
+    for (;;) {
+        if (tid == 0) s_ticket = atomicAdd(tile_counter, 1u);
+        for (int i = tid; i < kSortWarps * 256; i += kSortThreads) s_wh[i] = 0;
+        __syncthreads();
+        const size_t tile = s_ticket;
+        if (tile >= num_tiles) break; // grid-uniform per CTA
+        const size_t base = tile * (size_t)TILE;
 
-    unsigned long long klo[ITEMS], khi[ITEMS];
-    uint32_t           val[ITEMS], dig[ITEMS], rank[ITEMS];
-#pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-        size_t pos   = base + (size_t)warp * 32 * ITEMS + (size_t)i * 32 + lane;
-        bool   valid = pos < n;
-        klo[i]       = valid ? in_lo[pos] : 0ull;
-        khi[i]       = (W == 2 && valid) ? in_hi[pos] : 0ull;
-        val[i]       = valid ? in_v[pos] : 0u;
-        unsigned long long w = (W == 2 && word == 1) ? khi[i] : klo[i];
-        dig[i]       = valid ? (uint32_t)(w >> shift) & 255u : 256u + lane;
-    }
-    uint32_t *wh = s_wh + warp * 256;
-#pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-        unsigned peers = __match_any_sync(0xffffffffu, dig[i]);
-        bool     valid = dig[i] < 256u;
-        uint32_t before = valid ? wh[dig[i]] : 0u;
-        __syncwarp();
-        if (valid && lane == __ffs(peers) - 1) wh[dig[i]] = before + __popc(peers);
-        __syncwarp();
-        rank[i] = before + __popc(peers & lt_mask);
-    }
-    __syncthreads();
-
-    // per-digit: warp exclusive prefixes and the tile count
-    uint32_t run = 0;
-#pragma unroll
-    for (int w = 0; w < kSortWarps; ++w) {
-        uint32_t c            = s_wh[w * 256 + tid];
-        s_wh[w * 256 + tid]   = run;
-        run += c;
-    }
-    const uint32_t tile_count = run;
-
-    // exclusive scan of tile counts over digits (block scan, 256 threads)
-    uint32_t incl = tile_count;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        uint32_t v = __shfl_up_sync(0xffffffffu, incl, off);
-        if (lane >= off) incl += v;
-    }
-    if (lane == 31) s_wsum[warp] = incl;
-    __syncthreads();
-    uint32_t wpre = 0;
-    for (int w = 0; w < warp; ++w) wpre += s_wsum[w];
-    s_tile_excl[tid] = wpre + incl - tile_count;
-
-    // decoupled look-back for digit tid
-    uint32_t *lb     = lookback + tile * 256;
-    uint32_t  prefix = 0;
-    if (tile == 0) {
-        st_volatile(lb + tid, kFlagInc | tile_count);
-    } else {
-        st_volatile(lb + tid, kFlagAgg | tile_count);
-        for (long long j = (long long)tile - 1; j >= 0; --j) {
-            uint32_t s;
-            int      spins = 0;
-            for (;;) {
-                s = ld_volatile(lookback + (size_t)j * 256 + tid);
-                if (s & kFlagMask) break;
-                if (++spins > 64) __nanosleep(32);
-                if (spins > kSpinLimit) break;
+        if (copy) { // constant digit: the tile moves unchanged
+            const size_t end = min(base + (size_t)TILE, n);
+            for (size_t pos = base + tid; pos < end; pos += kSortThreads) {
+                out_lo[pos] = in_lo[pos];
+                if (W == 2) out_hi[pos] = in_hi[pos];
+                out_v[pos] = in_v[pos];
             }
-            if (!(s & kFlagMask)) {
-                atomicOr(status, STATUS_SPIN_LIMIT);
-                break;
-            }
-            prefix += s & kCountMask;
-            if (s & kFlagInc) break;
-        }
-        st_volatile(lb + tid, kFlagInc | (prefix + tile_count));
-    }
-    s_base[tid] = offsets[tid] + prefix;
-    __syncthreads();
-
-    // stage the tile in digit order
-#pragma unroll
-    for (int i = 0; i < ITEMS; ++i) {
-        if (dig[i] < 256u) {
-            uint32_t lp = s_tile_excl[dig[i]] + s_wh[warp * 256 + dig[i]] + rank[i];
-            s_lo[lp]    = klo[i];
-            if (W == 2) s_hi[lp] = khi[i];
-            s_v[lp] = val[i];
-        }
-    }
-    __syncthreads();
-    const int tile_n = (int)min((size_t)TILE, n - base);
-    for (int j = tid; j < tile_n; j += kSortThreads) {
-        unsigned long long lo = s_lo[j];
-        unsigned long long hi = (W == 2) ? s_hi[j] : 0ull;
-        unsigned long long w  = (W == 2 && word == 1) ? hi : lo;
-        uint32_t           d  = (uint32_t)(w >> shift) & 255u;
-        size_t             gp = (size_t)s_base[d] + (size_t)(j - (int)s_tile_excl[d]);
-        if (gp >= n) { // only reachable after a failed look-back; never write out of bounds
-            atomicOr(status, STATUS_SPIN_LIMIT);
+            __syncthreads();
             continue;
         }
-        out_lo[gp]            = lo;
-        if (W == 2) out_hi[gp] = hi;
-        out_v[gp] = s_v[j];
+
+        unsigned long long klo[ITEMS], khi[ITEMS];
+        uint32_t           val[ITEMS], dig[ITEMS], rank[ITEMS];
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            size_t pos   = base + (size_t)warp * 32 * ITEMS + (size_t)i * 32 + lane;
+            bool   valid = pos < n;
+            klo[i]       = valid ? in_lo[pos] : 0ull;
+            khi[i]       = (W == 2 && valid) ? in_hi[pos] : 0ull;
+            val[i]       = valid ? in_v[pos] : 0u;
+            unsigned long long w = (W == 2 && word == 1) ? khi[i] : klo[i];
+            dig[i]       = valid ? (uint32_t)(w >> shift) & 255u : 256u + lane;
+        }
+        uint32_t *wh = s_wh + warp * 256;
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            unsigned peers  = __match_any_sync(0xffffffffu, dig[i]);
+            bool     valid  = dig[i] < 256u;
+            uint32_t before = valid ? wh[dig[i]] : 0u;
+            __syncwarp();
+            if (valid && lane == __ffs(peers) - 1) wh[dig[i]] = before + __popc(peers);
+            __syncwarp();
+            rank[i] = before + __popc(peers & lt_mask);
+        }
+        __syncthreads();
+
+        // per-digit: warp exclusive prefixes and the tile count
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            uint32_t c          = s_wh[w * 256 + tid];
+            s_wh[w * 256 + tid] = run;
+            run += c;
+        }
+        const uint32_t tile_count = run;
+
+        // exclusive scan of tile counts over digits (block scan, 256 threads)
+        uint32_t incl = tile_count;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            uint32_t v = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl += v;
+        }
+        if (lane == 31) s_wsum[warp] = incl;
+        __syncthreads();
+        uint32_t wpre = 0;
+        for (int w = 0; w < warp; ++w) wpre += s_wsum[w];
+        s_tile_excl[tid] = wpre + incl - tile_count;
+
+        // decoupled look-back for digit tid (every earlier tile is held by a running CTA or
+        // done, since tickets are taken in order and a CTA finishes its tile first)
+        uint32_t *lb     = lookback + tile * 256;
+        uint32_t  prefix = 0;
+        if (tile == 0) {
+            st_volatile(lb + tid, kFlagInc | tile_count);
+        } else {
+            st_volatile(lb + tid, kFlagAgg | tile_count);
+            for (long long j = (long long)tile - 1; j >= 0; --j) {
+                uint32_t sv;
+                int      spins = 0;
+                for (;;) {
+                    sv = ld_volatile(lookback + (size_t)j * 256 + tid);
+                    if (sv & kFlagMask) break;
+                    if (++spins > 64) __nanosleep(32);
+                    if (spins > kSpinLimit) break;
+                }
+                if (!(sv & kFlagMask)) {
+                    atomicOr(status, STATUS_SPIN_LIMIT);
+                    break;
+                }
+                prefix += sv & kCountMask;
+                if (sv & kFlagInc) break;
+            }
+            st_volatile(lb + tid, kFlagInc | (prefix + tile_count));
+        }
+        s_base[tid] = offsets[tid] + prefix;
+        __syncthreads();
+
+        // stage the tile in digit order
+#pragma unroll
+        for (int i = 0; i < ITEMS; ++i) {
+            if (dig[i] < 256u) {
+                uint32_t lp = s_tile_excl[dig[i]] + s_wh[warp * 256 + dig[i]] + rank[i];
+                s_lo[lp]    = klo[i];
+                if (W == 2) s_hi[lp] = khi[i];
+                s_v[lp] = val[i];
+            }
+        }
+        __syncthreads();
+        const int tile_n = (int)min((size_t)TILE, n - base);
+        for (int j = tid; j < tile_n; j += kSortThreads) {
+            unsigned long long lo = s_lo[j];
+            unsigned long long hi = (W == 2) ? s_hi[j] : 0ull;
+            unsigned long long w  = (W == 2 && word == 1) ? hi : lo;
+            uint32_t           d  = (uint32_t)(w >> shift) & 255u;
+            size_t             gp = (size_t)s_base[d] + (size_t)(j - (int)s_tile_excl[d]);
+            if (gp >= n) { // only reachable after a failed look-back; never write out of bounds
+                atomicOr(status, STATUS_SPIN_LIMIT);
+                continue;
+            }
+            out_lo[gp]             = lo;
+            if (W == 2) out_hi[gp] = hi;
+            out_v[gp]              = s_v[j];
+        }
+        __syncthreads(); // the tile's shared memory is free for the next ticket
     }
 }
 
@@ -503,7 +537,7 @@ void ensure_scratch(TreeImpl &s, const ft_options &o, size_t n) {
     s.hist         = (uint32_t *)alloc_dev<uint32_t>(16 * 256 + 16);
     s.lookback_words = 16 * sort_tiles(cap, W) * 256;
     s.lookback     = (uint32_t *)alloc_dev<uint32_t>(s.lookback_words);
-    s.tile_counter = (uint32_t *)alloc_dev<uint32_t>(16);
+    s.tile_counter = (uint32_t *)alloc_dev<uint32_t>(kTicketWords);
     s.status       = (uint32_t *)alloc_dev<uint32_t>(4);
     FT_CUDA(cudaMemset(s.status, 0, 16));
 }
@@ -570,8 +604,8 @@ void sfc_encode_ref_layout(Context &ctx, TreeImpl &s, const void *x, const void 
 // Two-word keys, second stage: after the passes over the high word, runs of equal high
 // words are put in (low word, input index) order.  The thread at the start of each run
 // insertion-sorts it in place when it holds at most kRunCap keys (stable, so equal keys keep
-// the index order the high-word passes left); a longer run sets flag[0], and the host then
-// finishes with the low-word and high-word passes instead.
+// the index order the high-word passes left); a longer run sets flag[0], which switches on
+// the low-word and high-word passes queued behind this kernel.
 static constexpr int kRunCap = 32;
 
 __global__ void __launch_bounds__(256) hi_run_fixup_kernel(unsigned long long *__restrict__ klo,
@@ -601,72 +635,100 @@ __global__ void __launch_bounds__(256) hi_run_fixup_kernel(unsigned long long *_
     }
 }
 
+// Zeroes `words` words at p when *enable is set (the fallback's look-back status words).
+__global__ void __launch_bounds__(256) zero_if_kernel(uint32_t *p, size_t words, const uint32_t *enable) {
+    if (*enable == 0u) return;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < words; i += (size_t)gridDim.x * blockDim.x)
+        p[i] = 0u;
+}
+
+// Persistent grid of a onesweep pass: the CTAs resident at once (three per SM with the
+// tile's shared memory), never more than the tiles.
+template <int W> static unsigned sort_grid(size_t tiles) {
+    static int per_sm = 0, sms = 0;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaFuncSetAttribute(onesweep_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SortCfg<W>::smem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel<W>, kSortThreads,
+                                                          SortCfg<W>::smem) != cudaSuccess) {
+            cudaGetLastError();
+            per_sm = 1;
+            sms    = 148;
+        }
+        per_sm = std::max(per_sm, 1);
+    });
+    return (unsigned)std::max<size_t>(1, std::min<size_t>(tiles, (size_t)per_sm * (size_t)sms));
+}
+
+// The key sort of build_bvh, with no host synchronisation.  One-word keys: histograms of the
+// eight digits, then eight passes (a constant digit's pass copies).  Two-word keys: the
+// high word's eight passes, then runs of equal high words of at most 32 keys are ordered by
+// (low word, input index) in place; a longer run switches on, on the device, the full
+// two-word sort from that order (histograms of the low word, then the eight low-word and the
+// eight high-word passes: an even number, so the host's ping-pong order is the same whether
+// they run or not).
 template <int W> static void sort_impl(TreeImpl &s, size_t n, cudaStream_t st) {
-    using Cfg     = SortCfg<W>;
-    const int D   = 8 * W;
-    size_t tiles  = (n + Cfg::tile - 1) / Cfg::tile;
+    using Cfg            = SortCfg<W>;
+    const int      D     = 8 * W;
+    const size_t   tiles = (n + Cfg::tile - 1) / Cfg::tile;
+    const unsigned grid  = sort_grid<W>(tiles);
+    FT_CUDA(cudaFuncSetAttribute(onesweep_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem));
     FT_CUDA(cudaMemsetAsync(s.hist, 0, (16 * 256 + 16) * sizeof(uint32_t), st));
+    FT_CUDA(cudaMemsetAsync(s.tile_counter, 0, kTicketWords * sizeof(uint32_t), st));
     uint32_t *skip_dev = s.hist + 16 * 256;
-    uint32_t  skip[16] = {0};
-    // histograms of the digit positions [d0, d0 + 8) of one key word (W == 2: the high word
-    // first; the low word's only if a long run of equal high words needs the full sort)
-    auto histogram = [&](int d0) {
+    uint32_t *fallback = s.tile_counter + 32;
+    // histograms of the digit positions [d0, d0 + 8) of one key word
+    auto histogram = [&](int d0, const uint32_t *enable) {
         radix_hist_kernel<W, 8><<<grid_for(n, 256, 148 * 4), 256, 0, st>>>(
-            (const unsigned long long *)s.key_lo, (const unsigned long long *)s.key_hi, n, s.hist, d0);
-        radix_scan_kernel<<<8, 256, 0, st>>>(s.hist + d0 * 256, n, skip_dev + d0);
+            (const unsigned long long *)s.key_lo, (const unsigned long long *)s.key_hi, n, s.hist, d0, enable);
+        radix_scan_kernel<<<8, 256, 0, st>>>(s.hist + d0 * 256, n, skip_dev + d0, enable);
         FT_CUDA(cudaGetLastError());
-        FT_CUDA(cudaMemcpyAsync(skip + d0, skip_dev + d0, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        FT_CUDA(cudaStreamSynchronize(st));
     };
-    histogram(W == 2 ? 8 : 0);
-    FT_CUDA(cudaMemsetAsync(s.lookback, 0, (size_t)D * tiles * 256 * sizeof(uint32_t), st));
-    FT_CUDA(cudaMemsetAsync(s.tile_counter, 0, 16 * sizeof(uint32_t), st));
-    static bool attr_set = false;
-    if (!attr_set) {
-        FT_CUDA(cudaFuncSetAttribute(onesweep_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem));
-    }
-    auto pass = [&](int d) {
-        int word  = d >> 3;
-        int shift = 8 * (d & 7);
-        onesweep_kernel<W><<<(unsigned)tiles, kSortThreads, Cfg::smem, st>>>(
+    auto pass = [&](int d, uint32_t *ticket, const uint32_t *enable) {
+        onesweep_kernel<W><<<grid, kSortThreads, Cfg::smem, st>>>(
             (const unsigned long long *)s.key_lo, (const unsigned long long *)s.key_hi, s.perm,
-            (unsigned long long *)s.tmp_lo, (unsigned long long *)s.tmp_hi, s.tmp_perm, n, word, shift,
-            s.hist + d * 256, s.lookback + (size_t)d * tiles * 256, s.tile_counter + d, s.status);
+            (unsigned long long *)s.tmp_lo, (unsigned long long *)s.tmp_hi, s.tmp_perm, n, tiles, d >> 3,
+            8 * (d & 7), s.hist + d * 256, s.lookback + (size_t)d * tiles * 256, ticket, enable, skip_dev + d,
+            s.status);
         FT_CUDA(cudaGetLastError());
         std::swap(s.key_lo, s.tmp_lo);
         std::swap(s.key_hi, s.tmp_hi);
         std::swap(s.perm, s.tmp_perm);
     };
-    if constexpr (W == 2) {
-        // high-word passes first; equal high words are rare (a 62-bit prefix of the curve), so
-        // a fix-up of their short runs replaces the eight low-word passes
-        for (int d = 8; d < 16; ++d)
-            if (!skip[d]) pass(d);
-        uint32_t *flag = s.tile_counter + 15; // the last high-word pass is done with its counter
-        FT_CUDA(cudaMemsetAsync(flag, 0, sizeof(uint32_t), st));
+    histogram(W == 2 ? 8 : 0, nullptr);
+    FT_CUDA(cudaMemsetAsync(s.lookback, 0, (size_t)D * tiles * 256 * sizeof(uint32_t), st));
+    if constexpr (W == 1) {
+        for (int d = 0; d < 8; ++d) pass(d, s.tile_counter + d, nullptr);
+    } else {
+        // high-word passes first; equal high words are rare for data spread over the box (a
+        // 62-bit prefix of the curve), so a fix-up of their short runs replaces the low-word
+        // passes
+        for (int d = 8; d < 16; ++d) pass(d, s.tile_counter + d, nullptr);
         hi_run_fixup_kernel<<<grid_for(n, 256), 256, 0, st>>>((unsigned long long *)s.key_lo,
-                                                              (const unsigned long long *)s.key_hi, s.perm, n, flag);
+                                                              (const unsigned long long *)s.key_hi, s.perm, n,
+                                                              fallback);
         FT_CUDA(cudaGetLastError());
-        uint32_t long_run = 0;
-        FT_CUDA(cudaMemcpyAsync(&long_run, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        FT_CUDA(cudaStreamSynchronize(st));
-        if (!long_run) return;
-        // a long run of equal high words: the full two-word sort from the current order (it
-        // is stable, and within equal keys the current order is the input index order)
-        histogram(0);
-        FT_CUDA(cudaMemsetAsync(s.lookback, 0, (size_t)D * tiles * 256 * sizeof(uint32_t), st));
-        FT_CUDA(cudaMemsetAsync(s.tile_counter, 0, 16 * sizeof(uint32_t), st));
+        // a long run of equal high words: the full two-word sort from the current order (it is
+        // stable, and within equal keys the current order is the input index order)
+        histogram(0, fallback);
+        zero_if_kernel<<<grid_for((size_t)D * tiles * 256, 256, 148 * 8), 256, 0, st>>>(
+            s.lookback, (size_t)D * tiles * 256, fallback);
+        FT_CUDA(cudaGetLastError());
+        for (int d = 0; d < 16; ++d) pass(d, s.tile_counter + 16 + d, fallback);
     }
-    for (int d = 0; d < D; ++d)
-        if (!skip[d]) pass(d);
 }
 
-// The same sort over a fixed list of digit positions: no histogram read-back, so no host
-// synchronisation (used by the batched build, whose launch sequence is graph-captured).
+// The same sort over a fixed list of digit positions (every listed pass runs; no skips and no
+// fallback), used by the batched build and the query order.
 template <int W> static void sort_fixed_impl(TreeImpl &s, size_t n, int ndig, const int *digits, cudaStream_t st) {
-    using Cfg    = SortCfg<W>;
-    const int D  = 8 * W;
-    size_t tiles = (n + Cfg::tile - 1) / Cfg::tile;
+    using Cfg            = SortCfg<W>;
+    const int      D     = 8 * W;
+    const size_t   tiles = (n + Cfg::tile - 1) / Cfg::tile;
+    const unsigned grid  = sort_grid<W>(tiles);
     FT_CUDA(cudaMemsetAsync(s.hist, 0, (16 * 256 + 16) * sizeof(uint32_t), st));
     radix_hist_kernel<W><<<grid_for(n, 256, 148 * 4), 256, 0, st>>>((const unsigned long long *)s.key_lo,
                                                                       (const unsigned long long *)s.key_hi, n,
@@ -678,10 +740,10 @@ template <int W> static void sort_fixed_impl(TreeImpl &s, size_t n, int ndig, co
     FT_CUDA(cudaFuncSetAttribute(onesweep_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem));
     for (int i = 0; i < ndig; ++i) {
         const int d = digits[i];
-        onesweep_kernel<W><<<(unsigned)tiles, kSortThreads, Cfg::smem, st>>>(
+        onesweep_kernel<W><<<grid, kSortThreads, Cfg::smem, st>>>(
             (const unsigned long long *)s.key_lo, (const unsigned long long *)s.key_hi, s.perm,
-            (unsigned long long *)s.tmp_lo, (unsigned long long *)s.tmp_hi, s.tmp_perm, n, d >> 3, 8 * (d & 7),
-            s.hist + d * 256, s.lookback + (size_t)d * tiles * 256, s.tile_counter + d, s.status);
+            (unsigned long long *)s.tmp_lo, (unsigned long long *)s.tmp_hi, s.tmp_perm, n, tiles, d >> 3, 8 * (d & 7),
+            s.hist + d * 256, s.lookback + (size_t)d * tiles * 256, s.tile_counter + d, nullptr, nullptr, s.status);
         FT_CUDA(cudaGetLastError());
         std::swap(s.key_lo, s.tmp_lo);
         std::swap(s.key_hi, s.tmp_hi);

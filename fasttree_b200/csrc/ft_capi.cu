@@ -295,6 +295,24 @@ ft_status ft_get_query_stats(ft_context *ctx, ft_query_stats *out) {
     FT_API_END
 }
 
+ft_status ft_get_replayed_queries(ft_context *ctx, int32_t *rows_out, size_t capacity, size_t *count_out) {
+    FT_API_BEGIN
+    need(ctx && count_out, "null argument");
+    need(rows_out || capacity == 0, "null rows_out");
+    *count_out = 0;
+    if (!ctx->last_fast || !ctx->last_rows || !ctx->replay_rows) return FT_OK;
+    DeviceGuard g(ctx->device);
+    uint32_t    cnt = 0;
+    FT_CUDA(cudaDeviceSynchronize());
+    FT_CUDA(cudaMemcpy(&cnt, ctx->status + 1, sizeof(cnt), cudaMemcpyDeviceToHost));
+    const size_t c = std::min<size_t>(cnt, ctx->replay_cap);
+    *count_out     = c;
+    if (capacity > 0 && c > 0)
+        FT_CUDA(cudaMemcpy(rows_out, ctx->replay_rows, std::min(c, capacity) * sizeof(int32_t),
+                           cudaMemcpyDeviceToHost));
+    FT_API_END
+}
+
 ft_status ft_tree_create(ft_context *ctx, size_t n, ft_tree **out) {
     FT_API_BEGIN
     need(ctx && out, "null argument");
@@ -752,11 +770,16 @@ ft_status ft_self_knn_noalloc(ft_context *ctx, const ft_tree *tree, const int32_
     if (tree->num_leaves == 0 || num == 0 || k <= 0) return FT_OK;
     need(idx_out && dist_out, "null output array");
     if (k > 512) fail(FT_ERR_RUNTIME, "self_knn_query: k too large for shared memory.");
-    DeviceGuard  g(ctx->device);
+    DeviceGuard g(ctx->device);
+    // the kernels write straight into these arrays: pageable host memory would fault there
+    need_device(leaf_ids, "leaf_ids");
+    need_device(idx_out, "idx_out");
+    need_device(dist_out, "dist_out");
     cudaStream_t st = (cudaStream_t)stream;
     if (!ft::fast_self_knn_noalloc(*ctx, *tree, leaf_ids, num, k, exclude_self != 0, idx_out, dist_out, st)) {
         ft_query_options q{}; // reference traversal: it uses no scratch
-        q.max_k = k < 32 ? 32 : k;
+        q.max_k  = k < 32 ? 32 : k;
+        q.method = FT_METHOD_PLAIN;
         ft::self_knn(*ctx, *tree, leaf_ids, num, k, exclude_self != 0, idx_out, dist_out, q, st);
     }
     FT_API_END

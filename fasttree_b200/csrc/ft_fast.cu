@@ -1,4 +1,4 @@
-// ft_fast.cu -- fast self-kNN and knn_query with exact fallback ("method 1").
+// ft_fast.cu -- fast self-kNN and knn_query with exact fallback (FT_METHOD_FAST, the default).
 //
 // A warp takes 32 consecutive queries (sorted leaves, or external points sorted by their
 // SFC rank), so its lanes work on neighbouring parts of the tree.
@@ -21,6 +21,7 @@
 //     traversal (exact_replay_kernel, or knn_query's heap tier for external points).  Trees
 //     taller than 62 levels (where the reference's stack guard drops subtrees) always take the
 //     reference traversal.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1143,12 +1144,35 @@ static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocHeader + 2 *
 static constexpr int kNoAllocMaxDevices = 64;
 static std::mutex    g_noalloc_mutex;
 static uint32_t     *g_noalloc_addr[kNoAllocMaxDevices] = {};
+static CUcontext     g_noalloc_owner[kNoAllocMaxDevices] = {}; // the context the address belongs to
 
-// Device address of g_noalloc_scratch on `device` (looked up once; device must be current).
+// The current driver context, read through the runtime's driver entry point (the library
+// links no driver library); null when it cannot be read.
+static CUcontext current_context() {
+    using GetCurrent = CUresult (*)(CUcontext *);
+    static GetCurrent fn = [] {
+        void                           *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return reinterpret_cast<GetCurrent>(p);
+    }();
+    CUcontext c = nullptr;
+    if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+    return c;
+}
+
+// Device address of g_noalloc_scratch on `device` (device must be current).  Looked up on
+// the first call on a device and again whenever the device's context has changed since (a
+// cudaDeviceReset makes a new primary context, which holds its own copy of the array).
 static uint32_t *noalloc_scratch(int device) {
     if (device < 0 || device >= kNoAllocMaxDevices) fail(FT_ERR_INVALID_ARGUMENT, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[device]) {
+    const CUcontext cur = current_context();
+    if (!g_noalloc_addr[device] || cur == nullptr || cur != g_noalloc_owner[device]) {
         void       *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || p == nullptr) {
@@ -1156,7 +1180,8 @@ static uint32_t *noalloc_scratch(int device) {
             fail(FT_ERR_CUDA, std::string("cudaGetSymbolAddress of the no-allocation scratch failed: ") +
                                   cudaGetErrorString(e));
         }
-        g_noalloc_addr[device] = static_cast<uint32_t *>(p);
+        g_noalloc_addr[device]  = static_cast<uint32_t *>(p);
+        g_noalloc_owner[device] = cur;
     }
     return g_noalloc_addr[device];
 }
@@ -1187,6 +1212,15 @@ bool fast_self_knn_noalloc(Context &ctx, const ft_tree &tr, const int32_t *leaf_
     case U64: launch_fast<unsigned long long>(ctx.opts, tr, leaf_ids, (int)num, k, half, excl, nullptr, idx, dist, ranks, rows, rc, ctx.status, variant, visits, st); break;
     }
     replay_exact(ctx, tr, ranks, rows, rc, k, excl, idx, dist, st);
+    // query statistics as ft_self_knn keeps them: the replay count and visits move into the
+    // context's status words (a device-to-device copy on the stream; nothing is allocated)
+    // (scratch words: [0] replay count, [2..3] visits; context words: [1] and [2..3])
+    FT_CUDA(cudaMemcpyAsync(ctx.status + 1, rc, sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
+    FT_CUDA(cudaMemcpyAsync(ctx.status + 2, visits, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, st));
+    ctx.stats.queries  = (int64_t)num;
+    ctx.stats.replayed = 0;
+    ctx.last_fast      = true;
+    ctx.last_rows      = false; // the replayed rows stay in the fixed array
     return true;
 }
 

@@ -97,6 +97,7 @@ struct Context {
     int32_t       *seed_ranks   = nullptr; // SFC rank of each external query (fast knn)
     size_t         replay_cap   = 0;
     bool           last_fast    = false; // the last self-kNN call used the fast traversal
+    bool           last_rows    = false; // replay_rows holds the last fast call's replayed rows
     TreeImpl       qsort;                   // sort scratch of external queries (fast knn)
     void          *stage_idx[2]  = {nullptr, nullptr}; // device staging of host-output self-kNN
     void          *stage_dist[2] = {nullptr, nullptr};

@@ -1049,7 +1049,7 @@ void knn_learned(Context &ctx, const ft_tree &tr, BoundModel &b, const void *qx,
     bound_features_points(ctx, tr, qx, qy, qz, nq, k, ctx.learned_feats, st);
     bound_model_predict(ctx, b, ctx.learned_feats, nq, inflation, nullptr, ctx.learned_bound, st);
     ft_query_options qb = q;
-    qb.method           = 1;
+    qb.method           = FT_METHOD_FAST;
     knn(ctx, tr, qx, qy, qz, nq, k, max_k, idx, dist, qb, st, ctx.learned_bound);
 }
 

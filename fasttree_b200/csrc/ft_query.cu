@@ -637,9 +637,11 @@ void self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t n
     ctx.stats.queries  = (int64_t)num;
     ctx.stats.replayed = 0;
     ctx.last_fast      = false;
-    if ((qo.method == 1 || bound) &&
+    ctx.last_rows      = false;
+    if ((qo.method != FT_METHOD_PLAIN || bound) &&
         fast_self_knn(ctx, tr, leaf_ids, num, k, excl, idx, dist, bound, qo.reserved[0], qo.reserved[1], st)) {
         ctx.last_fast = true;
+        ctx.last_rows = true;
         return;
     }
     switch (ctx.opts.coord_type) {
@@ -742,6 +744,7 @@ void self_knn_to_host(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, 
     }
     copy_out(prev0, prevn, (c - 1) & 1);
     FT_CUDA(cudaStreamWaitEvent(st, ctx.ev_copied[(c - 1) & 1], 0));
+    ctx.last_rows = false; // the replay list holds the last chunk's rows, numbered within it
 }
 
 template <class T, int CAP, int QT, int PER>
@@ -884,9 +887,11 @@ void knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const 
     ctx.stats.queries  = (int64_t)nq;
     ctx.stats.replayed = 0;
     ctx.last_fast      = false;
-    if ((qo.method == 1 || bound) && fast_knn(ctx, tr, qx, qy, qz, nq, k, max_k, idx, dist, qo.reserved[0], st, bound,
-                                                qo.reserved[1])) {
+    ctx.last_rows      = false;
+    if ((qo.method != FT_METHOD_PLAIN || bound) &&
+        fast_knn(ctx, tr, qx, qy, qz, nq, k, max_k, idx, dist, qo.reserved[0], st, bound, qo.reserved[1])) {
         ctx.last_fast = true;
+        ctx.last_rows = true;
         return;
     }
     switch (ctx.opts.coord_type) {

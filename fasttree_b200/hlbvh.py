@@ -104,6 +104,21 @@ class Context:
         check(lib().ft_get_query_stats(self._h, ctypes.byref(s)))
         return {"queries": s.queries, "replayed": s.replayed, "visits": s.reserved[0]}
 
+    def check_device_status(self, stream=None):
+        """Synchronises the stream and raises what the kernels recorded (ft_check_device_status)."""
+        _call(lib().ft_check_device_status(self._h, _stream_handle(stream)))
+
+    def replayed_queries(self) -> np.ndarray:
+        """Output rows the last fast-walk query on this context handed to the reference
+        traversal (sorted; empty after a plain-method call).  Synchronises the device."""
+        cnt = ctypes.c_size_t(0)
+        check(lib().ft_get_replayed_queries(self._h, None, 0, ctypes.byref(cnt)))
+        rows = np.empty(cnt.value, dtype=np.int32)
+        if cnt.value:
+            check(lib().ft_get_replayed_queries(self._h, rows.ctypes.data_as(ctypes.c_void_p), cnt.value,
+                                                ctypes.byref(cnt)))
+        return np.sort(rows[: cnt.value])
+
     def close(self):
         if getattr(self, "_h", None):
             lib().ft_context_destroy(self._h)
@@ -391,8 +406,24 @@ def build_tree(ctx: Context, tree: TreeSoA, sorted_keys, sorted_x=None, sorted_y
     return tree
 
 
-def _qopts(max_k: int, method: int = 0, half_window: int = 0, variant: int = 0):
-    o = capi.FtQueryOptions(int(max_k), int(method))
+METHODS = {"default": 0, "fast": 1, "plain": 2}  # ft_query_options.method (FT_METHOD_*)
+
+
+def _method(method) -> int:
+    """"fast" (the default: the fast walk with exact replay), "plain" (the reference traversal
+    alone) or the C value (FT_METHOD_DEFAULT 0, FT_METHOD_FAST 1, FT_METHOD_PLAIN 2)."""
+    if isinstance(method, str):
+        if method not in METHODS:
+            raise ValueError(f"method must be one of {sorted(METHODS)}")
+        return METHODS[method]
+    m = int(method)
+    if m not in (0, 1, 2):
+        raise ValueError("method must be 0 (default), 1 (fast) or 2 (plain)")
+    return m
+
+
+def _qopts(max_k: int, method="fast", half_window: int = 0, variant: int = 0):
+    o = capi.FtQueryOptions(int(max_k), _method(method))
     o.reserved[0] = int(half_window)  # fast walk: SFC seeding half-window (0 = k)
     o.reserved[1] = int(variant)      # fast walk: 0 default, 1 per-lane, 2 compact, 3 warp-shared, 4 4-wide, 5 group
     return o
@@ -405,9 +436,10 @@ def _alloc_knn_out(ctx: Context, rows: int, k: int):
 
 
 def self_knn_query(ctx: Context, tree: TreeSoA, k: int, results=None, result_dists=None, exclude_self=True,
-                   max_k: int = 32, method: int = 0, stream=None, half_window: int = 0, variant: int = 0):
+                   max_k: int = 32, method="fast", stream=None, half_window: int = 0, variant: int = 0):
     """self_knn_query<MAXK> (src/hlbvh.hpp:1929-1954).  Asynchronous; returns (idx, dist) of shape
-    (num_leaves, k).  method=1 takes the fast walk (same output, see ft_fast.cu)."""
+    (num_leaves, k).  method "fast" (default) and "plain" (the reference traversal) return the
+    same rows bit for bit."""
     n = tree.num_leaves
     if results is None:
         results, result_dists = _alloc_knn_out(ctx, n, k)
@@ -433,7 +465,7 @@ def self_knn_query_bounded(ctx: Context, tree: TreeSoA, k: int, bound, results=N
 
 
 def self_knn_query_subset(ctx: Context, tree: TreeSoA, leaf_ids, k: int, results=None, result_dists=None,
-                          exclude_self=True, max_k: int = 256, method: int = 0, stream=None, variant: int = 0):
+                          exclude_self=True, max_k: int = 256, method="fast", stream=None, variant: int = 0):
     """self_knn_query_subset<MAXK> (src/hlbvh.hpp:1956-1983); leaf_ids is a device int32 tensor."""
     num = len(leaf_ids)
     if results is None:
@@ -445,7 +477,7 @@ def self_knn_query_subset(ctx: Context, tree: TreeSoA, leaf_ids, k: int, results
 
 
 def knn_query(ctx: Context, tree: TreeSoA, qx, qy, qz, k: int, results=None, result_dists=None, max_k: int = 256,
-              method: int = 0, stream=None, variant: int = 0):
+              method="fast", stream=None, variant: int = 0):
     """knn_query<MAXK> (src/hlbvh.hpp:1405-1472).  Blocking."""
     x, y, z = (_as_coord(a, ctx.coord) for a in (qx, qy, qz))
     nq = len(x)
@@ -529,7 +561,7 @@ class BatchedSets:
         self.num_sets, self.num_points = S, N
         return self
 
-    def self_knn(self, k: int, exclude_self=True, max_k: int = 32, method: int = 0, results=None,
+    def self_knn(self, k: int, exclude_self=True, max_k: int = 32, method="fast", results=None,
                  result_dists=None, stream=None, half_window: int = 0, variant: int = 0):
         """self_knn_query<MAXK> of every set; rows in set order, indices local to each set."""
         N = self.num_points
@@ -541,7 +573,7 @@ class BatchedSets:
         return _rows(results, N, k), _rows(result_dists, N, k)
 
     def build_knn(self, set_offsets, pos_x, pos_y, pos_z, k: int, results, result_dists, exclude_self=True,
-                  max_k: int = 32, method: int = 1, id=None, is_ghost=None, stream=None):
+                  max_k: int = 32, method="fast", id=None, is_ghost=None, stream=None):
         """build + self_knn as one CUDA graph (captured on the first call with these arrays, replayed
         afterwards).  The arrays must stay alive and in place between calls: pass device tensors
         of the right dtype, which are used as they are."""

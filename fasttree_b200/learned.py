@@ -125,7 +125,7 @@ def training_set(ctx: Context, x, y, z, k: int, stream=None):
     n = len(x)
     tree = TreeSoA(ctx, n)
     build_bvh(ctx, particles(x, y, z), tree, stream=stream)
-    idx, dist = self_knn_query(ctx, tree, k, max_k=max(32, k), method=0, stream=stream)
+    idx, dist = self_knn_query(ctx, tree, k, max_k=max(32, k), method="fast", stream=stream)
     tgt = targets(ctx, idx.reshape(-1), dist.reshape(-1), k, stream)
     f = features(ctx, tree, k, stream=stream)
     ok = torch.isfinite(tgt)

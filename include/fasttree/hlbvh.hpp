@@ -327,9 +327,9 @@ inline void load_tree(queue &q, const std::vector<unsigned char> &data, TreeSoA 
 // its output is bit-identical to the reference traversal's.  Define
 // FASTTREE_B200_PLAIN_TRAVERSAL to run the reference traversal itself.
 #if defined(FASTTREE_B200_PLAIN_TRAVERSAL)
-inline constexpr int kQueryMethod = 0;
+inline constexpr int kQueryMethod = FT_METHOD_PLAIN;
 #else
-inline constexpr int kQueryMethod = 1;
+inline constexpr int kQueryMethod = FT_METHOD_DEFAULT;
 #endif
 
 template <int _MAX_K_ = 256>

@@ -75,11 +75,20 @@ typedef struct ft_tree {
     void     *impl;      /* library-owned acceleration data; do not touch                  */
 } ft_tree;
 
+/* Query method (ft_query_options.method).  Both methods return the same rows bit for bit;
+ * the fast walk hands every query whose rows it cannot prove equal to the reference
+ * traversal's (ties, a stack that could overflow, the reference's stack guard) to that
+ * traversal, so the plain method is both fallback and check. */
+#define FT_METHOD_DEFAULT 0 /* the fast walk with exact replay (a zeroed ft_query_options)  */
+#define FT_METHOD_FAST    1 /* the same, named                                             */
+#define FT_METHOD_PLAIN   2 /* the reference traversal and heap alone                       */
+
 /* Per-query-call options (the reference's template parameters and dispatch choices). */
 typedef struct ft_query_options {
     int32_t max_k;        /* _MAX_K_ template argument; 0 = the reference's default         */
-    int32_t method;       /* 0 = plain (reference traversal), 1 = fast with exact fallback  */
-    int32_t reserved[6];
+    int32_t method;       /* FT_METHOD_DEFAULT / FT_METHOD_FAST / FT_METHOD_PLAIN           */
+    int32_t reserved[6];  /* [0] SFC seeding half-window (0 = k), [1] walk variant (0 = the
+                             tuned default), others 0                                      */
 } ft_query_options;
 
 /* Statistics of the last query on a context (fallback rate, visits). */
@@ -97,6 +106,14 @@ ft_status   ft_context_destroy(ft_context *ctx);
 const char *ft_last_error(void); /* thread-local message of the last failing call */
 int         ft_version(void);
 ft_status   ft_get_query_stats(ft_context *ctx, ft_query_stats *out);
+/* Output rows (query numbers) that the last fast-walk query on this context handed to the
+ * reference traversal (ties that could change the order, a full stack, the reference's
+ * stack guard, a bound that proved too small), in no particular order: *count_out receives
+ * how many, and up to `capacity` of them go to rows_out (host; NULL with capacity 0 to ask
+ * for the count).  Covers ft_self_knn / ft_self_knn_bounded / ft_self_knn_learned /
+ * ft_knn / ft_knn_learned with device outputs; 0 after a plain-method call.  Synchronises
+ * the device.  No counterpart in the reference (its callers cannot see which path ran). */
+ft_status   ft_get_replayed_queries(ft_context *ctx, int32_t *rows_out, size_t capacity, size_t *count_out);
 /* Synchronises stream and reports (then clears) the context's device status word: kernels
  * record bad leaf ids or an exceeded traversal bound there instead of trapping.  Blocking
  * calls check it themselves; call this after asynchronous self-kNN queries. */
@@ -325,8 +342,8 @@ ft_status ft_batch_build(ft_context *ctx, ft_batch *batch, const int64_t *set_of
 
 /* self_knn_query<MAXK> of every set: row j (set s = the set holding j) is leaf j - off[s] of
  * set s; indices are that set's leaf ranks (or input indices within the set with
- * return_orig_indices).  idx_out / dist_out: num_points x k.  Default max_k 32; method 1
- * selects the fast walk with exact replay.  Asynchronous. */
+ * return_orig_indices).  idx_out / dist_out: num_points x k.  Default max_k 32; the fast walk
+ * with exact replay unless method is FT_METHOD_PLAIN.  Asynchronous. */
 ft_status ft_batch_self_knn(ft_context *ctx, ft_batch *batch, int k, int exclude_self, uint64_t *idx_out,
                             void *dist_out, const ft_query_options *qopts, ft_stream_t stream);
 

@@ -2,11 +2,16 @@
 # against the host SYCL/oneDPL stand-ins in sycl_shim/, one shared object per compile-time
 # configuration, into oracle/_ref/.  Test infrastructure only (the checker).
 #
-#   make -C oracle -f ref.mk            # needs the reference sources at REF_SRC
+#   make -C oracle -f ref.mk REF_SRC=<reference checkout>/src
 #
 # The Morton configuration does not compile as shipped (see sycl_shim/morton_prelude.hpp);
 # its builds force-include that prelude, which declares the four missing names.
-REF_SRC  ?= /root/reference/src
+ifeq ($(REF_SRC),)
+REF_SRC  := $(FASTTREE_REF_SRC)
+endif
+ifeq ($(REF_SRC),)
+$(error set REF_SRC (or FASTTREE_REF_SRC) to the reference's src/ directory)
+endif
 CXX      := $(if $(wildcard /usr/bin/g++),/usr/bin/g++,g++)
 CXXFLAGS ?= -O2 -std=c++20 -fopenmp -ffp-contract=off -fPIC -shared -w -fno-strict-aliasing
 INC      := -Isycl_shim -I$(REF_SRC)

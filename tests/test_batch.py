@@ -38,7 +38,7 @@ def make_sets(coord, sizes, seed=7):
     return x, y, z, off
 
 
-def single(ctx, xs, ys, zs, k, method=0, ids=None):
+def single(ctx, xs, ys, zs, k, method="plain", ids=None):
     tree = ft.TreeSoA(ctx, len(xs))
     ft.build_bvh(ctx, ft.particles(xs, ys, zs, ids), tree)
     i, d = ft.self_knn_query(ctx, tree, k, max_k=max(32, k), method=method)
@@ -59,7 +59,7 @@ def test_each_set_equals_its_own_calls(coord, sfc, periodic):
     b.check()
     box, heights = b.set_info()
     for k in (1, 16, 32):
-        for method in (0, 1):
+        for method in ("plain", "fast"):
             bi, bd = b.self_knn(k, method=method)
             torch.cuda.synchronize()
             b.check()
@@ -71,7 +71,7 @@ def test_each_set_equals_its_own_calls(coord, sfc, periodic):
                 tree, si, sd = single(ctx, x[sl], y[sl], z[sl], k)
                 assert np.array_equal(rows(bi, off, s), si), (s, k, method)
                 assert np.array_equal(dist_bits(rows(bd, off, s)), dist_bits(sd)), (s, k, method)
-                if k == 16 and method == 0:
+                if k == 16 and method == "plain":
                     view = b.tree(s)
                     got, want = view.to_numpy(), tree.to_numpy()
                     for name, a in want.items():
@@ -89,7 +89,7 @@ def test_sets_against_the_oracle(coord, sfc, periodic):
     x, y, z, off = make_sets(coord, SIZES, seed=11)
     b = ft.BatchedSets(ctx, len(x), len(SIZES))
     b.build(off, x, y, z)
-    bi, bd = b.self_knn(32, method=1)
+    bi, bd = b.self_knn(32, method="fast")
     torch.cuda.synchronize()
     b.check()
     bi, bd = bi.cpu().numpy(), bd.cpu().numpy()
@@ -113,7 +113,7 @@ def test_ids_ghosts_and_original_indices():
     ghost = (rng.random(len(x)) < 0.2).astype(np.int8)
     b = ft.BatchedSets(ctx, len(x), len(sizes))
     b.build(off, x, y, z, id=ids, is_ghost=ghost)
-    bi, bd = b.self_knn(8, method=1, max_k=32)
+    bi, bd = b.self_knn(8, method="fast", max_k=32)
     torch.cuda.synchronize()
     b.check()
     bi, bd = bi.cpu().numpy(), bd.cpu().numpy()
@@ -138,7 +138,7 @@ def test_large_k_takes_the_reference_traversal():
     x, y, z, off = make_sets("f32", sizes, seed=9)
     b = ft.BatchedSets(ctx, len(x), len(sizes))
     b.build(off, x, y, z)
-    for k, method in ((100, 1), (100, 0), (64, 1)):
+    for k, method in ((100, "fast"), (100, "plain"), (64, "fast")):
         bi, bd = b.self_knn(k, method=method, max_k=128)
         torch.cuda.synchronize()
         b.check()
@@ -159,10 +159,10 @@ def test_plummer_sets_fast_equals_plain_and_sampled_sets_equal_single_builds():
     ctx = ft.Context("f32", "morton")
     b = ft.BatchedSets(ctx, len(x), len(sizes))
     b.build(off, x, y, z)
-    fi, fd = b.self_knn(32, method=1)
+    fi, fd = b.self_knn(32, method="fast")
     torch.cuda.synchronize()
     st = b.query_stats()
-    pi, pd = b.self_knn(32, method=0)
+    pi, pd = b.self_knn(32, method="plain")
     torch.cuda.synchronize()
     b.check()
     assert torch.equal(fi, pi) and torch.equal(fd, pd)
@@ -192,9 +192,9 @@ def test_graph_replay_follows_new_coordinates():
             x2, y2, z2, _ = make_sets("f32", sizes, seed=100 + rnd)
             for d, a in zip((dx, dy, dz), (x2, y2, z2)):
                 d.copy_(torch.as_tensor(a, device="cuda"))
-        b.build_knn(doff, dx, dy, dz, k, gi, gd, method=1)
+        b.build_knn(doff, dx, dy, dz, k, gi, gd, method="fast")
         ref.build(doff, dx, dy, dz)
-        ri, rd = ref.self_knn(k, method=0)
+        ri, rd = ref.self_knn(k, method="plain")
         torch.cuda.synchronize()
         b.check()
         assert torch.equal(gi.view(N, k), ri) and torch.equal(gd.view(N, k), rd), rnd
@@ -245,7 +245,7 @@ def test_periodic_sets_beyond_the_period():
         x[off[s]:off[s + 1]:37] += np.uint32(1 << 21)
     b = ft.BatchedSets(ctx, len(x), len(sizes))
     b.build(off, x, y, z)
-    bi, bd = b.self_knn(16, method=1)
+    bi, bd = b.self_knn(16, method="fast")
     torch.cuda.synchronize()
     b.check()
     bi, bd = bi.cpu().numpy(), bd.cpu().numpy()
@@ -256,6 +256,6 @@ def test_periodic_sets_beyond_the_period():
         oi, od = O.self_knn(opts, ot, 16)
         assert np.array_equal(rows(bi, off, s), oi), s
         assert np.array_equal(dist_bits(rows(bd, off, s)), dist_bits(od)), s
-        vi, vd = ft.self_knn_query(ctx, b.tree(s), 16, method=1)  # the set as a single tree
+        vi, vd = ft.self_knn_query(ctx, b.tree(s), 16, method="fast")  # the set as a single tree
         torch.cuda.synchronize()
         assert np.array_equal(vi.cpu().numpy(), oi), s

@@ -1,4 +1,4 @@
-"""Fast knn_query (method 1) of external query points: bit-identical to the plain traversal
+"""Fast knn_query (method "fast") of external query points: bit-identical to the plain traversal
 with each heap tier (register heap for k <= 32 or MAXK <= 32, SortedMergeHeap above), on
 the learned-bound workload's shape (uniform float64 tree, half uniform / half jittered
 queries), clustered and duplicate-heavy trees, queries outside the box, and trees whose keys
@@ -19,8 +19,8 @@ from tests.gpu_util import dist_bits, gen, to_coord  # noqa: E402
 
 
 def both(ctx, tree, q, k, max_k, variant=0):
-    pi, pd = ft.knn_query(ctx, tree, *q, k, max_k=max_k, method=0)
-    fi, fd = ft.knn_query(ctx, tree, *q, k, max_k=max_k, method=1, variant=variant)
+    pi, pd = ft.knn_query(ctx, tree, *q, k, max_k=max_k, method="plain")
+    fi, fd = ft.knn_query(ctx, tree, *q, k, max_k=max_k, method="fast", variant=variant)
     torch.cuda.synchronize()
     return (pi, pd), (fi, fd), ctx.query_stats()
 
@@ -84,7 +84,7 @@ def test_against_oracle_with_original_indices():
     ot = O.build_bvh(opts, x, y, z)
     qx, qy, qz = (to_coord(a, O.F64) for a in np.random.default_rng(1).uniform(0, 100.0, (3, 500)))
     for k, max_k in ((12, 32), (50, 256)):
-        gi, gd = ft.knn_query(ctx, tree, qx, qy, qz, k, max_k=max_k, method=1)
+        gi, gd = ft.knn_query(ctx, tree, qx, qy, qz, k, max_k=max_k, method="fast")
         oi, od = O.knn(opts, ot, qx, qy, qz, k, max_k)
         assert np.array_equal(gi.cpu().numpy(), oi)
         assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od))

@@ -58,7 +58,8 @@ def test_oracle_reproduces_golden(path):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("path", FIXTURES, ids=IDS)
-def test_gpu_reproduces_golden(path):
+@pytest.mark.parametrize("method", ["plain", "fast"])
+def test_gpu_reproduces_golden(path, method):
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
@@ -72,16 +73,16 @@ def test_gpu_reproduces_golden(path):
     a = tree.to_numpy()
     for k in TREE:
         assert same(a[k], g["tree_" + k]), k
-    i, d = ft.self_knn_query(ctx, tree, 16, exclude_self=True)
+    i, d = ft.self_knn_query(ctx, tree, 16, exclude_self=True, method=method)
     torch.cuda.synchronize()
     assert same(i.cpu().numpy(), g["self16_idx"]) and same(d.cpu().numpy(), g["self16_dist"])
     ids = torch.from_numpy(g["subset_ids"]).cuda()
-    i, d = ft.self_knn_query_subset(ctx, tree, ids, 40, exclude_self=False)
+    i, d = ft.self_knn_query_subset(ctx, tree, ids, 40, exclude_self=False, method=method)
     torch.cuda.synchronize()
     assert same(i.cpu().numpy(), g["sub40_idx"]) and same(d.cpu().numpy(), g["sub40_dist"])
-    i, d = ft.knn_query(ctx, tree, g["qx"], g["qy"], g["qz"], 5, max_k=256)
+    i, d = ft.knn_query(ctx, tree, g["qx"], g["qy"], g["qz"], 5, max_k=256, method=method)
     assert same(i.cpu().numpy(), g["knn5_idx"]) and same(d.cpu().numpy(), g["knn5_dist"])
-    i, d = ft.knn_query(ctx, tree, g["qx"], g["qy"], g["qz"], 48, max_k=64)
+    i, d = ft.knn_query(ctx, tree, g["qx"], g["qy"], g["qz"], 48, max_k=64, method=method)
     assert same(i.cpu().numpy(), g["knn48_idx"]) and same(d.cpu().numpy(), g["knn48_dist"])
     r, c = ft.range_query(ctx, tree, g["qx"], g["qy"], g["qz"], g["rmin"], g["rmax"], 12)
     c = c.cpu().numpy()

@@ -51,14 +51,15 @@ def test_build_matches_oracle(cfg, kind):
 @pytest.mark.parametrize("cfg", CONFIGS, ids=CONFIG_IDS)
 @pytest.mark.parametrize("kind", ["uniform", "clustered", "degenerate"])
 @pytest.mark.parametrize("k", [1, 16, 32, 33, 64])
-def test_self_knn_matches_oracle(cfg, kind, k):
+@pytest.mark.parametrize("method", ["plain", "fast"])
+def test_self_knn_matches_oracle(cfg, kind, k, method):
     coord, sfc, per = cfg
     ctx, opts = make(coord, sfc, per)
     n = 4000
     x, y, z = gen(kind, n, coord, seed=5)
     tree, ot = build_both(ctx, opts, x, y, z)
     for excl in (True, False):
-        gi, gd = ft.self_knn_query(ctx, tree, k, exclude_self=excl, max_k=max(k, 32))
+        gi, gd = ft.self_knn_query(ctx, tree, k, exclude_self=excl, max_k=max(k, 32), method=method)
         torch.cuda.synchronize()
         oi, od = O.self_knn(opts, ot, k, excl)
         gi, gd = gi.cpu().numpy(), gd.cpu().numpy()
@@ -68,7 +69,8 @@ def test_self_knn_matches_oracle(cfg, kind, k):
 
 @pytest.mark.parametrize("cfg", [CONFIGS[1], CONFIGS[7]], ids=[CONFIG_IDS[1], CONFIG_IDS[7]])
 @pytest.mark.parametrize("k", [16, 33, 128, 256])
-def test_self_knn_subset_and_orig_indices(cfg, k):
+@pytest.mark.parametrize("method", ["plain", "fast"])
+def test_self_knn_subset_and_orig_indices(cfg, k, method):
     coord, sfc, per = cfg
     for ret_orig in (False, True):
         ctx, opts = make(coord, sfc, per, ret_orig)
@@ -78,7 +80,7 @@ def test_self_knn_subset_and_orig_indices(cfg, k):
         sub = sorted(set(list(range(0, n, n // 17)) + [0, n - 1, n // 2]))
         leaf_ids = torch.tensor(sub, dtype=torch.int32, device="cuda")
         for excl in (True, False):
-            gi, gd = ft.self_knn_query_subset(ctx, tree, leaf_ids, k, exclude_self=excl)
+            gi, gd = ft.self_knn_query_subset(ctx, tree, leaf_ids, k, exclude_self=excl, method=method)
             torch.cuda.synchronize()
             oi, od = O.self_knn(opts, ot, k, excl, leaf_ids=np.array(sub, np.int32))
             assert np.array_equal(gi.cpu().numpy(), oi)
@@ -87,7 +89,7 @@ def test_self_knn_subset_and_orig_indices(cfg, k):
 
 @pytest.mark.parametrize("cfg", CONFIGS, ids=CONFIG_IDS)
 @pytest.mark.parametrize("k,max_k", [(5, 256), (32, 256), (33, 256), (48, 128), (64, 256), (64, 64), (128, 128)])
-@pytest.mark.parametrize("method", [0, 1])
+@pytest.mark.parametrize("method", ["plain", "fast"])
 def test_knn_query_matches_oracle(cfg, k, max_k, method):
     coord, sfc, per = cfg
     ctx, opts = make(coord, sfc, per)
@@ -133,7 +135,8 @@ def test_range_query_matches_oracle(cfg, max_per):
 
 @pytest.mark.parametrize("cfg", [CONFIGS[1], CONFIGS[4], CONFIGS[7]], ids=[CONFIG_IDS[1], CONFIG_IDS[4], CONFIG_IDS[7]])
 @pytest.mark.parametrize("n", [1, 2, 7, 31, 33, 63, 65, 99])
-def test_edge_sizes(cfg, n):
+@pytest.mark.parametrize("method", ["plain", "fast"])
+def test_edge_sizes(cfg, n, method):
     """n = 1, 2 and partial warps (test/test_self_knn.cpp:876-1003)."""
     coord, sfc, per = cfg
     ctx, opts = make(coord, sfc, per)
@@ -142,12 +145,12 @@ def test_edge_sizes(cfg, n):
     assert_tree_equal(tree.to_numpy(), ot, n)
     for k in (1, 2, 4, 32, 33, 64):
         for excl in (True, False):
-            gi, gd = ft.self_knn_query(ctx, tree, k, exclude_self=excl, max_k=max(k, 32))
+            gi, gd = ft.self_knn_query(ctx, tree, k, exclude_self=excl, max_k=max(k, 32), method=method)
             torch.cuda.synchronize()
             oi, od = O.self_knn(opts, ot, k, excl)
             assert np.array_equal(gi.cpu().numpy(), oi), (n, k, excl)
             assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od)), (n, k, excl)
-        gi, gd = ft.knn_query(ctx, tree, x[:3], y[:3], z[:3], k, max_k=64)
+        gi, gd = ft.knn_query(ctx, tree, x[:3], y[:3], z[:3], k, max_k=64, method=method)
         oi, od = O.knn(opts, ot, x[:3], y[:3], z[:3], k, 64)
         assert np.array_equal(gi.cpu().numpy(), oi)
 
@@ -226,7 +229,7 @@ def test_invalid_arguments():
 @pytest.mark.parametrize("kind", ["uniform", "clustered", "degenerate"])
 @pytest.mark.parametrize("k", [1, 8, 32, 33, 64])
 def test_fast_self_knn_matches_oracle(cfg, kind, k):
-    """method=1 (warp-shared walk + SFC-window seeding + exact replay of tied queries) gives
+    """method "fast" (warp-shared walk + SFC-window seeding + exact replay of tied queries) gives
     the reference's output bit for bit."""
     coord, sfc, per = cfg
     ctx, opts = make(coord, sfc, per)
@@ -234,7 +237,7 @@ def test_fast_self_knn_matches_oracle(cfg, kind, k):
     x, y, z = gen(kind, n, coord, seed=15)
     tree, ot = build_both(ctx, opts, x, y, z)
     for excl in (True, False):
-        gi, gd = ft.self_knn_query(ctx, tree, k, exclude_self=excl, max_k=max(k, 32), method=1)
+        gi, gd = ft.self_knn_query(ctx, tree, k, exclude_self=excl, max_k=max(k, 32), method="fast")
         torch.cuda.synchronize()
         stats = ctx.query_stats()
         oi, od = O.self_knn(opts, ot, k, excl)
@@ -254,7 +257,7 @@ def test_fast_walk_variants_match_oracle(cfg, variant):
     for kind, k in (("clustered", 32), ("degenerate", 16), ("uniform", 64)):
         x, y, z = gen(kind, 5000, coord, seed=23)
         tree, ot = build_both(ctx, opts, x, y, z)
-        gi, gd = ft.self_knn_query(ctx, tree, k, max_k=max(k, 32), method=1, variant=variant)
+        gi, gd = ft.self_knn_query(ctx, tree, k, max_k=max(k, 32), method="fast", variant=variant)
         torch.cuda.synchronize()
         oi, od = O.self_knn(opts, ot, k, True)
         assert np.array_equal(gi.cpu().numpy(), oi), (kind, k)
@@ -273,14 +276,14 @@ def test_fast_self_knn_subset_and_orig(cfg):
         sub = np.sort(rng.choice(n, 700, replace=False)).astype(np.int32)
         ids = torch.from_numpy(sub).cuda()
         for k in (16, 40):
-            gi, gd = ft.self_knn_query_subset(ctx, tree, ids, k, exclude_self=True, method=1)
+            gi, gd = ft.self_knn_query_subset(ctx, tree, ids, k, exclude_self=True, method="fast")
             torch.cuda.synchronize()
             oi, od = O.self_knn(opts, ot, k, True, leaf_ids=sub)
             assert np.array_equal(gi.cpu().numpy(), oi)
             assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od))
 
 
-@pytest.mark.parametrize("method,variant", [(0, 0), (1, 0), (1, 5)])
+@pytest.mark.parametrize("method,variant", [("plain", 0), ("fast", 0), ("fast", 5)])
 def test_periodic_wrap_edges_u64(method, variant):
     """42-bit periodic distances at the wrap: points at 0, 2^41 (half the period) and
     2^42 - 1, where the wrapped gap reaches its extreme values."""
@@ -318,14 +321,14 @@ def test_periodic_coordinates_beyond_the_period(coord):
     tree, ot = build_both(ctx, opts, x, y, z)
     for k in (8, 32):
         oi, od = O.self_knn(opts, ot, k, True)
-        for method in (0, 1):
+        for method in ("plain", "fast"):
             gi, gd = ft.self_knn_query(ctx, tree, k, max_k=32, method=method)
             torch.cuda.synchronize()
             assert np.array_equal(gi.cpu().numpy(), oi), (k, method)
             assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od)), (k, method)
     qx, qy, qz = gen("uniform", 300, coord, seed=52)
     oi, od = O.knn(opts, ot, qx, qy, qz, 16)
-    gi, gd = ft.knn_query(ctx, tree, qx, qy, qz, 16, method=1)
+    gi, gd = ft.knn_query(ctx, tree, qx, qy, qz, 16, method="fast")
     assert np.array_equal(gi.cpu().numpy(), oi) and np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od))
 
 
@@ -353,7 +356,7 @@ def test_u64_keys_equal_in_the_high_word(long_runs):
     z[:50] = z[50:100]
     tree, ot = build_both(ctx, opts, x, y, z)
     assert_tree_equal(tree.to_numpy(), ot, len(x))
-    gi, gd = ft.self_knn_query(ctx, tree, 16, method=1)
+    gi, gd = ft.self_knn_query(ctx, tree, 16, method="fast")
     oi, od = O.self_knn(opts, ot, 16, True)
     torch.cuda.synchronize()
     assert np.array_equal(gi.cpu().numpy(), oi) and np.array_equal(gd.cpu().numpy(), od)

@@ -40,9 +40,9 @@ def test_group_walk_equals_reference_traversal(coord, sfc, per, oc, kind):
     for k in (5, 16, 32, 64):
         mk = max(32, k)
         for excl in (True, False):
-            plain = ft.self_knn_query(ctx, tree, k, exclude_self=excl, max_k=mk, method=0)
+            plain = ft.self_knn_query(ctx, tree, k, exclude_self=excl, max_k=mk, method="plain")
             plain = (plain[0].clone(), plain[1].clone())
-            group = ft.self_knn_query(ctx, tree, k, exclude_self=excl, max_k=mk, method=1, variant=5)
+            group = ft.self_knn_query(ctx, tree, k, exclude_self=excl, max_k=mk, method="fast", variant=5)
             assert _same(plain, group), (k, excl)
 
 
@@ -54,12 +54,12 @@ def test_group_walk_subsets_orig_and_bounds(coord, sfc, per, oc):
     for ids in (np.sort(rng.choice(n, 5000, replace=False)), rng.choice(n, 5000, replace=False),
                 np.arange(n - 37, n), np.array([0, 1, 2])):
         t = torch.from_numpy(ids.astype(np.int32)).cuda()
-        a = ft.self_knn_query_subset(ctx, tree, t, k, max_k=32, method=0)
+        a = ft.self_knn_query_subset(ctx, tree, t, k, max_k=32, method="plain")
         a = (a[0].clone(), a[1].clone())
-        b = ft.self_knn_query_subset(ctx, tree, t, k, max_k=32, method=1, variant=5)
+        b = ft.self_knn_query_subset(ctx, tree, t, k, max_k=32, method="fast", variant=5)
         assert _same(a, b), len(ids)
     # per-query bounds: exact (bound at or above the k-th distance), too small, zero
-    plain = ft.self_knn_query(ctx, tree, k, max_k=32, method=0)
+    plain = ft.self_knn_query(ctx, tree, k, max_k=32, method="plain")
     plain = (plain[0].clone(), plain[1].clone())
     kth = plain[1][:, k - 1].contiguous()
     half = (kth.to(torch.int64) // 2).to(kth.dtype) if kth.dtype != torch.float64 else kth * 0.5
@@ -73,7 +73,7 @@ def test_group_walk_small_trees_fall_back():
     for n in (2, 3, 17, 40, 65, 66, 200):
         ctx, tree = _tree("u64", "ph", True, O.U64, "uniform", n, n)
         for k in (8, 32):
-            a = ft.self_knn_query(ctx, tree, k, max_k=32, method=0)
+            a = ft.self_knn_query(ctx, tree, k, max_k=32, method="plain")
             a = (a[0].clone(), a[1].clone())
-            b = ft.self_knn_query(ctx, tree, k, max_k=32, method=1, variant=5)
+            b = ft.self_knn_query(ctx, tree, k, max_k=32, method="fast", variant=5)
             assert _same(a, b), (n, k)

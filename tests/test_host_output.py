@@ -15,7 +15,7 @@ from fasttree_b200 import datasets  # noqa: E402
 
 
 @pytest.mark.parametrize("pinned", [True, False])
-@pytest.mark.parametrize("method", [0, 1])
+@pytest.mark.parametrize("method", ["plain", "fast"])
 def test_host_rows_equal_device_rows(pinned, method):
     n, k = 700_000, 16  # several chunks of 2^18 leaves
     x, y, z = datasets.clustered_fixed(n, n_spheres=1400, seed=6)
@@ -58,7 +58,7 @@ def test_sharded_rows_concatenate_to_the_full_query():
     ctx = ft.Context("u64", "ph", periodic=True)
     tree = ft.TreeSoA(ctx, n)
     ft.build_bvh(ctx, ft.particles(x, y, z), tree)
-    fi, fd = ft.self_knn_query(ctx, tree, k, method=1)
+    fi, fd = ft.self_knn_query(ctx, tree, k, method="fast")
     torch.cuda.synchronize()
     costs = np.random.default_rng(1).lognormal(0, 1, n)
     for world, c in ((3, None), (4, costs)):

@@ -131,7 +131,7 @@ def test_training_lowers_the_loss():
 
 
 def _plain(ctx, tree, k):
-    i, d = ft.self_knn_query(ctx, tree, k, max_k=max(32, k), method=0)
+    i, d = ft.self_knn_query(ctx, tree, k, max_k=max(32, k), method="plain")
     torch.cuda.synchronize()
     return i.clone(), d.clone()
 
@@ -180,7 +180,7 @@ def test_trained_bound_saves_visits():
     tree = ft.TreeSoA(ctx, len(x))
     ft.build_bvh(ctx, ft.particles(x, y, z), tree)
     pi, pd = _plain(ctx, tree, k)
-    ft.self_knn_query(ctx, tree, k, method=1)
+    ft.self_knn_query(ctx, tree, k, method="fast")
     torch.cuda.synchronize()
     fast = ctx.query_stats()
     i, d = L.self_knn_query_learned(ctx, tree, model, k, inflation=1.15)
@@ -257,7 +257,7 @@ def test_learned_knn_query_is_exact_for_any_network(coord, sfc, per):
     huge.params = p
     # both of knn_query's heap tiers: the register heap (MAXK <= 32) and the merge heap
     for k, max_k in ((16, 32), (16, 256), (32, 32), (40, 64)):
-        pi, pd = ft.knn_query(ctx, tree, qx, qy, qz, k, max_k=max_k, method=0)
+        pi, pd = ft.knn_query(ctx, tree, qx, qy, qz, k, max_k=max_k, method="plain")
         pi, pd = pi.clone(), pd.clone()
         for name, model in (("trained", trained), ("untrained", untrained), ("tiny", tiny), ("huge", huge)):
             i, d = L.knn_query_learned(ctx, tree, model, qx, qy, qz, k, max_k=max_k, inflation=1.15)

@@ -70,7 +70,7 @@ def test_tree_taller_than_62_matches_oracle():
     ot = O.build_bvh(opts, x, y, z, bbox=box.array(O.F64))
     assert tree.height() > 62, tree.height()
     for k in (1, 5, 32):
-        for method in (0, 1):
+        for method in ("plain", "fast"):
             gi, gd = ft.self_knn_query(ctx, tree, k, max_k=32, method=method)
             oi, od = O.self_knn(opts, ot, k)
             assert np.array_equal(gi.cpu().numpy(), oi), (k, method)
@@ -78,7 +78,7 @@ def test_tree_taller_than_62_matches_oracle():
     rng = np.random.default_rng(3)
     q = [np.concatenate([x, rng.uniform(0, 2.0 ** -10, 40)]) for _ in range(3)]
     for k, mk in ((4, 32), (40, 256)):
-        for method in (0, 1):
+        for method in ("plain", "fast"):
             gi, gd = ft.knn_query(ctx, tree, *q, k, max_k=mk, method=method)
             oi, od = O.knn(opts, ot, *q, k, mk)
             assert np.array_equal(gi.cpu().numpy(), oi), (k, method)

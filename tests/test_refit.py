@@ -61,7 +61,7 @@ def test_refit_equals_build_tree_with_the_same_keys(coord, sfc, per, scale):
     want = _oracle_refit(opts, ot, n, nx, ny, nz)
     assert_tree_equal(tree.to_numpy(), want, n)
     oi, od = O.self_knn(opts, want, k, True)
-    for method in (0, 1):
+    for method in ("plain", "fast"):
         gi, gd = ft.self_knn_query(ctx, tree, k, max_k=32, method=method)
         torch.cuda.synchronize()
         assert np.array_equal(gi.cpu().numpy(), oi), method
@@ -69,7 +69,7 @@ def test_refit_equals_build_tree_with_the_same_keys(coord, sfc, per, scale):
     # external queries too (the tree's keys no longer match the moved points: still exact)
     qx, qy, qz = gen("uniform", 500, coord, 13)
     oi, od = O.knn(opts, want, qx, qy, qz, k)
-    gi, gd = ft.knn_query(ctx, tree, qx, qy, qz, k, method=1)
+    gi, gd = ft.knn_query(ctx, tree, qx, qy, qz, k, method="fast")
     assert np.array_equal(gi.cpu().numpy(), oi)
     assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od))
 
@@ -93,7 +93,7 @@ def test_refit_leaf_order_and_repeated_updates():
             ft.refit_bvh(ctx, ft.particles(*cur), tree)
         want = _oracle_refit(opts, ot, n, *cur)
         assert_tree_equal(tree.to_numpy(), want, n)
-    gi, gd = ft.self_knn_query(ctx, tree, 32, method=1)
+    gi, gd = ft.self_knn_query(ctx, tree, 32, method="fast")
     oi, od = O.self_knn(opts, want, 32, True)
     torch.cuda.synchronize()
     assert np.array_equal(gi.cpu().numpy(), oi) and np.array_equal(gd.cpu().numpy(), od)
@@ -115,7 +115,7 @@ def test_refit_beyond_42_bits_takes_the_general_periodic_form():
     ft.refit_bvh(ctx, ft.particles(nx, y, z), tree)
     want = _oracle_refit(opts, ot, n, nx, y, z)
     assert_tree_equal(tree.to_numpy(), want, n)
-    for method in (0, 1):
+    for method in ("plain", "fast"):
         gi, gd = ft.self_knn_query(ctx, tree, 8, method=method)
         oi, od = O.self_knn(opts, want, 8, True)
         torch.cuda.synchronize()

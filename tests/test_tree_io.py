@@ -28,15 +28,15 @@ def _same_tree(a, b):
 
 
 def _same_queries(ctx, a, b, coord):
-    for k, mk, method in ((8, 32, 1), (32, 32, 0), (40, 64, 1)):
+    for k, mk, method in ((8, 32, "fast"), (32, 32, "plain"), (40, 64, "fast")):
         ia, da = ft.self_knn_query(ctx, a, k, max_k=mk, method=method)
         ia, da = ia.clone(), da.clone()
         ib, db = ft.self_knn_query(ctx, b, k, max_k=mk, method=method)
         torch.cuda.synchronize()
         assert torch.equal(ia, ib) and torch.equal(da, db), (k, method)
     qx, qy, qz = gen("uniform", 700, coord, 5)
-    ia, da = ft.knn_query(ctx, a, qx, qy, qz, 16, method=1)
-    ib, db = ft.knn_query(ctx, b, qx, qy, qz, 16, method=1)
+    ia, da = ft.knn_query(ctx, a, qx, qy, qz, 16, method="fast")
+    ib, db = ft.knn_query(ctx, b, qx, qy, qz, 16, method="fast")
     assert torch.equal(ia, ib) and torch.equal(da, db)
 
 

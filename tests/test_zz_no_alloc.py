@@ -2,7 +2,8 @@
 memory (a code that has handed the GPU to its own memory pool, or a step that must not be
 stalled by cudaMalloc's device-wide synchronisation).  Its scratch is a fixed array in the
 library; these tests call it through the C ABI twice in a row and check each result
-against ft_self_knn's, bit for bit.  Kept in a file of its own, collected last."""
+against ft_self_knn's, bit for bit, and the headline-shaped case against the oracle as well.
+Kept in a file of its own, collected last."""
 import ctypes
 
 import numpy as np
@@ -16,6 +17,7 @@ if not torch.cuda.is_available():
 
 import fasttree_b200 as ft  # noqa: E402
 from fasttree_b200 import capi, datasets  # noqa: E402
+from oracle import oracle as O  # noqa: E402
 from tests.gpu_util import gen  # noqa: E402
 
 MAX_QUERIES = 1 << 20
@@ -36,10 +38,10 @@ def noalloc(ctx, tree, k, leaf_ids=None, exclude_self=True):
 
 def existing(ctx, tree, k, leaf_ids=None, exclude_self=True):
     if leaf_ids is None:
-        i, d = ft.self_knn_query(ctx, tree, k, exclude_self=exclude_self, max_k=max(k, 32), method=1)
+        i, d = ft.self_knn_query(ctx, tree, k, exclude_self=exclude_self, max_k=max(k, 32), method="fast")
     else:
         i, d = ft.self_knn_query_subset(ctx, tree, leaf_ids, k, exclude_self=exclude_self, max_k=max(k, 32),
-                                        method=1)
+                                        method="fast")
     torch.cuda.synchronize()
     return i.cpu().numpy(), d.cpu().numpy()
 
@@ -55,10 +57,19 @@ def test_matches_existing_entry_point_twice_in_a_row():
     tree = ft.TreeSoA(ctx, len(x))
     ft.build_bvh(ctx, ft.particles(x, y, z), tree)
     want = existing(ctx, tree, 32)
+    want_stats = ctx.query_stats()
     first = noalloc(ctx, tree, 32)
     second = noalloc(ctx, tree, 32)
     assert same(first, want)
     assert same(second, want)
+    # the context's query statistics describe the no-allocation call, as after ft_self_knn
+    st = ctx.query_stats()
+    assert st["queries"] == len(x) and st["replayed"] == want_stats["replayed"]
+    assert st["visits"] == want_stats["visits"]
+    # and the rows are the oracle's (the reference's algorithm restated on the CPU)
+    opts = O.Options(O.U64, O.PEANO_HILBERT, True)
+    oi, od = O.self_knn(opts, O.build_bvh(opts, x, y, z), 32, True)
+    assert same(second, (oi, od))
 
 
 def test_shared_scratch_is_reset_between_calls():
@@ -102,3 +113,27 @@ def test_rejects_more_queries_than_the_fixed_scratch_holds():
                                         out_i.data_ptr(), out_d.data_ptr(), torch.cuda.current_stream().cuda_stream)
     assert st == capi.FT_ERR_INVALID_ARGUMENT
     assert b"1048576" in capi.lib().ft_last_error()
+
+
+def test_host_output_buffers_are_rejected_before_any_launch():
+    # the kernels write straight into the output arrays, so pageable host memory is refused
+    # with an error instead of reaching the GPU
+    ctx = ft.Context("f64", "morton")
+    x, y, z = gen("uniform", 1000, 1, seed=7)
+    tree = ft.TreeSoA(ctx, len(x))
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree)
+    host_i = np.empty(1000 * 8, np.uint64)
+    host_d = np.empty(1000 * 8, np.float64)
+    dev_i = torch.empty(1000 * 8, dtype=torch.uint64, device="cuda")
+    dev_d = torch.empty(1000 * 8, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for oi, od in ((host_i.ctypes.data, dev_d.data_ptr()), (dev_i.data_ptr(), host_d.ctypes.data),
+                   (host_i.ctypes.data, host_d.ctypes.data)):
+        st = capi.lib().ft_self_knn_noalloc(ctx.handle, tree.c, None, 1000, 8, 1, oi, od, stream)
+        assert st == capi.FT_ERR_INVALID_ARGUMENT
+        assert b"device memory" in capi.lib().ft_last_error()
+    host_ids = np.arange(10, dtype=np.int32)
+    st = capi.lib().ft_self_knn_noalloc(ctx.handle, tree.c, host_ids.ctypes.data, 10, 8, 1, dev_i.data_ptr(),
+                                        dev_d.data_ptr(), stream)
+    assert st == capi.FT_ERR_INVALID_ARGUMENT
+    capi.check(capi.lib().ft_check_device_status(ctx.handle, stream))
