@@ -172,15 +172,19 @@ def run_batched(args, dev, stream, timed_steps, warmup):
 
 def run_learned(args, ctx, tree, n, k, stream, fast_visits, ref_rows=None):
     """Self-kNN with the learned radius bound on the resident tree: network trained on the
-    exact self-kNN of a separate 2M draw (same generator, seed 12), 2000 Adam steps."""
+    exact self-kNN of 2M leaves of a separate draw of the same generator and size (seed 12),
+    2000 Adam steps."""
     import torch
 
     import fasttree_b200 as ft
     from fasttree_b200 import datasets
     from fasttree_b200 import learned as L
-    tx, ty, tz = datasets.clustered_fixed(2_000_000, n_spheres=4000, seed=12)
+    # a separate draw of the workload's generator at the workload's size (seed 12); the exact
+    # self-kNN of 2M of its leaves is the training set
+    tx, ty, tz = datasets.clustered_fixed(n, n_spheres=20000 if n >= 1_000_000 else max(10, n // 500), seed=12)
     t0 = time.perf_counter()
-    model, losses = L.train_bound(ctx, tx, ty, tz, k, steps=2000, batch=8192, lr=3e-3, seed=0)
+    model, losses = L.train_bound(ctx, tx, ty, tz, k, steps=2000, batch=8192, lr=3e-3, seed=0,
+                                  max_samples=2_000_000)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     dev = f"cuda:{ctx.device}"
@@ -198,7 +202,7 @@ def run_learned(args, ctx, tree, n, k, stream, fast_visits, ref_rows=None):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / steps
 
-    out = {"train_draw": "2M clustered uint64 (4000 spheres, seed 12)", "train_s": train_s,
+    out = {"train_draw": f"{n / 1e6:g}M clustered uint64 (seed 12), 2M sampled leaves", "train_s": train_s,
            "final_loss": float(np.mean(losses[-100:])), "by_inflation": {}}
     feats = L.features(ctx, tree, k)
     out["features_ms"] = timed(lambda: L.features(ctx, tree, k), 3)
@@ -415,8 +419,15 @@ def run_cfg5(args, stream):
         sub_rows[method] = (si.clone(), sd.clone())
     out["subset_fast"]["bit_exact"] = rows_equal(*sub_rows["fast"], *sub_rows["plain"])
     del si, sd, sub_rows
-    tx, ty, tz = datasets.clustered_fixed(2_000_000, n_spheres=4000, seed=15)
-    model, losses = L.train_bound(ctx, tx, ty, tz, k, steps=2000, batch=8192, seed=0)
+    # retrained on this distribution: a separate draw of the same generator at the same size
+    # (seed 15), exact self-kNN of 2M of its leaves as the training set
+    del idx, dst
+    torch.cuda.empty_cache()
+    tx, ty, tz = datasets.clustered_fixed(n, n_spheres=100_000 if n >= 5_000_000 else max(10, n // 500), seed=15)
+    model, losses = L.train_bound(ctx, tx, ty, tz, k, steps=2000, batch=8192, seed=0, max_samples=2_000_000)
+    del tx, ty, tz
+    idx = torch.empty(n * k, dtype=torch.uint64, device=dev)
+    dst = torch.empty(n * k, dtype=torch.uint64, device=dev)
     ms = _timed(stream, lambda: L.self_knn_query_learned(ctx, tree, model, k, idx, dst, inflation=1.3, max_k=k), 2)
     st = ctx.query_stats()
     lsame = True
@@ -428,7 +439,8 @@ def run_cfg5(args, stream):
         del pi2, pd2
     out["learned"] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s", "inflation": 1.3,
                       "bit_exact": lsame,
-                      "replayed": st["replayed"], "train_draw": "2M clustered uint64 (4000 spheres, seed 15)",
+                      "replayed": st["replayed"],
+                      "train_draw": f"{n / 1e6:g}M clustered uint64 (100,000 spheres, seed 15), 2M sampled leaves",
                       "final_loss": float(np.mean(losses[-100:]))}
     return out
 

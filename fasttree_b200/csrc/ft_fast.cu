@@ -18,9 +18,9 @@
 //     equal maximum (nodes at exactly the k-th distance are walked, not pruned, so such
 //     candidates are seen) -- or when an optional per-query bound cut off a possible
 //     neighbour, or its stack would overflow.  Flagged queries are rerun by the reference
-//     traversal (exact_replay_kernel, or knn_query's heap tier for external points).  Trees
-//     taller than 62 levels (where the reference's stack guard drops subtrees) always take the
-//     reference traversal.
+//     traversal (exact_replay_kernel, or knn_query's heap tier for external points).  On trees
+//     of height 63 or more the reference's stack guard drops subtrees; a query whose
+//     neighbourhood it could reach is replayed too (stack_guard_reaches).
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -151,6 +151,57 @@ template <class T> FT_D T coord_bottom() {
     else return T(0);
 }
 
+// The reference's traversal stack (MAX_STACK_DEPTH 64) pushes the children of a popped
+// internal node only while fewer than 62 entries are in use (src/hlbvh.hpp:1152, 1359, 1618,
+// 1788); on taller trees it drops them.  It pushes the farther child first and the nearer
+// one on top, so the entries below a popped node never change: after popping node v the
+// stack holds exactly the number of nearer-child turns (ld2 <= rd2 takes the left child) on
+// the root-to-v path, whatever the heap did.  The guard therefore fires only at an internal
+// node whose path has 62 such turns, and it can change the query's rows only when that node
+// lies within the query's k-th distance dk: a subtree beyond dk holds no neighbour, and no
+// point under a node is nearer than the node's box.  Returns true when some internal node
+// with 62 nearer-child turns lies within dk (then the reference traversal reruns the query).
+// The search follows a child only while its subtree is tall enough to still reach 62 turns
+// at an internal node (height >= 63 - turns); that slack never grows along a path and a far
+// turn spends one, so trees of height <= 62 need no search and taller ones are searched near
+// their tallest paths only.  Bounded: a search that runs long answers true.
+template <class T, int PER>
+FT_D bool stack_guard_reaches(const TreeDev<T> &t, T px, T py, T pz, typename Coord<T>::dist_t dk) {
+    using D = typename Coord<T>::dist_t;
+    const int n = t.n;
+    if (n < 2 || (int)t.height[0] < 63) return false;
+    constexpr int      kCap = 80;
+    unsigned long long stk[kCap]; // (node << 8) | nearer-child turns from the root
+    int                sp     = 1;
+    int                budget = 4096;
+    stk[0]                    = 0ull;
+    while (sp > 0) {
+        if (--budget < 0) return true;
+        const unsigned long long e = stk[--sp];
+        const int                u = (int)(e >> 8), s = (int)(e & 255ull);
+        T                        lb[6], rb[6];
+        int                      l, r;
+        load_rec(t.recs, u, lb, rb, l, r);
+        const D    ld2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, lb[0], lb[1], lb[2], lb[3],
+                                                                         lb[4], lb[5]);
+        const D    rd2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, rb[0], rb[1], rb[2], rb[3],
+                                                                         rb[4], rb[5]);
+        const bool left_near = ld2 <= rd2;
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const int c  = side == 0 ? l : r;
+            const D   dc = side == 0 ? ld2 : rd2;
+            const int sc = s + (((side == 0) == left_near) ? 1 : 0);
+            if (c >= n - 1 || dc > dk) continue; // a leaf, or no neighbour below it
+            if (sc >= 62) return true;            // popped with 62 entries below it: dropped
+            if ((int)t.height[c] + sc < 63) continue;
+            if (sp >= kCap) return true;
+            stk[sp++] = ((unsigned long long)c << 8) | (unsigned long long)sc;
+        }
+    }
+    return false;
+}
+
 template <class T> FT_D T warp_min_t(T v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -194,7 +245,7 @@ __global__ void __launch_bounds__(32 * fast_warps<KC>())
     const int q      = (qx && order && qbase + lane < num) ? (int)order[qbase + lane] : qbase + lane;
     bool      active = qbase + lane < num;
     // Batched sets: each lane walks the tree of the set its query belongs to (rank local to
-    // the set, output row global); a set taller than 62 goes straight to the replay.
+    // the set, output row global).
     TreeDev<T> t            = t_all;
     int        rank         = 0;
     bool       force_replay = false;
@@ -202,7 +253,7 @@ __global__ void __launch_bounds__(32 * fast_warps<KC>())
         const int s = find_set(bt.off, bt.S, active ? q : num - 1);
         t           = set_view(t_all, bt, s);
         rank        = (active ? q : num - 1) - (int)bt.off[s];
-        bool outside = bt.height[s] > 62;
+        bool outside = false;
         if constexpr (PER != 0 && !Coord<T>::is_float) {
             // periodic integer set with a coordinate at or above the period (root box maxima):
             // the box distance is not monotone there, so only the reference traversal applies
@@ -757,6 +808,11 @@ __global__ void __launch_bounds__(32 * fast_warps<KC>())
     if (active) {
         if (count >= k && hmax > B) flag = true;             // the bound may have cut a neighbour
         if (count < k && B != dist_heap_max<D>()) flag = true; // fewer than k inside the bound
+        // trees of height >= 63: the reference's stack guard may drop part of this query's
+        // neighbourhood (fewer than k points found: conservatively so)
+        if (!flag && n >= 2 && (int)t.height[0] >= 63 &&
+            (count < k || stack_guard_reaches<T, PER>(t, px, py, pz, hmax)))
+            flag = true;
         for (int hs = count; hs > 1; --hs) {
             D       last  = HD(hs - 1);
             int32_t lasti = HI(hs - 1);
@@ -933,7 +989,7 @@ static void seed_ranks(const ft_options &o, const TreeImpl &impl, const void *qx
 bool fast_self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, bool excl,
                    uint64_t *idx, void *dist, const void *bound, int half_window, int variant, cudaStream_t st) {
     TreeImpl *impl = (TreeImpl *)tr.impl;
-    if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0 || impl->height_root > 62) return false;
+    if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0) return false;
     if (!fast_walk_applies(ctx.opts, *impl)) return false;
     if (half_window <= 0) half_window = k;
     variant = walk_variant(variant, k);
@@ -1046,7 +1102,7 @@ bool fast_knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, c
               int max_k, uint64_t *idx, void *dist, int half_window, cudaStream_t st, const void *bound,
               int walk) {
     TreeImpl *impl = (TreeImpl *)tr.impl;
-    if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0 || impl->height_root > 62) return false;
+    if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0) return false;
     if (!fast_walk_applies(ctx.opts, *impl)) return false;
     // SortedMergeHeap with k equal to its capacity keeps the first k leaves it meets, not the
     // nearest: only the reference traversal reproduces that
@@ -1188,7 +1244,7 @@ static uint32_t *noalloc_scratch(int device) {
 
 size_t noalloc_max_queries() { return kNoAllocMaxQueries; }
 
-// Returns false when the fast walk does not apply (k > 64 or a tree taller than 62); the
+// Returns false when the fast walk does not apply (k > 64); the
 // caller then runs the reference traversal, which needs no scratch.
 bool fast_self_knn_noalloc(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, bool excl,
                            uint64_t *idx, void *dist, cudaStream_t st) {
@@ -1196,7 +1252,7 @@ bool fast_self_knn_noalloc(Context &ctx, const ft_tree &tr, const int32_t *leaf_
         fail(FT_ERR_INVALID_ARGUMENT, "ft_self_knn_noalloc: more than 1048576 queries in one call (the fixed "
                                       "scratch holds 2^20); split the call");
     TreeImpl *impl = (TreeImpl *)tr.impl;
-    if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0 || impl->height_root > 62) return false;
+    if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0) return false;
     if (!fast_walk_applies(ctx.opts, *impl)) return false;
     uint32_t           *s      = noalloc_scratch(ctx.device);
     uint32_t           *rc     = s;

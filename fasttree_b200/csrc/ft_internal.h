@@ -113,7 +113,8 @@ struct Context {
 };
 
 // ---- fast self-kNN (ft_fast.cu) ----
-// Returns false when the fast traversal does not apply (k > 64, tree taller than 62).
+// Returns false when the fast traversal does not apply (k > 64, a periodic tree with
+// coordinates beyond the period).
 bool fast_self_knn(Context &ctx, const ft_tree &tree, const int32_t *leaf_ids, size_t num, int k, bool exclude_self,
                    uint64_t *idx, void *dist, const void *bound, int half_window, int variant, cudaStream_t st);
 void ensure_replay(Context &ctx, size_t num);
@@ -138,7 +139,7 @@ void batch_self_knn_exact(Context &ctx, const ft_tree &all, const BatchDev &bt, 
 
 // Fast kNN of external query points (knn_query): the same walk seeded from the SFC window
 // around each query's key rank; tied queries replayed by the reference's heap tier.  False
-// when it does not apply (k > 64, k equal to the merge heap's capacity, tall tree).
+// when it does not apply (k > 64, k equal to the merge heap's capacity).
 void free_query_sort(Context &ctx);
 // Order of external query points along the tree's SFC (sorted by each point's key rank), so
 // that neighbouring threads take neighbouring queries; null when the tree's keys are not

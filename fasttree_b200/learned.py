@@ -17,7 +17,7 @@ import torch
 from . import capi
 from .capi import lib
 from .hlbvh import (Context, TreeSoA, _alloc_knn_out, _as_coord, _call, _ptr, _qopts, _rows, _stream_handle,
-                    build_bvh, dist_torch_dtype, particles, self_knn_query)
+                    build_bvh, dist_torch_dtype, particles, self_knn_query, self_knn_query_subset)
 
 N_FEATURES = 12
 N_PARAMS = 5057
@@ -119,23 +119,34 @@ class BoundModel:
             pass
 
 
-def training_set(ctx: Context, x, y, z, k: int, stream=None):
-    """(features, targets) of every leaf of a training draw: the exact self-kNN's k-th
-    distances (plain traversal) and the features of the same queries."""
+def training_set(ctx: Context, x, y, z, k: int, stream=None, max_samples: int = 0, seed: int = 0):
+    """(features, targets) of the leaves of a training draw: the exact self-kNN's k-th
+    distances and the features of the same queries.  Every leaf, or (max_samples > 0 and fewer
+    than the draw's points) that many leaves drawn at random with the seed: a draw as large as
+    the workload it serves keeps the workload's tree and density while the training set stays
+    small."""
     n = len(x)
     tree = TreeSoA(ctx, n)
     build_bvh(ctx, particles(x, y, z), tree, stream=stream)
-    idx, dist = self_knn_query(ctx, tree, k, max_k=max(32, k), method="fast", stream=stream)
+    ids = None
+    if 0 < max_samples < n:
+        g = torch.Generator(device="cpu").manual_seed(int(seed))
+        ids = torch.randperm(n, generator=g)[:max_samples].sort().values.to(torch.int32).to(f"cuda:{ctx.device}")
+        idx, dist = self_knn_query_subset(ctx, tree, ids, k, max_k=max(32, k), method="fast", stream=stream)
+    else:
+        idx, dist = self_knn_query(ctx, tree, k, max_k=max(32, k), method="fast", stream=stream)
     tgt = targets(ctx, idx.reshape(-1), dist.reshape(-1), k, stream)
-    f = features(ctx, tree, k, stream=stream)
+    f = features(ctx, tree, k, leaf_ids=ids, stream=stream)
+    del idx, dist
+    tree.free()
     ok = torch.isfinite(tgt)
     return f[ok].contiguous(), tgt[ok].contiguous()
 
 
 def train_bound(ctx: Context, x, y, z, k: int, steps: int = 2000, batch: int = 8192, lr: float = 3e-3,
-                seed: int = 0, stream=None):
+                seed: int = 0, stream=None, max_samples: int = 0):
     """Network trained on a draw's exact self-kNN (features / targets from training_set)."""
-    f, t = training_set(ctx, x, y, z, k, stream)
+    f, t = training_set(ctx, x, y, z, k, stream, max_samples=max_samples, seed=seed + 7)
     m = BoundModel(ctx, seed)
     m.fit_norm(f, t)
     losses = m.fit(f, t, steps=steps, batch=batch, lr=lr, seed=seed + 1, stream=stream)

@@ -207,7 +207,7 @@ ft_status ft_self_knn(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_
  * memory pool at start-up, or steps that must not be stalled by the device-wide
  * synchronisation of cudaMalloc / cudaFree.  No counterpart in the reference.
  * Same results as ft_self_knn (fast walk with exact replay; the reference traversal when
- * k > 64 or the tree is taller than 62).  The replay list lives in a fixed array that every
+ * k > 64).  The replay list lives in a fixed array that every
  * GPU loading this library holds until exit: at most 1048576 (2^20) queries per call, more
  * is FT_ERR_INVALID_ARGUMENT.  The first call on a device looks up that array's address;
  * make it before any stream capture.  All calls share the array: calls that overlap on the
@@ -221,7 +221,7 @@ ft_status ft_self_knn_noalloc(ft_context *ctx, const ft_tree *tree, const int32_
  * (the squared distance the query returns).  The fast walk prunes every node beyond the
  * bound; a query that ends with its k-th distance above its bound, or with fewer than k
  * points, is rerun by the reference traversal, so the output equals ft_self_knn's for any
- * bound (a good bound only saves work).  k <= 64 and tree height <= 62 use the bound; other
+ * bound (a good bound only saves work).  k <= 64 uses the bound; other
  * calls take the reference traversal.  Asynchronous. */
 ft_status ft_self_knn_bounded(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_ids, size_t num,
                               int k, int exclude_self, const void *bound, uint64_t *idx_out, void *dist_out,
@@ -242,8 +242,9 @@ ft_status ft_range(ft_context *ctx, const ft_tree *tree, const void *qx, const v
                    ft_stream_t stream);
 
 /* Height of the built tree (root to deepest leaf).  The traversal stack of the reference
- * drops children below depth 61 (src/hlbvh.hpp:1152, 1618); trees of height <= 62 never
- * reach that guard. */
+ * drops both children of a node popped with 62 entries below it (src/hlbvh.hpp:1152, 1618),
+ * which only trees of height >= 63 can reach; on those the fast walk tests each query for
+ * it and hands the queries it may affect to the reference traversal. */
 ft_status ft_tree_height(ft_context *ctx, const ft_tree *tree, int *height_out);
 
 /* ---------------------------------------------------------------------------------- */

@@ -91,3 +91,98 @@ def test_tree_taller_than_62_matches_oracle():
         assert np.array_equal(gc.cpu().numpy(), oc_), (r, max_per)
         if max_per:
             assert np.array_equal(gr.cpu().numpy(), orr), (r, max_per)
+
+
+def tall_chain_unit(duplicates: bool = False):
+    """The chain of tall_points() with one point at the origin (or its 16 copies), plus (1, .5,
+    .5), (.5, 1, .5) and (.5, .5, 1), so that the computed bounding box is the unit box and the
+    chain's keys stay single bits; each added point has one axis at the box maximum (cell 0
+    there, the reference's wrap) and its key far from the chain's.  Height 63 (67 with the
+    copies)."""
+    x, y, z = tall_points()
+    if not duplicates:
+        x, y, z = x[15:], y[15:], z[15:]
+    return np.append(x, [1.0, 0.5, 0.5]), np.append(y, [0.5, 1.0, 0.5]), np.append(z, [0.5, 0.5, 1.0])
+
+
+def tall_with_background(n_bg: int, seed: int = 5, duplicates: bool = False):
+    """Uniform background points in the unit box plus the tall chain of tall_chain_unit() at
+    the box's corner: a tree of height > 62 whose deep part is confined to the corner."""
+    cx, cy, cz = tall_chain_unit(duplicates)
+    rng = np.random.default_rng(seed)
+    bg = rng.uniform(0.0, 1.0, (3, n_bg))
+    return (np.concatenate([bg[0], cx]), np.concatenate([bg[1], cy]), np.concatenate([bg[2], cz]))
+
+
+@pytest.mark.parametrize("coord,oc", [("f64", O.F64), ("f32", O.F32)])
+def test_tall_tree_fast_walk_replays_only_guarded_queries(coord, oc):
+    """On a tree taller than 62 the fast walk answers the queries the reference's stack guard
+    cannot reach and hands the others to the reference traversal: rows equal the oracle's
+    (the reference's own drops included), and only a small part of the queries is replayed.
+    External points near the corner at k = 48 are the case where the guard matters: there the
+    reference's rows are not the nearest points (its stack drops part of the chain), and only
+    the replay reproduces them."""
+    x, y, z = (a.astype(O.NP_COORD[oc]) for a in tall_with_background(50_000))
+    n = len(x)
+    ctx = ft.Context(coord, "morton")
+    opts = O.Options(oc, O.MORTON, False)
+    box = ft.BoundingBox(0.0, 1.0, 0.0, 1.0, 0.0, 1.0)
+    tree = ft.TreeSoA(ctx, n)
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree, bbox=box)
+    ot = O.build_bvh(opts, x, y, z, bbox=box.array(oc))
+    assert tree.height() > 62, tree.height()
+    for k in (1, 8, 32, 64):
+        gi, gd = ft.self_knn_query(ctx, tree, k, max_k=max(32, k), method="fast")
+        replayed = len(ctx.replayed_queries())
+        oi, od = O.self_knn(opts, ot, k)
+        assert np.array_equal(gi.cpu().numpy(), oi), k
+        assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od)), k
+        assert replayed < n // 20, (k, replayed)
+    # external points: background-like queries and points near the corner
+    rng = np.random.default_rng(8)
+    q = [np.concatenate([rng.uniform(0, 1.0, 3000), rng.uniform(0, 2.0 ** -12, 200)]).astype(O.NP_COORD[oc])
+         for _ in range(3)]
+    for k, mk in ((16, 32), (48, 256)):
+        gi, gd = ft.knn_query(ctx, tree, *q, k, max_k=mk, method="fast")
+        replayed = len(ctx.replayed_queries())
+        oi, od = O.knn(opts, ot, *q, k, mk)
+        assert np.array_equal(gi.cpu().numpy(), oi), k
+        assert np.array_equal(dist_bits(gd.cpu().numpy()), dist_bits(od)), k
+        if k == 48:
+            assert replayed > 0
+    # a subset, twice the same leaves
+    ids = np.arange(n - 200, n, dtype=np.int32)
+    gi, gd = ft.self_knn_query_subset(ctx, tree, torch.from_numpy(ids).cuda(), 16, method="fast")
+    oi, od = O.self_knn(opts, ot, 16, True, leaf_ids=ids)
+    assert np.array_equal(gi.cpu().numpy(), oi)
+
+
+def test_tall_set_in_a_batch():
+    """A batch holding a set taller than 62 next to ordinary sets: every set's rows equal its
+    own single-tree query's."""
+    x0, y0, z0 = tall_chain_unit(duplicates=True)
+    rng = np.random.default_rng(2)
+    sets = [rng.uniform(0.0, 1.0, (3, m)) for m in (500, 3000)]
+    tx, ty, tz = tall_with_background(4000, seed=9, duplicates=True)
+    parts = [sets[0], np.stack([x0, y0, z0]), sets[1], np.stack([tx, ty, tz])]
+    x = np.concatenate([p[0] for p in parts]).astype(np.float32)
+    y = np.concatenate([p[1] for p in parts]).astype(np.float32)
+    z = np.concatenate([p[2] for p in parts]).astype(np.float32)
+    off = np.concatenate([[0], np.cumsum([p.shape[1] for p in parts])]).astype(np.int64)
+    ctx = ft.Context("f32", "morton")
+    b = ft.BatchedSets(ctx, len(x), len(parts))
+    b.build(off, x, y, z)
+    _, heights = b.set_info()
+    assert heights.max() > 62
+    for k in (4, 32):
+        fi, fd = b.self_knn(k, method="fast")
+        pi, pd = b.self_knn(k, method="plain")
+        b.check()
+        assert torch.equal(fi, pi) and torch.equal(fd, pd), k
+        opts = O.Options(O.F32, O.MORTON, False)
+        for s in range(len(parts)):
+            a, e = int(off[s]), int(off[s + 1])
+            ot = O.build_bvh(opts, x[a:e], y[a:e], z[a:e])
+            oi, od = O.self_knn(opts, ot, k)
+            assert np.array_equal(fi[a:e].cpu().numpy(), oi), (k, s)
+            assert np.array_equal(dist_bits(fd[a:e].cpu().numpy()), dist_bits(od)), (k, s)
