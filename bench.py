@@ -137,7 +137,9 @@ def run_batched(args, dev, stream, timed_steps, warmup):
     plain_ms = timed(lambda: b.self_knn(k, method="plain", results=pi, result_dists=pd), max(1, timed_steps // 2))
     b.check()
     bit_exact = {"graph_vs_plain": rows_equal(idx, dst, pi, pd), "fast_vs_plain": rows_equal(fi, fd, pi, pd)}
-    del fi, fd, pi, pd
+    del fi, fd
+    learned = run_batched_learned(args, ctx, b, off, x, y, z, k, idx, dst, (pi, pd), timed, timed_steps, plain_ms)
+    del pi, pd
     # the same sets one by one through the single-tree API (the non-batched way)
     offs = w["off"]
     if getattr(args, "no_per_set_loop", False):
@@ -145,7 +147,7 @@ def run_batched(args, dev, stream, timed_steps, warmup):
         return {"workload": w["name"], "n_sets": S, "n_points": N, "k": k,
                 "graph_build_plus_query_ms": graph_ms, "value": N / (graph_ms / 1e3), "unit": "queries/s",
                 "build_ms": build_ms, "query_fast_ms": fast_ms, "query_plain_ms": plain_ms,
-                "replayed": stats["replayed"], "bit_exact": bit_exact}
+                "replayed": stats["replayed"], "bit_exact": bit_exact, "learned": learned}
     tree = ft.TreeSoA(ctx, int(np.diff(offs).max()))
     li = torch.empty(int(np.diff(offs).max()) * k, dtype=torch.uint64, device=dev)
     ld = torch.empty_like(li, dtype=torch.float64)
@@ -165,9 +167,46 @@ def run_batched(args, dev, stream, timed_steps, warmup):
             "build_ms": build_ms, "query_fast_ms": fast_ms, "query_plain_ms": plain_ms,
             "query_fast_qps": N / (fast_ms / 1e3), "query_plain_qps": N / (plain_ms / 1e3),
             "per_set_loop_ms": loop_ms, "per_set_loop_qps": N / (loop_ms / 1e3),
-            "replayed": stats["replayed"], "bit_exact": bit_exact,
+            "replayed": stats["replayed"], "bit_exact": bit_exact, "learned": learned,
             "note": "graph = ft_batch_build_knn (build + fast self-kNN, one CUDA graph); per-set loop = "
                     "build_bvh + self_knn_query(method='fast') per set through the single-tree API (wall clock)"}
+
+
+def run_batched_learned(args, ctx, b, off, x, y, z, k, idx, dst, plain_rows, timed, steps, plain_ms):
+    """Learned radius bound on the batched sets: network trained on the exact self-kNN of a
+    separate batched draw (1024 sets of the same generator, seed 14); the learned batched
+    query alone and build + learned query in one CUDA graph, against the plain batched
+    traversal (the north-star ratio: learned + batched over plain)."""
+    import torch
+
+    from fasttree_b200 import datasets
+    from fasttree_b200 import learned as L
+    N = x.numel()
+    sizes = datasets.batched_set_sizes(1024, seed=14)
+    tx, ty, tz, toff = datasets.batched_sets(sizes=sizes, seed=14)
+    t0 = time.perf_counter()
+    model, losses = L.train_bound_batched(ctx, toff, tx, ty, tz, k, steps=2000, batch=8192)
+    torch.cuda.synchronize()
+    out = {"train_draw": f"{len(sizes)} Plummer sets ({len(tx) / 1e6:.1f}M points, seed 14), 2000 Adam steps",
+           "train_s": time.perf_counter() - t0, "final_loss": float(np.mean(losses[-100:])), "by_inflation": {}}
+    del tx, ty, tz
+    for infl in (1.15, 1.3):
+        ms = timed(lambda: b.self_knn_learned(model, k, inflation=infl, results=idx, result_dists=dst), steps)
+        st = b.query_stats()
+        out["by_inflation"][str(infl)] = {
+            "query_ms": ms, "value": N / (ms / 1e3), "unit": "queries/s", "vs_plain": plain_ms / ms,
+            "bound_misses": st["bound_misses"], "replayed": st["replayed"],
+            "visits_per_query": st["visits"] / N, "bit_exact": rows_equal(idx, dst, *plain_rows)}
+    infl = 1.3
+    gms = timed(lambda: b.build_knn_learned(model, off, x, y, z, k, idx, dst, inflation=infl), steps)
+    b.check()
+    out["graph_build_plus_learned_query"] = {"ms_per_step": gms, "value": N / (gms / 1e3), "unit": "queries/s",
+                                             "inflation": infl, "bit_exact": rows_equal(idx, dst, *plain_rows)}
+    out["note"] = ("features of every leaf on its own set + tensor-core prediction + bounded walk + rerun of the "
+                   "bound misses without the bound + replay of ties; vs_plain = plain batched traversal time / "
+                   "learned batched query time")
+    del model
+    return out
 
 
 def run_learned(args, ctx, tree, n, k, stream, fast_visits, ref_rows=None):
@@ -212,7 +251,9 @@ def run_learned(args, ctx, tree, n, k, stream, fast_visits, ref_rows=None):
                                                     max_k=max(32, k)), 3)
         st = ctx.query_stats()
         out["by_inflation"][str(infl)] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s",
-                                          "replayed": st["replayed"], "visits_per_query": st["visits"] / n}
+                                          "replayed": st["replayed"], "bound_misses": st["bound_misses"],
+                                          "visits_per_query": st["visits"] / n,
+                                          "rerun_visits_per_query": st["rerun_visits"] / n}
         if ref_rows is not None:
             out["by_inflation"][str(infl)]["bit_exact"] = rows_equal(idx, dst, *ref_rows)
     out["fast_visits_per_query"] = fast_visits
@@ -270,7 +311,8 @@ def run_knn_external(args, stream):
                                                         max_k=mk), 3)
         st = ctx.query_stats()
         learned["by_inflation"][str(infl)] = {"ms_per_step": ms, "value": nq / (ms / 1e3), "unit": "queries/s",
-                                              "replayed": st["replayed"], "visits_per_query": st["visits"] / nq,
+                                              "replayed": st["replayed"], "bound_misses": st["bound_misses"],
+                                              "visits_per_query": st["visits"] / nq,
                                               "bit_exact": rows_equal(pi, pd, idx, dst)}
     res["learned"] = learned
     res["workload"] = "1M external queries on 100K uniform float64, Morton, k=64, MAXK=256 (SortedMergeHeap)"

@@ -23,7 +23,8 @@ EXPORTED = (
     "ft_build_bvh", "ft_build_tree", "ft_refit_bvh", "ft_tree_export", "ft_tree_import", "ft_self_knn", "ft_knn", "ft_range", "ft_tree_height",
     "ft_self_knn_noalloc", "ft_self_knn_bounded",
     "ft_batch_create", "ft_batch_destroy", "ft_batch_build", "ft_batch_self_knn", "ft_batch_build_knn",
-    "ft_batch_tree", "ft_batch_set_info", "ft_batch_query_stats",
+    "ft_batch_tree", "ft_batch_set_info", "ft_batch_query_stats", "ft_batch_self_knn_learned",
+    "ft_batch_build_knn_learned", "ft_batch_bound_features",
     "ft_bound_model_create", "ft_bound_model_destroy", "ft_bound_model_get_params", "ft_bound_model_set_params",
     "ft_bound_model_set_norm", "ft_bound_features", "ft_bound_targets", "ft_bound_model_gradient",
     "ft_bound_model_fit", "ft_bound_model_predict", "ft_self_knn_learned", "ft_bound_features_points",
@@ -92,6 +93,11 @@ _SIGS = {
     "ft_batch_build_knn": [_vp, _vp, _vp, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp, _vp,
                            ctypes.POINTER(FtQueryOptions), _st],
     "ft_batch_tree": [_vp, _vp, _sz, ctypes.POINTER(FtTree), _st],
+    "ft_batch_bound_features": [_vp, _vp, _i, _vp, _st],
+    "ft_batch_self_knn_learned": [_vp, _vp, _vp, _i, _i, ctypes.c_float, _vp, _vp, ctypes.POINTER(FtQueryOptions),
+                                  _st],
+    "ft_batch_build_knn_learned": [_vp, _vp, _vp, ctypes.c_float, _vp, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _i, _i,
+                                   _vp, _vp, ctypes.POINTER(FtQueryOptions), _st],
     "ft_batch_set_info": [_vp, _vp, _vp, _vp, _st],
     "ft_batch_query_stats": [_vp, _vp, ctypes.POINTER(FtQueryStats)],
     "ft_bound_model_create": [_vp, ctypes.c_uint64, ctypes.POINTER(_vp)],

@@ -308,10 +308,13 @@ struct GraphKey {
     void       *idx = nullptr, *dist = nullptr;
     size_t      S = 0, N = 0;
     int         k = 0, excl = 0, method = 0, half = 0, variant = 0;
+    const void *model     = nullptr; // learned bound (its weights are read when the graph runs)
+    float       inflation = 0.0f;
     bool operator==(const GraphKey &o) const {
         return in_off == o.in_off && x == o.x && y == o.y && z == o.z && id == o.id && ghost == o.ghost &&
                idx == o.idx && dist == o.dist && S == o.S && N == o.N && k == o.k && excl == o.excl &&
-               method == o.method && half == o.half && variant == o.variant;
+               method == o.method && half == o.half && variant == o.variant && model == o.model &&
+               inflation == o.inflation;
     }
 };
 
@@ -324,7 +327,11 @@ struct BatchImpl {
     void      *bmin = nullptr, *bmax = nullptr; // ordered-integer boxes, 3 words per set each
     void      *bbox = nullptr, *par = nullptr;  // 6 coordinates per set each
     int32_t   *rr = nullptr, *rw = nullptr;     // replay list of the fast walk
-    uint32_t  *counters = nullptr;              // [0] replay count, [2..3] visits
+    int32_t   *mw = nullptr;                    // rows whose learned bound proved too small
+    uint32_t  *counters = nullptr;              // [0] replay count, [2..3] visits, [4] bound misses
+    float     *feats = nullptr;                 // learned bound: features and bounds of every leaf,
+    void      *bound = nullptr;                 // allocated by the first learned query
+    size_t     learned_cap = 0;
     size_t     S = 0, N = 0;
     bool       built = false;
     std::vector<std::unique_ptr<TreeImpl>> views;
@@ -351,7 +358,7 @@ void batch_free(BatchImpl *b) {
     void *ptrs[] = {b->all.min_x, b->all.max_x, b->all.min_y,  b->all.max_y,    b->all.min_z,  b->all.max_z,
                     b->all.left_child, b->all.right_child, b->all.parent, b->all.id, b->all.is_ghost,
                     b->all.orig_idx, b->off, b->node_off, b->rec_off, b->set_height, b->bmin, b->bmax, b->bbox,
-                    b->par, b->rr, b->rw, b->counters};
+                    b->par, b->rr, b->rw, b->mw, b->counters, b->feats, b->bound};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     free_scratch(b->scr);
@@ -414,8 +421,9 @@ BatchImpl *batch_create(Context &ctx, size_t max_points, size_t max_sets) {
     b->par        = dalloc<unsigned long long>(6 * max_sets);
     b->rr         = dalloc<int32_t>(P);
     b->rw         = dalloc<int32_t>(P);
-    b->counters   = dalloc<uint32_t>(4);
-    FT_CUDA(cudaMemset(b->counters, 0, 16));
+    b->mw         = dalloc<int32_t>(P);
+    b->counters   = dalloc<uint32_t>(8);
+    FT_CUDA(cudaMemset(b->counters, 0, 32));
     return b.release();
 }
 
@@ -534,28 +542,62 @@ void batch_build(Context &ctx, BatchImpl &b, const long long *in_off, size_t S, 
     }
 }
 
+// Feature and bound scratch of the learned batched query (every leaf of the batch's capacity);
+// the first learned query allocates it, later ones reuse it.
+static void ensure_batch_learned(BatchImpl &b) {
+    if (b.feats) return;
+    const size_t P = std::max<size_t>(b.max_points, 1);
+    b.feats        = dalloc<float>(P * FT_BOUND_FEATURES);
+    b.bound        = dalloc<unsigned long long>(P);
+    b.learned_cap  = P;
+}
+
+// model: null, or the learned radius bound (features -> prediction x inflation -> the walk's
+// per-query bound; queries whose bound proves too small rerun the walk without it).
 void batch_query(Context &ctx, BatchImpl &b, int k, bool excl, uint64_t *idx, void *dist, const ft_query_options &q,
-                 cudaStream_t st) {
+                 cudaStream_t st, BoundModel *model, float inflation) {
     if (!b.built) fail(FT_ERR_INVALID_ARGUMENT, "the batch has not been built");
     const int max_k = q.max_k > 0 ? q.max_k : 32;
     if (k > max_k)
         fail(FT_ERR_INVALID_ARGUMENT,
              "k exceeds _MAX_K_ template parameter. Instantiate self_knn_query with larger _MAX_K_.");
     if (k > 512) fail(FT_ERR_RUNTIME, "self_knn_query: k too large for shared memory.");
+    if (model && k > 64) fail(FT_ERR_INVALID_ARGUMENT, "learned bound: k must be in [1, 64]");
     if (b.N == 0 || k <= 0) return;
-    batch_self_knn(ctx, b.all, batch_dev(b), b.N, k, excl, idx, dist, q.method != FT_METHOD_PLAIN, q.reserved[0], q.reserved[1],
-                   b.rr, b.rw, b.counters, st);
+    const void *bound = nullptr;
+    if (model) {
+        if (!b.feats) fail(FT_ERR_RUNTIME, "the batch's learned-bound scratch is missing");
+        bound_features_batch(ctx, b.all, batch_dev(b), b.N, k, b.feats, st);
+        bound_model_predict(ctx, *model, b.feats, b.N, inflation, nullptr, b.bound, st);
+        bound = b.bound;
+    }
+    batch_self_knn(ctx, b.all, batch_dev(b), b.N, k, excl, idx, dist, q.method != FT_METHOD_PLAIN || model,
+                   q.reserved[0], q.reserved[1], b.rr, b.rw, b.counters, st, bound, b.mw);
+}
+
+void batch_features(Context &ctx, BatchImpl &b, int k, float *out, cudaStream_t st) {
+    if (!b.built) fail(FT_ERR_INVALID_ARGUMENT, "the batch has not been built");
+    bound_features_batch(ctx, b.all, batch_dev(b), b.N, k, out, st);
+}
+
+void batch_query_learned(Context &ctx, BatchImpl &b, BoundModel &model, int k, bool excl, float inflation,
+                         uint64_t *idx, void *dist, const ft_query_options &q, cudaStream_t st) {
+    ensure_batch_learned(b);
+    batch_query(ctx, b, k, excl, idx, dist, q, st, &model, inflation);
 }
 
 // Build + query as one CUDA graph: captured on the first call with these arguments (on the
 // batch's own stream, in relaxed mode), then replayed on `st`.
 void batch_build_query_graph(Context &ctx, BatchImpl &b, const long long *in_off, size_t S, size_t N, const void *x,
                              const void *y, const void *z, const uint32_t *id, const int8_t *ghost, int k, bool excl,
-                             uint64_t *idx, void *dist, const ft_query_options &q, cudaStream_t st) {
+                             uint64_t *idx, void *dist, const ft_query_options &q, cudaStream_t st, BoundModel *model,
+                             float inflation) {
+    if (model) ensure_batch_learned(b); // before any capture: the captured graph allocates nothing
     GraphKey key;
     key.in_off = in_off; key.x = x; key.y = y; key.z = z; key.id = id; key.ghost = ghost;
     key.idx = idx; key.dist = dist; key.S = S; key.N = N; key.k = k; key.excl = excl ? 1 : 0;
     key.method = q.method; key.half = q.reserved[0]; key.variant = q.reserved[1];
+    key.model = model; key.inflation = inflation;
     if (!(b.exec && key == b.key)) {
         if (b.exec) {
             FT_CUDA(cudaGraphExecDestroy(b.exec));
@@ -569,7 +611,7 @@ void batch_build_query_graph(Context &ctx, BatchImpl &b, const long long *in_off
         cudaGraph_t graph = nullptr;
         try {
             batch_build(ctx, b, in_off, S, N, x, y, z, id, ghost, b.cap_stream);
-            batch_query(ctx, b, k, excl, idx, dist, q, b.cap_stream);
+            batch_query(ctx, b, k, excl, idx, dist, q, b.cap_stream, model, inflation);
         } catch (...) {
             cudaStreamEndCapture(b.cap_stream, &graph);
             if (graph) cudaGraphDestroy(graph);
@@ -654,13 +696,16 @@ void batch_set_info(Context &ctx, BatchImpl &b, void *bbox_out, uint8_t *height_
 }
 
 void batch_stats(BatchImpl &b, ft_query_stats &out) {
-    uint32_t w[4] = {0, 0, 0, 0};
+    uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     FT_CUDA(cudaMemcpy(w, b.counters, sizeof(w), cudaMemcpyDeviceToHost));
     out.queries  = (int64_t)b.N;
     out.replayed = w[0];
-    unsigned long long v;
+    unsigned long long v, v2;
     std::memcpy(&v, &w[2], sizeof(v));
-    out.reserved[0] = (int64_t)v;
+    std::memcpy(&v2, &w[6], sizeof(v2));
+    out.reserved[0] = (int64_t)(v + v2);
+    out.reserved[1] = (int64_t)w[4];
+    out.reserved[2] = (int64_t)v2;
 }
 
 } // namespace ft

@@ -237,7 +237,7 @@ ft_status ft_context_create(const ft_options *opts, int device, ft_context **out
     ft_context *c = new ft_context();
     c->opts       = *opts;
     c->device     = device;
-    if (cudaMalloc(&c->status, 16) != cudaSuccess || cudaMemset(c->status, 0, 16) != cudaSuccess) {
+    if (cudaMalloc(&c->status, 32) != cudaSuccess || cudaMemset(c->status, 0, 32) != cudaSuccess) {
         cudaGetLastError();
         delete c;
         fail(FT_ERR_CUDA, "device status word allocation failed");
@@ -255,6 +255,8 @@ ft_status ft_context_destroy(ft_context *ctx) {
         if (ctx->replay_ranks) cudaFree(ctx->replay_ranks);
         if (ctx->replay_rows) cudaFree(ctx->replay_rows);
         if (ctx->seed_ranks) cudaFree(ctx->seed_ranks);
+        if (ctx->miss_ranks) cudaFree(ctx->miss_ranks);
+        if (ctx->miss_rows) cudaFree(ctx->miss_rows);
         for (int b = 0; b < 2; ++b) {
             if (ctx->stage_idx[b]) cudaFree(ctx->stage_idx[b]);
             if (ctx->stage_dist[b]) cudaFree(ctx->stage_dist[b]);
@@ -284,12 +286,15 @@ ft_status ft_get_query_stats(ft_context *ctx, ft_query_stats *out) {
     need(ctx && out, "null argument");
     if (ctx->last_fast) { // replay count of the last fast self-kNN (synchronises the device)
         DeviceGuard g(ctx->device);
-        uint32_t    w[3] = {0, 0, 0};
+        uint32_t    w[7] = {0, 0, 0, 0, 0, 0, 0};
         FT_CUDA(cudaMemcpy(w, ctx->status + 1, sizeof(w), cudaMemcpyDeviceToHost));
         ctx->stats.replayed = w[0];
-        unsigned long long v;
+        unsigned long long v, v2;
         std::memcpy(&v, &w[1], sizeof(v));
-        ctx->stats.reserved[0] = (int64_t)v; // lane-node visits of the fast walk
+        std::memcpy(&v2, &w[5], sizeof(v2));
+        ctx->stats.reserved[0] = (int64_t)(v + v2); // lane-node visits of the fast walk (both launches)
+        ctx->stats.reserved[1] = (int64_t)w[3];     // bound misses rerun by the walk without the bound
+        ctx->stats.reserved[2] = (int64_t)v2;       // visits of that rerun
     }
     *out = ctx->stats;
     FT_API_END
@@ -1104,6 +1109,58 @@ ft_status ft_batch_build_knn(ft_context *ctx, ft_batch *batch, const int64_t *se
     }
     ft::batch_build_query_graph(*ctx, *batch->impl, (const long long *)set_offsets, num_sets, num_points, x, y, z,
                                 id, is_ghost, k, exclude_self != 0, idx_out, dist_out, q, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_batch_bound_features(ft_context *ctx, ft_batch *batch, int k, float *features_out, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && batch, "null argument");
+    need_device(features_out, "features_out");
+    DeviceGuard g(ctx->device);
+    ft::batch_features(*ctx, *batch->impl, k, features_out, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_batch_self_knn_learned(ft_context *ctx, ft_batch *batch, ft_bound_model *model, int k, int exclude_self,
+                                    float inflation, uint64_t *idx_out, void *dist_out, const ft_query_options *qopts,
+                                    ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && batch && model, "null argument");
+    need(inflation > 0.0f, "inflation must be positive");
+    ft_query_options q{};
+    if (qopts) q = *qopts;
+    DeviceGuard g(ctx->device);
+    if (k > 0) {
+        need(idx_out && dist_out, "null output array");
+        need_device(idx_out, "idx_out");
+        need_device(dist_out, "dist_out");
+    }
+    ft::batch_query_learned(*ctx, *batch->impl, *model->impl, k, exclude_self != 0, inflation, idx_out, dist_out, q,
+                            (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_batch_build_knn_learned(ft_context *ctx, ft_batch *batch, ft_bound_model *model, float inflation,
+                                     const int64_t *set_offsets, size_t num_sets, size_t num_points, const void *x,
+                                     const void *y, const void *z, const uint32_t *id, const int8_t *is_ghost, int k,
+                                     int exclude_self, uint64_t *idx_out, void *dist_out,
+                                     const ft_query_options *qopts, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && batch && model, "null argument");
+    need(inflation > 0.0f, "inflation must be positive");
+    need(k <= 64, "learned bound: k must be in [1, 64]");
+    ft_query_options q{};
+    if (qopts) q = *qopts;
+    DeviceGuard g(ctx->device);
+    batch_args(set_offsets, num_points, x, y, z, id, is_ghost);
+    if (k > 0) {
+        need(idx_out && dist_out, "null output array");
+        need_device(idx_out, "idx_out");
+        need_device(dist_out, "dist_out");
+    }
+    ft::batch_build_query_graph(*ctx, *batch->impl, (const long long *)set_offsets, num_sets, num_points, x, y, z,
+                                id, is_ghost, k, exclude_self != 0, idx_out, dist_out, q, (cudaStream_t)stream,
+                                model->impl, inflation);
     FT_API_END
 }
 

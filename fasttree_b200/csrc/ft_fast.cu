@@ -219,40 +219,62 @@ template <class T> FT_D T warp_max_t(T v) {
     return v;
 }
 
+// Queries handed from one launch of the walk to the next (bound misses): list entry i is
+// output row rows[i] and, for self queries on one tree, leaf rank ranks[i]; *count entries.
+struct QueryList {
+    const int32_t  *ranks = nullptr;
+    const int32_t  *rows  = nullptr;
+    const uint32_t *count = nullptr; // null: no list, the launch covers queries [0, num)
+};
+// Where a launch sends the queries whose pruning bound proved too small (null rows: they
+// join the replay list like the other flagged queries).
+struct MissList {
+    int32_t  *ranks = nullptr;
+    int32_t  *rows  = nullptr;
+    uint32_t *count = nullptr;
+};
+struct ListArgs {
+    QueryList lst;
+    MissList  miss;
+};
+
+// One warp's 32 queries: entries [qbase, qbase + 32) of [0, num) -- query rows, or entries of
+// the list `lst` when it is given.
 template <class T, int PER, int KC, int VAR>
-__global__ void __launch_bounds__(32 * fast_warps<KC>())
-    fast_self_knn_kernel(TreeDev<T> t_all, BatchDev bt, const T *__restrict__ qx, const T *__restrict__ qy,
-                         const T *__restrict__ qz, const uint32_t *__restrict__ order,
-                         const int32_t *__restrict__ leaf_ids, int num, int k,
-                         int half_window, int exclude_self, int ret_orig,
-                         const typename Coord<T>::dist_t *__restrict__ bound,
-                         unsigned long long *__restrict__ out_idx, typename Coord<T>::dist_t *__restrict__ out_dist,
-                         int32_t *__restrict__ replay_ranks, int32_t *__restrict__ replay_rows,
-                         uint32_t *replay_count, uint32_t *status, unsigned long long *visit_count) {
+FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss, unsigned char *smem,
+                    TreeDev<T> t_all, BatchDev bt, const T *__restrict__ qx, const T *__restrict__ qy,
+                    const T *__restrict__ qz, const uint32_t *__restrict__ order,
+                    const int32_t *__restrict__ leaf_ids, int num, int k, int half_window, int exclude_self,
+                    int ret_orig, const typename Coord<T>::dist_t *__restrict__ bound,
+                    unsigned long long *__restrict__ out_idx, typename Coord<T>::dist_t *__restrict__ out_dist,
+                    int32_t *__restrict__ replay_ranks, int32_t *__restrict__ replay_rows, uint32_t *replay_count,
+                    uint32_t *status, unsigned long long *visit_count) {
     using D = typename Coord<T>::dist_t;
     constexpr int kFastWarps = fast_warps<KC>(), kFastThreads = 32 * kFastWarps; // this heap's block shape
-    extern __shared__ __align__(16) unsigned char smem[];
     D       *hd  = reinterpret_cast<D *>(smem);
     int32_t *hix = reinterpret_cast<int32_t *>(hd + k * kFastThreads); // heaps sized for k (<= KC)
     __shared__ int32_t s_node[kFastWarps][kFastStack];
 
     const int      tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned FULL = 0xffffffffu;
-    const int      qbase = (blockIdx.x * kFastWarps + warp) * 32;
     if (qbase >= num) return; // warp-uniform
     // External query points are walked in the order `order` (sorted by SFC rank, so a warp
-    // takes neighbouring queries); q is the output row.
-    const int q      = (qx && order && qbase + lane < num) ? (int)order[qbase + lane] : qbase + lane;
-    bool      active = qbase + lane < num;
+    // takes neighbouring queries); q is the output row.  A listed launch takes rows from the
+    // list (inactive lanes borrow the first lane's row, which is valid).
+    const bool listed = lst.count != nullptr;
+    bool       active = qbase + lane < num;
+    const int  q      = listed ? lst.rows[active ? qbase + lane : qbase]
+                               : ((qx && order && active) ? (int)order[qbase + lane] : qbase + lane);
     // Batched sets: each lane walks the tree of the set its query belongs to (rank local to
     // the set, output row global).
     TreeDev<T> t            = t_all;
     int        rank         = 0;
     bool       force_replay = false;
     if (bt.off) {
-        const int s = find_set(bt.off, bt.S, active ? q : num - 1);
-        t           = set_view(t_all, bt, s);
-        rank        = (active ? q : num - 1) - (int)bt.off[s];
+        const int qs = (active || listed) ? q : num - 1;
+        const int s  = find_set(bt.off, bt.S, qs);
+        t            = set_view(t_all, bt, s);
+        rank         = qs - (int)bt.off[s];
         bool outside = false;
         if constexpr (PER != 0 && !Coord<T>::is_float) {
             // periodic integer set with a coordinate at or above the period (root box maxima):
@@ -265,6 +287,8 @@ __global__ void __launch_bounds__(32 * fast_warps<KC>())
             force_replay = true;
             active       = false;
         }
+    } else if (listed && !qx) {
+        rank = active ? lst.ranks[qbase + lane] : 0;
     } else {
         rank = active ? (leaf_ids ? leaf_ids[q] : q) : 0;
     }
@@ -805,9 +829,18 @@ __global__ void __launch_bounds__(32 * fast_warps<KC>())
     if (lane == 0 && visit_count) atomicAdd(visit_count, (unsigned long long)visits);
 
     // ---- 3. sort, check, write ----
+    // a bound that proved too small: the bound may have cut a neighbour, or fewer than k
+    // points lie inside it.  With a miss list the query goes to the next launch (the walk
+    // without a bound); otherwise the reference traversal reruns it.
+    const bool bound_miss = active && ((count >= k && hmax > B) || (count < k && B != dist_heap_max<D>()));
+    if (bound_miss && miss.rows) {
+        const uint32_t at = atomicAdd(miss.count, 1u);
+        if (!ext && !bt.off) miss.ranks[at] = rank;
+        miss.rows[at] = q;
+        active        = false;
+    }
     if (active) {
-        if (count >= k && hmax > B) flag = true;             // the bound may have cut a neighbour
-        if (count < k && B != dist_heap_max<D>()) flag = true; // fewer than k inside the bound
+        if (bound_miss) flag = true;
         // trees of height >= 63: the reference's stack guard may drop part of this query's
         // neighbourhood (fewer than k points found: conservatively so)
         if (!flag && n >= 2 && (int)t.height[0] >= 63 &&
@@ -868,6 +901,34 @@ __global__ void __launch_bounds__(32 * fast_warps<KC>())
 #undef HI
 }
 
+// The fast walk over queries [0, num), one warp per 32 queries; or, with a list, a grid-stride
+// loop over the list's entries (the count lives on the device: no host synchronisation).
+template <class T, int PER, int KC, int VAR>
+__global__ void __launch_bounds__(32 * fast_warps<KC>())
+    fast_self_knn_kernel(QueryList lst, MissList miss, TreeDev<T> t_all, BatchDev bt, const T *__restrict__ qx,
+                         const T *__restrict__ qy, const T *__restrict__ qz, const uint32_t *__restrict__ order,
+                         const int32_t *__restrict__ leaf_ids, int num, int k, int half_window, int exclude_self,
+                         int ret_orig, const typename Coord<T>::dist_t *__restrict__ bound,
+                         unsigned long long *__restrict__ out_idx, typename Coord<T>::dist_t *__restrict__ out_dist,
+                         int32_t *__restrict__ replay_ranks, int32_t *__restrict__ replay_rows,
+                         uint32_t *replay_count, uint32_t *status, unsigned long long *visit_count) {
+    constexpr int W = fast_warps<KC>();
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int warp = threadIdx.x >> 5;
+    const int first = (blockIdx.x * W + warp) * 32;
+    if (!lst.count) {
+        fast_warp<T, PER, KC, VAR>(first, lst, miss, smem, t_all, bt, qx, qy, qz, order, leaf_ids, num, k,
+                                   half_window, exclude_self, ret_orig, bound, out_idx, out_dist, replay_ranks,
+                                   replay_rows, replay_count, status, visit_count);
+        return;
+    }
+    const int cnt = (int)*lst.count;
+    for (int base = first; base < cnt; base += gridDim.x * W * 32)
+        fast_warp<T, PER, KC, VAR>(base, lst, miss, smem, t_all, bt, qx, qy, qz, order, leaf_ids, cnt, k,
+                                   half_window, exclude_self, ret_orig, bound, out_idx, out_dist, replay_ranks,
+                                   replay_rows, replay_count, status, visit_count);
+}
+
 // -----------------------------------------------------------------------------------------
 // External query points: qx / qy / qz (else self queries) with leaf_ids = their seed ranks.
 struct ExtQueries {
@@ -894,7 +955,7 @@ template <class T, int PER, int KC>
 static void launch_fast_t(const TreeDev<T> &tv, const BatchDev &bt, const ExtQueries &eq, const int32_t *leaf_ids,
                           int num, int k, int half, bool excl, bool ro, const void *bound, uint64_t *idx, void *dist,
                           int32_t *rr, int32_t *rw, uint32_t *rc, uint32_t *status, int variant,
-                          unsigned long long *visits, cudaStream_t st) {
+                          unsigned long long *visits, cudaStream_t st, const ListArgs &la) {
     using D     = typename Coord<T>::dist_t;
     constexpr int threads = 32 * fast_warps<KC>();
     size_t        smem    = (size_t)std::max(k, 1) * threads * (sizeof(D) + 4); // heaps of k entries
@@ -904,11 +965,13 @@ static void launch_fast_t(const TreeDev<T> &tv, const BatchDev &bt, const ExtQue
                   : variant == 5 ? fast_self_knn_kernel<T, PER, KC, 5>
                                  : fast_self_knn_kernel<T, PER, KC, 2>;
     FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // a listed launch (num: the list's capacity) loops over its entries with a grid of a few
+    // blocks per SM; otherwise one warp per 32 queries
     int blocks = (num + threads - 1) / threads;
-    fn<<<blocks, threads, smem, st>>>(tv, bt, (const T *)eq.x, (const T *)eq.y, (const T *)eq.z, eq.order,
-                                           leaf_ids, num, k, half, excl ? 1 : 0, ro ? 1 : 0,
-                                           (const D *)bound, (unsigned long long *)idx, (D *)dist, rr, rw, rc,
-                                           status, visits);
+    if (la.lst.count) blocks = std::max(1, std::min(blocks, 148 * 8));
+    fn<<<blocks, threads, smem, st>>>(la.lst, la.miss, tv, bt, (const T *)eq.x, (const T *)eq.y, (const T *)eq.z,
+                                      eq.order, leaf_ids, num, k, half, excl ? 1 : 0, ro ? 1 : 0, (const D *)bound,
+                                      (unsigned long long *)idx, (D *)dist, rr, rw, rc, status, visits);
     FT_CUDA(cudaGetLastError());
 }
 
@@ -917,15 +980,16 @@ template <class T>
 static void launch_fast_view(const TreeDev<T> &tv, const BatchDev &bt, int met, bool ro, const int32_t *leaf_ids,
                              int num, int k, int half, bool excl, const void *bound, uint64_t *idx, void *dist,
                              int32_t *rr, int32_t *rw, uint32_t *rc, uint32_t *status, int variant,
-                             unsigned long long *visits, cudaStream_t st, const ExtQueries &eq = {}) {
+                             unsigned long long *visits, cudaStream_t st, const ExtQueries &eq = {},
+                             const ListArgs &la = {}) {
     met_dispatch<T>(met, [&](auto M) {
         constexpr int PER = decltype(M)::value;
         if (k <= 32)
             launch_fast_t<T, PER, 32>(tv, bt, eq, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc,
-                                      status, variant, visits, st);
+                                      status, variant, visits, st, la);
         else
             launch_fast_t<T, PER, 64>(tv, bt, eq, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc,
-                                      status, variant, visits, st);
+                                      status, variant, visits, st, la);
     });
 }
 
@@ -933,9 +997,22 @@ template <class T>
 static void launch_fast(const ft_options &o, const ft_tree &tr, const int32_t *leaf_ids, int num, int k, int half,
                         bool excl, const void *bound, uint64_t *idx, void *dist, int32_t *rr, int32_t *rw,
                         uint32_t *rc, uint32_t *status, int variant, unsigned long long *visits, cudaStream_t st,
-                        const ExtQueries &eq = {}) {
+                        const ExtQueries &eq = {}, const ListArgs &la = {}) {
     launch_fast_view<T>(tree_view<T>(tr), BatchDev{}, metric_mode<T>(o, tr), o.return_orig_indices != 0, leaf_ids,
-                        num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq);
+                        num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la);
+}
+
+// Every coordinate type: launch_fast<T> for the context's type.
+static void launch_fast_any(const ft_options &o, const ft_tree &tr, const int32_t *leaf_ids, int num, int k, int half,
+                            bool excl, const void *bound, uint64_t *idx, void *dist, int32_t *rr, int32_t *rw,
+                            uint32_t *rc, uint32_t *status, int variant, unsigned long long *visits, cudaStream_t st,
+                            const ExtQueries &eq = {}, const ListArgs &la = {}) {
+    switch (o.coord_type) {
+    case F32: launch_fast<float>(o, tr, leaf_ids, num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la); break;
+    case F64: launch_fast<double>(o, tr, leaf_ids, num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la); break;
+    case U32: launch_fast<uint32_t>(o, tr, leaf_ids, num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la); break;
+    case U64: launch_fast<unsigned long long>(o, tr, leaf_ids, num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la); break;
+    }
 }
 
 // SFC rank of external query points: the point's key (the tree's own encoding and box) and
@@ -986,6 +1063,47 @@ static void seed_ranks(const ft_options &o, const TreeImpl &impl, const void *qx
     FT_CUDA(cudaGetLastError());
 }
 
+// Bound-miss list of the context (queries whose bound proved too small in the first launch).
+static void ensure_miss(Context &ctx, size_t num) {
+    if (num <= ctx.miss_cap && ctx.miss_ranks) return;
+    if (ctx.miss_ranks) cudaFree(ctx.miss_ranks);
+    if (ctx.miss_rows) cudaFree(ctx.miss_rows);
+    ctx.miss_ranks = ctx.miss_rows = nullptr;
+    ctx.miss_cap                   = 0;
+    const size_t cap = num + num / 4 + 1024;
+    FT_CUDA(cudaMalloc(&ctx.miss_ranks, cap * sizeof(int32_t)));
+    FT_CUDA(cudaMalloc(&ctx.miss_rows, cap * sizeof(int32_t)));
+    ctx.miss_cap = cap;
+}
+
+// The fast walk over num queries (self queries, or external points with eq), its replay, and
+// with a per-query bound a second launch of the walk without the bound over the queries
+// whose bound proved too small (the walk flags its own ties there, so only those reach the
+// reference traversal).  Counters in the context's status words: [1] replayed, [2..3]
+// visits, [4] bound misses, [6..7] visits of the second launch.
+static void fast_walk_and_replay(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k,
+                                 bool excl, uint64_t *idx, void *dist, const void *bound, int half_window,
+                                 int variant, cudaStream_t st, const ExtQueries &eq = {}) {
+    uint32_t           *rc     = ctx.status + 1;
+    unsigned long long *visits = (unsigned long long *)(ctx.status + 2);
+    uint32_t           *mc     = ctx.status + 4;
+    FT_CUDA(cudaMemsetAsync(rc, 0, 7 * sizeof(uint32_t), st));
+    ListArgs la;
+    if (bound) {
+        ensure_miss(ctx, num);
+        la.miss = MissList{ctx.miss_ranks, ctx.miss_rows, mc};
+    }
+    launch_fast_any(ctx.opts, tr, leaf_ids, (int)num, k, half_window, excl, bound, idx, dist, ctx.replay_ranks,
+                    ctx.replay_rows, rc, ctx.status, variant, visits, st, eq, la);
+    if (bound) {
+        ListArgs again;
+        again.lst = QueryList{ctx.miss_ranks, ctx.miss_rows, mc};
+        launch_fast_any(ctx.opts, tr, leaf_ids, (int)num, k, half_window, excl, nullptr, idx, dist, ctx.replay_ranks,
+                        ctx.replay_rows, rc, ctx.status, variant, (unsigned long long *)(ctx.status + 6), st, eq,
+                        again);
+    }
+}
+
 bool fast_self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, bool excl,
                    uint64_t *idx, void *dist, const void *bound, int half_window, int variant, cudaStream_t st) {
     TreeImpl *impl = (TreeImpl *)tr.impl;
@@ -994,16 +1112,8 @@ bool fast_self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, siz
     if (half_window <= 0) half_window = k;
     variant = walk_variant(variant, k);
     ensure_replay(ctx, num);
-    uint32_t           *rc     = ctx.status + 1;
-    unsigned long long *visits = (unsigned long long *)(ctx.status + 2);
-    FT_CUDA(cudaMemsetAsync(rc, 0, 3 * sizeof(uint32_t), st));
-    switch (ctx.opts.coord_type) {
-    case F32: launch_fast<float>(ctx.opts, tr, leaf_ids, (int)num, k, half_window, excl, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st); break;
-    case F64: launch_fast<double>(ctx.opts, tr, leaf_ids, (int)num, k, half_window, excl, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st); break;
-    case U32: launch_fast<uint32_t>(ctx.opts, tr, leaf_ids, (int)num, k, half_window, excl, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st); break;
-    case U64: launch_fast<unsigned long long>(ctx.opts, tr, leaf_ids, (int)num, k, half_window, excl, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st); break;
-    }
-    replay_exact(ctx, tr, ctx.replay_ranks, ctx.replay_rows, rc, k, excl, idx, dist, st);
+    fast_walk_and_replay(ctx, tr, leaf_ids, num, k, excl, idx, dist, bound, half_window, variant, st);
+    replay_exact(ctx, tr, ctx.replay_ranks, ctx.replay_rows, ctx.status + 1, k, excl, idx, dist, st);
     return true;
 }
 
@@ -1112,28 +1222,20 @@ bool fast_knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, c
     if (half_window <= 0) half_window = k;
     const int  n      = (int)tr.num_leaves;
     const bool ranked = compute_seed_ranks(ctx, tr, qx, qy, qz, nq, st);
-    uint32_t           *rc     = ctx.status + 1;
-    unsigned long long *visits = (unsigned long long *)(ctx.status + 2);
-    FT_CUDA(cudaMemsetAsync(rc, 0, 3 * sizeof(uint32_t), st));
     ExtQueries eq;
     eq.x = qx;
     eq.y = qy;
     eq.z = qz;
     if (ranked && nq > 1) eq.order = order_by_rank(ctx, nq, n, st); // walk the queries in SFC order
     const int variant = walk_variant(walk, k);
-    switch (ctx.opts.coord_type) {
-    case F32: launch_fast<float>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
-    case F64: launch_fast<double>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
-    case U32: launch_fast<uint32_t>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
-    case U64: launch_fast<unsigned long long>(ctx.opts, tr, ctx.seed_ranks, (int)nq, k, half_window, false, bound, idx, dist, ctx.replay_ranks, ctx.replay_rows, rc, ctx.status, variant, visits, st, eq); break;
-    }
-    replay_external(ctx, tr, qx, qy, qz, ctx.replay_rows, rc, k, max_k, idx, dist, st);
+    fast_walk_and_replay(ctx, tr, ctx.seed_ranks, nq, k, false, idx, dist, bound, half_window, variant, st, eq);
+    replay_external(ctx, tr, qx, qy, qz, ctx.replay_rows, ctx.status + 1, k, max_k, idx, dist, st);
     return true;
 }
 
 void batch_self_knn(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, bool excl, uint64_t *idx,
                     void *dist, bool fast, int half_window, int variant, int32_t *rr, int32_t *rw, uint32_t *counters,
-                    cudaStream_t st) {
+                    cudaStream_t st, const void *bound, int32_t *mw) {
     if (num == 0 || k <= 0) return;
     if (!fast || k > 64) {
         batch_self_knn_exact(ctx, all, bt, num, k, excl, idx, dist, st);
@@ -1144,15 +1246,25 @@ void batch_self_knn(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t
     unsigned long long *visits     = (unsigned long long *)(counters + 2);
     const bool          ro         = ctx.opts.return_orig_indices != 0;
     const int           n          = (int)num;
-    FT_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(uint32_t), st));
-#define FT_BF(T)                                                                                                   \
+    FT_CUDA(cudaMemsetAsync(counters, 0, 8 * sizeof(uint32_t), st));
+    ListArgs first, again;
+    if (bound) { // bound misses: leaf ranks follow from the rows inside a batch, so rows suffice
+        first.miss = MissList{nullptr, mw, counters + 4};
+        again.lst  = QueryList{nullptr, mw, counters + 4};
+    }
+#define FT_BF(T, B, LA)                                                                                            \
     launch_fast_view<T>(tree_view<T>(all), bt, metric_mode<T>(ctx.opts, all), ro, nullptr, n, k, half_window, excl, \
-                        nullptr, idx, dist, rr, rw, counters, ctx.status, variant, visits, st)
-    switch (ctx.opts.coord_type) {
-    case F32: FT_BF(float); break;
-    case F64: FT_BF(double); break;
-    case U32: FT_BF(uint32_t); break;
-    case U64: FT_BF(unsigned long long); break;
+                        B, idx, dist, rr, rw, counters, ctx.status, variant, visits, st, ExtQueries{}, LA)
+    for (int pass = 0; pass < (bound ? 2 : 1); ++pass) {
+        const void     *b  = pass == 0 ? bound : nullptr;
+        const ListArgs &la = pass == 0 ? first : again;
+        if (pass == 1) visits = (unsigned long long *)(counters + 6); // the rerun's visits apart
+        switch (ctx.opts.coord_type) {
+        case F32: FT_BF(float, b, la); break;
+        case F64: FT_BF(double, b, la); break;
+        case U32: FT_BF(uint32_t, b, la); break;
+        case U64: FT_BF(unsigned long long, b, la); break;
+        }
     }
 #undef FT_BF
     replay_exact(ctx, all, rr, rw, counters, k, excl, idx, dist, st, bt);
@@ -1273,6 +1385,7 @@ bool fast_self_knn_noalloc(Context &ctx, const ft_tree &tr, const int32_t *leaf_
     // (scratch words: [0] replay count, [2..3] visits; context words: [1] and [2..3])
     FT_CUDA(cudaMemcpyAsync(ctx.status + 1, rc, sizeof(uint32_t), cudaMemcpyDeviceToDevice, st));
     FT_CUDA(cudaMemcpyAsync(ctx.status + 2, visits, sizeof(unsigned long long), cudaMemcpyDeviceToDevice, st));
+    FT_CUDA(cudaMemsetAsync(ctx.status + 4, 0, 4 * sizeof(uint32_t), st)); // no bound, no bound misses
     ctx.stats.queries  = (int64_t)num;
     ctx.stats.replayed = 0;
     ctx.last_fast      = true;

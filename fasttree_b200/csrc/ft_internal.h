@@ -91,11 +91,15 @@ struct Context {
     int            device = 0;
     int            num_sms = 148;
     ft_query_stats stats{};
-    uint32_t      *status = nullptr; // [0] status word of query kernels, [1] replay count
+    uint32_t      *status = nullptr; // [0] status word of query kernels, [1] replay count,
+                                     // [2..3] visits, [4] bound misses (8 words)
     int32_t       *replay_ranks = nullptr; // queries the fast traversal hands to the exact one
     int32_t       *replay_rows  = nullptr;
     int32_t       *seed_ranks   = nullptr; // SFC rank of each external query (fast knn)
     size_t         replay_cap   = 0;
+    int32_t       *miss_ranks   = nullptr; // queries whose pruning bound proved too small
+    int32_t       *miss_rows    = nullptr;
+    size_t         miss_cap     = 0;
     bool           last_fast    = false; // the last self-kNN call used the fast traversal
     bool           last_rows    = false; // replay_rows holds the last fast call's replayed rows
     TreeImpl       qsort;                   // sort scratch of external queries (fast knn)
@@ -130,9 +134,11 @@ void replay_exact(Context &ctx, const ft_tree &tree, const int32_t *ranks, const
 // Self-kNN over every leaf of a batch of trees (`all` spans the concatenated arrays):
 // the fast walk with its replay (replay lists rr / rw, counters = 4 device words) or, with
 // fast == false or k > 64, the reference traversal.  No allocation, no host synchronisation.
+// With a per-query bound (device, dist units) the queries whose bound proves too small go
+// through the miss list (mw, counters[4]) to a second launch of the walk without the bound.
 void batch_self_knn(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, bool exclude_self,
                     uint64_t *idx, void *dist, bool fast, int half_window, int variant, int32_t *rr, int32_t *rw,
-                    uint32_t *counters, cudaStream_t st);
+                    uint32_t *counters, cudaStream_t st, const void *bound = nullptr, int32_t *mw = nullptr);
 // The reference traversal over every leaf of a batch (ft_query.cu).
 void batch_self_knn_exact(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, bool exclude_self,
                           uint64_t *idx, void *dist, cudaStream_t st);
@@ -209,12 +215,19 @@ void       batch_free(BatchImpl *b);
 // set_offsets: device, S + 1 entries.  Asynchronous; no allocation, no host synchronisation.
 void batch_build(Context &ctx, BatchImpl &b, const long long *set_offsets, size_t S, size_t N, const void *x,
                  const void *y, const void *z, const uint32_t *id, const int8_t *ghost, cudaStream_t st);
+struct BoundModel;
+// model: null, or the learned radius bound (its scratch must exist: batch_query_learned or a
+// graph with the model makes it).
 void batch_query(Context &ctx, BatchImpl &b, int k, bool exclude_self, uint64_t *idx, void *dist,
-                 const ft_query_options &q, cudaStream_t st);
+                 const ft_query_options &q, cudaStream_t st, BoundModel *model = nullptr, float inflation = 0.0f);
+// The learned bound's 12 features of every leaf of every set (device, N x 12 floats).
+void batch_features(Context &ctx, BatchImpl &b, int k, float *out, cudaStream_t st);
+void batch_query_learned(Context &ctx, BatchImpl &b, BoundModel &model, int k, bool exclude_self, float inflation,
+                         uint64_t *idx, void *dist, const ft_query_options &q, cudaStream_t st);
 void batch_build_query_graph(Context &ctx, BatchImpl &b, const long long *set_offsets, size_t S, size_t N,
                              const void *x, const void *y, const void *z, const uint32_t *id, const int8_t *ghost,
                              int k, bool exclude_self, uint64_t *idx, void *dist, const ft_query_options &q,
-                             cudaStream_t st);
+                             cudaStream_t st, BoundModel *model = nullptr, float inflation = 0.0f);
 void batch_tree_view(Context &ctx, BatchImpl &b, size_t set, ft_tree &out, cudaStream_t st);
 void batch_set_info(Context &ctx, BatchImpl &b, void *bbox_out, uint8_t *height_out, cudaStream_t st);
 void batch_stats(BatchImpl &b, ft_query_stats &out);
@@ -236,6 +249,9 @@ void        bound_model_fit(BoundModel &b, const float *feats, const float *targ
                             float lr, unsigned long long seed, float *loss_host, cudaStream_t st);
 void        bound_model_predict(Context &ctx, BoundModel &b, const float *feats, size_t n, float inflation,
                                 float *pred, void *bound, cudaStream_t st);
+// Features of every leaf of a batch of sets (BatchDev over the concatenated arrays of `all`).
+void        bound_features_batch(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, float *out,
+                                 cudaStream_t st);
 void        bound_features_points(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
                                   size_t nq, int k, float *out, cudaStream_t st);
 void        knn_learned(Context &ctx, const ft_tree &tr, BoundModel &b, const void *qx, const void *qy,

@@ -151,19 +151,34 @@ FT_D float pick64(const float (&v)[64], int i) {
 
 template <class T, int PER>
 __global__ void __launch_bounds__(kFeatThreads)
-    bound_features_kernel(TreeDev<T> t, const int32_t *__restrict__ parent, const unsigned long long *klo,
-                          const unsigned long long *khi, const int32_t *__restrict__ leaf_ids, int num, int k,
-                          const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
-                          float *__restrict__ out, uint32_t *status) {
+    bound_features_kernel(TreeDev<T> t_all, BatchDev bt, const int32_t *__restrict__ parent_all,
+                          const unsigned long long *klo_all, const unsigned long long *khi_all,
+                          const int32_t *__restrict__ leaf_ids, int num, int k, const T *__restrict__ qx,
+                          const T *__restrict__ qy, const T *__restrict__ qz, float *__restrict__ out,
+                          uint32_t *status) {
     using D = typename Coord<T>::dist_t;
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= num) return;
+    // batched sets: query q is leaf q - off[s] of the set s holding it, and every array below
+    // is that set's (its own tree, parents and sorted keys)
+    TreeDev<T>                t      = t_all;
+    const int32_t            *parent = parent_all;
+    const unsigned long long *klo = klo_all, *khi = khi_all;
+    int                       set_rank = -1;
+    if (bt.off) {
+        const int s = find_set(bt.off, bt.S, q);
+        t           = set_view(t_all, bt, s);
+        parent      = parent_all + bt.node_off[s];
+        klo         = klo_all + bt.off[s];
+        khi         = nullptr; // batched sets have one-word keys
+        set_rank    = q - (int)bt.off[s];
+    }
     const int  n   = t.n;
     // external query points (qx != null): leaf_ids holds each point's SFC rank (the lower
     // bound of its key among the sorted keys); the leaf there stands for the point, and the
     // window is the 2k leaves [r - k, r + k) seen from the point itself
     const bool ext  = qx != nullptr;
-    const int  rank = ext ? min(max(leaf_ids[q], 0), n - 1) : (leaf_ids ? leaf_ids[q] : q);
+    const int  rank = set_rank >= 0 ? set_rank : ext ? min(max(leaf_ids[q], 0), n - 1) : (leaf_ids ? leaf_ids[q] : q);
     float     *f    = out + (size_t)q * kFeat;
     if (rank < 0 || rank >= n) {
         atomicOr(status, STATUS_BAD_INPUT);
@@ -959,28 +974,38 @@ void bound_model_predict(Context &ctx, BoundModel &b, const float *feats, size_t
 
 template <class T>
 static void features_typed(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, int num, int k, const void *qx,
-                           const void *qy, const void *qz, float *out, cudaStream_t st) {
+                           const void *qy, const void *qz, float *out, cudaStream_t st, const BatchDev &bt) {
     const TreeImpl &impl = *(const TreeImpl *)tr.impl;
     TreeDev<T>      tv   = tree_view<T>(tr);
     const int       grid = (num + kFeatThreads - 1) / kFeatThreads;
     met_dispatch<T>(metric_mode<T>(ctx.opts, tr), [&](auto M) {
         bound_features_kernel<T, decltype(M)::value><<<grid, kFeatThreads, 0, st>>>(
-            tv, tr.parent, (const unsigned long long *)impl.key_lo, (const unsigned long long *)impl.key_hi, leaf_ids,
-            num, k, (const T *)qx, (const T *)qy, (const T *)qz, out, ctx.status);
+            tv, bt, tr.parent, (const unsigned long long *)impl.key_lo, (const unsigned long long *)impl.key_hi,
+            leaf_ids, num, k, (const T *)qx, (const T *)qy, (const T *)qz, out, ctx.status);
     });
     FT_CUDA(cudaGetLastError());
 }
 
 // leaf_ids: self queries (null: every leaf); or, with qx/qy/qz, the SFC ranks of external
-// query points.
+// query points; with bt, every leaf of a batch of sets.
 static void features_impl(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k,
-                          const void *qx, const void *qy, const void *qz, float *out, cudaStream_t st) {
+                          const void *qx, const void *qy, const void *qz, float *out, cudaStream_t st,
+                          const BatchDev &bt = {}) {
     switch (ctx.opts.coord_type) {
-    case F32: features_typed<float>(ctx, tr, leaf_ids, (int)num, k, qx, qy, qz, out, st); break;
-    case F64: features_typed<double>(ctx, tr, leaf_ids, (int)num, k, qx, qy, qz, out, st); break;
-    case U32: features_typed<uint32_t>(ctx, tr, leaf_ids, (int)num, k, qx, qy, qz, out, st); break;
-    case U64: features_typed<unsigned long long>(ctx, tr, leaf_ids, (int)num, k, qx, qy, qz, out, st); break;
+    case F32: features_typed<float>(ctx, tr, leaf_ids, (int)num, k, qx, qy, qz, out, st, bt); break;
+    case F64: features_typed<double>(ctx, tr, leaf_ids, (int)num, k, qx, qy, qz, out, st, bt); break;
+    case U32: features_typed<uint32_t>(ctx, tr, leaf_ids, (int)num, k, qx, qy, qz, out, st, bt); break;
+    case U64: features_typed<unsigned long long>(ctx, tr, leaf_ids, (int)num, k, qx, qy, qz, out, st, bt); break;
     }
+}
+
+// The 12 features of every leaf of a batch of sets (`all` spans the concatenated arrays; its
+// sorted keys are the sets' own, back to back).  Asynchronous; allocates nothing.
+void bound_features_batch(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, float *out,
+                          cudaStream_t st) {
+    if (k < 1 || k > kMaxBoundK) fail(FT_ERR_INVALID_ARGUMENT, "learned bound: k must be in [1, 64]");
+    if (num == 0) return;
+    features_impl(ctx, all, nullptr, num, k, nullptr, nullptr, nullptr, out, st, bt);
 }
 
 static void check_bound_tree(const ft_tree &tr, int k) {

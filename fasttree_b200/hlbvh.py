@@ -102,7 +102,8 @@ class Context:
     def query_stats(self):
         s = capi.FtQueryStats()
         check(lib().ft_get_query_stats(self._h, ctypes.byref(s)))
-        return {"queries": s.queries, "replayed": s.replayed, "visits": s.reserved[0]}
+        return {"queries": s.queries, "replayed": s.replayed, "visits": s.reserved[0],
+                "bound_misses": s.reserved[1], "rerun_visits": s.reserved[2]}
 
     def check_device_status(self, stream=None):
         """Synchronises the stream and raises what the kernels recorded (ft_check_device_status)."""
@@ -587,6 +588,39 @@ class BatchedSets:
         self.num_sets, self.num_points = S, N
         return _rows(results, N, k), _rows(result_dists, N, k)
 
+    def bound_features(self, k: int, stream=None) -> torch.Tensor:
+        """(num_points, 12) float32 learned-bound features of every leaf, each on its own set."""
+        out = torch.empty((max(self.num_points, 1), 12), dtype=torch.float32, device=f"cuda:{self.ctx.device}")
+        _call(lib().ft_batch_bound_features(self.ctx.handle, self._h, int(k), _ptr(out), _stream_handle(stream)))
+        return out[: self.num_points]
+
+    def self_knn_learned(self, model, k: int, inflation: float = 1.3, exclude_self=True, max_k: int = 32,
+                         results=None, result_dists=None, stream=None):
+        """self_knn of every set with the learned radius bound (ft_batch_self_knn_learned): the
+        same rows as self_knn; `model` is a learned.BoundModel of this context."""
+        N = self.num_points
+        if results is None:
+            results, result_dists = _alloc_knn_out(self.ctx, N, k)
+        _call(lib().ft_batch_self_knn_learned(self.ctx.handle, self._h, model._h, int(k), int(bool(exclude_self)),
+                                              ctypes.c_float(inflation), _ptr(results), _ptr(result_dists),
+                                              ctypes.byref(_qopts(max_k, "fast")), _stream_handle(stream)))
+        return _rows(results, N, k), _rows(result_dists, N, k)
+
+    def build_knn_learned(self, model, set_offsets, pos_x, pos_y, pos_z, k: int, results, result_dists,
+                          inflation: float = 1.3, exclude_self=True, max_k: int = 32, id=None, is_ghost=None,
+                          stream=None):
+        """build + self_knn_learned as one CUDA graph (ft_batch_build_knn_learned); the arrays
+        must stay alive and in place between calls, as for build_knn."""
+        off, xyz, ids, gh = self._inputs(set_offsets, pos_x, pos_y, pos_z, id, is_ghost)
+        S, N = off.numel() - 1, xyz[0].numel()
+        _call(lib().ft_batch_build_knn_learned(self.ctx.handle, self._h, model._h, ctypes.c_float(inflation),
+                                               _ptr(off), S, N, *[_ptr(a) for a in xyz], _ptr(ids), _ptr(gh), int(k),
+                                               int(bool(exclude_self)), _ptr(results), _ptr(result_dists),
+                                               ctypes.byref(_qopts(max_k, "fast")), _stream_handle(stream)))
+        self._keep = (off, xyz, ids, gh, results, result_dists, model)
+        self.num_sets, self.num_points = S, N
+        return _rows(results, N, k), _rows(result_dists, N, k)
+
     def tree(self, s: int, stream=None) -> TreeSoA:
         c = capi.FtTree()
         _call(lib().ft_batch_tree(self.ctx.handle, self._h, int(s), ctypes.byref(c), _stream_handle(stream)))
@@ -604,7 +638,8 @@ class BatchedSets:
     def query_stats(self):
         st = capi.FtQueryStats()
         _call(lib().ft_batch_query_stats(self.ctx.handle, self._h, ctypes.byref(st)))
-        return {"queries": st.queries, "replayed": st.replayed, "visits": st.reserved[0]}
+        return {"queries": st.queries, "replayed": st.replayed, "visits": st.reserved[0],
+                "bound_misses": st.reserved[1], "rerun_visits": st.reserved[2]}
 
     def check(self, stream=None):
         """Reports errors the kernels recorded (bad set offsets, bounded waits); synchronises."""

@@ -143,6 +143,32 @@ def training_set(ctx: Context, x, y, z, k: int, stream=None, max_samples: int = 
     return f[ok].contiguous(), tgt[ok].contiguous()
 
 
+def training_set_batched(ctx: Context, set_offsets, x, y, z, k: int, stream=None):
+    """(features, targets) of every leaf of a batched training draw (BatchedSets): each set's
+    exact self-kNN and its features on its own tree."""
+    from .hlbvh import BatchedSets
+    off = np.asarray(set_offsets, np.int64)
+    b = BatchedSets(ctx, int(off[-1]), len(off) - 1)
+    b.build(off, x, y, z, stream=stream)
+    idx, dist = b.self_knn(k, max_k=max(32, k), method="fast", stream=stream)
+    tgt = targets(ctx, idx.reshape(-1), dist.reshape(-1), k, stream)
+    f = b.bound_features(k, stream=stream)
+    del idx, dist
+    b.free()
+    ok = torch.isfinite(tgt)
+    return f[ok].contiguous(), tgt[ok].contiguous()
+
+
+def train_bound_batched(ctx: Context, set_offsets, x, y, z, k: int, steps: int = 2000, batch: int = 8192,
+                        lr: float = 3e-3, seed: int = 0, stream=None):
+    """Network trained on a batched draw's exact self-kNN (training_set_batched)."""
+    f, t = training_set_batched(ctx, set_offsets, x, y, z, k, stream)
+    m = BoundModel(ctx, seed)
+    m.fit_norm(f, t)
+    losses = m.fit(f, t, steps=steps, batch=batch, lr=lr, seed=seed + 1, stream=stream)
+    return m, losses
+
+
 def train_bound(ctx: Context, x, y, z, k: int, steps: int = 2000, batch: int = 8192, lr: float = 3e-3,
                 seed: int = 0, stream=None, max_samples: int = 0):
     """Network trained on a draw's exact self-kNN (features / targets from training_set)."""

@@ -94,8 +94,10 @@ typedef struct ft_query_options {
 /* Statistics of the last query on a context (fallback rate, visits). */
 typedef struct ft_query_stats {
     int64_t queries;
-    int64_t replayed;      /* queries rerun by the plain traversal (ties / bound misses)    */
-    int64_t reserved[6];
+    int64_t replayed;      /* queries rerun by the plain traversal (ties, the stack guard)   */
+    int64_t reserved[6];   /* [0] node visits of the fast walk (lane-node evaluations, every
+                              launch); [1] queries whose pruning bound proved too small, rerun
+                              by the fast walk without the bound; [2] the visits of that rerun */
 } ft_query_stats;
 
 /* ---------------------------------------------------------------------------------- */
@@ -355,6 +357,33 @@ ft_status ft_batch_build_knn(ft_context *ctx, ft_batch *batch, const int64_t *se
                              size_t num_points, const void *x, const void *y, const void *z, const uint32_t *id,
                              const int8_t *is_ghost, int k, int exclude_self, uint64_t *idx_out, void *dist_out,
                              const ft_query_options *qopts, ft_stream_t stream);
+
+/* The learned bound's 12 features (ft_bound_features) of every leaf of every set of the last
+ * build, each computed on its own set's tree: features_out is device memory, num_points x 12
+ * floats.  Asynchronous. */
+ft_status ft_batch_bound_features(ft_context *ctx, ft_batch *batch, int k, float *features_out, ft_stream_t stream);
+
+/* ft_batch_self_knn with the learned radius bound (k <= 64): the 12 features of every leaf
+ * of every set (each set's own tree, parents and keys), the network's bound for each, the
+ * fast walk with that bound, a second launch of the walk without the bound for the queries
+ * whose bound proved too small, then the replay of tied queries.  Same rows as
+ * ft_batch_self_knn.  The first call on a batch allocates its feature and bound scratch
+ * (13 floats per point of max_points); later calls allocate nothing.  The model must live as
+ * long as the call runs.  Asynchronous. */
+ft_status ft_batch_self_knn_learned(ft_context *ctx, ft_batch *batch, ft_bound_model *model, int k, int exclude_self,
+                                    float inflation, uint64_t *idx_out, void *dist_out, const ft_query_options *qopts,
+                                    ft_stream_t stream);
+
+/* ft_batch_build + ft_batch_self_knn_learned as one CUDA graph (captured on the first call
+ * with these arguments, replayed by later calls; the scratch is allocated before the
+ * capture).  The graph reads the model's weights when it runs, so a retrained model is
+ * used as it stands; destroying the model while the batch may still replay the graph is
+ * an error of the caller.  Asynchronous. */
+ft_status ft_batch_build_knn_learned(ft_context *ctx, ft_batch *batch, ft_bound_model *model, float inflation,
+                                     const int64_t *set_offsets, size_t num_sets, size_t num_points, const void *x,
+                                     const void *y, const void *z, const uint32_t *id, const int8_t *is_ghost, int k,
+                                     int exclude_self, uint64_t *idx_out, void *dist_out,
+                                     const ft_query_options *qopts, ft_stream_t stream);
 
 /* View of one built set as an ft_tree (arrays inside the batch; valid until the next build
  * of the batch).  Usable with every query entry point; not with builds, ensure or destroy.

@@ -259,3 +259,68 @@ def test_periodic_sets_beyond_the_period():
         vi, vd = ft.self_knn_query(ctx, b.tree(s), 16, method="fast")  # the set as a single tree
         torch.cuda.synchronize()
         assert np.array_equal(vi.cpu().numpy(), oi), s
+
+
+@pytest.mark.parametrize("coord,sfc,periodic", [("f32", "morton", False), ("u32", "ph", True), ("f64", "ph", False)])
+def test_batch_features_equal_single_tree_features(coord, sfc, periodic):
+    """The learned bound's features of every leaf of a batch equal those of each set built as a
+    tree of its own."""
+    from fasttree_b200 import learned as L
+    ctx = ft.Context(coord, sfc, periodic=periodic)
+    x, y, z, off = make_sets(coord, [0, 300, 1, 2, 3, 17, 1000, 257, 2000])
+    b = ft.BatchedSets(ctx, len(x), len(off) - 1)
+    b.build(off, x, y, z)
+    for k in (1, 8, 32, 64):
+        f = b.bound_features(k).cpu().numpy()
+        for s in range(len(off) - 1):
+            a, e = int(off[s]), int(off[s + 1])
+            if e - a < 1:
+                continue
+            tree = ft.TreeSoA(ctx, e - a)
+            ft.build_bvh(ctx, ft.particles(x[a:e], y[a:e], z[a:e]), tree)
+            want = L.features(ctx, tree, k).cpu().numpy()
+            assert np.array_equal(f[a:e].view(np.uint32), want.view(np.uint32)), (k, s)
+
+
+@pytest.mark.parametrize("coord,sfc,periodic", [("f32", "morton", False), ("u32", "ph", True)])
+def test_learned_batched_query_is_exact_for_any_network(coord, sfc, periodic):
+    """ft_batch_self_knn_learned and ft_batch_build_knn_learned return ft_batch_self_knn's rows
+    for a trained, an untrained, a far-too-small and a far-too-large network; queries whose
+    bound proves too small rerun the walk without it, and only ties reach the replay."""
+    from fasttree_b200 import learned as L
+    from oracle import bound_oracle as BOR
+    ctx = ft.Context(coord, sfc, periodic=periodic)
+    sizes = [int(s) for s in datasets.batched_set_sizes(200, seed=14, median=2000.0)]
+    x, y, z, off = make_sets(coord, sizes, seed=31)
+    tx, ty, tz, toff = make_sets(coord, sizes[:120], seed=77)
+    N, k = len(x), 32
+    trained, _ = L.train_bound_batched(ctx, toff, tx, ty, tz, k, steps=300, batch=4096)
+    untrained = L.BoundModel(ctx, seed=3)
+    tiny, huge = L.BoundModel(ctx, seed=3), L.BoundModel(ctx, seed=3)
+    p = tiny.params
+    p[BOR.OFF_B3] = -60.0
+    tiny.params = p
+    p[BOR.OFF_B3] = 60.0
+    huge.params = p
+    b = ft.BatchedSets(ctx, N, len(sizes))
+    b.build(off, x, y, z)
+    pi, pd = b.self_knn(k, method="plain")
+    pi, pd = pi.clone(), pd.clone()
+    for name, model in (("trained", trained), ("untrained", untrained), ("tiny", tiny), ("huge", huge)):
+        li, ld = b.self_knn_learned(model, k, inflation=1.15)
+        b.check()
+        assert torch.equal(li, pi) and torch.equal(ld, pd), name
+        st = b.query_stats()
+        if name == "tiny":
+            assert st["bound_misses"] >= N - 10
+            assert st["replayed"] < 0.05 * N
+    # the same through one CUDA graph (build + learned query), replayed twice
+    dx, dy, dz = (torch.from_numpy(a).cuda() for a in (x, y, z))
+    doff = torch.from_numpy(off).cuda()
+    gi = torch.empty(N * k, dtype=torch.uint64, device="cuda")
+    gd = torch.empty(N * k, dtype=pd.dtype, device="cuda")
+    for _ in range(2):
+        gi.zero_()
+        b.build_knn_learned(trained, doff, dx, dy, dz, k, gi, gd, inflation=1.3)
+        b.check()
+        assert torch.equal(gi.view(N, k), pi) and torch.equal(gd.view(N, k), pd)
