@@ -70,6 +70,7 @@ def parse():
                    help="N > 1: one tree on every rank, its queries split into contiguous SFC ranges (strong "
                         "scaling); default: each rank its own point set (weak scaling)")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cfg5", action="store_true", help="skip the 50M-point section of the default run")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-sample", type=int, default=200_000)
     return p.parse_args()
@@ -404,6 +405,50 @@ def run_cfg2_extra(ctx, tree, x, y, z, n, stream):
                                                "self_knn_k32_on_refit_ms": q_refit,
                                                "self_knn_k32_on_rebuild_ms": q_fresh}
     del idx, dst, fresh
+    return out
+
+
+def run_cfg1(args, stream):
+    """Config 1, the reference's CPU-runnable case: 100K uniform float64 points (seed 1),
+    Morton keys, open box; build_bvh then self_knn_query k = 16, exclude_self.  Both methods,
+    every row against the oracle's, and the oracle port timed on this host at full size."""
+    import torch
+
+    import fasttree_b200 as ft
+    from fasttree_b200 import datasets
+    from oracle import oracle as O
+    n, k = 100_000, 16
+    x, y, z = datasets.uniform(n, seed=1)
+    ctx = ft.Context("f64", "morton")
+    dx, dy, dz = (torch.from_numpy(a).to(f"cuda:{ctx.device}") for a in (x, y, z))
+    tree = ft.TreeSoA(ctx, n)
+    p = ft.particles(dx, dy, dz)
+    build_ms = _timed(stream, lambda: ft.build_bvh(ctx, p, tree), 10, warmup=3)
+    rows = {}
+    out = {"workload": "cfg1: 100K uniform float64 (seed 1), Morton, open, k=16", "n_points": n, "k": k,
+           "build_ms": build_ms}
+    for name in ("fast", "plain"):
+        bi = torch.empty(n * k, dtype=torch.uint64, device=dx.device)
+        bd = torch.empty(n * k, dtype=torch.float64, device=dx.device)
+        ms = _timed(stream, lambda: ft.self_knn_query(ctx, tree, k, bi, bd, max_k=32, method=name), 20, warmup=3)
+        out[name] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s"}
+        if name == "fast":
+            out[name]["replayed"] = ctx.query_stats()["replayed"]
+        rows[name] = (bi, bd)
+    nthreads = O.set_threads(os.cpu_count() or 1)
+    opts = O.Options(O.F64, O.MORTON)
+    t0 = time.perf_counter()
+    ot = O.build_bvh(opts, x, y, z)
+    cpu_build = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oi, od = O.self_knn(opts, ot, k, True)
+    cpu_q = time.perf_counter() - t0
+    gi, gd = (a.view(n, k).cpu().numpy() for a in rows["fast"])
+    out["bit_exact"] = {"fast_vs_plain": rows_equal(*rows["fast"], *rows["plain"]),
+                        "oracle_all_rows": bool(np.array_equal(gi, oi) and
+                                                np.array_equal(gd.view(np.uint64), od.view(np.uint64)))}
+    out["cpu_baseline"] = {"value": n / cpu_q, "unit": "queries/s", "cores": nthreads, "kind": "port",
+                           "sample": "all 100K queries (full size)", "build_ms": cpu_build * 1e3}
     return out
 
 
@@ -865,12 +910,17 @@ def run_ours(args):
         knn_ext = run_knn_external(args, stream)
         extra = run_cfg2_extra(ctx, tree, x, y, z, n, stream)
 
-    batched = None
+    batched = cfg1 = cfg5 = None
     if world == 1 and not args.no_batched and args.workload == "cfg2":
-        del idx, dst
+        del idx, dst, headline_rows
         torch.cuda.empty_cache()
         batched = run_batched(args, dev, stream, 3, 2)
         torch.cuda.empty_cache()
+        cfg1 = run_cfg1(args, stream)
+        torch.cuda.empty_cache()
+        if not args.no_cfg5:
+            cfg5 = run_cfg5(argparse.Namespace(**{**vars(args), "n": 0}), stream)
+            torch.cuda.empty_cache()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -896,7 +946,8 @@ def run_ours(args):
                           "parallelism": f"query shards x{world}" if shard else f"replicas x{world}",
                           "l2": "inputs larger than L2: tree records + boxes ~2.3 GB, output 5.1 GB"},
                "plain": plain, "other_k_and_range": extra, "batched": batched, "learned": learned,
-               "knn_query": knn_ext, "build_ms": build_ms, "tree_height": height, "query_stats": stats,
+               "knn_query": knn_ext, "cfg1": cfg1, "cfg5": cfg5,
+               "build_ms": build_ms, "tree_height": height, "query_stats": stats,
                "bit_exact": bit_exact,
                "e2e": e2e, "gpu_launches": args.steps * (2 if method == 1 else 1),
                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
