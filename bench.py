@@ -71,6 +71,8 @@ def parse():
                         "scaling); default: each rank its own point set (weak scaling)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cfg5", action="store_true", help="skip the 50M-point section of the default run")
+    p.add_argument("--no-tune", action="store_true",
+                   help="skip the autotuner (build tile, walk variant / window / block shape per shape)")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-sample", type=int, default=200_000)
     return p.parse_args()
@@ -127,6 +129,10 @@ def run_batched(args, dev, stream, timed_steps, warmup):
         torch.cuda.synchronize()
         return g0.elapsed_time(g1) / steps
 
+    tuning = None
+    if not getattr(args, "no_tune", False):  # the walk's launch for this batch shape, before timing
+        b.build(off, x, y, z)
+        tuning = b.tune(k)
     graph_ms = timed(lambda: b.build_knn(off, x, y, z, k, idx, dst, method="fast"), timed_steps)
     b.check()
     stats = b.query_stats()
@@ -148,7 +154,7 @@ def run_batched(args, dev, stream, timed_steps, warmup):
         return {"workload": w["name"], "n_sets": S, "n_points": N, "k": k,
                 "graph_build_plus_query_ms": graph_ms, "value": N / (graph_ms / 1e3), "unit": "queries/s",
                 "build_ms": build_ms, "query_fast_ms": fast_ms, "query_plain_ms": plain_ms,
-                "replayed": stats["replayed"], "bit_exact": bit_exact, "learned": learned}
+                "replayed": stats["replayed"], "bit_exact": bit_exact, "learned": learned, "tuning": tuning}
     tree = ft.TreeSoA(ctx, int(np.diff(offs).max()))
     li = torch.empty(int(np.diff(offs).max()) * k, dtype=torch.uint64, device=dev)
     ld = torch.empty_like(li, dtype=torch.float64)
@@ -168,7 +174,7 @@ def run_batched(args, dev, stream, timed_steps, warmup):
             "build_ms": build_ms, "query_fast_ms": fast_ms, "query_plain_ms": plain_ms,
             "query_fast_qps": N / (fast_ms / 1e3), "query_plain_qps": N / (plain_ms / 1e3),
             "per_set_loop_ms": loop_ms, "per_set_loop_qps": N / (loop_ms / 1e3),
-            "replayed": stats["replayed"], "bit_exact": bit_exact, "learned": learned,
+            "replayed": stats["replayed"], "bit_exact": bit_exact, "learned": learned, "tuning": tuning,
             "note": "graph = ft_batch_build_knn (build + fast self-kNN, one CUDA graph); per-set loop = "
                     "build_bvh + self_knn_query(method='fast') per set through the single-tree API (wall clock)"}
 
@@ -343,7 +349,7 @@ def _timed(stream, fn, steps, warmup=1):
     return e0.elapsed_time(e1) / steps
 
 
-def run_cfg2_extra(ctx, tree, x, y, z, n, stream):
+def run_cfg2_extra(args, ctx, tree, x, y, z, n, stream):
     """The rest of the clustered workload on its resident tree: self-kNN at k=1 (register heap)
     and k=64 (shared-memory heap), fast and plain, range_query on all N points with
     r_min = 0, r_max = 2e-3 of the box (2e-3 * 2^40 units), 512 results per query, and a
@@ -357,6 +363,8 @@ def run_cfg2_extra(ctx, tree, x, y, z, n, stream):
         bufs = {m: (torch.empty(n * k2, dtype=torch.uint64, device=dev),
                     torch.empty(n * k2, dtype=ft.dist_torch_dtype(ctx.coord), device=dev)) for m in ("fast", "plain")}
         row = {}
+        if not getattr(args, "no_tune", False):
+            row["tuning"] = ft.tune_self_knn(ctx, tree, k2)
         for name, steps in (("fast", 3), ("plain", 2)):
             bi, bd = bufs[name]
             ms = _timed(stream, lambda: ft.self_knn_query(ctx, tree, k2, bi, bd, max_k=mk, method=name), steps)
@@ -423,10 +431,13 @@ def run_cfg1(args, stream):
     dx, dy, dz = (torch.from_numpy(a).to(f"cuda:{ctx.device}") for a in (x, y, z))
     tree = ft.TreeSoA(ctx, n)
     p = ft.particles(dx, dy, dz)
+    tuning = None
+    if not getattr(args, "no_tune", False):
+        tuning = {"build": ft.tune_build(ctx, p, tree), "self_knn": ft.tune_self_knn(ctx, tree, k)}
     build_ms = _timed(stream, lambda: ft.build_bvh(ctx, p, tree), 10, warmup=3)
     rows = {}
     out = {"workload": "cfg1: 100K uniform float64 (seed 1), Morton, open, k=16", "n_points": n, "k": k,
-           "build_ms": build_ms}
+           "build_ms": build_ms, "tuning": tuning}
     for name in ("fast", "plain"):
         bi = torch.empty(n * k, dtype=torch.uint64, device=dx.device)
         bd = torch.empty(n * k, dtype=torch.float64, device=dx.device)
@@ -471,11 +482,14 @@ def run_cfg5(args, stream):
     del x, y, z
     tree = ft.TreeSoA(ctx, n)
     p = ft.particles(dx, dy, dz)
+    tuning = None
+    if not getattr(args, "no_tune", False):
+        tuning = {"build": ft.tune_build(ctx, p, tree), "self_knn": ft.tune_self_knn(ctx, tree, k)}
     build_ms = _timed(stream, lambda: ft.build_bvh(ctx, p, tree), 2)
     idx = torch.empty(n * k, dtype=torch.uint64, device=dev)
     dst = torch.empty(n * k, dtype=torch.uint64, device=dev)
     out = {"workload": f"cfg5: {n / 1e6:g}M clustered uint64 (100,000 spheres, seed 5), Peano-Hilbert, periodic, k=64",
-           "n_points": n, "gen_s": gen_s, "build_ms": build_ms, "tree_height": tree.height(),
+           "n_points": n, "gen_s": gen_s, "build_ms": build_ms, "tree_height": tree.height(), "tuning": tuning,
            "output_bytes": 2 * idx.numel() * 8}
     ms = _timed(stream, lambda: ft.self_knn_query(ctx, tree, k, idx, dst, max_k=k, method="plain"), 1)
     out["plain"] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s"}
@@ -711,6 +725,16 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    # ---- autotuner: the build's sort tile and the walk's launch for this shape, chosen once
+    # before any timing (each candidate is checked to return the same rows) ----
+    tuning = None
+    if not args.no_tune:
+        t0 = time.perf_counter()
+        tuning = {"build": ft.tune_build(ctx, p, tree)}
+        if args.method == "fast" and k <= 64:
+            tuning["self_knn"] = ft.tune_self_knn(ctx, tree, k)
+        tuning["tune_s"] = time.perf_counter() - t0
+
     # ---- build_bvh timing ----
     for _ in range(args.warmup):
         ft.build_bvh(ctx, p, tree)
@@ -908,7 +932,7 @@ def run_ours(args):
         fast_visits = results[1][2]["visits"] / n if 1 in results else None
         learned = run_learned(args, ctx, tree, n, k, stream, fast_visits, headline_rows)
         knn_ext = run_knn_external(args, stream)
-        extra = run_cfg2_extra(ctx, tree, x, y, z, n, stream)
+        extra = run_cfg2_extra(args, ctx, tree, x, y, z, n, stream)
 
     batched = cfg1 = cfg5 = None
     if world == 1 and not args.no_batched and args.workload == "cfg2":
@@ -948,7 +972,7 @@ def run_ours(args):
                "plain": plain, "other_k_and_range": extra, "batched": batched, "learned": learned,
                "knn_query": knn_ext, "cfg1": cfg1, "cfg5": cfg5,
                "build_ms": build_ms, "tree_height": height, "query_stats": stats,
-               "bit_exact": bit_exact,
+               "bit_exact": bit_exact, "tuning": tuning,
                "e2e": e2e, "gpu_launches": args.steps * (2 if method == 1 else 1),
                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(out), flush=True)

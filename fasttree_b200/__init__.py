@@ -8,7 +8,7 @@ there is no CPU fallback.
 from .capi import F32, F64, U32, U64, MORTON, PEANO_HILBERT, FastTreeError  # noqa: F401
 from .hlbvh import (BatchedSets, BoundingBox, Context, TreePool, TreeSoA, build_bvh, build_tree,  # noqa: F401
                     compute_bbox, dist_torch_dtype, import_tree, knn_query, load_tree, particles, range_query,
-                    refit_bvh,
-                    self_knn_query, self_knn_query_bounded, self_knn_query_subset, sfc_encode)
+                    refit_bvh, self_knn_query, self_knn_query_bounded, self_knn_query_subset, sfc_encode,
+                    tune_build, tune_reset, tune_self_knn)
 
 __version__ = "0.1.0"

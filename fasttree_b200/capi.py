@@ -18,13 +18,14 @@ MORTON, PEANO_HILBERT = 0, 1
 # Every entry point declared in include/fasttree_b200.h.
 EXPORTED = (
     "ft_context_create", "ft_context_destroy", "ft_last_error", "ft_version", "ft_get_query_stats",
-    "ft_get_replayed_queries", "ft_check_device_status",
+    "ft_check_device_status",
     "ft_tree_create", "ft_tree_ensure", "ft_tree_destroy", "ft_compute_bbox", "ft_sfc_encode",
     "ft_build_bvh", "ft_build_tree", "ft_refit_bvh", "ft_tree_export", "ft_tree_import", "ft_self_knn", "ft_knn", "ft_range", "ft_tree_height",
     "ft_self_knn_noalloc", "ft_self_knn_bounded",
     "ft_batch_create", "ft_batch_destroy", "ft_batch_build", "ft_batch_self_knn", "ft_batch_build_knn",
     "ft_batch_tree", "ft_batch_set_info", "ft_batch_query_stats", "ft_batch_self_knn_learned",
-    "ft_batch_build_knn_learned", "ft_batch_bound_features",
+    "ft_batch_build_knn_learned", "ft_batch_bound_features", "ft_get_replayed_queries",
+    "ft_tune_self_knn", "ft_tune_batch_self_knn", "ft_tune_build", "ft_tune_reset",
     "ft_bound_model_create", "ft_bound_model_destroy", "ft_bound_model_get_params", "ft_bound_model_set_params",
     "ft_bound_model_set_norm", "ft_bound_features", "ft_bound_targets", "ft_bound_model_gradient",
     "ft_bound_model_fit", "ft_bound_model_predict", "ft_self_knn_learned", "ft_bound_features_points",
@@ -52,6 +53,15 @@ class FtQueryOptions(ctypes.Structure):
 
 class FtQueryStats(ctypes.Structure):
     _fields_ = [("queries", ctypes.c_int64), ("replayed", ctypes.c_int64), ("reserved", ctypes.c_int64 * 6)]
+
+
+class FtTuneResult(ctypes.Structure):
+    _fields_ = [("walk_variant", ctypes.c_int32), ("half_window", ctypes.c_int32), ("block_threads", ctypes.c_int32),
+                ("sort_items", ctypes.c_int32), ("candidates", ctypes.c_int32), ("best_ms", ctypes.c_float),
+                ("default_ms", ctypes.c_float), ("reserved", ctypes.c_int32 * 9)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
 
 
 class FastTreeError(RuntimeError):
@@ -94,6 +104,10 @@ _SIGS = {
                            ctypes.POINTER(FtQueryOptions), _st],
     "ft_batch_tree": [_vp, _vp, _sz, ctypes.POINTER(FtTree), _st],
     "ft_batch_bound_features": [_vp, _vp, _i, _vp, _st],
+    "ft_tune_self_knn": [_vp, ctypes.POINTER(FtTree), _i, _i, ctypes.POINTER(FtTuneResult), _st],
+    "ft_tune_batch_self_knn": [_vp, _vp, _i, _i, ctypes.POINTER(FtTuneResult), _st],
+    "ft_tune_build": [_vp, _vp, _vp, _vp, _sz, ctypes.POINTER(FtTree), ctypes.POINTER(FtTuneResult), _st],
+    "ft_tune_reset": [_vp],
     "ft_batch_self_knn_learned": [_vp, _vp, _vp, _i, _i, ctypes.c_float, _vp, _vp, ctypes.POINTER(FtQueryOptions),
                                   _st],
     "ft_batch_build_knn_learned": [_vp, _vp, _vp, ctypes.c_float, _vp, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _i, _i,

@@ -265,7 +265,8 @@ __global__ void __launch_bounds__(256)
     batch_refit_kernel(const long long *__restrict__ off, const long long *__restrict__ node_off,
                        const long long *__restrict__ rec_off, int S, long long N, const int32_t *__restrict__ left,
                        const int32_t *__restrict__ right, const int32_t *__restrict__ parent, T *mnx, T *mxx, T *mny,
-                       T *mxy, T *mnz, T *mxz, NodeRec<T> *recs, uint8_t *height, int32_t *counters) {
+                       T *mxy, T *mnz, T *mxz, NodeRec<T> *recs, uint8_t *height, int32_t *counters,
+                       const int32_t *__restrict__ leaves) {
     for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < N; j += (long long)gridDim.x * blockDim.x) {
         const int       s = find_set(off, S, j);
         const int       n = (int)(off[s + 1] - off[s]);
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(256)
         const long long no = node_off[s], ro = rec_off[s];
         T *const soa[6] = {mnx + no, mxx + no, mny + no, mxy + no, mnz + no, mxz + no};
         refit_leaf<T>((int)(j - off[s]), n, left + ro, right + ro, parent + no, soa, recs + ro, height + ro,
-                      counters + ro);
+                      counters + ro, leaves + ro);
     }
 }
 
@@ -517,7 +518,7 @@ static void batch_build_typed(Context &ctx, BatchImpl &b, const long long *in_of
     FT_CUDA(cudaMemsetAsync(s.counters, 0, (size_t)N * sizeof(int32_t), st));
     batch_refit_kernel<T><<<gK, 256, 0, st>>>(b.off, b.node_off, b.rec_off, S, N, t.left_child, t.right_child,
                                               t.parent, mnx, mxx, mny, mxy, mnz, mxz, (NodeRec<T> *)s.recs, s.height,
-                                              s.counters);
+                                              s.counters, s.leafcount);
     batch_collapse_kernel<T><<<gK, 256, 0, st>>>(b.off, b.node_off, b.rec_off, S, N, t.left_child, t.right_child,
                                                  mnx, mxx, mny, mxy, mnz, mxz, (WideRec<T> *)s.wide);
     batch_heights_kernel<<<grid_of((size_t)S, 256, sm * 4), 256, 0, st>>>(b.off, b.rec_off, S, s.height,
@@ -693,6 +694,11 @@ void batch_set_info(Context &ctx, BatchImpl &b, void *bbox_out, uint8_t *height_
     if (bbox_out) FT_CUDA(cudaMemcpyAsync(bbox_out, b.bbox, 6 * b.S * cb, cudaMemcpyDeviceToHost, st));
     if (height_out) FT_CUDA(cudaMemcpyAsync(height_out, b.set_height, b.S, cudaMemcpyDeviceToHost, st));
     FT_CUDA(cudaStreamSynchronize(st));
+}
+
+void batch_tune(Context &ctx, BatchImpl &b, int k, bool excl, ft_tune_result *out, cudaStream_t st) {
+    if (!b.built) fail(FT_ERR_INVALID_ARGUMENT, "the batch has not been built");
+    tune_batch_self_knn(ctx, b.all, batch_dev(b), b.N, k, excl, b.rr, b.rw, b.counters, out, st);
 }
 
 void batch_stats(BatchImpl &b, ft_query_stats &out) {

@@ -148,11 +148,15 @@ static constexpr int kTicketWords = 64;
 static constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kFlagMask = 3u << 30,
                           kCountMask = (1u << 30) - 1u;
 
-template <int W> struct SortCfg {
-    static constexpr int items = (W == 1) ? 16 : 12;
+// A onesweep tile: 256 threads x ITEMS keys (ITEMS 0: the default for the key width, 16 for
+// one-word keys and 12 for two-word keys).  The build's sort takes the tile the autotuner
+// chose for the shape (sort_items); every tile size gives the same order.
+template <int W, int ITEMS = 0> struct SortCfg {
+    static constexpr int items = ITEMS ? ITEMS : (W == 1) ? 16 : 12;
     static constexpr int tile  = kSortThreads * items;
     static constexpr size_t smem = (size_t)tile * (8 * W + 4) + (size_t)kSortWarps * 256 * 4;
 };
+static constexpr int kSortItemsMin = 8; // the smallest tile sizes the look-back scratch
 
 // Digit histograms of digit positions [d0, d0 + ND) (ND = 8 * W by default: every digit).
 // enable: null, or a device word whose 0 makes the launch a no-op.
@@ -223,14 +227,14 @@ FT_D void st_volatile(uint32_t *p, uint32_t v) { asm volatile("st.volatile.globa
 //    fallback, which only runs when a long run of equal high words was found);
 //  * skip (null or a device word): 1 when one digit value holds every key -- the pass then
 //    copies its tiles unchanged, so the ping-pong order the host planned still holds.
-template <int W>
+template <int W, int IT = 0>
 __global__ void __launch_bounds__(kSortThreads, 1)
     onesweep_kernel(const unsigned long long *__restrict__ in_lo, const unsigned long long *__restrict__ in_hi,
                     const uint32_t *__restrict__ in_v, unsigned long long *__restrict__ out_lo,
                     unsigned long long *__restrict__ out_hi, uint32_t *__restrict__ out_v, size_t n, size_t num_tiles,
                     int word, int shift, const uint32_t *__restrict__ offsets, uint32_t *lookback,
                     uint32_t *tile_counter, const uint32_t *enable, const uint32_t *skip, uint32_t *status) {
-    using Cfg           = SortCfg<W>;
+    using Cfg           = SortCfg<W, IT>;
     constexpr int ITEMS = Cfg::items;
     constexpr int TILE  = Cfg::tile;
     if (enable && *enable == 0u) return; // grid-uniform
@@ -459,10 +463,10 @@ __global__ void __launch_bounds__(256) refit_kernel(int n, const int32_t *__rest
                                                     const int32_t *__restrict__ right,
                                                     const int32_t *__restrict__ parent, T *mnx, T *mxx, T *mny,
                                                     T *mxy, T *mnz, T *mxz, NodeRec<T> *recs, uint8_t *height,
-                                                    int32_t *counters) {
+                                                    int32_t *counters, const int32_t *__restrict__ leaves) {
     T *const soa[6] = {mnx, mxx, mny, mxy, mnz, mxz};
     for (int leaf = blockIdx.x * blockDim.x + threadIdx.x; leaf < n; leaf += gridDim.x * blockDim.x)
-        refit_leaf<T>(leaf, n, left, right, parent, soa, recs, height, counters);
+        refit_leaf<T>(leaf, n, left, right, parent, soa, recs, height, counters, leaves);
 }
 
 // 4-wide records of every internal node (collapse_node), after the refit.
@@ -506,8 +510,9 @@ void free_scratch(TreeImpl &s) {
     s.coord   = coord;
 }
 
-static size_t sort_tiles(size_t n, int W) {
-    size_t tile = (W == 1) ? SortCfg<1>::tile : SortCfg<2>::tile;
+static size_t sort_tiles(size_t n, int W) { // the most tiles any tile size makes
+    (void)W;
+    const size_t tile = (size_t)kSortThreads * kSortItemsMin;
     return (n + tile - 1) / tile;
 }
 
@@ -644,17 +649,17 @@ __global__ void __launch_bounds__(256) zero_if_kernel(uint32_t *p, size_t words,
 
 // Persistent grid of a onesweep pass: the CTAs resident at once (three per SM with the
 // tile's shared memory), never more than the tiles.
-template <int W> static unsigned sort_grid(size_t tiles) {
+template <int W, int IT = 0> static unsigned sort_grid(size_t tiles) {
     static int per_sm = 0, sms = 0;
     static std::once_flag once;
     std::call_once(once, [] {
         int dev = 0;
         if (cudaGetDevice(&dev) != cudaSuccess ||
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-            cudaFuncSetAttribute(onesweep_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)SortCfg<W>::smem) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel<W>, kSortThreads,
-                                                          SortCfg<W>::smem) != cudaSuccess) {
+            cudaFuncSetAttribute(onesweep_kernel<W, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SortCfg<W, IT>::smem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel<W, IT>, kSortThreads,
+                                                          SortCfg<W, IT>::smem) != cudaSuccess) {
             cudaGetLastError();
             per_sm = 1;
             sms    = 148;
@@ -671,12 +676,13 @@ template <int W> static unsigned sort_grid(size_t tiles) {
 // two-word sort from that order (histograms of the low word, then the eight low-word and the
 // eight high-word passes: an even number, so the host's ping-pong order is the same whether
 // they run or not).
-template <int W> static void sort_impl(TreeImpl &s, size_t n, cudaStream_t st) {
-    using Cfg            = SortCfg<W>;
+template <int W, int IT = 0> static void sort_impl(TreeImpl &s, size_t n, cudaStream_t st) {
+    using Cfg            = SortCfg<W, IT>;
     const int      D     = 8 * W;
     const size_t   tiles = (n + Cfg::tile - 1) / Cfg::tile;
-    const unsigned grid  = sort_grid<W>(tiles);
-    FT_CUDA(cudaFuncSetAttribute(onesweep_kernel<W>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::smem));
+    const unsigned grid  = sort_grid<W, IT>(tiles);
+    FT_CUDA(cudaFuncSetAttribute(onesweep_kernel<W, IT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Cfg::smem));
     FT_CUDA(cudaMemsetAsync(s.hist, 0, (16 * 256 + 16) * sizeof(uint32_t), st));
     FT_CUDA(cudaMemsetAsync(s.tile_counter, 0, kTicketWords * sizeof(uint32_t), st));
     uint32_t *skip_dev = s.hist + 16 * 256;
@@ -689,7 +695,7 @@ template <int W> static void sort_impl(TreeImpl &s, size_t n, cudaStream_t st) {
         FT_CUDA(cudaGetLastError());
     };
     auto pass = [&](int d, uint32_t *ticket, const uint32_t *enable) {
-        onesweep_kernel<W><<<grid, kSortThreads, Cfg::smem, st>>>(
+        onesweep_kernel<W, IT><<<grid, kSortThreads, Cfg::smem, st>>>(
             (const unsigned long long *)s.key_lo, (const unsigned long long *)s.key_hi, s.perm,
             (unsigned long long *)s.tmp_lo, (unsigned long long *)s.tmp_hi, s.tmp_perm, n, tiles, d >> 3,
             8 * (d & 7), s.hist + d * 256, s.lookback + (size_t)d * tiles * 256, ticket, enable, skip_dev + d,
@@ -759,10 +765,29 @@ void sort_pairs_fixed(TreeImpl &s, size_t n, int words, int ndigits, const int *
 
 size_t sort_lookback_words(size_t n, int words) { return 16 * sort_tiles(n, words) * 256; }
 
-static void sort_keys(const ft_options &o, TreeImpl &s, size_t n, cudaStream_t st) {
+// items: keys per thread of a onesweep tile (0: the default for the key width).
+static void sort_keys(const ft_options &o, TreeImpl &s, size_t n, cudaStream_t st, int items = 0) {
     if (n < 2) return;
-    if (key_words(o) == 1) sort_impl<1>(s, n, st);
-    else sort_impl<2>(s, n, st);
+    if (key_words(o) == 1) {
+        switch (items) {
+        case 8: sort_impl<1, 8>(s, n, st); break;
+        case 12: sort_impl<1, 12>(s, n, st); break;
+        case 20: sort_impl<1, 20>(s, n, st); break;
+        default: sort_impl<1>(s, n, st); break; // 16
+        }
+    } else {
+        switch (items) {
+        case 8: sort_impl<2, 8>(s, n, st); break;
+        case 16: sort_impl<2, 16>(s, n, st); break;
+        default: sort_impl<2>(s, n, st); break; // 12
+        }
+    }
+}
+
+const int *sort_item_choices(int words, int *count) {
+    static const int one[4] = {16, 8, 12, 20}, two[3] = {12, 8, 16}; // the default first
+    *count = words == 1 ? 4 : 3;
+    return words == 1 ? one : two;
 }
 
 template <class T> struct SoA {
@@ -790,7 +815,8 @@ static void topology_and_refit(const ft_options &o, ft_tree &t, TreeImpl &s, siz
     FT_CUDA(cudaMemsetAsync(s.counters, 0, (n - 1) * sizeof(int32_t), st));
     SoA<T> a(t);
     refit_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, t.parent, a.mnx, a.mxx, a.mny,
-                                            a.mxy, a.mnz, a.mxz, (NodeRec<T> *)s.recs, s.height, s.counters);
+                                            a.mxy, a.mnz, a.mxz, (NodeRec<T> *)s.recs, s.height, s.counters,
+                                            s.leafcount);
     collapse_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, a.mnx, a.mxx, a.mny, a.mxy,
                                                a.mnz, a.mxz, (WideRec<T> *)s.wide);
     FT_CUDA(cudaGetLastError());
@@ -799,7 +825,7 @@ static void topology_and_refit(const ft_options &o, ft_tree &t, TreeImpl &s, siz
 template <class T>
 static void build_bvh_typed(Context &ctx, ft_tree &t, const void *x, const void *y, const void *z, size_t n,
                             const uint32_t *id, const int8_t *ghost, const void *bbox_host, void *caller_keys,
-                            cudaStream_t st) {
+                            cudaStream_t st, int sort_items) {
     TreeImpl &s = *(TreeImpl *)t.impl;
     ensure_scratch(s, ctx.opts, n);
     // 1. bounding box.  Only the float encode reads it; integer encoding ignores it, so an
@@ -816,8 +842,12 @@ static void build_bvh_typed(Context &ctx, ft_tree &t, const void *x, const void 
     } else {
         encode(ctx.opts, x, y, z, n, s.bbox, s, st);
     }
-    // 3. sort (key, perm)
-    sort_keys(ctx.opts, s, n, st);
+    // 3. sort (key, perm), with the tile the autotuner chose for this shape
+    if (sort_items <= 0) {
+        auto it = ctx.tuned.find(tune_key(TUNE_BUILD, key_words(ctx.opts), n));
+        if (it != ctx.tuned.end()) sort_items = it->second.items;
+    }
+    sort_keys(ctx.opts, s, n, st, sort_items);
     if (caller_keys) {
         keys_to_ref_kernel<<<grid_for(n, 256), 256, 0, st>>>((const unsigned long long *)s.key_lo,
                                                               (const unsigned long long *)s.key_hi, n,
@@ -841,14 +871,16 @@ static void build_bvh_typed(Context &ctx, ft_tree &t, const void *x, const void 
 }
 
 void build_bvh(Context &ctx, ft_tree &t, const void *x, const void *y, const void *z, size_t n, const uint32_t *id,
-               const int8_t *ghost, const void *bbox_host, void *caller_keys, cudaStream_t st) {
+               const int8_t *ghost, const void *bbox_host, void *caller_keys, cudaStream_t st, int sort_items) {
     switch (ctx.opts.coord_type) {
-    case F32: build_bvh_typed<float>(ctx, t, x, y, z, n, id, ghost, bbox_host, caller_keys, st); break;
-    case F64: build_bvh_typed<double>(ctx, t, x, y, z, n, id, ghost, bbox_host, caller_keys, st); break;
-    case U32: build_bvh_typed<uint32_t>(ctx, t, x, y, z, n, id, ghost, bbox_host, caller_keys, st); break;
-    case U64: build_bvh_typed<unsigned long long>(ctx, t, x, y, z, n, id, ghost, bbox_host, caller_keys, st); break;
+    case F32: build_bvh_typed<float>(ctx, t, x, y, z, n, id, ghost, bbox_host, caller_keys, st, sort_items); break;
+    case F64: build_bvh_typed<double>(ctx, t, x, y, z, n, id, ghost, bbox_host, caller_keys, st, sort_items); break;
+    case U32: build_bvh_typed<uint32_t>(ctx, t, x, y, z, n, id, ghost, bbox_host, caller_keys, st, sort_items); break;
+    case U64: build_bvh_typed<unsigned long long>(ctx, t, x, y, z, n, id, ghost, bbox_host, caller_keys, st, sort_items); break;
     }
 }
+
+int key_words_of(const ft_options &o) { return key_words(o); }
 
 template <class T>
 static void build_tree_typed(Context &ctx, ft_tree &t, const void *keys_ref, const void *sx, const void *sy,
@@ -889,7 +921,8 @@ static void refit_typed(ft_tree &t, const void *x, const void *y, const void *z,
     const int blocks = grid_for(n, 256, 148 * 32);
     FT_CUDA(cudaMemsetAsync(s.counters, 0, (n - 1) * sizeof(int32_t), st));
     refit_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, t.parent, a.mnx, a.mxx, a.mny,
-                                            a.mxy, a.mnz, a.mxz, (NodeRec<T> *)s.recs, s.height, s.counters);
+                                            a.mxy, a.mnz, a.mxz, (NodeRec<T> *)s.recs, s.height, s.counters,
+                                            s.leafcount);
     collapse_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, a.mnx, a.mxx, a.mny, a.mxy,
                                                a.mnz, a.mxz, (WideRec<T> *)s.wide);
     FT_CUDA(cudaGetLastError());

@@ -246,7 +246,7 @@ FT_D int atomic_add_acq_rel(int32_t *p, int v) {
 template <class T>
 FT_D void refit_leaf(int leaf, int n, const int32_t *__restrict__ left, const int32_t *__restrict__ right,
                      const int32_t *__restrict__ parent, T *const *soa, NodeRec<T> *recs, uint8_t *height,
-                     int32_t *counters) {
+                     int32_t *counters, const int32_t *__restrict__ leaves) {
     int curr  = leaf + n - 1;
     int steps = 0;
     while (curr != 0 && ++steps < n) {
@@ -282,6 +282,9 @@ FT_D void refit_leaf(int leaf, int n, const int32_t *__restrict__ left, const in
         rec.r = r;
 #pragma unroll
         for (int d = 0; d < (int)(sizeof(rec.pad) / 4); ++d) rec.pad[d] = 0;
+        // leaf counts (the Karras ranges) and heights of both children
+        rec.pad[0] = (int32_t)rec_child_info(l >= n - 1 ? 1u : (uint32_t)leaves[l], (uint32_t)hl);
+        rec.pad[1] = (int32_t)rec_child_info(r >= n - 1 ? 1u : (uint32_t)leaves[r], (uint32_t)hr);
         recs[p] = rec;
         int h   = 1 + max(hl, hr);
         __stcg(height + p, (uint8_t)min(h, 255));

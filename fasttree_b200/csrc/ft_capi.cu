@@ -1164,6 +1164,64 @@ ft_status ft_batch_build_knn_learned(ft_context *ctx, ft_batch *batch, ft_bound_
     FT_API_END
 }
 
+// ---------------------------------------------------------------------------------------
+// Autotuner (ft_tune.cu)
+// ---------------------------------------------------------------------------------------
+ft_status ft_tune_self_knn(ft_context *ctx, const ft_tree *tree, int k, int exclude_self, ft_tune_result *out,
+                           ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree, "null argument");
+    DeviceGuard g(ctx->device);
+    ft::tune_self_knn(*ctx, *tree, k, exclude_self != 0, out, (cudaStream_t)stream);
+    check_device_status(ctx->status, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_tune_batch_self_knn(ft_context *ctx, ft_batch *batch, int k, int exclude_self, ft_tune_result *out,
+                                 ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && batch, "null argument");
+    DeviceGuard g(ctx->device);
+    ft::batch_tune(*ctx, *batch->impl, k, exclude_self != 0, out, (cudaStream_t)stream);
+    check_device_status(ctx->status, (cudaStream_t)stream);
+    FT_API_END
+}
+
+ft_status ft_tune_build(ft_context *ctx, const void *x, const void *y, const void *z, size_t n, ft_tree *tree,
+                        ft_tune_result *out, ft_stream_t stream) {
+    FT_API_BEGIN
+    need(ctx && tree, "null argument");
+    need_owned(tree);
+    need(x && y && z, "null coordinate array");
+    need(n >= 2, "the build autotuner needs 2+ points");
+    need(n <= (size_t)(INT_MAX / 2), "Particle count n exceeds maximum supported tree size (INT_MAX / 2).");
+    need(tree->capacity >= n, "tree capacity is smaller than the particle count");
+    DeviceGuard  g(ctx->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    {
+        const size_t cb = coord_bytes(ctx->opts.coord_type);
+        Staged       sx, sy, sz;
+        sx.init(x, n * cb, true, false, st);
+        sy.init(y, n * cb, true, false, st);
+        sz.init(z, n * cb, true, false, st);
+        tree->num_leaves   = n;
+        tree->num_internal = n - 1;
+        ft::tune_build(*ctx, *tree, sx.dev, sy.dev, sz.dev, n, out, st);
+        check_status_word(*(TreeImpl *)tree->impl, st);
+    }
+    // leave the tree built the ordinary way (with the chosen tile)
+    const ft_status s2 = ft_build_bvh(ctx, x, y, z, n, nullptr, nullptr, nullptr, nullptr, tree, stream);
+    if (s2 != FT_OK) return s2;
+    FT_API_END
+}
+
+ft_status ft_tune_reset(ft_context *ctx) {
+    FT_API_BEGIN
+    need(ctx != nullptr, "null context");
+    ctx->tuned.clear();
+    FT_API_END
+}
+
 ft_status ft_batch_tree(ft_context *ctx, ft_batch *batch, size_t set, ft_tree *out, ft_stream_t stream) {
     FT_API_BEGIN
     need(ctx && batch && out, "null argument");

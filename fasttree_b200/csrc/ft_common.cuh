@@ -167,14 +167,24 @@ template <class T> struct Metric {
 // Internal node record used by the traversals: both child boxes and child indices in one
 // 16-word line (64 B for 4-byte coordinates, 128 B for 8-byte ones), fetched with 16-byte
 // vector loads.  Words 0-5: left box (minx,maxx,miny,maxy,minz,maxz); 6-11: right box;
-// then the child indices (Karras encoding: index >= n-1 is a leaf slot).
+// then the child indices (Karras encoding: index >= n-1 is a leaf slot), then one word per
+// child with its leaf count and subtree height (rec_child_info), read in the same vector load.
 // ---------------------------------------------------------------------------------------
 template <class T> struct alignas(16 * sizeof(T)) NodeRec {
     T       lb[6];
     T       rb[6];
     int32_t l, r;
-    int32_t pad[(16 * sizeof(T) - 12 * sizeof(T) - 8) / 4];
+    int32_t pad[(16 * sizeof(T) - 12 * sizeof(T) - 8) / 4]; // [0] left, [1] right: rec_child_info
 };
+
+// A child's leaf count (25 bits, saturated) and subtree height (7 bits, saturated) in one
+// word; saturated values are never used as exact (the range walk descends instead).
+static constexpr uint32_t kInfoCountMax = (1u << 25) - 1u, kInfoHeightMax = 127u;
+FT_HD uint32_t rec_child_info(uint32_t leaves, uint32_t height) {
+    return (leaves < kInfoCountMax ? leaves : kInfoCountMax) | ((height < kInfoHeightMax ? height : kInfoHeightMax) << 25);
+}
+FT_HD uint32_t info_leaves(uint32_t w) { return w & kInfoCountMax; }
+FT_HD uint32_t info_height(uint32_t w) { return w >> 25; }
 static_assert(sizeof(NodeRec<float>) == 64, "record size");
 static_assert(sizeof(NodeRec<double>) == 128, "record size");
 
@@ -201,6 +211,42 @@ template <class T> FT_D void load_wide(const WideRec<T> *w, int node, T b[4][6],
     const int32_t *ci = reinterpret_cast<const int32_t *>(f + 24);
 #pragma unroll
     for (int i = 0; i < 4; ++i) c[i] = ci[i];
+}
+
+// load_rec plus the two children's info words (rec_child_info).
+template <class T>
+FT_D void load_rec_info(const NodeRec<T> *recs, int node, T lb[6], T rb[6], int &l, int &r, uint32_t &il,
+                        uint32_t &ir) {
+    const uint4 *p = reinterpret_cast<const uint4 *>(recs + node);
+    if constexpr (sizeof(T) == 8) {
+        uint4 w[7];
+#pragma unroll
+        for (int i = 0; i < 7; ++i) w[i] = __ldg(p + i);
+        const T *v = reinterpret_cast<const T *>(w);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            lb[i] = v[i];
+            rb[i] = v[6 + i];
+        }
+        l  = (int)w[6].x;
+        r  = (int)w[6].y;
+        il = w[6].z;
+        ir = w[6].w;
+    } else {
+        uint4 w[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) w[i] = __ldg(p + i);
+        const T *v = reinterpret_cast<const T *>(w);
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            lb[i] = v[i];
+            rb[i] = v[6 + i];
+        }
+        l  = (int)w[3].x;
+        r  = (int)w[3].y;
+        il = w[3].z;
+        ir = w[3].w;
+    }
 }
 
 template <class T> FT_D void load_rec(const NodeRec<T> *recs, int node, T lb[6], T rb[6], int &l, int &r) {

@@ -165,13 +165,15 @@ template <class T> FT_D T coord_bottom() {
 // at an internal node (height >= 63 - turns); that slack never grows along a path and a far
 // turn spends one, so trees of height <= 62 need no search and taller ones are searched near
 // their tallest paths only.  Bounded: a search that runs long answers true.
+// stk: scratch of kGuardStack entries (the walk's own stack, free by then).
+static constexpr int kGuardStack = 80;
 template <class T, int PER>
-FT_D bool stack_guard_reaches(const TreeDev<T> &t, T px, T py, T pz, typename Coord<T>::dist_t dk) {
+FT_D bool stack_guard_reaches(const TreeDev<T> &t, T px, T py, T pz, typename Coord<T>::dist_t dk,
+                              unsigned long long *stk) {
     using D = typename Coord<T>::dist_t;
     const int n = t.n;
     if (n < 2 || (int)t.height[0] < 63) return false;
-    constexpr int      kCap = 80;
-    unsigned long long stk[kCap]; // (node << 8) | nearer-child turns from the root
+    constexpr int kCap = kGuardStack; // entries: (node << 8) | nearer-child turns from the root
     int                sp     = 1;
     int                budget = 4096;
     stk[0]                    = 0ull;
@@ -200,6 +202,20 @@ FT_D bool stack_guard_reaches(const TreeDev<T> &t, T px, T py, T pz, typename Co
         }
     }
     return false;
+}
+
+// Slot of this lane's entry in a list whose length is *count, for the lanes with `take`: one
+// atomic per warp, and a warp's entries stay together in lane order (so a later launch over
+// the list takes neighbouring queries in one warp).  Every lane of the warp must call it.
+FT_D uint32_t warp_append(uint32_t *count, bool take, int lane) {
+    const unsigned m    = __ballot_sync(0xffffffffu, take);
+    uint32_t       base = 0;
+    if (m) {
+        const int leader = __ffs(m) - 1;
+        if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, leader);
+    }
+    return base + (uint32_t)__popc(m & ((1u << lane) - 1u));
 }
 
 template <class T> FT_D T warp_min_t(T v) {
@@ -254,6 +270,9 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
     D       *hd  = reinterpret_cast<D *>(smem);
     int32_t *hix = reinterpret_cast<int32_t *>(hd + k * kFastThreads); // heaps sized for k (<= KC)
     __shared__ int32_t s_node[kFastWarps][kFastStack];
+    // the 4-wide walk's per-lane stack, then the stack-guard test's scratch
+    unsigned long long lane_stack[96];
+    static_assert(sizeof(lane_stack) / sizeof(lane_stack[0]) >= kGuardStack, "guard scratch");
 
     const int      tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const unsigned FULL = 0xffffffffu;
@@ -639,12 +658,12 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
         // (half the dependent steps of the binary walk); leaves go to the heap, the nearest
         // needed internal node is walked next and the others are stacked farthest first.  A
         // full stack hands the query to the replay instead of dropping anything.
-        constexpr int kWideStack = 96;
+        constexpr int kWideStack = sizeof(lane_stack) / sizeof(lane_stack[0]);
         const int     ws0 = w0 + n - 1, ws1 = w1 + n - 1; // the seeding window in slot numbers
         // stack entries: node index in the low word, a float lower bound of its distance in the
         // high word (one 8-byte local-memory access per push or pop); thr_up is the pruning
         // threshold rounded up, so a popped node is dropped only when it is surely beyond it
-        unsigned long long st[kWideStack];
+        unsigned long long *st = lane_stack;
         float              thr_up = stack_key_up<D>(thr);
         D                  thr_seen = thr;
         int           cur  = 0;
@@ -833,18 +852,20 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
     // points lie inside it.  With a miss list the query goes to the next launch (the walk
     // without a bound); otherwise the reference traversal reruns it.
     const bool bound_miss = active && ((count >= k && hmax > B) || (count < k && B != dist_heap_max<D>()));
-    if (bound_miss && miss.rows) {
-        const uint32_t at = atomicAdd(miss.count, 1u);
-        if (!ext && !bt.off) miss.ranks[at] = rank;
-        miss.rows[at] = q;
-        active        = false;
+    if (miss.rows) {
+        const uint32_t at = warp_append(miss.count, bound_miss, lane);
+        if (bound_miss) {
+            if (!ext && !bt.off) miss.ranks[at] = rank;
+            miss.rows[at] = q;
+            active        = false;
+        }
     }
     if (active) {
         if (bound_miss) flag = true;
         // trees of height >= 63: the reference's stack guard may drop part of this query's
         // neighbourhood (fewer than k points found: conservatively so)
         if (!flag && n >= 2 && (int)t.height[0] >= 63 &&
-            (count < k || stack_guard_reaches<T, PER>(t, px, py, pz, hmax)))
+            (count < k || stack_guard_reaches<T, PER>(t, px, py, pz, hmax, lane_stack)))
             flag = true;
         for (int hs = count; hs > 1; --hs) {
             D       last  = HD(hs - 1);
@@ -892,8 +913,9 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             }
         }
     }
-    if ((active && flag) || force_replay) {
-        uint32_t at = atomicAdd(replay_count, 1u);
+    const bool to_replay = (active && flag) || force_replay;
+    const uint32_t at    = warp_append(replay_count, to_replay, lane);
+    if (to_replay) {
         if (!ext) replay_ranks[at] = rank;
         replay_rows[at] = q;
     }
@@ -981,10 +1003,11 @@ static void launch_fast_view(const TreeDev<T> &tv, const BatchDev &bt, int met, 
                              int num, int k, int half, bool excl, const void *bound, uint64_t *idx, void *dist,
                              int32_t *rr, int32_t *rw, uint32_t *rc, uint32_t *status, int variant,
                              unsigned long long *visits, cudaStream_t st, const ExtQueries &eq = {},
-                             const ListArgs &la = {}) {
+                             const ListArgs &la = {}, int kc = 0) {
     met_dispatch<T>(met, [&](auto M) {
         constexpr int PER = decltype(M)::value;
-        if (k <= 32)
+        // heap template: 32 (two-warp blocks) for k <= 32 unless one-warp blocks were chosen
+        if (k <= 32 && kc != 64)
             launch_fast_t<T, PER, 32>(tv, bt, eq, leaf_ids, num, k, half, excl, ro, bound, idx, dist, rr, rw, rc,
                                       status, variant, visits, st, la);
         else
@@ -997,21 +1020,21 @@ template <class T>
 static void launch_fast(const ft_options &o, const ft_tree &tr, const int32_t *leaf_ids, int num, int k, int half,
                         bool excl, const void *bound, uint64_t *idx, void *dist, int32_t *rr, int32_t *rw,
                         uint32_t *rc, uint32_t *status, int variant, unsigned long long *visits, cudaStream_t st,
-                        const ExtQueries &eq = {}, const ListArgs &la = {}) {
+                        const ExtQueries &eq = {}, const ListArgs &la = {}, int kc = 0) {
     launch_fast_view<T>(tree_view<T>(tr), BatchDev{}, metric_mode<T>(o, tr), o.return_orig_indices != 0, leaf_ids,
-                        num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la);
+                        num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la, kc);
 }
 
 // Every coordinate type: launch_fast<T> for the context's type.
 static void launch_fast_any(const ft_options &o, const ft_tree &tr, const int32_t *leaf_ids, int num, int k, int half,
                             bool excl, const void *bound, uint64_t *idx, void *dist, int32_t *rr, int32_t *rw,
                             uint32_t *rc, uint32_t *status, int variant, unsigned long long *visits, cudaStream_t st,
-                            const ExtQueries &eq = {}, const ListArgs &la = {}) {
+                            const ExtQueries &eq = {}, const ListArgs &la = {}, int kc = 0) {
     switch (o.coord_type) {
-    case F32: launch_fast<float>(o, tr, leaf_ids, num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la); break;
-    case F64: launch_fast<double>(o, tr, leaf_ids, num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la); break;
-    case U32: launch_fast<uint32_t>(o, tr, leaf_ids, num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la); break;
-    case U64: launch_fast<unsigned long long>(o, tr, leaf_ids, num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la); break;
+    case F32: launch_fast<float>(o, tr, leaf_ids, num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la, kc); break;
+    case F64: launch_fast<double>(o, tr, leaf_ids, num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la, kc); break;
+    case U32: launch_fast<uint32_t>(o, tr, leaf_ids, num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la, kc); break;
+    case U64: launch_fast<unsigned long long>(o, tr, leaf_ids, num, k, half, excl, bound, idx, dist, rr, rw, rc, status, variant, visits, st, eq, la, kc); break;
     }
 }
 
@@ -1083,7 +1106,7 @@ static void ensure_miss(Context &ctx, size_t num) {
 // visits, [4] bound misses, [6..7] visits of the second launch.
 static void fast_walk_and_replay(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k,
                                  bool excl, uint64_t *idx, void *dist, const void *bound, int half_window,
-                                 int variant, cudaStream_t st, const ExtQueries &eq = {}) {
+                                 int variant, cudaStream_t st, const ExtQueries &eq = {}, int kc = 0) {
     uint32_t           *rc     = ctx.status + 1;
     unsigned long long *visits = (unsigned long long *)(ctx.status + 2);
     uint32_t           *mc     = ctx.status + 4;
@@ -1094,25 +1117,34 @@ static void fast_walk_and_replay(Context &ctx, const ft_tree &tr, const int32_t 
         la.miss = MissList{ctx.miss_ranks, ctx.miss_rows, mc};
     }
     launch_fast_any(ctx.opts, tr, leaf_ids, (int)num, k, half_window, excl, bound, idx, dist, ctx.replay_ranks,
-                    ctx.replay_rows, rc, ctx.status, variant, visits, st, eq, la);
+                    ctx.replay_rows, rc, ctx.status, variant, visits, st, eq, la, kc);
     if (bound) {
         ListArgs again;
         again.lst = QueryList{ctx.miss_ranks, ctx.miss_rows, mc};
         launch_fast_any(ctx.opts, tr, leaf_ids, (int)num, k, half_window, excl, nullptr, idx, dist, ctx.replay_ranks,
                         ctx.replay_rows, rc, ctx.status, variant, (unsigned long long *)(ctx.status + 6), st, eq,
-                        again);
+                        again, kc);
     }
 }
 
 bool fast_self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, size_t num, int k, bool excl,
-                   uint64_t *idx, void *dist, const void *bound, int half_window, int variant, cudaStream_t st) {
+                   uint64_t *idx, void *dist, const void *bound, int half_window, int variant, cudaStream_t st,
+                   int kc) {
     TreeImpl *impl = (TreeImpl *)tr.impl;
     if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0) return false;
     if (!fast_walk_applies(ctx.opts, *impl)) return false;
+    if (half_window <= 0 && variant <= 0 && kc <= 0) { // the autotuner's choice for this shape
+        auto it = ctx.tuned.find(tune_key(TUNE_SELF_KNN, k, tr.num_leaves));
+        if (it != ctx.tuned.end()) {
+            half_window = it->second.half;
+            variant     = it->second.variant;
+            kc          = it->second.kc;
+        }
+    }
     if (half_window <= 0) half_window = k;
     variant = walk_variant(variant, k);
     ensure_replay(ctx, num);
-    fast_walk_and_replay(ctx, tr, leaf_ids, num, k, excl, idx, dist, bound, half_window, variant, st);
+    fast_walk_and_replay(ctx, tr, leaf_ids, num, k, excl, idx, dist, bound, half_window, variant, st, {}, kc);
     replay_exact(ctx, tr, ctx.replay_ranks, ctx.replay_rows, ctx.status + 1, k, excl, idx, dist, st);
     return true;
 }
@@ -1235,11 +1267,19 @@ bool fast_knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, c
 
 void batch_self_knn(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, bool excl, uint64_t *idx,
                     void *dist, bool fast, int half_window, int variant, int32_t *rr, int32_t *rw, uint32_t *counters,
-                    cudaStream_t st, const void *bound, int32_t *mw) {
+                    cudaStream_t st, const void *bound, int32_t *mw, int kc) {
     if (num == 0 || k <= 0) return;
     if (!fast || k > 64) {
         batch_self_knn_exact(ctx, all, bt, num, k, excl, idx, dist, st);
         return;
+    }
+    if (half_window <= 0 && variant <= 0 && kc <= 0) { // the autotuner's choice for this shape
+        auto it = ctx.tuned.find(tune_key(TUNE_BATCH, k, num));
+        if (it != ctx.tuned.end()) {
+            half_window = it->second.half;
+            variant     = it->second.variant;
+            kc          = it->second.kc;
+        }
     }
     if (half_window <= 0) half_window = k;
     variant                        = walk_variant(variant, k);
@@ -1254,7 +1294,7 @@ void batch_self_knn(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t
     }
 #define FT_BF(T, B, LA)                                                                                            \
     launch_fast_view<T>(tree_view<T>(all), bt, metric_mode<T>(ctx.opts, all), ro, nullptr, n, k, half_window, excl, \
-                        B, idx, dist, rr, rw, counters, ctx.status, variant, visits, st, ExtQueries{}, LA)
+                        B, idx, dist, rr, rw, counters, ctx.status, variant, visits, st, ExtQueries{}, LA, kc)
     for (int pass = 0; pass < (bound ? 2 : 1); ++pass) {
         const void     *b  = pass == 0 ? bound : nullptr;
         const ListArgs &la = pass == 0 ? first : again;

@@ -5,6 +5,7 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <map>
 #include <string>
 #include <type_traits>
 
@@ -86,6 +87,24 @@ template <class T> inline int metric_mode(const ft_options &o, const ft_tree &t)
     return (sizeof(T) == 8 && ((const TreeImpl *)t.impl)->clean42) ? 2 : 1;
 }
 
+// The autotuner's choice for one shape (0: the built-in default of that parameter).
+struct TuneChoice {
+    int variant = 0; // fast walk variant (walk_variant's numbering)
+    int half    = 0; // SFC seeding half-window
+    int kc      = 0; // heap template of the walk: 32 (two-warp blocks) or 64 (one-warp blocks)
+    int items   = 0; // keys per thread of a onesweep tile (build)
+};
+enum TuneKind { TUNE_SELF_KNN = 0, TUNE_BATCH = 1, TUNE_BUILD = 2 };
+// Shape key: kind, k (or key words for the build) and the size class floor(log2 n).
+inline unsigned long long tune_key(int kind, int k, size_t n) {
+    int l = 0;
+    while (n > 1) {
+        n >>= 1;
+        ++l;
+    }
+    return ((unsigned long long)kind << 48) | ((unsigned long long)(unsigned)k << 16) | (unsigned long long)l;
+}
+
 struct Context {
     ft_options     opts{};
     int            device = 0;
@@ -111,6 +130,7 @@ struct Context {
     cudaStream_t   copy_stream   = nullptr;
     cudaEvent_t    ev_walked[2]  = {nullptr, nullptr};
     cudaEvent_t    ev_copied[2]  = {nullptr, nullptr};
+    std::map<unsigned long long, TuneChoice> tuned; // autotuner choices by shape (tune_key)
     float         *learned_feats = nullptr; // learned-bound scratch: features and bounds
     void          *learned_bound = nullptr;
     size_t         learned_cap   = 0;
@@ -119,8 +139,11 @@ struct Context {
 // ---- fast self-kNN (ft_fast.cu) ----
 // Returns false when the fast traversal does not apply (k > 64, a periodic tree with
 // coordinates beyond the period).
+// half_window / variant / kc <= 0: the autotuner's choice for the shape when there is one,
+// else the defaults.
 bool fast_self_knn(Context &ctx, const ft_tree &tree, const int32_t *leaf_ids, size_t num, int k, bool exclude_self,
-                   uint64_t *idx, void *dist, const void *bound, int half_window, int variant, cudaStream_t st);
+                   uint64_t *idx, void *dist, const void *bound, int half_window, int variant, cudaStream_t st,
+                   int kc = 0);
 void ensure_replay(Context &ctx, size_t num);
 // Fast self-kNN whose scratch is a fixed static device array (no allocation); false when
 // the fast walk does not apply.  At most noalloc_max_queries() queries per call.
@@ -138,7 +161,8 @@ void replay_exact(Context &ctx, const ft_tree &tree, const int32_t *ranks, const
 // through the miss list (mw, counters[4]) to a second launch of the walk without the bound.
 void batch_self_knn(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, bool exclude_self,
                     uint64_t *idx, void *dist, bool fast, int half_window, int variant, int32_t *rr, int32_t *rw,
-                    uint32_t *counters, cudaStream_t st, const void *bound = nullptr, int32_t *mw = nullptr);
+                    uint32_t *counters, cudaStream_t st, const void *bound = nullptr, int32_t *mw = nullptr,
+                    int kc = 0);
 // The reference traversal over every leaf of a batch (ft_query.cu).
 void batch_self_knn_exact(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, bool exclude_self,
                           uint64_t *idx, void *dist, cudaStream_t st);
@@ -169,10 +193,24 @@ void replay_external(Context &ctx, const ft_tree &tree, const void *qx, const vo
 // Reads and clears a device status word (synchronises the stream); throws on a set bit.
 void check_device_status(uint32_t *status, cudaStream_t st);
 
+// ---- autotuner (ft_tune.cu) ----
+// Each times its candidates on the caller's data, checks that every candidate returns the
+// default's rows (leaf order for the build), and keeps the fastest in ctx.tuned.
+void tune_self_knn(Context &ctx, const ft_tree &tree, int k, bool exclude_self, ft_tune_result *out, cudaStream_t st);
+void tune_batch_self_knn(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, bool exclude_self,
+                         int32_t *rr, int32_t *rw, uint32_t *counters, ft_tune_result *out, cudaStream_t st);
+void tune_build(Context &ctx, ft_tree &tree, const void *x, const void *y, const void *z, size_t n,
+                ft_tune_result *out, cudaStream_t st);
+
 // ---- build (ft_build.cu) ----
+// sort_items: keys per thread of the sort's tiles (0: the autotuner's choice for the shape,
+// else the default).
 void build_bvh(Context &ctx, ft_tree &tree, const void *x, const void *y, const void *z, size_t n,
                const uint32_t *id, const int8_t *ghost, const void *bbox_host, void *caller_keys_dev,
-               cudaStream_t st);
+               cudaStream_t st, int sort_items = 0);
+// Tile sizes the build's sort offers for one- or two-word keys (the default first).
+const int *sort_item_choices(int words, int *count);
+int        key_words_of(const ft_options &o);
 void build_tree_from_keys(Context &ctx, ft_tree &tree, const void *keys_ref_dev, const void *sx,
                           const void *sy, const void *sz, const uint32_t *sid, const int8_t *sghost,
                           const int32_t *sorig, cudaStream_t st);
@@ -231,6 +269,7 @@ void batch_build_query_graph(Context &ctx, BatchImpl &b, const long long *set_of
 void batch_tree_view(Context &ctx, BatchImpl &b, size_t set, ft_tree &out, cudaStream_t st);
 void batch_set_info(Context &ctx, BatchImpl &b, void *bbox_out, uint8_t *height_out, cudaStream_t st);
 void batch_stats(BatchImpl &b, ft_query_stats &out);
+void batch_tune(Context &ctx, BatchImpl &b, int k, bool exclude_self, ft_tune_result *out, cudaStream_t st);
 
 // ---- learned radius bound (ft_learned.cu) ----
 struct BoundModel;

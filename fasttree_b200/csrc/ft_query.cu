@@ -505,6 +505,145 @@ FT_D bool far_dist(T px, T py, T pz, const TreeDev<T> &t, int node, typename Coo
     }
 }
 
+// far_dist for a box held in registers (minx, maxx, miny, maxy, minz, maxz).
+template <class T, int PER>
+FT_D bool far_dist_box(T px, T py, T pz, const T b[6], typename Coord<T>::dist_t &out) {
+    using C      = Coord<T>;
+    const T p[3] = {px, py, pz};
+    if constexpr (C::is_float) {
+        T f[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) f[d] = c_fmax(sub_rn(b[2 * d + 1], p[d]), sub_rn(p[d], b[2 * d]));
+        out = (double)add_rn(add_rn(mul_rn(f[0], f[0]), mul_rn(f[1], f[1])), mul_rn(f[2], f[2]));
+        return true;
+    } else if constexpr (PER == 0) {
+        unsigned long long s = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const T                  lo = b[2 * d], hi = b[2 * d + 1];
+            const unsigned long long a  = p[d] > lo ? (unsigned long long)(T)(p[d] - lo) : 0ull;
+            const unsigned long long c  = hi > p[d] ? (unsigned long long)(T)(hi - p[d]) : 0ull;
+            s += Metric<T>::sq((a > c ? a : c) >> C::dist_shift);
+        }
+        out = s;
+        return true;
+    } else if constexpr (PER == 2 && sizeof(T) == 8) {
+        constexpr unsigned long long M = (1ull << C::bits) - 1ull, H = 1ull << (C::bits - 1);
+        unsigned long long           s = 0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const unsigned long long v = (unsigned long long)p[d] & M, l = b[2 * d], h = b[2 * d + 1];
+            const unsigned long long a = (v + H) & M; // antipode
+            auto w = [&](unsigned long long x) {
+                const unsigned long long u = (x - v) & M, e = (v - x) & M;
+                return u < e ? u : e;
+            };
+            const unsigned long long wl = w(l), wh = w(h);
+            const unsigned long long g  = (a >= l && a <= h) ? H : (wl > wh ? wl : wh);
+            s += Metric<T>::sq((unsigned long long)(uint32_t)(g >> C::dist_shift));
+        }
+        out = s;
+        return true;
+    } else {
+        return false;
+    }
+}
+
+// range_query on trees of height <= 62, where the reference's stack guard (which drops both
+// children of a node popped with 62 entries below it) cannot fire: the stack then only
+// orders the walk, so a child can be judged when its parent is expanded.  A child beyond
+// r_max is not pushed; once the row is full a child inside the shell is counted from its leaf
+// count (kept in the parent's record) instead of being walked.  Results are still written in
+// the reference's depth-first, left-first order.
+template <class T, int PER>
+__global__ void __launch_bounds__(128)
+    range_short_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
+                       const T *__restrict__ rmin, const T *__restrict__ rmax, int nq, int32_t *__restrict__ results,
+                       int32_t *__restrict__ counts, int max_per, int ret_orig, const uint32_t *__restrict__ order,
+                       uint32_t *status) {
+    using C = Coord<T>;
+    using D = typename C::dist_t;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    const int q = order ? (int)order[i] : i;
+    const int n = t.n;
+    D         rm2, RM2;
+    if constexpr (C::is_float) {
+        double a = (double)rmin[q], b = (double)rmax[q];
+        rm2      = __dmul_rn(a, a);
+        RM2      = __dmul_rn(b, b);
+    } else {
+        unsigned long long a = (unsigned long long)rmin[q] >> C::dist_shift;
+        unsigned long long b = (unsigned long long)rmax[q] >> C::dist_shift;
+        rm2                  = a * a;
+        RM2                  = b * b;
+    }
+    const T      px = qx[q], py = qy[q], pz = qz[q];
+    const size_t off   = (size_t)q * (size_t)max_per;
+    int          count = 0;
+    int          sn[kStack];
+    D            sd[kStack];
+    int          sp = 0;
+    const D      d0 = node_dist_soa<T, PER>(t, 0, px, py, pz);
+    if (d0 <= RM2) {
+        sn[0] = 0;
+        sd[0] = d0;
+        sp    = 1;
+    }
+    long long budget = 2ll * n + 64;
+    while (sp > 0) {
+        if (--budget < 0) {
+            atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+            break;
+        }
+        --sp;
+        const int node = sn[sp];
+        const D   d2   = sd[sp];
+        if (node >= n - 1) { // leaf (the n == 1 root included)
+            if (d2 >= rm2) {
+                if (count < max_per) results[off + count] = ret_orig ? t.orig_idx[node] : node - (n - 1);
+                ++count;
+            }
+            continue;
+        }
+        T        lb[6], rb[6];
+        int      l, r;
+        uint32_t il, ir;
+        load_rec_info(t.recs, node, lb, rb, l, r, il, ir);
+        const D    dl = box_dist<T, PER>(px, py, pz, lb), dr = box_dist<T, PER>(px, py, pz, rb);
+        const bool full = count >= max_per;
+        // right first on the stack, so the left subtree is walked (and written) first
+#pragma unroll
+        for (int side = 1; side >= 0; --side) {
+            const int      c  = side ? r : l;
+            const D        dc = side ? dr : dl;
+            const uint32_t ic = side ? ir : il;
+            if (!(dc <= RM2)) continue;
+            if (full) {
+                if (c >= n - 1) { // a leaf: counted now
+                    if (dc >= rm2) ++count;
+                    continue;
+                }
+                if (dc >= rm2 && info_leaves(ic) < kInfoCountMax) {
+                    D far;
+                    if (far_dist_box<T, PER>(px, py, pz, side ? rb : lb, far) && far <= RM2) {
+                        count += (int)info_leaves(ic); // every leaf below lies in the shell
+                        continue;
+                    }
+                }
+            }
+            if (sp >= kStack) {
+                atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+                break;
+            }
+            sn[sp] = c;
+            sd[sp] = dc;
+            ++sp;
+        }
+    }
+    counts[q] = count;
+}
+
 template <class T, int PER>
 __global__ void __launch_bounds__(128) range_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy,
                                                     const T *__restrict__ qz, const T *__restrict__ rmin,
@@ -909,10 +1048,13 @@ static void range_typed(const ft_options &o, const ft_tree &tr, const void *qx, 
     TreeDev<T> tv     = tree_view<T>(tr);
     int        blocks = (nq + 127) / 128;
     bool       ro     = o.return_orig_indices != 0;
+    // trees of height <= 62 never reach the reference's stack guard (range_short_kernel)
+    const TreeImpl *impl  = (const TreeImpl *)tr.impl;
+    const bool      short_walk = impl && impl->height_root >= 0 && impl->height_root <= 62;
     met_dispatch<T>(metric_mode<T>(o, tr), [&](auto M) {
-        range_kernel<T, decltype(M)::value><<<blocks, 128, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz,
-                                                                    (const T *)rmin, (const T *)rmax, nq, results,
-                                                                    counts, max_per, ro ? 1 : 0, order, status);
+        auto fn = short_walk ? range_short_kernel<T, decltype(M)::value> : range_kernel<T, decltype(M)::value>;
+        fn<<<blocks, 128, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz, (const T *)rmin, (const T *)rmax,
+                                   nq, results, counts, max_per, ro ? 1 : 0, order, status);
     });
     FT_CUDA(cudaGetLastError());
 }

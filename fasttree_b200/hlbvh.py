@@ -489,6 +489,29 @@ def knn_query(ctx: Context, tree: TreeSoA, qx, qy, qz, k: int, results=None, res
     return _rows(results, nq, k), _rows(result_dists, nq, k)
 
 
+def tune_self_knn(ctx: Context, tree: TreeSoA, k: int, exclude_self=True, stream=None) -> dict:
+    """Autotunes the fast walk for this tree's shape at k (ft_tune_self_knn); later default
+    calls take the choice.  Returns the choice and the sample's times."""
+    r = capi.FtTuneResult()
+    _call(lib().ft_tune_self_knn(ctx.handle, tree.c, int(k), int(bool(exclude_self)), ctypes.byref(r),
+                                 _stream_handle(stream)))
+    return r.as_dict()
+
+
+def tune_build(ctx: Context, p, tree: TreeSoA, stream=None) -> dict:
+    """Autotunes the build's sort tile on these points (ft_tune_build); the tree is left built."""
+    n = len(p.pos_x)
+    args = [_as_coord(a, ctx.coord) for a in (p.pos_x, p.pos_y, p.pos_z)]
+    r = capi.FtTuneResult()
+    _call(lib().ft_tune_build(ctx.handle, *[_ptr(a) for a in args], n, tree.c, ctypes.byref(r),
+                              _stream_handle(stream)))
+    return r.as_dict()
+
+
+def tune_reset(ctx: Context):
+    _call(lib().ft_tune_reset(ctx.handle))
+
+
 def range_query(ctx: Context, tree: TreeSoA, qx, qy, qz, r_min, r_max, max_results_per_query: int, results=None,
                 result_counts=None, stream=None):
     """range_query (src/hlbvh.hpp:2006-2136).  Blocking; returns (results, counts)."""
@@ -587,6 +610,13 @@ class BatchedSets:
         self._keep = (off, xyz, ids, gh, results, result_dists)
         self.num_sets, self.num_points = S, N
         return _rows(results, N, k), _rows(result_dists, N, k)
+
+    def tune(self, k: int, exclude_self=True, stream=None) -> dict:
+        """Autotunes the batched walk for the last build's shape at k (ft_tune_batch_self_knn)."""
+        r = capi.FtTuneResult()
+        _call(lib().ft_tune_batch_self_knn(self.ctx.handle, self._h, int(k), int(bool(exclude_self)),
+                                           ctypes.byref(r), _stream_handle(stream)))
+        return r.as_dict()
 
     def bound_features(self, k: int, stream=None) -> torch.Tensor:
         """(num_points, 12) float32 learned-bound features of every leaf, each on its own set."""

@@ -398,6 +398,41 @@ ft_status ft_batch_set_info(ft_context *ctx, ft_batch *batch, void *bbox_out, ui
 /* Replay count and visits of the last ft_batch_self_knn / ft_batch_build_knn (synchronises). */
 ft_status ft_batch_query_stats(ft_context *ctx, ft_batch *batch, ft_query_stats *out);
 
+/* ---------------------------------------------------------------------------------- */
+/* Autotuner.  The reference picks one kernel shape per device: the sub-group width from  */
+/* get_native_sub_group_width and its MAXK dispatchers (src/hlbvh.hpp:1828-1927).  Here    */
+/* every candidate returns the same rows bit for bit, so the tuner times the candidates on  */
+/* the caller's own data and keeps the fastest per shape (kind, k, size class floor(log2    */
+/* n)) in the context; later calls with default options (ft_query_options zeroed past       */
+/* method) take it.  Each tuner checks on the device that every candidate's rows (the leaf  */
+/* order, for the build) equal the default's and fails with FT_ERR_RUNTIME otherwise.       */
+/* Blocking; they allocate scratch of their own.                                            */
+/* ---------------------------------------------------------------------------------- */
+typedef struct ft_tune_result {
+    int32_t walk_variant;  /* fast walk: 2 compact binary, 4 4-wide per-lane, 5 group walk  */
+    int32_t half_window;   /* SFC seeding half-window                                      */
+    int32_t block_threads; /* 64 (two warps, 32-entry heap template) or 32 (one warp)      */
+    int32_t sort_items;    /* build: keys per thread of a onesweep tile                    */
+    int32_t candidates;    /* configurations timed                                         */
+    float   best_ms;       /* the sample's time with the choice                            */
+    float   default_ms;    /* and with the defaults                                        */
+    int32_t reserved[9];
+} ft_tune_result;
+
+/* Self-kNN on `tree` at k (1..64): walk variant x half-window x block shape, timed on up to
+ * 2^18 of its queries (four stretches of consecutive leaves). */
+ft_status ft_tune_self_knn(ft_context *ctx, const ft_tree *tree, int k, int exclude_self, ft_tune_result *out,
+                           ft_stream_t stream);
+/* The batched self-kNN of the batch's last build at k (1..64), timed on the whole batch. */
+ft_status ft_tune_batch_self_knn(ft_context *ctx, ft_batch *batch, int k, int exclude_self, ft_tune_result *out,
+                                 ft_stream_t stream);
+/* build_bvh of these points (host or device, as ft_build_bvh): the sort's tile size, timed
+ * over whole builds into `tree` (left holding the last candidate's build, equal to any). */
+ft_status ft_tune_build(ft_context *ctx, const void *x, const void *y, const void *z, size_t n, ft_tree *tree,
+                        ft_tune_result *out, ft_stream_t stream);
+/* Forgets every choice the tuners made on this context. */
+ft_status ft_tune_reset(ft_context *ctx);
+
 #ifdef __cplusplus
 }
 #endif

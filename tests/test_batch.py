@@ -312,7 +312,10 @@ def test_learned_batched_query_is_exact_for_any_network(coord, sfc, periodic):
         assert torch.equal(li, pi) and torch.equal(ld, pd), name
         st = b.query_stats()
         if name == "tiny":
-            assert st["bound_misses"] >= N - 10
+            # every bound is about zero: every row whose k-th distance is not zero misses it
+            # (the sets hold duplicate points, whose rows stay within a zero bound)
+            positive = int((pd[:, -1].view(torch.int64) > 0).sum())
+            assert st["bound_misses"] >= positive - 10, (st["bound_misses"], positive)
             assert st["replayed"] < 0.05 * N
     # the same through one CUDA graph (build + learned query), replayed twice
     dx, dy, dz = (torch.from_numpy(a).cuda() for a in (x, y, z))
