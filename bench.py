@@ -53,7 +53,9 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg1", "cfg3", "cfg4", "cfg5", "learned"])
+    p.add_argument("--workload", default="cfg2",
+                   choices=["cfg2", "cfg1", "cfg3", "cfg4", "cfg5", "learned", "profile"],
+                   help="profile: every kernel of the library once on small inputs (for ncu captures)")
     p.add_argument("--no-per-set-loop", action="store_true",
                    help="batched sets: skip the loop of single-set calls (profiling)")
     p.add_argument("--no-batched", action="store_true",
@@ -546,6 +548,87 @@ def run_cfg5(args, stream):
     return out
 
 
+def run_profile(args, stream):
+    """Every kernel family once on small inputs, for per-kernel ncu captures (the profiles/
+    summaries): the build and both self-kNN methods on 2M clustered uint64 points (k = 32),
+    range_query on 20K of them, knn_query of 100K external points on 100K uniform float64
+    points (k = 64, MAXK = 256, both methods), the learned bound's features and inference,
+    and a batch of 256 Plummer sets (build + fast self-kNN).  Prints what ran."""
+    import torch
+
+    import fasttree_b200 as ft
+    from fasttree_b200 import datasets
+    from fasttree_b200 import learned as L
+    n = args.n or 2_000_000
+    x, y, z = datasets.clustered_fixed(n, n_spheres=max(10, n // 500), seed=2)
+    ctx = ft.Context("u64", "ph", periodic=True)
+    dev = f"cuda:{ctx.device}"
+    dx, dy, dz = (torch.from_numpy(a).to(dev) for a in (x, y, z))
+    tree = ft.TreeSoA(ctx, n)
+    ft.build_bvh(ctx, ft.particles(dx, dy, dz), tree)
+    ft.self_knn_query(ctx, tree, 32, method="fast")
+    ft.self_knn_query(ctx, tree, 32, method="plain")
+    m = 20_000
+    r0 = torch.zeros(m, dtype=torch.int64, device=dev).view(torch.uint64)
+    r1 = torch.full((m,), int(2e-3 * 2 ** 40), dtype=torch.int64, device=dev).view(torch.uint64)
+    ft.range_query(ctx, tree, dx[:m], dy[:m], dz[:m], r0, r1, 512)
+    model = L.BoundModel(ctx, seed=1)
+    f = L.features(ctx, tree, 32)
+    model.predict(f, 1.3, want_bound=True)
+    ux, uy, uz = datasets.uniform(100_000, seed=1)
+    qx, qy, qz = datasets.external_queries(ux, uy, uz, 100_000, seed=3)
+    c2 = ft.Context("f64", "morton")
+    t2 = ft.TreeSoA(c2, len(ux))
+    ft.build_bvh(c2, ft.particles(ux, uy, uz), t2)
+    dq = [torch.from_numpy(a).to(dev) for a in (qx, qy, qz)]
+    ft.knn_query(c2, t2, *dq, 64, max_k=256, method="fast")
+    ft.knn_query(c2, t2, *dq, 64, max_k=256, method="plain")
+    sizes = datasets.batched_set_sizes(256, seed=4)
+    bx, by, bz, boff = datasets.batched_sets(sizes=sizes, seed=4)
+    c3 = ft.Context("f32", "morton")
+    b = ft.BatchedSets(c3, len(bx), len(sizes))
+    b.build(boff, bx, by, bz)
+    b.self_knn(32)
+    b.check()
+    torch.cuda.synchronize()
+    return {"workload": "profile", "self_knn_points": n, "range_queries": m, "external_queries": len(qx),
+            "batched_sets": len(sizes), "batched_points": len(bx)}
+
+
+def build_stage_roofline(ctx, p, tree, n, sc, stream):
+    """One more build with stage events (ft_set_build_profiling): each stage's time, its
+    as-designed bytes (every byte once: bbox 3 s_c N; keys N(3 s_c + s_k + 4); sort 8 passes
+    of 2N(s_k + 4) plus the N s_k histogram read; gather N(4 + 9 s_c + 9); topology
+    2N s_k + 12(N-1); refit (N-1)(18 s_c + 8); 4-wide records (N-1)(48 s_c + 16)) and the GB/s
+    and fraction of the measured HBM bandwidth they imply; and the whole build against the
+    compulsory bytes 3 s_c N + (2N-1)(6 s_c + 4) + 8(N-1) + 9N."""
+    import torch
+
+    import fasttree_b200 as ft
+    sk = 16 if ctx.coord == ft.U64 else 8
+    ctx.profile_builds(True)
+    ft.build_bvh(ctx, p, tree)
+    prof = ctx.build_profile()
+    ctx.profile_builds(False)
+    torch.cuda.synchronize()
+    peak, kind = measured_peaks()
+    designed = {"bbox_ms": 3 * sc * n, "encode_ms": n * (3 * sc + sk + 4), "sort_ms": 8 * 2 * n * (sk + 4) + n * sk,
+                "gather_ms": n * (4 + 9 * sc + 9), "topology_ms": 2 * n * sk + 12 * (n - 1),
+                "refit_ms": (n - 1) * (18 * sc + 8), "records_ms": (n - 1) * (48 * sc + 16)}
+    stages = {}
+    for key, b in designed.items():
+        ms = prof[key]
+        gbs = b / (ms / 1e3) / 1e9 if ms > 0 else None
+        stages[key[:-3]] = {"ms": ms, "bytes": b, "gbs": gbs, "frac": gbs / peak if gbs else None}
+    compulsory = 3 * sc * n + (2 * n - 1) * (6 * sc + 4) + 8 * (n - 1) + 9 * n
+    tot = prof["total_ms"]
+    return {"stages": stages, "total_ms": tot, "compulsory_bytes": compulsory,
+            "achieved_gbs": compulsory / (tot / 1e3) / 1e9, "frac": compulsory / (tot / 1e3) / 1e9 / peak,
+            "peak": peak, "peak_source": kind, "unit": "GB/s",
+            "note": "stage times from CUDA events inside one build_bvh (ft_get_build_profile); as-designed bytes "
+                    "per stage as in the docstring"}
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -690,6 +773,13 @@ def run_ours(args):
         if rank == 0:
             print(json.dumps(r), flush=True)
         return
+    if args.workload == "profile":
+        r = run_profile(args, torch.cuda.current_stream())
+        if world > 1:
+            dist.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(r), flush=True)
+        return
     if args.workload == "cfg5":
         r = run_cfg5(args, torch.cuda.current_stream())
         if world > 1:
@@ -749,6 +839,7 @@ def run_ours(args):
         bt.append(e0.elapsed_time(e1))
     build_ms = statistics.median(bt)
     height = tree.height()
+    build_roofline = build_stage_roofline(ctx, p, tree, n, x.element_size(), stream)
 
     # ---- self-kNN timing (device-resident tree and outputs) ----
     idx = torch.empty(n * k, dtype=torch.uint64, device=dev)
@@ -972,7 +1063,7 @@ def run_ours(args):
                "plain": plain, "other_k_and_range": extra, "batched": batched, "learned": learned,
                "knn_query": knn_ext, "cfg1": cfg1, "cfg5": cfg5,
                "build_ms": build_ms, "tree_height": height, "query_stats": stats,
-               "bit_exact": bit_exact, "tuning": tuning,
+               "bit_exact": bit_exact, "tuning": tuning, "build_roofline": build_roofline,
                "e2e": e2e, "gpu_launches": args.steps * (2 if method == 1 else 1),
                "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(out), flush=True)

@@ -25,7 +25,8 @@ EXPORTED = (
     "ft_batch_create", "ft_batch_destroy", "ft_batch_build", "ft_batch_self_knn", "ft_batch_build_knn",
     "ft_batch_tree", "ft_batch_set_info", "ft_batch_query_stats", "ft_batch_self_knn_learned",
     "ft_batch_build_knn_learned", "ft_batch_bound_features", "ft_get_replayed_queries",
-    "ft_tune_self_knn", "ft_tune_batch_self_knn", "ft_tune_build", "ft_tune_reset",
+    "ft_tune_self_knn", "ft_tune_batch_self_knn", "ft_tune_build", "ft_tune_reset", "ft_set_build_profiling",
+    "ft_get_build_profile",
     "ft_bound_model_create", "ft_bound_model_destroy", "ft_bound_model_get_params", "ft_bound_model_set_params",
     "ft_bound_model_set_norm", "ft_bound_features", "ft_bound_targets", "ft_bound_model_gradient",
     "ft_bound_model_fit", "ft_bound_model_predict", "ft_self_knn_learned", "ft_bound_features_points",
@@ -59,6 +60,15 @@ class FtTuneResult(ctypes.Structure):
     _fields_ = [("walk_variant", ctypes.c_int32), ("half_window", ctypes.c_int32), ("block_threads", ctypes.c_int32),
                 ("sort_items", ctypes.c_int32), ("candidates", ctypes.c_int32), ("best_ms", ctypes.c_float),
                 ("default_ms", ctypes.c_float), ("reserved", ctypes.c_int32 * 9)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
+
+
+class FtBuildProfile(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_float) for f in ("bbox_ms", "encode_ms", "sort_ms", "gather_ms", "topology_ms",
+                                              "refit_ms", "records_ms", "total_ms")] + [
+        ("reserved", ctypes.c_int32 * 8)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_ if f != "reserved"}
@@ -108,6 +118,8 @@ _SIGS = {
     "ft_tune_batch_self_knn": [_vp, _vp, _i, _i, ctypes.POINTER(FtTuneResult), _st],
     "ft_tune_build": [_vp, _vp, _vp, _vp, _sz, ctypes.POINTER(FtTree), ctypes.POINTER(FtTuneResult), _st],
     "ft_tune_reset": [_vp],
+    "ft_set_build_profiling": [_vp, _i],
+    "ft_get_build_profile": [_vp, ctypes.POINTER(FtBuildProfile)],
     "ft_batch_self_knn_learned": [_vp, _vp, _vp, _i, _i, ctypes.c_float, _vp, _vp, ctypes.POINTER(FtQueryOptions),
                                   _st],
     "ft_batch_build_knn_learned": [_vp, _vp, _vp, ctypes.c_float, _vp, _sz, _sz, _vp, _vp, _vp, _vp, _vp, _i, _i,

@@ -798,9 +798,13 @@ template <class T> struct SoA {
 };
 
 template <class T>
-static void topology_and_refit(const ft_options &o, ft_tree &t, TreeImpl &s, size_t n, cudaStream_t st) {
+static void topology_and_refit(const ft_options &o, ft_tree &t, TreeImpl &s, size_t n, cudaStream_t st,
+                               Context *prof = nullptr) {
     if (n < 2) {
         s.height_root = 0;
+        stage_mark(prof, BS_TOPOLOGY, st);
+        stage_mark(prof, BS_REFIT, st);
+        stage_mark(prof, BS_RECORDS, st);
         return;
     }
     FT_CUDA(cudaMemsetAsync(t.parent, 0xFF, (2 * n - 1) * sizeof(int32_t), st)); // -1 (849)
@@ -812,14 +816,17 @@ static void topology_and_refit(const ft_options &o, ft_tree &t, TreeImpl &s, siz
     default: karras_kernel<2><<<blocks, 256, 0, st>>>(lo, hi, (int)n, t.left_child, t.right_child, t.parent, s.leafcount); break;
     }
     FT_CUDA(cudaGetLastError());
+    stage_mark(prof, BS_TOPOLOGY, st);
     FT_CUDA(cudaMemsetAsync(s.counters, 0, (n - 1) * sizeof(int32_t), st));
     SoA<T> a(t);
     refit_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, t.parent, a.mnx, a.mxx, a.mny,
                                             a.mxy, a.mnz, a.mxz, (NodeRec<T> *)s.recs, s.height, s.counters,
                                             s.leafcount);
+    stage_mark(prof, BS_REFIT, st);
     collapse_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, a.mnx, a.mxx, a.mny, a.mxy,
                                                a.mnz, a.mxz, (WideRec<T> *)s.wide);
     FT_CUDA(cudaGetLastError());
+    stage_mark(prof, BS_RECORDS, st);
 }
 
 template <class T>
@@ -828,11 +835,13 @@ static void build_bvh_typed(Context &ctx, ft_tree &t, const void *x, const void 
                             cudaStream_t st, int sort_items) {
     TreeImpl &s = *(TreeImpl *)t.impl;
     ensure_scratch(s, ctx.opts, n);
+    stage_mark(&ctx, BS_START, st);
     // 1. bounding box.  Only the float encode reads it; integer encoding ignores it, so an
     // integer tree always keeps its true box (the query distance mode depends on it).
     if (bbox_host && Coord<T>::is_float)
         FT_CUDA(cudaMemcpyAsync(s.bbox, bbox_host, 6 * sizeof(T), cudaMemcpyHostToDevice, st));
     else compute_bbox(ctx, &s, x, y, z, n, s.bbox, st);
+    stage_mark(&ctx, BS_BBOX, st);
     // 2. keys + iota permutation
     if (caller_keys) {
         keys_from_ref_kernel<<<grid_for(n, 256), 256, 0, st>>>(caller_keys, n, ref_key_mode(ctx.opts),
@@ -842,12 +851,14 @@ static void build_bvh_typed(Context &ctx, ft_tree &t, const void *x, const void 
     } else {
         encode(ctx.opts, x, y, z, n, s.bbox, s, st);
     }
+    stage_mark(&ctx, BS_ENCODE, st);
     // 3. sort (key, perm), with the tile the autotuner chose for this shape
     if (sort_items <= 0) {
         auto it = ctx.tuned.find(tune_key(TUNE_BUILD, key_words(ctx.opts), n));
         if (it != ctx.tuned.end()) sort_items = it->second.items;
     }
     sort_keys(ctx.opts, s, n, st, sort_items);
+    stage_mark(&ctx, BS_SORT, st);
     if (caller_keys) {
         keys_to_ref_kernel<<<grid_for(n, 256), 256, 0, st>>>((const unsigned long long *)s.key_lo,
                                                               (const unsigned long long *)s.key_hi, n,
@@ -866,8 +877,10 @@ static void build_bvh_typed(Context &ctx, ft_tree &t, const void *x, const void 
                                                        t.orig_idx);
     FT_CUDA(cudaGetLastError());
     if (n == 1) FT_CUDA(cudaMemsetAsync(t.parent, 0xFF, sizeof(int32_t), st));
+    stage_mark(&ctx, BS_GATHER, st);
     // 5. topology + refit
-    topology_and_refit<T>(ctx.opts, t, s, n, st);
+    topology_and_refit<T>(ctx.opts, t, s, n, st, &ctx);
+    ctx.bprof.recorded = ctx.bprof.on;
 }
 
 void build_bvh(Context &ctx, ft_tree &t, const void *x, const void *y, const void *z, size_t n, const uint32_t *id,

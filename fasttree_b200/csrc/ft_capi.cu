@@ -266,6 +266,8 @@ ft_status ft_context_destroy(ft_context *ctx) {
         if (ctx->iota) cudaFree(ctx->iota);
         if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
         ft::free_query_sort(*ctx);
+        for (int i = 0; i < ft::BS_COUNT; ++i)
+            if (ctx->bprof.ev[i]) cudaEventDestroy(ctx->bprof.ev[i]);
         if (ctx->learned_feats) cudaFree(ctx->learned_feats);
         if (ctx->learned_bound) cudaFree(ctx->learned_bound);
     }
@@ -1212,6 +1214,40 @@ ft_status ft_tune_build(ft_context *ctx, const void *x, const void *y, const voi
     // leave the tree built the ordinary way (with the chosen tile)
     const ft_status s2 = ft_build_bvh(ctx, x, y, z, n, nullptr, nullptr, nullptr, nullptr, tree, stream);
     if (s2 != FT_OK) return s2;
+    FT_API_END
+}
+
+ft_status ft_set_build_profiling(ft_context *ctx, int enable) {
+    FT_API_BEGIN
+    need(ctx != nullptr, "null context");
+    DeviceGuard g(ctx->device);
+    if (enable && !ctx->bprof.ev[0])
+        for (int i = 0; i < BS_COUNT; ++i) FT_CUDA(cudaEventCreate(&ctx->bprof.ev[i]));
+    ctx->bprof.on       = enable != 0;
+    ctx->bprof.recorded = false;
+    FT_API_END
+}
+
+ft_status ft_get_build_profile(ft_context *ctx, ft_build_profile *out) {
+    FT_API_BEGIN
+    need(ctx && out, "null argument");
+    need(ctx->bprof.recorded, "no profiled build on this context (ft_set_build_profiling, then ft_build_bvh)");
+    DeviceGuard g(ctx->device);
+    FT_CUDA(cudaEventSynchronize(ctx->bprof.ev[BS_RECORDS]));
+    float ms[BS_COUNT] = {0};
+    for (int i = 1; i < BS_COUNT; ++i)
+        FT_CUDA(cudaEventElapsedTime(&ms[i], ctx->bprof.ev[i - 1], ctx->bprof.ev[i]));
+    *out             = ft_build_profile{};
+    out->bbox_ms     = ms[BS_BBOX];
+    out->encode_ms   = ms[BS_ENCODE];
+    out->sort_ms     = ms[BS_SORT];
+    out->gather_ms   = ms[BS_GATHER];
+    out->topology_ms = ms[BS_TOPOLOGY];
+    out->refit_ms    = ms[BS_REFIT];
+    out->records_ms  = ms[BS_RECORDS];
+    float total      = 0.0f;
+    FT_CUDA(cudaEventElapsedTime(&total, ctx->bprof.ev[BS_START], ctx->bprof.ev[BS_RECORDS]));
+    out->total_ms = total;
     FT_API_END
 }
 

@@ -105,6 +105,15 @@ inline unsigned long long tune_key(int kind, int k, size_t n) {
     return ((unsigned long long)kind << 48) | ((unsigned long long)(unsigned)k << 16) | (unsigned long long)l;
 }
 
+// Stage timing of build_bvh (ft_set_build_profiling): events recorded on the build's stream
+// between its stages.
+enum BuildStage { BS_START, BS_BBOX, BS_ENCODE, BS_SORT, BS_GATHER, BS_TOPOLOGY, BS_REFIT, BS_RECORDS, BS_COUNT };
+struct BuildProfile {
+    bool        on       = false;
+    bool        recorded = false; // the last build recorded every stage
+    cudaEvent_t ev[BS_COUNT] = {};
+};
+
 struct Context {
     ft_options     opts{};
     int            device = 0;
@@ -131,6 +140,7 @@ struct Context {
     cudaEvent_t    ev_walked[2]  = {nullptr, nullptr};
     cudaEvent_t    ev_copied[2]  = {nullptr, nullptr};
     std::map<unsigned long long, TuneChoice> tuned; // autotuner choices by shape (tune_key)
+    BuildProfile   bprof;
     float         *learned_feats = nullptr; // learned-bound scratch: features and bounds
     void          *learned_bound = nullptr;
     size_t         learned_cap   = 0;
@@ -201,6 +211,11 @@ void tune_batch_self_knn(Context &ctx, const ft_tree &all, const BatchDev &bt, s
                          int32_t *rr, int32_t *rw, uint32_t *counters, ft_tune_result *out, cudaStream_t st);
 void tune_build(Context &ctx, ft_tree &tree, const void *x, const void *y, const void *z, size_t n,
                 ft_tune_result *out, cudaStream_t st);
+
+// Records build stage i on st when build profiling is on.
+inline void stage_mark(Context *ctx, int i, cudaStream_t st) {
+    if (ctx && ctx->bprof.on) cudaEventRecord(ctx->bprof.ev[i], st);
+}
 
 // ---- build (ft_build.cu) ----
 // sort_items: keys per thread of the sort's tiles (0: the autotuner's choice for the shape,

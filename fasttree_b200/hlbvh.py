@@ -105,6 +105,16 @@ class Context:
         return {"queries": s.queries, "replayed": s.replayed, "visits": s.reserved[0],
                 "bound_misses": s.reserved[1], "rerun_visits": s.reserved[2]}
 
+    def profile_builds(self, enable: bool = True):
+        """Stage timing of later builds on this context (ft_set_build_profiling)."""
+        _call(lib().ft_set_build_profiling(self._h, int(bool(enable))))
+
+    def build_profile(self) -> dict:
+        """Stage times (ms) of the last profiled build (ft_get_build_profile; synchronises)."""
+        p = capi.FtBuildProfile()
+        _call(lib().ft_get_build_profile(self._h, ctypes.byref(p)))
+        return p.as_dict()
+
     def check_device_status(self, stream=None):
         """Synchronises the stream and raises what the kernels recorded (ft_check_device_status)."""
         _call(lib().ft_check_device_status(self._h, _stream_handle(stream)))

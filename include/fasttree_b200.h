@@ -433,6 +433,25 @@ ft_status ft_tune_build(ft_context *ctx, const void *x, const void *y, const voi
 /* Forgets every choice the tuners made on this context. */
 ft_status ft_tune_reset(ft_context *ctx);
 
+/* ---------------------------------------------------------------------------------- */
+/* Build stage timing (the reference reports per-stage build times in its profiling notes):  */
+/* with profiling on, ft_build_bvh records CUDA events on its stream between its stages;   */
+/* ft_get_build_profile returns the last profiled build's stage times (synchronises).       */
+/* ---------------------------------------------------------------------------------- */
+typedef struct ft_build_profile {
+    float   bbox_ms;      /* compute_bbox                                                  */
+    float   encode_ms;    /* SFC keys + permutation                                        */
+    float   sort_ms;      /* key + permutation sort                                        */
+    float   gather_ms;    /* leaf gather                                                   */
+    float   topology_ms;  /* Karras topology                                               */
+    float   refit_ms;     /* bottom-up refit (boxes, node records, heights)                */
+    float   records_ms;   /* 4-wide records of the fast walk                               */
+    float   total_ms;
+    int32_t reserved[8];
+} ft_build_profile;
+ft_status ft_set_build_profiling(ft_context *ctx, int enable);
+ft_status ft_get_build_profile(ft_context *ctx, ft_build_profile *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -304,6 +304,8 @@ def test_learned_batched_query_is_exact_for_any_network(coord, sfc, periodic):
     huge.params = p
     b = ft.BatchedSets(ctx, N, len(sizes))
     b.build(off, x, y, z)
+    b.self_knn(k, method="fast")
+    fast_replayed = b.query_stats()["replayed"]  # genuine ties (a third of the sets are duplicates)
     pi, pd = b.self_knn(k, method="plain")
     pi, pd = pi.clone(), pd.clone()
     for name, model in (("trained", trained), ("untrained", untrained), ("tiny", tiny), ("huge", huge)):
@@ -316,7 +318,10 @@ def test_learned_batched_query_is_exact_for_any_network(coord, sfc, periodic):
             # (the sets hold duplicate points, whose rows stay within a zero bound)
             positive = int((pd[:, -1].view(torch.int64) > 0).sum())
             assert st["bound_misses"] >= positive - 10, (st["bound_misses"], positive)
-            assert st["replayed"] < 0.05 * N
+            # the misses rerun the walk without the bound, so the replay list holds the rows
+            # the unbounded fast walk flags for ties (plus the few tied rows the first launch
+            # finished within the zero bound), not the misses
+            assert st["replayed"] <= fast_replayed + 0.01 * N, (st["replayed"], fast_replayed)
     # the same through one CUDA graph (build + learned query), replayed twice
     dx, dy, dz = (torch.from_numpy(a).cuda() for a in (x, y, z))
     doff = torch.from_numpy(off).cuda()

@@ -90,3 +90,21 @@ def test_tuner_rejections():
         ft.tune_self_knn(ctx, tree, 65)  # the fast walk serves k <= 64
     with pytest.raises(ValueError):
         ft.tune_self_knn(ctx, tree, 0)
+
+
+def test_build_stage_profile():
+    """ft_set_build_profiling / ft_get_build_profile: every stage of a build timed on its
+    stream; the stages add up to the whole build; a context without a profiled build says so."""
+    ctx = ft.Context("u64", "ph", periodic=True)
+    x, y, z = datasets.clustered_fixed(500_000, n_spheres=1000, seed=2)
+    tree = ft.TreeSoA(ctx, len(x))
+    with pytest.raises(ValueError):
+        ctx.build_profile()
+    ctx.profile_builds(True)
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree)
+    prof = ctx.build_profile()
+    stages = [prof[k] for k in ("bbox_ms", "encode_ms", "sort_ms", "gather_ms", "topology_ms", "refit_ms",
+                                "records_ms")]
+    assert all(v >= 0.0 for v in stages) and prof["total_ms"] > 0.0
+    assert abs(sum(stages) - prof["total_ms"]) < 0.05 * prof["total_ms"] + 0.01
+    ctx.profile_builds(False)
