@@ -138,6 +138,13 @@ def run_batched(args, dev, stream, timed_steps, warmup):
     graph_ms = timed(lambda: b.build_knn(off, x, y, z, k, idx, dst, method="fast"), timed_steps)
     b.check()
     stats = b.query_stats()
+    # the same build + query as one persistent launch (FT_METHOD_PERSISTENT), in its own graph
+    bp = ft.BatchedSets(ctx, N, S)
+    pidx, pdst = torch.empty_like(idx), torch.empty_like(dst)
+    persist_ms = timed(lambda: bp.build_knn(off, x, y, z, k, pidx, pdst, method="persistent"), timed_steps)
+    bp.check()
+    pstats = bp.query_stats()
+    del bp
     build_ms = timed(lambda: b.build(off, x, y, z), timed_steps)
     fi, fd = torch.empty_like(idx), torch.empty_like(dst)
     fast_ms = timed(lambda: b.self_knn(k, method="fast", results=fi, result_dists=fd,
@@ -145,8 +152,13 @@ def run_batched(args, dev, stream, timed_steps, warmup):
     pi, pd = torch.empty_like(idx), torch.empty_like(dst)
     plain_ms = timed(lambda: b.self_knn(k, method="plain", results=pi, result_dists=pd), max(1, timed_steps // 2))
     b.check()
-    bit_exact = {"graph_vs_plain": rows_equal(idx, dst, pi, pd), "fast_vs_plain": rows_equal(fi, fd, pi, pd)}
-    del fi, fd
+    bit_exact = {"graph_vs_plain": rows_equal(idx, dst, pi, pd), "fast_vs_plain": rows_equal(fi, fd, pi, pd),
+                 "persistent_vs_plain": rows_equal(pidx, pdst, pi, pd)}
+    del fi, fd, pidx, pdst
+    persistent = {"ms_per_step": persist_ms, "value": N / (persist_ms / 1e3), "unit": "queries/s",
+                  "replayed": pstats["replayed"],
+                  "note": "ft_batch_build_knn with FT_METHOD_PERSISTENT: prep + order + one persistent kernel "
+                          "(per-set builds, then 32-query chunks of finished sets) + replay, one CUDA graph"}
     learned = run_batched_learned(args, ctx, b, off, x, y, z, k, idx, dst, (pi, pd), timed, timed_steps, plain_ms)
     del pi, pd
     # the same sets one by one through the single-tree API (the non-batched way)
@@ -155,7 +167,7 @@ def run_batched(args, dev, stream, timed_steps, warmup):
         del b
         return {"workload": w["name"], "n_sets": S, "n_points": N, "k": k,
                 "graph_build_plus_query_ms": graph_ms, "value": N / (graph_ms / 1e3), "unit": "queries/s",
-                "build_ms": build_ms, "query_fast_ms": fast_ms, "query_plain_ms": plain_ms,
+                "persistent": persistent, "build_ms": build_ms, "query_fast_ms": fast_ms, "query_plain_ms": plain_ms,
                 "replayed": stats["replayed"], "bit_exact": bit_exact, "learned": learned, "tuning": tuning}
     tree = ft.TreeSoA(ctx, int(np.diff(offs).max()))
     li = torch.empty(int(np.diff(offs).max()) * k, dtype=torch.uint64, device=dev)
@@ -173,7 +185,7 @@ def run_batched(args, dev, stream, timed_steps, warmup):
     del b, tree
     return {"workload": w["name"], "n_sets": S, "n_points": N, "k": k,
             "graph_build_plus_query_ms": graph_ms, "value": N / (graph_ms / 1e3), "unit": "queries/s",
-            "build_ms": build_ms, "query_fast_ms": fast_ms, "query_plain_ms": plain_ms,
+            "persistent": persistent, "build_ms": build_ms, "query_fast_ms": fast_ms, "query_plain_ms": plain_ms,
             "query_fast_qps": N / (fast_ms / 1e3), "query_plain_qps": N / (plain_ms / 1e3),
             "per_set_loop_ms": loop_ms, "per_set_loop_qps": N / (loop_ms / 1e3),
             "replayed": stats["replayed"], "bit_exact": bit_exact, "learned": learned, "tuning": tuning,
@@ -388,9 +400,24 @@ def run_cfg2_extra(args, ctx, tree, x, y, z, n, stream):
     out["range_query"] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s",
                           "mean_count": float(c.mean()), "max_count": int(cnt.max()),
                           "truncated_queries": int((cnt > max_per).sum()), "max_results_per_query": max_per,
+                          "walk": "one walk per query (default)",
                           "queries": "the N particle positions in input order (the library walks them in SFC "
                                      "order); one blocking call, including its status check"}
-    del res, cnt
+    # the warp-shared walk (ft_set_range_walk 2) on the first 1M queries: its time, and its
+    # rows and counts against the default walk's
+    m = min(n, 1_000_000)
+    res1 = torch.empty(m * max_per, dtype=torch.int32, device=dev)
+    cnt1 = torch.empty(m, dtype=torch.int32, device=dev)
+    ctx.set_range_walk(2)
+    ms1 = _timed(stream, lambda: ft.range_query(ctx, tree, x[:m], y[:m], z[:m], r0[:m], r1[:m], max_per, res1, cnt1),
+                 1, warmup=0)
+    ctx.set_range_walk(0)
+    valid = torch.arange(max_per, device=dev)[None, :] < cnt1.clamp(max=max_per)[:, None]
+    same = bool(torch.equal(cnt1, cnt[:m])) and bool(torch.equal(res1.view(m, max_per)[valid],
+                                                                   res.view(n, max_per)[:m][valid]))
+    out["range_query"]["warp_walk_1M"] = {"ms_per_step": ms1, "value": m / (ms1 / 1e3), "unit": "queries/s",
+                                          "rows_and_counts_equal_default": same}
+    del res, cnt, res1, cnt1, valid
     # refit-only update (a simulation step): every point moved by N(0, sigma^2) per axis (kept
     # inside the 2^40 box), refit on the kept topology, then the fast self-kNN (k=32) on the
     # refit tree against a rebuild of the moved points.  sigma = 1e-6 of the box is a fraction

@@ -32,38 +32,13 @@
 
 #include "ft_build_dev.cuh"
 #include "ft_common.cuh"
+#include "ft_cta_build.cuh"
 #include "ft_internal.h"
 
 namespace ft {
 
 static constexpr int kPrepThreads = 1024;
 static constexpr int kChunk       = kBboxThreads * 16; // points per bbox chunk
-
-// ---- order-preserving unsigned images of coordinates (for atomic min / max) ----
-template <class T> struct Ord;
-template <> struct Ord<float> {
-    using type = unsigned int;
-    static FT_D type bits(float f) {
-        unsigned int u = __float_as_uint(f);
-        return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-    }
-    static FT_D float value(type u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u); }
-};
-template <> struct Ord<double> {
-    using type = unsigned long long;
-    static FT_D type bits(double f) {
-        unsigned long long u = (unsigned long long)__double_as_longlong(f);
-        return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
-    }
-    static FT_D double value(type u) {
-        return __longlong_as_double((long long)((u >> 63) ? (u & 0x7fffffffffffffffull) : ~u));
-    }
-};
-template <> struct Ord<uint32_t> {
-    using type = unsigned int;
-    static FT_D type     bits(uint32_t v) { return v; }
-    static FT_D uint32_t value(type u) { return u; }
-};
 
 // =========================================================================================
 // 1. prep: offsets check + node / record offsets.  Invalid offsets (off[0] != 0, off[S] != N
@@ -301,6 +276,31 @@ __global__ void batch_heights_kernel(const long long *__restrict__ off, const lo
         set_height[s] = (off[s + 1] - off[s] >= 2) ? height[rec_off[s]] : (uint8_t)0;
 }
 
+// Build order of the persistent launch: sets by decreasing size class (floor(log2 n)), so the
+// longest builds start first.  One block; the order inside a class is whatever the atomics
+// give (it schedules work and changes no result).
+__global__ void __launch_bounds__(1024) batch_order_kernel(const long long *__restrict__ off, int S, int32_t *order) {
+    __shared__ uint32_t s_cnt[64];
+    for (int i = threadIdx.x; i < 64; i += blockDim.x) s_cnt[i] = 0;
+    __syncthreads();
+    auto cls = [&](int s) {
+        const long long n = off[s + 1] - off[s];
+        return n > 0 ? 64 - __clzll((unsigned long long)n) : 0;
+    };
+    for (int s = threadIdx.x; s < S; s += blockDim.x) atomicAdd(&s_cnt[cls(s)], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int c = 63; c >= 0; --c) {
+            const uint32_t v = s_cnt[c];
+            s_cnt[c]         = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    for (int s = threadIdx.x; s < S; s += blockDim.x) order[atomicAdd(&s_cnt[cls(s)], 1u)] = s;
+}
+
 // =========================================================================================
 // Host side
 // =========================================================================================
@@ -329,6 +329,8 @@ struct BatchImpl {
     void      *bbox = nullptr, *par = nullptr;  // 6 coordinates per set each
     int32_t   *rr = nullptr, *rw = nullptr;     // replay list of the fast walk
     int32_t   *mw = nullptr;                    // rows whose learned bound proved too small
+    int32_t   *order = nullptr, *ready = nullptr, *chunk_next = nullptr; // persistent launch: max_sets each
+    uint32_t  *ctl = nullptr;                   // persistent launch: build tickets, ready slots, cursor
     uint32_t  *counters = nullptr;              // [0] replay count, [2..3] visits, [4] bound misses
     float     *feats = nullptr;                 // learned bound: features and bounds of every leaf,
     void      *bound = nullptr;                 // allocated by the first learned query
@@ -359,7 +361,8 @@ void batch_free(BatchImpl *b) {
     void *ptrs[] = {b->all.min_x, b->all.max_x, b->all.min_y,  b->all.max_y,    b->all.min_z,  b->all.max_z,
                     b->all.left_child, b->all.right_child, b->all.parent, b->all.id, b->all.is_ghost,
                     b->all.orig_idx, b->off, b->node_off, b->rec_off, b->set_height, b->bmin, b->bmax, b->bbox,
-                    b->par, b->rr, b->rw, b->mw, b->counters, b->feats, b->bound};
+                    b->par, b->rr, b->rw, b->mw, b->counters, b->feats, b->bound, b->order, b->ready,
+                    b->chunk_next, b->ctl};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     free_scratch(b->scr);
@@ -368,9 +371,6 @@ void batch_free(BatchImpl *b) {
 
 BatchImpl *batch_create(Context &ctx, size_t max_points, size_t max_sets) {
     const ft_options &o = ctx.opts;
-    if (o.coord_type == U64)
-        fail(FT_ERR_INVALID_ARGUMENT, "batched sets need 63-bit keys: F32 / F64 coordinates, or U32 with "
-                                      "Peano-Hilbert keys (U64 positions make 126-bit keys)");
     if (max_sets < 1 || max_sets > (size_t(1) << 24)) fail(FT_ERR_INVALID_ARGUMENT, "max_sets must be in [1, 2^24]");
     if (max_points > (size_t(1) << 30)) fail(FT_ERR_INVALID_ARGUMENT, "max_points must be at most 2^30");
     std::unique_ptr<BatchImpl, void (*)(BatchImpl *)> b(new BatchImpl(), batch_free);
@@ -402,6 +402,10 @@ BatchImpl *batch_create(Context &ctx, size_t max_points, size_t max_sets) {
     s.wide        = dalloc<unsigned char>(P * wide_bytes(o.coord_type));
     s.key_lo      = (uint64_t *)dalloc<unsigned long long>(P);
     s.tmp_lo      = (uint64_t *)dalloc<unsigned long long>(P);
+    if (o.coord_type == U64) { // 126-bit keys (built by the persistent launch only)
+        s.key_hi = (uint64_t *)dalloc<unsigned long long>(P);
+        s.tmp_hi = (uint64_t *)dalloc<unsigned long long>(P);
+    }
     s.perm        = dalloc<uint32_t>(P);
     s.tmp_perm    = dalloc<uint32_t>(P);
     s.hist        = dalloc<uint32_t>(16 * 256 + 16);
@@ -424,6 +428,10 @@ BatchImpl *batch_create(Context &ctx, size_t max_points, size_t max_sets) {
     b->rw         = dalloc<int32_t>(P);
     b->mw         = dalloc<int32_t>(P);
     b->counters   = dalloc<uint32_t>(8);
+    b->order      = dalloc<int32_t>(max_sets);
+    b->ready      = dalloc<int32_t>(max_sets);
+    b->chunk_next = dalloc<int32_t>(max_sets);
+    b->ctl        = dalloc<uint32_t>(4);
     FT_CUDA(cudaMemset(b->counters, 0, 32));
     return b.release();
 }
@@ -526,8 +534,56 @@ static void batch_build_typed(Context &ctx, BatchImpl &b, const long long *in_of
     FT_CUDA(cudaGetLastError());
 }
 
+// The persistent launch (batch_persistent): offsets prepared, the scheduling words reset, the
+// build order computed, then one kernel builds every set and, with `query`, answers its
+// self-kNN rows (tied rows replayed by a second launch).  No host synchronisation and no
+// allocation, so it is captured in the build + query graph like the launch sequence.
+struct PersistQuery {
+    int       k    = 0;
+    bool      excl = true;
+    uint64_t *idx  = nullptr;
+    void     *dist = nullptr;
+};
+static void batch_build_persistent(Context &ctx, BatchImpl &b, const long long *in_off, size_t S, size_t N,
+                                   const void *x, const void *y, const void *z, const uint32_t *id,
+                                   const int8_t *ghost, const PersistQuery *q, cudaStream_t st) {
+    if (S < 1 || S > b.max_sets) fail(FT_ERR_INVALID_ARGUMENT, "num_sets must be in [1, max_sets]");
+    if (N > b.max_points) fail(FT_ERR_INVALID_ARGUMENT, "num_points exceeds the batch's max_points");
+    b.S                = S;
+    b.N                = N;
+    b.built            = true;
+    b.all.num_leaves   = N;
+    b.all.num_internal = N;
+    batch_prep_kernel<<<1, kPrepThreads, 0, st>>>(in_off, (int)S, (long long)N, b.off, b.node_off, b.rec_off,
+                                                  ctx.status);
+    FT_CUDA(cudaGetLastError());
+    FT_CUDA(cudaMemsetAsync(b.ctl, 0, 4 * sizeof(uint32_t), st));
+    FT_CUDA(cudaMemsetAsync(b.ready, 0xFF, S * sizeof(int32_t), st));
+    FT_CUDA(cudaMemsetAsync(b.chunk_next, 0, S * sizeof(int32_t), st));
+    if (q) FT_CUDA(cudaMemsetAsync(b.counters, 0, 8 * sizeof(uint32_t), st));
+    batch_order_kernel<<<1, 1024, 0, st>>>(b.off, (int)S, b.order);
+    FT_CUDA(cudaGetLastError());
+    PersistLaunch p;
+    p.off = b.off; p.node_off = b.node_off; p.rec_off = b.rec_off; p.S = (int)S;
+    p.x = x; p.y = y; p.z = z; p.id = id; p.ghost = ghost;
+    p.all = b.all; p.scr = &b.scr; p.bbox = b.bbox; p.set_height = b.set_height;
+    p.order = b.order; p.ready = b.ready; p.chunk_next = b.chunk_next; p.ctl = b.ctl;
+    p.query = q != nullptr && N > 0;
+    if (p.query) {
+        p.k = q->k; p.excl = q->excl; p.idx = q->idx; p.dist = q->dist;
+        p.rr = b.rr; p.rw = b.rw; p.counters = b.counters;
+    }
+    batch_persistent(ctx, p, st);
+    if (p.query)
+        replay_exact(ctx, b.all, b.rr, b.rw, b.counters, q->k, q->excl, q->idx, q->dist, st, batch_dev(b));
+}
+
 void batch_build(Context &ctx, BatchImpl &b, const long long *in_off, size_t S, size_t N, const void *x,
                  const void *y, const void *z, const uint32_t *id, const int8_t *ghost, cudaStream_t st) {
+    if (ctx.opts.coord_type == U64) { // 126-bit keys: the per-set builds of the persistent launch
+        batch_build_persistent(ctx, b, in_off, S, N, x, y, z, id, ghost, nullptr, st);
+        return;
+    }
     if (S < 1 || S > b.max_sets) fail(FT_ERR_INVALID_ARGUMENT, "num_sets must be in [1, max_sets]");
     if (N > b.max_points) fail(FT_ERR_INVALID_ARGUMENT, "num_points exceeds the batch's max_points");
     b.S     = S;
@@ -555,14 +611,18 @@ static void ensure_batch_learned(BatchImpl &b) {
 
 // model: null, or the learned radius bound (features -> prediction x inflation -> the walk's
 // per-query bound; queries whose bound proves too small rerun the walk without it).
-void batch_query(Context &ctx, BatchImpl &b, int k, bool excl, uint64_t *idx, void *dist, const ft_query_options &q,
-                 cudaStream_t st, BoundModel *model, float inflation) {
-    if (!b.built) fail(FT_ERR_INVALID_ARGUMENT, "the batch has not been built");
+static void check_query_args(int k, const ft_query_options &q) {
     const int max_k = q.max_k > 0 ? q.max_k : 32;
     if (k > max_k)
         fail(FT_ERR_INVALID_ARGUMENT,
              "k exceeds _MAX_K_ template parameter. Instantiate self_knn_query with larger _MAX_K_.");
     if (k > 512) fail(FT_ERR_RUNTIME, "self_knn_query: k too large for shared memory.");
+}
+
+void batch_query(Context &ctx, BatchImpl &b, int k, bool excl, uint64_t *idx, void *dist, const ft_query_options &q,
+                 cudaStream_t st, BoundModel *model, float inflation) {
+    if (!b.built) fail(FT_ERR_INVALID_ARGUMENT, "the batch has not been built");
+    check_query_args(k, q);
     if (model && k > 64) fail(FT_ERR_INVALID_ARGUMENT, "learned bound: k must be in [1, 64]");
     if (b.N == 0 || k <= 0) return;
     const void *bound = nullptr;
@@ -611,8 +671,20 @@ void batch_build_query_graph(Context &ctx, BatchImpl &b, const long long *in_off
         FT_CUDA(cudaStreamBeginCapture(b.cap_stream, cudaStreamCaptureModeRelaxed));
         cudaGraph_t graph = nullptr;
         try {
-            batch_build(ctx, b, in_off, S, N, x, y, z, id, ghost, b.cap_stream);
-            batch_query(ctx, b, k, excl, idx, dist, q, b.cap_stream, model, inflation);
+            if (q.method == FT_METHOD_PERSISTENT && !model && k >= 1 && k <= 64) {
+                check_query_args(k, q);
+                PersistQuery pq;
+                pq.k    = k;
+                pq.excl = excl;
+                pq.idx  = idx;
+                pq.dist = dist;
+                batch_build_persistent(ctx, b, in_off, S, N, x, y, z, id, ghost, &pq, b.cap_stream);
+            } else {
+                if (q.method == FT_METHOD_PERSISTENT)
+                    batch_build_persistent(ctx, b, in_off, S, N, x, y, z, id, ghost, nullptr, b.cap_stream);
+                else batch_build(ctx, b, in_off, S, N, x, y, z, id, ghost, b.cap_stream);
+                batch_query(ctx, b, k, excl, idx, dist, q, b.cap_stream, model, inflation);
+            }
         } catch (...) {
             cudaStreamEndCapture(b.cap_stream, &graph);
             if (graph) cudaGraphDestroy(graph);

@@ -1217,6 +1217,14 @@ ft_status ft_tune_build(ft_context *ctx, const void *x, const void *y, const voi
     FT_API_END
 }
 
+ft_status ft_set_range_walk(ft_context *ctx, int walk) {
+    FT_API_BEGIN
+    need(ctx != nullptr, "null context");
+    need(walk >= 0 && walk <= 2, "range walk must be 0 (default), 1 (one walk per query) or 2 (warp-shared)");
+    ctx->range_walk = walk;
+    FT_API_END
+}
+
 ft_status ft_set_build_profiling(ft_context *ctx, int enable) {
     FT_API_BEGIN
     need(ctx != nullptr, "null context");

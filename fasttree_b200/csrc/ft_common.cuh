@@ -197,12 +197,27 @@ template <class T> struct alignas(16) WideRec {
 static_assert(sizeof(WideRec<float>) == 112, "wide record size");
 static_assert(sizeof(WideRec<double>) == 208, "wide record size");
 
-template <class T> FT_D void load_wide(const WideRec<T> *w, int node, T b[4][6], int c[4]) {
+// Record loads: through the read-only path by default.  COH: an ordinary (weak, L1-cached)
+// global load instead, for kernels that read records other blocks wrote earlier in the same
+// launch -- the read-only path is only valid for data that stays unchanged while the kernel
+// runs, while an ordinary load that follows an acquire of the writer's release (and a warp
+// barrier, for the other lanes) sees the written values.
+template <bool COH> FT_D uint4 ld_rec16(const uint4 *p) {
+    if constexpr (COH) {
+        uint4 v;
+        asm("ld.global.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+        return v;
+    } else {
+        return __ldg(p);
+    }
+}
+
+template <class T, bool COH = false> FT_D void load_wide(const WideRec<T> *w, int node, T b[4][6], int c[4]) {
     constexpr int NW = (int)(sizeof(WideRec<T>) / 16);
     const uint4  *p  = reinterpret_cast<const uint4 *>(w + node);
     uint4         v[NW];
 #pragma unroll
-    for (int i = 0; i < NW; ++i) v[i] = __ldg(p + i);
+    for (int i = 0; i < NW; ++i) v[i] = ld_rec16<COH>(p + i);
     const T *f = reinterpret_cast<const T *>(v);
 #pragma unroll
     for (int i = 0; i < 4; ++i)
@@ -214,14 +229,14 @@ template <class T> FT_D void load_wide(const WideRec<T> *w, int node, T b[4][6],
 }
 
 // load_rec plus the two children's info words (rec_child_info).
-template <class T>
+template <class T, bool COH = false>
 FT_D void load_rec_info(const NodeRec<T> *recs, int node, T lb[6], T rb[6], int &l, int &r, uint32_t &il,
                         uint32_t &ir) {
     const uint4 *p = reinterpret_cast<const uint4 *>(recs + node);
     if constexpr (sizeof(T) == 8) {
         uint4 w[7];
 #pragma unroll
-        for (int i = 0; i < 7; ++i) w[i] = __ldg(p + i);
+        for (int i = 0; i < 7; ++i) w[i] = ld_rec16<COH>(p + i);
         const T *v = reinterpret_cast<const T *>(w);
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
@@ -235,7 +250,7 @@ FT_D void load_rec_info(const NodeRec<T> *recs, int node, T lb[6], T rb[6], int 
     } else {
         uint4 w[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) w[i] = __ldg(p + i);
+        for (int i = 0; i < 4; ++i) w[i] = ld_rec16<COH>(p + i);
         const T *v = reinterpret_cast<const T *>(w);
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
@@ -249,12 +264,13 @@ FT_D void load_rec_info(const NodeRec<T> *recs, int node, T lb[6], T rb[6], int 
     }
 }
 
-template <class T> FT_D void load_rec(const NodeRec<T> *recs, int node, T lb[6], T rb[6], int &l, int &r) {
+template <class T, bool COH = false>
+FT_D void load_rec(const NodeRec<T> *recs, int node, T lb[6], T rb[6], int &l, int &r) {
     const uint4 *p = reinterpret_cast<const uint4 *>(recs + node);
     if constexpr (sizeof(T) == 8) {
         uint4 w[7];
 #pragma unroll
-        for (int i = 0; i < 7; ++i) w[i] = __ldg(p + i);
+        for (int i = 0; i < 7; ++i) w[i] = ld_rec16<COH>(p + i);
         const T *v = reinterpret_cast<const T *>(w);
 #pragma unroll
         for (int i = 0; i < 6; ++i) {
@@ -266,7 +282,7 @@ template <class T> FT_D void load_rec(const NodeRec<T> *recs, int node, T lb[6],
     } else {
         uint4 w[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) w[i] = __ldg(p + i);
+        for (int i = 0; i < 4; ++i) w[i] = ld_rec16<COH>(p + i);
         const T *v = reinterpret_cast<const T *>(w);
 #pragma unroll
         for (int i = 0; i < 6; ++i) {

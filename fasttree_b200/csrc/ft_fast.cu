@@ -31,6 +31,7 @@
 
 #include "ft_build_dev.cuh"
 #include "ft_common.cuh"
+#include "ft_cta_build.cuh"
 #include "ft_internal.h"
 
 namespace ft {
@@ -44,6 +45,12 @@ static constexpr int kFastThreads = 32 * kFastWarps;
 // fit 9 per SM; 64-entry heaps take 24 KB per warp, and one-warp blocks fit 9 warps per SM
 // where two-warp blocks fit 8.
 template <int KC> constexpr int fast_warps() { return KC > 32 ? 1 : kFastWarps; }
+// Distance type of the fast walk's heap entries: float coordinates' distances are float sums
+// widened to double (node_distance_sq), so their heaps keep the float, exactly, in 4 bytes
+// (12 -> 8 bytes an entry: more resident blocks); other types keep dist_t.
+template <class T>
+using heap_dist_t =
+    typename std::conditional<std::is_same<T, float>::value, float, typename Coord<T>::dist_t>::type;
 
 // Group walk (variant 5): a lower bound of the walk's distance from every point of the
 // group box [g0, g1] (per axis) to a node box b (minx, maxx, miny, maxy, minz, maxz).  Each
@@ -167,7 +174,7 @@ template <class T> FT_D T coord_bottom() {
 // their tallest paths only.  Bounded: a search that runs long answers true.
 // stk: scratch of kGuardStack entries (the walk's own stack, free by then).
 static constexpr int kGuardStack = 80;
-template <class T, int PER>
+template <class T, int PER, bool COH = false>
 FT_D bool stack_guard_reaches(const TreeDev<T> &t, T px, T py, T pz, typename Coord<T>::dist_t dk,
                               unsigned long long *stk) {
     using D = typename Coord<T>::dist_t;
@@ -183,7 +190,7 @@ FT_D bool stack_guard_reaches(const TreeDev<T> &t, T px, T py, T pz, typename Co
         const int                u = (int)(e >> 8), s = (int)(e & 255ull);
         T                        lb[6], rb[6];
         int                      l, r;
-        load_rec(t.recs, u, lb, rb, l, r);
+        load_rec<T, COH>(t.recs, u, lb, rb, l, r);
         const D    ld2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, lb[0], lb[1], lb[2], lb[3],
                                                                          lb[4], lb[5]);
         const D    rd2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, rb[0], rb[1], rb[2], rb[3],
@@ -255,8 +262,10 @@ struct ListArgs {
 };
 
 // One warp's 32 queries: entries [qbase, qbase + 32) of [0, num) -- query rows, or entries of
-// the list `lst` when it is given.
-template <class T, int PER, int KC, int VAR>
+// the list `lst` when it is given.  NW: warps of the calling block (the heaps are laid out
+// per thread of the block); COH: tree records read through L2 (the persistent batch kernel,
+// whose blocks read trees that other blocks built earlier in the same launch).
+template <class T, int PER, int KC, int VAR, int NW = fast_warps<KC>(), bool COH = false>
 FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss, unsigned char *smem,
                     TreeDev<T> t_all, BatchDev bt, const T *__restrict__ qx, const T *__restrict__ qy,
                     const T *__restrict__ qz, const uint32_t *__restrict__ order,
@@ -266,8 +275,9 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
                     int32_t *__restrict__ replay_ranks, int32_t *__restrict__ replay_rows, uint32_t *replay_count,
                     uint32_t *status, unsigned long long *visit_count) {
     using D = typename Coord<T>::dist_t;
-    constexpr int kFastWarps = fast_warps<KC>(), kFastThreads = 32 * kFastWarps; // this heap's block shape
-    D       *hd  = reinterpret_cast<D *>(smem);
+    constexpr int kFastWarps = NW, kFastThreads = 32 * kFastWarps; // the block's shape
+    using H      = heap_dist_t<T>;
+    H       *hd  = reinterpret_cast<H *>(smem);
     int32_t *hix = reinterpret_cast<int32_t *>(hd + k * kFastThreads); // heaps sized for k (<= KC)
     __shared__ int32_t s_node[kFastWarps][kFastStack];
     // the 4-wide walk's per-lane stack, then the stack-guard test's scratch
@@ -348,11 +358,11 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
                 int p  = (i - 1) >> 1;
                 D   pd = HD(p);
                 if (d2 <= pd) break;
-                HD(i) = pd;
+                HD(i) = (H)pd;
                 HI(i) = HI(p);
                 i     = p;
             }
-            HD(i) = d2;
+            HD(i) = (H)d2;
             HI(i) = id;
             ++count;
             if (count == k) {
@@ -381,11 +391,11 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
                     }
                 }
                 if (c == i) break;
-                HD(i) = cd;
+                HD(i) = (H)cd;
                 HI(i) = HI(c);
                 i     = c;
             }
-            HD(i) = d2;
+            HD(i) = (H)d2;
             HI(i) = id;
             hmax  = HD(0);
             thr   = hmax < B ? hmax : B;
@@ -555,7 +565,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
                 unsigned kl = 0, ki = 0;
                 if (node >= 0) {
                     ++visits;
-                    load_wide(t.wide, node, bx, ch);
+                    load_wide<T, COH>(t.wide, node, bx, ch);
 #pragma unroll
                     for (int i = 0; i < 4; ++i)
                         if (ch[i] >= 0 && !(group_lb<T, PER>(g0, g1, bx[i]) > R)) {
@@ -616,7 +626,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             ++visits;
             T   lb[6], rb[6];
             int l, r;
-            load_rec(t.recs, cur, lb, rb, l, r);
+            load_rec<T, COH>(t.recs, cur, lb, rb, l, r);
             const D    ld2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, lb[0], lb[1], lb[2], lb[3], lb[4], lb[5]);
             const D    rd2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, rb[0], rb[1], rb[2], rb[3], rb[4], rb[5]);
             const bool lleaf = l >= n - 1, rleaf = r >= n - 1;
@@ -677,7 +687,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             ++visits;
             T   bx[4][6];
             int ch[4];
-            load_wide(t.wide, cur, bx, ch);
+            load_wide<T, COH>(t.wide, cur, bx, ch);
             D  d[4];
             bool in[4]; // needed internal child
 #pragma unroll
@@ -767,7 +777,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             } else {
                 T   lb[6], rb[6];
                 int l, r;
-                load_rec(t.recs, node, lb, rb, l, r);
+                load_rec<T, COH>(t.recs, node, lb, rb, l, r);
                 const D ld2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, lb[0], lb[1], lb[2], lb[3], lb[4], lb[5]);
                 const D rd2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, rb[0], rb[1], rb[2], rb[3], rb[4], rb[5]);
                 if (sp + 2 > kFastStack) {
@@ -810,7 +820,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
         } else {
             T   lb[6], rb[6];
             int l, r;
-            load_rec(t.recs, node, lb, rb, l, r);
+            load_rec<T, COH>(t.recs, node, lb, rb, l, r);
             const D  ld2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, lb[0], lb[1], lb[2], lb[3], lb[4], lb[5]);
             const D  rd2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, rb[0], rb[1], rb[2], rb[3], rb[4], rb[5]);
             const bool nl = needs(ld2), nr = needs(rd2);
@@ -865,7 +875,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
         // trees of height >= 63: the reference's stack guard may drop part of this query's
         // neighbourhood (fewer than k points found: conservatively so)
         if (!flag && n >= 2 && (int)t.height[0] >= 63 &&
-            (count < k || stack_guard_reaches<T, PER>(t, px, py, pz, hmax, lane_stack)))
+            (count < k || stack_guard_reaches<T, PER, COH>(t, px, py, pz, hmax, lane_stack)))
             flag = true;
         for (int hs = count; hs > 1; --hs) {
             D       last  = HD(hs - 1);
@@ -893,11 +903,11 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
                     }
                 }
                 if (c == i) break;
-                HD(i) = cd;
+                HD(i) = (H)cd;
                 HI(i) = HI(c);
                 i     = c;
             }
-            HD(i) = last;
+            HD(i) = (H)last;
             HI(i) = lasti;
         }
         for (int i = 1; i < count; ++i)
@@ -906,7 +916,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
         for (int i = 0; i < k; ++i) {
             if (i < count) {
                 __stcs(out_idx + off + i, (unsigned long long)(long long)HI(i));
-                __stcs(out_dist + off + i, HD(i));
+                __stcs(out_dist + off + i, (D)HD(i));
             } else {
                 __stcs(out_idx + off + i, ~0ull);
                 __stcs(out_dist + off + i, dist_missing<D>());
@@ -980,7 +990,7 @@ static void launch_fast_t(const TreeDev<T> &tv, const BatchDev &bt, const ExtQue
                           unsigned long long *visits, cudaStream_t st, const ListArgs &la) {
     using D     = typename Coord<T>::dist_t;
     constexpr int threads = 32 * fast_warps<KC>();
-    size_t        smem    = (size_t)std::max(k, 1) * threads * (sizeof(D) + 4); // heaps of k entries
+    size_t        smem    = (size_t)std::max(k, 1) * threads * (sizeof(heap_dist_t<T>) + 4); // heaps of k entries
     auto   fn   = variant == 0 ? fast_self_knn_kernel<T, PER, KC, 0>
                   : variant == 1 ? fast_self_knn_kernel<T, PER, KC, 1>
                   : variant == 4 ? fast_self_knn_kernel<T, PER, KC, 4>
@@ -1133,7 +1143,9 @@ bool fast_self_knn(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, siz
     TreeImpl *impl = (TreeImpl *)tr.impl;
     if (k > 64 || tr.num_leaves < 2 || !impl || impl->height_root < 0) return false;
     if (!fast_walk_applies(ctx.opts, *impl)) return false;
-    if (half_window <= 0 && variant <= 0 && kc <= 0) { // the autotuner's choice for this shape
+    // the autotuner's choice for this shape; it was made on every leaf in SFC order, so a
+    // subset (whose warps hold unrelated leaves) keeps the defaults
+    if (half_window <= 0 && variant <= 0 && kc <= 0 && !leaf_ids) {
         auto it = ctx.tuned.find(tune_key(TUNE_SELF_KNN, k, tr.num_leaves));
         if (it != ctx.tuned.end()) {
             half_window = it->second.half;
@@ -1431,6 +1443,266 @@ bool fast_self_knn_noalloc(Context &ctx, const ft_tree &tr, const int32_t *leaf_
     ctx.last_fast      = true;
     ctx.last_rows      = false; // the replayed rows stay in the fixed array
     return true;
+}
+
+// =========================================================================================
+// Persistent batched launch: build every set and answer its self-kNN queries in one kernel.
+//
+// Phase 1 -- builds.  Blocks take sets by ticket in the order `order` (largest first, so the
+// longest builds start first) and build each whole set (cta_build_set).  A finished set is
+// published: after a fence, its id goes to the next slot of `ready` with a release store.
+// Phase 2 -- queries.  Each warp takes 32 queries of the set at the cursor of `ready` (one
+// atomic per chunk on the set's chunk counter); when that set has no chunk left the cursor
+// moves on.  The warp runs the fast walk on its 32 queries, reading the set's
+// tree through L2 (the records were written by another block of this launch, so the
+// read-only path cannot be used for them); tied queries go to the replay list as in every
+// other fast walk.
+// A block waits only for a set whose build another running block has claimed (every build is
+// claimed before any block queries), so the waits end; they are bounded all the same (30 s of
+// global time), after which the block sets STATUS_SPIN_LIMIT and stops.
+// =========================================================================================
+// Two-warp blocks, the standalone walk's shape: the heaps take the same shared memory per
+// warp, so as many warps fit on an SM (18 with k <= 32 heaps); a block builds its sets with
+// its 64 threads.
+template <int KC> constexpr int persist_warps() { return 2; }
+template <int KC> constexpr int persist_blocks_per_sm() { return KC > 32 ? 4 : 9; }
+static constexpr int kPersistItems = 8; // keys per thread of a sort tile
+
+template <class T> struct PersistDev {
+    const long long *off, *node_off, *rec_off;
+    int              S;
+    const T         *x, *y, *z;
+    const uint32_t  *id;
+    const int8_t    *ghost;
+    T               *mnx, *mxx, *mny, *mxy, *mnz, *mxz;
+    int32_t         *left, *right, *parent;
+    uint32_t        *tid_out;
+    int8_t          *ghost_out;
+    int32_t         *orig;
+    NodeRec<T>      *recs;
+    WideRec<T>      *wide;
+    uint8_t         *height;
+    int32_t         *counters, *leaves;
+    unsigned long long *klo, *khi, *tlo, *thi;
+    uint32_t        *perm, *tperm;
+    T               *bbox;
+    uint8_t         *set_height;
+    const int32_t   *order;
+    int32_t         *ready, *chunk_next;
+    uint32_t        *ctl;
+    int              query;
+};
+
+FT_D unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+FT_D int ld_acquire_gpu(const int32_t *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+FT_D void st_release_gpu(int32_t *p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+FT_D int ld_relaxed_gpu_i(const int32_t *p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+FT_D uint32_t ld_relaxed_gpu(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+template <class T, int PER, int KC, int SFC, int KIND>
+__global__ void __launch_bounds__(32 * persist_warps<KC>(), persist_blocks_per_sm<KC>())
+    batch_persistent_kernel(PersistDev<T> a, TreeDev<T> t_all, BatchDev bt, int k, int half_window,
+                            int exclude_self, int ret_orig, unsigned long long *out_idx,
+                            typename Coord<T>::dist_t *out_dist, int32_t *replay_ranks, int32_t *replay_rows,
+                            uint32_t *replay_count, uint32_t *status, unsigned long long *visit_count) {
+    constexpr int NW = persist_warps<KC>(), PT = 32 * NW;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int s_item;
+    const int      tid = threadIdx.x;
+
+    // ---- 1. builds ----
+    for (;;) {
+        if (tid == 0) s_item = (int)atomicAdd(&a.ctl[0], 1u);
+        __syncthreads();
+        const int i = s_item;
+        __syncthreads();
+        if (i >= a.S) break; // block-uniform
+        const int       s = a.order[i];
+        const long long o = a.off[s];
+        const int       n = (int)(a.off[s + 1] - o);
+        if (n > 0) {
+            const long long no = a.node_off[s], ro = a.rec_off[s];
+            CtaTreeOut<T>   out;
+            out.mnx      = a.mnx + no;
+            out.mxx      = a.mxx + no;
+            out.mny      = a.mny + no;
+            out.mxy      = a.mxy + no;
+            out.mnz      = a.mnz + no;
+            out.mxz      = a.mxz + no;
+            out.left     = a.left + ro;
+            out.right    = a.right + ro;
+            out.parent   = a.parent + no;
+            out.id       = a.tid_out + no;
+            out.ghost    = a.ghost_out + no;
+            out.orig     = a.orig + no;
+            out.recs     = a.recs + ro;
+            out.wide     = a.wide + ro;
+            out.height   = a.height + ro;
+            out.counters = a.counters + ro;
+            out.leaves   = a.leaves + ro;
+            cta_build_set<T, SFC, KIND, PT, kPersistItems>(
+                n, a.x + o, a.y + o, a.z + o, a.id ? a.id + o : nullptr, a.ghost ? a.ghost + o : nullptr, a.klo + o,
+                a.khi ? a.khi + o : nullptr, a.perm + o, a.tlo + o, a.thi ? a.thi + o : nullptr, a.tperm + o, out,
+                a.bbox + 6 * (size_t)s, a.set_height + s, smem);
+        } else if (tid == 0) {
+            // an empty set: the box the atomic min / max build leaves (no point folded in)
+            using O = typename Ord<T>::type;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                a.bbox[6 * (size_t)s + 2 * d]     = Ord<T>::value((O)~(O)0);
+                a.bbox[6 * (size_t)s + 2 * d + 1] = Ord<T>::value((O)0);
+            }
+            a.set_height[s] = 0;
+        }
+        if (tid == 0) { // publish the set: its tree is complete
+            __threadfence();
+            const uint32_t p = atomicAdd(&a.ctl[1], 1u);
+            st_release_gpu(&a.ready[p], s);
+        }
+    }
+    if (!a.query) return;
+
+    // ---- 2. queries: each warp takes 32 queries at a time ----
+    // A warp acquires a set's publication before it first reads the set's tree; the warp
+    // barrier after the broadcast orders the other lanes' reads after it.
+    const int lane     = tid & 31;
+    int       acquired = -1; // the last set this warp acquired (lane 0)
+    for (;;) {
+        int s = -1, j = 0;
+        if (lane == 0) {
+            const unsigned long long t0 = global_ns();
+            for (;;) {
+                const uint32_t c = ld_relaxed_gpu(&a.ctl[2]);
+                if (c >= (uint32_t)a.S) break;
+                int r = ld_relaxed_gpu_i(&a.ready[c]);
+                if (r >= 0 && r != acquired) {
+                    r        = ld_acquire_gpu(&a.ready[c]);
+                    acquired = r;
+                }
+                if (r < 0) { // a build another block holds is still running
+                    if (global_ns() - t0 > 30000000000ull) {
+                        atomicOr(status, STATUS_SPIN_LIMIT);
+                        break;
+                    }
+                    __nanosleep(256);
+                    continue;
+                }
+                const int n   = (int)(a.off[r + 1] - a.off[r]);
+                const int nch = (n + 31) >> 5;
+                if (nch > 0) {
+                    const int jj = (int)atomicAdd(reinterpret_cast<uint32_t *>(&a.chunk_next[r]), 1u);
+                    if (jj < nch) {
+                        s = r;
+                        j = jj;
+                        break;
+                    }
+                }
+                atomicCAS(&a.ctl[2], c, c + 1u); // this set has no chunk left
+            }
+        }
+        s = __shfl_sync(0xffffffffu, s, 0);
+        j = __shfl_sync(0xffffffffu, j, 0);
+        __syncwarp();
+        if (s < 0) break; // warp-uniform
+        const int qbase = (int)a.off[s] + j * 32;
+        const int end   = (int)a.off[s + 1];
+        fast_warp<T, PER, KC, 4, NW, true>(qbase, QueryList{}, MissList{}, smem, t_all, bt, nullptr, nullptr, nullptr,
+                                           nullptr, nullptr, end, k, half_window, exclude_self, ret_orig, nullptr,
+                                           out_idx, out_dist, replay_ranks, replay_rows, replay_count, status,
+                                           visit_count);
+    }
+}
+
+template <class T, int PER, int KC, int SFC, int KIND>
+static void launch_persistent_t(Context &ctx, const PersistLaunch &p, const PersistDev<T> &a, const TreeDev<T> &tv,
+                                const BatchDev &bt, cudaStream_t st) {
+    using D               = typename Coord<T>::dist_t;
+    constexpr int NW      = persist_warps<KC>(), PT = 32 * NW;
+    const size_t  heaps   = p.query ? (size_t)std::max(p.k, 1) * PT * (sizeof(heap_dist_t<T>) + 4) : 0;
+    const size_t  sorting = cta_sort_smem<Coord<T>::key_words, PT, kPersistItems>();
+    const size_t  smem    = std::max(heaps, sorting);
+    auto          fn      = batch_persistent_kernel<T, PER, KC, SFC, KIND>;
+    FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    FT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, PT, smem));
+    const int blocks = std::max(1, per_sm) * ctx.num_sms;
+    const int half   = p.k; // the seeding window of the fast walk's default
+    fn<<<blocks, PT, smem, st>>>(a, tv, bt, p.k, half, p.excl ? 1 : 0, ctx.opts.return_orig_indices ? 1 : 0,
+                                 (unsigned long long *)p.idx, (D *)p.dist, p.rr, p.rw, p.counters, ctx.status,
+                                 (unsigned long long *)(p.counters + 2));
+    FT_CUDA(cudaGetLastError());
+}
+
+template <class T, int SFC, int KIND>
+static void persistent_typed(Context &ctx, const PersistLaunch &p, cudaStream_t st) {
+    PersistDev<T> a;
+    a.off = p.off; a.node_off = p.node_off; a.rec_off = p.rec_off; a.S = p.S;
+    a.x = (const T *)p.x; a.y = (const T *)p.y; a.z = (const T *)p.z; a.id = p.id; a.ghost = p.ghost;
+    a.mnx = (T *)p.all.min_x; a.mxx = (T *)p.all.max_x; a.mny = (T *)p.all.min_y;
+    a.mxy = (T *)p.all.max_y; a.mnz = (T *)p.all.min_z; a.mxz = (T *)p.all.max_z;
+    a.left = p.all.left_child; a.right = p.all.right_child; a.parent = p.all.parent;
+    a.tid_out = p.all.id; a.ghost_out = p.all.is_ghost; a.orig = p.all.orig_idx;
+    a.recs = (NodeRec<T> *)p.scr->recs; a.wide = (WideRec<T> *)p.scr->wide; a.height = p.scr->height;
+    a.counters = p.scr->counters; a.leaves = p.scr->leafcount;
+    a.klo = (unsigned long long *)p.scr->key_lo; a.khi = (unsigned long long *)p.scr->key_hi;
+    a.tlo = (unsigned long long *)p.scr->tmp_lo; a.thi = (unsigned long long *)p.scr->tmp_hi;
+    a.perm = p.scr->perm; a.tperm = p.scr->tmp_perm;
+    a.bbox = (T *)p.bbox; a.set_height = p.set_height;
+    a.order = p.order; a.ready = p.ready; a.chunk_next = p.chunk_next; a.ctl = p.ctl;
+    a.query = p.query ? 1 : 0;
+    BatchDev bt;
+    bt.off = p.off; bt.node_off = p.node_off; bt.rec_off = p.rec_off; bt.height = p.set_height; bt.S = p.S;
+    const TreeDev<T> tv = tree_view<T>(p.all);
+    if (!p.query) { // builds only: the smallest block shape's instance
+        launch_persistent_t<T, 0, 32, SFC, KIND>(ctx, p, a, tv, bt, st);
+        return;
+    }
+    met_dispatch<T>(metric_mode<T>(ctx.opts, p.all), [&](auto M) {
+        constexpr int PER = decltype(M)::value;
+        if (p.k <= 32) launch_persistent_t<T, PER, 32, SFC, KIND>(ctx, p, a, tv, bt, st);
+        else launch_persistent_t<T, PER, 64, SFC, KIND>(ctx, p, a, tv, bt, st);
+    });
+}
+
+void batch_persistent(Context &ctx, const PersistLaunch &p, cudaStream_t st) {
+    if (p.query && (p.k < 1 || p.k > 64)) fail(FT_ERR_INVALID_ARGUMENT, "the persistent batched launch serves k <= 64");
+    const bool morton = ctx.opts.sfc_type == MORTON;
+    switch (ctx.opts.coord_type) {
+    case F32:
+        if (morton) persistent_typed<float, MORTON, 0>(ctx, p, st);
+        else persistent_typed<float, PEANO_HILBERT, 1>(ctx, p, st);
+        break;
+    case F64:
+        if (morton) persistent_typed<double, MORTON, 0>(ctx, p, st);
+        else persistent_typed<double, PEANO_HILBERT, 1>(ctx, p, st);
+        break;
+    case U32: // integer positions always take Peano-Hilbert keys; the delta follows build_bvh's
+        if (morton) persistent_typed<uint32_t, MORTON, 0>(ctx, p, st);
+        else persistent_typed<uint32_t, PEANO_HILBERT, 1>(ctx, p, st);
+        break;
+    case U64:
+        if (morton) persistent_typed<unsigned long long, MORTON, 0>(ctx, p, st);
+        else persistent_typed<unsigned long long, PEANO_HILBERT, 2>(ctx, p, st);
+        break;
+    }
 }
 
 } // namespace ft

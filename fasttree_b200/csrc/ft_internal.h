@@ -141,6 +141,7 @@ struct Context {
     cudaEvent_t    ev_copied[2]  = {nullptr, nullptr};
     std::map<unsigned long long, TuneChoice> tuned; // autotuner choices by shape (tune_key)
     BuildProfile   bprof;
+    int            range_walk = 0; // range_query on trees of height <= 62: 0/1 one walk per query, 2 warp-shared
     float         *learned_feats = nullptr; // learned-bound scratch: features and bounds
     void          *learned_bound = nullptr;
     size_t         learned_cap   = 0;
@@ -173,6 +174,34 @@ void batch_self_knn(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t
                     uint64_t *idx, void *dist, bool fast, int half_window, int variant, int32_t *rr, int32_t *rw,
                     uint32_t *counters, cudaStream_t st, const void *bound = nullptr, int32_t *mw = nullptr,
                     int kc = 0);
+// The persistent batched launch (ft_fast.cu): one kernel whose blocks first build whole sets
+// (largest first, one set per block, ft_cta_build.cuh), each published when done, then take
+// chunks of queries of the published sets and walk them (the fast walk; tied queries go to
+// the replay list).  With query == false only the builds run.  The scheduling words (ctl,
+// ready, chunk_next) must be zeroed / set to -1 on the stream before the launch.
+struct PersistLaunch {
+    const long long *off = nullptr, *node_off = nullptr, *rec_off = nullptr; // prepared offsets
+    int              S   = 0;
+    const void      *x = nullptr, *y = nullptr, *z = nullptr;
+    const uint32_t  *id    = nullptr;
+    const int8_t    *ghost = nullptr;
+    ft_tree          all{};        // the batch's node arrays
+    TreeImpl        *scr = nullptr; // records, heights, counters, leaf counts and key buffers
+    void            *bbox       = nullptr; // 6 coordinates per set
+    uint8_t         *set_height = nullptr;
+    const int32_t   *order = nullptr; // build order of the sets (largest first)
+    int32_t         *ready = nullptr; // sets in the order their builds finished (-1: not yet)
+    int32_t         *chunk_next = nullptr;
+    uint32_t        *ctl        = nullptr; // [0] build tickets, [1] ready slots, [2] query cursor
+    bool             query      = true;
+    int              k          = 0;
+    bool             excl       = true;
+    uint64_t        *idx        = nullptr;
+    void            *dist       = nullptr;
+    int32_t         *rr = nullptr, *rw = nullptr;
+    uint32_t        *counters   = nullptr; // [0] replay count, [2..3] visits
+};
+void batch_persistent(Context &ctx, const PersistLaunch &p, cudaStream_t st);
 // The reference traversal over every leaf of a batch (ft_query.cu).
 void batch_self_knn_exact(Context &ctx, const ft_tree &all, const BatchDev &bt, size_t num, int k, bool exclude_self,
                           uint64_t *idx, void *dist, cudaStream_t st);

@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(kFeatThreads)
         t           = set_view(t_all, bt, s);
         parent      = parent_all + bt.node_off[s];
         klo         = klo_all + bt.off[s];
-        khi         = nullptr; // batched sets have one-word keys
+        khi         = khi_all ? khi_all + bt.off[s] : nullptr; // high words: 126-bit keys only
         set_rank    = q - (int)bt.off[s];
     }
     const int  n   = t.n;
@@ -976,6 +976,8 @@ template <class T>
 static void features_typed(Context &ctx, const ft_tree &tr, const int32_t *leaf_ids, int num, int k, const void *qx,
                            const void *qy, const void *qz, float *out, cudaStream_t st, const BatchDev &bt) {
     const TreeImpl &impl = *(const TreeImpl *)tr.impl;
+    if (!impl.key_lo || (Coord<T>::key_words == 2 && !impl.key_hi))
+        fail(FT_ERR_INVALID_ARGUMENT, "learned bound: the tree's sorted keys are missing");
     TreeDev<T>      tv   = tree_view<T>(tr);
     const int       grid = (num + kFeatThreads - 1) / kFeatThreads;
     met_dispatch<T>(metric_mode<T>(ctx.opts, tr), [&](auto M) {

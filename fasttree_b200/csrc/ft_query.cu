@@ -555,39 +555,39 @@ FT_D bool far_dist_box(T px, T py, T pz, const T b[6], typename Coord<T>::dist_t
 // r_max is not pushed; once the row is full a child inside the shell is counted from its leaf
 // count (kept in the parent's record) instead of being walked.  Results are still written in
 // the reference's depth-first, left-first order.
-template <class T, int PER>
-__global__ void __launch_bounds__(128)
-    range_short_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
-                       const T *__restrict__ rmin, const T *__restrict__ rmax, int nq, int32_t *__restrict__ results,
-                       int32_t *__restrict__ counts, int max_per, int ret_orig, const uint32_t *__restrict__ order,
-                       uint32_t *status) {
+// The query's squared shell radii in the walk's distance units (src/hlbvh.hpp:2032-2043).
+template <class T>
+FT_D void range_radii(const T *__restrict__ rmin, const T *__restrict__ rmax, int q, typename Coord<T>::dist_t &rm2,
+                      typename Coord<T>::dist_t &RM2) {
     using C = Coord<T>;
-    using D = typename C::dist_t;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nq) return;
-    const int q = order ? (int)order[i] : i;
-    const int n = t.n;
-    D         rm2, RM2;
     if constexpr (C::is_float) {
-        double a = (double)rmin[q], b = (double)rmax[q];
-        rm2      = __dmul_rn(a, a);
-        RM2      = __dmul_rn(b, b);
+        const double a = (double)rmin[q], b = (double)rmax[q];
+        rm2            = __dmul_rn(a, a);
+        RM2            = __dmul_rn(b, b);
     } else {
-        unsigned long long a = (unsigned long long)rmin[q] >> C::dist_shift;
-        unsigned long long b = (unsigned long long)rmax[q] >> C::dist_shift;
-        rm2                  = a * a;
-        RM2                  = b * b;
+        const unsigned long long a = (unsigned long long)rmin[q] >> C::dist_shift;
+        const unsigned long long b = (unsigned long long)rmax[q] >> C::dist_shift;
+        rm2                        = a * a;
+        RM2                        = b * b;
     }
-    const T      px = qx[q], py = qy[q], pz = qz[q];
-    const size_t off   = (size_t)q * (size_t)max_per;
-    int          count = 0;
-    int          sn[kStack];
-    D            sd[kStack];
-    int          sp = 0;
-    const D      d0 = node_dist_soa<T, PER>(t, 0, px, py, pz);
-    if (d0 <= RM2) {
+}
+
+// One query's range walk on a tree of height <= 62; returns its full count.
+template <class T, int PER>
+FT_D int range_one(const TreeDev<T> &t, T px, T py, T pz, typename Coord<T>::dist_t rm2,
+                   typename Coord<T>::dist_t RM2, int32_t *__restrict__ results, size_t off, int max_per, int ret_orig,
+                   uint32_t *status) {
+    using D     = typename Coord<T>::dist_t;
+    const int n = t.n;
+    int       count = 0;
+    // the stack holds node indices only: a leaf is stacked only when it lies in the shell
+    // (its distance is known when its parent is expanded), an internal node when it is within
+    // r_max, so a popped leaf is always counted
+    int       sn[kStack];
+    int       sp = 0;
+    const D   d0 = node_dist_soa<T, PER>(t, 0, px, py, pz);
+    if (d0 <= RM2 && (n > 1 || d0 >= rm2)) {
         sn[0] = 0;
-        sd[0] = d0;
         sp    = 1;
     }
     long long budget = 2ll * n + 64;
@@ -598,12 +598,9 @@ __global__ void __launch_bounds__(128)
         }
         --sp;
         const int node = sn[sp];
-        const D   d2   = sd[sp];
-        if (node >= n - 1) { // leaf (the n == 1 root included)
-            if (d2 >= rm2) {
-                if (count < max_per) results[off + count] = ret_orig ? t.orig_idx[node] : node - (n - 1);
-                ++count;
-            }
+        if (node >= n - 1) { // leaf in the shell (the n == 1 root included)
+            if (count < max_per) results[off + count] = ret_orig ? t.orig_idx[node] : node - (n - 1);
+            ++count;
             continue;
         }
         T        lb[6], rb[6];
@@ -619,9 +616,10 @@ __global__ void __launch_bounds__(128)
             const D        dc = side ? dr : dl;
             const uint32_t ic = side ? ir : il;
             if (!(dc <= RM2)) continue;
+            if (c >= n - 1 && !(dc >= rm2)) continue; // a leaf inside r_min
             if (full) {
                 if (c >= n - 1) { // a leaf: counted now
-                    if (dc >= rm2) ++count;
+                    ++count;
                     continue;
                 }
                 if (dc >= rm2 && info_leaves(ic) < kInfoCountMax) {
@@ -637,11 +635,187 @@ __global__ void __launch_bounds__(128)
                 break;
             }
             sn[sp] = c;
-            sd[sp] = dc;
             ++sp;
         }
     }
-    counts[q] = count;
+    return count;
+}
+
+template <class T, int PER>
+__global__ void __launch_bounds__(128)
+    range_short_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
+                       const T *__restrict__ rmin, const T *__restrict__ rmax, int nq, int32_t *__restrict__ results,
+                       int32_t *__restrict__ counts, int max_per, int ret_orig, const uint32_t *__restrict__ order,
+                       uint32_t *status) {
+    using D     = typename Coord<T>::dist_t;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    const int q = order ? (int)order[i] : i;
+    D         rm2, RM2;
+    range_radii<T>(rmin, rmax, q, rm2, RM2);
+    counts[q] = range_one<T, PER>(t, qx[q], qy[q], qz[q], rm2, RM2, results, (size_t)q * (size_t)max_per, max_per,
+                                  ret_orig, status);
+}
+
+// range_query on trees of height <= 62, a warp's 32 queries (neighbours in SFC order, so their
+// balls overlap) walking the tree together: one depth-first, left-first walk over the union
+// of the nodes the lanes need, each stack entry carrying the mask of the lanes that need it.
+// Every lane takes exactly the decisions range_short_kernel takes for its query (push a child
+// within r_max; once its row is full, count a leaf child or a child inside the shell from the
+// record instead of walking it), and meets its nodes in the same left-first order, so its
+// row and count are the same; the node type and the record are the warp's, so the lanes
+// diverge far less than in one walk per lane.
+template <class T, int PER>
+__global__ void __launch_bounds__(128)
+    range_group_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
+                       const T *__restrict__ rmin, const T *__restrict__ rmax, int nq, int32_t *__restrict__ results,
+                       int32_t *__restrict__ counts, int max_per, int ret_orig, const uint32_t *__restrict__ order,
+                       uint32_t *status) {
+    using C                = Coord<T>;
+    using D                = typename C::dist_t;
+    constexpr int  kWarps  = 4;
+    const unsigned FULL    = 0xffffffffu;
+    __shared__ int32_t  s_node[kWarps][kStack];
+    __shared__ uint32_t s_mask[kWarps][kStack];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int base = (blockIdx.x * kWarps + warp) * 32;
+    if (base >= nq) return; // warp-uniform
+    const int  i      = base + lane;
+    const bool active = i < nq;
+    const int  q      = active ? (order ? (int)order[i] : i) : 0;
+    const int  n      = t.n;
+    D          rm2 = D(0), RM2 = D(0);
+    if (active) range_radii<T>(rmin, rmax, q, rm2, RM2);
+    const T      px = qx[q], py = qy[q], pz = qz[q];
+    // Walk together only when the lanes' balls overlap: the warp's query points lie within a
+    // box whose diagonal is no longer than the smallest r_max; otherwise (sparse regions, or
+    // points on both sides of a periodic edge) each lane takes its own walk.
+    {
+        const T  p[3] = {px, py, pz};
+        D        span = D(0);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            T lo = p[a], hi = p[a];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const T u = __shfl_xor_sync(FULL, lo, o), w = __shfl_xor_sync(FULL, hi, o);
+                lo        = u < lo ? u : lo;
+                hi        = w > hi ? w : hi;
+            }
+            if constexpr (C::is_float) {
+                const double e = (double)hi - (double)lo;
+                span += e * e;
+            } else {
+                const unsigned long long e = (unsigned long long)(hi - lo) >> C::dist_shift;
+                span += e < (1ull << 31) ? e * e : (1ull << 62);
+            }
+        }
+        D rmin2 = active ? RM2 : dist_heap_max<D>();
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const D u = __shfl_xor_sync(FULL, rmin2, o);
+            rmin2     = u < rmin2 ? u : rmin2;
+        }
+        if (!(span <= rmin2)) { // warp-uniform
+            if (active)
+                counts[q] = range_one<T, PER>(t, px, py, pz, rm2, RM2, results, (size_t)q * (size_t)max_per, max_per,
+                                              ret_orig, status);
+            return;
+        }
+    }
+    const size_t off   = (size_t)q * (size_t)max_per;
+    int          count = 0;
+    D            sd[kStack]; // this lane's distance of each stacked node
+    int          sp = 0;
+    const D      d0 = node_dist_soa<T, PER>(t, 0, px, py, pz);
+    const unsigned m0 = __ballot_sync(FULL, active && d0 <= RM2);
+    if (m0) {
+        if (lane == 0) {
+            s_node[warp][0] = 0;
+            s_mask[warp][0] = m0;
+        }
+        sd[0] = d0;
+        sp    = 1;
+    }
+    __syncwarp();
+    long long budget = 2ll * n + 64;
+    while (sp > 0) {
+        if (--budget < 0) {
+            if (lane == 0) atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+            break;
+        }
+        --sp;
+        const int      node = s_node[warp][sp];
+        const uint32_t mask = s_mask[warp][sp];
+        const bool     in   = (mask >> lane) & 1u;
+        const D        d2   = sd[sp];
+        __syncwarp(); // every lane has read the entry before pushes reuse the slot
+        if (node >= n - 1) { // leaf (the n == 1 root included)
+            if (in && d2 >= rm2) {
+                if (count < max_per) results[off + count] = ret_orig ? t.orig_idx[node] : node - (n - 1);
+                ++count;
+            }
+            continue;
+        }
+        T        lb[6], rb[6];
+        int      l, r;
+        uint32_t il, ir;
+        load_rec_info(t.recs, node, lb, rb, l, r, il, ir);
+        bool need_l = false, need_r = false;
+        D    dl = D(0), dr = D(0);
+        if (in) {
+            dl              = box_dist<T, PER>(px, py, pz, lb);
+            dr              = box_dist<T, PER>(px, py, pz, rb);
+            const bool full = count >= max_per;
+#pragma unroll
+            for (int side = 1; side >= 0; --side) {
+                const int      c  = side ? r : l;
+                const D        dc = side ? dr : dl;
+                const uint32_t ic = side ? ir : il;
+                if (!(dc <= RM2)) continue;
+                if (full) {
+                    if (c >= n - 1) { // a leaf: counted now
+                        if (dc >= rm2) ++count;
+                        continue;
+                    }
+                    if (dc >= rm2 && info_leaves(ic) < kInfoCountMax) {
+                        D far;
+                        if (far_dist_box<T, PER>(px, py, pz, side ? rb : lb, far) && far <= RM2) {
+                            count += (int)info_leaves(ic); // every leaf below lies in the shell
+                            continue;
+                        }
+                    }
+                }
+                if (side) need_r = true;
+                else need_l = true;
+            }
+        }
+        const unsigned mr = __ballot_sync(FULL, need_r), ml = __ballot_sync(FULL, need_l);
+        const int      add = (mr != 0u) + (ml != 0u);
+        if (sp + add > kStack) {
+            if (lane == 0) atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+            break;
+        }
+        // right first on the stack, so the left subtree is walked (and written) first
+        if (mr) {
+            if (lane == 0) {
+                s_node[warp][sp] = r;
+                s_mask[warp][sp] = mr;
+            }
+            sd[sp] = dr;
+            ++sp;
+        }
+        if (ml) {
+            if (lane == 0) {
+                s_node[warp][sp] = l;
+                s_mask[warp][sp] = ml;
+            }
+            sd[sp] = dl;
+            ++sp;
+        }
+        __syncwarp();
+    }
+    if (active) counts[q] = count;
 }
 
 template <class T, int PER>
@@ -1044,7 +1218,7 @@ void knn(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, const 
 template <class T>
 static void range_typed(const ft_options &o, const ft_tree &tr, const void *qx, const void *qy, const void *qz,
                         const void *rmin, const void *rmax, int nq, int32_t *results, int32_t *counts, int max_per,
-                        const uint32_t *order, uint32_t *status, cudaStream_t st) {
+                        const uint32_t *order, uint32_t *status, cudaStream_t st, int walk) {
     TreeDev<T> tv     = tree_view<T>(tr);
     int        blocks = (nq + 127) / 128;
     bool       ro     = o.return_orig_indices != 0;
@@ -1052,7 +1226,9 @@ static void range_typed(const ft_options &o, const ft_tree &tr, const void *qx, 
     const TreeImpl *impl  = (const TreeImpl *)tr.impl;
     const bool      short_walk = impl && impl->height_root >= 0 && impl->height_root <= 62;
     met_dispatch<T>(metric_mode<T>(o, tr), [&](auto M) {
-        auto fn = short_walk ? range_short_kernel<T, decltype(M)::value> : range_kernel<T, decltype(M)::value>;
+        auto fn = !short_walk ? range_kernel<T, decltype(M)::value>
+                  : walk == 2 ? range_group_kernel<T, decltype(M)::value>
+                              : range_short_kernel<T, decltype(M)::value>;
         fn<<<blocks, 128, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz, (const T *)rmin, (const T *)rmax,
                                    nq, results, counts, max_per, ro ? 1 : 0, order, status);
     });
@@ -1066,10 +1242,10 @@ void range(Context &ctx, const ft_tree &tr, const void *qx, const void *qy, cons
     // each query's output is independent of the others: take them in SFC order
     const uint32_t *order = sfc_query_order(ctx, tr, qx, qy, qz, nq, st);
     switch (ctx.opts.coord_type) {
-    case F32: range_typed<float>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, order, ctx.status, st); break;
-    case F64: range_typed<double>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, order, ctx.status, st); break;
-    case U32: range_typed<uint32_t>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, order, ctx.status, st); break;
-    case U64: range_typed<unsigned long long>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, order, ctx.status, st); break;
+    case F32: range_typed<float>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, order, ctx.status, st, ctx.range_walk); break;
+    case F64: range_typed<double>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, order, ctx.status, st, ctx.range_walk); break;
+    case U32: range_typed<uint32_t>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, order, ctx.status, st, ctx.range_walk); break;
+    case U64: range_typed<unsigned long long>(ctx.opts, tr, qx, qy, qz, rmin, rmax, (int)nq, results, counts, max_per, order, ctx.status, st, ctx.range_walk); break;
     }
 }
 

@@ -105,6 +105,11 @@ class Context:
         return {"queries": s.queries, "replayed": s.replayed, "visits": s.reserved[0],
                 "bound_misses": s.reserved[1], "rerun_visits": s.reserved[2]}
 
+    def set_range_walk(self, walk: int):
+        """range_query's walk on trees of height <= 62: 0 default / 1 one walk per query, 2 a
+        warp's queries together when their balls overlap (ft_set_range_walk)."""
+        _call(lib().ft_set_range_walk(self._h, int(walk)))
+
     def profile_builds(self, enable: bool = True):
         """Stage timing of later builds on this context (ft_set_build_profiling)."""
         _call(lib().ft_set_build_profiling(self._h, int(bool(enable))))
@@ -417,19 +422,20 @@ def build_tree(ctx: Context, tree: TreeSoA, sorted_keys, sorted_x=None, sorted_y
     return tree
 
 
-METHODS = {"default": 0, "fast": 1, "plain": 2}  # ft_query_options.method (FT_METHOD_*)
+METHODS = {"default": 0, "fast": 1, "plain": 2, "persistent": 3}  # ft_query_options.method (FT_METHOD_*)
 
 
 def _method(method) -> int:
     """"fast" (the default: the fast walk with exact replay), "plain" (the reference traversal
-    alone) or the C value (FT_METHOD_DEFAULT 0, FT_METHOD_FAST 1, FT_METHOD_PLAIN 2)."""
+    alone), "persistent" (batched build + query in one persistent launch; elsewhere "fast") or
+    the C value (FT_METHOD_DEFAULT 0, FT_METHOD_FAST 1, FT_METHOD_PLAIN 2, FT_METHOD_PERSISTENT 3)."""
     if isinstance(method, str):
         if method not in METHODS:
             raise ValueError(f"method must be one of {sorted(METHODS)}")
         return METHODS[method]
     m = int(method)
-    if m not in (0, 1, 2):
-        raise ValueError("method must be 0 (default), 1 (fast) or 2 (plain)")
+    if m not in (0, 1, 2, 3):
+        raise ValueError("method must be 0 (default), 1 (fast), 2 (plain) or 3 (persistent)")
     return m
 
 

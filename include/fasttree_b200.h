@@ -82,6 +82,9 @@ typedef struct ft_tree {
 #define FT_METHOD_DEFAULT 0 /* the fast walk with exact replay (a zeroed ft_query_options)  */
 #define FT_METHOD_FAST    1 /* the same, named                                             */
 #define FT_METHOD_PLAIN   2 /* the reference traversal and heap alone                       */
+#define FT_METHOD_PERSISTENT 3 /* ft_batch_build_knn: one persistent launch builds every set
+                                  and walks its queries (k <= 64; else its build, then the fast
+                                  walk); other calls treat it as FT_METHOD_FAST               */
 
 /* Per-query-call options (the reference's template parameters and dispatch choices). */
 typedef struct ft_query_options {
@@ -243,6 +246,13 @@ ft_status ft_range(ft_context *ctx, const ft_tree *tree, const void *qx, const v
                    int32_t *results, int32_t *counts, int max_results_per_query,
                    ft_stream_t stream);
 
+/* How ft_range walks trees of height <= 62 on this context: 0 (default) or 1, one walk per
+ * query; 2, the 32 queries of a warp (neighbours in SFC order) walk the union of their nodes
+ * together, each stack entry with the mask of the queries that need it, when their balls
+ * overlap (else one walk each).  Same rows and counts either way.  (Taller trees keep the
+ * reference's walk with its stack guard.) */
+ft_status ft_set_range_walk(ft_context *ctx, int walk);
+
 /* Height of the built tree (root to deepest leaf).  The traversal stack of the reference
  * drops both children of a node popped with 62 entries below it (src/hlbvh.hpp:1152, 1618),
  * which only trees of height >= 63 can reach; on those the fast walk tests each query for
@@ -352,7 +362,10 @@ ft_status ft_batch_self_knn(ft_context *ctx, ft_batch *batch, int k, int exclude
 
 /* ft_batch_build + ft_batch_self_knn as one CUDA graph, captured on the first call with
  * these arguments and replayed by later calls with the same arguments (array contents may
- * change between calls).  Asynchronous. */
+ * change between calls).  With method FT_METHOD_PERSISTENT the graph holds one persistent
+ * kernel instead of the launch sequence: each block builds whole sets (largest first, the
+ * same trees as ft_batch_build), then takes chunks of queries of the finished sets; tied
+ * queries are replayed by a second launch.  Same rows either way.  Asynchronous. */
 ft_status ft_batch_build_knn(ft_context *ctx, ft_batch *batch, const int64_t *set_offsets, size_t num_sets,
                              size_t num_points, const void *x, const void *y, const void *z, const uint32_t *id,
                              const int8_t *is_ghost, int k, int exclude_self, uint64_t *idx_out, void *dist_out,

@@ -216,7 +216,7 @@ def test_bad_offsets_are_reported_and_contained():
 
 def test_rejections():
     with pytest.raises(ValueError):
-        ft.BatchedSets(ft.Context("u64", "ph", periodic=True), 100, 2)
+        ft.BatchedSets(ft.Context("u64", "ph", periodic=True), 100, 0)  # no sets
     ctx = ft.Context("f32", "morton")
     x, y, z, off = make_sets("f32", [10, 20], seed=1)
     b = ft.BatchedSets(ctx, 30, 2)

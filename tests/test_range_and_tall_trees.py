@@ -21,10 +21,12 @@ CASES = [("f32", "morton", False, O.F32, O.MORTON), ("f64", "ph", False, O.F64, 
 
 @pytest.mark.parametrize("coord,sfc,per,oc,os_", CASES, ids=[f"{c[0]}-{c[1]}{'-per' if c[2] else ''}" for c in CASES])
 @pytest.mark.parametrize("r_phys,max_per", [(8.0, 16), (30.0, 64), (60.0, 0), (200.0, 7)])
-def test_range_large_radii_match_oracle(coord, sfc, per, oc, os_, r_phys, max_per):
+@pytest.mark.parametrize("walk", [2, 1], ids=["warp-walk", "lane-walk"])
+def test_range_large_radii_match_oracle(coord, sfc, per, oc, os_, r_phys, max_per, walk):
     n = 6000
     x, y, z = gen("clustered", n, oc, 12)
     ctx = ft.Context(coord, sfc, periodic=per)
+    ctx.set_range_walk(walk)
     tree = ft.TreeSoA(ctx, n)
     ft.build_bvh(ctx, ft.particles(x, y, z), tree)
     opts = O.Options(oc, os_, per)
