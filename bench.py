@@ -144,6 +144,9 @@ def run_batched(args, dev, stream, timed_steps, warmup):
     persist_ms = timed(lambda: bp.build_knn(off, x, y, z, k, pidx, pdst, method="persistent"), timed_steps)
     bp.check()
     pstats = bp.query_stats()
+    bp.set_build_method("persistent")  # its builds alone (the same kernel without the queries)
+    persist_build_ms = timed(lambda: bp.build(off, x, y, z), timed_steps)
+    bp.check()
     del bp
     build_ms = timed(lambda: b.build(off, x, y, z), timed_steps)
     fi, fd = torch.empty_like(idx), torch.empty_like(dst)
@@ -156,7 +159,7 @@ def run_batched(args, dev, stream, timed_steps, warmup):
                  "persistent_vs_plain": rows_equal(pidx, pdst, pi, pd)}
     del fi, fd, pidx, pdst
     persistent = {"ms_per_step": persist_ms, "value": N / (persist_ms / 1e3), "unit": "queries/s",
-                  "replayed": pstats["replayed"],
+                  "replayed": pstats["replayed"], "build_only_ms": persist_build_ms,
                   "note": "ft_batch_build_knn with FT_METHOD_PERSISTENT: prep + order + one persistent kernel "
                           "(per-set builds, then 32-query chunks of finished sets) + replay, one CUDA graph"}
     learned = run_batched_learned(args, ctx, b, off, x, y, z, k, idx, dst, (pi, pd), timed, timed_steps, plain_ms)
@@ -400,22 +403,22 @@ def run_cfg2_extra(args, ctx, tree, x, y, z, n, stream):
     out["range_query"] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s",
                           "mean_count": float(c.mean()), "max_count": int(cnt.max()),
                           "truncated_queries": int((cnt > max_per).sum()), "max_results_per_query": max_per,
-                          "walk": "one walk per query (default)",
+                          "walk": "one walk per query over the 4-wide records (default)",
                           "queries": "the N particle positions in input order (the library walks them in SFC "
                                      "order); one blocking call, including its status check"}
-    # the warp-shared walk (ft_set_range_walk 2) on the first 1M queries: its time, and its
-    # rows and counts against the default walk's
+    # the binary walk (ft_set_range_walk 1) on the first 1M queries: its time, and its rows and
+    # counts against the default walk's
     m = min(n, 1_000_000)
     res1 = torch.empty(m * max_per, dtype=torch.int32, device=dev)
     cnt1 = torch.empty(m, dtype=torch.int32, device=dev)
-    ctx.set_range_walk(2)
+    ctx.set_range_walk(1)
     ms1 = _timed(stream, lambda: ft.range_query(ctx, tree, x[:m], y[:m], z[:m], r0[:m], r1[:m], max_per, res1, cnt1),
                  1, warmup=0)
     ctx.set_range_walk(0)
     valid = torch.arange(max_per, device=dev)[None, :] < cnt1.clamp(max=max_per)[:, None]
     same = bool(torch.equal(cnt1, cnt[:m])) and bool(torch.equal(res1.view(m, max_per)[valid],
                                                                    res.view(n, max_per)[:m][valid]))
-    out["range_query"]["warp_walk_1M"] = {"ms_per_step": ms1, "value": m / (ms1 / 1e3), "unit": "queries/s",
+    out["range_query"]["binary_walk_1M"] = {"ms_per_step": ms1, "value": m / (ms1 / 1e3), "unit": "queries/s",
                                           "rows_and_counts_equal_default": same}
     del res, cnt, res1, cnt1, valid
     # refit-only update (a simulation step): every point moved by N(0, sigma^2) per axis (kept
@@ -580,7 +583,8 @@ def run_profile(args, stream):
     summaries): the build and both self-kNN methods on 2M clustered uint64 points (k = 32),
     range_query on 20K of them, knn_query of 100K external points on 100K uniform float64
     points (k = 64, MAXK = 256, both methods), the learned bound's features and inference,
-    and a batch of 256 Plummer sets (build + fast self-kNN).  Prints what ran."""
+    and a batch of 256 Plummer sets (launch sequence: build + fast self-kNN; then the
+    persistent launch).  Prints what ran."""
     import torch
 
     import fasttree_b200 as ft
@@ -617,6 +621,14 @@ def run_profile(args, stream):
     b.build(boff, bx, by, bz)
     b.self_knn(32)
     b.check()
+    # the same sets through the persistent launch (per-set builds, then query chunks)
+    dbx, dby, dbz = (torch.from_numpy(a).to(dev) for a in (bx, by, bz))
+    dboff = torch.from_numpy(boff).to(dev)
+    pi = torch.empty(len(bx) * 32, dtype=torch.uint64, device=dev)
+    pd = torch.empty(len(bx) * 32, dtype=torch.float64, device=dev)
+    bp = ft.BatchedSets(c3, len(bx), len(sizes))
+    bp.build_knn(dboff, dbx, dby, dbz, 32, pi, pd, method="persistent")
+    bp.check()
     torch.cuda.synchronize()
     return {"workload": "profile", "self_knn_points": n, "range_queries": m, "external_queries": len(qx),
             "batched_sets": len(sizes), "batched_points": len(bx)}

@@ -25,7 +25,7 @@ EXPORTED = (
     "ft_batch_create", "ft_batch_destroy", "ft_batch_build", "ft_batch_self_knn", "ft_batch_build_knn",
     "ft_batch_tree", "ft_batch_set_info", "ft_batch_query_stats", "ft_batch_self_knn_learned",
     "ft_batch_build_knn_learned", "ft_batch_bound_features", "ft_get_replayed_queries",
-    "ft_tune_self_knn", "ft_tune_batch_self_knn", "ft_tune_build", "ft_tune_reset", "ft_set_build_profiling", "ft_set_range_walk",
+    "ft_tune_self_knn", "ft_tune_batch_self_knn", "ft_tune_build", "ft_tune_reset", "ft_set_build_profiling", "ft_set_range_walk", "ft_batch_set_build_method",
     "ft_get_build_profile",
     "ft_bound_model_create", "ft_bound_model_destroy", "ft_bound_model_get_params", "ft_bound_model_set_params",
     "ft_bound_model_set_norm", "ft_bound_features", "ft_bound_targets", "ft_bound_model_gradient",
@@ -120,6 +120,7 @@ _SIGS = {
     "ft_tune_reset": [_vp],
     "ft_set_build_profiling": [_vp, _i],
     "ft_set_range_walk": [_vp, _i],
+    "ft_batch_set_build_method": [_vp, _vp, _i],
     "ft_get_build_profile": [_vp, ctypes.POINTER(FtBuildProfile)],
     "ft_batch_self_knn_learned": [_vp, _vp, _vp, _i, _i, ctypes.c_float, _vp, _vp, ctypes.POINTER(FtQueryOptions),
                                   _st],

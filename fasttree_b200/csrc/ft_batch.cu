@@ -341,6 +341,7 @@ struct BatchImpl {
     cudaStream_t    cap_stream = nullptr;
     cudaGraphExec_t exec       = nullptr;
     GraphKey        key{};
+    bool            per_set_build = false; // ft_batch_build through the persistent launch's per-set builds
 };
 
 template <class T> static T *dalloc(size_t count) {
@@ -580,7 +581,7 @@ static void batch_build_persistent(Context &ctx, BatchImpl &b, const long long *
 
 void batch_build(Context &ctx, BatchImpl &b, const long long *in_off, size_t S, size_t N, const void *x,
                  const void *y, const void *z, const uint32_t *id, const int8_t *ghost, cudaStream_t st) {
-    if (ctx.opts.coord_type == U64) { // 126-bit keys: the per-set builds of the persistent launch
+    if (ctx.opts.coord_type == U64 || b.per_set_build) { // (126-bit keys: always) the per-set builds
         batch_build_persistent(ctx, b, in_off, S, N, x, y, z, id, ghost, nullptr, st);
         return;
     }
@@ -772,6 +773,8 @@ void batch_tune(Context &ctx, BatchImpl &b, int k, bool excl, ft_tune_result *ou
     if (!b.built) fail(FT_ERR_INVALID_ARGUMENT, "the batch has not been built");
     tune_batch_self_knn(ctx, b.all, batch_dev(b), b.N, k, excl, b.rr, b.rw, b.counters, out, st);
 }
+
+void batch_set_build_method(BatchImpl &b, int method) { b.per_set_build = method == FT_METHOD_PERSISTENT; }
 
 void batch_stats(BatchImpl &b, ft_query_stats &out) {
     uint32_t w[8] = {0, 0, 0, 0, 0, 0, 0, 0};

@@ -1078,6 +1078,14 @@ ft_status ft_batch_build(ft_context *ctx, ft_batch *batch, const int64_t *set_of
     FT_API_END
 }
 
+ft_status ft_batch_set_build_method(ft_context *ctx, ft_batch *batch, int method) {
+    FT_API_BEGIN
+    need(ctx && batch, "null argument");
+    need(method >= FT_METHOD_DEFAULT && method <= FT_METHOD_PERSISTENT, "unknown method");
+    ft::batch_set_build_method(*batch->impl, method);
+    FT_API_END
+}
+
 ft_status ft_batch_self_knn(ft_context *ctx, ft_batch *batch, int k, int exclude_self, uint64_t *idx_out,
                             void *dist_out, const ft_query_options *qopts, ft_stream_t stream) {
     FT_API_BEGIN
@@ -1220,7 +1228,8 @@ ft_status ft_tune_build(ft_context *ctx, const void *x, const void *y, const voi
 ft_status ft_set_range_walk(ft_context *ctx, int walk) {
     FT_API_BEGIN
     need(ctx != nullptr, "null context");
-    need(walk >= 0 && walk <= 2, "range walk must be 0 (default), 1 (one walk per query) or 2 (warp-shared)");
+    need(walk >= 0 && walk <= 3, "range walk must be 0 (default), 1 (binary walk per query), 2 (warp-shared) or "
+                                 "3 (4-wide walk per query)");
     ctx->range_walk = walk;
     FT_API_END
 }

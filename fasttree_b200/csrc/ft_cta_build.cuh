@@ -4,7 +4,8 @@
 // The steps and their results are those of build_bvh on the set alone (src/hlbvh.hpp:
 // 2165-2290): the set's bounding box (462-572), its SFC keys (357-423), the keys sorted with
 // their input indices (2202-2232; equal keys in input order), the leaf gather (2266-2279),
-// Karras topology (861-903) and the bottom-up refit (925-969), then this library's 4-wide
+// the Karras topology (861-903) and the bottom-up refit (925-969) -- here one agglomerative
+// climb that yields the same tree, numbering and boxes -- then this library's 4-wide
 // records.  Only the schedule differs: every step runs inside the block, with block barriers
 // between them, over the set's slice of the batch's arrays.  The key sort is a stable LSD
 // radix sort over 8-bit digits whose tiles the block takes in order, so a tile's place in
@@ -215,6 +216,122 @@ FT_D bool cta_sort(unsigned long long *alo, unsigned long long *ahi, uint32_t *a
     return in_b;
 }
 
+// Common-prefix length of the sorted keys at positions x and x + 1: the Karras delta of that
+// adjacent pair (src/hlbvh.hpp:852-859; equal keys compare by index).
+template <int KIND>
+FT_D int adjacent_delta(const unsigned long long *klo, const unsigned long long *khi, int x) {
+    const unsigned long long a = klo[x], b = klo[x + 1];
+    if (KIND == 2) {
+        const unsigned long long ah = khi[x], bh = khi[x + 1];
+        if (ah != bh) return clz64(ah ^ bh) - 2;
+        if (a != b) return 62 + clz64(a ^ b);
+    } else if (a != b) {
+        return clz64(a ^ b) - (KIND == 1 ? 1 : 0);
+    }
+    return (KIND == 2 ? 126 : 63) + clz64((unsigned long long)x ^ (unsigned long long)(x + 1));
+}
+
+// Topology and refit of one set in one bottom-up climb per leaf (the agglomerative form of
+// the binary radix tree, Apetrei 2014).  A node covering leaves [l, r] has its parent on the
+// side whose adjacent delta is larger: at split r (it is the left child) when
+// delta(r) > delta(l - 1), else at split l - 1 (the right child); the two deltas are never
+// equal (between them lie keys sharing a longer prefix).  It is therefore the Karras tree of
+// the same keys, and the climb gives each node the Karras number: a left child [l, r] is
+// internal node r, a right child internal node l, the root 0; a one-leaf range is its leaf.
+// At each split the first arrival leaves its far end in slot[split] (an acquire-release
+// exchange) and stops; the second forms the parent, merges the two boxes in (left, right)
+// order as the refit does (src/hlbvh.hpp:925-969), and climbs on.  Each internal node's
+// children, parent links, box, record, height and leaf count are written by the thread
+// that formed it, before its own exchange, so a sibling that reads them (through L2) after
+// the exchange sees them.  delta: n - 1 adjacent deltas; slot: n - 1 words set to -1.
+template <class T>
+FT_D void climb_build(int j, int n, const int *__restrict__ delta, int *slot, const CtaTreeOut<T> &o) {
+    T *const soa[6] = {o.mnx, o.mxx, o.mny, o.mxy, o.mnz, o.mxz};
+    int      l = j, r = j;
+    T        box[6];
+#pragma unroll
+    for (int d = 0; d < 6; ++d) box[d] = __ldcg(soa[d] + (j + n - 1));
+    int      lc = -1, rc = -1, h = 0; // the current node's children (internal) and height
+    T        lb[6], rb[6];
+    int      hl = 0, hr = 0, nl = 1, nr = 1; // the children's heights and leaf counts
+    for (int steps = 0; steps <= n; ++steps) {
+        const bool root = (l == 0 && r == n - 1);
+        const bool up_right = !root && (l == 0 || (r != n - 1 && delta[r] > delta[l - 1]));
+        const int  ci = (l == r) ? l + n - 1 : root ? 0 : (up_right ? r : l);
+        if (l != r) { // an internal node, formed by this thread: write it out
+            o.left[ci]  = lc;
+            o.right[ci] = rc;
+            o.parent[lc] = ci;
+            o.parent[rc] = ci;
+            o.leaves[ci] = r - l + 1;
+#pragma unroll
+            for (int d = 0; d < 6; ++d) __stcg(soa[d] + ci, box[d]);
+            NodeRec<T> rec;
+#pragma unroll
+            for (int d = 0; d < 6; ++d) {
+                rec.lb[d] = lb[d];
+                rec.rb[d] = rb[d];
+            }
+            rec.l = lc;
+            rec.r = rc;
+#pragma unroll
+            for (int d = 0; d < (int)(sizeof(rec.pad) / 4); ++d) rec.pad[d] = 0;
+            rec.pad[0] = (int32_t)rec_child_info((uint32_t)nl, (uint32_t)hl);
+            rec.pad[1] = (int32_t)rec_child_info((uint32_t)nr, (uint32_t)hr);
+            o.recs[ci] = rec;
+            __stcg(o.height + ci, (uint8_t)min(h, 255));
+        }
+        if (root) return;
+        const int split = up_right ? r : l - 1;
+        int       prev;
+        asm volatile("atom.acq_rel.gpu.global.exch.b32 %0, [%1], %2;"
+                     : "=r"(prev)
+                     : "l"(slot + split), "r"(up_right ? l : r)
+                     : "memory");
+        if (prev < 0) return; // first arrival: the sibling forms the parent
+        // the sibling: [split + 1, prev] on the right, or [prev, split] on the left
+        const int sl = up_right ? split + 1 : prev, sr = up_right ? prev : split;
+        const int si = (sl == sr) ? sl + n - 1 : (up_right ? sl : sr);
+        T         sb[6];
+#pragma unroll
+        for (int d = 0; d < 6; ++d) sb[d] = __ldcg(soa[d] + si);
+        const int sh = (sl == sr) ? 0 : (int)__ldcg(o.height + si);
+        if (up_right) { // this node on the left
+            lc = ci;
+            rc = si;
+#pragma unroll
+            for (int d = 0; d < 6; ++d) {
+                lb[d] = box[d];
+                rb[d] = sb[d];
+            }
+            hl = h;
+            hr = sh;
+            nl = r - l + 1;
+            nr = sr - sl + 1;
+            r  = sr;
+        } else {
+            lc = si;
+            rc = ci;
+#pragma unroll
+            for (int d = 0; d < 6; ++d) {
+                lb[d] = sb[d];
+                rb[d] = box[d];
+            }
+            hl = sh;
+            hr = h;
+            nl = sr - sl + 1;
+            nr = r - l + 1;
+            l  = sl;
+        }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            box[2 * d]     = box_min(lb[2 * d], rb[2 * d]);
+            box[2 * d + 1] = box_max(lb[2 * d + 1], rb[2 * d + 1]);
+        }
+        h = 1 + max(hl, hr);
+    }
+}
+
 // The whole build of one non-empty set of n points by one block of PT threads.
 //  x/y/z/id/ghost: the set's input slices; klo/khi/perm (A) and tlo/thi/tperm (B): the set's
 //  sort buffers -- on return A holds the sorted keys and input indices (as the single-tree
@@ -302,10 +419,9 @@ FT_D void cta_build_set(int n, const T *__restrict__ x, const T *__restrict__ y,
         o.orig[leaf]  = (int32_t)src;
     }
     for (int i = tid; i < n - 1; i += PT) {
-        o.id[i]       = 0u;
-        o.ghost[i]    = (int8_t)0;
-        o.orig[i]     = 0;
-        o.counters[i] = 0;
+        o.id[i]    = 0u;
+        o.ghost[i] = (int8_t)0;
+        o.orig[i]  = 0;
     }
     if (tid == 0) o.parent[0] = -1;
     if (n < 2) {
@@ -313,15 +429,17 @@ FT_D void cta_build_set(int n, const T *__restrict__ x, const T *__restrict__ y,
         __syncthreads();
         return;
     }
-    // 5. topology
-    for (int i = tid; i < n - 1; i += PT)
-        karras_node<KIND>(klo, KW == 2 ? khi : nullptr, n, i, o.left, o.right, o.parent, o.leaves);
+    // 5-6. topology and refit in one climb per leaf: the adjacent deltas (into the sort's
+    // spare buffer), the exchange slots, then the climbs
+    int *delta = reinterpret_cast<int *>(tlo);
+    for (int x = tid; x < n - 1; x += PT) {
+        delta[x]      = adjacent_delta<KIND>(klo, KW == 2 ? khi : nullptr, x);
+        o.counters[x] = -1;
+    }
     __syncthreads();
-    // 6. refit, one climb per leaf (first arrival stops, second merges)
+    for (int j = tid; j < n; j += PT) climb_build<T>(j, n, delta, o.counters, o);
+    __syncthreads();
     T *const soa[6] = {o.mnx, o.mxx, o.mny, o.mxy, o.mnz, o.mxz};
-    for (int j = tid; j < n; j += PT)
-        refit_leaf<T>(j, n, o.left, o.right, o.parent, soa, o.recs, o.height, o.counters, o.leaves);
-    __syncthreads();
     // 7. 4-wide records (boxes read through L2, where the refit wrote them)
     for (int v = tid; v < n - 1; v += PT) {
         int       ch[4] = {-1, -1, -1, -1};

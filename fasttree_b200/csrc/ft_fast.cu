@@ -1464,9 +1464,15 @@ bool fast_self_knn_noalloc(Context &ctx, const ft_tree &tr, const int32_t *leaf_
 // Two-warp blocks, the standalone walk's shape: the heaps take the same shared memory per
 // warp, so as many warps fit on an SM (18 with k <= 32 heaps); a block builds its sets with
 // its 64 threads.
-template <int KC> constexpr int persist_warps() { return 2; }
-template <int KC> constexpr int persist_blocks_per_sm() { return KC > 32 ? 4 : 9; }
-static constexpr int kPersistItems = 8; // keys per thread of a sort tile
+// Block shape: as many warps per SM as the standalone walk's heaps allow (28 for k <= 32 with
+// 8-byte heap entries, 16 with 12-byte ones), in blocks as large as that allows, because a
+// block builds a whole set and the largest sets' builds (latency-bound climbs and searches)
+// set the launch's tail: 4 warps a block for float coordinates, 8 otherwise.
+template <class T> constexpr int persist_warps() { return sizeof(heap_dist_t<T>) == 4 ? 4 : 8; }
+template <class T, int KC> constexpr int persist_blocks_per_sm() {
+    return sizeof(heap_dist_t<T>) == 4 ? (KC > 32 ? 3 : 7) : (KC > 32 ? 1 : 2);
+}
+static constexpr int kPersistItems = 4; // keys per thread of a sort tile
 
 template <class T> struct PersistDev {
     const long long *off, *node_off, *rec_off;
@@ -1518,12 +1524,12 @@ FT_D uint32_t ld_relaxed_gpu(const uint32_t *p) {
 }
 
 template <class T, int PER, int KC, int SFC, int KIND>
-__global__ void __launch_bounds__(32 * persist_warps<KC>(), persist_blocks_per_sm<KC>())
+__global__ void __launch_bounds__(32 * persist_warps<T>(), persist_blocks_per_sm<T, KC>())
     batch_persistent_kernel(PersistDev<T> a, TreeDev<T> t_all, BatchDev bt, int k, int half_window,
                             int exclude_self, int ret_orig, unsigned long long *out_idx,
                             typename Coord<T>::dist_t *out_dist, int32_t *replay_ranks, int32_t *replay_rows,
                             uint32_t *replay_count, uint32_t *status, unsigned long long *visit_count) {
-    constexpr int NW = persist_warps<KC>(), PT = 32 * NW;
+    constexpr int NW = persist_warps<T>(), PT = 32 * NW;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_item;
     const int      tid = threadIdx.x;
@@ -1635,7 +1641,7 @@ template <class T, int PER, int KC, int SFC, int KIND>
 static void launch_persistent_t(Context &ctx, const PersistLaunch &p, const PersistDev<T> &a, const TreeDev<T> &tv,
                                 const BatchDev &bt, cudaStream_t st) {
     using D               = typename Coord<T>::dist_t;
-    constexpr int NW      = persist_warps<KC>(), PT = 32 * NW;
+    constexpr int NW      = persist_warps<T>(), PT = 32 * NW;
     const size_t  heaps   = p.query ? (size_t)std::max(p.k, 1) * PT * (sizeof(heap_dist_t<T>) + 4) : 0;
     const size_t  sorting = cta_sort_smem<Coord<T>::key_words, PT, kPersistItems>();
     const size_t  smem    = std::max(heaps, sorting);

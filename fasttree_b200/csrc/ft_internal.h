@@ -141,7 +141,7 @@ struct Context {
     cudaEvent_t    ev_copied[2]  = {nullptr, nullptr};
     std::map<unsigned long long, TuneChoice> tuned; // autotuner choices by shape (tune_key)
     BuildProfile   bprof;
-    int            range_walk = 0; // range_query on trees of height <= 62: 0/1 one walk per query, 2 warp-shared
+    int            range_walk = 0; // range_query, trees of height <= 62: 0 default, 1 binary, 2 warp-shared, 3 4-wide
     float         *learned_feats = nullptr; // learned-bound scratch: features and bounds
     void          *learned_bound = nullptr;
     size_t         learned_cap   = 0;
@@ -294,6 +294,10 @@ inline size_t wide_bytes(int coord) { return coord_bytes(coord) == 8 ? 208 : 112
 struct BatchImpl;
 BatchImpl *batch_create(Context &ctx, size_t max_points, size_t max_sets);
 void       batch_free(BatchImpl *b);
+// ft_batch_build's method: FT_METHOD_PERSISTENT builds every set in one block (the
+// persistent launch without its queries), otherwise the launch sequence (126-bit keys always
+// take the per-set builds).
+void batch_set_build_method(BatchImpl &b, int method);
 // set_offsets: device, S + 1 entries.  Asynchronous; no allocation, no host synchronisation.
 void batch_build(Context &ctx, BatchImpl &b, const long long *set_offsets, size_t S, size_t N, const void *x,
                  const void *y, const void *z, const uint32_t *id, const int8_t *ghost, cudaStream_t st);

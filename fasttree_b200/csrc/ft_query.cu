@@ -641,6 +641,94 @@ FT_D int range_one(const TreeDev<T> &t, T px, T py, T pz, typename Coord<T>::dis
     return count;
 }
 
+// One query's range walk over the 4-wide records (trees of height <= 62 whose box distance
+// is monotone over nested boxes): each expansion judges up to four grandchildren at once,
+// and they are stacked rightmost first, so the walk stays depth-first and left-first and
+// writes the row in the reference's order.  Skipping the binary level between is exact here:
+// a grandchild beyond r_max has a parent beyond it too, and the reference prunes there.  Once
+// the row is full, a leaf is counted at once and an internal grandchild inside the shell is
+// counted from its leaf count.
+template <class T, int PER>
+FT_D int range_one_wide(const TreeDev<T> &t, T px, T py, T pz, typename Coord<T>::dist_t rm2,
+                        typename Coord<T>::dist_t RM2, int32_t *__restrict__ results, size_t off, int max_per,
+                        int ret_orig, uint32_t *status) {
+    using D     = typename Coord<T>::dist_t;
+    const int n = t.n;
+    int       count = 0;
+    int       sn[kStack * 2];
+    int       sp = 0;
+    const D   d0 = node_dist_soa<T, PER>(t, 0, px, py, pz);
+    if (d0 <= RM2 && (n > 1 || d0 >= rm2)) {
+        sn[0] = 0;
+        sp    = 1;
+    }
+    long long budget = 2ll * n + 64;
+    while (sp > 0) {
+        if (--budget < 0) {
+            atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+            break;
+        }
+        const int node = sn[--sp];
+        if (node >= n - 1) { // leaf in the shell (the n == 1 root included)
+            if (count < max_per) results[off + count] = ret_orig ? t.orig_idx[node] : node - (n - 1);
+            ++count;
+            continue;
+        }
+        T   bx[4][6];
+        int ch[4];
+        load_wide(t.wide, node, bx, ch);
+        D d[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) d[i] = ch[i] >= 0 ? box_dist<T, PER>(px, py, pz, bx[i]) : D(0);
+        const bool full = count >= max_per;
+        bool       over = false;
+#pragma unroll
+        for (int i = 3; i >= 0; --i) {
+            const int c = ch[i];
+            if (c < 0 || !(d[i] <= RM2)) continue;
+            if (c >= n - 1) {             // a leaf
+                if (!(d[i] >= rm2)) continue; // inside r_min
+                if (full) {
+                    ++count;
+                    continue;
+                }
+            } else if (full && d[i] >= rm2) {
+                D far;
+                if (far_dist_box<T, PER>(px, py, pz, bx[i], far) && far <= RM2) {
+                    count += t.leaves[c]; // every leaf below lies in the shell
+                    continue;
+                }
+            }
+            if (sp >= kStack * 2) {
+                over = true;
+                break;
+            }
+            sn[sp++] = c;
+        }
+        if (over) {
+            atomicOr(status, STATUS_TRAVERSAL_LIMIT);
+            break;
+        }
+    }
+    return count;
+}
+
+template <class T, int PER>
+__global__ void __launch_bounds__(128)
+    range_wide_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
+                      const T *__restrict__ rmin, const T *__restrict__ rmax, int nq, int32_t *__restrict__ results,
+                      int32_t *__restrict__ counts, int max_per, int ret_orig, const uint32_t *__restrict__ order,
+                      uint32_t *status) {
+    using D     = typename Coord<T>::dist_t;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    const int q = order ? (int)order[i] : i;
+    D         rm2, RM2;
+    range_radii<T>(rmin, rmax, q, rm2, RM2);
+    counts[q] = range_one_wide<T, PER>(t, qx[q], qy[q], qz[q], rm2, RM2, results, (size_t)q * (size_t)max_per,
+                                       max_per, ret_orig, status);
+}
+
 template <class T, int PER>
 __global__ void __launch_bounds__(128)
     range_short_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
@@ -1225,10 +1313,14 @@ static void range_typed(const ft_options &o, const ft_tree &tr, const void *qx, 
     // trees of height <= 62 never reach the reference's stack guard (range_short_kernel)
     const TreeImpl *impl  = (const TreeImpl *)tr.impl;
     const bool      short_walk = impl && impl->height_root >= 0 && impl->height_root <= 62;
+    // the 4-wide walk skips the binary level between a node and its grandchildren, exact when
+    // the box distance is monotone over nested boxes (the fast walks' condition)
+    const bool      wide = impl && fast_walk_applies(o, *impl);
     met_dispatch<T>(metric_mode<T>(o, tr), [&](auto M) {
         auto fn = !short_walk ? range_kernel<T, decltype(M)::value>
                   : walk == 2 ? range_group_kernel<T, decltype(M)::value>
-                              : range_short_kernel<T, decltype(M)::value>;
+                  : (walk == 1 || !wide) ? range_short_kernel<T, decltype(M)::value>
+                                         : range_wide_kernel<T, decltype(M)::value>;
         fn<<<blocks, 128, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz, (const T *)rmin, (const T *)rmax,
                                    nq, results, counts, max_per, ro ? 1 : 0, order, status);
     });

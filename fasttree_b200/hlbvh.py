@@ -106,8 +106,9 @@ class Context:
                 "bound_misses": s.reserved[1], "rerun_visits": s.reserved[2]}
 
     def set_range_walk(self, walk: int):
-        """range_query's walk on trees of height <= 62: 0 default / 1 one walk per query, 2 a
-        warp's queries together when their balls overlap (ft_set_range_walk)."""
+        """range_query's walk on trees of height <= 62 (ft_set_range_walk): 0 default (4-wide
+        walk per query where it applies), 1 binary walk per query, 2 a warp's queries together
+        when their balls overlap, 3 4-wide walk per query."""
         _call(lib().ft_set_range_walk(self._h, int(walk)))
 
     def profile_builds(self, enable: bool = True):
@@ -591,6 +592,11 @@ class BatchedSets:
             ids = ids.to(f"cuda:{self.ctx.device}").contiguous()
         gh = None if is_ghost is None else self._device(is_ghost, torch.int8)
         return off, xyz, ids, gh
+
+    def set_build_method(self, method="default"):
+        """How build() builds the sets: "persistent" (each set whole in one thread block) or
+        "default" (the launch sequence); ft_batch_set_build_method."""
+        _call(lib().ft_batch_set_build_method(self.ctx.handle, self._h, _method(method)))
 
     def build(self, set_offsets, pos_x, pos_y, pos_z, id=None, is_ghost=None, stream=None):
         off, xyz, ids, gh = self._inputs(set_offsets, pos_x, pos_y, pos_z, id, is_ghost)

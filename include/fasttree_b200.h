@@ -246,11 +246,13 @@ ft_status ft_range(ft_context *ctx, const ft_tree *tree, const void *qx, const v
                    int32_t *results, int32_t *counts, int max_results_per_query,
                    ft_stream_t stream);
 
-/* How ft_range walks trees of height <= 62 on this context: 0 (default) or 1, one walk per
- * query; 2, the 32 queries of a warp (neighbours in SFC order) walk the union of their nodes
- * together, each stack entry with the mask of the queries that need it, when their balls
- * overlap (else one walk each).  Same rows and counts either way.  (Taller trees keep the
- * reference's walk with its stack guard.) */
+/* How ft_range walks trees of height <= 62 on this context: 0 (default), one walk per query
+ * over the 4-wide records (the binary records where the box distance is not monotone); 1, one
+ * walk per query over the binary records; 2, the 32 queries of a warp (neighbours in SFC
+ * order) walk the union of their nodes together, each stack entry with the mask of the
+ * queries that need it, when their balls overlap (else one walk each); 3, the 4-wide walk
+ * where it applies.  Same rows and counts either way.  (Taller trees keep the reference's
+ * walk with its stack guard.) */
 ft_status ft_set_range_walk(ft_context *ctx, int walk);
 
 /* Height of the built tree (root to deepest leaf).  The traversal stack of the reference
@@ -352,6 +354,12 @@ ft_status ft_batch_destroy(ft_context *ctx, ft_batch *batch);
 ft_status ft_batch_build(ft_context *ctx, ft_batch *batch, const int64_t *set_offsets, size_t num_sets,
                          size_t num_points, const void *x, const void *y, const void *z, const uint32_t *id,
                          const int8_t *is_ghost, ft_stream_t stream);
+
+/* How ft_batch_build builds the sets: FT_METHOD_PERSISTENT, each set whole in one thread
+ * block (the persistent launch's builds, without its queries; the trees are the same);
+ * otherwise the launch sequence over all points.  Batches of 64-bit integer positions
+ * (126-bit keys) always take the per-set builds. */
+ft_status ft_batch_set_build_method(ft_context *ctx, ft_batch *batch, int method);
 
 /* self_knn_query<MAXK> of every set: row j (set s = the set holding j) is leaf j - off[s] of
  * set s; indices are that set's leaf ranks (or input indices within the set with

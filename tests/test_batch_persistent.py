@@ -217,3 +217,27 @@ def test_persistent_bad_offsets_are_reported_and_contained():
             persistent(ctx, x, y, z, bad, 4)
     b, gi, gd, _ = persistent(ctx, x, y, z, off, 4)  # a fresh batch with good offsets works
     assert b.query_stats()["queries"] == len(x)
+
+
+@pytest.mark.parametrize("coord,sfc,periodic", [("f32", "morton", False), ("u32", "ph", True)])
+def test_per_set_build_method(coord, sfc, periodic):
+    """ft_batch_set_build_method(FT_METHOD_PERSISTENT): ft_batch_build through the per-set
+    builds gives the launch sequence's trees, and the batched queries on them its rows."""
+    ctx = ft.Context(coord, sfc, periodic=periodic)
+    x, y, z, off = make_sets(coord, SIZES, seed=23)
+    seq = ft.BatchedSets(ctx, len(x), len(SIZES))
+    seq.build(off, x, y, z)
+    per = ft.BatchedSets(ctx, len(x), len(SIZES))
+    per.set_build_method("persistent")
+    per.build(off, x, y, z)
+    per.check()
+    for s, n in enumerate(SIZES):
+        if n == 0:
+            continue
+        got, want = per.tree(s).to_numpy(), seq.tree(s).to_numpy()
+        for name in TREE_ARRAYS:
+            assert np.array_equal(got[name].view(np.uint8), want[name].view(np.uint8)), (s, name)
+    a = per.self_knn(32, method="fast")
+    b = seq.self_knn(32, method="plain")
+    torch.cuda.synchronize()
+    assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])

@@ -21,7 +21,7 @@ CASES = [("f32", "morton", False, O.F32, O.MORTON), ("f64", "ph", False, O.F64, 
 
 @pytest.mark.parametrize("coord,sfc,per,oc,os_", CASES, ids=[f"{c[0]}-{c[1]}{'-per' if c[2] else ''}" for c in CASES])
 @pytest.mark.parametrize("r_phys,max_per", [(8.0, 16), (30.0, 64), (60.0, 0), (200.0, 7)])
-@pytest.mark.parametrize("walk", [2, 1], ids=["warp-walk", "lane-walk"])
+@pytest.mark.parametrize("walk", [0, 1, 2], ids=["default-walk", "binary-walk", "warp-walk"])
 def test_range_large_radii_match_oracle(coord, sfc, per, oc, os_, r_phys, max_per, walk):
     n = 6000
     x, y, z = gen("clustered", n, oc, 12)
