@@ -672,7 +672,10 @@ void batch_build_query_graph(Context &ctx, BatchImpl &b, const long long *in_off
         FT_CUDA(cudaStreamBeginCapture(b.cap_stream, cudaStreamCaptureModeRelaxed));
         cudaGraph_t graph = nullptr;
         try {
-            if (q.method == FT_METHOD_PERSISTENT && !model && k >= 1 && k <= 64) {
+            // the persistent launch is the default for the fast walk's k (measured faster than
+            // the launch sequence on the 4096-set workload); FT_METHOD_FAST names the sequence
+            const bool persistent = q.method == FT_METHOD_PERSISTENT || q.method == FT_METHOD_DEFAULT;
+            if (persistent && !model && k >= 1 && k <= 64) {
                 check_query_args(k, q);
                 PersistQuery pq;
                 pq.k    = k;

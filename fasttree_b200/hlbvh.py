@@ -619,10 +619,11 @@ class BatchedSets:
         return _rows(results, N, k), _rows(result_dists, N, k)
 
     def build_knn(self, set_offsets, pos_x, pos_y, pos_z, k: int, results, result_dists, exclude_self=True,
-                  max_k: int = 32, method="fast", id=None, is_ghost=None, stream=None):
+                  max_k: int = 32, method="default", id=None, is_ghost=None, stream=None):
         """build + self_knn as one CUDA graph (captured on the first call with these arrays, replayed
-        afterwards).  The arrays must stay alive and in place between calls: pass device tensors
-        of the right dtype, which are used as they are."""
+        afterwards): "default" / "persistent", one persistent launch (k <= 64); "fast" / "plain",
+        the launch sequence.  The arrays must stay alive and in place between calls: pass device
+        tensors of the right dtype, which are used as they are."""
         off, xyz, ids, gh = self._inputs(set_offsets, pos_x, pos_y, pos_z, id, is_ghost)
         S, N = off.numel() - 1, xyz[0].numel()
         _call(lib().ft_batch_build_knn(self.ctx.handle, self._h, _ptr(off), S, N, *[_ptr(a) for a in xyz],

@@ -84,7 +84,9 @@ typedef struct ft_tree {
 #define FT_METHOD_PLAIN   2 /* the reference traversal and heap alone                       */
 #define FT_METHOD_PERSISTENT 3 /* ft_batch_build_knn: one persistent launch builds every set
                                   and walks its queries (k <= 64; else its build, then the fast
-                                  walk); other calls treat it as FT_METHOD_FAST               */
+                                  walk) -- also what FT_METHOD_DEFAULT does there, while
+                                  FT_METHOD_FAST selects the launch sequence; other calls
+                                  treat it as FT_METHOD_FAST                                  */
 
 /* Per-query-call options (the reference's template parameters and dispatch choices). */
 typedef struct ft_query_options {
@@ -217,6 +219,9 @@ ft_status ft_self_knn(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_
  * is FT_ERR_INVALID_ARGUMENT.  The first call on a device looks up that array's address;
  * make it before any stream capture.  All calls share the array: calls that overlap on the
  * GPU race and must be serialised by the caller.  leaf_ids, idx_out, dist_out: device.
+ * The walk keeps a per-thread stack in local memory, and the first launch on a device may
+ * make the driver enlarge its local-memory reservation: make one call before giving the
+ * rest of the GPU's memory to a pool.
  * Asynchronous on stream; errors from the kernels surface in ft_check_device_status. */
 ft_status ft_self_knn_noalloc(ft_context *ctx, const ft_tree *tree, const int32_t *leaf_ids, size_t num,
                               int k, int exclude_self, uint64_t *idx_out, void *dist_out, ft_stream_t stream);
@@ -370,10 +375,12 @@ ft_status ft_batch_self_knn(ft_context *ctx, ft_batch *batch, int k, int exclude
 
 /* ft_batch_build + ft_batch_self_knn as one CUDA graph, captured on the first call with
  * these arguments and replayed by later calls with the same arguments (array contents may
- * change between calls).  With method FT_METHOD_PERSISTENT the graph holds one persistent
- * kernel instead of the launch sequence: each block builds whole sets (largest first, the
- * same trees as ft_batch_build), then takes chunks of queries of the finished sets; tied
- * queries are replayed by a second launch.  Same rows either way.  Asynchronous. */
+ * change between calls).  With method FT_METHOD_DEFAULT or FT_METHOD_PERSISTENT (and k <= 64)
+ * the graph holds one persistent kernel: each block builds whole sets (largest first, the
+ * same trees as ft_batch_build), then its warps take chunks of queries of the finished sets;
+ * tied queries are replayed by a second launch.  FT_METHOD_FAST / FT_METHOD_PLAIN select the
+ * launch sequence (ft_batch_build, then ft_batch_self_knn).  Same rows either way.
+ * Asynchronous. */
 ft_status ft_batch_build_knn(ft_context *ctx, ft_batch *batch, const int64_t *set_offsets, size_t num_sets,
                              size_t num_points, const void *x, const void *y, const void *z, const uint32_t *id,
                              const int8_t *is_ghost, int k, int exclude_self, uint64_t *idx_out, void *dist_out,

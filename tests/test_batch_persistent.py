@@ -241,3 +241,24 @@ def test_per_set_build_method(coord, sfc, periodic):
     b = seq.self_knn(32, method="plain")
     torch.cuda.synchronize()
     assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
+
+
+def test_default_build_knn_is_the_persistent_launch():
+    """ft_batch_build_knn's default method runs the persistent launch for k <= 64 (the launch
+    sequence with FT_METHOD_FAST); both give the plain batched traversal's rows."""
+    ctx = ft.Context("f32", "morton")
+    x, y, z, off = make_sets("f32", SIZES, seed=29)
+    N, k = len(x), 16
+    dx, dy, dz = (torch.as_tensor(a, device="cuda") for a in (x, y, z))
+    doff = torch.as_tensor(off, device="cuda")
+    ref = ft.BatchedSets(ctx, N, len(SIZES))
+    ref.build(doff, dx, dy, dz)
+    pi, pd = ref.self_knn(k, method="plain")
+    for method in ("default", "fast"):
+        b = ft.BatchedSets(ctx, N, len(SIZES))
+        gi = torch.empty(N * k, dtype=torch.uint64, device="cuda")
+        gd = torch.empty(N * k, dtype=torch.float64, device="cuda")
+        b.build_knn(doff, dx, dy, dz, k, gi, gd, method=method)
+        torch.cuda.synchronize()
+        b.check()
+        assert torch.equal(gi.view(N, k), pi) and torch.equal(gd.view(N, k), pd), method
