@@ -412,21 +412,23 @@ def run_cfg2_extra(args, ctx, tree, x, y, z, n, stream):
                           "walk": "one walk per query over the 4-wide records (default)",
                           "queries": "the N particle positions in input order (the library walks them in SFC "
                                      "order); one blocking call, including its status check"}
-    # the binary walk (ft_set_range_walk 1) on the first 1M queries: its time, and its rows and
-    # counts against the default walk's
+    # the binary walk (ft_set_range_walk 1) and the warp-shared walk (2) on the first 1M
+    # queries: their times, and their rows and counts against the default walk's
     m = min(n, 1_000_000)
     res1 = torch.empty(m * max_per, dtype=torch.int32, device=dev)
     cnt1 = torch.empty(m, dtype=torch.int32, device=dev)
-    ctx.set_range_walk(1)
-    ms1 = _timed(stream, lambda: ft.range_query(ctx, tree, x[:m], y[:m], z[:m], r0[:m], r1[:m], max_per, res1, cnt1),
-                 1, warmup=0)
-    ctx.set_range_walk(0)
-    valid = torch.arange(max_per, device=dev)[None, :] < cnt1.clamp(max=max_per)[:, None]
-    same = bool(torch.equal(cnt1, cnt[:m])) and bool(torch.equal(res1.view(m, max_per)[valid],
-                                                                   res.view(n, max_per)[:m][valid]))
-    out["range_query"]["binary_walk_1M"] = {"ms_per_step": ms1, "value": m / (ms1 / 1e3), "unit": "queries/s",
-                                          "rows_and_counts_equal_default": same}
-    del res, cnt, res1, cnt1, valid
+    for walk, name in ((1, "binary_walk_1M"), (2, "warp_walk_1M")):
+        ctx.set_range_walk(walk)
+        ms1 = _timed(stream, lambda: ft.range_query(ctx, tree, x[:m], y[:m], z[:m], r0[:m], r1[:m], max_per, res1,
+                                                    cnt1), 1, warmup=0)
+        ctx.set_range_walk(0)
+        valid = torch.arange(max_per, device=dev)[None, :] < cnt1.clamp(max=max_per)[:, None]
+        same = bool(torch.equal(cnt1, cnt[:m])) and bool(torch.equal(res1.view(m, max_per)[valid],
+                                                                       res.view(n, max_per)[:m][valid]))
+        out["range_query"][name] = {"ms_per_step": ms1, "value": m / (ms1 / 1e3), "unit": "queries/s",
+                                    "rows_and_counts_equal_default": same}
+        del valid
+    del res, cnt, res1, cnt1
     # refit-only update (a simulation step): every point moved by N(0, sigma^2) per axis (kept
     # inside the 2^40 box), refit on the kept topology, then the fast self-kNN (k=32) on the
     # refit tree against a rebuild of the moved points.  sigma = 1e-6 of the box is a fraction

@@ -21,7 +21,7 @@ CASES = [("f32", "morton", False, O.F32, O.MORTON), ("f64", "ph", False, O.F64, 
 
 @pytest.mark.parametrize("coord,sfc,per,oc,os_", CASES, ids=[f"{c[0]}-{c[1]}{'-per' if c[2] else ''}" for c in CASES])
 @pytest.mark.parametrize("r_phys,max_per", [(8.0, 16), (30.0, 64), (60.0, 0), (200.0, 7)])
-@pytest.mark.parametrize("walk", [0, 1, 2], ids=["default-walk", "binary-walk", "warp-walk"])
+@pytest.mark.parametrize("walk", [0, 1, 2, 3], ids=["default-walk", "binary-walk", "warp-walk", "wide-walk"])
 def test_range_large_radii_match_oracle(coord, sfc, per, oc, os_, r_phys, max_per, walk):
     n = 6000
     x, y, z = gen("clustered", n, oc, 12)
@@ -188,3 +188,31 @@ def test_tall_set_in_a_batch():
             oi, od = O.self_knn(opts, ot, k)
             assert np.array_equal(fi[a:e].cpu().numpy(), oi), (k, s)
             assert np.array_equal(dist_bits(fd[a:e].cpu().numpy()), dist_bits(od)), (k, s)
+
+
+@pytest.mark.parametrize("coord,sfc,per,oc,os_", [("f64", "morton", False, O.F64, O.MORTON),
+                                                   ("u64", "ph", True, O.U64, O.PEANO_HILBERT)],
+                         ids=["f64-morton", "u64-ph-per"])
+@pytest.mark.parametrize("walk", [0, 1], ids=["default-walk", "binary-walk"])
+def test_range_counts_of_large_balls_match_oracle(coord, sfc, per, oc, os_, walk):
+    """Balls of 10% of 400K points: long count-only tails after the rows fill up, counted from
+    whole subtrees inside the shell; rows and counts bit for bit."""
+    n = 400_000
+    x, y, z = gen("uniform", n, oc, 5)
+    ctx = ft.Context(coord, sfc, periodic=per)
+    ctx.set_range_walk(walk)
+    tree = ft.TreeSoA(ctx, n)
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree)
+    opts = O.Options(oc, os_, per)
+    ot = O.build_bvh(opts, x, y, z)
+    q = [a[:160].copy() for a in (x, y, z)]
+    r0 = np.zeros(160, q[0].dtype)
+    r1 = np.full(160, radius(29.0, oc), q[0].dtype)
+    r0[:40] = radius(10.0, oc)
+    gr, gc = ft.range_query(ctx, tree, *q, r0, r1, 32)
+    orr, oc_ = O.range_query(opts, ot, *q, r0, r1, 32)
+    assert np.array_equal(gc.cpu().numpy(), oc_)
+    g = gr.cpu().numpy()
+    for i in range(160):
+        m = min(int(oc_[i]), 32)
+        assert np.array_equal(g[i, :m], orr[i, :m]), i
