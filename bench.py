@@ -781,14 +781,39 @@ def run_reference(args):
         times.append(time.perf_counter() - t0)
     t = sum(times) / len(times)
     v = sample / t
+    compiled = reference_compiled_rate(opts, tree, ids, args.k, nthreads)
+    if compiled:
+        compiled["port_over_compiled"] = v / compiled["value"]
     out = {"impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": w["dtype"], "data": "synthetic",
            "config": {"workload": w["name"], "n_points": w["n"], "k": args.k, "exclude_self": True},
            "cpu_baseline": {"value": v, "unit": "queries/s", "cores": nthreads, "kind": "port",
                             "sample": f"{sample} evenly spaced leaf queries per step on the full tree"},
-           "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+           "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "reference_compiled": compiled}
     print(json.dumps(out), flush=True)
+
+
+def reference_compiled_rate(opts, tree, ids, k, nthreads):
+    """The reference's own self-kNN code (its headers compiled on the host against this
+    project's SYCL stand-in, oracle/_ref; work-groups run as fibers, OpenMP over them) on the
+    first 20K queries of the same sample, on the same tree: its queries/s and rows against the
+    timed port's.  None when the compiled reference is not on this machine."""
+    from oracle import oracle as O
+    from oracle import reference as R
+    if not R.available(opts):
+        return None
+    sub = ids[:20_000]
+    R.self_knn(opts, tree, k, True, leaf_ids=sub[:1000])
+    t0 = time.perf_counter()
+    ri, rd = R.self_knn(opts, tree, k, True, leaf_ids=sub)
+    t = time.perf_counter() - t0
+    oi, od = O.self_knn(opts, tree, k, True, leaf_ids=sub)
+    same = bool(np.array_equal(ri, oi) and np.array_equal(rd.view(np.uint64) if rd.dtype == np.float64 else rd,
+                                                          od.view(np.uint64) if od.dtype == np.float64 else od))
+    return {"value": len(sub) / t, "unit": "queries/s", "cores": nthreads, "sample": f"{len(sub)} queries",
+            "rows_equal_port": same}
 
 
 def run_ours(args):
