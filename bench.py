@@ -409,15 +409,21 @@ def run_cfg2_extra(args, ctx, tree, x, y, z, n, stream):
     out["range_query"] = {"ms_per_step": ms, "value": n / (ms / 1e3), "unit": "queries/s",
                           "mean_count": float(c.mean()), "max_count": int(cnt.max()),
                           "truncated_queries": int((cnt > max_per).sum()), "max_results_per_query": max_per,
-                          "walk": "one walk per query over the 4-wide records (default)",
+                          "walk": "default: rows by a 4-wide walk per query that stops once the row is full, "
+                                  "then the full rows' counts by a warp's 32 SFC-neighbour queries together "
+                                  "when their points lie close against the radius, else per query",
                           "queries": "the N particle positions in input order (the library walks them in SFC "
                                      "order); one blocking call, including its status check"}
-    # the binary walk (ft_set_range_walk 1) and the warp-shared walk (2) on the first 1M
-    # queries: their times, and their rows and counts against the default walk's
+    # the other walks on the first 1M queries (ft_set_range_walk 1: binary walk per query, 2:
+    # warp-shared walk, 3: 4-wide walk per query, 4: the default with every group counted
+    # together): their times, and their rows and counts against the default walk's
     m = min(n, 1_000_000)
     res1 = torch.empty(m * max_per, dtype=torch.int32, device=dev)
     cnt1 = torch.empty(m, dtype=torch.int32, device=dev)
-    for walk, name in ((1, "binary_walk_1M"), (2, "warp_walk_1M")):
+    ms0 = _timed(stream, lambda: ft.range_query(ctx, tree, x[:m], y[:m], z[:m], r0[:m], r1[:m], max_per, res1,
+                                                cnt1), 1, warmup=0)
+    out["range_query"]["default_walk_1M"] = {"ms_per_step": ms0, "value": m / (ms0 / 1e3), "unit": "queries/s"}
+    for walk, name in ((1, "binary_walk_1M"), (2, "warp_walk_1M"), (3, "wide_walk_1M"), (4, "group_counts_1M")):
         ctx.set_range_walk(walk)
         ms1 = _timed(stream, lambda: ft.range_query(ctx, tree, x[:m], y[:m], z[:m], r0[:m], r1[:m], max_per, res1,
                                                     cnt1), 1, warmup=0)
@@ -589,7 +595,7 @@ def run_cfg5(args, stream):
 def run_profile(args, stream):
     """Every kernel family once on small inputs, for per-kernel ncu captures (the profiles/
     summaries): the build and both self-kNN methods on 2M clustered uint64 points (k = 32),
-    range_query on 20K of them, knn_query of 100K external points on 100K uniform float64
+    range_query on 200K of them, knn_query of 100K external points on 100K uniform float64
     points (k = 64, MAXK = 256, both methods), the learned bound's features and inference,
     and a batch of 256 Plummer sets (launch sequence: build + fast self-kNN; then the
     persistent launch).  Prints what ran."""
@@ -607,7 +613,7 @@ def run_profile(args, stream):
     ft.build_bvh(ctx, ft.particles(dx, dy, dz), tree)
     ft.self_knn_query(ctx, tree, 32, method="fast")
     ft.self_knn_query(ctx, tree, 32, method="plain")
-    m = 20_000
+    m = 200_000
     r0 = torch.zeros(m, dtype=torch.int64, device=dev).view(torch.uint64)
     r1 = torch.full((m,), int(2e-3 * 2 ** 40), dtype=torch.int64, device=dev).view(torch.uint64)
     ft.range_query(ctx, tree, dx[:m], dy[:m], dz[:m], r0, r1, 512)

@@ -1228,8 +1228,8 @@ ft_status ft_tune_build(ft_context *ctx, const void *x, const void *y, const voi
 ft_status ft_set_range_walk(ft_context *ctx, int walk) {
     FT_API_BEGIN
     need(ctx != nullptr, "null context");
-    need(walk >= 0 && walk <= 3, "range walk must be 0 (default), 1 (binary walk per query), 2 (warp-shared) or "
-                                 "3 (4-wide walk per query)");
+    need(walk >= 0 && walk <= 4, "range walk must be 0 (default), 1 (binary walk per query), 2 (warp-shared), "
+                                 "3 (4-wide walk per query) or 4 (the default with every count taken by groups)");
     ctx->range_walk = walk;
     FT_API_END
 }

@@ -37,20 +37,50 @@
 namespace ft {
 
 static constexpr int kFastStack = 64;
-// Two warps per block: each thread's heap takes k x 12 B of shared memory (48 KB per 128
-// threads at k = 32), so small blocks pack 9 per SM (18 warps) where 128-thread blocks fit 4.
+#ifndef FT_FAST_MINB
+#define FT_FAST_MINB 10
+#endif
+// Two warps per block: each thread's heap takes k x 8 B of shared memory (16 KB per 64 threads
+// at k = 32); the 4-wide walk is compiled for 10 such blocks per SM (20 warps, 96 registers a
+// thread; measured on 10M clustered points: 9 / 10 / 11 / 12 / 13 blocks 52.7 / 48.8 / 52.1 /
+// 52.0 / 56.2 ms, the tighter budgets spilling).
 static constexpr int kFastWarps = 2;
 static constexpr int kFastThreads = 32 * kFastWarps;
-// Warps per block for a heap capacity: k <= 32 heaps take 12 KB per warp, so two-warp blocks
-// fit 9 per SM; 64-entry heaps take 24 KB per warp, and one-warp blocks fit 9 warps per SM
-// where two-warp blocks fit 8.
+// Warps per block for a heap capacity: k <= 32 heaps take 8 KB per warp (two-warp blocks);
+// 64-entry heaps take 16 KB per warp, in one-warp blocks.
 template <int KC> constexpr int fast_warps() { return KC > 32 ? 1 : kFastWarps; }
-// Distance type of the fast walk's heap entries: float coordinates' distances are float sums
-// widened to double (node_distance_sq), so their heaps keep the float, exactly, in 4 bytes
-// (12 -> 8 bytes an entry: more resident blocks); other types keep dist_t.
-template <class T>
-using heap_dist_t =
-    typename std::conditional<std::is_same<T, float>::value, float, typename Coord<T>::dist_t>::type;
+// The fast walk's heap entries are 8 bytes: a float key of the distance and the leaf rank.
+// Float coordinates' distances are float sums widened to double (node_distance_sq), so their
+// key is the distance itself, exactly.  Other types key a distance by rounding it toward zero
+// to a float, which keeps the order (a < b implies key(a) <= key(b)): every decision the
+// heap takes on two different keys is the one the exact distances would take, and a decision
+// on equal keys (a candidate at the k-th key, an eviction leaving an equal maximum, equal keys
+// in the sorted result) flags the query for the exact replay, as exact ties already do.  The
+// output distances are recomputed exactly from the leaves.  8 bytes instead of 12 (16 with
+// alignment) an entry keep more warps resident and make the sifts 32-bit.
+template <class T> using heap_dist_t = float;
+template <class T> constexpr bool heap_keyed() { return !std::is_same<T, float>::value; }
+template <class T> FT_D float heap_key(typename Coord<T>::dist_t d) {
+    if constexpr (!heap_keyed<T>()) return (float)d;
+    else if constexpr (Coord<T>::is_float) return __double2float_rz(d);
+    else return __ull2float_rz(d);
+}
+// The largest distance whose key is `key` (so a distance above it has a larger key).
+template <class T> FT_D typename Coord<T>::dist_t heap_key_ub(float key) {
+    if constexpr (!heap_keyed<T>()) {
+        return (double)key;
+    } else if constexpr (Coord<T>::is_float) {
+        // distances are not negative; FLT_MAX keys every double from FLT_MAX up, infinity and
+        // NaN key only themselves
+        if (!(key < FLT_MAX)) return key == FLT_MAX ? DBL_MAX : (double)key;
+        const float up = __uint_as_float(__float_as_uint(key) + 1u); // the next float
+        return __longlong_as_double(__double_as_longlong((double)up) - 1ll); // the double below it
+    } else {
+        if (key < 16777216.0f) return (unsigned long long)key; // below 2^24 the key is exact
+        const float up = __uint_as_float(__float_as_uint(key) + 1u); // an integer from 2^24 up
+        return up >= 18446744073709551616.0f ? ~0ull : (unsigned long long)up - 1ull;
+    }
+}
 
 // Group walk (variant 5): a lower bound of the walk's distance from every point of the
 // group box [g0, g1] (per axis) to a node box b (minx, maxx, miny, maxy, minz, maxz).  Each
@@ -265,7 +295,7 @@ struct ListArgs {
 // the list `lst` when it is given.  NW: warps of the calling block (the heaps are laid out
 // per thread of the block); COH: tree records read through L2 (the persistent batch kernel,
 // whose blocks read trees that other blocks built earlier in the same launch).
-template <class T, int PER, int KC, int VAR, int NW = fast_warps<KC>(), bool COH = false>
+template <class T, int PER, int KC, int VAR, int NW = fast_warps<KC>(), bool COH = false, bool XB = false>
 FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss, unsigned char *smem,
                     TreeDev<T> t_all, BatchDev bt, const T *__restrict__ qx, const T *__restrict__ qy,
                     const T *__restrict__ qz, const uint32_t *__restrict__ order,
@@ -347,61 +377,126 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
     const D   B         = (bound && active) ? bound[q] : dist_heap_max<D>();
 
     int  count = 0;
-    D    hmax  = D(0);
-    D    thr   = B; // pruning threshold: B until the heap is full, then min(B, k-th distance)
+    H    hk    = H(0); // key of the k-th entry (the heap's root) once the heap is full
+    D    hmax  = D(0); // the largest distance with that key: at least the k-th distance
+    D    thr   = B;    // pruning threshold: B until the heap is full, then min(B, hmax)
     bool flag  = false;
 
+    // exact distance of the query to a leaf (by rank), as the walk computes it
+    auto exact = [&](int32_t leaf) -> D {
+        const int s = leaf + n - 1;
+        const T   x = t.min_x[s], y = t.min_y[s], z = t.min_z[s];
+        return Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, x, x, y, y, z, z);
+    };
+    // Keyed heaps: the entries sharing the k-th key sit at the top of the max-heap, and
+    // exchanging leaves between equal keys keeps the heap valid.  Finds the slot of the
+    // exactly largest of them (the root's slot first), its distance, and whether another
+    // entry ties it exactly.  Used with XB (external queries, whose replay -- knn_query's
+    // heap tier -- costs far more than the self queries' replay): without it a candidate or
+    // an eviction on the k-th key flags the query instead.
+    auto kth_exact = [&](int &slot, D &dmax, bool &tie) {
+        slot = 0;
+        dmax = exact(HI(0));
+        tie  = false;
+        for (int s2 = 1; s2 < k; ++s2)
+            if (HD(s2) == hk) {
+                const D e = exact(HI(s2));
+                if (e > dmax) {
+                    dmax = e;
+                    slot = s2;
+                    tie  = false;
+                } else if (!(e < dmax)) {
+                    tie = true; // equal (or not comparable)
+                }
+            }
+    };
+    // id: the leaf's rank (original indices are looked up when the rows are written)
     auto insert = [&](D d2, int32_t id) {
+        const H kd = heap_key<T>(d2);
         if (count < k) {
             int i = count;
             while (i > 0) {
                 int p  = (i - 1) >> 1;
-                D   pd = HD(p);
-                if (d2 <= pd) break;
-                HD(i) = (H)pd;
+                H   pd = HD(p);
+                if (kd <= pd) break;
+                HD(i) = pd;
                 HI(i) = HI(p);
                 i     = p;
             }
-            HD(i) = (H)d2;
+            HD(i) = kd;
             HI(i) = id;
             ++count;
             if (count == k) {
-                hmax = HD(0);
+                hk   = HD(0);
+                hmax = heap_key_ub<T>(hk);
                 thr  = hmax < B ? hmax : B;
             }
-        } else if (d2 < hmax) {
-            const D old = hmax;
+        } else if (kd < hk) {
+            if constexpr (heap_keyed<T>() && XB) {
+                // another entry shares the k-th key: evict the exactly largest of them
+                if ((k > 1 && HD(1) == hk) || (k > 2 && HD(2) == hk)) {
+                    int  slot;
+                    D    dmax;
+                    bool tie;
+                    kth_exact(slot, dmax, tie);
+                    if (tie) flag = true; // which of the tied leaves stays is the reference's order
+                    if (slot != 0) {
+                        const int32_t tmp = HI(0);
+                        HI(0)             = HI(slot);
+                        HI(slot)          = tmp;
+                    }
+                }
+            }
+            const H old = hk;
             int     i   = 0;
             for (;;) {
                 int l = 2 * i + 1;
                 if (l >= k) break;
                 int r  = l + 1;
                 int c  = i;
-                D   cd = d2;
-                D   ld = HD(l);
+                H   cd = kd;
+                H   ld = HD(l);
                 if (ld > cd) {
                     c  = l;
                     cd = ld;
                 }
                 if (r < k) {
-                    D rd = HD(r);
+                    H rd = HD(r);
                     if (rd > cd) {
                         c  = r;
                         cd = rd;
                     }
                 }
                 if (c == i) break;
-                HD(i) = (H)cd;
+                HD(i) = cd;
                 HI(i) = HI(c);
                 i     = c;
             }
-            HD(i) = (H)d2;
+            HD(i) = kd;
             HI(i) = id;
-            hmax  = HD(0);
+            hk    = HD(0);
+            hmax  = heap_key_ub<T>(hk);
             thr   = hmax < B ? hmax : B;
-            if (hmax == old) flag = true; // an equal distance stays at the boundary
-        } else if (d2 == hmax) {
-            flag = true; // a candidate at exactly the k-th distance was left out
+            // an equal distance stays at the boundary (keyed: the entries left on the old key
+            // are exactly nearer than the one evicted, unless tied, flagged above)
+            if (!(heap_keyed<T>() && XB) && hk == old) flag = true;
+        } else if (kd == hk) {
+            if constexpr (heap_keyed<T>() && XB) {
+                // the candidate's key is the k-th key: compare it exactly with the largest entry
+                // on that key, and take that entry's place (same key: the heap stays valid)
+                int  slot;
+                D    dmax;
+                bool tie;
+                kth_exact(slot, dmax, tie);
+                if (d2 < dmax) {
+                    HI(slot) = id;
+                    if (tie) flag = true;
+                } else if (!(d2 > dmax)) {
+                    flag = true; // a candidate at exactly the k-th distance was left out
+                }
+            } else {
+                flag = true; // a candidate at exactly the k-th distance was left out
+            }
         }
     };
 
@@ -416,7 +511,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             const int s  = leaf + n - 1;
             const T   x = t.min_x[s], y = t.min_y[s], z = t.min_z[s];
             const D   d2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, x, x, y, y, z, z);
-            insert(d2, ret_orig ? t.orig_idx[s] : leaf);
+            insert(d2, leaf);
         }
     }
 
@@ -498,7 +593,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             auto offer = [&](D d2, int s) {
                 const int leaf = s - (n - 1);
                 if (active && !(d2 > hmax) && !(d2 > B) && (leaf < w0 || leaf > w1) && s != self_leaf)
-                    insert(d2, ret_orig ? t.orig_idx[s] : leaf);
+                    insert(d2, leaf);
             };
             auto flush = [&]() {
                 if constexpr (FILT) {
@@ -631,9 +726,9 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             const D    rd2 = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, rb[0], rb[1], rb[2], rb[3], rb[4], rb[5]);
             const bool lleaf = l >= n - 1, rleaf = r >= n - 1;
             if (lleaf && needs(ld2) && (l - (n - 1) < w0 || l - (n - 1) > w1) && l != self_leaf)
-                insert(ld2, ret_orig ? t.orig_idx[l] : l - (n - 1));
+                insert(ld2, l - (n - 1));
             if (rleaf && needs(rd2) && (r - (n - 1) < w0 || r - (n - 1) > w1) && r != self_leaf)
-                insert(rd2, ret_orig ? t.orig_idx[r] : r - (n - 1));
+                insert(rd2, r - (n - 1));
             const bool li = !lleaf && needs(ld2), ri = !rleaf && needs(rd2);
             if (li && ri) {
                 const bool ln = ld2 <= rd2;
@@ -688,16 +783,25 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             T   bx[4][6];
             int ch[4];
             load_wide<T, COH>(t.wide, cur, bx, ch);
-            D  d[4];
-            bool in[4]; // needed internal child
+            D        d[4];
+            bool     in[4]; // needed internal child
+            unsigned lm = 0; // leaves to offer to the heap
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 d[i] = ch[i] >= 0 ? Metric<T>::template dist<(PER != 0), (PER == 2)>(
                                         px, py, pz, bx[i][0], bx[i][1], bx[i][2], bx[i][3], bx[i][4], bx[i][5])
                                   : dist_heap_max<D>();
                 const bool leaf = ch[i] >= n - 1;
-                if (leaf && needs(d[i]) && (ch[i] < ws0 || ch[i] > ws1) && ch[i] != self_leaf)
-                    insert(d[i], ret_orig ? t.orig_idx[ch[i]] : ch[i] - (n - 1));
+                if (leaf && needs(d[i]) && (ch[i] < ws0 || ch[i] > ws1) && ch[i] != self_leaf) lm |= 1u << i;
+            }
+            // one insertion site: lanes whose leaves sit at different child positions insert
+            // together (the warp loops as often as its lane with the most leaves)
+            while (lm) {
+                const int i = __ffs(lm) - 1;
+                lm &= lm - 1;
+                const D   di = i == 0 ? d[0] : i == 1 ? d[1] : i == 2 ? d[2] : d[3];
+                const int ci = i == 0 ? ch[0] : i == 1 ? ch[1] : i == 2 ? ch[2] : ch[3];
+                if (needs(di)) insert(di, ci - (n - 1)); // the threshold may have tightened
             }
 #pragma unroll
             for (int i = 0; i < 4; ++i) in[i] = ch[i] >= 0 && ch[i] < n - 1 && needs(d[i]);
@@ -773,7 +877,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             ++visits;
             if (node >= n - 1) {
                 const int lr = node - (n - 1);
-                if ((lr < w0 || lr > w1) && node != self_leaf) insert(d2, ret_orig ? t.orig_idx[node] : lr);
+                if ((lr < w0 || lr > w1) && node != self_leaf) insert(d2, lr);
             } else {
                 T   lb[6], rb[6];
                 int l, r;
@@ -816,7 +920,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
         if (node >= n - 1) {
             const int lr = node - (n - 1);
             // window leaves were already offered to the heap during seeding
-            if (nd && (lr < w0 || lr > w1) && node != self_leaf) insert(d2, ret_orig ? t.orig_idx[node] : lr);
+            if (nd && (lr < w0 || lr > w1) && node != self_leaf) insert(d2, lr);
         } else {
             T   lb[6], rb[6];
             int l, r;
@@ -861,7 +965,9 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
     // a bound that proved too small: the bound may have cut a neighbour, or fewer than k
     // points lie inside it.  With a miss list the query goes to the next launch (the walk
     // without a bound); otherwise the reference traversal reruns it.
-    const bool bound_miss = active && ((count >= k && hmax > B) || (count < k && B != dist_heap_max<D>()));
+    // (k-th key not below the bound's key: the k-th distance may exceed the bound)
+    const bool bound_miss =
+        active && B != dist_heap_max<D>() && (count < k || !(hk < heap_key<T>(B)));
     if (miss.rows) {
         const uint32_t at = warp_append(miss.count, bound_miss, lane);
         if (bound_miss) {
@@ -878,7 +984,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             (count < k || stack_guard_reaches<T, PER, COH>(t, px, py, pz, hmax, lane_stack)))
             flag = true;
         for (int hs = count; hs > 1; --hs) {
-            D       last  = HD(hs - 1);
+            H       last  = HD(hs - 1);
             int32_t lasti = HI(hs - 1);
             HD(hs - 1)    = HD(0);
             HI(hs - 1)    = HI(0);
@@ -889,34 +995,62 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
                 if (l >= size) break;
                 int r  = l + 1;
                 int c  = i;
-                D   cd = last;
-                D   ld = HD(l);
+                H   cd = last;
+                H   ld = HD(l);
                 if (ld > cd) {
                     c  = l;
                     cd = ld;
                 }
                 if (r < size) {
-                    D rd = HD(r);
+                    H rd = HD(r);
                     if (rd > cd) {
                         c  = r;
                         cd = rd;
                     }
                 }
                 if (c == i) break;
-                HD(i) = (H)cd;
+                HD(i) = cd;
                 HI(i) = HI(c);
                 i     = c;
             }
-            HD(i) = (H)last;
+            HD(i) = last;
             HI(i) = lasti;
         }
-        for (int i = 1; i < count; ++i)
-            if (HD(i) == HD(i - 1)) flag = true;
+        if constexpr (heap_keyed<T>()) {
+            // runs of equal keys inside the top k: the exact distances order them (the exact
+            // order refines the key order); only an exact tie can differ from the reference
+            for (int i = 1; i < count; ++i) {
+                for (int j = i; j > 0 && HD(j) == HD(j - 1); --j) {
+                    const D a = exact(HI(j - 1)), b = exact(HI(j));
+                    if (!(b < a)) { // in order, or equal (or not comparable): a tie
+                        if (!(a < b)) flag = true;
+                        break;
+                    }
+                    const int32_t tmp = HI(j);
+                    HI(j)             = HI(j - 1);
+                    HI(j - 1)         = tmp;
+                }
+            }
+        } else {
+            // equal distances: their order may differ from the reference's
+            for (int i = 1; i < count; ++i)
+                if (HD(i) == HD(i - 1)) flag = true;
+        }
         const size_t off = (size_t)q * (size_t)k;
         for (int i = 0; i < k; ++i) {
             if (i < count) {
-                __stcs(out_idx + off + i, (unsigned long long)(long long)HI(i));
-                __stcs(out_dist + off + i, (D)HD(i));
+                const int32_t leaf = HI(i);
+                const int     s    = leaf + n - 1;
+                D             dd;
+                if constexpr (heap_keyed<T>()) {
+                    // the exact distance, as the walk computed it (a leaf's box is its point)
+                    const T x = t.min_x[s], y = t.min_y[s], z = t.min_z[s];
+                    dd = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, x, x, y, y, z, z);
+                } else {
+                    dd = (D)HD(i);
+                }
+                __stcs(out_idx + off + i, (unsigned long long)(long long)(ret_orig ? t.orig_idx[s] : leaf));
+                __stcs(out_dist + off + i, dd);
             } else {
                 __stcs(out_idx + off + i, ~0ull);
                 __stcs(out_dist + off + i, dist_missing<D>());
@@ -935,8 +1069,14 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
 
 // The fast walk over queries [0, num), one warp per 32 queries; or, with a list, a grid-stride
 // loop over the list's entries (the count lives on the device: no host synchronisation).
-template <class T, int PER, int KC, int VAR>
-__global__ void __launch_bounds__(32 * fast_warps<KC>())
+// Resident blocks the 4-wide walk is compiled for (a register budget): its 8-byte heap entries
+// leave room for more blocks than the registers it would otherwise take.
+template <class T, int KC, int VAR> constexpr int fast_min_blocks() {
+    // (VAR 4 with k <= 32 only: the other shapes keep the registers they take)
+    return (VAR == 4 && KC <= 32) ? FT_FAST_MINB : 1;
+}
+template <class T, int PER, int KC, int VAR, bool XB = false>
+__global__ void __launch_bounds__(32 * fast_warps<KC>(), fast_min_blocks<T, KC, VAR>())
     fast_self_knn_kernel(QueryList lst, MissList miss, TreeDev<T> t_all, BatchDev bt, const T *__restrict__ qx,
                          const T *__restrict__ qy, const T *__restrict__ qz, const uint32_t *__restrict__ order,
                          const int32_t *__restrict__ leaf_ids, int num, int k, int half_window, int exclude_self,
@@ -949,14 +1089,14 @@ __global__ void __launch_bounds__(32 * fast_warps<KC>())
     const int warp = threadIdx.x >> 5;
     const int first = (blockIdx.x * W + warp) * 32;
     if (!lst.count) {
-        fast_warp<T, PER, KC, VAR>(first, lst, miss, smem, t_all, bt, qx, qy, qz, order, leaf_ids, num, k,
+        fast_warp<T, PER, KC, VAR, fast_warps<KC>(), false, XB>(first, lst, miss, smem, t_all, bt, qx, qy, qz, order, leaf_ids, num, k,
                                    half_window, exclude_self, ret_orig, bound, out_idx, out_dist, replay_ranks,
                                    replay_rows, replay_count, status, visit_count);
         return;
     }
     const int cnt = (int)*lst.count;
     for (int base = first; base < cnt; base += gridDim.x * W * 32)
-        fast_warp<T, PER, KC, VAR>(base, lst, miss, smem, t_all, bt, qx, qy, qz, order, leaf_ids, cnt, k,
+        fast_warp<T, PER, KC, VAR, fast_warps<KC>(), false, XB>(base, lst, miss, smem, t_all, bt, qx, qy, qz, order, leaf_ids, cnt, k,
                                    half_window, exclude_self, ret_orig, bound, out_idx, out_dist, replay_ranks,
                                    replay_rows, replay_count, status, visit_count);
 }
@@ -993,7 +1133,7 @@ static void launch_fast_t(const TreeDev<T> &tv, const BatchDev &bt, const ExtQue
     size_t        smem    = (size_t)std::max(k, 1) * threads * (sizeof(heap_dist_t<T>) + 4); // heaps of k entries
     auto   fn   = variant == 0 ? fast_self_knn_kernel<T, PER, KC, 0>
                   : variant == 1 ? fast_self_knn_kernel<T, PER, KC, 1>
-                  : variant == 4 ? fast_self_knn_kernel<T, PER, KC, 4>
+                  : variant == 4 ? (eq.x ? fast_self_knn_kernel<T, PER, KC, 4, true> : fast_self_knn_kernel<T, PER, KC, 4>)
                   : variant == 5 ? fast_self_knn_kernel<T, PER, KC, 5>
                                  : fast_self_knn_kernel<T, PER, KC, 2>;
     FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1461,16 +1601,13 @@ bool fast_self_knn_noalloc(Context &ctx, const ft_tree &tr, const int32_t *leaf_
 // claimed before any block queries), so the waits end; they are bounded all the same (30 s of
 // global time), after which the block sets STATUS_SPIN_LIMIT and stops.
 // =========================================================================================
-// Two-warp blocks, the standalone walk's shape: the heaps take the same shared memory per
-// warp, so as many warps fit on an SM (18 with k <= 32 heaps); a block builds its sets with
-// its 64 threads.
-// Block shape: as many warps per SM as the standalone walk's heaps allow (28 for k <= 32 with
-// 8-byte heap entries, 16 with 12-byte ones), in blocks as large as that allows, because a
-// block builds a whole set and the largest sets' builds (latency-bound climbs and searches)
-// set the launch's tail: 4 warps a block for float coordinates, 8 otherwise.
-template <class T> constexpr int persist_warps() { return sizeof(heap_dist_t<T>) == 4 ? 4 : 8; }
+// Block shape: blocks as large as the SM's room for them allows, because a block builds a
+// whole set and the largest sets' builds (latency-bound climbs and searches) set the launch's
+// tail: for float coordinates 4 warps a block, 7 blocks (28 warps) with k <= 32 heaps; other
+// types take more registers a thread (the exact 64-bit distances), 8 warps a block, 2 blocks.
+template <class T> constexpr int persist_warps() { return std::is_same<T, float>::value ? 4 : 8; }
 template <class T, int KC> constexpr int persist_blocks_per_sm() {
-    return sizeof(heap_dist_t<T>) == 4 ? (KC > 32 ? 3 : 7) : (KC > 32 ? 1 : 2);
+    return std::is_same<T, float>::value ? (KC > 32 ? 3 : 7) : (KC > 32 ? 1 : 2);
 }
 static constexpr int kPersistItems = 4; // keys per thread of a sort tile
 

@@ -141,7 +141,7 @@ struct Context {
     cudaEvent_t    ev_copied[2]  = {nullptr, nullptr};
     std::map<unsigned long long, TuneChoice> tuned; // autotuner choices by shape (tune_key)
     BuildProfile   bprof;
-    int            range_walk = 0; // range_query, trees of height <= 62: 0 default, 1 binary, 2 warp-shared, 3 4-wide
+    int            range_walk = 0; // range_query, trees of height <= 62: 0 default, 1 binary, 2 warp-shared, 3 4-wide, 4 group counts forced
     float         *learned_feats = nullptr; // learned-bound scratch: features and bounds
     void          *learned_bound = nullptr;
     size_t         learned_cap   = 0;

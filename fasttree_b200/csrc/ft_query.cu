@@ -648,10 +648,11 @@ FT_D int range_one(const TreeDev<T> &t, T px, T py, T pz, typename Coord<T>::dis
 // a grandchild beyond r_max has a parent beyond it too, and the reference prunes there.  Once
 // the row is full, a leaf is counted at once and an internal grandchild inside the shell is
 // counted from its leaf count.
-template <class T, int PER>
+// STOP: return as soon as the row is full (*filled set), leaving the count to range_count_group.
+template <class T, int PER, bool STOP = false>
 FT_D int range_one_wide(const TreeDev<T> &t, T px, T py, T pz, typename Coord<T>::dist_t rm2,
                         typename Coord<T>::dist_t RM2, int32_t *__restrict__ results, size_t off, int max_per,
-                        int ret_orig, uint32_t *status) {
+                        int ret_orig, uint32_t *status, bool *filled = nullptr) {
     using D     = typename Coord<T>::dist_t;
     const int n = t.n;
     int       count = 0;
@@ -661,6 +662,13 @@ FT_D int range_one_wide(const TreeDev<T> &t, T px, T py, T pz, typename Coord<T>
     if (d0 <= RM2 && (n > 1 || d0 >= rm2)) {
         sn[0] = 0;
         sp    = 1;
+    }
+    if constexpr (STOP) {
+        *filled = false;
+        if (max_per <= 0) {
+            *filled = sp > 0;
+            return 0;
+        }
     }
     long long budget = 2ll * n + 64;
     while (sp > 0) {
@@ -672,6 +680,12 @@ FT_D int range_one_wide(const TreeDev<T> &t, T px, T py, T pz, typename Coord<T>
         if (node >= n - 1) { // leaf in the shell (the n == 1 root included)
             if (count < max_per) results[off + count] = ret_orig ? t.orig_idx[node] : node - (n - 1);
             ++count;
+            if constexpr (STOP) {
+                if (count >= max_per) {
+                    *filled = true;
+                    break;
+                }
+            }
             continue;
         }
         T   bx[4][6];
@@ -727,6 +741,349 @@ __global__ void __launch_bounds__(128)
     range_radii<T>(rmin, rmax, q, rm2, RM2);
     counts[q] = range_one_wide<T, PER>(t, qx[q], qy[q], qz[q], rm2, RM2, results, (size_t)q * (size_t)max_per,
                                        max_per, ret_orig, status);
+}
+
+// -----------------------------------------------------------------------------------------
+// range_query counts, a warp's queries together.  A row's count is the number of leaves in
+// the query's shell (rmin^2 <= d <= rmax^2): on trees where the box distance is monotone over
+// nested boxes (the 4-wide walk's condition) a leaf's own distance decides it, whatever order
+// the walk takes, so the count needs no walk order.  The lanes that still need a count (their
+// rows are full) are neighbours on the curve; their query points lie in a small group box.
+// For a node box, group_near_far bounds, per axis, the gap node_distance_sq measures between
+// any of the group's points and any point of the box (near: no gap is smaller; far: none is
+// larger); the squared distances built from them bound every lane's distance to every leaf
+// below the node, since the shift, the squares, rounding and the sums are monotone.  A node
+// beyond every lane's r_max is skipped; one inside every lane's shell adds its leaf count to
+// every lane; the rest are expanded, and their leaves are staged for a test by each lane.
+// -----------------------------------------------------------------------------------------
+// Group frame: per axis the group's points lie in [g0, g0 + span] (for the 42-bit periodic
+// metric an arc of the circle starting at g0; for floating point, [g0, g1]).
+template <class T> struct RangeGroup {
+    T                  g0[3], g1[3];
+    unsigned long long span[3];
+};
+
+template <class T, int PER>
+FT_D void group_near_far(const RangeGroup<T> &g, const T b[6], typename Coord<T>::dist_t &near,
+                         typename Coord<T>::dist_t &far) {
+    using C = Coord<T>;
+    if constexpr (C::is_float) {
+        T n3[3], f3[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const T lo = b[2 * a], hi = b[2 * a + 1];
+            n3[a] = c_fmax(c_fmax(T(0), sub_rn(lo, g.g1[a])), sub_rn(g.g0[a], hi));
+            f3[a] = c_fmax(sub_rn(hi, g.g0[a]), sub_rn(g.g1[a], lo));
+        }
+        near = (double)add_rn(add_rn(mul_rn(n3[0], n3[0]), mul_rn(n3[1], n3[1])), mul_rn(n3[2], n3[2]));
+        far  = (double)add_rn(add_rn(mul_rn(f3[0], f3[0]), mul_rn(f3[1], f3[1])), mul_rn(f3[2], f3[2]));
+    } else if constexpr (PER == 2) {
+        // gaps between the arc G = [g0, g0 + span] and the box [lo, hi] are the circular
+        // distances w(u) = min(u, P - u) of the differences u in D = [lo - g0 - span, hi - g0]
+        // (mod P), an arc of length len: w is 0 where D holds 0, P/2 where it holds P/2, and
+        // otherwise takes its extremes at D's ends
+        constexpr unsigned long long P = 1ull << C::bits, M = P - 1ull, H = P >> 1;
+        unsigned long long sn = 0, sf = 0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const unsigned long long lo = (unsigned long long)b[2 * a], hi = (unsigned long long)b[2 * a + 1];
+            const unsigned long long st  = (lo - (unsigned long long)g.g0[a] - g.span[a]) & M;
+            const unsigned long long len = (hi - lo) + g.span[a];
+            unsigned long long       gn = 0, gf = H;
+            if (len < P) {
+                const unsigned long long en = (st + len) & M;
+                const unsigned long long wa = st <= H ? st : P - st, we = en <= H ? en : P - en;
+                const bool               z  = st == 0 || st + len >= P;
+                const bool               h  = ((H - st) & M) <= len;
+                gn = z ? 0ull : (wa < we ? wa : we);
+                gf = h ? H : (wa > we ? wa : we);
+            }
+            sn += Metric<T>::sq((unsigned long long)(uint32_t)(gn >> C::dist_shift));
+            sf += Metric<T>::sq((unsigned long long)(uint32_t)(gf >> C::dist_shift));
+        }
+        near = sn;
+        far  = sf;
+    } else {
+        unsigned long long sn = 0, sf = 0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const T lo = b[2 * a], hi = b[2 * a + 1], g0 = g.g0[a], g1 = g.g1[a];
+            const unsigned long long gn = lo > g1   ? (unsigned long long)(T)(lo - g1)
+                                          : g0 > hi ? (unsigned long long)(T)(g0 - hi)
+                                                    : 0ull;
+            const unsigned long long fa = g1 > lo ? (unsigned long long)(T)(g1 - lo) : 0ull;
+            const unsigned long long fb = hi > g0 ? (unsigned long long)(T)(hi - g0) : 0ull;
+            sn += Metric<T>::sq(gn >> C::dist_shift);
+            sf += Metric<T>::sq((fa > fb ? fa : fb) >> C::dist_shift);
+        }
+        near = sn;
+        far  = sf;
+    }
+}
+
+// Offset of coordinate v from the group's corner, as a float for the leaf filter: the signed
+// 42-bit wrapped difference (periodic), else the plain difference.
+template <class T, int PER> FT_D float group_off(T v, const RangeGroup<T> &g, int a) {
+    if constexpr (Coord<T>::is_float) {
+        return (float)sub_rn(v, g.g0[a]);
+    } else if constexpr (PER == 2) {
+        constexpr int sh = 64 - Coord<T>::bits;
+        return (float)((long long)(((unsigned long long)v - (unsigned long long)g.g0[a]) << sh) >> sh);
+    } else {
+        return (float)((long long)(unsigned long long)v - (long long)(unsigned long long)g.g0[a]);
+    }
+}
+
+#ifndef FT_RANGE_WARPS
+#define FT_RANGE_WARPS 4
+#endif
+#ifndef FT_RANGE_MINB
+#define FT_RANGE_MINB 1
+#endif
+static constexpr int kRangeWarps = FT_RANGE_WARPS, kRangeGStack = 512, kRangeStage = 256;
+// The group counts a warp's full rows together when its points' largest axis extent is at
+// most 1/FT_RANGE_SPREAD of the smallest radius (measured on 10M clustered points, r = 2e-3 of
+// the box, all N queries: factors 1 / 4 / 16 2.38 / 2.39 / 3.48 s, every group together
+// 2.37 s, the per-query 4-wide walk 5.87 s).
+#ifndef FT_RANGE_SPREAD
+#define FT_RANGE_SPREAD 1
+#endif
+
+// The group count of the lanes with `need` (every lane of the warp calls it).  Returns false
+// (counts unset) when the group is too spread out for its bounds to help (FORCE: only when
+// the float filter's accuracy needs it), or a stack would overflow; the caller then counts
+// per lane.  count: this lane's shell count.
+template <class T, int PER, bool FORCE = false>
+FT_D bool range_count_group(const TreeDev<T> &t, bool need, T px, T py, T pz, typename Coord<T>::dist_t rm2,
+                            typename Coord<T>::dist_t RM2, int32_t *stk, float4 *stage, int &count) {
+    using C                = Coord<T>;
+    using D                = typename C::dist_t;
+    const unsigned FULL    = 0xffffffffu;
+    const int      lane    = threadIdx.x & 31;
+    const int      n       = t.n;
+    if (n < 2) return false;
+    if constexpr (PER == 1) return false; // the general periodic form: no group bounds
+    RangeGroup<T> g;
+    T             v[3] = {px, py, pz};
+    if constexpr (PER == 2) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) v[a] = (T)((unsigned long long)v[a] & ((1ull << C::bits) - 1ull));
+    }
+    if constexpr (C::is_float) {
+        bool fin = true;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) fin = fin && isfinite((double)v[a]);
+        if (!__all_sync(FULL, !need || fin)) return false;
+    }
+    const unsigned nm  = __ballot_sync(FULL, need);
+    const int      ref = __ffs(nm) - 1;
+    double         spread = 0.0; // largest axis extent, in coordinate units
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if constexpr (PER == 2) {
+            constexpr int sh = 64 - C::bits;
+            const T       r  = __shfl_sync(FULL, v[a], ref);
+            long long     o  = (long long)(((unsigned long long)v[a] - (unsigned long long)r) << sh) >> sh;
+            long long     lo = need ? o : LLONG_MAX, hi = need ? o : LLONG_MIN;
+#pragma unroll
+            for (int m = 16; m > 0; m >>= 1) {
+                lo = min(lo, __shfl_xor_sync(FULL, lo, m));
+                hi = max(hi, __shfl_xor_sync(FULL, hi, m));
+            }
+            g.g0[a]   = (T)(((unsigned long long)r + (unsigned long long)lo) & ((1ull << C::bits) - 1ull));
+            g.span[a] = (unsigned long long)(hi - lo);
+            g.g1[a]   = g.g0[a];
+            spread    = fmax(spread, (double)g.span[a]);
+        } else {
+            const T r  = __shfl_sync(FULL, v[a], ref);
+            T       lo = need ? v[a] : r, hi = lo;
+#pragma unroll
+            for (int m = 16; m > 0; m >>= 1) {
+                const T u = __shfl_xor_sync(FULL, lo, m), w = __shfl_xor_sync(FULL, hi, m);
+                lo        = u < lo ? u : lo;
+                hi        = w > hi ? w : hi;
+            }
+            g.g0[a]   = lo;
+            g.g1[a]   = hi;
+            g.span[a] = C::is_float ? 0ull : (unsigned long long)(T)(hi - lo);
+            spread    = fmax(spread, (double)hi - (double)lo);
+        }
+    }
+    // the lanes' radii
+    D R_lo = need ? RM2 : dist_heap_max<D>(), R_hi = need ? RM2 : D(0);
+    D r_lo = need ? rm2 : dist_heap_max<D>(), r_hi = need ? rm2 : D(0);
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) {
+        const D a = __shfl_xor_sync(FULL, R_lo, m), b = __shfl_xor_sync(FULL, R_hi, m);
+        const D c = __shfl_xor_sync(FULL, r_lo, m), d = __shfl_xor_sync(FULL, r_hi, m);
+        R_lo = a < R_lo ? a : R_lo;
+        R_hi = b > R_hi ? b : R_hi;
+        r_lo = c < r_lo ? c : r_lo;
+        r_hi = d > r_hi ? d : r_hi;
+    }
+    // worth it only when the group is small against the radius (its fuzzy shell thin), and the
+    // leaf filter's float offsets stay accurate: every staged leaf lies within
+    // lam = spread + (sqrt(R_hi) + 2) 2^shift of the group's corner on each axis
+    const double unit = C::is_float ? 1.0 : (double)(1ull << C::dist_shift);
+    const double rad  = sqrt((double)R_lo) * unit, Rad = (sqrt((double)R_hi) + 2.0) * unit;
+    const double lam  = spread + Rad * (1.0 + 0x1p-20);
+    bool         ok   = (FORCE || spread * (double)FT_RANGE_SPREAD <= rad) && lam > 0.0;
+    if constexpr (C::is_float) ok = ok && lam < 0x1p100 && lam > 0x1p-100 && R_hi < 0x1p200;
+    else ok = ok && lam < 0x1p40;
+    if (!ok) return false; // warp-uniform
+    const float gerr = (float)(lam * 0x1p-21);
+    const float scl_dn = C::is_float ? 1.0f - 0x1p-20f : (1.0f / (float)(1ull << C::dist_shift)) * (1.0f - 0x1p-20f);
+    const float scl_up = C::is_float ? 1.0f + 0x1p-20f : (1.0f / (float)(1ull << C::dist_shift)) * (1.0f + 0x1p-20f);
+    const float floor1 = C::is_float ? 0.0f : 1.0f; // integer terms floor the shifted gap
+    float       RMf_up, RMf_dn, rmf_up, rmf_dn;
+    if constexpr (C::is_float) {
+        RMf_up = __double2float_ru(RM2);
+        RMf_dn = __double2float_rd(RM2);
+        rmf_up = __double2float_ru(rm2);
+        rmf_dn = __double2float_rd(rm2);
+    } else {
+        RMf_up = __ull2float_ru(RM2);
+        RMf_dn = __ull2float_rd(RM2);
+        rmf_up = __ull2float_ru(rm2);
+        rmf_dn = __ull2float_rd(rm2);
+    }
+    const float qf[3] = {group_off<T, PER>(v[0], g, 0), group_off<T, PER>(v[1], g, 1), group_off<T, PER>(v[2], g, 2)};
+
+    int       mine = 0;    // this lane's count from staged leaves
+    long long part = 0;    // leaves in nodes inside every lane's shell, found by this lane
+    int       top = 0, cc = 0;
+    bool      overflow = false;
+    {
+        const T rb[6] = {t.min_x[0], t.max_x[0], t.min_y[0], t.max_y[0], t.min_z[0], t.max_z[0]};
+        D       rn, rf;
+        group_near_far<T, PER>(g, rb, rn, rf);
+        if (rn <= R_hi) {
+            if (rn >= r_hi && rf <= R_lo) part = lane == 0 ? n : 0;
+            else if (!(rf < r_lo)) top = 1;
+        }
+    }
+    if (lane == 0) stk[0] = 0;
+    __syncwarp();
+    // each lane tests every staged leaf: the float filter, then the exact distance where the
+    // filter cannot decide
+    auto flush = [&]() {
+        for (int j = 0; j < cc; ++j) {
+            const float4 e = stage[j];
+            if (!need) continue;
+            const float dx = fabsf(e.x - qf[0]), dy = fabsf(e.y - qf[1]), dz = fabsf(e.z - qf[2]);
+            const float lx = fmaxf(0.0f, fmaf(dx - gerr, scl_dn, -floor1));
+            const float ly = fmaxf(0.0f, fmaf(dy - gerr, scl_dn, -floor1));
+            const float lz = fmaxf(0.0f, fmaf(dz - gerr, scl_dn, -floor1));
+            const float ux = (dx + gerr) * scl_up, uy = (dy + gerr) * scl_up, uz = (dz + gerr) * scl_up;
+            const float L  = fmaf(lz, lz, fmaf(ly, ly, lx * lx)) * (1.0f - 0x1p-16f);
+            const float U  = fmaf(uz, uz, fmaf(uy, uy, ux * ux)) * (1.0f + 0x1p-16f);
+            if (L > RMf_up || U < rmf_dn) continue; // surely outside the shell
+            if (L >= rmf_up && U <= RMf_dn) {       // surely inside
+                ++mine;
+                continue;
+            }
+            const int s = __float_as_int(e.w);
+            const T   x = t.min_x[s], y = t.min_y[s], z = t.min_z[s];
+            const D   d = Metric<T>::template dist<(PER != 0), (PER == 2)>(px, py, pz, x, x, y, y, z, z);
+            mine += (d >= rm2 && d <= RM2) ? 1 : 0;
+        }
+        cc = 0;
+        __syncwarp();
+    };
+    long long budget = 2ll * n + 64;
+    while (top > 0) {
+        const int m = min(min(top, 32), (kRangeGStack - top) / 3);
+        if (m <= 0 || (budget -= m) < 0) {
+            overflow = true;
+            break;
+        }
+        const int base = top - m;
+        const int node = lane < m ? stk[base + lane] : -1;
+        top            = base;
+        __syncwarp();
+        T        bx[4][6];
+        int      ch[4] = {-1, -1, -1, -1};
+        unsigned kl = 0, ki = 0;
+        if (node >= 0) {
+            load_wide(t.wide, node, bx, ch);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                if (ch[i] < 0) continue;
+                D dn, dfar;
+                group_near_far<T, PER>(g, bx[i], dn, dfar);
+                if (!(dn <= R_hi) || dfar < r_lo) continue; // outside every ball, or inside every r_min
+                const bool leaf = ch[i] >= n - 1;
+                if (dn >= r_hi && dfar <= R_lo) part += leaf ? 1 : t.leaves[ch[i]]; // inside every shell
+                else if (leaf) kl |= 1u << i;
+                else ki |= 1u << i;
+            }
+        }
+        const int nl = __popc(kl), ni = __popc(ki);
+        int       incl = nl | (ni << 16);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += u;
+        }
+        const int tot = __shfl_sync(FULL, incl, 31);
+        if (cc + (tot & 0xffff) > kRangeStage) flush();
+        int pl = cc + (incl & 0xffff) - nl, pi = top + (incl >> 16) - ni;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if ((kl >> i) & 1u)
+                stage[pl++] = make_float4(group_off<T, PER>(bx[i][0], g, 0), group_off<T, PER>(bx[i][2], g, 1),
+                                          group_off<T, PER>(bx[i][4], g, 2), __int_as_float(ch[i]));
+            if ((ki >> i) & 1u) stk[pi++] = ch[i];
+        }
+        cc += tot & 0xffff;
+        top += tot >> 16;
+        __syncwarp();
+    }
+    if (overflow) return false; // warp-uniform (every lane ran the same steps)
+    flush();
+#pragma unroll
+    for (int m = 16; m > 0; m >>= 1) part += __shfl_xor_sync(FULL, part, m);
+    count = (int)min(part + (long long)mine, (long long)INT_MAX);
+    return true;
+}
+
+// range_query on trees of height <= 62 with a monotone box distance (default): phase 1 writes
+// each row in the reference's order with the 4-wide walk and stops once the row is full;
+// phase 2 counts the full rows' shells with range_count_group (per lane when the group's
+// bounds cannot help).  Counts, rows and their order equal range_wide_kernel's.
+template <class T, int PER, bool FORCE = false>
+__global__ void __launch_bounds__(32 * kRangeWarps, FT_RANGE_MINB)
+    range_split_kernel(TreeDev<T> t, const T *__restrict__ qx, const T *__restrict__ qy, const T *__restrict__ qz,
+                       const T *__restrict__ rmin, const T *__restrict__ rmax, int nq, int32_t *__restrict__ results,
+                       int32_t *__restrict__ counts, int max_per, int ret_orig, const uint32_t *__restrict__ order,
+                       uint32_t *status) {
+    using D = typename Coord<T>::dist_t;
+    __shared__ int32_t s_stk[kRangeWarps][kRangeGStack];
+    __shared__ float4  s_stage[kRangeWarps][kRangeStage];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int base = (blockIdx.x * kRangeWarps + warp) * 32;
+    if (base >= nq) return; // warp-uniform
+    const int  i      = base + lane;
+    const bool active = i < nq;
+    const int  q      = active ? (order ? (int)order[i] : i) : (order ? (int)order[base] : base);
+    D          rm2 = D(0), RM2 = D(0);
+    range_radii<T>(rmin, rmax, q, rm2, RM2);
+    const T      px = qx[q], py = qy[q], pz = qz[q];
+    const size_t off = (size_t)q * (size_t)max_per;
+    bool         filled = false;
+    int          cnt    = 0;
+    if (active)
+        cnt = range_one_wide<T, PER, true>(t, px, py, pz, rm2, RM2, results, off, max_per, ret_orig, status, &filled);
+    const bool need = active && filled;
+    if (__any_sync(0xffffffffu, need)) {
+        int total = 0;
+        if (range_count_group<T, PER, FORCE>(t, need, px, py, pz, rm2, RM2, s_stk[warp], s_stage[warp], total)) {
+            if (need) cnt = total;
+        } else if (need) {
+            cnt = range_one_wide<T, PER>(t, px, py, pz, rm2, RM2, results, off, 0, ret_orig, status);
+        }
+    }
+    if (active) counts[q] = cnt;
 }
 
 template <class T, int PER>
@@ -1308,7 +1665,6 @@ static void range_typed(const ft_options &o, const ft_tree &tr, const void *qx, 
                         const void *rmin, const void *rmax, int nq, int32_t *results, int32_t *counts, int max_per,
                         const uint32_t *order, uint32_t *status, cudaStream_t st, int walk) {
     TreeDev<T> tv     = tree_view<T>(tr);
-    int        blocks = (nq + 127) / 128;
     bool       ro     = o.return_orig_indices != 0;
     // trees of height <= 62 never reach the reference's stack guard (range_short_kernel)
     const TreeImpl *impl  = (const TreeImpl *)tr.impl;
@@ -1320,9 +1676,15 @@ static void range_typed(const ft_options &o, const ft_tree &tr, const void *qx, 
         auto fn = !short_walk ? range_kernel<T, decltype(M)::value>
                   : walk == 2 ? range_group_kernel<T, decltype(M)::value>
                   : (walk == 1 || !wide) ? range_short_kernel<T, decltype(M)::value>
-                                         : range_wide_kernel<T, decltype(M)::value>;
-        fn<<<blocks, 128, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz, (const T *)rmin, (const T *)rmax,
-                                   nq, results, counts, max_per, ro ? 1 : 0, order, status);
+                  : walk == 3 ? range_wide_kernel<T, decltype(M)::value>
+                  : walk == 4 ? range_split_kernel<T, decltype(M)::value, true>
+                              : range_split_kernel<T, decltype(M)::value>;
+        // the split kernel's blocks have 32 * kRangeWarps threads, the others 128
+        const bool split = short_walk && wide && walk != 1 && walk != 2 && walk != 3;
+        const int  thr   = split ? 32 * kRangeWarps : 128;
+        fn<<<(nq + thr - 1) / thr, thr, 0, st>>>(tv, (const T *)qx, (const T *)qy, (const T *)qz, (const T *)rmin,
+                                                 (const T *)rmax, nq, results, counts, max_per, ro ? 1 : 0, order,
+                                                 status);
     });
     FT_CUDA(cudaGetLastError());
 }

@@ -106,9 +106,11 @@ class Context:
                 "bound_misses": s.reserved[1], "rerun_visits": s.reserved[2]}
 
     def set_range_walk(self, walk: int):
-        """range_query's walk on trees of height <= 62 (ft_set_range_walk): 0 default (4-wide
-        walk per query where it applies), 1 binary walk per query, 2 a warp's queries together
-        when their balls overlap, 3 4-wide walk per query."""
+        """range_query's walk on trees of height <= 62 (ft_set_range_walk): 0 default (rows by
+        a 4-wide walk per query that stops once the row is full, full rows counted by a warp's
+        queries together when they lie close, where the 4-wide walk applies), 1 binary walk per
+        query, 2 a warp's queries together when their balls overlap, 3 4-wide walk per query,
+        4 as 0 with every group counted together."""
         _call(lib().ft_set_range_walk(self._h, int(walk)))
 
     def profile_builds(self, enable: bool = True):

@@ -251,13 +251,17 @@ ft_status ft_range(ft_context *ctx, const ft_tree *tree, const void *qx, const v
                    int32_t *results, int32_t *counts, int max_results_per_query,
                    ft_stream_t stream);
 
-/* How ft_range walks trees of height <= 62 on this context: 0 (default), one walk per query
- * over the 4-wide records (the binary records where the box distance is not monotone); 1, one
- * walk per query over the binary records; 2, the 32 queries of a warp (neighbours in SFC
- * order) walk the union of their nodes together, each stack entry with the mask of the
- * queries that need it, when their balls overlap (else one walk each); 3, the 4-wide walk
- * where it applies.  Same rows and counts either way.  (Taller trees keep the reference's
- * walk with its stack guard.) */
+/* How ft_range walks trees of height <= 62 on this context: 0 (default), where the box
+ * distance is monotone over nested boxes, each query writes its row with a walk over the
+ * 4-wide records and stops once the row is full, then the full rows of a warp's 32 queries
+ * (neighbours in SFC order) are counted together when their points lie close against the
+ * radius (nodes inside every query's shell counted whole, nodes beyond every ball skipped,
+ * the leaves between tested per query), else per query; elsewhere one walk per query over the
+ * binary records; 1, one walk per query over the binary records; 2, the 32 queries of a warp
+ * walk the union of their nodes together, each stack entry with the mask of the queries that
+ * need it, when their balls overlap (else one walk each); 3, one 4-wide walk per query where
+ * it applies; 4, as 0 with every group counted together whatever its spread.  Same rows and
+ * counts either way.  (Taller trees keep the reference's walk with its stack guard.) */
 ft_status ft_set_range_walk(ft_context *ctx, int walk);
 
 /* Height of the built tree (root to deepest leaf).  The traversal stack of the reference

@@ -216,3 +216,50 @@ def test_range_counts_of_large_balls_match_oracle(coord, sfc, per, oc, os_, walk
     for i in range(160):
         m = min(int(oc_[i]), 32)
         assert np.array_equal(g[i, :m], orr[i, :m]), i
+
+
+GROUP_CASES = CASES
+
+
+@pytest.mark.parametrize("coord,sfc,per,oc,os_", GROUP_CASES,
+                         ids=[f"{c[0]}-{c[1]}{'-per' if c[2] else ''}" for c in GROUP_CASES])
+@pytest.mark.parametrize("r_phys,max_per", [(6.0, 16), (15.0, 0)])
+@pytest.mark.parametrize("walk", [0, 4], ids=["default-walk", "group-counts"])
+def test_range_group_counts_match_oracle(coord, sfc, per, oc, os_, r_phys, max_per, walk):
+    """Dense queries with full rows: a warp's neighbouring queries count their shells together
+    (nodes inside every query's shell counted whole, nodes beyond every ball skipped, the
+    leaves between screened by a float filter and decided exactly where it cannot tell).
+    Walk 4 takes every group that way, however spread out; the periodic cases put a cluster
+    across the period's edge.  Rows and counts bit for bit against the oracle."""
+    n = 40_000
+    rng = np.random.default_rng(21)
+    p = np.empty((3, n))
+    n1, n2 = int(n * 0.45), int(n * 0.85)
+    p[:, :n1] = rng.normal(25.0, 4.0, (3, n1))
+    p[:, n1:n2] = rng.normal(75.0, 4.0, (3, n2 - n1))
+    p[:, n2:] = rng.uniform(0.0, 100.0, (3, n - n2))
+    if per:
+        p = np.mod(p + 27.0, 100.0)  # the second cluster straddles the period's edge
+    p = np.clip(p, 1e-4, 100.0 - 1e-4)
+    x, y, z = (to_coord(a, oc) for a in p)
+    ctx = ft.Context(coord, sfc, periodic=per)
+    ctx.set_range_walk(walk)
+    tree = ft.TreeSoA(ctx, n)
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree)
+    opts = O.Options(oc, os_, per)
+    ot = O.build_bvh(opts, x, y, z)
+    nq = 3000
+    pick = rng.choice(n, nq - 200, replace=False)
+    q = [np.concatenate([a[pick], to_coord(rng.uniform(0, 100.0, 200), oc)]) for a in (x, y, z)]
+    r0 = np.zeros(nq, q[0].dtype)
+    r1 = np.full(nq, radius(r_phys, oc), q[0].dtype)
+    r0[::4] = radius(r_phys / 3, oc)  # hollow shells for a quarter of the queries
+    gr, gc = ft.range_query(ctx, tree, *q, r0, r1, max_per)
+    orr, oc_ = O.range_query(opts, ot, *q, r0, r1, max_per)
+    assert (oc_ > max(max_per, 1)).mean() > 0.5  # most rows are full: the counts come from the groups
+    assert np.array_equal(gc.cpu().numpy(), oc_)
+    if max_per:
+        g = gr.cpu().numpy()
+        for i in range(nq):
+            m = min(int(oc_[i]), max_per)
+            assert np.array_equal(g[i, :m], orr[i, :m]), i
