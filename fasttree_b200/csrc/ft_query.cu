@@ -849,7 +849,8 @@ static constexpr int kRangeWarps = FT_RANGE_WARPS, kRangeGStack = 512, kRangeSta
 // The group counts a warp's full rows together when its points' largest axis extent is at
 // most 1/FT_RANGE_SPREAD of the smallest radius (measured on 10M clustered points, r = 2e-3 of
 // the box, all N queries: factors 1 / 4 / 16 2.38 / 2.39 / 3.48 s, every group together
-// 2.37 s, the per-query 4-wide walk 5.87 s).
+// 2.37 s, the per-query 4-wide walk 5.87 s; then 2.04 s with the threshold leaf filter, of
+// which the rows take 0.12 s).
 #ifndef FT_RANGE_SPREAD
 #define FT_RANGE_SPREAD 1
 #endif
@@ -933,25 +934,45 @@ FT_D bool range_count_group(const TreeDev<T> &t, bool need, T px, T py, T pz, ty
     const double rad  = sqrt((double)R_lo) * unit, Rad = (sqrt((double)R_hi) + 2.0) * unit;
     const double lam  = spread + Rad * (1.0 + 0x1p-20);
     bool         ok   = (FORCE || spread * (double)FT_RANGE_SPREAD <= rad) && lam > 0.0;
-    if constexpr (C::is_float) ok = ok && lam < 0x1p100 && lam > 0x1p-100 && R_hi < 0x1p200;
+    // (floating point: squared offsets stay normal floats)
+    if constexpr (C::is_float) ok = ok && lam < 0x1p60 && lam > 0x1p-60;
     else ok = ok && lam < 0x1p40;
     if (!ok) return false; // warp-uniform
-    const float gerr = (float)(lam * 0x1p-21);
-    const float scl_dn = C::is_float ? 1.0f - 0x1p-20f : (1.0f / (float)(1ull << C::dist_shift)) * (1.0f - 0x1p-20f);
-    const float scl_up = C::is_float ? 1.0f + 0x1p-20f : (1.0f / (float)(1ull << C::dist_shift)) * (1.0f + 0x1p-20f);
-    const float floor1 = C::is_float ? 0.0f : 1.0f; // integer terms floor the shifted gap
-    float       RMf_up, RMf_dn, rmf_up, rmf_dn;
-    if constexpr (C::is_float) {
-        RMf_up = __double2float_ru(RM2);
-        RMf_dn = __double2float_rd(RM2);
-        rmf_up = __double2float_ru(rm2);
-        rmf_dn = __double2float_rd(rm2);
-    } else {
-        RMf_up = __ull2float_ru(RM2);
-        RMf_dn = __ull2float_rd(RM2);
-        rmf_up = __ull2float_ru(rm2);
-        rmf_dn = __ull2float_rd(rm2);
-    }
+    // Leaf filter.  In shifted units u (offsets / 2^shift for integers, plain offsets for
+    // floating point) a lane's float estimate of a gap is y = |e - q|, within eps of the exact
+    // gap (conversions and the subtraction: at most 2^-22 lam, taken as 2^-20 lam).  Integer
+    // terms floor the shifted gap, t in (y - eps - 1, y + eps], so with Y = sum y^2 and
+    // sum y <= sqrt(3 Y) the exact distance lies in [Y - c_lo sqrt(Y), Y + c_hi sqrt(Y) + 3 eps^2],
+    // c_lo = 2 sqrt(3) (1 + eps), c_hi = 2 sqrt(3) eps; floating-point terms have no floor
+    // (c_lo = c_hi) and the reference's rounded sum lies within 1 +- 2^-20 of the real one.
+    // Each bound is monotone in Y, so four thresholds on Y decide a leaf: beyond r_max, inside
+    // r_max, at least r_min, below r_min.  The leaf's Y is computed in float (relative error
+    // under 2^-22, covered by a factor 1 +- 2^-21 on the thresholds) from offsets in units of
+    // 2^shift: 3 subtractions and 3 multiply-adds a leaf, the exact distance only in the thin
+    // band around the lane's spheres.
+    const double eps  = lam * 0x1p-20 / unit;
+    const double c_lo = 3.4641016151377546 * ((C::is_float ? 0.0 : 1.0) + eps) * (1.0 + 0x1p-40);
+    const double c_hi = 3.4641016151377546 * eps * (1.0 + 0x1p-40);
+    const double rho  = C::is_float ? 0x1p-20 : 0.0;
+    const double u2   = unit * unit; // shifted units^2 -> offset units^2
+    // smallest Y whose lower bound exceeds (or reaches) X, and largest Y whose upper bound
+    // stays at or below X (-1: none)
+    auto y_lower = [&](double X) {
+        const double r = (c_lo + sqrt(c_lo * c_lo + 4.0 * X)) * 0.5;
+        return r * r;
+    };
+    auto y_upper = [&](double X) {
+        const double a = X - 3.0 * eps * eps;
+        if (a < 0.0) return -1.0;
+        const double r = (-c_hi + sqrt(c_hi * c_hi + 4.0 * a)) * 0.5;
+        return r * r;
+    };
+    const double Rd = (double)RM2, rd = (double)rm2;
+    // out if Y > t_out; in r_max if Y <= t_in; at least r_min if Y >= t_ge; below r_min if Y < t_lt
+    const float t_out = __double2float_ru(y_lower(Rd / (1.0 - rho)) * u2 * (1.0 + 0x1p-21));
+    const float t_in  = __double2float_rd(fmax(y_upper(Rd / (1.0 + rho)), -1.0) * u2 * (1.0 - 0x1p-21));
+    const float t_ge  = rd <= 0.0 ? 0.0f : __double2float_ru(y_lower(rd / (1.0 - rho)) * u2 * (1.0 + 0x1p-21));
+    const float t_lt  = rd <= 0.0 ? -1.0f : __double2float_rd(fmax(y_upper(rd / (1.0 + rho)), -1.0) * u2 * (1.0 - 0x1p-21));
     const float qf[3] = {group_off<T, PER>(v[0], g, 0), group_off<T, PER>(v[1], g, 1), group_off<T, PER>(v[2], g, 2)};
 
     int       mine = 0;    // this lane's count from staged leaves
@@ -975,15 +996,10 @@ FT_D bool range_count_group(const TreeDev<T> &t, bool need, T px, T py, T pz, ty
         for (int j = 0; j < cc; ++j) {
             const float4 e = stage[j];
             if (!need) continue;
-            const float dx = fabsf(e.x - qf[0]), dy = fabsf(e.y - qf[1]), dz = fabsf(e.z - qf[2]);
-            const float lx = fmaxf(0.0f, fmaf(dx - gerr, scl_dn, -floor1));
-            const float ly = fmaxf(0.0f, fmaf(dy - gerr, scl_dn, -floor1));
-            const float lz = fmaxf(0.0f, fmaf(dz - gerr, scl_dn, -floor1));
-            const float ux = (dx + gerr) * scl_up, uy = (dy + gerr) * scl_up, uz = (dz + gerr) * scl_up;
-            const float L  = fmaf(lz, lz, fmaf(ly, ly, lx * lx)) * (1.0f - 0x1p-16f);
-            const float U  = fmaf(uz, uz, fmaf(uy, uy, ux * ux)) * (1.0f + 0x1p-16f);
-            if (L > RMf_up || U < rmf_dn) continue; // surely outside the shell
-            if (L >= rmf_up && U <= RMf_dn) {       // surely inside
+            const float dx = e.x - qf[0], dy = e.y - qf[1], dz = e.z - qf[2];
+            const float Y  = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            if (Y > t_out || Y < t_lt) continue; // surely outside the shell
+            if (Y <= t_in && Y >= t_ge) {        // surely inside
                 ++mine;
                 continue;
             }
