@@ -149,33 +149,11 @@ FT_D float group_filter(const float4 &e, const float q[3], float gerr, float sca
     return fmaf(lz, lz, fmaf(ly, ly, lx * lx));
 }
 
-// Float bounds of a distance for the 4-wide walk's stack: rounded down for a stacked node,
-// rounded up for the threshold it is compared with (non-negative values, so the float order
-// never drops a node whose exact distance is within the threshold).  Only active lanes pop.
-template <class D> FT_D float stack_key_down(D d) {
-    if constexpr (std::is_floating_point<D>::value) return __double2float_rd((double)d);
-    else return __ull2float_rd((unsigned long long)d);
-}
+// A distance rounded up to a float (non-negative values): the 4-wide walk's key threshold for
+// float coordinates, whose keys are the distances themselves.
 template <class D> FT_D float stack_key_up(D d) {
     if constexpr (std::is_floating_point<D>::value) return __double2float_ru((double)d);
     else return __ull2float_ru((unsigned long long)d);
-}
-
-// Sort key of a needed child in the 4-wide walk and its inverse.  Integer keys are d + 1
-// (0 marks a child that is not needed), saturating at the largest value, whose inverse is
-// then one below the distance: the stacked distance can only err low, which keeps the node
-// (never prunes it).  Floating-point distances are not negative, so -1 marks the others.
-template <class D> FT_D D walk_key(D d) {
-    if constexpr (std::is_floating_point<D>::value) return d;
-    else return d + D(d != ~D(0));
-}
-template <class D> FT_D D walk_key_none() {
-    if constexpr (std::is_floating_point<D>::value) return D(-1);
-    else return D(0);
-}
-template <class D> FT_D D walk_key_dist(D key) {
-    if constexpr (std::is_floating_point<D>::value) return key;
-    else return key - D(1);
 }
 
 template <class T> FT_D T coord_top() {
@@ -381,6 +359,17 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
     D    hmax  = D(0); // the largest distance with that key: at least the k-th distance
     D    thr   = B;    // pruning threshold: B until the heap is full, then min(B, hmax)
     bool flag  = false;
+    // The same threshold on keys (the 4-wide walk prunes, orders and stacks by key): a distance
+    // within thr has a key within kthr (keyed: thr is hmax or B, and d <= hmax gives
+    // key(d) <= hk, d <= B gives key(d) <= key(B); float coordinates: the key is the distance
+    // and kthr is thr rounded up), so a node whose key exceeds kthr is surely beyond thr.
+    const H kB   = heap_keyed<T>() ? heap_key<T>(B) : stack_key_up<D>(B);
+    H       kthr = kB;
+    auto    set_thr = [&]() {
+        thr = hmax < B ? hmax : B;
+        if constexpr (heap_keyed<T>()) kthr = hk < kB ? hk : kB;
+        else kthr = stack_key_up<D>(thr);
+    };
 
     // exact distance of the query to a leaf (by rank), as the walk computes it
     auto exact = [&](int32_t leaf) -> D {
@@ -410,9 +399,9 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
                 }
             }
     };
-    // id: the leaf's rank (original indices are looked up when the rows are written)
-    auto insert = [&](D d2, int32_t id) {
-        const H kd = heap_key<T>(d2);
+    // id: the leaf's rank (original indices are looked up when the rows are written); kd: the
+    // distance's key, heap_key(d2)
+    auto insert_k = [&](D d2, H kd, int32_t id) {
         if (count < k) {
             int i = count;
             while (i > 0) {
@@ -429,7 +418,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             if (count == k) {
                 hk   = HD(0);
                 hmax = heap_key_ub<T>(hk);
-                thr  = hmax < B ? hmax : B;
+                set_thr();
             }
         } else if (kd < hk) {
             if constexpr (heap_keyed<T>() && XB) {
@@ -476,7 +465,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             HI(i) = id;
             hk    = HD(0);
             hmax  = heap_key_ub<T>(hk);
-            thr   = hmax < B ? hmax : B;
+            set_thr();
             // an equal distance stays at the boundary (keyed: the entries left on the old key
             // are exactly nearer than the one evicted, unless tied, flagged above)
             if (!(heap_keyed<T>() && XB) && hk == old) flag = true;
@@ -499,6 +488,7 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             }
         }
     };
+    auto insert = [&](D d2, int32_t id) { insert_k(d2, heap_key<T>(d2), id); };
 
     // ---- 1. seed from the SFC window ----
     const int W  = seeded ? min(n, 2 * half_window + 1) : 0;
@@ -765,12 +755,11 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
         // full stack hands the query to the replay instead of dropping anything.
         constexpr int kWideStack = sizeof(lane_stack) / sizeof(lane_stack[0]);
         const int     ws0 = w0 + n - 1, ws1 = w1 + n - 1; // the seeding window in slot numbers
-        // stack entries: node index in the low word, a float lower bound of its distance in the
-        // high word (one 8-byte local-memory access per push or pop); thr_up is the pruning
-        // threshold rounded up, so a popped node is dropped only when it is surely beyond it
+        // Children are judged, ordered and stacked by their keys (a key is at most the
+        // distance, and within kthr whenever the distance is within thr): stack entries hold the
+        // node index in the low word and its key in the high word (one 8-byte local-memory access
+        // per push or pop), and a popped node is dropped only when its key exceeds kthr.
         unsigned long long *st = lane_stack;
-        float              thr_up = stack_key_up<D>(thr);
-        D                  thr_seen = thr;
         int           cur  = 0;
         int           wsp  = 0;
         bool          have = !group_done && active && n > 1 && needs(sd[0]);
@@ -784,37 +773,41 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
             int ch[4];
             load_wide<T, COH>(t.wide, cur, bx, ch);
             D        d[4];
+            H        kf[4]; // the distances' keys
             bool     in[4]; // needed internal child
             unsigned lm = 0; // leaves to offer to the heap
+            auto needs_k = [&](H key) { return active && !(key > kthr); };
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
                 d[i] = ch[i] >= 0 ? Metric<T>::template dist<(PER != 0), (PER == 2)>(
                                         px, py, pz, bx[i][0], bx[i][1], bx[i][2], bx[i][3], bx[i][4], bx[i][5])
                                   : dist_heap_max<D>();
+                kf[i] = heap_key<T>(d[i]);
                 const bool leaf = ch[i] >= n - 1;
-                if (leaf && needs(d[i]) && (ch[i] < ws0 || ch[i] > ws1) && ch[i] != self_leaf) lm |= 1u << i;
+                if (leaf && needs_k(kf[i]) && (ch[i] < ws0 || ch[i] > ws1) && ch[i] != self_leaf) lm |= 1u << i;
             }
             // one insertion site: lanes whose leaves sit at different child positions insert
             // together (the warp loops as often as its lane with the most leaves)
             while (lm) {
-                const int i = __ffs(lm) - 1;
+                const int i  = __ffs(lm) - 1;
                 lm &= lm - 1;
                 const D   di = i == 0 ? d[0] : i == 1 ? d[1] : i == 2 ? d[2] : d[3];
+                const H   ki = i == 0 ? kf[0] : i == 1 ? kf[1] : i == 2 ? kf[2] : kf[3];
                 const int ci = i == 0 ? ch[0] : i == 1 ? ch[1] : i == 2 ? ch[2] : ch[3];
-                if (needs(di)) insert(di, ci - (n - 1)); // the threshold may have tightened
+                if (needs_k(ki)) insert_k(di, ki, ci - (n - 1)); // the threshold may have tightened
             }
 #pragma unroll
-            for (int i = 0; i < 4; ++i) in[i] = ch[i] >= 0 && ch[i] < n - 1 && needs(d[i]);
-            // order the needed internal children farthest first (4-element network on one
-            // sort key, walk_key: children that are not needed sort behind the needed ones)
+            for (int i = 0; i < 4; ++i) in[i] = ch[i] >= 0 && ch[i] < n - 1 && needs_k(kf[i]);
+            // order the needed internal children farthest first (4-element network on the keys;
+            // children that are not needed, -1, sort behind the needed ones)
             int oc[4] = {ch[0], ch[1], ch[2], ch[3]};
-            D   od[4];
+            H   od[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) od[i] = in[i] ? walk_key<D>(d[i]) : walk_key_none<D>();
+            for (int i = 0; i < 4; ++i) od[i] = in[i] ? kf[i] : H(-1);
             auto cx = [&](int a, int b) {
                 if (od[a] < od[b]) {
                     const int tc = oc[a];
-                    const D   td = od[a];
+                    const H   td = od[a];
                     oc[a]        = oc[b];
                     od[a]        = od[b];
                     oc[b]        = tc;
@@ -835,22 +828,16 @@ FT_D void fast_warp(const int qbase, const QueryList &lst, const MissList &miss,
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
                     if (i < nv - 1) {
-                        st[wsp] = ((unsigned long long)__float_as_uint(stack_key_down<D>(walk_key_dist<D>(od[i])))
-                                   << 32) |
-                                  (uint32_t)oc[i];
+                        st[wsp] = ((unsigned long long)__float_as_uint(od[i]) << 32) | (uint32_t)oc[i];
                         ++wsp;
                     }
                 cur = nv == 1 ? oc[0] : nv == 2 ? oc[1] : nv == 3 ? oc[2] : oc[3];
             } else {
                 have = false;
-                if (thr != thr_seen) { // the heap tightened since the last pop
-                    thr_seen = thr;
-                    thr_up   = stack_key_up<D>(thr);
-                }
                 while (wsp > 0) {
                     --wsp;
                     const unsigned long long e = st[wsp];
-                    if (!(__uint_as_float((uint32_t)(e >> 32)) > thr_up)) {
+                    if (!(__uint_as_float((uint32_t)(e >> 32)) > kthr)) {
                         cur  = (int)(uint32_t)e;
                         have = true;
                         break;
