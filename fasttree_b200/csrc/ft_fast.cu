@@ -37,6 +37,9 @@
 namespace ft {
 
 static constexpr int kFastStack = 64;
+#ifndef FT_XB_MAX_QUERIES
+#define FT_XB_MAX_QUERIES (1 << 21)
+#endif
 #ifndef FT_FAST_MINB
 #define FT_FAST_MINB 10
 #endif
@@ -1119,9 +1122,12 @@ static void launch_fast_t(const TreeDev<T> &tv, const BatchDev &bt, const ExtQue
     using D     = typename Coord<T>::dist_t;
     constexpr int threads = 32 * fast_warps<KC>();
     size_t        smem    = (size_t)std::max(k, 1) * threads * (sizeof(heap_dist_t<T>) + 4); // heaps of k entries
+    // the k-th key settled exactly (XB) for external queries, whose replay is knn_query's heap
+    // tier, and for short launches, where one replay's latency outweighs the settling code
+    const bool xb = eq.x != nullptr || num <= FT_XB_MAX_QUERIES;
     auto   fn   = variant == 0 ? fast_self_knn_kernel<T, PER, KC, 0>
                   : variant == 1 ? fast_self_knn_kernel<T, PER, KC, 1>
-                  : variant == 4 ? (eq.x ? fast_self_knn_kernel<T, PER, KC, 4, true> : fast_self_knn_kernel<T, PER, KC, 4>)
+                  : variant == 4 ? (xb ? fast_self_knn_kernel<T, PER, KC, 4, true> : fast_self_knn_kernel<T, PER, KC, 4>)
                   : variant == 5 ? fast_self_knn_kernel<T, PER, KC, 5>
                                  : fast_self_knn_kernel<T, PER, KC, 2>;
     FT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
