@@ -16,6 +16,9 @@ repeats the comparisons on the bench workloads themselves:
 * 4096 Plummer sets, float32, Morton (65.6M points): the batched build and self-kNN k = 32,
   both methods equal on every row, and 64 sets (the largest among them) against the oracle's
   own build_bvh + self_knn_query of that set alone.
+* 50M clustered uint64 points, Peano-Hilbert, periodic (the large workload, a tree 65 levels
+  tall, where the reference's stack guard can drop subtrees): self-kNN k = 64 on 200,000
+  evenly spaced leaves, both methods equal and the oracle's rows.
 
 The reference tests pin results by brute force on the fly (test/test_self_knn.cpp:153-266);
 the oracle here is the restatement pinned to the reference compiled from its own headers.
@@ -195,4 +198,33 @@ def test_batched_sets_4096():
         assert np.array_equal(fi[a:e].cpu().numpy(), oi), s
         assert np.array_equal(dist_bits(fd[a:e].cpu().numpy()), dist_bits(od)), s
     del b, pi, pd, fi, fd
+    torch.cuda.empty_cache()
+
+
+# -----------------------------------------------------------------------------------------
+# 50M clustered uint64 points (a tree taller than 62 levels)
+# -----------------------------------------------------------------------------------------
+def test_large_tall_tree_sample():
+    n, k = 50_000_000, 64
+    x, y, z = datasets.clustered_fixed(n, n_spheres=100_000, seed=5)
+    ctx = ft.Context("u64", "ph", periodic=True)
+    tree = ft.TreeSoA(ctx, n)
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree)
+    assert tree.height() > 62, tree.height()
+    ids = np.linspace(0, n - 1, SAMPLE).astype(np.int32)
+    t = torch.from_numpy(ids).cuda()
+    fi, fd = ft.self_knn_query_subset(ctx, tree, t, k, max_k=k, method="fast")
+    replayed = len(ctx.replayed_queries())
+    pi, pd = ft.self_knn_query_subset(ctx, tree, t, k, max_k=k, method="plain")
+    ctx.check_device_status()
+    assert _rows_equal(fi, fd, pi, pd)
+    assert replayed < SAMPLE // 10, replayed  # the guard hands only some queries to the replay
+    _threads()
+    opts = O.Options(O.U64, O.PEANO_HILBERT, True)
+    ot = O.build_bvh(opts, x, y, z)
+    oi, od = O.self_knn(opts, ot, k, True, leaf_ids=ids)
+    gi, gd = fi.cpu().numpy(), fd.cpu().numpy()
+    assert np.array_equal(gi, oi), f"first differing sampled row {ids[np.argmax((gi != oi).any(1))]}"
+    assert np.array_equal(dist_bits(gd), dist_bits(od))
+    del tree, fi, fd, pi, pd
     torch.cuda.empty_cache()
