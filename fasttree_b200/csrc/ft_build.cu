@@ -456,17 +456,58 @@ __global__ void __launch_bounds__(256) karras_kernel(const unsigned long long *_
 }
 
 // =========================================================================================
-// Bottom-up refit (src/hlbvh.hpp:925-969), one thread per leaf (refit_leaf).
+// Bottom-up refit (src/hlbvh.hpp:925-969): climbs from the leaves, refit_step per level.
 // =========================================================================================
+// A climb ends at its first arrival at a node, so one thread per leaf (refit_leaf) leaves most
+// lanes of a warp idle while its longest climb goes on (about 5 of 32 lanes active).  Here the
+// warps of a grid of a few blocks per SM take leaves in chunks from a device counter (*work,
+// zero at launch), and a lane whose climb ended takes the warp's next leaf: one climb step
+// per lane and loop iteration.  The merges,
+// boxes, records and heights are those of one climb per leaf (min / max do not depend on the
+// order of the arrivals).
 template <class T>
-__global__ void __launch_bounds__(256) refit_kernel(int n, const int32_t *__restrict__ left,
-                                                    const int32_t *__restrict__ right,
-                                                    const int32_t *__restrict__ parent, T *mnx, T *mxx, T *mny,
-                                                    T *mxy, T *mnz, T *mxz, NodeRec<T> *recs, uint8_t *height,
-                                                    int32_t *counters, const int32_t *__restrict__ leaves) {
-    T *const soa[6] = {mnx, mxx, mny, mxy, mnz, mxz};
-    for (int leaf = blockIdx.x * blockDim.x + threadIdx.x; leaf < n; leaf += gridDim.x * blockDim.x)
-        refit_leaf<T>(leaf, n, left, right, parent, soa, recs, height, counters, leaves);
+__global__ void __launch_bounds__(256) refit_stream_kernel(int n, const int32_t *__restrict__ left,
+                                                           const int32_t *__restrict__ right,
+                                                           const int32_t *__restrict__ parent, T *mnx, T *mxx,
+                                                           T *mny, T *mxy, T *mnz, T *mxz, NodeRec<T> *recs,
+                                                           uint8_t *height, int32_t *counters,
+                                                           const int32_t *__restrict__ leaves, int32_t *work) {
+    T *const       soa[6] = {mnx, mxx, mny, mxy, mnz, mxz};
+    const unsigned FULL   = 0xffffffffu;
+    const int      lane   = threadIdx.x & 31;
+    constexpr int  kChunk = 256;
+    int            next = 0, end = 0; // the warp's chunk of leaves [next, end) (warp-uniform)
+    bool           more = true;       // the counter may still hold leaves (warp-uniform)
+    int            curr = -1, steps = 0;
+    for (;;) {
+        // lanes without a climb take the chunk's next leaves, in lane order
+        unsigned idle = __ballot_sync(FULL, curr < 0);
+        while (idle && more) {
+            if (next >= end) {
+                int b = 0;
+                if (lane == 0) b = atomicAdd(work, kChunk);
+                b = __shfl_sync(FULL, b, 0);
+                if (b >= n) {
+                    more = false;
+                    break;
+                }
+                next = b;
+                end  = min(b + kChunk, n);
+            }
+            const int take = min(__popc(idle), end - next);
+            const int rank = __popc(idle & ((1u << lane) - 1u));
+            if (curr < 0 && rank < take) {
+                curr  = next + rank + n - 1;
+                steps = 0;
+            }
+            next += take;
+            idle = __ballot_sync(FULL, curr < 0);
+        }
+        if (!__any_sync(FULL, curr >= 0)) break;
+        if (curr >= 0) curr = ++steps < n ? refit_step<T>(curr, n, left, right, parent, soa, recs, height, counters,
+                                                           leaves)
+                                          : -1;
+    }
 }
 
 // 4-wide records of every internal node (collapse_node), after the refit.
@@ -817,11 +858,12 @@ static void topology_and_refit(const ft_options &o, ft_tree &t, TreeImpl &s, siz
     }
     FT_CUDA(cudaGetLastError());
     stage_mark(prof, BS_TOPOLOGY, st);
-    FT_CUDA(cudaMemsetAsync(s.counters, 0, (n - 1) * sizeof(int32_t), st));
+    // arrival counters of the n - 1 internal nodes, then the streaming refit's leaf counter
+    FT_CUDA(cudaMemsetAsync(s.counters, 0, n * sizeof(int32_t), st));
     SoA<T> a(t);
-    refit_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, t.parent, a.mnx, a.mxx, a.mny,
-                                            a.mxy, a.mnz, a.mxz, (NodeRec<T> *)s.recs, s.height, s.counters,
-                                            s.leafcount);
+    refit_stream_kernel<T><<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(
+        (int)n, t.left_child, t.right_child, t.parent, a.mnx, a.mxx, a.mny, a.mxy, a.mnz, a.mxz,
+        (NodeRec<T> *)s.recs, s.height, s.counters, s.leafcount, s.counters + (n - 1));
     stage_mark(prof, BS_REFIT, st);
     collapse_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, a.mnx, a.mxx, a.mny, a.mxy,
                                                a.mnz, a.mxz, (WideRec<T> *)s.wide);
@@ -932,10 +974,10 @@ static void refit_typed(ft_tree &t, const void *x, const void *y, const void *z,
     FT_CUDA(cudaGetLastError());
     if (n < 2) return;
     const int blocks = grid_for(n, 256, 148 * 32);
-    FT_CUDA(cudaMemsetAsync(s.counters, 0, (n - 1) * sizeof(int32_t), st));
-    refit_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, t.parent, a.mnx, a.mxx, a.mny,
-                                            a.mxy, a.mnz, a.mxz, (NodeRec<T> *)s.recs, s.height, s.counters,
-                                            s.leafcount);
+    FT_CUDA(cudaMemsetAsync(s.counters, 0, n * sizeof(int32_t), st));
+    refit_stream_kernel<T><<<grid_for(n, 256, 148 * 8), 256, 0, st>>>(
+        (int)n, t.left_child, t.right_child, t.parent, a.mnx, a.mxx, a.mny, a.mxy, a.mnz, a.mxz,
+        (NodeRec<T> *)s.recs, s.height, s.counters, s.leafcount, s.counters + (n - 1));
     collapse_kernel<T><<<blocks, 256, 0, st>>>((int)n, t.left_child, t.right_child, a.mnx, a.mxx, a.mny, a.mxy,
                                                a.mnz, a.mxz, (WideRec<T> *)s.wide);
     FT_CUDA(cudaGetLastError());

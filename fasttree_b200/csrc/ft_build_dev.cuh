@@ -243,53 +243,71 @@ FT_D int atomic_add_acq_rel(int32_t *p, int v) {
     return old;
 }
 
+// The merge at internal node p (both children's boxes are final): p's box, its traversal
+// record (both child boxes and indices, leaf counts and heights) and its height.
+template <class T>
+FT_D void refit_merge(int p, int n, const int32_t *__restrict__ left, const int32_t *__restrict__ right,
+                      T *const *soa, NodeRec<T> *recs, uint8_t *height, const int32_t *__restrict__ leaves) {
+    int l = left[p], r = right[p];
+    T   lb[6], rb[6];
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+        lb[d] = __ldcg(soa[d] + l);
+        rb[d] = __ldcg(soa[d] + r);
+    }
+    int hl = (l >= n - 1) ? 0 : (int)__ldcg(height + l);
+    int hr = (r >= n - 1) ? 0 : (int)__ldcg(height + r);
+    T   pb[6];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        pb[2 * d]     = box_min(lb[2 * d], rb[2 * d]);
+        pb[2 * d + 1] = box_max(lb[2 * d + 1], rb[2 * d + 1]);
+    }
+#pragma unroll
+    for (int d = 0; d < 6; ++d) __stcg(soa[d] + p, pb[d]);
+    NodeRec<T> rec;
+#pragma unroll
+    for (int d = 0; d < 6; ++d) {
+        rec.lb[d] = lb[d];
+        rec.rb[d] = rb[d];
+    }
+    rec.l = l;
+    rec.r = r;
+#pragma unroll
+    for (int d = 0; d < (int)(sizeof(rec.pad) / 4); ++d) rec.pad[d] = 0;
+    // leaf counts (the Karras ranges) and heights of both children
+    rec.pad[0] = (int32_t)rec_child_info(l >= n - 1 ? 1u : (uint32_t)leaves[l], (uint32_t)hl);
+    rec.pad[1] = (int32_t)rec_child_info(r >= n - 1 ? 1u : (uint32_t)leaves[r], (uint32_t)hr);
+    recs[p] = rec;
+    int h   = 1 + max(hl, hr);
+    __stcg(height + p, (uint8_t)min(h, 255));
+}
+
+// One step of a climb at node curr: the arrival at its parent.  Returns the parent when this
+// arrival is the second (the merge is done, the climb goes on), else -1 (first arrival, the
+// root, or a bad parent: the climb ends).
+template <class T>
+FT_D int refit_step(int curr, int n, const int32_t *__restrict__ left, const int32_t *__restrict__ right,
+                    const int32_t *__restrict__ parent, T *const *soa, NodeRec<T> *recs, uint8_t *height,
+                    int32_t *counters, const int32_t *__restrict__ leaves) {
+    if (curr == 0) return -1;
+    const int p = parent[curr];
+    if (p < 0 || p >= n - 1) return -1;
+    // one acquire-release arrival: this thread's writes of curr are released to the sibling
+    // that arrives second, and the second arrival acquires the first's writes
+    if (atomic_add_acq_rel(&counters[p], 1) == 0) return -1;
+    refit_merge<T>(p, n, left, right, soa, recs, height, leaves);
+    return p;
+}
+
 template <class T>
 FT_D void refit_leaf(int leaf, int n, const int32_t *__restrict__ left, const int32_t *__restrict__ right,
                      const int32_t *__restrict__ parent, T *const *soa, NodeRec<T> *recs, uint8_t *height,
                      int32_t *counters, const int32_t *__restrict__ leaves) {
     int curr  = leaf + n - 1;
     int steps = 0;
-    while (curr != 0 && ++steps < n) {
-        int p = parent[curr];
-        if (p < 0 || p >= n - 1) break;
-        // one acquire-release arrival: this thread's writes of curr are released to the sibling
-        // that arrives second, and the second arrival acquires the first's writes
-        if (atomic_add_acq_rel(&counters[p], 1) == 0) break;
-        int l = left[p], r = right[p];
-        T   lb[6], rb[6];
-#pragma unroll
-        for (int d = 0; d < 6; ++d) {
-            lb[d] = __ldcg(soa[d] + l);
-            rb[d] = __ldcg(soa[d] + r);
-        }
-        int hl = (l >= n - 1) ? 0 : (int)__ldcg(height + l);
-        int hr = (r >= n - 1) ? 0 : (int)__ldcg(height + r);
-        T   pb[6];
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            pb[2 * d]     = box_min(lb[2 * d], rb[2 * d]);
-            pb[2 * d + 1] = box_max(lb[2 * d + 1], rb[2 * d + 1]);
-        }
-#pragma unroll
-        for (int d = 0; d < 6; ++d) __stcg(soa[d] + p, pb[d]);
-        NodeRec<T> rec;
-#pragma unroll
-        for (int d = 0; d < 6; ++d) {
-            rec.lb[d] = lb[d];
-            rec.rb[d] = rb[d];
-        }
-        rec.l = l;
-        rec.r = r;
-#pragma unroll
-        for (int d = 0; d < (int)(sizeof(rec.pad) / 4); ++d) rec.pad[d] = 0;
-        // leaf counts (the Karras ranges) and heights of both children
-        rec.pad[0] = (int32_t)rec_child_info(l >= n - 1 ? 1u : (uint32_t)leaves[l], (uint32_t)hl);
-        rec.pad[1] = (int32_t)rec_child_info(r >= n - 1 ? 1u : (uint32_t)leaves[r], (uint32_t)hr);
-        recs[p] = rec;
-        int h   = 1 + max(hl, hr);
-        __stcg(height + p, (uint8_t)min(h, 255));
-        curr = p;
-    }
+    while (curr >= 0 && ++steps < n)
+        curr = refit_step<T>(curr, n, left, right, parent, soa, recs, height, counters, leaves);
 }
 
 
