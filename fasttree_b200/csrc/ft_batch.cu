@@ -233,23 +233,63 @@ __global__ void __launch_bounds__(256)
 }
 
 // =========================================================================================
-// 7. refit per leaf of every set with >= 2 leaves, then the root height of each set
+// 7. refit of every set with >= 2 leaves (climbs from its leaves), then the root height of
+//    each set
 // =========================================================================================
+// The same refit with every lane kept busy (as refit_stream_kernel for one tree): warps take
+// leaves in chunks from a device counter (*work, zero at launch) and a lane whose climb ended
+// takes the next leaf, finding its set by binary search over the offsets.
 template <class T>
 __global__ void __launch_bounds__(256)
-    batch_refit_kernel(const long long *__restrict__ off, const long long *__restrict__ node_off,
-                       const long long *__restrict__ rec_off, int S, long long N, const int32_t *__restrict__ left,
-                       const int32_t *__restrict__ right, const int32_t *__restrict__ parent, T *mnx, T *mxx, T *mny,
-                       T *mxy, T *mnz, T *mxz, NodeRec<T> *recs, uint8_t *height, int32_t *counters,
-                       const int32_t *__restrict__ leaves) {
-    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < N; j += (long long)gridDim.x * blockDim.x) {
-        const int       s = find_set(off, S, j);
-        const int       n = (int)(off[s + 1] - off[s]);
-        if (n < 2) continue;
-        const long long no = node_off[s], ro = rec_off[s];
-        T *const soa[6] = {mnx + no, mxx + no, mny + no, mxy + no, mnz + no, mxz + no};
-        refit_leaf<T>((int)(j - off[s]), n, left + ro, right + ro, parent + no, soa, recs + ro, height + ro,
-                      counters + ro, leaves + ro);
+    batch_refit_stream_kernel(const long long *__restrict__ off, const long long *__restrict__ node_off,
+                              const long long *__restrict__ rec_off, int S, long long N,
+                              const int32_t *__restrict__ left, const int32_t *__restrict__ right,
+                              const int32_t *__restrict__ parent, T *mnx, T *mxx, T *mny, T *mxy, T *mnz, T *mxz,
+                              NodeRec<T> *recs, uint8_t *height, int32_t *counters,
+                              const int32_t *__restrict__ leaves, int32_t *work) {
+    const unsigned FULL   = 0xffffffffu;
+    const int      lane   = threadIdx.x & 31;
+    constexpr int  kChunk = 256;
+    const int      total  = (int)N; // at most 2^30 (batch_create)
+    int            next = 0, end = 0;
+    bool           more = true;
+    int            curr = -1, steps = 0, n = 0;
+    long long      no = 0, ro = 0;
+    for (;;) {
+        unsigned idle = __ballot_sync(FULL, curr < 0);
+        while (idle && more) {
+            if (next >= end) {
+                int b = 0;
+                if (lane == 0) b = atomicAdd(work, kChunk);
+                b = __shfl_sync(FULL, b, 0);
+                if (b >= total) {
+                    more = false;
+                    break;
+                }
+                next = b;
+                end  = min(b + kChunk, total);
+            }
+            const int take = min(__popc(idle), end - next);
+            const int rank = __popc(idle & ((1u << lane) - 1u));
+            if (curr < 0 && rank < take) {
+                const long long g = next + rank;
+                const int       s = find_set(off, S, g);
+                n                 = (int)(off[s + 1] - off[s]);
+                no                = node_off[s];
+                ro                = rec_off[s];
+                curr              = n >= 2 ? (int)(g - off[s]) + n - 1 : -1; // one-leaf sets have no refit
+                steps             = 0;
+            }
+            next += take;
+            idle = __ballot_sync(FULL, curr < 0);
+        }
+        if (!__any_sync(FULL, curr >= 0)) break;
+        if (curr >= 0) {
+            T *const soa[6] = {mnx + no, mxx + no, mny + no, mxy + no, mnz + no, mxz + no};
+            curr = ++steps < n ? refit_step<T>(curr, n, left + ro, right + ro, parent + no, soa, recs + ro,
+                                               height + ro, counters + ro, leaves + ro)
+                               : -1;
+        }
     }
 }
 
@@ -524,10 +564,12 @@ static void batch_build_typed(Context &ctx, BatchImpl &b, const long long *in_of
                                                    (const unsigned long long *)s.key_lo, t.left_child, t.right_child,
                                                    t.parent, s.leafcount);
     FT_CUDA(cudaGetLastError());
+    // arrival counters of the sets' internal nodes (at most N - 1 of them), and in the last
+    // slot the streaming refit's leaf counter
     FT_CUDA(cudaMemsetAsync(s.counters, 0, (size_t)N * sizeof(int32_t), st));
-    batch_refit_kernel<T><<<gK, 256, 0, st>>>(b.off, b.node_off, b.rec_off, S, N, t.left_child, t.right_child,
-                                              t.parent, mnx, mxx, mny, mxy, mnz, mxz, (NodeRec<T> *)s.recs, s.height,
-                                              s.counters, s.leafcount);
+    batch_refit_stream_kernel<T><<<grid_of((size_t)N, 256, sm * 8), 256, 0, st>>>(
+        b.off, b.node_off, b.rec_off, S, N, t.left_child, t.right_child, t.parent, mnx, mxx, mny, mxy, mnz, mxz,
+        (NodeRec<T> *)s.recs, s.height, s.counters, s.leafcount, s.counters + (N - 1));
     batch_collapse_kernel<T><<<gK, 256, 0, st>>>(b.off, b.node_off, b.rec_off, S, N, t.left_child, t.right_child,
                                                  mnx, mxx, mny, mxy, mnz, mxz, (WideRec<T> *)s.wide);
     batch_heights_kernel<<<grid_of((size_t)S, 256, sm * 4), 256, 0, st>>>(b.off, b.rec_off, S, s.height,
