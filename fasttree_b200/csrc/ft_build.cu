@@ -462,9 +462,8 @@ __global__ void __launch_bounds__(256) karras_kernel(const unsigned long long *_
 // lanes of a warp idle while its longest climb goes on (about 5 of 32 lanes active).  Here the
 // warps of a grid of a few blocks per SM take leaves in chunks from a device counter (*work,
 // zero at launch), and a lane whose climb ended takes the warp's next leaf: one climb step
-// per lane and loop iteration.  The merges,
-// boxes, records and heights are those of one climb per leaf (min / max do not depend on the
-// order of the arrivals).
+// per lane and loop iteration.  The merges, boxes, records and heights are those of one climb
+// per leaf (min / max do not depend on the order of the arrivals).
 template <class T>
 __global__ void __launch_bounds__(256) refit_stream_kernel(int n, const int32_t *__restrict__ left,
                                                            const int32_t *__restrict__ right,
