@@ -19,6 +19,9 @@ repeats the comparisons on the bench workloads themselves:
 * 50M clustered uint64 points, Peano-Hilbert, periodic (the large workload, a tree 65 levels
   tall, where the reference's stack guard can drop subtrees): self-kNN k = 64 on 200,000
   evenly spaced leaves, both methods equal and the oracle's rows.
+* 2.2M clustered float64 and uint32 points: launches above 2^21 queries, where the walk
+  flags equal heap keys for the replay instead of settling them; both methods equal on every
+  row, the oracle on a sample plus every replayed query.
 
 The reference tests pin results by brute force on the fly (test/test_self_knn.cpp:153-266);
 the oracle here is the restatement pinned to the reference compiled from its own headers.
@@ -227,4 +230,38 @@ def test_large_tall_tree_sample():
     assert np.array_equal(gi, oi), f"first differing sampled row {ids[np.argmax((gi != oi).any(1))]}"
     assert np.array_equal(dist_bits(gd), dist_bits(od))
     del tree, fi, fd, pi, pd
+    torch.cuda.empty_cache()
+
+
+# -----------------------------------------------------------------------------------------
+# launches above 2^21 queries keep the flag-only keyed heap: float64 and uint32 coordinates
+# -----------------------------------------------------------------------------------------
+@pytest.mark.parametrize("coord,sfc,per,oc,os_,k", [("f64", "morton", False, O.F64, O.MORTON, 16),
+                                                    ("u32", "ph", True, O.U32, O.PEANO_HILBERT, 32)],
+                         ids=["f64-k16", "u32-per-k32"])
+def test_large_launch_keyed_heap(coord, sfc, per, oc, os_, k):
+    """Self-kNN of 2.2M points (a launch above the 2^21 queries below which the walk settles
+    the k-th key exactly): equal heap keys go to the replay; every row equal to the plain
+    traversal's, and the oracle's on a sample plus every replayed query."""
+    from tests.gpu_util import gen
+    n = 2_200_000
+    x, y, z = gen("clustered", n, oc, 31)
+    ctx = ft.Context(coord, sfc, periodic=per)
+    tree = ft.TreeSoA(ctx, n)
+    ft.build_bvh(ctx, ft.particles(x, y, z), tree)
+    pi, pd = ft.self_knn_query(ctx, tree, k, max_k=32, method="plain")
+    fi, fd = torch.empty_like(pi), torch.empty_like(pd)
+    ft.self_knn_query(ctx, tree, k, fi, fd, max_k=32, method="fast")
+    replayed = ctx.replayed_queries()
+    ctx.check_device_status()
+    assert _rows_equal(fi, fd, pi, pd)
+    _threads()
+    opts = O.Options(oc, os_, per)
+    ot = O.build_bvh(opts, x, y, z)
+    ids = _sample_rows(n, replayed, 100_000)
+    oi, od = O.self_knn(opts, ot, k, True, leaf_ids=ids)
+    t = torch.from_numpy(ids.astype(np.int64)).to(fi.device)
+    assert np.array_equal(fi.index_select(0, t).cpu().numpy(), oi)
+    assert np.array_equal(dist_bits(fd.index_select(0, t).cpu().numpy()), dist_bits(od))
+    del tree, pi, pd, fi, fd
     torch.cuda.empty_cache()
