@@ -148,11 +148,13 @@ static constexpr int kTicketWords = 64;
 static constexpr uint32_t kFlagAgg = 1u << 30, kFlagInc = 2u << 30, kFlagMask = 3u << 30,
                           kCountMask = (1u << 30) - 1u;
 
-// A onesweep tile: 256 threads x ITEMS keys (ITEMS 0: the default for the key width, 16 for
-// one-word keys and 12 for two-word keys).  The build's sort takes the tile the autotuner
-// chose for the shape (sort_items); every tile size gives the same order.
+// A onesweep tile: 256 threads x ITEMS keys (ITEMS 0: the default, 8; the autotuner chose 8
+// on every shape measured -- 100K float64 Morton, 10M and 50M uint64 Peano-Hilbert points --
+// where the larger tiles' registers leave one block per SM: 10M points, untuned 12-key tiles
+// 2.83 ms against 2.15 ms).  The build's sort takes the tile the autotuner chose for the shape
+// (sort_items); every tile size gives the same order.
 template <int W, int ITEMS = 0> struct SortCfg {
-    static constexpr int items = ITEMS ? ITEMS : (W == 1) ? 16 : 12;
+    static constexpr int items = ITEMS ? ITEMS : 8;
     static constexpr int tile  = kSortThreads * items;
     static constexpr size_t smem = (size_t)tile * (8 * W + 4) + (size_t)kSortWarps * 256 * 4;
 };
@@ -810,22 +812,22 @@ static void sort_keys(const ft_options &o, TreeImpl &s, size_t n, cudaStream_t s
     if (n < 2) return;
     if (key_words(o) == 1) {
         switch (items) {
-        case 8: sort_impl<1, 8>(s, n, st); break;
         case 12: sort_impl<1, 12>(s, n, st); break;
+        case 16: sort_impl<1, 16>(s, n, st); break;
         case 20: sort_impl<1, 20>(s, n, st); break;
-        default: sort_impl<1>(s, n, st); break; // 16
+        default: sort_impl<1>(s, n, st); break; // 8
         }
     } else {
         switch (items) {
-        case 8: sort_impl<2, 8>(s, n, st); break;
+        case 12: sort_impl<2, 12>(s, n, st); break;
         case 16: sort_impl<2, 16>(s, n, st); break;
-        default: sort_impl<2>(s, n, st); break; // 12
+        default: sort_impl<2>(s, n, st); break; // 8
         }
     }
 }
 
 const int *sort_item_choices(int words, int *count) {
-    static const int one[4] = {16, 8, 12, 20}, two[3] = {12, 8, 16}; // the default first
+    static const int one[4] = {8, 12, 16, 20}, two[3] = {8, 12, 16}; // the default first
     *count = words == 1 ? 4 : 3;
     return words == 1 ? one : two;
 }
