@@ -229,8 +229,9 @@ FT_D void st_volatile(uint32_t *p, uint32_t v) { asm volatile("st.volatile.globa
 //    fallback, which only runs when a long run of equal high words was found);
 //  * skip (null or a device word): 1 when one digit value holds every key -- the pass then
 //    copies its tiles unchanged, so the ping-pong order the host planned still holds.
+// (8-key tiles are compiled for three resident blocks: 80 registers, no spills, 24 warps per SM)
 template <int W, int IT = 0>
-__global__ void __launch_bounds__(kSortThreads, 1)
+__global__ void __launch_bounds__(kSortThreads, (SortCfg<W, IT>::items <= 8 ? 3 : 1))
     onesweep_kernel(const unsigned long long *__restrict__ in_lo, const unsigned long long *__restrict__ in_hi,
                     const uint32_t *__restrict__ in_v, unsigned long long *__restrict__ out_lo,
                     unsigned long long *__restrict__ out_hi, uint32_t *__restrict__ out_v, size_t n, size_t num_tiles,
