@@ -835,15 +835,16 @@ template <class T, int PER> FT_D float group_off(T v, const RangeGroup<T> &g, in
 }
 
 // range_split_kernel's shape: two-warp blocks (a block keeps its SM slots until its slowest
-// warp ends, and the warps' work is very uneven) compiled for 10 resident blocks (102
-// registers a thread).  Measured on 10M clustered points, all N queries, back to back on one
-// GPU: 4-warp blocks 2.83 s, 2-warp 2.85 s, 1-warp 2.80 s (123 registers each), 2-warp with
-// 10 / 12 resident blocks 2.42 / 2.44 s.
+// warp ends, and the warps' work is very uneven) compiled for 8 resident blocks (124
+// registers a thread, no spills).  Measured on 10M clustered points, all N queries, back to
+// back on one GPU: 4-warp blocks 2.83 s, 2-warp 2.85 s, 1-warp 2.80 s (123 registers each),
+// 2-warp with 10 / 12 resident blocks 2.42 / 2.44 s; with the threshold leaf filter, 8 / 10 /
+// 12 resident blocks 1.93 / 2.05 / 2.11 s (the tighter budgets spill).
 #ifndef FT_RANGE_WARPS
 #define FT_RANGE_WARPS 2
 #endif
 #ifndef FT_RANGE_MINB
-#define FT_RANGE_MINB 10
+#define FT_RANGE_MINB 8
 #endif
 static constexpr int kRangeWarps = FT_RANGE_WARPS, kRangeGStack = 512, kRangeStage = 256;
 // The group counts a warp's full rows together when its points' largest axis extent is at
